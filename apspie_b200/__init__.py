@@ -1,0 +1,17 @@
+"""apspie_b200 -- B200-native (sm_100a) SpMSpV / hash-SpGEMM hot path of apspie.
+
+Python mirror of the reference's host entry points on top of the C ABI in
+include/apspie.h (libapspie_b200.so).  Device arrays are torch tensors (torch
+is the device allocator and stream provider only); every compute call goes
+through the native library, which raises on import if it is not built.
+"""
+from ._native import ApspieError, lib  # noqa: F401  (raises if the .so is missing)
+from .graph import (DeviceGraph, HostGraph, from_edges, gen_er, gen_grid, gen_rmat,  # noqa: F401
+                    largest_cc_vertex, mt19937, read_mtx, seeded_sources, weights_f32, weights_u32)
+from .ops import Context, bfs, bfs_set_params, bfs_stats  # noqa: F401
+
+__all__ = [
+    "ApspieError", "Context", "DeviceGraph", "HostGraph", "bfs", "bfs_set_params", "bfs_stats", "from_edges",
+    "gen_er", "gen_grid", "gen_rmat", "largest_cc_vertex", "mt19937", "read_mtx", "seeded_sources",
+    "weights_f32", "weights_u32",
+]

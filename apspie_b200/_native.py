@@ -1,0 +1,76 @@
+"""ctypes binding of libapspie_b200.so (the C ABI declared in include/apspie.h).
+
+The library is built in-tree by ``python -m apspie_b200.build``.  There is no
+fallback: importing this module raises if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libapspie_b200.so"
+
+if not LIB_PATH.exists():
+    raise ImportError(
+        f"apspie_b200 native library not built: {LIB_PATH} is missing "
+        "(run `python apspie_b200/build.py`)")
+
+lib = C.CDLL(str(LIB_PATH))
+
+c_int, c_i64, c_u64, c_u32, c_f32 = C.c_int, C.c_int64, C.c_uint64, C.c_uint32, C.c_float
+vp = C.c_void_p
+P_int = C.POINTER(C.c_int)
+P_i64 = C.POINTER(C.c_int64)
+P_u64 = C.POINTER(C.c_uint64)
+P_size = C.POINTER(C.c_size_t)
+P_vp = C.POINTER(C.c_void_p)
+
+
+class BfsStats(C.Structure):
+    _fields_ = [("levels", C.c_int32), ("pull_levels", C.c_int32),
+                ("vertices_reached", C.c_int64), ("edges_traversed", C.c_int64)]
+
+
+# name -> (restype, argtypes); every symbol declared in include/apspie.h
+PROTOS: dict[str, tuple] = {
+    "apspie_ctx_create": (c_int, [c_int, vp, P_vp]),
+    "apspie_ctx_destroy": (c_int, [vp]),
+    "apspie_ctx_set_stream": (c_int, [vp, vp]),
+    "apspie_ctx_sync": (c_int, [vp]),
+    "apspie_ctx_launch_count": (c_int, [vp, P_u64]),
+    "apspie_ctx_workspace_bytes": (c_int, [vp, P_size]),
+    "apspie_last_error": (C.c_char_p, [vp]),
+    "apspie_status_string": (C.c_char_p, [c_int]),
+    "apspie_bfs": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, c_int]),
+    "apspie_bfs_get_stats": (c_int, [vp, C.POINTER(BfsStats)]),
+    "apspie_bfs_set_params": (c_int, [vp, c_int, c_int, c_int]),
+    "apspie_gen_rmat_host": (c_int, [c_int, c_int, c_u64, c_int, c_int, P_int, P_i64, P_vp, P_vp]),
+    "apspie_gen_er_host": (c_int, [c_int, c_int, c_u64, P_i64, P_vp, P_vp]),
+    "apspie_gen_grid_host": (c_int, [c_int, c_int, P_i64, P_vp, P_vp]),
+    "apspie_gen_weights_u32_host": (c_int, [c_int, vp, vp, c_u64, c_u32, c_u32, vp]),
+    "apspie_gen_weights_f32_host": (c_int, [c_int, vp, vp, c_u64, vp]),
+    "apspie_mt19937_fill_host": (c_int, [c_u32, c_i64, vp]),
+    "apspie_read_mtx_host": (c_int, [C.c_char_p, c_int, P_int, P_i64, P_vp, P_vp, P_vp, P_int]),
+    "apspie_host_free": (None, [vp]),
+}
+
+for _name, (_res, _args) in PROTOS.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+class ApspieError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+def check(status: int, ctx=None, what: str = "") -> None:
+    if status != 0:
+        detail = ""
+        if ctx is not None:
+            detail = (lib.apspie_last_error(ctx) or b"").decode()
+        if not detail:
+            detail = (lib.apspie_status_string(status) or b"").decode()
+        raise ApspieError(status, f"{what}: {detail}" if what else detail)

@@ -1,0 +1,340 @@
+// bfs.cu -- direction-optimising BFS as one persistent kernel per traversal.
+//
+// Replaces the reference's level loop of mXv + addResult (src/bfs.cuh:87-110)
+// and the keys-only spmspvBfs (src/spmspvBfs.cuh:150-224).  The reference does
+// ~15 launches, 3 host syncs and a cudaMalloc per level; here one cooperative
+// kernel runs every level, separated by a bounded software grid barrier.
+//
+// Per level L (frontier = vertices with depth L):
+//   push (top-down): the frontier queue is expanded with a warp-level
+//     scan-based gather (32 queued vertices per warp, edges dealt round-robin
+//     to lanes, coalesced reads of the column segments); vertices of degree
+//     > kBigDeg are split into kChunk-edge chunks shared by all warps.
+//     Discovery is an atomicCAS on depth (the visited mask update fused into
+//     the SpMSpV, replacing addResult, src/bfs.cuh:16-24).
+//   pull (bottom-up): every unvisited vertex scans its neighbours, one warp
+//     per vertex, until one has depth L (ballot early exit).
+// The switch follows Beamer's rule: push->pull when the frontier's edges
+// exceed (unexplored edges)/alpha, pull->push when the frontier has fewer
+// than m/beta vertices.  Discovered vertices are appended to the next queue
+// with one atomic per warp; the per-level counters rotate over three slots so
+// no block reads a counter while another resets it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "context.h"
+
+namespace apspie {
+namespace {
+
+constexpr int kBfsThreads = 512;
+constexpr int kBigDeg = 1024;  // out-degree above which a vertex is chunked
+constexpr int kChunk = 1024;   // edges per chunk
+
+struct LevelCounters {
+  unsigned q;        // frontier vertices in the queue (degree <= kBigDeg)
+  unsigned chunks;   // entries in the chunk list
+  unsigned nbig;     // frontier vertices in the chunk list
+  unsigned pad;
+  unsigned long long edges;  // sum of out-degrees of the frontier
+};
+
+struct BfsState {
+  LevelCounters c[3];
+  unsigned bar[2];
+  int err;
+  int levels;
+  int pull_levels;
+  int pad;
+  unsigned long long reached;
+  unsigned long long edges;
+};
+
+__device__ __forceinline__ void discover(bool found, int u, const int *__restrict__ ptr,
+                                         int *qout, int2 *cout, LevelCounters *nxt) {
+  int deg = 0;
+  if (found) deg = __ldg(ptr + u + 1) - __ldg(ptr + u);
+  bool big = found && deg > kBigDeg;
+  bool small = found && !big;
+  unsigned slot = warp_append(small, &nxt->q);
+  if (small) qout[slot] = u;
+  if (big) {
+    int nch = (deg + kChunk - 1) / kChunk;
+    unsigned base = atomicAdd(&nxt->chunks, (unsigned)nch);
+    atomicAdd(&nxt->nbig, 1u);
+    for (int j = 0; j < nch; ++j) cout[base + j] = make_int2(u, j);
+  }
+  unsigned long long e = warp_sum((unsigned long long)deg);
+  if (lane_id() == 0 && e) atomicAdd(&nxt->edges, e);
+}
+
+__device__ __forceinline__ bool claim(int u, int level, int32_t *depth) {
+  if (__ldcg(depth + u) != -1) return false;
+  return atomicCAS(depth + u, -1, level) == -1;
+}
+
+__global__ void bfs_init(int m, int src, int32_t *depth, const int *__restrict__ ptr,
+                         int *queue, int2 *chunks, BfsState *st) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < m; v += gridDim.x * blockDim.x)
+    depth[v] = (v == src) ? 0 : -1;
+  if (blockIdx.x == 0) {
+    int deg = __ldg(ptr + src + 1) - __ldg(ptr + src);
+    int nch = deg > kBigDeg ? (deg + kChunk - 1) / kChunk : 0;
+    for (int j = threadIdx.x; j < nch; j += blockDim.x) chunks[j] = make_int2(src, j);
+    if (threadIdx.x == 0) {
+      for (int i = 0; i < 3; ++i) st->c[i] = LevelCounters{0, 0, 0, 0, 0ull};
+      if (nch) {
+        st->c[0].chunks = (unsigned)nch;
+        st->c[0].nbig = 1;
+      } else {
+        queue[0] = src;
+        st->c[0].q = 1;
+      }
+      st->c[0].edges = (unsigned long long)deg;
+      st->bar[0] = st->bar[1] = 0;
+      st->err = 0;
+      st->levels = 0;
+      st->pull_levels = 0;
+      st->reached = 0;
+      st->edges = 0;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBfsThreads)
+bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__restrict__ ind,
+               int32_t *depth, int *qa, int *qb, int2 *ca, int2 *cb, BfsState *st,
+               int max_levels, int alpha, int beta, int mode) {
+  const int lane = lane_id();
+  const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  __shared__ unsigned s_q, s_chunks, s_nbig;
+  __shared__ unsigned long long s_edges;
+
+  bool pull = false;
+  int pull_levels = 0;
+  unsigned long long reached = 0, explored = 0;
+  int L = 0;
+  for (;; ++L) {
+    LevelCounters *cur = &st->c[L % 3];
+    LevelCounters *nxt = &st->c[(L + 1) % 3];
+    LevelCounters *clr = &st->c[(L + 2) % 3];
+    if (threadIdx.x == 0) {
+      s_q = __ldcg(&cur->q);
+      s_chunks = __ldcg(&cur->chunks);
+      s_nbig = __ldcg(&cur->nbig);
+      s_edges = __ldcg(&cur->edges);
+      if (blockIdx.x == 0) {
+        clr->q = 0;
+        clr->chunks = 0;
+        clr->nbig = 0;
+        clr->edges = 0;
+      }
+    }
+    __syncthreads();
+    const unsigned nq = s_q, nch = s_chunks;
+    const unsigned long long nf = (unsigned long long)nq + s_nbig;
+    const unsigned long long mf = s_edges;
+    if (nf == 0) break;
+    reached += nf;
+    explored += mf;
+    if (max_levels > 0 && L + 1 >= max_levels) {
+      ++L;
+      break;
+    }
+    const long long unexplored = nnz - (long long)explored;
+    if (mode == 1) {
+      pull = false;
+    } else if (mode == 2) {
+      pull = true;
+    } else if (!pull) {
+      if ((long long)mf * alpha > unexplored) pull = true;
+    } else if ((long long)nf * beta < (long long)m) {
+      pull = false;
+    }
+    int *qin = (L & 1) ? qb : qa;
+    int *qout = (L & 1) ? qa : qb;
+    int2 *cin = (L & 1) ? cb : ca;
+    int2 *cout = (L & 1) ? ca : cb;
+    const int next = L + 1;
+
+    if (!pull) {
+      // ---- push: queued vertices, warp scan-based gather ----
+      for (unsigned base = (unsigned)gwarp * 32u; base < nq; base += (unsigned)nwarps * 32u) {
+        unsigned idx = base + lane;
+        int v = idx < nq ? __ldcg(qin + idx) : -1;
+        int s = 0, d = 0;
+        if (v >= 0) {
+          s = __ldg(ptr + v);
+          d = __ldg(ptr + v + 1) - s;
+        }
+        int incl = warp_incl_scan(d);
+        int excl = incl - d;
+        int total = __shfl_sync(kFull, incl, 31);
+        for (int e0 = 0; e0 < total; e0 += 32) {
+          int e = e0 + lane;
+          int owner = warp_owner(excl, e);
+          int so = __shfl_sync(kFull, s, owner);
+          int eo = __shfl_sync(kFull, excl, owner);
+          bool found = false;
+          int u = -1;
+          if (e < total) {
+            u = __ldg(ind + so + (e - eo));
+            found = claim(u, next, depth);
+          }
+          discover(found, u, ptr, qout, cout, nxt);
+        }
+      }
+      // ---- push: chunks of high-degree frontier vertices ----
+      for (unsigned c = (unsigned)gwarp; c < nch; c += (unsigned)nwarps) {
+        int2 ch = __ldcg(cin + c);
+        int s = __ldg(ptr + ch.x) + ch.y * kChunk;
+        int e = min(s + kChunk, __ldg(ptr + ch.x + 1));
+        for (int k0 = s; k0 < e; k0 += 32) {
+          int k = k0 + lane;
+          bool found = false;
+          int u = -1;
+          if (k < e) {
+            u = __ldg(ind + k);
+            found = claim(u, next, depth);
+          }
+          discover(found, u, ptr, qout, cout, nxt);
+        }
+      }
+    } else {
+      ++pull_levels;
+      // ---- pull: unvisited vertices look for a parent at depth L ----
+      for (int base = gwarp * 32; base < m; base += nwarps * 32) {
+        int v = base + lane;
+        int s = 0, e = 0;
+        bool cand = false;
+        if (v < m && __ldcg(depth + v) == -1) {
+          s = __ldg(ptr + v);
+          e = __ldg(ptr + v + 1);
+          cand = e > s;
+        }
+        unsigned mask = __ballot_sync(kFull, cand);
+        unsigned found_mask = 0;
+        while (mask) {
+          int j = __ffs(mask) - 1;
+          mask &= mask - 1;
+          int sj = __shfl_sync(kFull, s, j);
+          int ej = __shfl_sync(kFull, e, j);
+          for (int k0 = sj; k0 < ej; k0 += 32) {
+            int k = k0 + lane;
+            bool hit = false;
+            if (k < ej) hit = __ldcg(depth + __ldg(ind + k)) == L;
+            if (__any_sync(kFull, hit)) {
+              found_mask |= 1u << j;
+              break;
+            }
+          }
+        }
+        bool found = (found_mask >> lane) & 1u;
+        if (found) depth[v] = next;
+        discover(found, v, ptr, qout, cout, nxt);
+      }
+    }
+    if (!grid_barrier(st->bar, &st->err)) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->levels = L;
+    st->pull_levels = pull_levels;
+    st->reached = reached;
+    st->edges = explored;
+  }
+}
+
+struct BfsLaunch {
+  int grid = 0;
+};
+
+int bfs_grid(apspie_context *ctx) {
+  static int cached_dev = -1, cached_grid = 0;
+  if (cached_dev == ctx->device && cached_grid > 0) return cached_grid;
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bfs_persistent, kBfsThreads, 0) !=
+          cudaSuccess ||
+      occ < 1) {
+    cudaGetLastError();
+    return 0;
+  }
+  cached_dev = ctx->device;
+  cached_grid = occ * ctx->num_sms;
+  return cached_grid;
+}
+
+}  // namespace
+}  // namespace apspie
+
+using namespace apspie;
+
+extern "C" {
+
+int apspie_bfs(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
+               const int *d_ind, int32_t *d_depth, int max_levels) {
+  APSPIE_CHECK_CTX(ctx);
+  if (m <= 0 || src < 0 || src >= m)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_bfs: src %d outside [0,%d)", src, m);
+  if (nnz < 0 || nnz >= (int64_t)INT32_MAX)
+    return set_error(ctx, APSPIE_ERR_OVERFLOW, "apspie_bfs: nnz %lld exceeds int32 offsets",
+                     (long long)nnz);
+  if (!d_ptr || !d_depth || (nnz > 0 && !d_ind))
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_bfs: null pointer");
+  size_t chunk_cap = (size_t)(nnz / kChunk + nnz / kBigDeg + 2);
+  auto *st = (BfsState *)workspace(ctx, kSlotBfsState, sizeof(BfsState));
+  auto *qa = (int *)workspace(ctx, kSlotBfsQueueA, sizeof(int) * (size_t)m);
+  auto *qb = (int *)workspace(ctx, kSlotBfsQueueB, sizeof(int) * (size_t)m);
+  auto *ca = (int2 *)workspace(ctx, kSlotBfsChunksA, sizeof(int2) * chunk_cap);
+  auto *cb = (int2 *)workspace(ctx, kSlotBfsChunksB, sizeof(int2) * chunk_cap);
+  if (!st || !qa || !qb || !ca || !cb) return APSPIE_ERR_OOM;
+  ctx->bfs_state = st;
+  int grid = bfs_grid(ctx);
+  if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_bfs: occupancy query failed");
+
+  int init_grid = std::min((m + 255) / 256, ctx->num_sms * 8);
+  bfs_init<<<init_grid, 256, 0, ctx->stream>>>(m, src, d_depth, d_ptr, qa, ca, st);
+  int rc = check_launch(ctx, "bfs_init");
+  if (rc) return rc;
+  long long nnz_ll = (long long)nnz;
+  int alpha = ctx->bfs_alpha, beta = ctx->bfs_beta, mode = ctx->bfs_mode;
+  void *args[] = {&m, &nnz_ll, (void *)&d_ptr, (void *)&d_ind, &d_depth, &qa, &qb,
+                  &ca, &cb, &st, &max_levels, &alpha, &beta, &mode};
+  cudaError_t e = cudaLaunchCooperativeKernel((const void *)bfs_persistent, dim3(grid),
+                                              dim3(kBfsThreads), args, 0, ctx->stream);
+  if (e != cudaSuccess) return check_cuda(ctx, e, "bfs_persistent");
+  ctx->launches += 1;
+  return APSPIE_OK;
+}
+
+int apspie_bfs_get_stats(apspie_ctx ctx, apspie_bfs_stats *out) {
+  APSPIE_CHECK_CTX(ctx);
+  if (!out || !ctx->bfs_state)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_bfs_get_stats: no BFS has run");
+  auto *h = (BfsState *)pinned(ctx, sizeof(BfsState));
+  if (!h) return APSPIE_ERR_OOM;
+  cudaError_t e = cudaMemcpyAsync(h, ctx->bfs_state, sizeof(BfsState), cudaMemcpyDeviceToHost,
+                                  ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return check_cuda(ctx, e, "apspie_bfs_get_stats");
+  out->levels = h->levels;
+  out->pull_levels = h->pull_levels;
+  out->vertices_reached = (int64_t)h->reached;
+  out->edges_traversed = (int64_t)h->edges;
+  if (h->err)
+    return set_error(ctx, APSPIE_ERR_TIMEOUT, "apspie_bfs: grid barrier timed out (status %d)",
+                     h->err);
+  return APSPIE_OK;
+}
+
+int apspie_bfs_set_params(apspie_ctx ctx, int alpha, int beta, int mode) {
+  if (!ctx || alpha <= 0 || beta <= 0 || mode < 0 || mode > 2) return APSPIE_ERR_INVALID;
+  ctx->bfs_alpha = alpha;
+  ctx->bfs_beta = beta;
+  ctx->bfs_mode = mode;
+  return APSPIE_OK;
+}
+
+}  // extern "C"

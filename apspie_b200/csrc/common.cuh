@@ -1,0 +1,106 @@
+// common.cuh -- shared device primitives for the apspie_b200 kernels (sm_100a).
+//
+// Warp-level scan / compaction, warp-aggregated queue append and a bounded
+// software grid barrier for the persistent traversal kernels.  Every spin in
+// this library has an iteration cap: on timeout it records APSPIE_ERR_TIMEOUT
+// in the kernel's status word and the kernel returns.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "apspie.h"
+
+namespace apspie {
+
+constexpr int kWarp = 32;
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ int warp_in_block() { return threadIdx.x >> 5; }
+
+// Inclusive warp scan (Kogge-Stone over shuffles).
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T v) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T n = __shfl_up_sync(kFull, v, o);
+    if (lane_id() >= o) v += n;
+  }
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// Largest lane j with excl[j] <= e, for a non-decreasing per-lane excl.
+// Used to map a flat edge index back to its owner vertex inside a warp.
+__device__ __forceinline__ int warp_owner(int excl, int e) {
+  int lo = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1) {
+    int probe = lo + step;
+    int val = __shfl_sync(kFull, excl, probe & 31);
+    if (probe <= 31 && val <= e) lo = probe;
+  }
+  return lo;
+}
+
+// Warp-aggregated append of the lanes with pred set: one atomicAdd per warp.
+// Returns this lane's slot (undefined where pred is false).
+__device__ __forceinline__ unsigned warp_append(bool pred, unsigned *counter) {
+  unsigned mask = __ballot_sync(kFull, pred);
+  unsigned base = 0;
+  int leader = __ffs(mask) - 1;
+  if (mask && lane_id() == leader) base = atomicAdd(counter, (unsigned)__popc(mask));
+  base = __shfl_sync(kFull, base, leader < 0 ? 0 : leader);
+  return base + __popc(mask & ((1u << lane_id()) - 1u));
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Sense-counting grid barrier for cooperatively launched kernels.
+// bar[0] = arrival count, bar[1] = generation.  Returns false (and sets
+// *err = APSPIE_ERR_TIMEOUT) if the other blocks do not arrive within
+// kSpinLimit polls; the caller must then leave the kernel.
+constexpr unsigned kSpinLimit = 1u << 24;
+
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+    unsigned gen = ld_acquire(bar + 1);
+    __threadfence();
+    unsigned arrived = atomicAdd(bar, 1u);
+    int ok = 1;
+    if (arrived == nblocks - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      unsigned spins = 0;
+      while (ld_acquire(bar + 1) == gen) {
+        if (++spins > kSpinLimit || *(volatile int *)err != 0) {
+          atomicCAS(err, 0, (int)APSPIE_ERR_TIMEOUT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+}  // namespace apspie

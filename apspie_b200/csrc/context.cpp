@@ -1,0 +1,157 @@
+// context.cpp -- apspie_ctx lifetime, workspace slots and error reporting.
+#include "context.h"
+
+#include <cstdarg>
+#include <cstdlib>
+
+namespace apspie {
+
+int set_error(apspie_context *ctx, int status, const char *fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    ctx->last_error = buf;
+  }
+  return status;
+}
+
+int check_cuda(apspie_context *ctx, cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return APSPIE_OK;
+  int st = (e == cudaErrorMemoryAllocation) ? APSPIE_ERR_OOM : APSPIE_ERR_CUDA;
+  return set_error(ctx, st, "%s: %s", what, cudaGetErrorString(e));
+}
+
+int check_launch(apspie_context *ctx, const char *what, int nlaunches) {
+  ctx->launches += (uint64_t)nlaunches;
+  return check_cuda(ctx, cudaGetLastError(), what);
+}
+
+void *workspace(apspie_context *ctx, int id, size_t bytes) {
+  if (id < 0) return nullptr;
+  if ((size_t)id >= ctx->slots.size()) ctx->slots.resize(id + 1);
+  auto &s = ctx->slots[id];
+  if (bytes == 0) bytes = 16;
+  if (s.bytes >= bytes) return s.ptr;
+  if (s.ptr) {
+    // the stream may still use the old buffer
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(s.ptr);
+    s.ptr = nullptr;
+    s.bytes = 0;
+  }
+  size_t want = (bytes + 255) & ~size_t(255);
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error(ctx, APSPIE_ERR_OOM, "workspace slot %d: cudaMalloc(%zu) failed: %s",
+              id, want, cudaGetErrorString(e));
+    return nullptr;
+  }
+  s.ptr = p;
+  s.bytes = want;
+  return p;
+}
+
+void *pinned(apspie_context *ctx, size_t bytes) {
+  if (ctx->pinned_bytes >= bytes) return ctx->pinned;
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  ctx->pinned = nullptr;
+  ctx->pinned_bytes = 0;
+  size_t want = bytes < 4096 ? 4096 : bytes;
+  if (cudaMallocHost(&ctx->pinned, want) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->pinned = nullptr;
+    set_error(ctx, APSPIE_ERR_OOM, "cudaMallocHost(%zu) failed", want);
+    return nullptr;
+  }
+  ctx->pinned_bytes = want;
+  return ctx->pinned;
+}
+
+}  // namespace apspie
+
+using namespace apspie;
+
+extern "C" {
+
+int apspie_ctx_create(int device, void *stream, apspie_ctx *out) {
+  if (!out) return APSPIE_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return APSPIE_ERR_INVALID;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return APSPIE_ERR_CUDA;
+  }
+  auto *ctx = new (std::nothrow) apspie_context();
+  if (!ctx) return APSPIE_ERR_OOM;
+  ctx->device = device;
+  ctx->stream = (cudaStream_t)stream;
+  cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  ctx->slots.resize(kSlotCount);
+  *out = ctx;
+  return APSPIE_OK;
+}
+
+int apspie_ctx_destroy(apspie_ctx ctx) {
+  if (!ctx) return APSPIE_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto &s : ctx->slots)
+    if (s.ptr) cudaFree(s.ptr);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  delete ctx;
+  return APSPIE_OK;
+}
+
+int apspie_ctx_set_stream(apspie_ctx ctx, void *stream) {
+  if (!ctx) return APSPIE_ERR_INVALID;
+  ctx->stream = (cudaStream_t)stream;
+  return APSPIE_OK;
+}
+
+int apspie_ctx_sync(apspie_ctx ctx) {
+  APSPIE_CHECK_CTX(ctx);
+  return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+}
+
+int apspie_ctx_launch_count(apspie_ctx ctx, uint64_t *out) {
+  if (!ctx || !out) return APSPIE_ERR_INVALID;
+  *out = ctx->launches;
+  return APSPIE_OK;
+}
+
+int apspie_ctx_workspace_bytes(apspie_ctx ctx, size_t *out) {
+  if (!ctx || !out) return APSPIE_ERR_INVALID;
+  size_t t = 0;
+  for (auto &s : ctx->slots) t += s.bytes;
+  *out = t;
+  return APSPIE_OK;
+}
+
+const char *apspie_last_error(apspie_ctx ctx) {
+  return ctx ? ctx->last_error.c_str() : "null context";
+}
+
+const char *apspie_status_string(int status) {
+  switch (status) {
+    case APSPIE_OK: return "ok";
+    case APSPIE_ERR_INVALID: return "invalid argument";
+    case APSPIE_ERR_OOM: return "out of memory";
+    case APSPIE_ERR_CUDA: return "CUDA error";
+    case APSPIE_ERR_TIMEOUT: return "device-side wait timed out";
+    case APSPIE_ERR_OVERFLOW: return "result exceeds int32 layout";
+    case APSPIE_ERR_UNSUPPORTED: return "unsupported";
+    case APSPIE_ERR_BUSY: return "busy";
+    default: return "unknown status";
+  }
+}
+
+}  // extern "C"

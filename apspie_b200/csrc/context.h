@@ -1,0 +1,92 @@
+// context.h -- the per-device context behind apspie_ctx.
+//
+// Owns the stream, a grow-only device workspace split into named slots, a
+// pinned host staging word array, the last error message and a launch
+// counter.  All algorithm entry points draw their scratch from here.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "apspie.h"
+
+struct apspie_context {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  uint64_t launches = 0;
+
+  struct Slot {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+  };
+  std::vector<Slot> slots;
+
+  // pinned host scratch for small device->host reads
+  void *pinned = nullptr;
+  size_t pinned_bytes = 0;
+
+  // BFS tuning and the device block that holds the last run's statistics
+  int bfs_alpha = 14;
+  int bfs_beta = 24;
+  int bfs_mode = 0;  // 0 auto, 1 push only, 2 pull only
+  void *bfs_state = nullptr;  // device pointer into a workspace slot
+};
+
+namespace apspie {
+
+// Workspace slot ids (one buffer per id, grown on demand).
+enum SlotId : int {
+  kSlotBfsState = 0,
+  kSlotBfsQueueA,
+  kSlotBfsQueueB,
+  kSlotBfsChunksA,
+  kSlotBfsChunksB,
+  kSlotSsspState,
+  kSlotSsspQueueA,
+  kSlotSsspQueueB,
+  kSlotSsspChunksA,
+  kSlotSsspChunksB,
+  kSlotSsspStamp,
+  kSlotMisState,
+  kSlotMisQueueA,
+  kSlotMisQueueB,
+  kSlotSortKeysA,
+  kSlotSortKeysB,
+  kSlotSortValsA,
+  kSlotSortValsB,
+  kSlotSortHist,
+  kSlotSortTiles,
+  kSlotScan,
+  kSlotDense,
+  kSlotBitmap,
+  kSlotMisc0,
+  kSlotMisc1,
+  kSlotMisc2,
+  kSlotMisc3,
+  kSlotCount
+};
+
+int set_error(apspie_context *ctx, int status, const char *fmt, ...);
+// Returns a device buffer of at least `bytes` for slot `id` (contents
+// undefined).  nullptr and an OOM error on failure.
+void *workspace(apspie_context *ctx, int id, size_t bytes);
+// Pinned host buffer of at least `bytes`.
+void *pinned(apspie_context *ctx, size_t bytes);
+// Checks cudaGetLastError after launches; records the launch count.
+int check_launch(apspie_context *ctx, const char *what, int nlaunches = 1);
+int check_cuda(apspie_context *ctx, cudaError_t e, const char *what);
+
+}  // namespace apspie
+
+#define APSPIE_CHECK_CTX(ctx)                                   \
+  do {                                                          \
+    if (!(ctx)) return APSPIE_ERR_INVALID;                      \
+    cudaError_t _e = cudaSetDevice((ctx)->device);              \
+    if (_e != cudaSuccess)                                      \
+      return apspie::check_cuda((ctx), _e, "cudaSetDevice");    \
+  } while (0)

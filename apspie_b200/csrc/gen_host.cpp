@@ -1,0 +1,269 @@
+// gen_host.cpp -- host builders for the synthetic benchmark graphs.
+//
+// The reference reads Matrix Market files and symmetrises them with a qsort
+// (src/util.cuh:522-643, src/matrix.cpp:56-111); the benchmark graphs here are
+// generated instead.  Every random draw is a counter-based splitmix64 hash of
+// (seed, sample index), so the same edge multiset comes out on any thread
+// count and on the device builder (gen.cu).  Edges are packed as
+// (row << 32 | col), radix-sorted with a multi-threaded LSD sort, deduplicated
+// and turned into CSR.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "apspie.h"
+#include "gen_common.h"
+
+namespace {
+
+int num_threads() {
+  unsigned n = std::thread::hardware_concurrency();
+  if (n == 0) n = 1;
+  if (n > 64) n = 64;
+  return (int)n;
+}
+
+template <typename F>
+void parallel_for(int64_t n, F f) {
+  int nt = num_threads();
+  if (n < 100000) nt = 1;
+  std::vector<std::thread> th;
+  int64_t per = (n + nt - 1) / nt;
+  for (int t = 0; t < nt; ++t) {
+    int64_t b = t * per, e = std::min<int64_t>(n, b + per);
+    if (b >= e) break;
+    th.emplace_back([=] { f(b, e, t); });
+  }
+  for (auto &x : th) x.join();
+}
+
+// LSD radix sort of 64-bit keys on the low `bits` bits, 11-bit digits.
+void radix_sort_u64(std::vector<uint64_t> &a, int bits) {
+  const int64_t n = (int64_t)a.size();
+  if (n < 2) return;
+  std::vector<uint64_t> tmp(n);
+  const int D = 11, R = 1 << D;
+  int nt = num_threads();
+  if (n < 100000) nt = 1;
+  int64_t per = (n + nt - 1) / nt;
+  std::vector<int64_t> hist((size_t)nt * R);
+  uint64_t *src = a.data(), *dst = tmp.data();
+  int passes = 0;
+  for (int shift = 0; shift < bits; shift += D, ++passes) {
+    std::fill(hist.begin(), hist.end(), 0);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+      th.emplace_back([&, t] {
+        int64_t b = t * per, e = std::min<int64_t>(n, b + per);
+        int64_t *h = &hist[(size_t)t * R];
+        for (int64_t i = b; i < e; ++i) h[(src[i] >> shift) & (R - 1)]++;
+      });
+    for (auto &x : th) x.join();
+    th.clear();
+    int64_t run = 0;
+    for (int d = 0; d < R; ++d)
+      for (int t = 0; t < nt; ++t) {
+        int64_t c = hist[(size_t)t * R + d];
+        hist[(size_t)t * R + d] = run;
+        run += c;
+      }
+    for (int t = 0; t < nt; ++t)
+      th.emplace_back([&, t] {
+        int64_t b = t * per, e = std::min<int64_t>(n, b + per);
+        int64_t *h = &hist[(size_t)t * R];
+        for (int64_t i = b; i < e; ++i) dst[h[(src[i] >> shift) & (R - 1)]++] = src[i];
+      });
+    for (auto &x : th) x.join();
+    std::swap(src, dst);
+  }
+  if (passes & 1) a.swap(tmp);
+}
+
+// Sorted, deduplicated (row<<32|col) keys -> CSR.  Keys equal to ~0 are
+// padding and are dropped (they sort last).
+int keys_to_csr(std::vector<uint64_t> &keys, int m, int64_t *nnz_out, int **h_ptr,
+                int **h_ind) {
+  int64_t n = (int64_t)keys.size();
+  while (n > 0 && keys[n - 1] == ~0ull) --n;
+  int64_t w = 0;
+  for (int64_t i = 0; i < n; ++i)
+    if (i == 0 || keys[i] != keys[i - 1]) keys[w++] = keys[i];
+  if (w >= (int64_t)INT32_MAX) return APSPIE_ERR_OVERFLOW;
+  int *ptr = (int *)malloc(sizeof(int) * ((size_t)m + 1));
+  int *ind = (int *)malloc(sizeof(int) * (size_t)(w > 0 ? w : 1));
+  if (!ptr || !ind) {
+    free(ptr);
+    free(ind);
+    return APSPIE_ERR_OOM;
+  }
+  std::memset(ptr, 0, sizeof(int) * ((size_t)m + 1));
+  for (int64_t i = 0; i < w; ++i) ptr[(keys[i] >> 32) + 1]++;
+  for (int i = 0; i < m; ++i) ptr[i + 1] += ptr[i];
+  parallel_for(w, [&](int64_t b, int64_t e, int) {
+    for (int64_t i = b; i < e; ++i) ind[i] = (int)(keys[i] & 0xffffffffu);
+  });
+  *nnz_out = w;
+  *h_ptr = ptr;
+  *h_ind = ind;
+  return APSPIE_OK;
+}
+
+int bits_for(int m) {
+  int b = 0;
+  while ((1ll << b) < (long long)m) ++b;
+  return b;
+}
+
+}  // namespace
+
+using namespace apspie_gen;
+
+extern "C" {
+
+int apspie_gen_rmat_host(int scale, int edge_factor, uint64_t seed, int symmetric,
+                         int scramble, int *m_out, int64_t *nnz_out, int **h_ptr,
+                         int **h_ind) {
+  if (scale < 1 || scale > 30 || edge_factor < 1 || !m_out || !nnz_out || !h_ptr || !h_ind)
+    return APSPIE_ERR_INVALID;
+  const int m = 1 << scale;
+  const int64_t samples = (int64_t)edge_factor << scale;
+  const int per = symmetric ? 2 : 1;
+  std::vector<uint64_t> keys;
+  try {
+    keys.resize((size_t)(samples * per));
+  } catch (...) {
+    return APSPIE_ERR_OOM;
+  }
+  const RmatParams P = rmat_params(scale, seed, scramble != 0);
+  parallel_for(samples, [&](int64_t b, int64_t e, int) {
+    for (int64_t s = b; s < e; ++s) {
+      uint32_t u, v;
+      rmat_sample(P, (uint64_t)s, &u, &v);
+      if (u == v) {
+        keys[(size_t)(s * per)] = ~0ull;
+        if (symmetric) keys[(size_t)(s * per + 1)] = ~0ull;
+      } else {
+        keys[(size_t)(s * per)] = ((uint64_t)u << 32) | v;
+        if (symmetric) keys[(size_t)(s * per + 1)] = ((uint64_t)v << 32) | u;
+      }
+    }
+  });
+  // pad keys (~0) must sort last: sort on all 64 bits only when needed
+  radix_sort_u64(keys, 32 + scale + (1));
+  *m_out = m;
+  return keys_to_csr(keys, m, nnz_out, h_ptr, h_ind);
+}
+
+int apspie_gen_er_host(int n, int mean_degree, uint64_t seed, int64_t *nnz_out, int **h_ptr,
+                       int **h_ind) {
+  if (n < 2 || mean_degree < 1 || !nnz_out || !h_ptr || !h_ind) return APSPIE_ERR_INVALID;
+  const int64_t samples = (int64_t)n * mean_degree / 2;
+  std::vector<uint64_t> keys;
+  try {
+    keys.resize((size_t)(2 * samples));
+  } catch (...) {
+    return APSPIE_ERR_OOM;
+  }
+  const uint64_t sm = mix64(seed ^ 0x45524552ull);
+  parallel_for(samples, [&](int64_t b, int64_t e, int) {
+    for (int64_t s = b; s < e; ++s) {
+      uint32_t u, v;
+      er_sample(sm, (uint64_t)s, (uint32_t)n, &u, &v);
+      if (u == v) {
+        keys[(size_t)(2 * s)] = keys[(size_t)(2 * s + 1)] = ~0ull;
+      } else {
+        keys[(size_t)(2 * s)] = ((uint64_t)u << 32) | v;
+        keys[(size_t)(2 * s + 1)] = ((uint64_t)v << 32) | u;
+      }
+    }
+  });
+  radix_sort_u64(keys, 32 + bits_for(n) + 1);
+  return keys_to_csr(keys, n, nnz_out, h_ptr, h_ind);
+}
+
+int apspie_gen_grid_host(int rows, int cols, int64_t *nnz_out, int **h_ptr, int **h_ind) {
+  if (rows < 1 || cols < 1 || (int64_t)rows * cols >= INT32_MAX || !nnz_out || !h_ptr || !h_ind)
+    return APSPIE_ERR_INVALID;
+  const int m = rows * cols;
+  int *ptr = (int *)malloc(sizeof(int) * ((size_t)m + 1));
+  int64_t nnz = 4ll * rows * cols - 2ll * rows - 2ll * cols;
+  int *ind = (int *)malloc(sizeof(int) * (size_t)(nnz > 0 ? nnz : 1));
+  if (!ptr || !ind) {
+    free(ptr);
+    free(ind);
+    return APSPIE_ERR_OOM;
+  }
+  int64_t k = 0;
+  for (int r = 0; r < rows; ++r)
+    for (int c = 0; c < cols; ++c) {
+      ptr[r * cols + c] = (int)k;
+      // neighbours in ascending id order: up, left, right, down
+      if (r > 0) ind[k++] = (r - 1) * cols + c;
+      if (c > 0) ind[k++] = r * cols + c - 1;
+      if (c + 1 < cols) ind[k++] = r * cols + c + 1;
+      if (r + 1 < rows) ind[k++] = (r + 1) * cols + c;
+    }
+  ptr[m] = (int)k;
+  *nnz_out = k;
+  *h_ptr = ptr;
+  *h_ind = ind;
+  return APSPIE_OK;
+}
+
+int apspie_gen_weights_u32_host(int m, const int *h_ptr, const int *h_ind, uint64_t seed,
+                                uint32_t lo, uint32_t hi, uint32_t *h_w) {
+  if (m < 0 || !h_ptr || !h_w || hi < lo) return APSPIE_ERR_INVALID;
+  parallel_for(m, [&](int64_t b, int64_t e, int) {
+    for (int64_t u = b; u < e; ++u)
+      for (int k = h_ptr[u]; k < h_ptr[u + 1]; ++k)
+        h_w[k] = weight_u32(seed, (uint32_t)u, (uint32_t)h_ind[k], lo, hi);
+  });
+  return APSPIE_OK;
+}
+
+int apspie_gen_weights_f32_host(int m, const int *h_ptr, const int *h_ind, uint64_t seed,
+                                float *h_w) {
+  if (m < 0 || !h_ptr || !h_w) return APSPIE_ERR_INVALID;
+  parallel_for(m, [&](int64_t b, int64_t e, int) {
+    for (int64_t u = b; u < e; ++u)
+      for (int k = h_ptr[u]; k < h_ptr[u + 1]; ++k)
+        h_w[k] = weight_f32(seed, (uint32_t)u, (uint32_t)h_ind[k]);
+  });
+  return APSPIE_OK;
+}
+
+int apspie_mt19937_fill_host(uint32_t seed, int64_t n, uint32_t *h_out) {
+  if (n < 0 || (n > 0 && !h_out)) return APSPIE_ERR_INVALID;
+  uint32_t mt[624];
+  int mti;
+  mt[0] = seed;
+  for (mti = 1; mti < 624; ++mti)
+    mt[mti] = 1812433253u * (mt[mti - 1] ^ (mt[mti - 1] >> 30)) + (uint32_t)mti;
+  for (int64_t t = 0; t < n; ++t) {
+    if (mti >= 624) {
+      // twist: the first 227 words read words not yet updated in this pass,
+      // the rest read already-updated ones
+      for (int k = 0; k < 624; ++k) {
+        uint32_t y = (mt[k] & 0x80000000u) | (mt[k + 1 < 624 ? k + 1 : 0] & 0x7fffffffu);
+        uint32_t src = mt[k + 397 < 624 ? k + 397 : k + 397 - 624];
+        mt[k] = src ^ (y >> 1) ^ ((y & 1u) * 0x9908b0dfu);
+      }
+      mti = 0;
+    }
+    uint32_t y = mt[mti++];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    h_out[t] = y;
+  }
+  return APSPIE_OK;
+}
+
+void apspie_host_free(void *p) { free(p); }
+
+}  // extern "C"

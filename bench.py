@@ -1,0 +1,362 @@
+"""Benchmark: single-source BFS GTEPS on R-MAT scale 22 (one B200), with the
+HBM roofline of the traversal kernel, the end-to-end figure through the C ABI
+with host buffers, and the reference's CPU BFS timed on the host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+A step is one BFS traversal from one seed-chosen source of the largest
+connected component.  Inputs are resident in HBM before timing; the CSR
+(~530 MB) is larger than the 126 MB L2, so no flush is needed between steps.
+Multi-GPU runs are independent replicas (queries shard with no data-path
+collective): value = all ranks' traversed edges / max-over-ranks time.
+Prints exactly one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SCALE = 22
+EDGE_FACTOR = 16
+SEED = 1
+WORKLOAD = (f"bfs_rmat{SCALE}: R-MAT scale {SCALE} (2^{SCALE} vertices), edge factor "
+            f"{EDGE_FACTOR}, (0.57,0.19,0.19,0.05), symmetrised, self-loops/duplicates removed, "
+            f"int32 CSR, single source per step from the largest connected component")
+METRIC = "BFS GTEPS (R-MAT scale 22, single source, 1 B200)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--scale", type=int, default=SCALE)
+    p.add_argument("--profile-run", action="store_true",
+                   help="only the timed traversals (for ncu captures): no clock extension, "
+                        "no end-to-end leg, no CPU baseline")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text()), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def profile_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        for line in f.read_text().splitlines():
+            if line.startswith(f"traffic_bytes_per_launch[{kernel}]:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_graph(scale):
+    import apspie_b200 as ap
+    h = ap.gen_rmat(scale, EDGE_FACTOR, seed=SEED, symmetric=True)
+    return h
+
+
+def cpu_reference_bfs(h, sources, threads, budget_s, stop=1 << 30):
+    """The reference's SimpleReferenceBfs (oracle/_ref) on `threads` host
+    threads, one source each per round, until the sources or the time budget
+    run out.  Returns (edges, seconds, bfs_count)."""
+    import oracle
+    deg = h.degrees()
+    results = []
+    lock = threading.Lock()
+    it = iter(sources)
+    t_end = time.perf_counter() + budget_s
+
+    def worker():
+        while time.perf_counter() < t_end:
+            with lock:
+                s = next(it, None)
+            if s is None:
+                return
+            d = np.empty(h.m, np.int32)
+            t0 = time.perf_counter()
+            oracle._r.ref_bfs_cpu(int(s), h.m, h.ptr.ctypes.data, h.ind.ctypes.data,
+                                  d.ctypes.data, stop)
+            dt = time.perf_counter() - t0
+            e = int(deg[d >= 0].sum())
+            with lock:
+                results.append((e, dt))
+
+    import ctypes
+    sys.stdout.flush()
+    ctypes.CDLL(None).fflush(None)
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    try:
+        t0 = time.perf_counter()
+        th = [threading.Thread(target=worker) for _ in range(threads)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        wall = time.perf_counter() - t0
+    finally:
+        ctypes.CDLL(None).fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+    edges = sum(e for e, _ in results)
+    return edges, wall, len(results), sum(dt for _, dt in results)
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    kind = "reference" if oracle.have_reference() else "port"
+    h = build_graph(args.scale)
+    import apspie_b200 as ap
+    threads = os.cpu_count() or 1
+    sources = ap.seeded_sources(h, max(args.steps, 1) * threads, seed=0)
+    # warm-up: a depth-limited traversal per thread
+    cpu_reference_bfs(h, sources[:threads], threads, 30.0, stop=1)
+    edges, wall, n, _ = cpu_reference_bfs(h, sources, threads, 120.0)
+    gteps = edges / wall / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": gteps, "unit": "GTEPS",
+        "n_gpus": args.gpus, "steps": n, "warmup": args.warmup,
+        "ms_per_step": 1e3 * wall / max(n, 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "scale": args.scale},
+        "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": threads, "kind": kind,
+                         "sample": f"{n} full BFS traversals of R-MAT {args.scale}, "
+                                   f"{threads} concurrent single-threaded SimpleReferenceBfs "
+                                   f"(src/testBfs.cpp:7-72), 120 s budget"},
+        "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import apspie_b200 as ap
+
+    h = build_graph(args.scale)
+    g = h.to_device(local)
+    deg = h.degrees()
+    nsrc = max(args.steps, 1)
+    sources = ap.seeded_sources(h, nsrc + args.warmup, seed=rank)
+    ctx = ap.Context(local)
+    stream = torch.cuda.current_stream(local)
+    depth = torch.empty(h.m, dtype=torch.int32, device=g.ptr.device)
+
+    # untimed pass: edges traversed per source (and warm-up)
+    e_r = []
+    for s in sources[:nsrc]:
+        ap.bfs(ctx, g, s, depth)
+        e_r.append(ap.bfs_stats(ctx)["edges_traversed"])
+    reached = ap.bfs_stats(ctx)["vertices_reached"]
+    for s in sources[nsrc:]:
+        ap.bfs(ctx, g, s, depth)
+    torch.cuda.synchronize()
+
+    # ---- timed: K traversals, inputs resident ----
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(nsrc)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launches
+    with ClockSampler(local) as clk:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for i, s in enumerate(sources[:nsrc]):
+            ev[i][0].record(stream)
+            ap.bfs(ctx, g, s, depth)
+            ev[i][1].record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        launches = ctx.launches - launches0
+        # keep sampling a little longer for a usable clock record on short runs
+        total_ms = t0.elapsed_time(t1)
+        if total_ms < 1500 and not args.profile_run:
+            extra = int(1500 / max(total_ms / nsrc, 1e-3))
+            for i in range(min(extra, 20000)):
+                ap.bfs(ctx, g, sources[i % nsrc], depth)
+            torch.cuda.synchronize()
+    per = [a.elapsed_time(b) for a, b in ev]
+    ms = total_ms
+    if dist:
+        t = torch.tensor([ms], device=g.ptr.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        et = torch.tensor([float(sum(e_r))], device=g.ptr.device, dtype=torch.float64)
+        dist.all_reduce(et)
+        edges_all = float(et.item())
+    else:
+        edges_all = float(sum(e_r))
+    value = edges_all / (ms * 1e-3) / 1e9
+
+    # ---- roofline of the traversal kernel (bfs_init + bfs_persistent per launch) ----
+    pk, pk_kind = peaks()
+    b_alg = 4.0 * np.mean(e_r) + 8.0 * reached + 4.0 * h.m
+    avg_launch_s = float(np.mean(per)) * 1e-3
+    achieved = b_alg / avg_launch_s / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / pk["hbm_gbs"], "peak_kind": pk_kind,
+            "kernel": "bfs_persistent (+ bfs_init)",
+            "algorithmic_bytes_per_launch": b_alg,
+            "traffic": profile_traffic("bfs_persistent"),
+            "vs_nominal_8tbs": achieved / 8000.0}
+
+    # ---- end to end through the C ABI with host buffers ----
+    ptr_h = torch.from_numpy(h.ptr).pin_memory()
+    ind_h = torch.from_numpy(h.ind).pin_memory()
+    depth_h = torch.empty(h.m, dtype=torch.int32).pin_memory()
+    e2e_steps = 0 if args.profile_run else min(nsrc, 10)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for s in sources[:e2e_steps]:
+        g.ptr.copy_(ptr_h, non_blocking=True)
+        g.ind.copy_(ind_h, non_blocking=True)
+        ap.bfs(ctx, g, s, depth)
+        depth_h.copy_(depth, non_blocking=True)
+    b.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max(a.elapsed_time(b), 1e-6)
+    e2e = {"value": sum(e_r[:e2e_steps]) / (e2e_ms * 1e-3) / 1e9, "unit": "GTEPS",
+           "h2d_bytes_per_step": int(h.ptr.nbytes + h.ind.nbytes),
+           "d2h_bytes_per_step": int(depth_h.numel() * 4),
+           "note": "graph CSR copied host->device and depths device->host every step"}
+
+    # ---- reference CPU BFS on a bounded sample (rank 0, N=1) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.profile_run:
+        import oracle
+        if oracle.have_reference():
+            edges, wall, n, busy = cpu_reference_bfs(h, sources[:8], 1, 20.0)
+            cpu = {"value": edges / wall / 1e9, "unit": "GTEPS", "cores": 1,
+                   "kind": "reference",
+                   "sample": f"{n} BFS traversals of the same graph and sources, "
+                             f"SimpleReferenceBfs (src/testBfs.cpp:7-72) -O3, 1 thread, "
+                             f"host nproc={os.cpu_count()}"}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": nsrc,
+        "warmup": args.warmup, "ms_per_step": ms / nsrc, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "scale": args.scale, "m": h.m, "nnz": h.nnz,
+                   "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (CSR %.0f MB), no flush" %
+                         ((h.ptr.nbytes + h.ind.nbytes) / 1e6),
+                   "edges_traversed_per_step": float(np.mean(e_r)),
+                   "vertices_reached": int(reached)},
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "per_step_ms": {"min": min(per), "median": statistics.median(per), "max": max(per)},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

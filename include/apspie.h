@@ -1,0 +1,130 @@
+/*
+ * apspie.h -- C ABI of apspie_b200, a B200-native (sm_100a) implementation of
+ * apspie's SpMSpV / hash-SpGEMM hot path.
+ *
+ * Conventions
+ *   - Every entry point returns an int status (APSPIE_OK == 0) and never
+ *     exits the process.  apspie_last_error() gives a message for the last
+ *     failure on a context.
+ *   - Pointers named d_* are device pointers on the context's device; h_*
+ *     are host pointers.  Graphs are CSR with int32 row offsets and int32
+ *     column indices (the reference's layout, src/matrix.hpp:6-37).  For
+ *     traversal the CSR row of u lists u's out-neighbours, which is the
+ *     "CSC" the reference drivers pass to mXv (test/bfs/main.cu:140).
+ *   - Work is stream-ordered on the context's stream.  Calls that return a
+ *     value to the host (counts, statistics) synchronise that stream.
+ *   - A context must not be used from two host threads at once.
+ *
+ * Each entry point names the reference interface it replaces (file:line in
+ * the apspie source tree).
+ */
+#ifndef APSPIE_H
+#define APSPIE_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  APSPIE_OK = 0,
+  APSPIE_ERR_INVALID = 1,     /* bad argument (size, vertex id, null pointer) */
+  APSPIE_ERR_OOM = 2,         /* device or host allocation failed */
+  APSPIE_ERR_CUDA = 3,        /* CUDA runtime error */
+  APSPIE_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+  APSPIE_ERR_OVERFLOW = 5,    /* a result does not fit the int32 layout */
+  APSPIE_ERR_UNSUPPORTED = 6, /* feature not available on this device */
+  APSPIE_ERR_BUSY = 7         /* serving queue full / admission refused */
+} apspie_status;
+
+typedef struct apspie_context *apspie_ctx;
+
+/* ------------------------------------------------------------ context ---
+ * Replaces mgpu::CreateCudaDevice (test/bfs/main.cu:27) plus the scratch
+ * workspace of allocScratch (src/util.cuh:646-672, src/scratch.hpp:5-31):
+ * the context owns a grow-only device workspace reused across calls, so no
+ * call allocates once the workspace has grown to the graph's size.
+ * stream may be NULL (the legacy default stream). */
+int apspie_ctx_create(int device, void *stream, apspie_ctx *out);
+int apspie_ctx_destroy(apspie_ctx ctx);
+int apspie_ctx_set_stream(apspie_ctx ctx, void *stream);
+int apspie_ctx_sync(apspie_ctx ctx);
+/* Number of kernels this context has launched since creation. */
+int apspie_ctx_launch_count(apspie_ctx ctx, uint64_t *out);
+/* Bytes of device workspace currently held by the context. */
+int apspie_ctx_workspace_bytes(apspie_ctx ctx, size_t *out);
+const char *apspie_last_error(apspie_ctx ctx);
+const char *apspie_status_string(int status);
+
+/* ---------------------------------------------------------------- BFS ---
+ * Replaces bfs<T>() (src/bfs.cuh:33-125, mXv + addResult per level) and the
+ * keys-only spmspvBfs() (src/spmspvBfs.cuh:96-243).
+ * d_depth[v] = level of v (source 0, unreached -1), bit-exact with the
+ * reference's CPU BFS (src/testBfs.cpp:7-72).  max_levels > 0 stops after
+ * levels 1..max_levels-1 have been assigned, as the reference's fixed
+ * iteration count does (src/bfs.cuh:87); max_levels <= 0 runs to convergence.
+ * Direction-optimising: push over the frontier queue while it is small, pull
+ * over the unvisited vertices while it is large. */
+int apspie_bfs(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
+               const int *d_ind, int32_t *d_depth, int max_levels);
+
+typedef struct {
+  int32_t levels;            /* deepest level + 1 (the reference's "search depth") */
+  int32_t pull_levels;       /* levels run in the pull direction */
+  int64_t vertices_reached;  /* |R| */
+  int64_t edges_traversed;   /* E_R = sum of out-degrees of reached vertices */
+} apspie_bfs_stats;
+
+/* Statistics of the last apspie_bfs on this context (synchronises). Also
+ * reports a device-side timeout of that run as APSPIE_ERR_TIMEOUT. */
+int apspie_bfs_get_stats(apspie_ctx ctx, apspie_bfs_stats *out);
+
+/* Direction-switch thresholds (Beamer's alpha, beta; defaults 14 and 24) and
+ * mode: 0 = switch automatically, 1 = push only, 2 = pull only. */
+int apspie_bfs_set_params(apspie_ctx ctx, int alpha, int beta, int mode);
+
+/* ------------------------------------------------- host graph builders ---
+ * Synthetic inputs of the benchmark configurations (no reference
+ * counterpart: the reference reads .mtx files, src/util.cuh:355-430).
+ * Results are malloc'ed; release them with apspie_host_free.
+ *
+ * R-MAT (a,b,c,d) = (0.57,0.19,0.19,0.05), edge_factor * 2^scale samples,
+ * self-loops and duplicates removed, optionally symmetrised; vertex ids are
+ * scrambled by a seeded bijection when scramble != 0. */
+int apspie_gen_rmat_host(int scale, int edge_factor, uint64_t seed,
+                         int symmetric, int scramble, int *m_out,
+                         int64_t *nnz_out, int **h_ptr, int **h_ind);
+/* Erdos-Renyi: n*mean_degree/2 uniform vertex pairs, symmetrised, deduped. */
+int apspie_gen_er_host(int n, int mean_degree, uint64_t seed, int64_t *nnz_out,
+                       int **h_ptr, int **h_ind);
+/* rows x cols 2-D 5-point grid, vertex id = r*cols + c. */
+int apspie_gen_grid_host(int rows, int cols, int64_t *nnz_out, int **h_ptr,
+                         int **h_ind);
+/* Edge weights as a function of (row, col, seed), so they do not depend on
+ * the CSR build order.  u32: uniform in [lo, hi].  f32: uniform in (0, 1]
+ * on the grid k * 2^-24. */
+int apspie_gen_weights_u32_host(int m, const int *h_ptr, const int *h_ind,
+                                uint64_t seed, uint32_t lo, uint32_t hi,
+                                uint32_t *h_w);
+int apspie_gen_weights_f32_host(int m, const int *h_ptr, const int *h_ind,
+                                uint64_t seed, float *h_w);
+/* MT19937 priorities: n outputs of genrand_int32() after init_genrand(seed)
+ * (src/mt19937ar.cpp:57-150), the generator the reference uses for its hash
+ * constants (src/spgemmKernel.cuh:173-177). */
+int apspie_mt19937_fill_host(uint32_t seed, int64_t n, uint32_t *h_out);
+/* Matrix Market ingest with the reference's orientation: readEdge/readMtx
+ * (src/util.cuh:355-430) store a line's first index as the column and the
+ * second as the row; buildMatrix (src/matrix.cpp:56-111) keeps file order
+ * inside a row.  undirected != 0 symmetrises as makeSymmetric
+ * (src/util.cuh:573-643): mirrors added, sorted by (row, col), repeats
+ * dropped, self-loops kept.  h_val may be NULL. */
+int apspie_read_mtx_host(const char *path, int undirected, int *m_out,
+                         int64_t *nnz_out, int **h_ptr, int **h_ind,
+                         float **h_val, int *weighted_out);
+void apspie_host_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* APSPIE_H */

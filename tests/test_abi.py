@@ -1,0 +1,45 @@
+"""The C-ABI library loads and exports every symbol include/*.h declares
+(no compute calls: this runs without a GPU)."""
+import ctypes
+import re
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_symbols() -> set[str]:
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        for m in re.finditer(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b(apspie_\w+)\s*\(", text, re.M):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    from apspie_b200 import _native
+    lib = ctypes.CDLL(str(_native.LIB_PATH))
+    names = declared_symbols()
+    assert len(names) >= 10
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, f"declared but not exported: {missing}"
+    # the Python binding declares a prototype for each of them too
+    assert not (names - set(_native.PROTOS)), sorted(names - set(_native.PROTOS))
+
+
+def test_status_strings_and_null_context():
+    from apspie_b200._native import lib
+    assert lib.apspie_status_string(0) == b"ok"
+    assert lib.apspie_status_string(4) == b"device-side wait timed out"
+    # calls on a null context return an error instead of crashing
+    assert lib.apspie_ctx_sync(None) == 1
+    assert lib.apspie_bfs(None, 0, 0, 1, None, None, None, 0) == 1
+
+
+def test_library_is_built_for_sm_100a():
+    from apspie_b200 import _native
+    out = __import__("subprocess").run(
+        ["/usr/local/cuda/bin/cuobjdump", "--list-elf", str(_native.LIB_PATH)],
+        capture_output=True, text=True)
+    if out.returncode == 0:
+        assert "sm_100a" in out.stdout
