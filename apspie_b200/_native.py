@@ -31,6 +31,11 @@ class BfsStats(C.Structure):
                 ("vertices_reached", C.c_int64), ("edges_traversed", C.c_int64)]
 
 
+class SsspStats(C.Structure):
+    _fields_ = [("rounds", C.c_int32), ("pad", C.c_int32), ("vertices_reached", C.c_int64),
+                ("edges_traversed", C.c_int64), ("relaxations", C.c_int64)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/apspie.h
 PROTOS: dict[str, tuple] = {
     "apspie_ctx_create": (c_int, [c_int, vp, P_vp]),
@@ -41,9 +46,16 @@ PROTOS: dict[str, tuple] = {
     "apspie_ctx_workspace_bytes": (c_int, [vp, P_size]),
     "apspie_last_error": (C.c_char_p, [vp]),
     "apspie_status_string": (C.c_char_p, [c_int]),
-    "apspie_bfs": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, c_int]),
+    "apspie_bfs": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, vp, c_int]),
     "apspie_bfs_get_stats": (c_int, [vp, C.POINTER(BfsStats)]),
+    "apspie_bfs_get_trace": (c_int, [vp, c_int, P_int, vp, vp, vp, vp]),
     "apspie_bfs_set_params": (c_int, [vp, c_int, c_int, c_int]),
+    "apspie_sssp_u32": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, c_int]),
+    "apspie_sssp_f32": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, c_int]),
+    "apspie_sssp_get_stats": (c_int, [vp, C.POINTER(SsspStats)]),
+    "apspie_mis": (c_int, [vp, c_i64, c_int, vp, vp, vp, vp, c_f32]),
+    "apspie_mis_get_rounds": (c_int, [vp, P_int]),
+    "apspie_neighbor_flags": (c_int, [vp, c_i64, c_int, vp, vp, vp, vp]),
     "apspie_gen_rmat_host": (c_int, [c_int, c_int, c_u64, c_int, c_int, P_int, P_i64, P_vp, P_vp]),
     "apspie_gen_er_host": (c_int, [c_int, c_int, c_u64, P_i64, P_vp, P_vp]),
     "apspie_gen_grid_host": (c_int, [c_int, c_int, P_i64, P_vp, P_vp]),

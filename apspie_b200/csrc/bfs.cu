@@ -25,20 +25,20 @@
 
 #include "common.cuh"
 #include "context.h"
+#include "frontier.cuh"
 
 namespace apspie {
 namespace {
 
 constexpr int kBfsThreads = 512;
-constexpr int kBigDeg = 1024;  // out-degree above which a vertex is chunked
-constexpr int kChunk = 1024;   // edges per chunk
+constexpr int kProbe = 4;         // in-neighbours a lane checks alone in a pull level
+constexpr int kTraceLevels = 64;  // levels recorded in the per-run trace
 
-struct LevelCounters {
-  unsigned q;        // frontier vertices in the queue (degree <= kBigDeg)
-  unsigned chunks;   // entries in the chunk list
-  unsigned nbig;     // frontier vertices in the chunk list
-  unsigned pad;
-  unsigned long long edges;  // sum of out-degrees of the frontier
+struct LevelTrace {
+  int mode;  // 1 push, 2 pull
+  int pad;
+  unsigned long long nf, mf;
+  unsigned long long t_end;  // %globaltimer at the end of the level (ns)
 };
 
 struct BfsState {
@@ -50,25 +50,9 @@ struct BfsState {
   int pad;
   unsigned long long reached;
   unsigned long long edges;
+  unsigned long long t_start;
+  LevelTrace trace[kTraceLevels];
 };
-
-__device__ __forceinline__ void discover(bool found, int u, const int *__restrict__ ptr,
-                                         int *qout, int2 *cout, LevelCounters *nxt) {
-  int deg = 0;
-  if (found) deg = __ldg(ptr + u + 1) - __ldg(ptr + u);
-  bool big = found && deg > kBigDeg;
-  bool small = found && !big;
-  unsigned slot = warp_append(small, &nxt->q);
-  if (small) qout[slot] = u;
-  if (big) {
-    int nch = (deg + kChunk - 1) / kChunk;
-    unsigned base = atomicAdd(&nxt->chunks, (unsigned)nch);
-    atomicAdd(&nxt->nbig, 1u);
-    for (int j = 0; j < nch; ++j) cout[base + j] = make_int2(u, j);
-  }
-  unsigned long long e = warp_sum((unsigned long long)deg);
-  if (lane_id() == 0 && e) atomicAdd(&nxt->edges, e);
-}
 
 __device__ __forceinline__ bool claim(int u, int level, int32_t *depth) {
   if (__ldcg(depth + u) != -1) return false;
@@ -80,19 +64,10 @@ __global__ void bfs_init(int m, int src, int32_t *depth, const int *__restrict__
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < m; v += gridDim.x * blockDim.x)
     depth[v] = (v == src) ? 0 : -1;
   if (blockIdx.x == 0) {
-    int deg = __ldg(ptr + src + 1) - __ldg(ptr + src);
-    int nch = deg > kBigDeg ? (deg + kChunk - 1) / kChunk : 0;
-    for (int j = threadIdx.x; j < nch; j += blockDim.x) chunks[j] = make_int2(src, j);
+    seed_frontier(src, ptr, queue, chunks, &st->c[0]);
     if (threadIdx.x == 0) {
-      for (int i = 0; i < 3; ++i) st->c[i] = LevelCounters{0, 0, 0, 0, 0ull};
-      if (nch) {
-        st->c[0].chunks = (unsigned)nch;
-        st->c[0].nbig = 1;
-      } else {
-        queue[0] = src;
-        st->c[0].q = 1;
-      }
-      st->c[0].edges = (unsigned long long)deg;
+      st->c[1] = LevelCounters{0, 0, 0, 0, 0ull};
+      st->c[2] = LevelCounters{0, 0, 0, 0, 0ull};
       st->bar[0] = st->bar[1] = 0;
       st->err = 0;
       st->levels = 0;
@@ -105,7 +80,7 @@ __global__ void bfs_init(int m, int src, int32_t *depth, const int *__restrict__
 
 __global__ void __launch_bounds__(kBfsThreads)
 bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__restrict__ ind,
-               int32_t *depth, int *qa, int *qb, int2 *ca, int2 *cb, BfsState *st,
+               const int *__restrict__ tptr, const int *__restrict__ tind, int32_t *depth, int *qa, int *qb, int2 *ca, int2 *cb, BfsState *st,
                int max_levels, int alpha, int beta, int mode) {
   const int lane = lane_id();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -113,6 +88,7 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
   __shared__ unsigned s_q, s_chunks, s_nbig;
   __shared__ unsigned long long s_edges;
 
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->t_start = globaltimer();
   bool pull = false;
   int pull_levels = 0;
   unsigned long long reached = 0, explored = 0;
@@ -161,62 +137,36 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
     const int next = L + 1;
 
     if (!pull) {
-      // ---- push: queued vertices, warp scan-based gather ----
-      for (unsigned base = (unsigned)gwarp * 32u; base < nq; base += (unsigned)nwarps * 32u) {
-        unsigned idx = base + lane;
-        int v = idx < nq ? __ldcg(qin + idx) : -1;
-        int s = 0, d = 0;
-        if (v >= 0) {
-          s = __ldg(ptr + v);
-          d = __ldg(ptr + v + 1) - s;
-        }
-        int incl = warp_incl_scan(d);
-        int excl = incl - d;
-        int total = __shfl_sync(kFull, incl, 31);
-        for (int e0 = 0; e0 < total; e0 += 32) {
-          int e = e0 + lane;
-          int owner = warp_owner(excl, e);
-          int so = __shfl_sync(kFull, s, owner);
-          int eo = __shfl_sync(kFull, excl, owner);
-          bool found = false;
-          int u = -1;
-          if (e < total) {
-            u = __ldg(ind + so + (e - eo));
-            found = claim(u, next, depth);
-          }
-          discover(found, u, ptr, qout, cout, nxt);
-        }
-      }
-      // ---- push: chunks of high-degree frontier vertices ----
-      for (unsigned c = (unsigned)gwarp; c < nch; c += (unsigned)nwarps) {
-        int2 ch = __ldcg(cin + c);
-        int s = __ldg(ptr + ch.x) + ch.y * kChunk;
-        int e = min(s + kChunk, __ldg(ptr + ch.x + 1));
-        for (int k0 = s; k0 < e; k0 += 32) {
-          int k = k0 + lane;
-          bool found = false;
-          int u = -1;
-          if (k < e) {
-            u = __ldg(ind + k);
-            found = claim(u, next, depth);
-          }
-          discover(found, u, ptr, qout, cout, nxt);
-        }
-      }
+      expand_push(
+          ptr, ind, qin, nq, cin, nch, qout, cout, nxt, gwarp, nwarps,
+          [](int) { return 0u; },
+          [&](unsigned, int, int u) { return claim(u, next, depth); });
     } else {
       ++pull_levels;
       // ---- pull: unvisited vertices look for a parent at depth L ----
+      // Each lane first probes the first kProbe in-neighbours of its own
+      // vertex (32 independent load chains per warp; most vertices of a large
+      // frontier find a parent there), then the warp sweeps the remaining
+      // in-neighbours of the unresolved vertices 32 at a time.
       for (int base = gwarp * 32; base < m; base += nwarps * 32) {
         int v = base + lane;
         int s = 0, e = 0;
-        bool cand = false;
+        bool cand = false, found = false;
         if (v < m && __ldcg(depth + v) == -1) {
-          s = __ldg(ptr + v);
-          e = __ldg(ptr + v + 1);
+          s = __ldg(tptr + v);
+          e = __ldg(tptr + v + 1);
           cand = e > s;
         }
-        unsigned mask = __ballot_sync(kFull, cand);
-        unsigned found_mask = 0;
+        if (cand) {
+          int stop = min(e, s + kProbe);
+          for (int k = s; k < stop; ++k)
+            if (__ldcg(depth + __ldg(tind + k)) == L) {
+              found = true;
+              break;
+            }
+          s = stop;
+        }
+        unsigned mask = __ballot_sync(kFull, cand && !found && s < e);
         while (mask) {
           int j = __ffs(mask) - 1;
           mask &= mask - 1;
@@ -225,19 +175,24 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
           for (int k0 = sj; k0 < ej; k0 += 32) {
             int k = k0 + lane;
             bool hit = false;
-            if (k < ej) hit = __ldcg(depth + __ldg(ind + k)) == L;
+            if (k < ej) hit = __ldcg(depth + __ldg(tind + k)) == L;
             if (__any_sync(kFull, hit)) {
-              found_mask |= 1u << j;
+              if (lane == j) found = true;
               break;
             }
           }
         }
-        bool found = (found_mask >> lane) & 1u;
         if (found) depth[v] = next;
         discover(found, v, ptr, qout, cout, nxt);
       }
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && L < kTraceLevels) {
+      st->trace[L].mode = pull ? 2 : 1;
+      st->trace[L].nf = nf;
+      st->trace[L].mf = mf;
+    }
     if (!grid_barrier(st->bar, &st->err)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && L < kTraceLevels) st->trace[L].t_end = globaltimer();
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->levels = L;
@@ -246,10 +201,6 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
     st->edges = explored;
   }
 }
-
-struct BfsLaunch {
-  int grid = 0;
-};
 
 int bfs_grid(apspie_context *ctx) {
   static int cached_dev = -1, cached_grid = 0;
@@ -274,16 +225,17 @@ using namespace apspie;
 extern "C" {
 
 int apspie_bfs(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
-               const int *d_ind, int32_t *d_depth, int max_levels) {
+               const int *d_ind, const int *d_tptr, const int *d_tind, int32_t *d_depth,
+               int max_levels) {
   APSPIE_CHECK_CTX(ctx);
   if (m <= 0 || src < 0 || src >= m)
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_bfs: src %d outside [0,%d)", src, m);
   if (nnz < 0 || nnz >= (int64_t)INT32_MAX)
     return set_error(ctx, APSPIE_ERR_OVERFLOW, "apspie_bfs: nnz %lld exceeds int32 offsets",
                      (long long)nnz);
-  if (!d_ptr || !d_depth || (nnz > 0 && !d_ind))
+  if (!d_ptr || !d_depth || (nnz > 0 && !d_ind) || (d_tptr && nnz > 0 && !d_tind))
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_bfs: null pointer");
-  size_t chunk_cap = (size_t)(nnz / kChunk + nnz / kBigDeg + 2);
+  size_t chunk_cap = chunk_capacity(nnz);
   auto *st = (BfsState *)workspace(ctx, kSlotBfsState, sizeof(BfsState));
   auto *qa = (int *)workspace(ctx, kSlotBfsQueueA, sizeof(int) * (size_t)m);
   auto *qb = (int *)workspace(ctx, kSlotBfsQueueB, sizeof(int) * (size_t)m);
@@ -300,8 +252,9 @@ int apspie_bfs(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
   if (rc) return rc;
   long long nnz_ll = (long long)nnz;
   int alpha = ctx->bfs_alpha, beta = ctx->bfs_beta, mode = ctx->bfs_mode;
-  void *args[] = {&m, &nnz_ll, (void *)&d_ptr, (void *)&d_ind, &d_depth, &qa, &qb,
-                  &ca, &cb, &st, &max_levels, &alpha, &beta, &mode};
+  if (!d_tptr) mode = 1;  // no in-adjacency: push only
+  void *args[] = {&m,  &nnz_ll, (void *)&d_ptr, (void *)&d_ind, (void *)&d_tptr, (void *)&d_tind,
+                  &d_depth, &qa, &qb, &ca, &cb, &st, &max_levels, &alpha, &beta, &mode};
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)bfs_persistent, dim3(grid),
                                               dim3(kBfsThreads), args, 0, ctx->stream);
   if (e != cudaSuccess) return check_cuda(ctx, e, "bfs_persistent");
@@ -338,3 +291,28 @@ int apspie_bfs_set_params(apspie_ctx ctx, int alpha, int beta, int mode) {
 }
 
 }  // extern "C"
+
+extern "C" int apspie_bfs_get_trace(apspie_ctx ctx, int max_levels, int *n_out,
+                                    int32_t *h_mode, int64_t *h_frontier,
+                                    int64_t *h_frontier_edges, int64_t *h_ns) {
+  APSPIE_CHECK_CTX(ctx);
+  if (!ctx->bfs_state || max_levels < 0 || !n_out)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_bfs_get_trace: no BFS has run");
+  auto *h = (BfsState *)pinned(ctx, sizeof(BfsState));
+  if (!h) return APSPIE_ERR_OOM;
+  cudaError_t e = cudaMemcpyAsync(h, ctx->bfs_state, sizeof(BfsState), cudaMemcpyDeviceToHost,
+                                  ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return check_cuda(ctx, e, "apspie_bfs_get_trace");
+  int n = std::min(std::min(max_levels, kTraceLevels), std::max(0, h->levels - 1));
+  unsigned long long prev = h->t_start;
+  for (int i = 0; i < n; ++i) {
+    if (h_mode) h_mode[i] = h->trace[i].mode;
+    if (h_frontier) h_frontier[i] = (int64_t)h->trace[i].nf;
+    if (h_frontier_edges) h_frontier_edges[i] = (int64_t)h->trace[i].mf;
+    if (h_ns) h_ns[i] = (int64_t)(h->trace[i].t_end - prev);
+    prev = h->trace[i].t_end;
+  }
+  *n_out = n;
+  return APSPIE_OK;
+}

@@ -60,6 +60,12 @@ __device__ __forceinline__ unsigned warp_append(bool pred, unsigned *counter) {
   return base + __popc(mask & ((1u << lane_id()) - 1u));
 }
 
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");

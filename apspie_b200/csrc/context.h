@@ -35,6 +35,8 @@ struct apspie_context {
   int bfs_beta = 24;
   int bfs_mode = 0;  // 0 auto, 1 push only, 2 pull only
   void *bfs_state = nullptr;  // device pointer into a workspace slot
+  void *sssp_state = nullptr;
+  void *mis_state = nullptr;
 };
 
 namespace apspie {

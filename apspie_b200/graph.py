@@ -32,6 +32,7 @@ class HostGraph:
     name: str = ""
     w_u32: np.ndarray | None = None
     w_f32: np.ndarray | None = None
+    symmetric: bool = False
 
     @property
     def nnz(self) -> int:
@@ -40,14 +41,33 @@ class HostGraph:
     def degrees(self) -> np.ndarray:
         return np.diff(self.ptr)
 
-    def to_device(self, device: int | str = 0) -> "DeviceGraph":
+    def transpose(self) -> "HostGraph":
+        """CSR of the transpose (in-adjacency), rows sorted by source id."""
+        src = np.repeat(np.arange(self.m, dtype=np.int32), np.diff(self.ptr))
+        order = np.argsort(self.ind, kind="stable")
+        ptr = np.zeros(self.m + 1, dtype=np.int64)
+        np.add.at(ptr, self.ind.astype(np.int64) + 1, 1)
+        return HostGraph(self.m, np.cumsum(ptr).astype(np.int32), src[order].copy(),
+                         name=self.name + "^T")
+
+    def to_device(self, device: int | str = 0, with_transpose: bool = True) -> "DeviceGraph":
         import torch
         dev = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
-        t = lambda a: None if a is None else torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+        def t(a):
+            if a is None:
+                return None
+            if a.size == 0:
+                return torch.zeros(1, dtype=torch.from_numpy(a[:0]).dtype, device=dev)
+            return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
         w_u32 = None if self.w_u32 is None else t(self.w_u32.view(np.int32))
-        return DeviceGraph(self.m, self.nnz, t(self.ptr), t(self.ind) if self.nnz else
-                           torch.zeros(1, dtype=torch.int32, device=dev),
-                           w_u32=w_u32, w_f32=t(self.w_f32), name=self.name)
+        g = DeviceGraph(self.m, self.nnz, t(self.ptr), t(self.ind), w_u32=w_u32,
+                        w_f32=t(self.w_f32), name=self.name, symmetric=self.symmetric)
+        if with_transpose and not self.symmetric:
+            tr = self.transpose()
+            g.tptr, g.tind = t(tr.ptr), t(tr.ind)
+        return g
 
 
 @dataclass
@@ -59,6 +79,9 @@ class DeviceGraph:
     w_u32: "object" = None   # stored as int32 tensor holding uint32 bits
     w_f32: "object" = None
     name: str = ""
+    symmetric: bool = False
+    tptr: "object" = None    # in-adjacency (transpose CSR) for pull traversal
+    tind: "object" = None
     extra: dict = field(default_factory=dict)
 
 
@@ -73,7 +96,7 @@ def gen_rmat(scale: int, edge_factor: int = 16, seed: int = 1, symmetric: bool =
           what="gen_rmat")
     name = f"rmat{scale}{'s' if symmetric else 'd'}"
     return HostGraph(m.value, _take_int_array(p, m.value + 1), _take_int_array(i, nnz.value),
-                     name=name)
+                     name=name, symmetric=symmetric)
 
 
 def gen_er(n: int, mean_degree: int = 8, seed: int = 1) -> HostGraph:
@@ -81,7 +104,8 @@ def gen_er(n: int, mean_degree: int = 8, seed: int = 1) -> HostGraph:
     p, i = C.c_void_p(), C.c_void_p()
     check(lib.apspie_gen_er_host(n, mean_degree, seed, C.byref(nnz), C.byref(p), C.byref(i)),
           what="gen_er")
-    return HostGraph(n, _take_int_array(p, n + 1), _take_int_array(i, nnz.value), name=f"er{n}")
+    return HostGraph(n, _take_int_array(p, n + 1), _take_int_array(i, nnz.value), name=f"er{n}",
+                     symmetric=True)
 
 
 def gen_grid(rows: int, cols: int) -> HostGraph:
@@ -91,7 +115,7 @@ def gen_grid(rows: int, cols: int) -> HostGraph:
           what="gen_grid")
     m = rows * cols
     return HostGraph(m, _take_int_array(p, m + 1), _take_int_array(i, nnz.value),
-                     name=f"grid{rows}x{cols}")
+                     name=f"grid{rows}x{cols}", symmetric=True)
 
 
 def weights_u32(g: HostGraph, seed: int = 7, lo: int = 1, hi: int = 255) -> np.ndarray:
@@ -131,7 +155,7 @@ def read_mtx(path: str, undirected: bool = False) -> HostGraph:
         C.memmove(vals.ctypes.data, v.value, 4 * nnz.value)
     lib.apspie_host_free(v)
     g = HostGraph(m.value, _take_int_array(p, m.value + 1), _take_int_array(i, nnz.value),
-                  name=str(path).rsplit("/", 1)[-1])
+                  name=str(path).rsplit("/", 1)[-1], symmetric=bool(undirected))
     if weighted.value:
         g.w_f32 = vals
     return g

@@ -5,7 +5,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-from ._native import BfsStats, check, lib
+from ._native import BfsStats, SsspStats, check, lib
 
 
 class Context:
@@ -71,13 +71,34 @@ def _p(t) -> C.c_void_p:
 
 
 def bfs(ctx: Context, g, src: int, depth=None, max_levels: int = 0):
-    """bfs<T>() (src/bfs.cuh:33): int32 depth per vertex, -1 unreached."""
+    """bfs<T>() (src/bfs.cuh:33): int32 depth per vertex, -1 unreached.
+    The pull direction uses g.tptr / g.tind (in-adjacency): the same arrays
+    for a symmetric graph; a directed graph without them is traversed by
+    push only."""
     import torch
     if depth is None:
         depth = torch.empty(g.m, dtype=torch.int32, device=g.ptr.device)
+    tptr, tind = (g.ptr, g.ind) if g.symmetric else (g.tptr, g.tind)
     check(lib.apspie_bfs(ctx.handle, int(src), int(g.nnz), int(g.m), _p(g.ptr), _p(g.ind),
-                         _p(depth), int(max_levels)), ctx.handle, "apspie_bfs")
+                         _p(tptr), _p(tind), _p(depth), int(max_levels)), ctx.handle,
+          "apspie_bfs")
     return depth
+
+
+def bfs_trace(ctx: Context, max_levels: int = 64) -> list[dict]:
+    """Per-level direction, frontier size / edges and device ns of the last BFS."""
+    import numpy as np
+    mode = np.zeros(max_levels, np.int32)
+    nf = np.zeros(max_levels, np.int64)
+    mf = np.zeros(max_levels, np.int64)
+    ns = np.zeros(max_levels, np.int64)
+    cnt = C.c_int()
+    check(lib.apspie_bfs_get_trace(ctx.handle, max_levels, C.byref(cnt), mode.ctypes.data,
+                                   nf.ctypes.data, mf.ctypes.data, ns.ctypes.data), ctx.handle,
+          "apspie_bfs_get_trace")
+    n = cnt.value
+    return [{"level": i, "dir": "pull" if mode[i] == 2 else "push", "frontier": int(nf[i]),
+             "frontier_edges": int(mf[i]), "us": ns[i] / 1e3} for i in range(n)]
 
 
 def bfs_stats(ctx: Context) -> dict:
@@ -91,3 +112,59 @@ def bfs_set_params(ctx: Context, alpha: int = 14, beta: int = 24, mode: int = 0)
     """Direction-switch thresholds; mode 0 auto, 1 push only, 2 pull only."""
     check(lib.apspie_bfs_set_params(ctx.handle, alpha, beta, mode), ctx.handle,
           "apspie_bfs_set_params")
+
+
+def sssp(ctx: Context, g, src: int, dist=None, weights: str = "u32", max_rounds: int = 0):
+    """sssp<V>() (src/sssp.cuh:28): min-plus SpMSpV to convergence.
+    weights "u32" uses g.w_u32 and returns int32-viewed uint32 distances
+    (0xFFFFFFFF unreached); "f32" uses g.w_f32 and returns float32 (+inf)."""
+    import torch
+    if weights == "u32":
+        if dist is None:
+            dist = torch.empty(g.m, dtype=torch.int32, device=g.ptr.device)
+        fn, w = lib.apspie_sssp_u32, g.w_u32
+    elif weights == "f32":
+        if dist is None:
+            dist = torch.empty(g.m, dtype=torch.float32, device=g.ptr.device)
+        fn, w = lib.apspie_sssp_f32, g.w_f32
+    else:
+        raise ValueError(weights)
+    if w is None:
+        raise ValueError(f"graph has no {weights} weights")
+    check(fn(ctx.handle, int(src), int(g.nnz), int(g.m), _p(g.ptr), _p(g.ind), _p(w), _p(dist),
+             int(max_rounds)), ctx.handle, "apspie_sssp")
+    return dist
+
+
+def sssp_stats(ctx: Context) -> dict:
+    s = SsspStats()
+    check(lib.apspie_sssp_get_stats(ctx.handle, C.byref(s)), ctx.handle, "apspie_sssp_get_stats")
+    return {"rounds": s.rounds, "vertices_reached": s.vertices_reached,
+            "edges_traversed": s.edges_traversed, "relaxations": s.relaxations}
+
+
+def mis(ctx: Context, g, prio, out=None, delta: float = 1.0):
+    """spmspvMis<V>() (src/spmspvMis.cuh:150): int32 membership (1 / 0).
+    prio: device tensor of uint32 priorities (int32 view)."""
+    import torch
+    if out is None:
+        out = torch.empty(g.m, dtype=torch.int32, device=g.ptr.device)
+    check(lib.apspie_mis(ctx.handle, int(g.nnz), int(g.m), _p(g.ptr), _p(g.ind), _p(prio),
+                         _p(out), float(delta)), ctx.handle, "apspie_mis")
+    return out
+
+
+def mis_rounds(ctx: Context) -> int:
+    r = C.c_int()
+    check(lib.apspie_mis_get_rounds(ctx.handle, C.byref(r)), ctx.handle, "apspie_mis_get_rounds")
+    return int(r.value)
+
+
+def neighbor_flags(ctx: Context, g, flags, out=None):
+    """spmspvCsr() (src/spmspvMis.cuh:81): 1 for out-neighbours of flagged vertices."""
+    import torch
+    if out is None:
+        out = torch.empty(g.m, dtype=torch.int32, device=g.ptr.device)
+    check(lib.apspie_neighbor_flags(ctx.handle, int(g.nnz), int(g.m), _p(g.ptr), _p(g.ind),
+                                    _p(flags), _p(out)), ctx.handle, "apspie_neighbor_flags")
+    return out

@@ -242,6 +242,7 @@ def run_ours(args):
         ap.bfs(ctx, g, s, depth)
         e_r.append(ap.bfs_stats(ctx)["edges_traversed"])
     reached = ap.bfs_stats(ctx)["vertices_reached"]
+    trace = ap.bfs_trace(ctx)
     for s in sources[nsrc:]:
         ap.bfs(ctx, g, s, depth)
     torch.cuda.synchronize()
@@ -346,6 +347,8 @@ def run_ours(args):
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "per_step_ms": {"min": min(per), "median": statistics.median(per), "max": max(per)},
+        "level_trace": [[t["dir"], t["frontier"], t["frontier_edges"], round(t["us"], 1)]
+                        for t in trace],
     }
     print(json.dumps(line), flush=True)
 

@@ -64,10 +64,13 @@ const char *apspie_status_string(int status);
  * reference's CPU BFS (src/testBfs.cpp:7-72).  max_levels > 0 stops after
  * levels 1..max_levels-1 have been assigned, as the reference's fixed
  * iteration count does (src/bfs.cuh:87); max_levels <= 0 runs to convergence.
- * Direction-optimising: push over the frontier queue while it is small, pull
- * over the unvisited vertices while it is large. */
+ * Direction-optimising: push over the frontier queue (out-adjacency d_ptr /
+ * d_ind) while it is small, pull over the unvisited vertices while it is
+ * large.  Pull reads the in-adjacency d_tptr / d_tind (CSR of the transpose);
+ * pass d_ptr / d_ind again for an undirected graph, or NULL to push only. */
 int apspie_bfs(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
-               const int *d_ind, int32_t *d_depth, int max_levels);
+               const int *d_ind, const int *d_tptr, const int *d_tind,
+               int32_t *d_depth, int max_levels);
 
 typedef struct {
   int32_t levels;            /* deepest level + 1 (the reference's "search depth") */
@@ -80,9 +83,69 @@ typedef struct {
  * reports a device-side timeout of that run as APSPIE_ERR_TIMEOUT. */
 int apspie_bfs_get_stats(apspie_ctx ctx, apspie_bfs_stats *out);
 
+/* Per-level trace of the last apspie_bfs (synchronises): for each level
+ * i < max_levels (at most 64) the direction (1 push, 2 pull), frontier size,
+ * frontier out-edges and device time in ns; *n_out = levels written.  The
+ * array outputs may be NULL. */
+int apspie_bfs_get_trace(apspie_ctx ctx, int max_levels, int *n_out,
+                         int32_t *h_mode, int64_t *h_frontier,
+                         int64_t *h_frontier_edges, int64_t *h_ns);
+
 /* Direction-switch thresholds (Beamer's alpha, beta; defaults 14 and 24) and
  * mode: 0 = switch automatically, 1 = push only, 2 = pull only. */
 int apspie_bfs_set_params(apspie_ctx ctx, int alpha, int beta, int mode);
+
+/* --------------------------------------------------------------- SSSP ---
+ * Replaces sssp<V>() (src/sssp.cuh:28-115) with its per-iteration min-plus
+ * spmspvSssp<V>() (src/spmspvSssp.cuh:92-291).  Frontier-driven
+ * Bellman-Ford: each round expands the vertices whose distance dropped in the
+ * previous round, relaxing with atomicMin.  Unreached vertices get
+ * UINT32_MAX (u32) or +inf (f32); the reference uses -1 on the CPU and
+ * 1.70141e38 on the GPU.  u32 sums saturate at UINT32_MAX - 1.  The f32
+ * result is bit-identical to the reference's CPU SSSP (src/testSssp.cpp:33-
+ * 115): every relaxation is one round-to-nearest single add and both reach
+ * the same fixpoint.  max_rounds > 0 bounds the number of rounds (the
+ * reference's `depth` argument; its unit-weight rounds after the first,
+ * src/sssp.cuh:83,91, are not reproduced); <= 0 runs to convergence. */
+int apspie_sssp_u32(apspie_ctx ctx, int src, int64_t nnz, int m,
+                    const int *d_ptr, const int *d_ind, const uint32_t *d_w,
+                    uint32_t *d_dist, int max_rounds);
+int apspie_sssp_f32(apspie_ctx ctx, int src, int64_t nnz, int m,
+                    const int *d_ptr, const int *d_ind, const float *d_w,
+                    float *d_dist, int max_rounds);
+
+typedef struct {
+  int32_t rounds;            /* frontier rounds run */
+  int32_t pad;
+  int64_t vertices_reached;  /* |R| */
+  int64_t edges_traversed;   /* E_R = sum of out-degrees of reached vertices */
+  int64_t relaxations;       /* edges scanned over all rounds (>= E_R) */
+} apspie_sssp_stats;
+
+/* Statistics of the last SSSP on this context (synchronises). */
+int apspie_sssp_get_stats(apspie_ctx ctx, apspie_sssp_stats *out);
+
+/* ---------------------------------------------------------------- MIS ---
+ * Replaces spmspvMis<V>() (src/spmspvMis.cuh:150-344).  d_prio holds one
+ * uint32 priority per vertex (mt19937 draws, apspie_mt19937_fill_host).  A
+ * vertex joins when it beats every undecided neighbour in key
+ * (prio << 32 | id): the result is the greedy MIS in descending key order,
+ * independent of delta, which only sets how fast the candidate threshold
+ * falls (the reference's `minimum -= delta`, src/spmspvMis.cuh:235-236;
+ * delta <= 0 means 1).  d_mis[v] = 1 (in the set) or 0.  Self-loops are
+ * ignored.  The graph must be symmetric. */
+int apspie_mis(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr,
+               const int *d_ind, const uint32_t *d_prio, int32_t *d_mis,
+               float delta);
+/* Rounds used by the last apspie_mis (synchronises). */
+int apspie_mis_get_rounds(apspie_ctx ctx, int *rounds);
+
+/* Neighbour flags: d_out[v] = 1 if v is an out-neighbour of some u with
+ * d_in[u] != 0, else 0.  Replaces spmspvCsr() (src/spmspvMis.cuh:81-147),
+ * the SpMSpV behind the reference's MIS check (test/mis/main.cu:217-221). */
+int apspie_neighbor_flags(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr,
+                          const int *d_ind, const int32_t *d_in,
+                          int32_t *d_out);
 
 /* ------------------------------------------------- host graph builders ---
  * Synthetic inputs of the benchmark configurations (no reference

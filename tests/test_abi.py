@@ -33,7 +33,7 @@ def test_status_strings_and_null_context():
     assert lib.apspie_status_string(4) == b"device-side wait timed out"
     # calls on a null context return an error instead of crashing
     assert lib.apspie_ctx_sync(None) == 1
-    assert lib.apspie_bfs(None, 0, 0, 1, None, None, None, 0) == 1
+    assert lib.apspie_bfs(None, 0, 0, 1, None, None, None, None, None, 0) == 1
 
 
 def test_library_is_built_for_sm_100a():

@@ -116,3 +116,15 @@ def test_mtx_weighted_and_malformed(tmp_path):
     bad.write_text("3 3 1\n7 1\n")
     with pytest.raises(ap.ApspieError):
         ap.read_mtx(bad)
+
+
+def test_transpose_host():
+    g = ap.gen_rmat(10, 8, seed=2, symmetric=False)
+    t = g.transpose()
+    tt = t.transpose()
+    np.testing.assert_array_equal(tt.ptr, g.ptr)
+    np.testing.assert_array_equal(tt.ind, g.ind)
+    assert t.nnz == g.nnz
+    sym = ap.gen_rmat(10, 8, seed=2)
+    st = sym.transpose()
+    np.testing.assert_array_equal(st.ind, sym.ind)
