@@ -37,6 +37,8 @@ struct apspie_context {
   void *bfs_state = nullptr;  // device pointer into a workspace slot
   void *sssp_state = nullptr;
   void *mis_state = nullptr;
+  // SpMSpV: the bitmap path is taken when E * factor > m
+  double spmspv_sort_factor = 4.0;
 };
 
 namespace apspie {
@@ -70,6 +72,9 @@ enum SlotId : int {
   kSlotMisc1,
   kSlotMisc2,
   kSlotMisc3,
+  kSlotMxvBuf,
+  kSlotMxvFlags,
+  kSlotSmall,
   kSlotCount
 };
 
