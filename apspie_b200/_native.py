@@ -56,6 +56,10 @@ PROTOS: dict[str, tuple] = {
     "apspie_mis": (c_int, [vp, c_i64, c_int, vp, vp, vp, vp, c_f32]),
     "apspie_mis_get_rounds": (c_int, [vp, P_int]),
     "apspie_neighbor_flags": (c_int, [vp, c_i64, c_int, vp, vp, vp, vp]),
+    "apspie_spmspv": (c_int, [vp, c_int, c_int, c_i64, vp, vp, vp, c_int, vp, vp, vp, vp, P_int,
+                              P_i64]),
+    "apspie_mxv_dense": (c_int, [vp, c_int, c_int, c_i64, vp, vp, vp, vp, vp, P_i64]),
+    "apspie_spmspv_set_params": (c_int, [vp, C.c_double]),
     "apspie_gen_rmat_host": (c_int, [c_int, c_int, c_u64, c_int, c_int, P_int, P_i64, P_vp, P_vp]),
     "apspie_gen_er_host": (c_int, [c_int, c_int, c_u64, P_i64, P_vp, P_vp]),
     "apspie_gen_grid_host": (c_int, [c_int, c_int, P_i64, P_vp, P_vp]),

@@ -31,7 +31,8 @@ namespace apspie {
 namespace {
 
 constexpr int kBfsThreads = 512;
-constexpr int kProbe = 4;         // in-neighbours a lane checks alone in a pull level
+constexpr int kProbe = 4;         // in-neighbours a lane loads per batch in a pull level
+constexpr int kLaneScan = 64;     // in-neighbours a lane scans before the warp takes over
 constexpr int kTraceLevels = 64;  // levels recorded in the per-run trace
 
 struct LevelTrace {
@@ -54,10 +55,17 @@ struct BfsState {
   LevelTrace trace[kTraceLevels];
 };
 
-__device__ __forceinline__ bool claim(int u, int level, int32_t *depth) {
-  if (__ldcg(depth + u) != -1) return false;
-  return atomicCAS(depth + u, -1, level) == -1;
-}
+// Push visitor: an unvisited destination is claimed with one CAS.
+struct BfsVisit {
+  int next;
+  int32_t *depth;
+  __device__ __forceinline__ bool check(unsigned, int, int u, unsigned &) const {
+    return __ldcg(depth + u) == -1;
+  }
+  __device__ __forceinline__ bool commit(unsigned, int, int u, unsigned) const {
+    return atomicCAS(depth + u, -1, next) == -1;
+  }
+};
 
 __global__ void bfs_init(int m, int src, int32_t *depth, const int *__restrict__ ptr,
                          int *queue, int2 *chunks, BfsState *st) {
@@ -78,7 +86,7 @@ __global__ void bfs_init(int m, int src, int32_t *depth, const int *__restrict__
   }
 }
 
-__global__ void __launch_bounds__(kBfsThreads)
+__global__ void __launch_bounds__(kBfsThreads, 3)
 bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__restrict__ ind,
                const int *__restrict__ tptr, const int *__restrict__ tind, int32_t *depth, int *qa, int *qb, int2 *ca, int2 *cb, BfsState *st,
                int max_levels, int alpha, int beta, int mode) {
@@ -137,36 +145,35 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
     const int next = L + 1;
 
     if (!pull) {
-      expand_push(
-          ptr, ind, qin, nq, cin, nch, qout, cout, nxt, gwarp, nwarps,
-          [](int) { return 0u; },
-          [&](unsigned, int, int u) { return claim(u, next, depth); });
+      BfsVisit vis{next, depth};
+      expand_push(ptr, ind, qin, nq, cin, nch, qout, cout, nxt, gwarp, nwarps,
+                  [](int) { return 0u; }, vis);
     } else {
       ++pull_levels;
       // ---- pull: unvisited vertices look for a parent at depth L ----
-      // Each lane first probes the first kProbe in-neighbours of its own
-      // vertex (32 independent load chains per warp; most vertices of a large
-      // frontier find a parent there), then the warp sweeps the remaining
-      // in-neighbours of the unresolved vertices 32 at a time.
+      // Each lane scans the in-neighbours of its own vertex in batches of
+      // kProbe (all index loads of a batch, then all depth loads, so a lane
+      // keeps kProbe loads in flight), for up to kLaneScan neighbours; the
+      // rare vertices with longer unresolved lists are then swept by the
+      // whole warp, 32 neighbours per step.
       for (int base = gwarp * 32; base < m; base += nwarps * 32) {
         int v = base + lane;
         int s = 0, e = 0;
-        bool cand = false, found = false;
+        bool found = false;
         if (v < m && __ldcg(depth + v) == -1) {
           s = __ldg(tptr + v);
           e = __ldg(tptr + v + 1);
-          cand = e > s;
         }
-        if (cand) {
-          int stop = min(e, s + kProbe);
-          for (int k = s; k < stop; ++k)
-            if (__ldcg(depth + __ldg(tind + k)) == L) {
-              found = true;
-              break;
-            }
-          s = stop;
+        const int lane_end = min(e, s + kLaneScan);
+        while (s < lane_end && !found) {
+          int nb[kProbe];
+#pragma unroll
+          for (int i = 0; i < kProbe; ++i) nb[i] = s + i < lane_end ? __ldg(tind + s + i) : -1;
+#pragma unroll
+          for (int i = 0; i < kProbe; ++i) found |= nb[i] >= 0 && __ldcg(depth + nb[i]) == L;
+          s += kProbe;
         }
-        unsigned mask = __ballot_sync(kFull, cand && !found && s < e);
+        unsigned mask = __ballot_sync(kFull, !found && s < e);
         while (mask) {
           int j = __ffs(mask) - 1;
           mask &= mask - 1;

@@ -8,18 +8,24 @@
 //     consecutive edges to the lanes (coalesced reads of ind[]), and a 5-step
 //     shuffle search maps an edge back to its owner lane;
 //   * vertices of degree > kBigDeg are split into kChunk-edge chunks, listed
-//     as (vertex, chunk) pairs that every warp of the grid pulls from.
-// A visitor decides per edge whether the destination enters the next
-// frontier; discover() appends it (warp-aggregated) to the next queue or, if
-// it is a big vertex, to the next chunk list, and accumulates the next
-// frontier's edge count.
+//     as (vertex, chunk) pairs that every warp of the grid pulls from, so a
+//     small frontier of hubs still spreads over the whole GPU.
+// Rounds are issued kUnroll at a time: all index loads of the batch, then all
+// visitor checks (the random loads), then the atomic commits, so each lane
+// keeps several independent loads in flight.  A visitor provides
+//   check(payload, k, u, &aux) -> bool   (plain loads only)
+//   commit(payload, k, u, aux) -> bool   (atomics; true = u joins the next frontier)
+// discover() appends joiners (warp-aggregated) to the next queue or, for big
+// vertices, writes their chunk entries cooperatively, and accumulates the
+// next frontier's edge count.
 #pragma once
 #include "common.cuh"
 
 namespace apspie {
 
-constexpr int kBigDeg = 1024;  // out-degree above which a vertex is chunked
-constexpr int kChunk = 1024;   // edges per chunk
+constexpr int kBigDeg = 64;   // out-degree above which a vertex is chunked
+constexpr int kChunk = 256;   // edges per chunk
+constexpr int kUnroll = 4;    // rounds of 32 edges issued together
 
 struct LevelCounters {
   unsigned q;       // vertices in the queue (degree <= kBigDeg)
@@ -29,7 +35,8 @@ struct LevelCounters {
   unsigned long long edges;  // sum of out-degrees of those vertices
 };
 
-// Capacity of a chunk list for a graph with nnz edges.
+// Capacity of a chunk list for a graph with nnz edges: every big vertex has
+// more than kBigDeg edges, so there are fewer than nnz / kBigDeg of them.
 inline size_t chunk_capacity(long long nnz) {
   return (size_t)(nnz / kChunk + nnz / kBigDeg + 2);
 }
@@ -37,20 +44,35 @@ inline size_t chunk_capacity(long long nnz) {
 // Called by all 32 lanes; lanes with found == true append vertex u.
 __device__ __forceinline__ void discover(bool found, int u, const int *__restrict__ ptr,
                                          int *qout, int2 *cout, LevelCounters *nxt) {
+  const int lane = lane_id();
   int deg = 0;
   if (found) deg = __ldg(ptr + u + 1) - __ldg(ptr + u);
   bool big = found && deg > kBigDeg;
   bool small = found && !big;
   unsigned slot = warp_append(small, &nxt->q);
   if (small) qout[slot] = u;
-  if (big) {
-    int nch = (deg + kChunk - 1) / kChunk;
-    unsigned base = atomicAdd(&nxt->chunks, (unsigned)nch);
-    atomicAdd(&nxt->nbig, 1u);
-    for (int j = 0; j < nch; ++j) cout[base + j] = make_int2(u, j);
+  unsigned bmask = __ballot_sync(kFull, big);
+  if (bmask) {
+    int nch = big ? (deg + kChunk - 1) / kChunk : 0;
+    int incl = warp_incl_scan(nch);
+    int total = __shfl_sync(kFull, incl, 31);
+    unsigned base = 0;
+    if (lane == 0) {
+      base = atomicAdd(&nxt->chunks, (unsigned)total);
+      atomicAdd(&nxt->nbig, (unsigned)__popc(bmask));
+    }
+    base = __shfl_sync(kFull, base, 0) + (unsigned)(incl - nch);
+    while (bmask) {
+      int j = __ffs(bmask) - 1;
+      bmask &= bmask - 1;
+      int uj = __shfl_sync(kFull, u, j);
+      unsigned bj = __shfl_sync(kFull, base, j);
+      int nj = __shfl_sync(kFull, nch, j);
+      for (int c = lane; c < nj; c += 32) cout[bj + c] = make_int2(uj, c);
+    }
   }
   unsigned long long e = warp_sum((unsigned long long)deg);
-  if (lane_id() == 0 && e) atomicAdd(&nxt->edges, e);
+  if (lane == 0 && e) atomicAdd(&nxt->edges, e);
 }
 
 // Seeds a frontier of one vertex (used by the init kernels; block-wide).
@@ -72,16 +94,14 @@ __device__ __forceinline__ void seed_frontier(int src, const int *__restrict__ p
   }
 }
 
-// Push expansion of (qin[0..nq), cin[0..nch)).  Per source vertex v the
-// functor `load(v)` returns a 32-bit payload (e.g. its distance) that is
-// broadcast to its edges; `visit(payload, edge_index, dst)` returns true when
-// dst must join the next frontier.  Warp-uniform control flow throughout.
+// Push expansion of (qin[0..nq), cin[0..nch)).  `load(v)` gives the 32-bit
+// payload of a source vertex (e.g. its distance), broadcast to its edges.
 template <typename Load, typename Visit>
 __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
                                             const int *__restrict__ ind, const int *qin,
                                             unsigned nq, const int2 *cin, unsigned nch,
                                             int *qout, int2 *cout, LevelCounters *nxt,
-                                            int gwarp, int nwarps, Load load, Visit visit) {
+                                            int gwarp, int nwarps, Load load, Visit &visit) {
   const int lane = lane_id();
   for (unsigned base = (unsigned)gwarp * 32u; base < nq; base += (unsigned)nwarps * 32u) {
     unsigned idx = base + lane;
@@ -96,20 +116,29 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
     int incl = warp_incl_scan(d);
     int excl = incl - d;
     int total = __shfl_sync(kFull, incl, 31);
-    for (int e0 = 0; e0 < total; e0 += 32) {
-      int e = e0 + lane;
-      int owner = warp_owner(excl, e);
-      int so = __shfl_sync(kFull, s, owner);
-      int eo = __shfl_sync(kFull, excl, owner);
-      unsigned po = __shfl_sync(kFull, pay, owner);
-      bool found = false;
-      int u = -1;
-      if (e < total) {
-        int k = so + (e - eo);
-        u = __ldg(ind + k);
-        found = visit(po, k, u);
+    for (int e0 = 0; e0 < total; e0 += 32 * kUnroll) {
+      int kk[kUnroll], uu[kUnroll];
+      unsigned pp[kUnroll], aux[kUnroll];
+      bool ok[kUnroll];
+#pragma unroll
+      for (int r = 0; r < kUnroll; ++r) {
+        int e = e0 + r * 32 + lane;
+        int owner = warp_owner(excl, e);
+        int so = __shfl_sync(kFull, s, owner);
+        int eo = __shfl_sync(kFull, excl, owner);
+        pp[r] = __shfl_sync(kFull, pay, owner);
+        kk[r] = e < total ? so + (e - eo) : -1;
       }
-      discover(found, u, ptr, qout, cout, nxt);
+#pragma unroll
+      for (int r = 0; r < kUnroll; ++r) uu[r] = kk[r] >= 0 ? __ldg(ind + kk[r]) : -1;
+#pragma unroll
+      for (int r = 0; r < kUnroll; ++r)
+        ok[r] = uu[r] >= 0 && visit.check(pp[r], kk[r], uu[r], aux[r]);
+#pragma unroll
+      for (int r = 0; r < kUnroll; ++r) {
+        bool f = ok[r] && visit.commit(pp[r], kk[r], uu[r], aux[r]);
+        discover(f, uu[r], ptr, qout, cout, nxt);
+      }
     }
   }
   for (unsigned c = (unsigned)gwarp; c < nch; c += (unsigned)nwarps) {
@@ -117,15 +146,23 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
     int s = __ldg(ptr + ch.x) + ch.y * kChunk;
     int e = min(s + kChunk, __ldg(ptr + ch.x + 1));
     unsigned pay = load(ch.x);
-    for (int k0 = s; k0 < e; k0 += 32) {
-      int k = k0 + lane;
-      bool found = false;
-      int u = -1;
-      if (k < e) {
-        u = __ldg(ind + k);
-        found = visit(pay, k, u);
+    for (int k0 = s; k0 < e; k0 += 32 * kUnroll) {
+      int uu[kUnroll];
+      unsigned aux[kUnroll];
+      bool ok[kUnroll];
+#pragma unroll
+      for (int r = 0; r < kUnroll; ++r) {
+        int k = k0 + r * 32 + lane;
+        uu[r] = k < e ? __ldg(ind + k) : -1;
       }
-      discover(found, u, ptr, qout, cout, nxt);
+#pragma unroll
+      for (int r = 0; r < kUnroll; ++r)
+        ok[r] = uu[r] >= 0 && visit.check(pay, k0 + r * 32 + lane, uu[r], aux[r]);
+#pragma unroll
+      for (int r = 0; r < kUnroll; ++r) {
+        bool f = ok[r] && visit.commit(pay, k0 + r * 32 + lane, uu[r], aux[r]);
+        discover(f, uu[r], ptr, qout, cout, nxt);
+      }
     }
   }
 }

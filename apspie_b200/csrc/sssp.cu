@@ -60,6 +60,23 @@ struct Arith<float> {
   }
 };
 
+// Push visitor: relax (u, w[k]) with the source's distance du as payload.
+template <typename W>
+struct SsspVisit {
+  const W *__restrict__ w;
+  unsigned *dist;
+  int *stamp;
+  int round;
+  __device__ __forceinline__ bool check(unsigned du, int k, int u, unsigned &nd) const {
+    nd = Arith<W>::add(du, __ldg(w + k));
+    return nd < __ldcg(dist + u);
+  }
+  __device__ __forceinline__ bool commit(unsigned, int, int u, unsigned nd) const {
+    if (nd >= atomicMin(dist + u, nd)) return false;
+    return atomicExch(stamp + u, round) != round;
+  }
+};
+
 template <typename W>
 __global__ void sssp_init(int m, int src, unsigned *dist, int *stamp, const int *__restrict__ ptr,
                           int *queue, int2 *chunks, SsspState *st) {
@@ -83,7 +100,7 @@ __global__ void sssp_init(int m, int src, unsigned *dist, int *stamp, const int 
 }
 
 template <typename W>
-__global__ void __launch_bounds__(kSsspThreads)
+__global__ void __launch_bounds__(kSsspThreads, 3)
 sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
                 const W *__restrict__ w, unsigned *dist, int *stamp, int *qa, int *qb, int2 *ca,
                 int2 *cb, SsspState *st, int max_rounds) {
@@ -112,15 +129,9 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
     int *qout = (r & 1) ? qa : qb;
     int2 *cin = (r & 1) ? cb : ca;
     int2 *cout = (r & 1) ? ca : cb;
-    expand_push(
-        ptr, ind, qin, nq, cin, nch, qout, cout, nxt, gwarp, nwarps,
-        [&](int v) { return __ldcg(dist + v); },
-        [&](unsigned du, int k, int u) {
-          unsigned nd = Arith<W>::add(du, __ldg(w + k));
-          if (nd >= __ldcg(dist + u)) return false;
-          if (nd >= atomicMin(dist + u, nd)) return false;
-          return atomicExch(stamp + u, r) != r;
-        });
+    SsspVisit<W> vis{w, dist, stamp, r};
+    expand_push(ptr, ind, qin, nq, cin, nch, qout, cout, nxt, gwarp, nwarps,
+                [&](int v) { return __ldcg(dist + v); }, vis);
     if (!grid_barrier(st->bar, &st->err)) return;
   }
   // reached vertices and their out-degrees (E_R)

@@ -168,3 +168,37 @@ def neighbor_flags(ctx: Context, g, flags, out=None):
     check(lib.apspie_neighbor_flags(ctx.handle, int(g.nnz), int(g.m), _p(g.ptr), _p(g.ind),
                                     _p(flags), _p(out)), ctx.handle, "apspie_neighbor_flags")
     return out
+
+
+PLUS_TIMES, MIN_PLUS, MAX_TIMES, OR_AND = 0, 1, 2, 3
+
+
+def spmspv(ctx: Context, semiring: int, g, xind, xval=None, val=None):
+    """Sparse mXv<T>() (src/mXv.cuh:250): returns (yind, yval, expanded).
+    g.ptr / g.ind list the columns of A; val (float32 tensor, nnz) or None."""
+    import torch
+    dev = g.ptr.device
+    yind = torch.empty(max(g.m, 1), dtype=torch.int32, device=dev)
+    yval = torch.empty(max(g.m, 1), dtype=torch.float32, device=dev)
+    n = C.c_int()
+    e = C.c_int64()
+    check(lib.apspie_spmspv(ctx.handle, int(semiring), int(g.m), int(g.nnz), _p(g.ptr), _p(g.ind),
+                            _p(val), int(xind.numel()), _p(xind), _p(xval), _p(yind), _p(yval),
+                            C.byref(n), C.byref(e)), ctx.handle, "apspie_spmspv")
+    return yind[:n.value], yval[:n.value], int(e.value)
+
+
+def mxv_dense(ctx: Context, semiring: int, g, x, val=None, y=None):
+    """Dense mXv<T>() (src/mXv.cuh:111): returns (y, total)."""
+    import torch
+    if y is None:
+        y = torch.empty(g.m, dtype=torch.float32, device=g.ptr.device)
+    e = C.c_int64()
+    check(lib.apspie_mxv_dense(ctx.handle, int(semiring), int(g.m), int(g.nnz), _p(g.ptr),
+                               _p(g.ind), _p(val), _p(x), _p(y), C.byref(e)), ctx.handle,
+          "apspie_mxv_dense")
+    return y, int(e.value)
+
+
+def spmspv_set_params(ctx: Context, sort_factor: float = 4.0) -> None:
+    check(lib.apspie_spmspv_set_params(ctx.handle, float(sort_factor)), ctx.handle)

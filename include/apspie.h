@@ -147,6 +147,43 @@ int apspie_neighbor_flags(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr,
                           const int *d_ind, const int32_t *d_in,
                           int32_t *d_out);
 
+/* ------------------------------------------------------------- SpMSpV ---
+ * Semirings of the reference's three SpMSpV variants. */
+typedef enum {
+  APSPIE_PLUS_TIMES = 0, /* mXv (src/mXv.cuh:106 multiply, :201 ReduceByKey plus) */
+  APSPIE_MIN_PLUS = 1,   /* spmspvSssp (src/spmspvSssp.cuh:87 add, :232 minimum) */
+  APSPIE_MAX_TIMES = 2,  /* spmspvMis (src/spmspvMis.cuh:289 maximum) */
+  APSPIE_OR_AND = 3      /* Boolean reachability (keys-only spmspvBfs) */
+} apspie_semiring;
+
+/* Sparse x (d_xind ascending-unique, d_xval or NULL = ones) times A, where
+ * d_ptr / d_ind / d_val (NULL = ones) list A's columns: y[r] = (+) over x's
+ * entries j of A(r, j) (x) x[j].  Replaces the sparse mXv<T>()
+ * (src/mXv.cuh:250-389).  y comes back sorted by row with one entry per
+ * touched row (structural, as the reference's ReduceByKey); d_yind / d_yval
+ * must hold m entries.  *h_ynnz = nnz(y); *h_expanded (may be NULL) = number
+ * of products.  PLUS_TIMES sums in double and rounds once; MIN_PLUS and
+ * MAX_TIMES form each term with one float op, as the reference does.
+ * Synchronises (the output size goes to the host, as in the reference). */
+int apspie_spmspv(apspie_ctx ctx, int semiring, int m, int64_t nnz,
+                  const int *d_ptr, const int *d_ind, const float *d_val,
+                  int xnnz, const int *d_xind, const float *d_xval, int *d_yind,
+                  float *d_yval, int *h_ynnz, int64_t *h_expanded);
+
+/* Dense x in, dense y out: the dense mXv<T>() (src/mXv.cuh:111-247) and
+ * spmspvSssp (src/spmspvSssp.cuh:92).  The frontier is {j : x[j] > 0.5}
+ * for PLUS_TIMES (bitify, src/mXv.cuh:50), {j : -1 < x[j] < 1e38} for
+ * MIN_PLUS (src/spmspvSssp.cuh:31) and {j : x[j] != 0} otherwise; untouched
+ * y entries are 0 (1.70141e38 for MIN_PLUS), as preprocessFlag sets them.
+ * *h_expanded (may be NULL) = the reference's return value `total`. */
+int apspie_mxv_dense(apspie_ctx ctx, int semiring, int m, int64_t nnz,
+                     const int *d_ptr, const int *d_ind, const float *d_val,
+                     const float *d_x, float *d_y, int64_t *h_expanded);
+
+/* SpMSpV path choice: the bitmap (dense accumulator) path is used when
+ * products * sort_factor > m, else the radix-sort path.  Default 4. */
+int apspie_spmspv_set_params(apspie_ctx ctx, double sort_factor);
+
 /* ------------------------------------------------- host graph builders ---
  * Synthetic inputs of the benchmark configurations (no reference
  * counterpart: the reference reads .mtx files, src/util.cuh:355-430).
