@@ -6,14 +6,15 @@ is the device allocator and stream provider only); every compute call goes
 through the native library, which raises on import if it is not built.
 """
 from ._native import ApspieError, lib  # noqa: F401  (raises if the .so is missing)
-from .graph import (DeviceGraph, HostGraph, from_edges, gen_er, gen_grid, gen_rmat,  # noqa: F401
+from .graph import (DeviceGraph, HostGraph, from_edges, gen_er, gen_grid, gen_powerlaw, gen_rmat,  # noqa: F401
                     largest_cc_vertex, mt19937, read_mtx, seeded_sources, weights_f32, weights_u32)
 from .ops import (Context, bfs, bfs_set_params, bfs_stats, bfs_trace, mis, mis_rounds,  # noqa: F401
                   neighbor_flags, sssp, sssp_stats, spmspv, mxv_dense, spmspv_set_params,
-                  PLUS_TIMES, MIN_PLUS, MAX_TIMES, OR_AND)
+                  PLUS_TIMES, MIN_PLUS, MAX_TIMES, OR_AND, spgemm, tc_prepare,
+                  triangle_count)
 
 __all__ = [
     "ApspieError", "Context", "DeviceGraph", "HostGraph", "bfs", "bfs_set_params", "bfs_stats", "bfs_trace", "from_edges",
-    "sssp", "sssp_stats", "mis", "mis_rounds", "neighbor_flags", "spmspv", "mxv_dense", "spmspv_set_params", "gen_er", "gen_grid", "gen_rmat", "largest_cc_vertex", "mt19937", "read_mtx", "seeded_sources",
+    "sssp", "sssp_stats", "mis", "mis_rounds", "neighbor_flags", "spmspv", "mxv_dense", "spmspv_set_params", "spgemm", "tc_prepare", "triangle_count", "gen_er", "gen_grid", "gen_powerlaw", "gen_rmat", "largest_cc_vertex", "mt19937", "read_mtx", "seeded_sources",
     "weights_f32", "weights_u32",
 ]

@@ -36,6 +36,11 @@ class SsspStats(C.Structure):
                 ("edges_traversed", C.c_int64), ("relaxations", C.c_int64)]
 
 
+class Csr(C.Structure):
+    _fields_ = [("m", C.c_int), ("n", C.c_int), ("nnz", C.c_int64), ("d_ptr", C.c_void_p),
+                ("d_ind", C.c_void_p), ("d_val", C.c_void_p)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/apspie.h
 PROTOS: dict[str, tuple] = {
     "apspie_ctx_create": (c_int, [c_int, vp, P_vp]),
@@ -60,11 +65,18 @@ PROTOS: dict[str, tuple] = {
                               P_i64]),
     "apspie_mxv_dense": (c_int, [vp, c_int, c_int, c_i64, vp, vp, vp, vp, vp, P_i64]),
     "apspie_spmspv_set_params": (c_int, [vp, C.c_double]),
+    "apspie_spgemm": (c_int, [vp, C.POINTER(Csr), C.POINTER(Csr), C.POINTER(Csr)]),
+    "apspie_csr_free": (c_int, [vp, C.POINTER(Csr)]),
+    "apspie_csr_copy_out": (c_int, [vp, C.POINTER(Csr), vp, vp, vp]),
+    "apspie_tc_prepare": (c_int, [vp, c_i64, c_int, vp, vp, vp, vp, vp, P_i64]),
+    "apspie_tc": (c_int, [vp, c_int, c_i64, vp, vp, P_i64]),
     "apspie_gen_rmat_host": (c_int, [c_int, c_int, c_u64, c_int, c_int, P_int, P_i64, P_vp, P_vp]),
     "apspie_gen_er_host": (c_int, [c_int, c_int, c_u64, P_i64, P_vp, P_vp]),
     "apspie_gen_grid_host": (c_int, [c_int, c_int, P_i64, P_vp, P_vp]),
     "apspie_gen_weights_u32_host": (c_int, [c_int, vp, vp, c_u64, c_u32, c_u32, vp]),
     "apspie_gen_weights_f32_host": (c_int, [c_int, vp, vp, c_u64, vp]),
+    "apspie_gen_powerlaw_host": (c_int, [c_int, c_int, C.c_double, C.c_double, c_int, c_u64,
+                                         C.POINTER(C.c_double), P_i64, P_vp, P_vp, P_vp]),
     "apspie_mt19937_fill_host": (c_int, [c_u32, c_i64, vp]),
     "apspie_read_mtx_host": (c_int, [C.c_char_p, c_int, P_int, P_i64, P_vp, P_vp, P_vp, P_int]),
     "apspie_host_free": (None, [vp]),

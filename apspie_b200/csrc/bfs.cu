@@ -31,8 +31,7 @@ namespace apspie {
 namespace {
 
 constexpr int kBfsThreads = 512;
-constexpr int kProbe = 4;         // in-neighbours a lane loads per batch in a pull level
-constexpr int kLaneScan = 64;     // in-neighbours a lane scans before the warp takes over
+constexpr int kProbe = 4;         // in-neighbours a lane probes alone in a pull level
 constexpr int kTraceLevels = 64;  // levels recorded in the per-run trace
 
 struct LevelTrace {
@@ -95,6 +94,8 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
   __shared__ unsigned s_q, s_chunks, s_nbig;
   __shared__ unsigned long long s_edges;
+  __shared__ unsigned s_found[kBfsThreads / 32];
+  const int warp = warp_in_block();
 
   if (blockIdx.x == 0 && threadIdx.x == 0) st->t_start = globaltimer();
   bool pull = false;
@@ -151,11 +152,12 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
     } else {
       ++pull_levels;
       // ---- pull: unvisited vertices look for a parent at depth L ----
-      // Each lane scans the in-neighbours of its own vertex in batches of
-      // kProbe (all index loads of a batch, then all depth loads, so a lane
-      // keeps kProbe loads in flight), for up to kLaneScan neighbours; the
-      // rare vertices with longer unresolved lists are then swept by the
-      // whole warp, 32 neighbours per step.
+      // Each lane first probes kProbe in-neighbours of its own vertex (all
+      // index loads, then all depth loads).  The remaining in-neighbours of
+      // the still-unresolved vertices of the warp are then laid out flat
+      // (warp scan) and dealt 32 x kUnroll at a time, like a push gather; a
+      // hit sets the owner's bit in a per-warp mask, slots of resolved owners
+      // are skipped, and the warp stops once every owner is resolved.
       for (int base = gwarp * 32; base < m; base += nwarps * 32) {
         int v = base + lane;
         int s = 0, e = 0;
@@ -164,30 +166,42 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
           s = __ldg(tptr + v);
           e = __ldg(tptr + v + 1);
         }
-        const int lane_end = min(e, s + kLaneScan);
-        while (s < lane_end && !found) {
+        if (s < e) {
           int nb[kProbe];
 #pragma unroll
-          for (int i = 0; i < kProbe; ++i) nb[i] = s + i < lane_end ? __ldg(tind + s + i) : -1;
+          for (int i = 0; i < kProbe; ++i) nb[i] = s + i < e ? __ldg(tind + s + i) : -1;
 #pragma unroll
           for (int i = 0; i < kProbe; ++i) found |= nb[i] >= 0 && __ldcg(depth + nb[i]) == L;
-          s += kProbe;
+          s = min(s + kProbe, e);
         }
-        unsigned mask = __ballot_sync(kFull, !found && s < e);
-        while (mask) {
-          int j = __ffs(mask) - 1;
-          mask &= mask - 1;
-          int sj = __shfl_sync(kFull, s, j);
-          int ej = __shfl_sync(kFull, e, j);
-          for (int k0 = sj; k0 < ej; k0 += 32) {
-            int k = k0 + lane;
-            bool hit = false;
-            if (k < ej) hit = __ldcg(depth + __ldg(tind + k)) == L;
-            if (__any_sync(kFull, hit)) {
-              if (lane == j) found = true;
-              break;
+        int d = found ? 0 : e - s;
+        int incl = warp_incl_scan(d);
+        int excl = incl - d;
+        int total = __shfl_sync(kFull, incl, 31);
+        if (total) {
+          const unsigned want = __ballot_sync(kFull, d > 0);
+          if (lane == 0) s_found[warp] = 0u;
+          __syncwarp();
+          for (int e0 = 0; e0 < total; e0 += 32 * kUnroll) {
+            int nb[kUnroll], own[kUnroll];
+            const unsigned done = *(volatile unsigned *)&s_found[warp];
+#pragma unroll
+            for (int r = 0; r < kUnroll; ++r) {
+              int ee = e0 + r * 32 + lane;
+              int owner = warp_owner(excl, ee);
+              int so = __shfl_sync(kFull, s, owner);
+              int eo = __shfl_sync(kFull, excl, owner);
+              own[r] = owner;
+              nb[r] = (ee < total && !((done >> owner) & 1u)) ? __ldg(tind + so + (ee - eo)) : -1;
             }
+#pragma unroll
+            for (int r = 0; r < kUnroll; ++r)
+              if (nb[r] >= 0 && __ldcg(depth + nb[r]) == L) atomicOr(&s_found[warp], 1u << own[r]);
+            __syncwarp();
+            if ((*(volatile unsigned *)&s_found[warp] & want) == want) break;
           }
+          found |= (*(volatile unsigned *)&s_found[warp] >> lane) & 1u;
+          __syncwarp();
         }
         if (found) depth[v] = next;
         discover(found, v, ptr, qout, cout, nxt);

@@ -24,7 +24,7 @@
 namespace apspie {
 
 constexpr int kBigDeg = 64;   // out-degree above which a vertex is chunked
-constexpr int kChunk = 256;   // edges per chunk
+constexpr int kChunk = 128;   // edges per chunk (one unrolled batch of a warp)
 constexpr int kUnroll = 4;    // rounds of 32 edges issued together
 
 struct LevelCounters {
@@ -41,38 +41,75 @@ inline size_t chunk_capacity(long long nnz) {
   return (size_t)(nnz / kChunk + nnz / kBigDeg + 2);
 }
 
-// Called by all 32 lanes; lanes with found == true append vertex u.
-__device__ __forceinline__ void discover(bool found, int u, const int *__restrict__ ptr,
-                                         int *qout, int2 *cout, LevelCounters *nxt) {
+// Called by all 32 lanes with N candidates per lane; candidate r of a lane
+// joins the next frontier when found[r].  One queue append, one chunk
+// reservation and one edge-count update per warp for all N x 32 candidates.
+template <int N>
+__device__ __forceinline__ void discover_n(const bool (&found)[N], const int (&u)[N],
+                                           const int *__restrict__ ptr, int *qout, int2 *cout,
+                                           LevelCounters *nxt) {
   const int lane = lane_id();
-  int deg = 0;
-  if (found) deg = __ldg(ptr + u + 1) - __ldg(ptr + u);
-  bool big = found && deg > kBigDeg;
-  bool small = found && !big;
-  unsigned slot = warp_append(small, &nxt->q);
-  if (small) qout[slot] = u;
-  unsigned bmask = __ballot_sync(kFull, big);
+  int deg[N];
+#pragma unroll
+  for (int r = 0; r < N; ++r) deg[r] = found[r] ? __ldg(ptr + u[r] + 1) - __ldg(ptr + u[r]) : 0;
+  int nsmall = 0, nbig = 0, nchunk = 0;
+  unsigned long long edges = 0;
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    bool big = found[r] && deg[r] > kBigDeg;
+    nsmall += (found[r] && !big) ? 1 : 0;
+    nbig += big ? 1 : 0;
+    nchunk += big ? (deg[r] + kChunk - 1) / kChunk : 0;
+    edges += (unsigned long long)deg[r];
+  }
+  // queue slots
+  int qincl = warp_incl_scan(nsmall);
+  int qtot = __shfl_sync(kFull, qincl, 31);
+  if (qtot) {
+    unsigned qbase = 0;
+    if (lane == 31) qbase = atomicAdd(&nxt->q, (unsigned)qtot);
+    qbase = __shfl_sync(kFull, qbase, 31) + (unsigned)(qincl - nsmall);
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+      if (found[r] && deg[r] <= kBigDeg) qout[qbase++] = u[r];
+  }
+  // chunk entries of big vertices, written cooperatively
+  unsigned bmask = __ballot_sync(kFull, nbig > 0);
   if (bmask) {
-    int nch = big ? (deg + kChunk - 1) / kChunk : 0;
-    int incl = warp_incl_scan(nch);
-    int total = __shfl_sync(kFull, incl, 31);
-    unsigned base = 0;
+    int cincl = warp_incl_scan(nchunk);
+    int ctot = __shfl_sync(kFull, cincl, 31);
+    int btot = warp_sum(nbig);
+    unsigned cbase = 0;
     if (lane == 0) {
-      base = atomicAdd(&nxt->chunks, (unsigned)total);
-      atomicAdd(&nxt->nbig, (unsigned)__popc(bmask));
+      cbase = atomicAdd(&nxt->chunks, (unsigned)ctot);
+      atomicAdd(&nxt->nbig, (unsigned)btot);
     }
-    base = __shfl_sync(kFull, base, 0) + (unsigned)(incl - nch);
-    while (bmask) {
-      int j = __ffs(bmask) - 1;
-      bmask &= bmask - 1;
-      int uj = __shfl_sync(kFull, u, j);
-      unsigned bj = __shfl_sync(kFull, base, j);
-      int nj = __shfl_sync(kFull, nch, j);
-      for (int c = lane; c < nj; c += 32) cout[bj + c] = make_int2(uj, c);
+    cbase = __shfl_sync(kFull, cbase, 0) + (unsigned)(cincl - nchunk);
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      bool big = found[r] && deg[r] > kBigDeg;
+      int nch = big ? (deg[r] + kChunk - 1) / kChunk : 0;
+      unsigned rm = __ballot_sync(kFull, big);
+      while (rm) {
+        int j = __ffs(rm) - 1;
+        rm &= rm - 1;
+        int uj = __shfl_sync(kFull, u[r], j);
+        unsigned bj = __shfl_sync(kFull, cbase, j);
+        int nj = __shfl_sync(kFull, nch, j);
+        for (int c = lane; c < nj; c += 32) cout[bj + c] = make_int2(uj, c);
+      }
+      cbase += (unsigned)nch;
     }
   }
-  unsigned long long e = warp_sum((unsigned long long)deg);
-  if (lane == 0 && e) atomicAdd(&nxt->edges, e);
+  edges = warp_sum(edges);
+  if (lane == 0 && edges) atomicAdd(&nxt->edges, edges);
+}
+
+__device__ __forceinline__ void discover(bool found, int u, const int *__restrict__ ptr,
+                                         int *qout, int2 *cout, LevelCounters *nxt) {
+  bool f[1] = {found};
+  int uu[1] = {u};
+  discover_n<1>(f, uu, ptr, qout, cout, nxt);
 }
 
 // Seeds a frontier of one vertex (used by the init kernels; block-wide).
@@ -134,11 +171,10 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
 #pragma unroll
       for (int r = 0; r < kUnroll; ++r)
         ok[r] = uu[r] >= 0 && visit.check(pp[r], kk[r], uu[r], aux[r]);
+      bool f[kUnroll];
 #pragma unroll
-      for (int r = 0; r < kUnroll; ++r) {
-        bool f = ok[r] && visit.commit(pp[r], kk[r], uu[r], aux[r]);
-        discover(f, uu[r], ptr, qout, cout, nxt);
-      }
+      for (int r = 0; r < kUnroll; ++r) f[r] = ok[r] && visit.commit(pp[r], kk[r], uu[r], aux[r]);
+      discover_n<kUnroll>(f, uu, ptr, qout, cout, nxt);
     }
   }
   for (unsigned c = (unsigned)gwarp; c < nch; c += (unsigned)nwarps) {
@@ -158,11 +194,11 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
 #pragma unroll
       for (int r = 0; r < kUnroll; ++r)
         ok[r] = uu[r] >= 0 && visit.check(pay, k0 + r * 32 + lane, uu[r], aux[r]);
+      bool f[kUnroll];
 #pragma unroll
-      for (int r = 0; r < kUnroll; ++r) {
-        bool f = ok[r] && visit.commit(pay, k0 + r * 32 + lane, uu[r], aux[r]);
-        discover(f, uu[r], ptr, qout, cout, nxt);
-      }
+      for (int r = 0; r < kUnroll; ++r)
+        f[r] = ok[r] && visit.commit(pay, k0 + r * 32 + lane, uu[r], aux[r]);
+      discover_n<kUnroll>(f, uu, ptr, qout, cout, nxt);
     }
   }
 }

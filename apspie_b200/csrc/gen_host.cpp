@@ -264,6 +264,93 @@ int apspie_mt19937_fill_host(uint32_t seed, int64_t n, uint32_t *h_out) {
   return APSPIE_OK;
 }
 
+// Mean of floor(X) for X ~ Pareto(alpha, xmin) truncated at T (continuous).
+static double powerlaw_floor_mean(double alpha, double xmin, double T, int max_deg) {
+  double tail = std::pow(xmin / T, alpha - 1.0);
+  double mean = 0.0;
+  for (int k = 1; k <= max_deg; ++k) {
+    double p = (double)k <= xmin ? 1.0 : (std::pow(xmin / k, alpha - 1.0) - tail) / (1.0 - tail);
+    if (p <= 0) break;
+    mean += p;
+  }
+  return mean;
+}
+
+int apspie_gen_powerlaw_host(int m, int n, double alpha, double mean, int max_deg, uint64_t seed,
+                             double *xmin_out, int64_t *nnz_out, int **h_ptr, int **h_ind,
+                             float **h_val) {
+  if (m < 1 || n < 1 || alpha <= 1.0 || mean < 1.0 || max_deg < 1 || !nnz_out || !h_ptr ||
+      !h_ind || !h_val)
+    return APSPIE_ERR_INVALID;
+  const double T = (double)max_deg + 1.0;
+  // x_min such that E[floor(X)] = mean, by bisection
+  double lo = 1.0, hi = (double)max_deg;
+  for (int it = 0; it < 200; ++it) {
+    double mid = 0.5 * (lo + hi);
+    if (powerlaw_floor_mean(alpha, mid, T, max_deg) < mean) lo = mid; else hi = mid;
+  }
+  const double xmin = 0.5 * (lo + hi);
+  if (xmin_out) *xmin_out = xmin;
+  const double tail = std::pow(xmin / T, alpha - 1.0);
+  const uint64_t sd = mix64(seed ^ 0x504c4157ull);
+  std::vector<int> k((size_t)m);
+  parallel_for(m, [&](int64_t b, int64_t e, int) {
+    for (int64_t i = b; i < e; ++i) {
+      // u uniform in (0, 1]; inverse CDF of the truncated Pareto
+      double u = ((double)(mix64(sd ^ (uint64_t)i) >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+      double x = xmin * std::pow(1.0 - u * (1.0 - tail), -1.0 / (alpha - 1.0));
+      int d = (int)std::floor(x);
+      k[(size_t)i] = std::max(1, std::min(d, std::min(max_deg, n)));
+    }
+  });
+  std::vector<int64_t> off((size_t)m + 1, 0);
+  for (int i = 0; i < m; ++i) off[(size_t)i + 1] = off[(size_t)i] + k[(size_t)i];
+  std::vector<int> cols((size_t)off[(size_t)m]);
+  std::vector<int> cnt((size_t)m);
+  parallel_for(m, [&](int64_t b, int64_t e, int) {
+    for (int64_t i = b; i < e; ++i) {
+      int *c = cols.data() + off[(size_t)i];
+      int ki = k[(size_t)i];
+      for (int t = 0; t < ki; ++t) {
+        uint64_t h = mix64(mix64(sd ^ 0xC01ull ^ ((uint64_t)i << 20)) ^ (uint64_t)t);
+        c[t] = (int)(((h & 0xffffffffull) * (uint64_t)n) >> 32);
+      }
+      std::sort(c, c + ki);
+      cnt[(size_t)i] = (int)(std::unique(c, c + ki) - c);
+    }
+  });
+  int64_t nnz = 0;
+  for (int i = 0; i < m; ++i) nnz += cnt[(size_t)i];
+  if (nnz >= (int64_t)INT32_MAX) return APSPIE_ERR_OVERFLOW;
+  int *ptr = (int *)malloc(sizeof(int) * ((size_t)m + 1));
+  int *ind = (int *)malloc(sizeof(int) * (size_t)std::max<int64_t>(1, nnz));
+  float *val = (float *)malloc(sizeof(float) * (size_t)std::max<int64_t>(1, nnz));
+  if (!ptr || !ind || !val) {
+    free(ptr);
+    free(ind);
+    free(val);
+    return APSPIE_ERR_OOM;
+  }
+  ptr[0] = 0;
+  for (int i = 0; i < m; ++i) ptr[i + 1] = ptr[i] + cnt[(size_t)i];
+  parallel_for(m, [&](int64_t b, int64_t e, int) {
+    for (int64_t i = b; i < e; ++i) {
+      const int *c = cols.data() + off[(size_t)i];
+      for (int t = 0; t < cnt[(size_t)i]; ++t) {
+        int p = ptr[i] + t;
+        ind[p] = c[t];
+        uint64_t h = mix64(mix64(sd ^ 0x7A1ull) ^ (((uint64_t)i << 32) | (uint32_t)c[t]));
+        val[p] = (float)((double)(h >> 40) * (1.0 / 8388608.0) - 1.0);  // k*2^-23 - 1 in [-1, 1)
+      }
+    }
+  });
+  *nnz_out = nnz;
+  *h_ptr = ptr;
+  *h_ind = ind;
+  *h_val = val;
+  return APSPIE_OK;
+}
+
 void apspie_host_free(void *p) { free(p); }
 
 }  // extern "C"

@@ -1,0 +1,342 @@
+// tc.cu -- triangle counting as an L-masked hash SpGEMM with an int64 count,
+// and the device-side degree relabelling that builds L.
+//
+// Replaces the reference's TC path (test/tc/main.cu:139-261): host buildLower
+// of the strict lower / upper triangles, cuSPARSE csrgemm U * L materialising
+// every wedge (src/tc.cuh:63-165), the ewiseMultTc merge-intersect
+// (src/tc.cuh:169-199) and a float mgpu::Reduce.  Here nothing but the count
+// is produced: for each row i of L, L(i,:) goes into a shared-memory hash
+// set, and every wedge j in L(k,:) for k in L(i,:) probes it; a hit is a
+// triangle (i > k > j).  Rows are binned by |L(i,:)|: one warp per row up to
+// 256 entries (table 512), one block per row up to 4096 (table 8192), and a
+// binary-search fallback over the sorted row beyond that.  Per-warp partial
+// counts are summed in 64-bit and added with one atomic per warp.
+//
+// tc_prepare relabels vertices by ascending (degree, id) with the stable
+// radix sort, keeps the edges with new(col) < new(row), sorts them by
+// (row, col) with one radix sort on the packed key and builds L's offsets.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+
+#include "common.cuh"
+#include "context.h"
+#include "primitives.cuh"
+
+namespace apspie {
+namespace {
+
+constexpr int kTcWarpMax = 256, kTcWarpTable = 512;
+constexpr int kTcBlockMax = 4096, kTcBlockTable = 8192;
+constexpr int kTcThreads = 256;
+constexpr int kTcWarps = 4;
+constexpr int kNone = INT_MAX;
+
+__device__ __forceinline__ unsigned tc_hash(int j) { return (unsigned)j * 0x9E3779B1u; }
+
+__device__ __forceinline__ void set_insert(int *keys, int bits, int j) {
+  unsigned mask = (1u << bits) - 1u, h = tc_hash(j) >> (32 - bits);
+  for (unsigned p = 0; p <= mask; ++p) {
+    int old = atomicCAS(keys + h, kNone, j);
+    if (old == kNone || old == j) return;
+    h = (h + 1) & mask;
+  }
+}
+
+__device__ __forceinline__ bool set_has(const int *keys, int bits, int j) {
+  unsigned mask = (1u << bits) - 1u, h = tc_hash(j) >> (32 - bits);
+  for (unsigned p = 0; p <= mask; ++p) {
+    int k = keys[h];
+    if (k == j) return true;
+    if (k == kNone) return false;
+    h = (h + 1) & mask;
+  }
+  return false;
+}
+
+__device__ __forceinline__ int tbits(int n, int cap) {
+  int b = 5;
+  while ((1 << b) < 2 * n && b < cap) ++b;
+  return b;
+}
+
+struct TcBins {
+  unsigned n[3];
+  unsigned pad;
+  unsigned long long count;
+};
+
+__global__ void tc_bin(int m, const int *__restrict__ Lp, int *lists, TcBins *bins) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    int d = Lp[i + 1] - Lp[i];
+    if (d < 2) continue;  // a triangle needs two lower neighbours
+    int b = d <= kTcWarpMax ? 0 : (d <= kTcBlockMax ? 1 : 2);
+    unsigned s = atomicAdd(&bins->n[b], 1u);
+    lists[(size_t)b * m + s] = i;
+  }
+}
+
+// Wedges of row i dealt over a group (warp or block): visit(j) per wedge.
+template <bool WARP, typename F>
+__device__ __forceinline__ void for_each_wedge(int i, const int *__restrict__ Lp,
+                                               const int *__restrict__ Li, int *s_off, int *s_bs,
+                                               F visit) {
+  const int a0 = __ldg(Lp + i), a1 = __ldg(Lp + i + 1);
+  const int width = WARP ? 32 : (int)blockDim.x;
+  const int tid = WARP ? lane_id() : (int)threadIdx.x;
+  for (int c0 = a0; c0 < a1; c0 += width) {
+    int a = c0 + tid, bs = 0, d = 0;
+    if (a < a1) {
+      int k = __ldg(Li + a);
+      bs = __ldg(Lp + k);
+      d = __ldg(Lp + k + 1) - bs;
+    }
+    int excl, total;
+    if (WARP) {
+      int incl = warp_incl_scan(d);
+      excl = incl - d;
+      total = __shfl_sync(kFull, incl, 31);
+    } else {
+      __shared__ int sw[33];
+      excl = block_excl_scan(d, sw, &total);
+    }
+    s_off[tid] = excl;
+    s_bs[tid] = bs;
+    if (WARP) __syncwarp(); else __syncthreads();
+    const int n_a = min(width, a1 - c0);
+    for (int p = tid; p < total; p += width) {
+      int lo = 0, hi = n_a - 1;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (s_off[mid] <= p) lo = mid; else hi = mid - 1;
+      }
+      visit(__ldg(Li + s_bs[lo] + (p - s_off[lo])));
+    }
+    if (WARP) __syncwarp(); else __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(32 * kTcWarps)
+tc_warp_rows(const int *list, TcBins *bins, const int *__restrict__ Lp, const int *__restrict__ Li) {
+  __shared__ int s_keys[kTcWarps][kTcWarpTable];
+  __shared__ int s_off[kTcWarps][32], s_bs[kTcWarps][32];
+  const int w = warp_in_block(), lane = lane_id();
+  int *keys = s_keys[w];
+  unsigned long long cnt = 0;
+  const unsigned nrows = bins->n[0];
+  for (unsigned r = blockIdx.x * kTcWarps + w; r < nrows; r += gridDim.x * kTcWarps) {
+    int i = list[r];
+    int a0 = __ldg(Lp + i), d = __ldg(Lp + i + 1) - a0;
+    int bits = tbits(d, 9);
+    for (int t = lane; t < (1 << bits); t += 32) keys[t] = kNone;
+    __syncwarp();
+    for (int t = lane; t < d; t += 32) set_insert(keys, bits, __ldg(Li + a0 + t));
+    __syncwarp();
+    for_each_wedge<true>(i, Lp, Li, s_off[w], s_bs[w],
+                         [&](int j) { cnt += set_has(keys, bits, j) ? 1 : 0; });
+    __syncwarp();
+  }
+  cnt = warp_sum(cnt);
+  if (lane == 0 && cnt) atomicAdd(&bins->count, cnt);
+}
+
+__global__ void __launch_bounds__(kTcThreads)
+tc_block_rows(const int *list, TcBins *bins, const int *__restrict__ Lp, const int *__restrict__ Li) {
+  __shared__ int keys[kTcBlockTable];
+  __shared__ int s_off[kTcThreads], s_bs[kTcThreads];
+  unsigned long long cnt = 0;
+  const unsigned nrows = bins->n[1];
+  for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
+    int i = list[r];
+    int a0 = __ldg(Lp + i), d = __ldg(Lp + i + 1) - a0;
+    int bits = tbits(d, 13);
+    for (int t = threadIdx.x; t < (1 << bits); t += blockDim.x) keys[t] = kNone;
+    __syncthreads();
+    for (int t = threadIdx.x; t < d; t += blockDim.x) set_insert(keys, bits, __ldg(Li + a0 + t));
+    __syncthreads();
+    for_each_wedge<false>(i, Lp, Li, s_off, s_bs,
+                          [&](int j) { cnt += set_has(keys, bits, j) ? 1 : 0; });
+    __syncthreads();
+  }
+  cnt = warp_sum(cnt);
+  if (lane_id() == 0 && cnt) atomicAdd(&bins->count, cnt);
+}
+
+// Rows longer than the block table: binary search in the sorted row.
+__global__ void __launch_bounds__(kTcThreads)
+tc_search_rows(const int *list, TcBins *bins, const int *__restrict__ Lp, const int *__restrict__ Li) {
+  __shared__ int s_off[kTcThreads], s_bs[kTcThreads];
+  unsigned long long cnt = 0;
+  const unsigned nrows = bins->n[2];
+  for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
+    int i = list[r];
+    const int a0 = __ldg(Lp + i), a1 = __ldg(Lp + i + 1);
+    for_each_wedge<false>(i, Lp, Li, s_off, s_bs, [&](int j) {
+      int lo = a0, hi = a1;
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(Li + mid) < j) lo = mid + 1; else hi = mid;
+      }
+      cnt += (lo < a1 && __ldg(Li + lo) == j) ? 1 : 0;
+    });
+  }
+  cnt = warp_sum(cnt);
+  if (lane_id() == 0 && cnt) atomicAdd(&bins->count, cnt);
+}
+
+// ------------------------------------------------------------- prepare ---
+__global__ void degree_keys(int m, const int *__restrict__ ptr, unsigned *keys, int *ids,
+                            unsigned *maxdeg) {
+  unsigned mx = 0;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < m; v += gridDim.x * blockDim.x) {
+    unsigned d = (unsigned)(__ldg(ptr + v + 1) - __ldg(ptr + v));
+    keys[v] = d;
+    ids[v] = v;
+    mx = max(mx, d);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+  if (lane_id() == 0) atomicMax(maxdeg, mx);
+}
+
+__global__ void rank_to_perm(int m, const int *order, int *perm) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x)
+    perm[order[r]] = r;
+}
+
+__global__ void lower_edges(int m, int cbits, const int *__restrict__ ptr,
+                            const int *__restrict__ ind, const int *__restrict__ perm,
+                            unsigned long long *keys, unsigned *count) {
+  const int lane = lane_id();
+  const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  for (int u = gwarp; u < m; u += nwarps) {
+    const int pu = __ldg(perm + u);
+    const int s = __ldg(ptr + u), e = __ldg(ptr + u + 1);
+    for (int k0 = s; k0 < e; k0 += 32) {
+      int k = k0 + lane;
+      int pv = k < e ? __ldg(perm + __ldg(ind + k)) : INT_MAX;
+      bool keep = pv < pu;
+      unsigned slot = warp_append(keep, count);
+      if (keep) keys[slot] = ((unsigned long long)pu << cbits) | (unsigned)pv;
+    }
+  }
+}
+
+__global__ void unpack_lower(long long n, int cbits, const unsigned long long *keys, int *Li,
+                             int *rowcnt) {
+  const unsigned long long mask = (1ull << cbits) - 1ull;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    unsigned long long k = keys[t];
+    Li[t] = (int)(k & mask);
+    atomicAdd(rowcnt + (int)(k >> cbits), 1);
+  }
+}
+
+__global__ void zero_ints(int n, int *p) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0;
+}
+
+int tgrid(apspie_context *ctx, long long n, int threads, int per_sm = 16) {
+  long long g = (n + threads - 1) / threads;
+  return (int)std::max(1ll, std::min(g, (long long)ctx->num_sms * per_sm));
+}
+
+}  // namespace
+}  // namespace apspie
+
+using namespace apspie;
+
+extern "C" {
+
+int apspie_tc_prepare(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr, const int *d_ind,
+                      int *d_perm, int *d_Lptr, int *d_Lind, int64_t *h_lnnz) {
+  APSPIE_CHECK_CTX(ctx);
+  if (m <= 0 || nnz < 0 || nnz >= (int64_t)INT32_MAX || !d_ptr || !d_perm || !d_Lptr ||
+      (nnz > 0 && (!d_ind || !d_Lind)) || !h_lnnz)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_tc_prepare: bad arguments");
+  cudaStream_t st = ctx->stream;
+  const int cbits = bits_for(m);
+  if (2 * cbits > 62) return set_error(ctx, APSPIE_ERR_OVERFLOW, "apspie_tc_prepare: m too large");
+  // 1. order by (degree, id): stable radix sort of degree keys over ids
+  auto *dk = (unsigned *)workspace(ctx, kSlotSortKeysA, sizeof(unsigned) * (size_t)m);
+  auto *dk2 = (unsigned *)workspace(ctx, kSlotSortKeysB, sizeof(unsigned) * (size_t)m);
+  auto *ids = (int *)workspace(ctx, kSlotSortValsA, sizeof(int) * (size_t)m);
+  auto *ids2 = (int *)workspace(ctx, kSlotSortValsB, sizeof(int) * (size_t)m);
+  auto *small = (unsigned *)workspace(ctx, kSlotSmall, 64);
+  if (!dk || !dk2 || !ids || !ids2 || !small) return APSPIE_ERR_OOM;
+  cudaMemsetAsync(small, 0, 64, st);
+  degree_keys<<<tgrid(ctx, m, 256), 256, 0, st>>>(m, d_ptr, dk, ids, small);
+  int rc = check_launch(ctx, "degree_keys");
+  if (rc) return rc;
+  unsigned *hs = (unsigned *)pinned(ctx, 64);
+  if (!hs) return APSPIE_ERR_OOM;
+  cudaMemcpyAsync(hs, small, 8, cudaMemcpyDeviceToHost, st);
+  rc = check_cuda(ctx, cudaStreamSynchronize(st), "tc_prepare maxdeg");
+  if (rc) return rc;
+  const int dbits = std::max(1, bits_for((long long)hs[0] + 1));
+  bool in_b = false;
+  rc = device_radix_sort<unsigned, int>(ctx, dk, ids, dk2, ids2, m, dbits, &in_b);
+  if (rc) return rc;
+  rank_to_perm<<<tgrid(ctx, m, 256), 256, 0, st>>>(m, in_b ? ids2 : ids, d_perm);
+  // 2. keep new(v) < new(u), packed (new(u) << cbits | new(v))
+  size_t cap = (size_t)std::max<int64_t>(1, nnz);
+  auto *ka = (unsigned long long *)workspace(ctx, kSlotMisc0, sizeof(unsigned long long) * cap);
+  auto *kb = (unsigned long long *)workspace(ctx, kSlotMisc1, sizeof(unsigned long long) * cap);
+  auto *va = (int *)workspace(ctx, kSlotMisc2, sizeof(int) * cap);
+  auto *vb = (int *)workspace(ctx, kSlotMisc3, sizeof(int) * cap);
+  if (!ka || !kb || !va || !vb) return APSPIE_ERR_OOM;
+  lower_edges<<<tgrid(ctx, (long long)m * 32, 256), 256, 0, st>>>(m, cbits, d_ptr, d_ind, d_perm,
+                                                                  ka, small + 2);
+  rc = check_launch(ctx, "lower_edges", 2);
+  if (rc) return rc;
+  cudaMemcpyAsync(hs, small + 2, 4, cudaMemcpyDeviceToHost, st);
+  rc = check_cuda(ctx, cudaStreamSynchronize(st), "tc_prepare count");
+  if (rc) return rc;
+  const long long lnnz = hs[0];
+  // 3. sort by (row, col); values are unused
+  rc = device_radix_sort<unsigned long long, int>(ctx, ka, va, kb, vb, lnnz, 2 * cbits, &in_b);
+  if (rc) return rc;
+  // 4. columns and row offsets
+  zero_ints<<<tgrid(ctx, m + 1, 256), 256, 0, st>>>(m + 1, d_Lptr);
+  unpack_lower<<<tgrid(ctx, lnnz, 256), 256, 0, st>>>(lnnz, cbits, in_b ? kb : ka, d_Lind,
+                                                      d_Lptr);
+  rc = check_launch(ctx, "unpack_lower", 2);
+  if (rc) return rc;
+  // d_Lptr[i] holds row i's count and d_Lptr[m] = 0: the exclusive scan of
+  // the m + 1 entries is the offset array
+  rc = device_exclusive_scan<int>(ctx, d_Lptr, d_Lptr, (long long)m + 1, nullptr);
+  if (rc) return rc;
+  *h_lnnz = lnnz;
+  return APSPIE_OK;
+}
+
+int apspie_tc(apspie_ctx ctx, int m, int64_t lnnz, const int *d_Lptr, const int *d_Lind,
+              int64_t *h_count) {
+  APSPIE_CHECK_CTX(ctx);
+  if (m <= 0 || lnnz < 0 || !d_Lptr || (lnnz > 0 && !d_Lind) || !h_count)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_tc: bad arguments");
+  cudaStream_t st = ctx->stream;
+  auto *lists = (int *)workspace(ctx, kSlotMisc0, sizeof(int) * 3 * (size_t)m);
+  auto *bins = (TcBins *)workspace(ctx, kSlotSmall, sizeof(TcBins));
+  if (!lists || !bins) return APSPIE_ERR_OOM;
+  cudaMemsetAsync(bins, 0, sizeof(TcBins), st);
+  tc_bin<<<tgrid(ctx, m, 256), 256, 0, st>>>(m, d_Lptr, lists, bins);
+  tc_warp_rows<<<ctx->num_sms * 16, 32 * kTcWarps, 0, st>>>(lists, bins, d_Lptr, d_Lind);
+  tc_block_rows<<<ctx->num_sms * 4, kTcThreads, 0, st>>>(lists + m, bins, d_Lptr, d_Lind);
+  tc_search_rows<<<ctx->num_sms * 2, kTcThreads, 0, st>>>(lists + 2 * (size_t)m, bins, d_Lptr,
+                                                          d_Lind);
+  int rc = check_launch(ctx, "apspie_tc", 4);
+  if (rc) return rc;
+  auto *h = (TcBins *)pinned(ctx, sizeof(TcBins));
+  if (!h) return APSPIE_ERR_OOM;
+  cudaMemcpyAsync(h, bins, sizeof(TcBins), cudaMemcpyDeviceToHost, st);
+  rc = check_cuda(ctx, cudaStreamSynchronize(st), "apspie_tc");
+  if (rc) return rc;
+  *h_count = (int64_t)h->count;
+  return APSPIE_OK;
+}
+
+}  // extern "C"

@@ -134,6 +134,29 @@ def weights_f32(g: HostGraph, seed: int = 7) -> np.ndarray:
     return w
 
 
+def gen_powerlaw(m: int = 1 << 18, n: int | None = None, alpha: float = 2.1, mean: float = 16.0,
+                 max_deg: int = 4096, seed: int = 1) -> HostGraph:
+    """Power-law-row matrix of the SpGEMM benchmark; values in w_f32,
+    the solved x_min in .name."""
+    n = m if n is None else n
+    xmin = C.c_double()
+    nnz = C.c_int64()
+    p, i, v = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    check(lib.apspie_gen_powerlaw_host(m, n, alpha, mean, max_deg, seed, C.byref(xmin),
+                                       C.byref(nnz), C.byref(p), C.byref(i), C.byref(v)),
+          what="gen_powerlaw")
+    vals = np.empty(nnz.value, dtype=np.float32)
+    if nnz.value:
+        C.memmove(vals.ctypes.data, v.value, 4 * nnz.value)
+    lib.apspie_host_free(v)
+    g = HostGraph(m, _take_int_array(p, m + 1), _take_int_array(i, nnz.value),
+                  name=f"powerlaw{m}x{n}(xmin={xmin.value:.4f})")
+    g.w_f32 = vals
+    g.ncols = n
+    g.xmin = xmin.value
+    return g
+
+
 def mt19937(seed: int, n: int) -> np.ndarray:
     out = np.empty(n, dtype=np.uint32)
     check(lib.apspie_mt19937_fill_host(seed, n, out.ctypes.data), what="mt19937")

@@ -5,7 +5,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-from ._native import BfsStats, SsspStats, check, lib
+from ._native import BfsStats, Csr, SsspStats, check, lib
 
 
 class Context:
@@ -202,3 +202,54 @@ def mxv_dense(ctx: Context, semiring: int, g, x, val=None, y=None):
 
 def spmspv_set_params(ctx: Context, sort_factor: float = 4.0) -> None:
     check(lib.apspie_spmspv_set_params(ctx.handle, float(sort_factor)), ctx.handle)
+
+
+def _csr(m, n, ptr, ind, val) -> Csr:
+    return Csr(int(m), int(n), int(ind.numel()) if ind is not None else 0,
+               C.c_void_p(ptr.data_ptr()), C.c_void_p(0 if ind is None else ind.data_ptr()),
+               C.c_void_p(0 if val is None else val.data_ptr()))
+
+
+def spgemm(ctx: Context, A, B):
+    """C = A * B (spgemm(d_matrix*...), src/spgemm.cuh:132).  A and B are
+    (m, n, ptr, ind, val) tuples of device tensors (val may be None = ones);
+    returns (ptr, ind, val) tensors of C (columns ascending per row)."""
+    import torch
+    a, b = _csr(*A), _csr(*B)
+    c = Csr()
+    check(lib.apspie_spgemm(ctx.handle, C.byref(a), C.byref(b), C.byref(c)), ctx.handle,
+          "apspie_spgemm")
+    try:
+        dev = A[2].device
+        ptr = torch.empty(c.m + 1, dtype=torch.int32, device=dev)
+        ind = torch.empty(max(c.nnz, 1), dtype=torch.int32, device=dev)
+        val = torch.empty(max(c.nnz, 1), dtype=torch.float32, device=dev)
+        check(lib.apspie_csr_copy_out(ctx.handle, C.byref(c), C.c_void_p(ptr.data_ptr()),
+                                      C.c_void_p(ind.data_ptr()), C.c_void_p(val.data_ptr())),
+              ctx.handle, "apspie_csr_copy_out")
+        ctx.sync()
+    finally:
+        lib.apspie_csr_free(ctx.handle, C.byref(c))
+    return ptr, ind[:c.nnz], val[:c.nnz]
+
+
+def tc_prepare(ctx: Context, g):
+    """Degree-ordered strict lower triangle of a symmetric graph:
+    returns (perm, Lptr, Lind) device tensors."""
+    import torch
+    dev = g.ptr.device
+    perm = torch.empty(g.m, dtype=torch.int32, device=dev)
+    lp = torch.empty(g.m + 1, dtype=torch.int32, device=dev)
+    li = torch.empty(max(1, g.nnz // 2 + 1), dtype=torch.int32, device=dev)
+    n = C.c_int64()
+    check(lib.apspie_tc_prepare(ctx.handle, int(g.nnz), int(g.m), _p(g.ptr), _p(g.ind), _p(perm),
+                                _p(lp), _p(li), C.byref(n)), ctx.handle, "apspie_tc_prepare")
+    return perm, lp, li[:n.value]
+
+
+def triangle_count(ctx: Context, m: int, lptr, lind) -> int:
+    """Masked hash SpGEMM (L*L).*L summed in int64 (test/tc/main.cu:243-261)."""
+    out = C.c_int64()
+    check(lib.apspie_tc(ctx.handle, int(m), int(lind.numel()), _p(lptr), _p(lind),
+                        C.byref(out)), ctx.handle, "apspie_tc")
+    return int(out.value)

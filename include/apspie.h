@@ -184,6 +184,51 @@ int apspie_mxv_dense(apspie_ctx ctx, int semiring, int m, int64_t nnz,
  * products * sort_factor > m, else the radix-sort path.  Default 4. */
 int apspie_spmspv_set_params(apspie_ctx ctx, double sort_factor);
 
+/* ------------------------------------------------------------- SpGEMM ---
+ * The reference's d_matrix (src/matrix.hpp:6-37) reduced to its CSR part:
+ * int32 row offsets (m + 1), int32 column indices and float values, all
+ * device pointers.  d_val may be NULL (all ones) for inputs. */
+typedef struct {
+  int m, n;
+  int64_t nnz;
+  int *d_ptr;
+  int *d_ind;
+  float *d_val;
+} apspie_csr;
+
+/* C = A * B (A->n == B->m).  Replaces the hash SpGEMM
+ * spgemm(d_matrix *C, d_matrix *A, d_matrix *B, partSize, partNum, ctx)
+ * (src/spgemm.cuh:132-342) and the column-by-column mXm
+ * (src/tc.cuh:315-375).  C's structure is the symbolic product (an entry for
+ * every (i, j) with some A(i,k) B(k,j), cancellations kept), columns
+ * ascending in each row; values are the double-accumulated sums rounded to
+ * float.  C's arrays are allocated by the library, as the reference's are;
+ * release them with apspie_csr_free.  Synchronises. */
+int apspie_spgemm(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B,
+                  apspie_csr *C);
+int apspie_csr_free(apspie_ctx ctx, apspie_csr *C);
+/* Stream-ordered device-to-device copy of a library-owned CSR into caller
+ * buffers (m + 1 offsets, nnz indices, nnz values; d_ind / d_val may be
+ * NULL). */
+int apspie_csr_copy_out(apspie_ctx ctx, const apspie_csr *C, int *d_ptr,
+                        int *d_ind, float *d_val);
+
+/* ----------------------------------------------------- triangle count ---
+ * L of a symmetric graph (no self-loops counted): vertices relabelled by
+ * ascending (degree, id) -- d_perm[v] = new id -- and L(new(u), :) = the new
+ * ids of u's neighbours below new(u), rows sorted.  test/tc/main.cu:40-55,
+ * 172-175 builds the strict triangles on the host.  d_Lptr holds m + 1
+ * entries, d_Lind at least nnz / 2; *h_lnnz = nnz(L).  Synchronises. */
+int apspie_tc_prepare(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr,
+                      const int *d_ind, int *d_perm, int *d_Lptr, int *d_Lind,
+                      int64_t *h_lnnz);
+/* Triangles = sum over (i, k) in L of |L(i,:) n L(k,:)|, as the masked
+ * product (L * L) .* L, counted in int64.  Replaces cuSPARSE U * L
+ * (src/tc.cuh:63-165) + ewiseMultTc (src/tc.cuh:169-199) + the float
+ * reduction of test/tc/main.cu:249.  Synchronises. */
+int apspie_tc(apspie_ctx ctx, int m, int64_t lnnz, const int *d_Lptr,
+              const int *d_Lind, int64_t *h_count);
+
 /* ------------------------------------------------- host graph builders ---
  * Synthetic inputs of the benchmark configurations (no reference
  * counterpart: the reference reads .mtx files, src/util.cuh:355-430).
@@ -209,6 +254,16 @@ int apspie_gen_weights_u32_host(int m, const int *h_ptr, const int *h_ind,
                                 uint32_t *h_w);
 int apspie_gen_weights_f32_host(int m, const int *h_ptr, const int *h_ind,
                                 uint64_t seed, float *h_w);
+/* m x n matrix whose row lengths follow a power law: k = floor(X), X a
+ * Pareto(alpha, x_min) truncated at max_deg + 1, with x_min solved by
+ * bisection so that E[k] = mean (written to *xmin_out); k uniform columns
+ * per row (duplicates dropped, so rows can be shorter), values uniform in
+ * [-1, 1) on the 2^-23 grid.  The SpGEMM benchmark input (2^18 x 2^18,
+ * alpha 2.1, mean 16, max 4096). */
+int apspie_gen_powerlaw_host(int m, int n, double alpha, double mean,
+                             int max_deg, uint64_t seed, double *xmin_out,
+                             int64_t *nnz_out, int **h_ptr, int **h_ind,
+                             float **h_val);
 /* MT19937 priorities: n outputs of genrand_int32() after init_genrand(seed)
  * (src/mt19937ar.cpp:57-150), the generator the reference uses for its hash
  * constants (src/spgemmKernel.cuh:173-177). */

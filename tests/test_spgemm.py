@@ -1,0 +1,121 @@
+"""Hash SpGEMM and triangle counting parity against the oracle (FP64
+Gustavson; int64 sorted-merge triangle count): SpGEMM structure exact,
+values within 1e-5 relative (plus a double-rounding floor relative to the
+sum of |products|); triangle counts exact."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+VAL_RTOL = 1e-5
+
+
+def _dev_csr(h):
+    import torch
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    ind = t(h.ind) if h.nnz else torch.zeros(1, dtype=torch.int32, device="cuda")
+    val = t(h.w_f32) if h.w_f32 is not None and h.nnz else None
+    return (h.m, getattr(h, "ncols", h.m), t(h.ptr), ind if h.nnz else ind[:0], val)
+
+
+def _check_product(ctx, A, B):
+    import apspie_b200 as ap
+    cp, ci, cv = ap.spgemm(ctx, _dev_csr(A), _dev_csr(B))
+    cp, ci, cv = cp.cpu().numpy(), ci.cpu().numpy(), cv.cpu().numpy()
+    n = getattr(B, "ncols", B.m)
+    rp, ri, rv = oracle.spgemm(A.m, n, A.ptr, A.ind, A.w_f32, B.ptr, B.ind, B.w_f32)
+    np.testing.assert_array_equal(cp, rp.astype(np.int32))
+    np.testing.assert_array_equal(ci, ri)
+    absA = None if A.w_f32 is None else np.abs(A.w_f32)
+    absB = None if B.w_f32 is None else np.abs(B.w_f32)
+    _, _, mag = oracle.spgemm(A.m, n, A.ptr, A.ind, absA, B.ptr, B.ind, absB)
+    err = np.abs(cv.astype(np.float64) - rv)
+    assert np.all(err <= VAL_RTOL * np.abs(rv) + 1e-12 * mag + 1e-30), err.max()
+    return cp[-1]
+
+
+def test_spgemm_fixture_and_small(ctx, golden):
+    import apspie_b200 as ap
+    h = ap.HostGraph(4, golden["mtx/test_spgemm/dir_ptr"], golden["mtx/test_spgemm/dir_ind"])
+    h.w_f32 = np.arange(1, h.nnz + 1, dtype=np.float32)
+    _check_product(ctx, h, h)
+    rng = np.random.default_rng(0)
+    for m in (1, 7, 300):
+        rows = rng.integers(0, m, 5 * m)
+        cols = rng.integers(0, m, 5 * m)
+        key = np.unique(rows * m + cols)
+        g = ap.from_edges(m, key // m, key % m)
+        g.w_f32 = rng.uniform(-1, 1, g.nnz).astype(np.float32)
+        _check_product(ctx, g, g)
+
+
+def test_spgemm_keeps_cancellation(ctx):
+    import apspie_b200 as ap
+    A = ap.HostGraph(1, np.array([0, 2], np.int32), np.array([0, 1], np.int32))
+    A.w_f32 = np.array([1.0, -1.0], np.float32)
+    A.ncols = 2
+    B = ap.HostGraph(2, np.array([0, 1, 2], np.int32), np.array([0, 0], np.int32))
+    B.w_f32 = np.array([1.0, 1.0], np.float32)
+    B.ncols = 1
+    import torch
+    cp, ci, cv = ap.spgemm(ctx, _dev_csr(A), _dev_csr(B))
+    assert cp.tolist() == [0, 1] and ci.tolist() == [0] and cv.tolist() == [0.0]
+
+
+def test_spgemm_all_bins_rectangular(ctx):
+    """Power-law rows reach the warp, block and dense-accumulator bins."""
+    import apspie_b200 as ap
+    A = ap.gen_powerlaw(1 << 12, 1 << 11, max_deg=1024, seed=2)
+    B = ap.gen_powerlaw(1 << 11, 1 << 12, max_deg=1024, seed=3)
+    prod = np.array([B.degrees()[A.ind[A.ptr[i]:A.ptr[i + 1]]].sum() for i in range(A.m)])
+    assert (prod <= 256).any() and ((prod > 256) & (prod <= 8192)).any() and (prod > 8192).any()
+    _check_product(ctx, A, B)
+
+
+def test_spgemm_powerlaw_full_config(ctx):
+    """2^18 x 2^18, row nnz power law (alpha 2.1, mean 16, max 4096): A * A."""
+    import apspie_b200 as ap
+    A = ap.gen_powerlaw(1 << 18, seed=1)
+    nnz_c = _check_product(ctx, A, A)
+    assert nnz_c > 6e7
+
+
+def _tc(ctx, h):
+    import apspie_b200 as ap
+    g = h.to_device(with_transpose=False)
+    perm, lp, li = ap.tc_prepare(ctx, g)
+    operm, olp, oli = oracle.tc_build_lower(h.m, h.ptr, h.ind)
+    np.testing.assert_array_equal(perm.cpu().numpy(), operm)
+    np.testing.assert_array_equal(lp.cpu().numpy(), olp)
+    np.testing.assert_array_equal(li.cpu().numpy(), oli)
+    got = ap.triangle_count(ctx, h.m, lp, li)
+    assert got == oracle.tc_lower(h.m, olp, oli)
+    return got
+
+
+def test_tc_known_answers(ctx):
+    import apspie_b200 as ap
+    k4 = ap.HostGraph(4, np.array([0, 3, 6, 9, 12], np.int32),
+                      np.array([1, 2, 3, 0, 2, 3, 0, 1, 3, 0, 1, 2], np.int32))
+    assert _tc(ctx, k4) == 4
+    assert _tc(ctx, ap.gen_grid(32, 32)) == 0
+
+
+def test_tc_fixtures(ctx, golden, fixture_names):
+    import apspie_b200 as ap
+    for name in fixture_names:
+        ptr, ind = golden[f"mtx/{name}/und_ptr"], golden[f"mtx/{name}/und_ind"]
+        src = np.repeat(np.arange(len(ptr) - 1), np.diff(ptr))
+        keep = src != ind   # self-loops carry no triangles
+        h = ap.from_edges(len(ptr) - 1, src[keep], ind[keep])
+        _tc(ctx, h)
+
+
+@pytest.mark.parametrize("scale", [12, 18])
+def test_tc_rmat(ctx, scale):
+    """R-MAT scale 18, edge factor 16, symmetrised: the TC configuration."""
+    import apspie_b200 as ap
+    count = _tc(ctx, ap.gen_rmat(scale, 16, seed=1))
+    assert count > 0
