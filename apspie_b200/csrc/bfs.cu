@@ -38,11 +38,18 @@ struct LevelTrace {
   int mode;  // 1 push, 2 pull
   int pad;
   unsigned long long nf, mf;
-  unsigned long long t_end;  // %globaltimer at the end of the level (ns)
+  unsigned long long t_end;      // %globaltimer at the end of the level (ns)
+  unsigned long long queued;     // vertices queued from an implicit frontier (== nf when it ran)
+  unsigned long long expanded;   // edges the push expansion walked (== mf)
 };
 
 struct BfsState {
   LevelCounters c[3];
+  // Queue counters of a frontier rebuilt from depth == L before a push level.
+  // They must not be the level's own counters: slower blocks may still be
+  // reading those to choose the direction while faster ones already append.
+  // Two sets, by level parity; block 0 clears the other one each level.
+  LevelCounters comp[2];
   unsigned bar[2];
   int err;
   int levels;
@@ -75,6 +82,8 @@ __global__ void bfs_init(int m, int src, int32_t *depth, const int *__restrict__
     if (threadIdx.x == 0) {
       st->c[1] = LevelCounters{0, 0, 0, 0, 0ull};
       st->c[2] = LevelCounters{0, 0, 0, 0, 0ull};
+      st->comp[0] = LevelCounters{0, 0, 0, 0, 0ull};
+      st->comp[1] = LevelCounters{0, 0, 0, 0, 0ull};
       st->bar[0] = st->bar[1] = 0;
       st->err = 0;
       st->levels = 0;
@@ -82,20 +91,28 @@ __global__ void bfs_init(int m, int src, int32_t *depth, const int *__restrict__
       st->reached = 0;
       st->edges = 0;
     }
+    for (int i = threadIdx.x; i < kTraceLevels; i += blockDim.x) {
+      st->trace[i].queued = 0;
+      st->trace[i].expanded = 0;
+    }
   }
 }
 
 __global__ void __launch_bounds__(kBfsThreads, 3)
 bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__restrict__ ind,
-               const int *__restrict__ tptr, const int *__restrict__ tind, int32_t *depth, int *qa, int *qb, int2 *ca, int2 *cb, BfsState *st,
-               int max_levels, int alpha, int beta, int mode) {
+               const int *__restrict__ tptr, const int *__restrict__ tind, int32_t *depth,
+               int *qa, int *qb, int2 *ca, int2 *cb, BfsState *st, int max_levels, int alpha,
+               int beta, int mode) {
   const int lane = lane_id();
+  const int warp = warp_in_block();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
-  __shared__ unsigned s_q, s_chunks, s_nbig;
+  __shared__ unsigned s_q, s_chunks, s_nbig, s_nimpl;
   __shared__ unsigned long long s_edges;
   __shared__ unsigned s_found[kBfsThreads / 32];
-  const int warp = warp_in_block();
+  __shared__ int s_rank[kBfsThreads / 32][32];
+  __shared__ unsigned s_bcnt;
+  __shared__ unsigned long long s_bedg;
 
   if (blockIdx.x == 0 && threadIdx.x == 0) st->t_start = globaltimer();
   bool pull = false;
@@ -110,17 +127,19 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
       s_q = __ldcg(&cur->q);
       s_chunks = __ldcg(&cur->chunks);
       s_nbig = __ldcg(&cur->nbig);
+      s_nimpl = __ldcg(&cur->nimpl);
       s_edges = __ldcg(&cur->edges);
+      s_bcnt = 0;
+      s_bedg = 0;
       if (blockIdx.x == 0) {
-        clr->q = 0;
-        clr->chunks = 0;
-        clr->nbig = 0;
-        clr->edges = 0;
+        *clr = LevelCounters{0, 0, 0, 0, 0ull};
+        st->comp[(L + 1) & 1] = LevelCounters{0, 0, 0, 0, 0ull};
       }
     }
     __syncthreads();
-    const unsigned nq = s_q, nch = s_chunks;
-    const unsigned long long nf = (unsigned long long)nq + s_nbig;
+    unsigned nq = s_q, nch = s_chunks;
+    const unsigned nimpl = s_nimpl;
+    const unsigned long long nf = (unsigned long long)nq + s_nbig + nimpl;
     const unsigned long long mf = s_edges;
     if (nf == 0) break;
     reached += nf;
@@ -146,65 +165,100 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
     const int next = L + 1;
 
     if (!pull) {
+      if (nimpl) {
+        // the frontier came from a pull level and exists only as depth == L:
+        // queue it (and chunk its hubs) before expanding
+        for (int base = gwarp * 32; base < m; base += nwarps * 32) {
+          int v = base + lane;
+          bool f[1] = {v < m && __ldcg(depth + v) == L};
+          int u[1] = {v};
+          unsigned fm = __ballot_sync(kFull, f[0]);
+          if (fm) {
+            discover_n<1, false>(f, u, ptr, qin, cin, &st->comp[L & 1]);
+            if (lane == 0 && L < kTraceLevels) atomicAdd(&st->trace[L].queued, (unsigned long long)__popc(fm));
+          }
+        }
+        if (!grid_barrier(st->bar, &st->err)) return;
+        if (threadIdx.x == 0) {
+          s_q = __ldcg(&st->comp[L & 1].q);
+          s_chunks = __ldcg(&st->comp[L & 1].chunks);
+        }
+        __syncthreads();
+        nq = s_q;
+        nch = s_chunks;
+      }
       BfsVisit vis{next, depth};
       expand_push(ptr, ind, qin, nq, cin, nch, qout, cout, nxt, gwarp, nwarps,
-                  [](int) { return 0u; }, vis);
+                  [](int) { return 0u; }, vis,
+                  L < kTraceLevels ? &st->trace[L].expanded : nullptr);
     } else {
       ++pull_levels;
       // ---- pull: unvisited vertices look for a parent at depth L ----
-      // Each lane first probes kProbe in-neighbours of its own vertex (all
-      // index loads, then all depth loads).  The remaining in-neighbours of
-      // the still-unresolved vertices of the warp are then laid out flat
-      // (warp scan) and dealt 32 x kUnroll at a time, like a push gather; a
-      // hit sets the owner's bit in a per-warp mask, slots of resolved owners
-      // are skipped, and the warp stops once every owner is resolved.
+      // The unresolved vertices of a warp share its lanes round-robin: with k
+      // of them unresolved, vertex of rank j gets lanes j, j+k, j+2k, ... and
+      // each of those lanes probes kProbe in-neighbours (all index loads, then
+      // all depth loads), so every round keeps 32 x kProbe probes in flight and
+      // a vertex leaves as soon as one probe hits.  Discoveries are counted,
+      // not queued: the next frontier is depth == L + 1.
+      unsigned cnt = 0;
+      unsigned long long edg = 0;
       for (int base = gwarp * 32; base < m; base += nwarps * 32) {
         int v = base + lane;
         int s = 0, e = 0;
-        bool found = false;
         if (v < m && __ldcg(depth + v) == -1) {
           s = __ldg(tptr + v);
           e = __ldg(tptr + v + 1);
         }
-        if (s < e) {
-          int nb[kProbe];
-#pragma unroll
-          for (int i = 0; i < kProbe; ++i) nb[i] = s + i < e ? __ldg(tind + s + i) : -1;
-#pragma unroll
-          for (int i = 0; i < kProbe; ++i) found |= nb[i] >= 0 && __ldcg(depth + nb[i]) == L;
-          s = min(s + kProbe, e);
-        }
-        int d = found ? 0 : e - s;
-        int incl = warp_incl_scan(d);
-        int excl = incl - d;
-        int total = __shfl_sync(kFull, incl, 31);
-        if (total) {
-          const unsigned want = __ballot_sync(kFull, d > 0);
+        bool found = false;
+        unsigned U = __ballot_sync(kFull, s < e);
+        if (U) {
           if (lane == 0) s_found[warp] = 0u;
           __syncwarp();
-          for (int e0 = 0; e0 < total; e0 += 32 * kUnroll) {
-            int nb[kUnroll], own[kUnroll];
-            const unsigned done = *(volatile unsigned *)&s_found[warp];
-#pragma unroll
-            for (int r = 0; r < kUnroll; ++r) {
-              int ee = e0 + r * 32 + lane;
-              int owner = warp_owner(excl, ee);
-              int so = __shfl_sync(kFull, s, owner);
-              int eo = __shfl_sync(kFull, excl, owner);
-              own[r] = owner;
-              nb[r] = (ee < total && !((done >> owner) & 1u)) ? __ldg(tind + so + (ee - eo)) : -1;
-            }
-#pragma unroll
-            for (int r = 0; r < kUnroll; ++r)
-              if (nb[r] >= 0 && __ldcg(depth + nb[r]) == L) atomicOr(&s_found[warp], 1u << own[r]);
-            __syncwarp();
-            if ((*(volatile unsigned *)&s_found[warp] & want) == want) break;
-          }
-          found |= (*(volatile unsigned *)&s_found[warp] >> lane) & 1u;
-          __syncwarp();
         }
-        if (found) depth[v] = next;
-        discover(found, v, ptr, qout, cout, nxt);
+        while (U) {
+          const int k = __popc(U);
+          const bool mine = (U >> lane) & 1u;
+          const int myrank = __popc(U & ((1u << lane) - 1u));
+          if (mine) s_rank[warp][myrank] = lane;
+          __syncwarp();
+          const int per = 32 / k, extra = 32 % k;
+          const int j = lane % k, slot = lane / k;
+          const int nl = per + (j < extra ? 1 : 0);
+          const int owner = s_rank[warp][j];
+          const int so = __shfl_sync(kFull, s, owner);
+          const int eo = __shfl_sync(kFull, e, owner);
+          int nb[kProbe];
+#pragma unroll
+          for (int i = 0; i < kProbe; ++i) {
+            int idx = so + slot + i * nl;
+            nb[i] = idx < eo ? __ldg(tind + idx) : -1;
+          }
+          bool hit = false;
+#pragma unroll
+          for (int i = 0; i < kProbe; ++i) hit |= nb[i] >= 0 && __ldcg(depth + nb[i]) == L;
+          if (hit) atomicOr(&s_found[warp], 1u << owner);
+          __syncwarp();
+          const unsigned fm = *(volatile unsigned *)&s_found[warp];
+          if (mine) s += (per + (myrank < extra ? 1 : 0)) * kProbe;
+          found = (fm >> lane) & 1u;
+          U = __ballot_sync(kFull, mine && !found && s < e);
+        }
+        if (found) {
+          depth[v] = next;
+          ++cnt;
+          edg += (unsigned long long)(__ldg(ptr + v + 1) - __ldg(ptr + v));
+        }
+      }
+      cnt = warp_sum(cnt);
+      edg = warp_sum(edg);
+      if (lane == 0 && cnt) {
+        atomicAdd(&s_bcnt, cnt);
+        atomicAdd(&s_bedg, edg);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0 && s_bcnt) {
+        atomicAdd(&nxt->nimpl, s_bcnt);
+        atomicAdd(&nxt->edges, s_bedg);
       }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && L < kTraceLevels) {
@@ -315,7 +369,8 @@ int apspie_bfs_set_params(apspie_ctx ctx, int alpha, int beta, int mode) {
 
 extern "C" int apspie_bfs_get_trace(apspie_ctx ctx, int max_levels, int *n_out,
                                     int32_t *h_mode, int64_t *h_frontier,
-                                    int64_t *h_frontier_edges, int64_t *h_ns) {
+                                    int64_t *h_frontier_edges, int64_t *h_ns,
+                                    int64_t *h_queued, int64_t *h_expanded) {
   APSPIE_CHECK_CTX(ctx);
   if (!ctx->bfs_state || max_levels < 0 || !n_out)
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_bfs_get_trace: no BFS has run");
@@ -332,8 +387,11 @@ extern "C" int apspie_bfs_get_trace(apspie_ctx ctx, int max_levels, int *n_out,
     if (h_frontier) h_frontier[i] = (int64_t)h->trace[i].nf;
     if (h_frontier_edges) h_frontier_edges[i] = (int64_t)h->trace[i].mf;
     if (h_ns) h_ns[i] = (int64_t)(h->trace[i].t_end - prev);
+    if (h_queued) h_queued[i] = (int64_t)h->trace[i].queued;
+    if (h_expanded) h_expanded[i] = (int64_t)h->trace[i].expanded;
     prev = h->trace[i].t_end;
   }
   *n_out = n;
   return APSPIE_OK;
 }
+

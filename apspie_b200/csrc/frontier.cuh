@@ -31,8 +31,8 @@ struct LevelCounters {
   unsigned q;       // vertices in the queue (degree <= kBigDeg)
   unsigned chunks;  // entries in the chunk list
   unsigned nbig;    // vertices in the chunk list
-  unsigned pad;
-  unsigned long long edges;  // sum of out-degrees of those vertices
+  unsigned nimpl;   // vertices of an implicit frontier (BFS pull: depth == level), not queued
+  unsigned long long edges;  // sum of out-degrees of the frontier
 };
 
 // Capacity of a chunk list for a graph with nnz edges: every big vertex has
@@ -44,7 +44,7 @@ inline size_t chunk_capacity(long long nnz) {
 // Called by all 32 lanes with N candidates per lane; candidate r of a lane
 // joins the next frontier when found[r].  One queue append, one chunk
 // reservation and one edge-count update per warp for all N x 32 candidates.
-template <int N>
+template <int N, bool kCountEdges = true>
 __device__ __forceinline__ void discover_n(const bool (&found)[N], const int (&u)[N],
                                            const int *__restrict__ ptr, int *qout, int2 *cout,
                                            LevelCounters *nxt) {
@@ -101,8 +101,10 @@ __device__ __forceinline__ void discover_n(const bool (&found)[N], const int (&u
       cbase += (unsigned)nch;
     }
   }
-  edges = warp_sum(edges);
-  if (lane == 0 && edges) atomicAdd(&nxt->edges, edges);
+  if (kCountEdges) {
+    edges = warp_sum(edges);
+    if (lane == 0 && edges) atomicAdd(&nxt->edges, edges);
+  }
 }
 
 __device__ __forceinline__ void discover(bool found, int u, const int *__restrict__ ptr,
@@ -138,8 +140,10 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
                                             const int *__restrict__ ind, const int *qin,
                                             unsigned nq, const int2 *cin, unsigned nch,
                                             int *qout, int2 *cout, LevelCounters *nxt,
-                                            int gwarp, int nwarps, Load load, Visit &visit) {
+                                            int gwarp, int nwarps, Load load, Visit &visit,
+                                            unsigned long long *walked = nullptr) {
   const int lane = lane_id();
+  unsigned long long nwalk = 0;
   for (unsigned base = (unsigned)gwarp * 32u; base < nq; base += (unsigned)nwarps * 32u) {
     unsigned idx = base + lane;
     int v = idx < nq ? __ldcg(qin + idx) : -1;
@@ -153,6 +157,7 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
     int incl = warp_incl_scan(d);
     int excl = incl - d;
     int total = __shfl_sync(kFull, incl, 31);
+    nwalk += (unsigned long long)total;
     for (int e0 = 0; e0 < total; e0 += 32 * kUnroll) {
       int kk[kUnroll], uu[kUnroll];
       unsigned pp[kUnroll], aux[kUnroll];
@@ -181,6 +186,7 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
     int2 ch = __ldcg(cin + c);
     int s = __ldg(ptr + ch.x) + ch.y * kChunk;
     int e = min(s + kChunk, __ldg(ptr + ch.x + 1));
+    nwalk += (unsigned long long)(e - s);
     unsigned pay = load(ch.x);
     for (int k0 = s; k0 < e; k0 += 32 * kUnroll) {
       int uu[kUnroll];
@@ -201,6 +207,7 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
       discover_n<kUnroll>(f, uu, ptr, qout, cout, nxt);
     }
   }
+  if (walked && lane == 0 && nwalk) atomicAdd(walked, nwalk);
 }
 
 }  // namespace apspie

@@ -92,13 +92,17 @@ def bfs_trace(ctx: Context, max_levels: int = 64) -> list[dict]:
     nf = np.zeros(max_levels, np.int64)
     mf = np.zeros(max_levels, np.int64)
     ns = np.zeros(max_levels, np.int64)
+    qd = np.zeros(max_levels, np.int64)
+    ex = np.zeros(max_levels, np.int64)
     cnt = C.c_int()
     check(lib.apspie_bfs_get_trace(ctx.handle, max_levels, C.byref(cnt), mode.ctypes.data,
-                                   nf.ctypes.data, mf.ctypes.data, ns.ctypes.data), ctx.handle,
+                                   nf.ctypes.data, mf.ctypes.data, ns.ctypes.data,
+                                   qd.ctypes.data, ex.ctypes.data), ctx.handle,
           "apspie_bfs_get_trace")
     n = cnt.value
     return [{"level": i, "dir": "pull" if mode[i] == 2 else "push", "frontier": int(nf[i]),
-             "frontier_edges": int(mf[i]), "us": ns[i] / 1e3} for i in range(n)]
+             "frontier_edges": int(mf[i]), "us": ns[i] / 1e3, "queued": int(qd[i]),
+             "expanded": int(ex[i])} for i in range(n)]
 
 
 def bfs_stats(ctx: Context) -> dict:
@@ -219,6 +223,7 @@ def spgemm(ctx: Context, A, B):
     c = Csr()
     check(lib.apspie_spgemm(ctx.handle, C.byref(a), C.byref(b), C.byref(c)), ctx.handle,
           "apspie_spgemm")
+    nnz = int(c.nnz)
     try:
         dev = A[2].device
         ptr = torch.empty(c.m + 1, dtype=torch.int32, device=dev)
@@ -230,7 +235,7 @@ def spgemm(ctx: Context, A, B):
         ctx.sync()
     finally:
         lib.apspie_csr_free(ctx.handle, C.byref(c))
-    return ptr, ind[:c.nnz], val[:c.nnz]
+    return ptr, ind[:nnz], val[:nnz]
 
 
 def tc_prepare(ctx: Context, g):

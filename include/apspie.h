@@ -85,11 +85,14 @@ int apspie_bfs_get_stats(apspie_ctx ctx, apspie_bfs_stats *out);
 
 /* Per-level trace of the last apspie_bfs (synchronises): for each level
  * i < max_levels (at most 64) the direction (1 push, 2 pull), frontier size,
- * frontier out-edges and device time in ns; *n_out = levels written.  The
- * array outputs may be NULL. */
+ * frontier out-edges, device time in ns, and two self-checks: vertices
+ * queued from an implicit (pull-produced) frontier before a push level, and
+ * edges the push expansion walked (== frontier out-edges).  *n_out = levels
+ * written.  The array outputs may be NULL. */
 int apspie_bfs_get_trace(apspie_ctx ctx, int max_levels, int *n_out,
                          int32_t *h_mode, int64_t *h_frontier,
-                         int64_t *h_frontier_edges, int64_t *h_ns);
+                         int64_t *h_frontier_edges, int64_t *h_ns,
+                         int64_t *h_queued, int64_t *h_expanded);
 
 /* Direction-switch thresholds (Beamer's alpha, beta; defaults 14 and 24) and
  * mode: 0 = switch automatically, 1 = push only, 2 = pull only. */

@@ -1,0 +1,193 @@
+// ref_api_main.cpp -- a test driver written against the reference's API.
+//
+// Mirrors the reference's test/<algo>/main.cu drivers: read a Matrix Market
+// file, build the CSR with buildMatrix, run the CPU oracle, run the GPU
+// routine through the reference's signatures (include/apspie_ref.hpp), then
+// verify() / unverify().  Exit status 0 means CORRECT.
+//
+//   ref_api_main <bfs|spmspvbfs|sssp|mis|mxv|spgemm|tc> file.mtx [-source N] [-undirected]
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "apspie_ref.hpp"
+#include "oracle.h"
+
+namespace {
+
+struct HostCsr {
+  int m = 0;
+  int64_t nnz = 0;
+  std::vector<int> ptr, ind;
+  std::vector<float> val;
+};
+
+HostCsr read(const char *path, bool undirected) {
+  HostCsr g;
+  int *p = nullptr, *i = nullptr, weighted = 0;
+  float *v = nullptr;
+  apspie::check(apspie_read_mtx_host(path, undirected, &g.m, &g.nnz, &p, &i, &v, &weighted),
+                nullptr, "read_mtx");
+  g.ptr.assign(p, p + g.m + 1);
+  g.ind.assign(i, i + g.nnz);
+  g.val.assign(v, v + g.nnz);
+  apspie_host_free(p);
+  apspie_host_free(i);
+  apspie_host_free(v);
+  if (!weighted)
+    for (int64_t k = 0; k < g.nnz; ++k) g.val[k] = 1.0f + (float)((k * 37) % 11);
+  return g;
+}
+
+// COO (row, col, val) of a CSR, as the reference drivers hold before buildMatrix
+void to_coo(const HostCsr &g, std::vector<int> &r, std::vector<int> &c, std::vector<float> &v) {
+  for (int u = 0; u < g.m; ++u)
+    for (int k = g.ptr[u]; k < g.ptr[u + 1]; ++k) {
+      r.push_back(u);
+      c.push_back(g.ind[k]);
+      v.push_back(g.val[k]);
+    }
+}
+
+template <typename T>
+std::vector<T> download(const T *d, size_t n) {
+  std::vector<T> h(n);
+  cudaMemcpy(h.data(), d, sizeof(T) * n, cudaMemcpyDeviceToHost);
+  return h;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  if (argc < 3) {
+    printf("Usage: %s algo file.mtx [-source N] [-undirected]\n", argv[0]);
+    return 2;
+  }
+  std::string algo = argv[1];
+  int source = 0;
+  bool undirected = false;
+  for (int a = 3; a < argc; ++a) {
+    if (!strcmp(argv[a], "-source") && a + 1 < argc) source = atoi(argv[++a]);
+    else if (!strcmp(argv[a], "-undirected")) undirected = true;
+  }
+  HostCsr g = read(argv[2], undirected);
+  const int m = g.m, edge = (int)g.nnz;
+  printf("Testing %s on %s from source %d: %d nodes, %d edges\n", algo.c_str(), argv[2], source, m,
+         edge);
+  mgpu::ContextPtr context = mgpu::CreateCudaDevice(0);
+  context->SetUndirected(undirected);
+
+  std::vector<int> rows, cols;
+  std::vector<float> vals;
+  to_coo(g, rows, cols, vals);
+  d_matrix A;
+  matrix_new(&A, m, m);
+  buildMatrix<float>(&A, edge, rows.data(), cols.data(), vals.data());
+
+  int errors = 0;
+  try {
+    if (algo == "bfs" || algo == "spmspvbfs") {
+      int *d_bfs = nullptr;
+      cudaMalloc(&d_bfs, sizeof(int) * m);
+      std::vector<int> cpu(m);
+      int depth = orc_bfs(m, g.ptr.data(), g.ind.data(), source, 1 << 30, cpu.data());
+      if (algo == "bfs")
+        bfs<int>(source, edge, m, A.h_cscColPtr, A.d_cscColPtr, A.d_cscRowInd, d_bfs, depth,
+                 *context);
+      else
+        spmspvBfs(source, edge, m, A.h_cscColPtr, A.d_cscColPtr, A.d_cscRowInd, d_bfs, depth,
+                  *context);
+      errors = verify(m, download(d_bfs, m).data(), cpu.data());
+      cudaFree(d_bfs);
+    } else if (algo == "sssp") {
+      float *d_dist = nullptr;
+      cudaMalloc(&d_dist, sizeof(float) * m);
+      std::vector<float> cpu(m);
+      orc_sssp_f32(m, g.ptr.data(), g.ind.data(), g.val.data(), source, cpu.data());
+      sssp<float>(source, edge, m, A.d_cscVal, A.d_cscColPtr, A.d_cscRowInd, d_dist, 1000,
+                  *context);
+      errors = verify(m, download(d_dist, m).data(), cpu.data());
+      cudaFree(d_dist);
+    } else if (algo == "mis") {
+      std::vector<uint32_t> prio(m);
+      apspie_mt19937_fill_host(5489u, m, prio.data());
+      uint32_t *d_prio = nullptr;
+      int *d_mis = nullptr, *d_flags = nullptr;
+      cudaMalloc(&d_prio, sizeof(uint32_t) * m);
+      cudaMalloc(&d_mis, sizeof(int) * m);
+      cudaMalloc(&d_flags, sizeof(int) * m);
+      cudaMemcpy(d_prio, prio.data(), sizeof(uint32_t) * m, cudaMemcpyHostToDevice);
+      spmspvMis<uint32_t>(edge, m, A.h_cscColPtr, A.d_cscColPtr, A.d_cscRowInd, d_prio, d_mis,
+                          0.1f, *context);
+      // the reference's check: neighbour flags + membership == 1
+      spmspvCsr<int>(d_mis, edge, m, A.d_cscColPtr, A.d_cscRowInd, d_flags, *context);
+      std::vector<int> h_mis = download(d_mis, m), h_flags = download(d_flags, m);
+      errors = unverify(m, h_flags.data(), h_mis.data());
+      std::vector<int> cpu(m);
+      orc_mis(m, g.ptr.data(), g.ind.data(), prio.data(), cpu.data());
+      errors += verify(m, h_mis.data(), cpu.data());
+      cudaFree(d_prio);
+      cudaFree(d_mis);
+      cudaFree(d_flags);
+    } else if (algo == "mxv") {
+      // dense mXv with a one-hot frontier: y = A^T e_source as in one BFS level
+      std::vector<float> x(m, 0.0f);
+      x[source] = 1.0f;
+      float *d_x = nullptr, *d_y = nullptr;
+      cudaMalloc(&d_x, sizeof(float) * m);
+      cudaMalloc(&d_y, sizeof(float) * m);
+      cudaMemcpy(d_x, x.data(), sizeof(float) * m, cudaMemcpyHostToDevice);
+      d_scratch *d;
+      allocScratch(&d, edge, m);
+      int total = mXv<float>(d_x, edge, m, A.d_cscVal, A.d_cscColPtr, A.d_cscRowInd, d_y, d,
+                             *context);
+      std::vector<float> expect(m, 0.0f);
+      for (int k = g.ptr[source]; k < g.ptr[source + 1]; ++k) expect[g.ind[k]] += g.val[k];
+      errors = verify(m, download(d_y, m).data(), expect.data());
+      errors += total != g.ptr[source + 1] - g.ptr[source];
+      delete d;
+      cudaFree(d_x);
+      cudaFree(d_y);
+    } else if (algo == "spgemm") {
+      d_matrix C;
+      spgemm(&C, &A, &A, 0, 0, *context);
+      std::vector<int64_t> cp(m + 1);
+      int64_t nnz = orc_spgemm_symbolic(m, m, g.ptr.data(), g.ind.data(), g.ptr.data(),
+                                        g.ind.data(), cp.data());
+      std::vector<int> ci(nnz > 0 ? nnz : 1);
+      std::vector<double> cv(nnz > 0 ? nnz : 1);
+      orc_spgemm_numeric(m, m, g.ptr.data(), g.ind.data(), g.val.data(), g.ptr.data(),
+                         g.ind.data(), g.val.data(), cp.data(), ci.data(), cv.data());
+      std::vector<int> gptr = download(C.d_cscColPtr, m + 1);
+      std::vector<int> gind = download(C.d_cscRowInd, (size_t)C.nnz);
+      std::vector<float> gval = download(C.d_cscVal, (size_t)C.nnz);
+      errors = (C.nnz != nnz);
+      std::vector<int> cp32(cp.begin(), cp.end());
+      errors += verify(m + 1, gptr.data(), cp32.data());
+      if (!errors) {
+        errors += verify((int)nnz, gind.data(), ci.data());
+        std::vector<float> cvf(cv.begin(), cv.end());
+        errors += verify((int)nnz, gval.data(), cvf.data());
+      }
+      matrix_delete(&C);
+    } else if (algo == "tc") {
+      std::vector<int> perm(m), lp(m + 1), li(g.nnz / 2 + 1);
+      orc_tc_build_lower(m, g.ptr.data(), g.ind.data(), perm.data(), lp.data(), li.data());
+      long long cpu = orc_tc_lower(m, lp.data(), li.data());
+      long long gpu = triangleCount(edge, m, A.d_cscColPtr, A.d_cscRowInd, *context);
+      printf("Number of triangles: %lld (CPU %lld)\n", gpu, cpu);
+      errors = gpu != cpu;
+      printf(errors ? "INCORRECT\n" : "CORRECT\n");
+    } else {
+      printf("unknown algo %s\n", algo.c_str());
+      return 2;
+    }
+  } catch (const apspie::Error &e) {
+    printf("ERROR: %s\n", e.what());
+    return 3;
+  }
+  matrix_delete(&A);
+  return errors ? 1 : 0;
+}

@@ -114,3 +114,26 @@ def test_bfs_rmat22_full_size(ctx):
     st = ap.bfs_stats(ctx)
     assert st["levels"] == depth and st["pull_levels"] > 0
     assert st["edges_traversed"] == int(h.degrees()[ref >= 0].sum())
+
+
+def test_bfs_repeated_runs_with_direction_switches(ctx):
+    """Repeated traversals that switch push -> pull -> push are all exact.
+    (A frontier rebuilt for a push level once shared its counters with the
+    level's direction decision; slower blocks then chose a different
+    direction in a few percent of the runs.)"""
+    import apspie_b200 as ap
+    h = ap.gen_rmat(16, 16, seed=16)
+    g = h.to_device()
+    for s in (2300, 30945):
+        ref, _ = oracle.bfs(h.m, h.ptr, h.ind, s)
+        dirs = None
+        for _ in range(40):
+            np.testing.assert_array_equal(ap.bfs(ctx, g, s).cpu().numpy(), ref)
+            tr = ap.bfs_trace(ctx)
+            dirs = [t["dir"] for t in tr]
+            for t in tr:
+                if t["dir"] == "push":
+                    assert t["expanded"] == t["frontier_edges"]
+                    if t["queued"]:
+                        assert t["queued"] == t["frontier"]
+        assert "pull" in dirs and dirs[-1] == "push"
