@@ -52,6 +52,7 @@ PROTOS: dict[str, tuple] = {
     "apspie_last_error": (C.c_char_p, [vp]),
     "apspie_status_string": (C.c_char_p, [c_int]),
     "apspie_bfs": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, vp, c_int]),
+    "apspie_bfs_noalloc": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, vp, c_int]),
     "apspie_bfs_get_stats": (c_int, [vp, C.POINTER(BfsStats)]),
     "apspie_bfs_get_trace": (c_int, [vp, c_int, P_int, vp, vp, vp, vp, vp, vp]),
     "apspie_bfs_set_params": (c_int, [vp, c_int, c_int, c_int]),

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "context.h"
@@ -395,3 +396,107 @@ extern "C" int apspie_bfs_get_trace(apspie_ctx ctx, int max_levels, int *n_out,
   return APSPIE_OK;
 }
 
+// ---------------------------------------------------------------------------
+// BFS that allocates nothing.
+//
+// Some callers cannot call cudaMalloc: code running while a stream is being
+// captured into a CUDA graph, real-time or embedded hosts whose device memory
+// is reserved up front by a fixed budget, and plugins loaded into a process
+// whose allocator they do not own.  apspie_bfs_noalloc serves them with the
+// same kernels as apspie_bfs, but its scratch (the level counters, the two
+// frontier queues and the two chunk lists) lives in the fixed-size device
+// array below instead of a context workspace.  The array is sized for graphs
+// of at most kNoAllocMaxVertices vertices and kNoAllocMaxEdges edges (about
+// 14 MiB); every GPU that loads this library holds it until the process
+// exits.
+namespace apspie {
+namespace {
+
+constexpr int kNoAllocMaxVertices = 1 << 20;
+constexpr long long kNoAllocMaxEdges = 1ll << 24;
+constexpr size_t kNoAllocChunkCap = (size_t)(kNoAllocMaxEdges / kChunk + kNoAllocMaxEdges / kBigDeg + 2);
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t kNaOffQa = align256(sizeof(BfsState));
+constexpr size_t kNaOffQb = kNaOffQa + align256(sizeof(int) * (size_t)kNoAllocMaxVertices);
+constexpr size_t kNaOffCa = kNaOffQb + align256(sizeof(int) * (size_t)kNoAllocMaxVertices);
+constexpr size_t kNaOffCb = kNaOffCa + align256(sizeof(int2) * kNoAllocChunkCap);
+constexpr size_t kNaBytes = kNaOffCb + align256(sizeof(int2) * kNoAllocChunkCap);
+
+static __device__ __align__(256) unsigned char g_bfs_noalloc_scratch[kNaBytes];
+
+// Device address of the scratch array, looked up once per device.  In host
+// code g_bfs_noalloc_scratch names a host-side stand-in, never the device
+// memory, so it must not be passed to a kernel.
+constexpr int kNaMaxDevices = 64;
+std::mutex g_na_mutex;
+unsigned char *g_na_ptr[kNaMaxDevices] = {};
+int g_na_grid[kNaMaxDevices] = {};
+
+int noalloc_setup(int dev, unsigned char **ptr, int *grid) {
+  if (dev < 0 || dev >= kNaMaxDevices) return APSPIE_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_na_mutex);
+  if (!g_na_ptr[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_bfs_noalloc_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return APSPIE_ERR_CUDA;
+    }
+    int occ = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bfs_persistent, kBfsThreads, 0) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        occ < 1) {
+      cudaGetLastError();
+      return APSPIE_ERR_CUDA;
+    }
+    g_na_grid[dev] = occ * sms;
+    g_na_ptr[dev] = (unsigned char *)p;
+  }
+  *ptr = g_na_ptr[dev];
+  *grid = g_na_grid[dev];
+  return APSPIE_OK;
+}
+
+}  // namespace
+}  // namespace apspie
+
+extern "C" int apspie_bfs_noalloc(void *stream, int src, int64_t nnz, int m, const int *d_ptr,
+                                  const int *d_ind, const int *d_tptr, const int *d_tind,
+                                  int32_t *d_depth, int max_levels) {
+  using namespace apspie;
+  if (m <= 0 || src < 0 || src >= m || nnz < 0) return APSPIE_ERR_INVALID;
+  if (m > kNoAllocMaxVertices || nnz > kNoAllocMaxEdges) return APSPIE_ERR_TOO_LARGE;
+  if (!d_ptr || !d_depth || (nnz > 0 && !d_ind) || (d_tptr && nnz > 0 && !d_tind))
+    return APSPIE_ERR_INVALID;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return APSPIE_ERR_CUDA;
+  }
+  unsigned char *base = nullptr;
+  int grid = 0;
+  int rc = noalloc_setup(dev, &base, &grid);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  auto *state = (BfsState *)base;
+  auto *qa = (int *)(base + kNaOffQa);
+  auto *qb = (int *)(base + kNaOffQb);
+  auto *ca = (int2 *)(base + kNaOffCa);
+  auto *cb = (int2 *)(base + kNaOffCb);
+  // bfs_init clears every counter and status word the kernel reads, so the
+  // contents left by the previous call do not matter
+  int init_grid = std::min((m + 255) / 256, grid * 2);
+  bfs_init<<<init_grid, 256, 0, st>>>(m, src, d_depth, d_ptr, qa, ca, state);
+  if (cudaGetLastError() != cudaSuccess) return APSPIE_ERR_CUDA;
+  long long nnz_ll = (long long)nnz;
+  int alpha = 14, beta = 24, mode = d_tptr ? 0 : 1;
+  void *args[] = {&m,  &nnz_ll, (void *)&d_ptr, (void *)&d_ind, (void *)&d_tptr, (void *)&d_tind,
+                  &d_depth, &qa, &qb, &ca, &cb, &state, &max_levels, &alpha, &beta, &mode};
+  if (cudaLaunchCooperativeKernel((const void *)bfs_persistent, dim3(grid), dim3(kBfsThreads), args,
+                                  0, st) != cudaSuccess) {
+    cudaGetLastError();
+    return APSPIE_ERR_CUDA;
+  }
+  return APSPIE_OK;
+}

@@ -150,6 +150,7 @@ const char *apspie_status_string(int status) {
     case APSPIE_ERR_OVERFLOW: return "result exceeds int32 layout";
     case APSPIE_ERR_UNSUPPORTED: return "unsupported";
     case APSPIE_ERR_BUSY: return "busy";
+    case APSPIE_ERR_TOO_LARGE: return "input exceeds the fixed scratch size";
     default: return "unknown status";
   }
 }

@@ -35,7 +35,8 @@ typedef enum {
   APSPIE_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
   APSPIE_ERR_OVERFLOW = 5,    /* a result does not fit the int32 layout */
   APSPIE_ERR_UNSUPPORTED = 6, /* feature not available on this device */
-  APSPIE_ERR_BUSY = 7         /* serving queue full / admission refused */
+  APSPIE_ERR_BUSY = 7,        /* serving queue full / admission refused */
+  APSPIE_ERR_TOO_LARGE = 8    /* input exceeds a fixed buffer's stated maximum */
 } apspie_status;
 
 typedef struct apspie_context *apspie_ctx;
@@ -93,6 +94,25 @@ int apspie_bfs_get_trace(apspie_ctx ctx, int max_levels, int *n_out,
                          int32_t *h_mode, int64_t *h_frontier,
                          int64_t *h_frontier_edges, int64_t *h_ns,
                          int64_t *h_queued, int64_t *h_expanded);
+
+/* BFS that allocates no memory: apspie_bfs's traversal (same arguments and
+ * result, push/pull chosen automatically, or push only when d_tptr is NULL)
+ * for callers that cannot call cudaMalloc -- code running while a stream is
+ * captured into a CUDA graph, hosts whose device memory is fixed up front,
+ * plugins inside a process whose allocator they do not own.  No context is
+ * needed: work goes on `stream` (NULL = legacy default stream) of the current
+ * device.  Its scratch is one fixed array in device memory, held by every GPU
+ * that loads the library until the process exits, sized for at most 2^20
+ * vertices and 2^24 edges; larger inputs return APSPIE_ERR_TOO_LARGE without
+ * launching anything.  The first call on a device looks up that array's
+ * device address (and may load the library's device code); make that first
+ * call before any stream capture.  All calls share the one array, so calls
+ * that overlap on the GPU (other streams, other host threads) race; run them
+ * one after another.  Statistics are not reported.  No counterpart in the
+ * reference. */
+int apspie_bfs_noalloc(void *stream, int src, int64_t nnz, int m,
+                       const int *d_ptr, const int *d_ind, const int *d_tptr,
+                       const int *d_tind, int32_t *d_depth, int max_levels);
 
 /* Direction-switch thresholds (Beamer's alpha, beta; defaults 14 and 24) and
  * mode: 0 = switch automatically, 1 = push only, 2 = pull only. */

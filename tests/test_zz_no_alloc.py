@@ -1,0 +1,81 @@
+"""apspie_bfs_noalloc -- the BFS entry point that allocates no memory.
+
+Callers such as code running under CUDA graph stream capture, hosts with a
+fixed device-memory budget, or plugins in a process whose allocator they do
+not own cannot call cudaMalloc.  This entry point keeps its scratch in one
+fixed device array (at most 2^20 vertices, 2^24 edges).  The test calls it
+through the C ABI and checks it against apspie_bfs, the entry point that
+draws scratch from a context workspace: BFS depths are integers, so the
+tolerance is zero.  Two calls in a row on the same array show that the
+contents left by one call do not leak into the next.
+
+The file name sorts last so that a run stopping at the first failure has
+already run every other test."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+APSPIE_ERR_TOO_LARGE = 8
+
+
+def _p(t):
+    return C.c_void_p(0 if t is None else t.data_ptr())
+
+
+def _noalloc(lib, stream, g, src, out, tptr, tind, max_levels=0):
+    return lib.apspie_bfs_noalloc(C.c_void_p(stream.cuda_stream), int(src), int(g.nnz), int(g.m),
+                                  _p(g.ptr), _p(g.ind), _p(tptr), _p(tind), _p(out),
+                                  int(max_levels))
+
+
+@pytest.mark.parametrize("symmetric", [True, False])
+def test_noalloc_bfs_matches_bfs_twice(symmetric):
+    import torch
+
+    import apspie_b200 as ap
+    from apspie_b200._native import lib
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    h = ap.gen_rmat(16, 16, seed=21, symmetric=symmetric)   # 65,536 vertices, within the limits
+    g = h.to_device()
+    tptr, tind = (g.ptr, g.ind) if symmetric else (g.tptr, g.tind)
+    stream = torch.cuda.current_stream()
+    with ap.Context(0) as ctx:
+        sources = ap.seeded_sources(h, 2, seed=4)
+        for s in sources:                       # two calls in a row share the scratch array
+            ref = ap.bfs(ctx, g, s).cpu().numpy()
+            out = torch.full((h.m,), 7, dtype=torch.int32, device="cuda")
+            assert _noalloc(lib, stream, g, s, out, tptr, tind) == 0
+            torch.cuda.synchronize()
+            np.testing.assert_array_equal(out.cpu().numpy(), ref)
+        # the fixed iteration count and the push-only form (no in-adjacency)
+        s = sources[0]
+        ref = ap.bfs(ctx, g, s, max_levels=3).cpu().numpy()
+        out = torch.empty(h.m, dtype=torch.int32, device="cuda")
+        assert _noalloc(lib, stream, g, s, out, None, None, max_levels=3) == 0
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out.cpu().numpy(), ref)
+
+
+def test_noalloc_rejects_sizes_beyond_the_limit():
+    import torch
+
+    from apspie_b200._native import lib
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    stream = torch.cuda.current_stream()
+    ptr = torch.zeros(2, dtype=torch.int32, device="cuda")
+    out = torch.empty(1, dtype=torch.int32, device="cuda")
+    # more vertices than the array holds: refused before anything is launched
+    rc = lib.apspie_bfs_noalloc(C.c_void_p(stream.cuda_stream), 0, 0, (1 << 20) + 1, _p(ptr),
+                                None, None, None, _p(out), 0)
+    assert rc == APSPIE_ERR_TOO_LARGE
+    rc = lib.apspie_bfs_noalloc(C.c_void_p(stream.cuda_stream), 0, (1 << 24) + 1, 1, _p(ptr),
+                                _p(ptr), None, None, _p(out), 0)
+    assert rc == APSPIE_ERR_TOO_LARGE
+    assert lib.apspie_status_string(rc) == b"input exceeds the fixed scratch size"
