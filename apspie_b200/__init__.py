@@ -8,13 +8,14 @@ through the native library, which raises on import if it is not built.
 from ._native import ApspieError, lib  # noqa: F401  (raises if the .so is missing)
 from .graph import (DeviceGraph, HostGraph, from_edges, gen_er, gen_grid, gen_powerlaw, gen_rmat,  # noqa: F401
                     largest_cc_vertex, mt19937, read_mtx, seeded_sources, weights_f32, weights_u32)
+from .serving import Server  # noqa: F401
 from .ops import (Context, bfs, bfs_set_params, bfs_stats, bfs_trace, mis, mis_rounds,  # noqa: F401
                   neighbor_flags, sssp, sssp_stats, spmspv, mxv_dense, spmspv_set_params,
                   PLUS_TIMES, MIN_PLUS, MAX_TIMES, OR_AND, spgemm, tc_prepare,
-                  triangle_count)
+                  triangle_count, batch_run, batch_stats, autotune_bfs, autotune_spmspv)
 
-__all__ = [
+__all__ = ["Server",
     "ApspieError", "Context", "DeviceGraph", "HostGraph", "bfs", "bfs_set_params", "bfs_stats", "bfs_trace", "from_edges",
-    "sssp", "sssp_stats", "mis", "mis_rounds", "neighbor_flags", "spmspv", "mxv_dense", "spmspv_set_params", "spgemm", "tc_prepare", "triangle_count", "gen_er", "gen_grid", "gen_powerlaw", "gen_rmat", "largest_cc_vertex", "mt19937", "read_mtx", "seeded_sources",
+    "sssp", "sssp_stats", "mis", "mis_rounds", "neighbor_flags", "spmspv", "mxv_dense", "spmspv_set_params", "spgemm", "tc_prepare", "triangle_count", "batch_run", "batch_stats", "autotune_bfs", "autotune_spmspv", "gen_er", "gen_grid", "gen_powerlaw", "gen_rmat", "largest_cc_vertex", "mt19937", "read_mtx", "seeded_sources",
     "weights_f32", "weights_u32",
 ]

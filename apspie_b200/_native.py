@@ -41,6 +41,24 @@ class Csr(C.Structure):
                 ("d_ind", C.c_void_p), ("d_val", C.c_void_p)]
 
 
+class Job(C.Structure):
+    _fields_ = [("type", C.c_int), ("m", C.c_int), ("nnz", C.c_int64), ("d_ptr", C.c_void_p),
+                ("d_ind", C.c_void_p), ("d_tptr", C.c_void_p), ("d_tind", C.c_void_p),
+                ("d_w", C.c_void_p), ("symmetric", C.c_int), ("nsrc", C.c_int),
+                ("h_src", C.POINTER(C.c_int)), ("d_out", C.c_void_p), ("alpha", C.c_int),
+                ("beta", C.c_int)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("super_steps", C.c_int32), ("pad", C.c_int32), ("frontier_edges", C.c_int64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("batches", C.c_uint64), ("jobs", C.c_uint64),
+                ("pending", C.c_uint64), ("in_flight_bytes", C.c_uint64), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("max_ms", C.c_double)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/apspie.h
 PROTOS: dict[str, tuple] = {
     "apspie_ctx_create": (c_int, [c_int, vp, P_vp]),
@@ -71,6 +89,20 @@ PROTOS: dict[str, tuple] = {
     "apspie_csr_copy_out": (c_int, [vp, C.POINTER(Csr), vp, vp, vp]),
     "apspie_tc_prepare": (c_int, [vp, c_i64, c_int, vp, vp, vp, vp, vp, P_i64]),
     "apspie_tc": (c_int, [vp, c_int, c_i64, vp, vp, P_i64]),
+    "apspie_batch_run": (c_int, [vp, c_int, C.POINTER(Job), c_int]),
+    "apspie_batch_get_stats": (c_int, [vp, C.POINTER(BatchStats)]),
+    "apspie_autotune_bfs": (c_int, [vp, c_int, P_int, c_i64, c_int, vp, vp, vp, vp, vp, P_int,
+                                    P_int, C.POINTER(C.c_float)]),
+    "apspie_autotune_spmspv": (c_int, [vp, c_int, c_i64, vp, vp, vp, vp, vp, vp, vp,
+                                       C.POINTER(C.c_double)]),
+    "apspie_server_create": (c_int, [c_int, C.c_size_t, c_int, P_vp]),
+    "apspie_server_add_graph": (c_int, [vp, c_int, c_i64, vp, vp, vp, vp, vp, c_int, P_int]),
+    "apspie_server_submit": (c_int, [vp, c_int, c_int, c_int, c_u32, vp, P_u64]),
+    "apspie_server_poll": (c_int, [vp, c_u64, P_int, C.POINTER(C.c_double)]),
+    "apspie_server_wait": (c_int, [vp, c_u64, C.POINTER(C.c_double)]),
+    "apspie_server_get_stats": (c_int, [vp, C.POINTER(ServerStats)]),
+    "apspie_server_reset_stats": (c_int, [vp]),
+    "apspie_server_destroy": (c_int, [vp]),
     "apspie_gen_rmat_host": (c_int, [c_int, c_int, c_u64, c_int, c_int, P_int, P_i64, P_vp, P_vp]),
     "apspie_gen_er_host": (c_int, [c_int, c_int, c_u64, P_i64, P_vp, P_vp]),
     "apspie_gen_grid_host": (c_int, [c_int, c_int, P_i64, P_vp, P_vp]),

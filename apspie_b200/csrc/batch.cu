@@ -1,0 +1,798 @@
+// batch.cu -- many traversals on graphs of uneven size in one launch.
+//
+// A persistent work-queue kernel runs a set of jobs together.  A job is
+//   * a multi-source BFS over up to 64 sources of one graph: every vertex
+//     carries 64-bit masks (visited, and the frontier of three consecutive
+//     levels), bit s standing for source s -- the "frontier matrix" of
+//     MS-BFS; or
+//   * a batched uint32 SSSP over up to 64 sources of one graph: frontier
+//     items are (source, vertex) pairs, relaxed with atomicMin on
+//     dist[source][vertex].
+// Each super-step advances every unfinished job by one level / round.  The
+// work of a super-step is cut into units (32 frontier vertices, one 128-edge
+// chunk of a hub, 32 vertices of a pull sweep, 32 stale frontier words to
+// clear) and the units of all jobs are dealt round-robin over the warps of
+// the grid, so a large graph and a small one share the GPU in the same
+// launch.  Super-steps are separated by the bounded grid barrier; per-job
+// direction switches (push / pull, Beamer's rule with per-job thresholds from
+// the autotuner) are decided identically by every block from counters that
+// nobody writes during the step in which they are read.
+//
+// Per source, the results are exactly those of the single-source kernels:
+// BFS levels are set once per (source, vertex) by the thread whose atomicOr
+// on the visited mask first sets the bit; SSSP converges to the same
+// min-plus fixpoint.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "context.h"
+#include "frontier.cuh"
+
+namespace apspie {
+namespace {
+
+constexpr int kBatchThreads = 512;
+constexpr int kMaxJobs = 64;
+constexpr int kJobBfs = 0, kJobSssp = 1;
+
+struct JobCounters {
+  unsigned q, chunks, nbig, pad;
+  unsigned long long edges;
+};
+
+struct BatchJob {
+  int type, m, nsrc, alpha;
+  int beta, pad0;
+  long long nnz;
+  const int *ptr, *ind, *tptr, *tind;
+  const uint32_t *w;
+  const int *src;
+  int32_t *out;  // BFS: vertex-major depth [m][64]; SSSP: dist [nsrc][m]
+  unsigned long long *visited, *F0, *F1, *F2;
+  int *q0, *q1, *q2;
+  int2 *c0, *c1, *c2;
+  int *stamp;
+  JobCounters c[3];
+};
+
+struct BatchState {
+  unsigned bar[2];
+  int err;
+  int steps;
+  unsigned long long edges;  // sum over jobs of frontier edges walked
+};
+
+__device__ __forceinline__ unsigned long long *jobF(BatchJob *j, int i) {
+  return i == 0 ? j->F0 : (i == 1 ? j->F1 : j->F2);
+}
+__device__ __forceinline__ int *jobQ(BatchJob *j, int i) {
+  return i == 0 ? j->q0 : (i == 1 ? j->q1 : j->q2);
+}
+__device__ __forceinline__ int2 *jobC(BatchJob *j, int i) {
+  return i == 0 ? j->c0 : (i == 1 ? j->c1 : j->c2);
+}
+
+__device__ __forceinline__ unsigned long long srcmask(int nsrc) {
+  return nsrc >= 64 ? ~0ull : ((1ull << nsrc) - 1ull);
+}
+
+// ------------------------------------------------------------------ init ---
+__global__ void batch_init_bfs(BatchJob *jobs, int jid) {
+  BatchJob *j = jobs + jid;
+  const int m = j->m;
+  const size_t n64 = (size_t)m * 64;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n64;
+       i += (size_t)gridDim.x * blockDim.x)
+    j->out[i] = -1;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < m; v += gridDim.x * blockDim.x) {
+    j->visited[v] = 0ull;
+    j->F0[v] = 0ull;
+    j->F1[v] = 0ull;
+    j->F2[v] = 0ull;
+  }
+}
+
+// sources: set visited / frontier bits and depth 0, queue each distinct source
+__global__ void batch_seed_bfs(BatchJob *jobs, int jid) {
+  BatchJob *j = jobs + jid;
+  if (blockIdx.x != 0) return;
+  for (int s = threadIdx.x; s < j->nsrc; s += blockDim.x) {
+    int v = j->src[s];
+    atomicOr(j->visited + v, 1ull << s);
+    atomicOr(j->F0 + v, 1ull << s);
+    j->out[(size_t)v * 64 + s] = 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 3; ++i) j->c[i] = JobCounters{0, 0, 0, 0, 0ull};
+    // queue the distinct sources (those whose frontier word was set first here)
+    for (int s = 0; s < j->nsrc; ++s) {
+      int v = j->src[s];
+      bool first = true;
+      for (int t = 0; t < s; ++t)
+        if (j->src[t] == v) first = false;
+      if (!first) continue;
+      int deg = __ldg(j->ptr + v + 1) - __ldg(j->ptr + v);
+      if (deg > kBigDeg) {
+        int nch = (deg + kChunk - 1) / kChunk;
+        for (int c = 0; c < nch; ++c) j->c0[j->c[0].chunks + c] = make_int2(v, c);
+        j->c[0].chunks += (unsigned)nch;
+        j->c[0].nbig += 1;
+      } else {
+        j->q0[j->c[0].q++] = v;
+      }
+      j->c[0].edges += (unsigned long long)deg;
+    }
+  }
+}
+
+__global__ void batch_init_sssp(BatchJob *jobs, int jid) {
+  BatchJob *j = jobs + jid;
+  const size_t n = (size_t)j->m * j->nsrc;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    j->out[i] = -1;  // 0xFFFFFFFF: unreached
+    j->stamp[i] = -1;
+  }
+}
+
+__global__ void batch_seed_sssp(BatchJob *jobs, int jid) {
+  BatchJob *j = jobs + jid;
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int i = 0; i < 3; ++i) j->c[i] = JobCounters{0, 0, 0, 0, 0ull};
+  for (int s = 0; s < j->nsrc; ++s) {
+    int v = j->src[s];
+    int item = s * j->m + v;
+    j->out[item] = 0;
+    int deg = __ldg(j->ptr + v + 1) - __ldg(j->ptr + v);
+    if (deg > kBigDeg) {
+      int nch = (deg + kChunk - 1) / kChunk;
+      for (int c = 0; c < nch; ++c) j->c0[j->c[0].chunks + c] = make_int2(item, c);
+      j->c[0].chunks += (unsigned)nch;
+      j->c[0].nbig += 1;
+    } else {
+      j->q0[j->c[0].q++] = item;
+    }
+    j->c[0].edges += (unsigned long long)deg;
+  }
+}
+
+// --------------------------------------------------------- append helper ---
+// Appends up to N candidates per lane (an item id u with degree deg, or
+// nothing) to the job's next queue / chunk list.  Warp-collective.
+template <int N>
+__device__ __forceinline__ void append_n(const bool (&found)[N], const int (&u)[N],
+                                         const int (&deg)[N], int *qout, int2 *cout,
+                                         JobCounters *nxt) {
+  const int lane = lane_id();
+  int nsmall = 0, nbig = 0, nchunk = 0;
+  unsigned long long edges = 0;
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    bool big = found[r] && deg[r] > kBigDeg;
+    nsmall += (found[r] && !big) ? 1 : 0;
+    nbig += big ? 1 : 0;
+    nchunk += big ? (deg[r] + kChunk - 1) / kChunk : 0;
+    edges += found[r] ? (unsigned long long)deg[r] : 0ull;
+  }
+  int qincl = warp_incl_scan(nsmall);
+  int qtot = __shfl_sync(kFull, qincl, 31);
+  if (qtot) {
+    unsigned qbase = 0;
+    if (lane == 31) qbase = atomicAdd(&nxt->q, (unsigned)qtot);
+    qbase = __shfl_sync(kFull, qbase, 31) + (unsigned)(qincl - nsmall);
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+      if (found[r] && deg[r] <= kBigDeg) qout[qbase++] = u[r];
+  }
+  unsigned bmask = __ballot_sync(kFull, nbig > 0);
+  if (bmask) {
+    int cincl = warp_incl_scan(nchunk);
+    int ctot = __shfl_sync(kFull, cincl, 31);
+    int btot = warp_sum(nbig);
+    unsigned cbase = 0;
+    if (lane == 0) {
+      cbase = atomicAdd(&nxt->chunks, (unsigned)ctot);
+      atomicAdd(&nxt->nbig, (unsigned)btot);
+    }
+    cbase = __shfl_sync(kFull, cbase, 0) + (unsigned)(cincl - nchunk);
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      bool big = found[r] && deg[r] > kBigDeg;
+      int nch = big ? (deg[r] + kChunk - 1) / kChunk : 0;
+      unsigned rm = __ballot_sync(kFull, big);
+      while (rm) {
+        int jl = __ffs(rm) - 1;
+        rm &= rm - 1;
+        int uj = __shfl_sync(kFull, u[r], jl);
+        unsigned bj = __shfl_sync(kFull, cbase, jl);
+        int nj = __shfl_sync(kFull, nch, jl);
+        for (int c = lane; c < nj; c += 32) cout[bj + c] = make_int2(uj, c);
+      }
+      cbase += (unsigned)nch;
+    }
+  }
+  edges = warp_sum(edges);
+  if (lane == 0 && edges) atomicAdd(&nxt->edges, edges);
+}
+
+// ------------------------------------------------------------ MS-BFS ---
+// Push relaxation of edge (v -> u) carrying frontier mask f at level L:
+// claims the bits of f that u has not seen; returns true when u enters the
+// next frontier for the first time in this level.
+__device__ __forceinline__ bool msbfs_relax(BatchJob *j, unsigned long long f, int u, int next,
+                                            unsigned long long *Fn) {
+  unsigned long long nb = f & ~__ldcg(j->visited + u);
+  if (!nb) return false;
+  unsigned long long old = atomicOr(j->visited + u, nb);
+  unsigned long long mine = nb & ~old;
+  if (!mine) return false;
+  int32_t *row = j->out + (size_t)u * 64;
+  for (unsigned long long b = mine; b; b &= b - 1) row[__ffsll((long long)b) - 1] = next;
+  return atomicOr(Fn + u, mine) == 0ull;
+}
+
+// 32 queued frontier vertices, edges dealt flat over the warp
+__device__ void msbfs_push_queue(BatchJob *j, int L, int unit, unsigned nq) {
+  const int lane = lane_id();
+  int *qin = jobQ(j, L % 3), *qout = jobQ(j, (L + 1) % 3);
+  int2 *cout = jobC(j, (L + 1) % 3);
+  unsigned long long *Fc = jobF(j, L % 3), *Fn = jobF(j, (L + 1) % 3);
+  JobCounters *nxt = &j->c[(L + 1) % 3];
+  unsigned idx = (unsigned)unit * 32u + lane;
+  int v = idx < nq ? __ldcg(qin + idx) : -1;
+  int s = 0, d = 0;
+  unsigned long long f = 0;
+  if (v >= 0) {
+    s = __ldg(j->ptr + v);
+    d = __ldg(j->ptr + v + 1) - s;
+    f = __ldcg(Fc + v);
+  }
+  int incl = warp_incl_scan(d);
+  int excl = incl - d;
+  int total = __shfl_sync(kFull, incl, 31);
+  for (int e0 = 0; e0 < total; e0 += 32) {
+    int e = e0 + lane;
+    int owner = warp_owner(excl, e);
+    int so = __shfl_sync(kFull, s, owner);
+    int eo = __shfl_sync(kFull, excl, owner);
+    unsigned long long fo = __shfl_sync(kFull, f, owner);
+    bool found[1] = {false};
+    int u[1] = {-1}, dg[1] = {0};
+    if (e < total) {
+      u[0] = __ldg(j->ind + so + (e - eo));
+      found[0] = msbfs_relax(j, fo, u[0], L + 1, Fn);
+      if (found[0]) dg[0] = __ldg(j->ptr + u[0] + 1) - __ldg(j->ptr + u[0]);
+    }
+    append_n<1>(found, u, dg, qout, cout, nxt);
+  }
+}
+
+__device__ void msbfs_push_chunk(BatchJob *j, int L, int unit) {
+  const int lane = lane_id();
+  int2 *cin = jobC(j, L % 3), *cout = jobC(j, (L + 1) % 3);
+  int *qout = jobQ(j, (L + 1) % 3);
+  unsigned long long *Fc = jobF(j, L % 3), *Fn = jobF(j, (L + 1) % 3);
+  JobCounters *nxt = &j->c[(L + 1) % 3];
+  int2 ch = __ldcg(cin + unit);
+  int s = __ldg(j->ptr + ch.x) + ch.y * kChunk;
+  int e = min(s + kChunk, __ldg(j->ptr + ch.x + 1));
+  unsigned long long f = __ldcg(Fc + ch.x);
+  for (int k0 = s; k0 < e; k0 += 32) {
+    int k = k0 + lane;
+    bool found[1] = {false};
+    int u[1] = {-1}, dg[1] = {0};
+    if (k < e) {
+      u[0] = __ldg(j->ind + k);
+      found[0] = msbfs_relax(j, f, u[0], L + 1, Fn);
+      if (found[0]) dg[0] = __ldg(j->ptr + u[0] + 1) - __ldg(j->ptr + u[0]);
+    }
+    append_n<1>(found, u, dg, qout, cout, nxt);
+  }
+}
+
+// pull: vertices [32*unit, 32*unit+32) OR the frontier masks of their
+// in-neighbours (round-robin over the warp) until every source still missing
+// at the vertex is covered or the list ends
+__device__ void msbfs_pull(BatchJob *j, int L, int unit, unsigned long long *s_acc,
+                           int *s_rank) {
+  const int lane = lane_id();
+  const int m = j->m;
+  const unsigned long long all = srcmask(j->nsrc);
+  unsigned long long *Fc = jobF(j, L % 3), *Fn = jobF(j, (L + 1) % 3);
+  int *qout = jobQ(j, (L + 1) % 3);
+  int2 *cout = jobC(j, (L + 1) % 3);
+  JobCounters *nxt = &j->c[(L + 1) % 3];
+  int v = unit * 32 + lane;
+  int s = 0, e = 0;
+  unsigned long long want = 0;
+  if (v < m) {
+    want = all & ~__ldcg(j->visited + v);
+    if (want) {
+      s = __ldg(j->tptr + v);
+      e = __ldg(j->tptr + v + 1);
+    }
+  }
+  s_acc[lane] = 0ull;
+  __syncwarp();
+  unsigned U = __ballot_sync(kFull, want != 0 && s < e);
+  while (U) {
+    const int k = __popc(U);
+    const bool mine = (U >> lane) & 1u;
+    const int myrank = __popc(U & ((1u << lane) - 1u));
+    if (mine) s_rank[myrank] = lane;
+    __syncwarp();
+    const int per = 32 / k, extra = 32 % k;
+    const int jr = lane % k, slot = lane / k;
+    const int nl = per + (jr < extra ? 1 : 0);
+    const int owner = s_rank[jr];
+    const int so = __shfl_sync(kFull, s, owner);
+    const int eo = __shfl_sync(kFull, e, owner);
+    unsigned long long acc = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      int idx = so + slot + i * nl;
+      if (idx < eo) acc |= __ldcg(Fc + __ldg(j->tind + idx));
+    }
+    if (acc) atomicOr(s_acc + owner, acc);
+    __syncwarp();
+    if (mine) s += (per + (myrank < extra ? 1 : 0)) * 4;
+    unsigned long long got = *(volatile unsigned long long *)(s_acc + lane);
+    U = __ballot_sync(kFull, mine && (want & ~got) != 0ull && s < e);
+  }
+  unsigned long long nb = want & *(volatile unsigned long long *)(s_acc + lane);
+  bool found[1] = {nb != 0ull};
+  int u[1] = {v}, dg[1] = {0};
+  if (found[0]) {
+    j->visited[v] |= nb;  // only this lane touches v's masks in a pull step
+    Fn[v] = nb;
+    int32_t *row = j->out + (size_t)v * 64;
+    for (unsigned long long b = nb; b; b &= b - 1) row[__ffsll((long long)b) - 1] = L + 1;
+    dg[0] = __ldg(j->ptr + v + 1) - __ldg(j->ptr + v);
+  }
+  append_n<1>(found, u, dg, qout, cout, nxt);
+  __syncwarp();
+}
+
+// clear the frontier words of the level before last (they become the next
+// level's frontier buffer)
+__device__ void msbfs_clear(BatchJob *j, int L, int unit, unsigned prevq, bool chunks) {
+  const int lane = lane_id();
+  const int slot = (L + 2) % 3;
+  unsigned long long *F = jobF(j, slot);
+  unsigned idx = (unsigned)unit * 32u + lane;
+  if (idx >= prevq) return;
+  if (chunks) {
+    int2 c = __ldcg(jobC(j, slot) + idx);
+    if (c.y == 0) F[c.x] = 0ull;
+  } else {
+    F[__ldcg(jobQ(j, slot) + idx)] = 0ull;
+  }
+}
+
+// ------------------------------------------------------------ SSSP lanes ---
+__device__ __forceinline__ bool sssp_relax(BatchJob *j, int item_base, unsigned du, int k, int u,
+                                           int round) {
+  unsigned nd = du + __ldg(j->w + k);
+  if (nd < du || nd == 0xffffffffu) nd = 0xfffffffeu;
+  unsigned *dist = (unsigned *)j->out;
+  int it = item_base + u;
+  if (nd >= __ldcg(dist + it)) return false;
+  if (nd >= atomicMin(dist + it, nd)) return false;
+  return atomicExch(j->stamp + it, round) != round;
+}
+
+__device__ void sssp_queue(BatchJob *j, int L, int unit, unsigned nq) {
+  const int lane = lane_id();
+  const int m = j->m;
+  int *qin = jobQ(j, L % 2), *qout = jobQ(j, (L + 1) % 2);
+  int2 *cout = jobC(j, (L + 1) % 2);
+  JobCounters *nxt = &j->c[(L + 1) % 3];
+  const unsigned *dist = (const unsigned *)j->out;
+  unsigned idx = (unsigned)unit * 32u + lane;
+  int item = idx < nq ? __ldcg(qin + idx) : -1;
+  int s = 0, d = 0, base = 0;
+  unsigned du = 0;
+  if (item >= 0) {
+    int v = item % m;
+    base = item - v;
+    s = __ldg(j->ptr + v);
+    d = __ldg(j->ptr + v + 1) - s;
+    du = __ldcg(dist + item);
+  }
+  int incl = warp_incl_scan(d);
+  int excl = incl - d;
+  int total = __shfl_sync(kFull, incl, 31);
+  for (int e0 = 0; e0 < total; e0 += 32) {
+    int e = e0 + lane;
+    int owner = warp_owner(excl, e);
+    int so = __shfl_sync(kFull, s, owner);
+    int eo = __shfl_sync(kFull, excl, owner);
+    unsigned duo = __shfl_sync(kFull, du, owner);
+    int bo = __shfl_sync(kFull, base, owner);
+    bool found[1] = {false};
+    int u[1] = {-1}, dg[1] = {0};
+    if (e < total) {
+      int k = so + (e - eo);
+      int dst = __ldg(j->ind + k);
+      found[0] = sssp_relax(j, bo, duo, k, dst, L);
+      if (found[0]) {
+        u[0] = bo + dst;
+        dg[0] = __ldg(j->ptr + dst + 1) - __ldg(j->ptr + dst);
+      }
+    }
+    append_n<1>(found, u, dg, qout, cout, nxt);
+  }
+}
+
+__device__ void sssp_chunk(BatchJob *j, int L, int unit) {
+  const int lane = lane_id();
+  const int m = j->m;
+  int2 *cin = jobC(j, L % 2), *cout = jobC(j, (L + 1) % 2);
+  int *qout = jobQ(j, (L + 1) % 2);
+  JobCounters *nxt = &j->c[(L + 1) % 3];
+  int2 ch = __ldcg(cin + unit);
+  int v = ch.x % m, base = ch.x - v;
+  int s = __ldg(j->ptr + v) + ch.y * kChunk;
+  int e = min(s + kChunk, __ldg(j->ptr + v + 1));
+  unsigned du = __ldcg((const unsigned *)j->out + ch.x);
+  for (int k0 = s; k0 < e; k0 += 32) {
+    int k = k0 + lane;
+    bool found[1] = {false};
+    int u[1] = {-1}, dg[1] = {0};
+    if (k < e) {
+      int dst = __ldg(j->ind + k);
+      found[0] = sssp_relax(j, base, du, k, dst, L);
+      if (found[0]) {
+        u[0] = base + dst;
+        dg[0] = __ldg(j->ptr + dst + 1) - __ldg(j->ptr + dst);
+      }
+    }
+    append_n<1>(found, u, dg, qout, cout, nxt);
+  }
+}
+
+// ---------------------------------------------------------------- kernel ---
+__global__ void __launch_bounds__(kBatchThreads, 2)
+batch_persistent(BatchJob *jobs, int njobs, BatchState *st, int max_steps) {
+  const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  const int warp = warp_in_block();
+  __shared__ unsigned s_q[kMaxJobs], s_ch[kMaxJobs];
+  __shared__ unsigned long long s_edges[kMaxJobs], s_explored[kMaxJobs];
+  __shared__ unsigned s_prevq[kMaxJobs], s_prevch[kMaxJobs];
+  __shared__ int s_pull[kMaxJobs], s_done[kMaxJobs];
+  // unit layout per job: [clear queue][clear chunks][work: queue or pull][work chunks]
+  __shared__ unsigned s_u0[kMaxJobs], s_u1[kMaxJobs], s_u2[kMaxJobs], s_u3[kMaxJobs];
+  __shared__ unsigned s_pre[kMaxJobs + 1];
+  __shared__ unsigned long long s_acc[kBatchThreads / 32][32];
+  __shared__ int s_rank[kBatchThreads / 32][32];
+
+  for (int jj = threadIdx.x; jj < njobs; jj += blockDim.x) {
+    s_explored[jj] = 0;
+    s_pull[jj] = 0;
+    s_done[jj] = 0;
+    s_prevq[jj] = 0;
+    s_prevch[jj] = 0;
+  }
+  __syncthreads();
+  int step = 0;
+  for (;; ++step) {
+    if (threadIdx.x == 0) {
+      unsigned run = 0;
+      for (int jj = 0; jj < njobs; ++jj) {
+        BatchJob *j = jobs + jj;
+        JobCounters *cur = &j->c[step % 3];
+        unsigned q = __ldcg(&cur->q), ch = __ldcg(&cur->chunks), nb = __ldcg(&cur->nbig);
+        unsigned long long ed = __ldcg(&cur->edges);
+        s_q[jj] = q;
+        s_ch[jj] = ch;
+        s_edges[jj] = ed;
+        if (blockIdx.x == 0) j->c[(step + 2) % 3] = JobCounters{0, 0, 0, 0, 0ull};
+        unsigned long long nf = (unsigned long long)q + nb;
+        bool active = !s_done[jj] && nf > 0 && (max_steps <= 0 || step < max_steps);
+        if (!active) s_done[jj] = 1;
+        unsigned u0 = 0, u1 = 0, u2 = 0, u3 = 0;
+        if (j->type == kJobBfs) {
+          // clear the frontier words of level step-1 (they are reused at step+1)
+          u0 = (s_prevq[jj] + 31) / 32;
+          u1 = (s_prevch[jj] + 31) / 32;
+        }
+        if (active) {
+          s_explored[jj] += ed;
+          if (j->type == kJobBfs) {
+            long long unexplored = j->nnz * (long long)1 - (long long)s_explored[jj];
+            if (!s_pull[jj]) {
+              if ((long long)ed * j->alpha > unexplored) s_pull[jj] = 1;
+            } else if ((long long)nf * j->beta < (long long)j->m) {
+              s_pull[jj] = 0;
+            }
+            if (s_pull[jj]) {
+              u2 = (unsigned)((j->m + 31) / 32);
+            } else {
+              u2 = (q + 31) / 32;
+              u3 = ch;
+            }
+          } else {
+            u2 = (q + 31) / 32;
+            u3 = ch;
+          }
+        }
+        s_u0[jj] = u0;
+        s_u1[jj] = u1;
+        s_u2[jj] = u2;
+        s_u3[jj] = u3;
+        s_pre[jj] = run;
+        run += u0 + u1 + u2 + u3;
+      }
+      s_pre[njobs] = run;
+    }
+    __syncthreads();
+    const unsigned total = s_pre[njobs];
+    bool any_active = false;
+    for (int jj = 0; jj < njobs; ++jj) any_active |= !s_done[jj];
+    if (!any_active) break;
+    for (unsigned g = (unsigned)gwarp; g < total; g += (unsigned)nwarps) {
+      int lo = 0, hi = njobs - 1;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (s_pre[mid] <= g) lo = mid; else hi = mid - 1;
+      }
+      // skip empty jobs that share the same prefix
+      while (lo + 1 < njobs && s_pre[lo + 1] <= g) ++lo;
+      BatchJob *j = jobs + lo;
+      unsigned loc = g - s_pre[lo];
+      if (loc < s_u0[lo]) {
+        msbfs_clear(j, step, (int)loc, s_prevq[lo], false);
+        continue;
+      }
+      loc -= s_u0[lo];
+      if (loc < s_u1[lo]) {
+        msbfs_clear(j, step, (int)loc, s_prevch[lo], true);
+        continue;
+      }
+      loc -= s_u1[lo];
+      if (j->type == kJobBfs) {
+        if (s_pull[lo]) {
+          msbfs_pull(j, step, (int)loc, s_acc[warp], s_rank[warp]);
+        } else if (loc < s_u2[lo]) {
+          msbfs_push_queue(j, step, (int)loc, s_q[lo]);
+        } else {
+          msbfs_push_chunk(j, step, (int)(loc - s_u2[lo]));
+        }
+      } else {
+        if (loc < s_u2[lo])
+          sssp_queue(j, step, (int)loc, s_q[lo]);
+        else
+          sssp_chunk(j, step, (int)(loc - s_u2[lo]));
+      }
+    }
+    if (threadIdx.x == 0) {
+      for (int jj = 0; jj < njobs; ++jj) {
+        // the frontier of this step is cleared two steps later
+        bool was_active = s_u2[jj] + s_u3[jj] > 0;
+        s_prevq[jj] = was_active ? s_q[jj] : 0;
+        s_prevch[jj] = was_active ? s_ch[jj] : 0;
+      }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      unsigned long long ed = 0;
+      for (int jj = 0; jj < njobs; ++jj)
+        if (s_u2[jj] + s_u3[jj] > 0) ed += s_edges[jj];
+      st->edges += ed;
+    }
+    if (!grid_barrier(st->bar, &st->err)) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->steps = step;
+}
+
+// vertex-major depth [m][64] -> source-major out[s][m] for s < nsrc
+__global__ void batch_transpose(const int32_t *vm, int m, int nsrc, int32_t *out) {
+  __shared__ int32_t tile[32][65];
+  const int v0 = blockIdx.x * 32;
+  for (int t = threadIdx.x; t < 32 * 64; t += blockDim.x) {
+    int vv = t / 64, s = t % 64;
+    tile[vv][s] = (v0 + vv < m) ? vm[(size_t)(v0 + vv) * 64 + s] : -1;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < 32 * 64; t += blockDim.x) {
+    int s = t / 32, vv = t % 32;
+    if (s < nsrc && v0 + vv < m) out[(size_t)s * m + v0 + vv] = tile[vv][s];
+  }
+}
+
+int batch_grid(apspie_context *ctx) {
+  static int cached_dev = -1, cached_grid = 0;
+  if (cached_dev == ctx->device && cached_grid > 0) return cached_grid;
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_persistent, kBatchThreads, 0) !=
+          cudaSuccess ||
+      occ < 1) {
+    cudaGetLastError();
+    return 0;
+  }
+  cached_dev = ctx->device;
+  cached_grid = occ * ctx->num_sms;
+  return cached_grid;
+}
+
+size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+}  // namespace apspie
+
+using namespace apspie;
+
+extern "C" {
+
+int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_steps) {
+  APSPIE_CHECK_CTX(ctx);
+  if (njobs <= 0 || !jobs)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: no jobs");
+  // split jobs into device jobs of at most 64 sources
+  struct Part {
+    int job, first, n;
+  };
+  std::vector<Part> parts;
+  for (int i = 0; i < njobs; ++i) {
+    const apspie_job &J = jobs[i];
+    if ((J.type != APSPIE_JOB_BFS && J.type != APSPIE_JOB_SSSP_U32) || J.m <= 0 || J.nnz < 0 ||
+        J.nnz >= (int64_t)INT32_MAX || J.nsrc <= 0 || !J.h_src || !J.d_ptr || !J.d_out ||
+        (J.nnz > 0 && !J.d_ind) || (J.type == APSPIE_JOB_SSSP_U32 && J.nnz > 0 && !J.d_w))
+      return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: bad job %d", i);
+    for (int s = 0; s < J.nsrc; ++s)
+      if (J.h_src[s] < 0 || J.h_src[s] >= J.m)
+        return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: job %d source %d out of range",
+                         i, J.h_src[s]);
+    for (int f = 0; f < J.nsrc; f += 64) parts.push_back(Part{i, f, std::min(64, J.nsrc - f)});
+  }
+  const int nparts = (int)parts.size();
+  if (nparts > kMaxJobs)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: %d device jobs > %d", nparts,
+                     kMaxJobs);
+  // workspace layout per device job
+  std::vector<size_t> off(nparts + 1, 0);
+  size_t total = align_up(sizeof(BatchJob) * kMaxJobs) + align_up(sizeof(BatchState)) +
+                 align_up(sizeof(int) * 64 * kMaxJobs);
+  const size_t head = total;
+  for (int p = 0; p < nparts; ++p) {
+    const apspie_job &J = jobs[parts[p].job];
+    size_t m = (size_t)J.m, cap = chunk_capacity(J.nnz);
+    size_t b = 0;
+    if (J.type == APSPIE_JOB_BFS) {
+      b += align_up(8 * m) * 4;           // visited + 3 frontier masks
+      b += align_up(4 * m) * 3;           // queues
+      b += align_up(8 * cap) * 3;         // chunk lists
+      b += align_up(4 * m * 64);          // vertex-major depths
+    } else {
+      size_t items = m * (size_t)parts[p].n;
+      if (items >= (size_t)INT32_MAX)
+        return set_error(ctx, APSPIE_ERR_OVERFLOW, "apspie_batch_run: sources x vertices too large");
+      size_t icap = std::min(items, cap * (size_t)parts[p].n);
+      b += align_up(4 * items) * 2;        // queues (two rotate)
+      b += align_up(8 * icap) * 2;         // chunk lists
+      b += align_up(4 * items);            // stamps
+    }
+    off[p] = total;
+    total += b;
+  }
+  unsigned char *ws = (unsigned char *)workspace(ctx, kSlotBatch, total);
+  if (!ws) return APSPIE_ERR_OOM;
+  auto *djobs = (BatchJob *)ws;
+  auto *dstate = (BatchState *)(ws + align_up(sizeof(BatchJob) * kMaxJobs));
+  int *dsrc = (int *)(ws + align_up(sizeof(BatchJob) * kMaxJobs) + align_up(sizeof(BatchState)));
+  (void)head;
+  // host image of the job table (pinned, copied in one transfer); earlier
+  // copies out of the pinned buffer must have completed before it is reused
+  int src_rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "apspie_batch_run");
+  if (src_rc) return src_rc;
+  size_t host_bytes = sizeof(BatchJob) * nparts + sizeof(int) * 64 * nparts;
+  auto *hjobs = (BatchJob *)pinned(ctx, host_bytes);
+  if (!hjobs) return APSPIE_ERR_OOM;
+  int *hsrc = (int *)(hjobs + nparts);
+  for (int p = 0; p < nparts; ++p) {
+    const apspie_job &J = jobs[parts[p].job];
+    BatchJob &B = hjobs[p];
+    std::memset(&B, 0, sizeof(B));
+    B.type = J.type == APSPIE_JOB_BFS ? kJobBfs : kJobSssp;
+    B.m = J.m;
+    B.nnz = J.nnz;
+    B.nsrc = parts[p].n;
+    B.ptr = J.d_ptr;
+    B.ind = J.d_ind;
+    B.tptr = J.d_tptr ? J.d_tptr : J.d_ptr;
+    B.tind = J.d_tptr ? J.d_tind : J.d_ind;
+    B.w = J.d_w;
+    B.alpha = J.alpha >= 0 ? J.alpha : ctx->bfs_alpha;
+    B.beta = J.beta >= 0 ? J.beta : ctx->bfs_beta;
+    // no in-adjacency for a directed graph: never pull (alpha 0)
+    if (!J.d_tptr && !J.symmetric) B.alpha = 0;
+    for (int s = 0; s < parts[p].n; ++s) hsrc[p * 64 + s] = J.h_src[parts[p].first + s];
+    B.src = dsrc + p * 64;
+    unsigned char *b = ws + off[p];
+    size_t m = (size_t)J.m, cap = chunk_capacity(J.nnz);
+    if (B.type == kJobBfs) {
+      B.visited = (unsigned long long *)b; b += align_up(8 * m);
+      B.F0 = (unsigned long long *)b; b += align_up(8 * m);
+      B.F1 = (unsigned long long *)b; b += align_up(8 * m);
+      B.F2 = (unsigned long long *)b; b += align_up(8 * m);
+      B.q0 = (int *)b; b += align_up(4 * m);
+      B.q1 = (int *)b; b += align_up(4 * m);
+      B.q2 = (int *)b; b += align_up(4 * m);
+      B.c0 = (int2 *)b; b += align_up(8 * cap);
+      B.c1 = (int2 *)b; b += align_up(8 * cap);
+      B.c2 = (int2 *)b; b += align_up(8 * cap);
+      B.out = (int32_t *)b;  // vertex-major; transposed into the caller's array after
+    } else {
+      size_t items = m * (size_t)B.nsrc;
+      size_t icap = std::min(items, cap * (size_t)B.nsrc);
+      B.q0 = (int *)b; b += align_up(4 * items);
+      B.q1 = (int *)b; b += align_up(4 * items);
+      B.q2 = B.q0;
+      B.c0 = (int2 *)b; b += align_up(8 * icap);
+      B.c1 = (int2 *)b; b += align_up(8 * icap);
+      B.c2 = B.c0;
+      B.stamp = (int *)b;
+      B.out = (int32_t *)J.d_out + (size_t)parts[p].first * m;
+    }
+  }
+  cudaStream_t st = ctx->stream;
+  cudaMemcpyAsync(djobs, hjobs, host_bytes, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(dsrc, hsrc, sizeof(int) * 64 * nparts, cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(dstate, 0, sizeof(BatchState), st);
+  int rc = check_cuda(ctx, cudaGetLastError(), "apspie_batch_run upload");
+  if (rc) return rc;
+  for (int p = 0; p < nparts; ++p) {
+    const int m = jobs[parts[p].job].m;
+    int g = std::max(1, std::min((m * (hjobs[p].type == kJobBfs ? 64 : hjobs[p].nsrc) + 255) / 256,
+                                 ctx->num_sms * 8));
+    if (hjobs[p].type == kJobBfs) {
+      batch_init_bfs<<<g, 256, 0, st>>>(djobs, p);
+      batch_seed_bfs<<<1, 64, 0, st>>>(djobs, p);
+    } else {
+      batch_init_sssp<<<g, 256, 0, st>>>(djobs, p);
+      batch_seed_sssp<<<1, 32, 0, st>>>(djobs, p);
+    }
+  }
+  rc = check_launch(ctx, "batch init", 2 * nparts);
+  if (rc) return rc;
+  int grid = batch_grid(ctx);
+  if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_batch_run: occupancy query failed");
+  int np = nparts;
+  void *args[] = {&djobs, &np, &dstate, &max_steps};
+  cudaError_t e = cudaLaunchCooperativeKernel((const void *)batch_persistent, dim3(grid),
+                                              dim3(kBatchThreads), args, 0, st);
+  if (e != cudaSuccess) return check_cuda(ctx, e, "batch_persistent");
+  ctx->launches += 1;
+  for (int p = 0; p < nparts; ++p) {
+    if (hjobs[p].type != kJobBfs) continue;
+    const apspie_job &J = jobs[parts[p].job];
+    batch_transpose<<<(J.m + 31) / 32, 256, 0, st>>>(hjobs[p].out, J.m, parts[p].n,
+                                                     J.d_out + (size_t)parts[p].first * J.m);
+  }
+  rc = check_launch(ctx, "batch_transpose", nparts);
+  if (rc) return rc;
+  ctx->batch_state = dstate;
+  return APSPIE_OK;
+}
+
+int apspie_batch_get_stats(apspie_ctx ctx, apspie_batch_stats *out) {
+  APSPIE_CHECK_CTX(ctx);
+  if (!out || !ctx->batch_state)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_get_stats: no batch has run");
+  auto *h = (BatchState *)pinned(ctx, sizeof(BatchState));
+  if (!h) return APSPIE_ERR_OOM;
+  cudaMemcpyAsync(h, ctx->batch_state, sizeof(BatchState), cudaMemcpyDeviceToHost, ctx->stream);
+  int rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "apspie_batch_get_stats");
+  if (rc) return rc;
+  out->super_steps = h->steps;
+  out->frontier_edges = (int64_t)h->edges;
+  if (h->err) return set_error(ctx, APSPIE_ERR_TIMEOUT, "apspie_batch_run: grid barrier timed out");
+  return APSPIE_OK;
+}
+
+}  // extern "C"

@@ -359,7 +359,7 @@ int apspie_bfs_get_stats(apspie_ctx ctx, apspie_bfs_stats *out) {
 }
 
 int apspie_bfs_set_params(apspie_ctx ctx, int alpha, int beta, int mode) {
-  if (!ctx || alpha <= 0 || beta <= 0 || mode < 0 || mode > 2) return APSPIE_ERR_INVALID;
+  if (!ctx || alpha < 0 || beta < 0 || mode < 0 || mode > 2) return APSPIE_ERR_INVALID;
   ctx->bfs_alpha = alpha;
   ctx->bfs_beta = beta;
   ctx->bfs_mode = mode;

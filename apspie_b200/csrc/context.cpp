@@ -58,7 +58,10 @@ void *workspace(apspie_context *ctx, int id, size_t bytes) {
 
 void *pinned(apspie_context *ctx, size_t bytes) {
   if (ctx->pinned_bytes >= bytes) return ctx->pinned;
-  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  if (ctx->pinned) {
+    cudaStreamSynchronize(ctx->stream);  // copies may still read the old buffer
+    cudaFreeHost(ctx->pinned);
+  }
   ctx->pinned = nullptr;
   ctx->pinned_bytes = 0;
   size_t want = bytes < 4096 ? 4096 : bytes;

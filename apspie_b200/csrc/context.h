@@ -37,8 +37,16 @@ struct apspie_context {
   void *bfs_state = nullptr;  // device pointer into a workspace slot
   void *sssp_state = nullptr;
   void *mis_state = nullptr;
+  void *batch_state = nullptr;
   // SpMSpV: the bitmap path is taken when E * factor > m
   double spmspv_sort_factor = 4.0;
+  // autotuner results by graph fingerprint
+  struct TuneEntry {
+    uint64_t fp;
+    int alpha, beta;
+    float ms;
+  };
+  std::vector<TuneEntry> tune_cache;
 };
 
 namespace apspie {
@@ -75,6 +83,7 @@ enum SlotId : int {
   kSlotMxvBuf,
   kSlotMxvFlags,
   kSlotSmall,
+  kSlotBatch,
   kSlotCount
 };
 

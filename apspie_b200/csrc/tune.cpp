@@ -1,0 +1,172 @@
+// tune.cpp -- per-graph autotuner for the traversal and SpMSpV choices.
+//
+// The reference hard-codes its launch shapes (NTHREADS 512, TABLE_SIZE,
+// partSize from an "aggro" factor, src/spgemm.cuh:15, test/spgemm/main.cu:
+// 362-377).  Here the data-dependent choices are measured once per graph:
+//   * BFS push/pull switch points (Beamer's alpha, beta), including
+//     "never pull", timed on sample sources with CUDA events;
+//   * the SpMSpV sort-vs-bitmap threshold, timed on frontiers of growing
+//     density.
+// Results are cached in the context under a fingerprint of the graph (m,
+// nnz and a hash of a sample of the row offsets), so a graph seen again is
+// not re-measured; the batched kernel takes its per-job thresholds from the
+// same cache.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <vector>
+
+#include "context.h"
+
+namespace apspie {
+namespace {
+
+uint64_t fingerprint(apspie_context *ctx, int m, int64_t nnz, const int *d_ptr) {
+  // offsets sampled at 64 evenly spaced rows (plus the last)
+  int *h = (int *)pinned(ctx, sizeof(int) * 65);
+  uint64_t f = 1469598103934665603ull ^ ((uint64_t)m << 32) ^ (uint64_t)nnz;
+  if (!h) return f;
+  for (int i = 0; i <= 64; ++i) {
+    size_t row = (size_t)((int64_t)m * i / 64);
+    cudaMemcpyAsync(h + i, d_ptr + row, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  }
+  cudaStreamSynchronize(ctx->stream);
+  for (int i = 0; i <= 64; ++i) f = (f ^ (uint64_t)(uint32_t)h[i]) * 1099511628211ull;
+  return f;
+}
+
+float time_bfs(apspie_context *ctx, int nsrc, const int *src, int64_t nnz, int m, const int *ptr,
+               const int *ind, const int *tptr, const int *tind, int32_t *depth, int *rc) {
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  // one untimed traversal to settle caches and the workspace
+  *rc = apspie_bfs(ctx, src[0], nnz, m, ptr, ind, tptr, tind, depth, 0);
+  cudaEventRecord(a, ctx->stream);
+  for (int i = 0; i < nsrc && *rc == 0; ++i)
+    *rc = apspie_bfs(ctx, src[i], nnz, m, ptr, ind, tptr, tind, depth, 0);
+  cudaEventRecord(b, ctx->stream);
+  cudaEventSynchronize(b);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return ms;
+}
+
+}  // namespace
+}  // namespace apspie
+
+using namespace apspie;
+
+extern "C" {
+
+int apspie_autotune_bfs(apspie_ctx ctx, int nsrc, const int *h_src, int64_t nnz, int m,
+                        const int *d_ptr, const int *d_ind, const int *d_tptr, const int *d_tind,
+                        int32_t *d_depth_scratch, int *alpha_out, int *beta_out,
+                        float *ms_out) {
+  APSPIE_CHECK_CTX(ctx);
+  if (nsrc <= 0 || !h_src || !d_depth_scratch || !alpha_out || !beta_out)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_bfs: bad arguments");
+  const uint64_t fp = fingerprint(ctx, m, nnz, d_ptr);
+  for (auto &e : ctx->tune_cache)
+    if (e.fp == fp) {
+      *alpha_out = e.alpha;
+      *beta_out = e.beta;
+      if (ms_out) *ms_out = e.ms;
+      ctx->bfs_alpha = e.alpha;
+      ctx->bfs_beta = e.beta;
+      return APSPIE_OK;
+    }
+  const int saved_mode = ctx->bfs_mode;
+  struct Cand {
+    int alpha, beta, mode;
+  };
+  std::vector<Cand> cands = {{14, 24, 0}, {4, 24, 0}, {8, 24, 0},  {32, 24, 0},
+                             {64, 24, 0}, {14, 8, 0}, {14, 64, 0}, {14, 24, 1}};
+  if (!d_tptr) cands = {{14, 24, 1}};
+  float best = 1e30f;
+  Cand pick = cands[0];
+  int rc = 0;
+  for (const Cand &c : cands) {
+    ctx->bfs_alpha = c.alpha;
+    ctx->bfs_beta = c.beta;
+    ctx->bfs_mode = c.mode;
+    float ms = time_bfs(ctx, nsrc, h_src, nnz, m, d_ptr, d_ind, d_tptr, d_tind, d_depth_scratch,
+                        &rc);
+    if (rc) break;
+    if (ms < best) {
+      best = ms;
+      pick = c;
+    }
+  }
+  ctx->bfs_mode = saved_mode;
+  if (rc) return rc;
+  // "never pull" is alpha 0: no frontier satisfies edges * 0 > unexplored
+  int alpha = pick.mode == 1 ? 0 : pick.alpha;
+  ctx->bfs_alpha = alpha;
+  ctx->bfs_beta = pick.beta;
+  ctx->tune_cache.push_back(apspie_context::TuneEntry{fp, alpha, pick.beta, best / nsrc});
+  *alpha_out = alpha;
+  *beta_out = pick.beta;
+  if (ms_out) *ms_out = best / nsrc;
+  return APSPIE_OK;
+}
+
+int apspie_autotune_spmspv(apspie_ctx ctx, int m, int64_t nnz, const int *d_ptr, const int *d_ind,
+                           const float *d_val, int *d_xind_scratch, float *d_xval_scratch,
+                           int *d_yind_scratch, float *d_yval_scratch, double *factor_out) {
+  APSPIE_CHECK_CTX(ctx);
+  if (m <= 0 || !d_xind_scratch || !d_yind_scratch || !d_yval_scratch || !factor_out)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_spmspv: bad arguments");
+  // frontiers of m / 2^k evenly spaced vertices; for each, time both paths
+  // and find the density where the bitmap path starts to win
+  std::vector<int> hx;
+  const double saved = ctx->spmspv_sort_factor;
+  double cross = saved;
+  bool found = false;
+  for (int k = 12; k >= 1 && !found; --k) {
+    int xn = std::max(1, m >> k);
+    hx.resize(xn);
+    for (int i = 0; i < xn; ++i) hx[i] = (int)((int64_t)i * m / xn);
+    cudaMemcpyAsync(d_xind_scratch, hx.data(), sizeof(int) * xn, cudaMemcpyHostToDevice,
+                    ctx->stream);
+    float t[2] = {0, 0};
+    int64_t expanded = 0;
+    for (int path = 0; path < 2; ++path) {
+      ctx->spmspv_sort_factor = path == 0 ? 0.0 : 1e300;  // 0: sort, 1: bitmap
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      int ynnz = 0;
+      int rc = apspie_spmspv(ctx, APSPIE_PLUS_TIMES, m, nnz, d_ptr, d_ind, d_val, xn,
+                             d_xind_scratch, nullptr, d_yind_scratch, d_yval_scratch, &ynnz,
+                             &expanded);
+      cudaEventRecord(a, ctx->stream);
+      for (int r = 0; r < 3 && rc == 0; ++r)
+        rc = apspie_spmspv(ctx, APSPIE_PLUS_TIMES, m, nnz, d_ptr, d_ind, d_val, xn,
+                           d_xind_scratch, nullptr, d_yind_scratch, d_yval_scratch, &ynnz,
+                           &expanded);
+      cudaEventRecord(b, ctx->stream);
+      cudaEventSynchronize(b);
+      cudaEventElapsedTime(&t[path], a, b);
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+      if (rc) {
+        ctx->spmspv_sort_factor = saved;
+        return rc;
+      }
+    }
+    if (t[1] < t[0] && expanded > 0) {
+      // bitmap wins from this density on: E * factor > m  <=>  factor > m / E
+      cross = (double)m / (double)expanded;
+      found = true;
+    }
+  }
+  ctx->spmspv_sort_factor = found ? cross : saved;
+  *factor_out = ctx->spmspv_sort_factor;
+  return APSPIE_OK;
+}
+
+}  // extern "C"

@@ -5,7 +5,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-from ._native import BfsStats, Csr, SsspStats, check, lib
+from ._native import BatchStats, BfsStats, Csr, Job, SsspStats, check, lib
 
 
 class Context:
@@ -258,3 +258,70 @@ def triangle_count(ctx: Context, m: int, lptr, lind) -> int:
     check(lib.apspie_tc(ctx.handle, int(m), int(lind.numel()), _p(lptr), _p(lind),
                         C.byref(out)), ctx.handle, "apspie_tc")
     return int(out.value)
+
+
+JOB_BFS, JOB_SSSP_U32 = 0, 1
+
+
+def batch_run(ctx: Context, jobs: list[dict], max_steps: int = 0):
+    """Run many BFS / SSSP traversals on several graphs in one persistent
+    launch.  Each job: {"type": "bfs" | "sssp", "graph": DeviceGraph,
+    "sources": [...], optional "alpha", "beta"}.  Returns one int32 tensor of
+    shape (len(sources), m) per job (SSSP: uint32 bits, 0xFFFFFFFF
+    unreached)."""
+    import torch
+    outs, keep = [], []
+    arr = (Job * len(jobs))()
+    for i, jd in enumerate(jobs):
+        g = jd["graph"]
+        src = (C.c_int * len(jd["sources"]))(*[int(s) for s in jd["sources"]])
+        keep.append(src)
+        out = torch.empty((len(jd["sources"]), g.m), dtype=torch.int32, device=g.ptr.device)
+        outs.append(out)
+        sym = bool(getattr(g, "symmetric", False))
+        tptr = None if sym else getattr(g, "tptr", None)
+        tind = None if sym else getattr(g, "tind", None)
+        arr[i] = Job(JOB_BFS if jd["type"] == "bfs" else JOB_SSSP_U32, int(g.m), int(g.nnz),
+                     C.c_void_p(g.ptr.data_ptr()), C.c_void_p(g.ind.data_ptr()),
+                     C.c_void_p(0 if tptr is None else tptr.data_ptr()),
+                     C.c_void_p(0 if tind is None else tind.data_ptr()),
+                     C.c_void_p(0 if g.w_u32 is None else g.w_u32.data_ptr()), int(sym),
+                     len(jd["sources"]), src, C.c_void_p(out.data_ptr()),
+                     int(jd.get("alpha", -1)), int(jd.get("beta", -1)))
+    check(lib.apspie_batch_run(ctx.handle, len(jobs), arr, int(max_steps)), ctx.handle,
+          "apspie_batch_run")
+    return outs
+
+
+def batch_stats(ctx: Context) -> dict:
+    s = BatchStats()
+    check(lib.apspie_batch_get_stats(ctx.handle, C.byref(s)), ctx.handle, "apspie_batch_get_stats")
+    return {"super_steps": s.super_steps, "frontier_edges": s.frontier_edges}
+
+
+def autotune_bfs(ctx: Context, g, sources) -> dict:
+    """Pick and cache the BFS direction thresholds for graph g."""
+    import torch
+    depth = torch.empty(g.m, dtype=torch.int32, device=g.ptr.device)
+    src = (C.c_int * len(sources))(*[int(s) for s in sources])
+    sym = bool(getattr(g, "symmetric", False))
+    tptr, tind = (g.ptr, g.ind) if sym else (g.tptr, g.tind)
+    a, b, ms = C.c_int(), C.c_int(), C.c_float()
+    check(lib.apspie_autotune_bfs(ctx.handle, len(sources), src, int(g.nnz), int(g.m), _p(g.ptr),
+                                  _p(g.ind), _p(tptr), _p(tind), _p(depth), C.byref(a),
+                                  C.byref(b), C.byref(ms)), ctx.handle, "apspie_autotune_bfs")
+    return {"alpha": a.value, "beta": b.value, "ms_per_bfs": ms.value}
+
+
+def autotune_spmspv(ctx: Context, g, val=None) -> float:
+    import torch
+    dev = g.ptr.device
+    xi = torch.empty(g.m, dtype=torch.int32, device=dev)
+    xv = torch.empty(g.m, dtype=torch.float32, device=dev)
+    yi = torch.empty(g.m, dtype=torch.int32, device=dev)
+    yv = torch.empty(g.m, dtype=torch.float32, device=dev)
+    f = C.c_double()
+    check(lib.apspie_autotune_spmspv(ctx.handle, int(g.m), int(g.nnz), _p(g.ptr), _p(g.ind),
+                                     _p(val), _p(xi), _p(xv), _p(yi), _p(yv), C.byref(f)),
+          ctx.handle, "apspie_autotune_spmspv")
+    return f.value

@@ -1,0 +1,82 @@
+"""Python handle on the native query server (apspie_server_* in
+include/apspie.h): continuous batching of BFS / SSSP / MIS queries over
+device-resident graphs, with per-query latency."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._native import ServerStats, check, lib
+
+BFS, SSSP, MIS = 0, 1, 2
+
+
+class Server:
+    def __init__(self, device: int = 0, budget_bytes: int = 120 << 30, max_batch: int = 256):
+        self._h = C.c_void_p()
+        check(lib.apspie_server_create(device, budget_bytes, max_batch, C.byref(self._h)),
+              what="apspie_server_create")
+        self._graphs = []      # keep the device tensors alive
+        self._live = {}        # req id -> (result array, graph m)
+
+    def add_graph(self, g) -> int:
+        gid = C.c_int()
+        sym = bool(getattr(g, "symmetric", False))
+        tptr = None if sym else getattr(g, "tptr", None)
+        tind = None if sym else getattr(g, "tind", None)
+        p = lambda t: C.c_void_p(0 if t is None else t.data_ptr())
+        check(lib.apspie_server_add_graph(self._h, int(g.m), int(g.nnz), p(g.ptr), p(g.ind),
+                                          p(tptr), p(tind), p(g.w_u32), int(sym), C.byref(gid)),
+              what="apspie_server_add_graph")
+        self._graphs.append(g)
+        return gid.value
+
+    def submit(self, kind: int, graph: int, source: int = 0, seed: int = 0) -> int:
+        m = self._graphs[graph].m
+        out = np.empty(m, dtype=np.int32)
+        rid = C.c_uint64()
+        check(lib.apspie_server_submit(self._h, int(kind), int(graph), int(source), int(seed),
+                                       C.c_void_p(out.ctypes.data), C.byref(rid)),
+              what="apspie_server_submit")
+        self._live[rid.value] = out
+        return rid.value
+
+    def wait(self, rid: int):
+        lat = C.c_double()
+        check(lib.apspie_server_wait(self._h, C.c_uint64(rid), C.byref(lat)),
+              what="apspie_server_wait")
+        return self._live.pop(rid), lat.value
+
+    def poll(self, rid: int):
+        done, lat = C.c_int(), C.c_double()
+        check(lib.apspie_server_poll(self._h, C.c_uint64(rid), C.byref(done), C.byref(lat)),
+              what="apspie_server_poll")
+        if done.value:
+            return self._live.pop(rid), lat.value
+        return None
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        check(lib.apspie_server_get_stats(self._h, C.byref(s)), what="apspie_server_get_stats")
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def reset_stats(self) -> None:
+        check(lib.apspie_server_reset_stats(self._h), what="apspie_server_reset_stats")
+
+    def close(self) -> None:
+        if self._h:
+            lib.apspie_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -114,8 +114,10 @@ int apspie_bfs_noalloc(void *stream, int src, int64_t nnz, int m,
                        const int *d_ptr, const int *d_ind, const int *d_tptr,
                        const int *d_tind, int32_t *d_depth, int max_levels);
 
-/* Direction-switch thresholds (Beamer's alpha, beta; defaults 14 and 24) and
- * mode: 0 = switch automatically, 1 = push only, 2 = pull only. */
+/* Direction-switch thresholds (Beamer's alpha, beta; defaults 14 and 24):
+ * push -> pull when frontier edges * alpha > unexplored edges, pull -> push
+ * when frontier vertices * beta < m (alpha 0 never pulls).  mode: 0 = switch
+ * automatically, 1 = push only, 2 = pull only. */
 int apspie_bfs_set_params(apspie_ctx ctx, int alpha, int beta, int mode);
 
 /* --------------------------------------------------------------- SSSP ---
@@ -169,6 +171,102 @@ int apspie_mis_get_rounds(apspie_ctx ctx, int *rounds);
 int apspie_neighbor_flags(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr,
                           const int *d_ind, const int32_t *d_in,
                           int32_t *d_out);
+
+/* ------------------------------------------------------ batched traversal ---
+ * Many BFS / SSSP traversals, on graphs of different sizes, in one
+ * persistent launch (no reference counterpart: the reference runs one query
+ * per driver invocation).  A BFS job runs up to 64 sources of a graph as one
+ * multi-source BFS (64-bit per-vertex source masks); more sources are split
+ * into several device jobs.  An SSSP job relaxes (source, vertex) items with
+ * uint32 weights.  Per source the results equal apspie_bfs / apspie_sssp_u32:
+ * d_out holds nsrc rows of m entries (depths, -1 unreached; or distances,
+ * UINT32_MAX unreached).  alpha / beta < 0 take the context's defaults (the
+ * autotuner sets them per graph); alpha 0 never pulls.  At most 64 device jobs per call; nsrc * m
+ * must stay below 2^31 for SSSP jobs.  max_steps > 0 caps the super-steps. */
+typedef enum { APSPIE_JOB_BFS = 0, APSPIE_JOB_SSSP_U32 = 1 } apspie_job_type;
+typedef struct {
+  int type;             /* apspie_job_type */
+  int m;
+  int64_t nnz;
+  const int *d_ptr, *d_ind;    /* out-adjacency */
+  const int *d_tptr, *d_tind;  /* in-adjacency for pull, or NULL */
+  const uint32_t *d_w;         /* SSSP weights */
+  int symmetric;               /* 1: pull may use d_ptr / d_ind */
+  int nsrc;
+  const int *h_src;            /* host array of nsrc sources */
+  int32_t *d_out;              /* nsrc x m results */
+  int alpha, beta;             /* BFS direction thresholds, < 0 = default */
+} apspie_job;
+typedef struct {
+  int32_t super_steps;
+  int32_t pad;
+  int64_t frontier_edges;  /* sum of frontier out-edges over all jobs and steps */
+} apspie_batch_stats;
+
+int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs,
+                     int max_steps);
+/* Statistics of the last batch (synchronises; reports a barrier timeout). */
+int apspie_batch_get_stats(apspie_ctx ctx, apspie_batch_stats *out);
+
+/* ------------------------------------------------------------- serving ---
+ * A query server over device-resident graphs (no reference counterpart).
+ * Queries arrive at any time; a worker thread admits them in arrival order
+ * while their device state fits state_budget_bytes, coalesces the admitted
+ * BFS / SSSP queries by (graph, kind) into one apspie_batch_run launch, runs
+ * MIS queries after it, and copies each result row into the caller's host
+ * buffer.  Two batch slots (each its own context and stream) keep a new batch
+ * queued on the GPU while the previous one is still running.  Query kinds:
+ * 0 = BFS (int32 depths), 1 = SSSP over the graph's uint32 weights (uint32
+ * distances), 2 = MIS with mt19937(seed) priorities (int32 membership).
+ * h_result must hold m 32-bit entries and stay valid until the query is done.
+ * The graphs' device arrays must outlive the server. */
+typedef struct apspie_server *apspie_server_t;
+typedef struct {
+  uint64_t completed, batches, jobs, pending;
+  uint64_t in_flight_bytes;
+  double p50_ms, p99_ms, max_ms;  /* submit -> result in host memory */
+} apspie_server_stats;
+
+int apspie_server_create(int device, size_t state_budget_bytes, int max_batch,
+                         apspie_server_t *out);
+int apspie_server_add_graph(apspie_server_t s, int m, int64_t nnz,
+                            const int *d_ptr, const int *d_ind,
+                            const int *d_tptr, const int *d_tind,
+                            const uint32_t *d_w, int symmetric, int *graph_id);
+/* Non-blocking; APSPIE_ERR_BUSY when the pending queue is full. */
+int apspie_server_submit(apspie_server_t s, int type, int graph, int source,
+                         uint32_t seed, void *h_result, uint64_t *req_id);
+/* *done = 1 once the result is in h_result (the request is then retired and
+ * its status returned). */
+int apspie_server_poll(apspie_server_t s, uint64_t req_id, int *done,
+                       double *latency_ms);
+/* Blocks until the query is done (at most 600 s, else APSPIE_ERR_TIMEOUT). */
+int apspie_server_wait(apspie_server_t s, uint64_t req_id, double *latency_ms);
+int apspie_server_get_stats(apspie_server_t s, apspie_server_stats *out);
+int apspie_server_reset_stats(apspie_server_t s);
+/* Finishes the queued queries, then stops the worker and frees the server. */
+int apspie_server_destroy(apspie_server_t s);
+
+/* ----------------------------------------------------------- autotuner ---
+ * Measures the BFS direction thresholds on the given sample sources (a grid
+ * of alpha / beta values and push-only, timed with CUDA events), stores the
+ * fastest in the context (used by apspie_bfs and, for jobs with alpha / beta
+ * < 0, by apspie_batch_run) and caches it under a fingerprint of the graph
+ * (m, nnz, sampled row offsets); a cached graph is not re-measured.
+ * d_depth_scratch: m int32.  *ms_out (may be NULL) = mean ms per BFS. */
+int apspie_autotune_bfs(apspie_ctx ctx, int nsrc, const int *h_src, int64_t nnz,
+                        int m, const int *d_ptr, const int *d_ind,
+                        const int *d_tptr, const int *d_tind,
+                        int32_t *d_depth_scratch, int *alpha_out, int *beta_out,
+                        float *ms_out);
+/* Finds the frontier density at which the SpMSpV bitmap path beats the
+ * radix-sort path on this matrix and sets the context's sort factor (see
+ * apspie_spmspv_set_params).  Scratch: m ints (x), m ints + m floats (y). */
+int apspie_autotune_spmspv(apspie_ctx ctx, int m, int64_t nnz, const int *d_ptr,
+                           const int *d_ind, const float *d_val,
+                           int *d_xind_scratch, float *d_xval_scratch,
+                           int *d_yind_scratch, float *d_yval_scratch,
+                           double *factor_out);
 
 /* ------------------------------------------------------------- SpMSpV ---
  * Semirings of the reference's three SpMSpV variants. */

@@ -1,0 +1,95 @@
+"""Batched traversal (many BFS / SSSP sources on uneven graphs in one
+persistent launch): every source's result equals the plain single-source
+path and the oracle, bit for bit."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _graphs():
+    import apspie_b200 as ap
+    a = ap.gen_rmat(12, 16, seed=5)
+    b = ap.gen_rmat(14, 16, seed=6)
+    c = ap.gen_grid(64, 64)
+    d = ap.gen_rmat(12, 16, seed=7, symmetric=False)
+    ap.weights_u32(d, seed=2)
+    ap.weights_u32(a, seed=3)
+    return a, b, c, d
+
+
+def test_batch_bfs_and_sssp_mixed(ctx):
+    import apspie_b200 as ap
+    a, b, c, d = _graphs()
+    ga, gb, gc, gd = (x.to_device() for x in (a, b, c, d))
+    rng = np.random.default_rng(0)
+    jobs = [
+        {"type": "bfs", "graph": ga, "sources": ap.seeded_sources(a, 40, seed=1)},
+        {"type": "bfs", "graph": gb, "sources": ap.seeded_sources(b, 100, seed=2)},  # 2 device jobs
+        {"type": "bfs", "graph": gc, "sources": [0, 4095, 2080, 2080]},              # duplicate
+        {"type": "bfs", "graph": gd, "sources": [int(x) for x in rng.integers(0, d.m, 9)]},
+        {"type": "sssp", "graph": gd, "sources": ap.seeded_sources(d, 20, seed=3)},
+        {"type": "sssp", "graph": ga, "sources": ap.seeded_sources(a, 5, seed=4)},
+    ]
+    outs = ap.batch_run(ctx, jobs)
+    st = ap.batch_stats(ctx)
+    assert st["super_steps"] >= 127  # the 64 x 64 grid from a corner has 127 levels
+    for jd, out, h in zip(jobs, outs, (a, b, c, d, d, a)):
+        out = out.cpu().numpy()
+        for i, s in enumerate(jd["sources"]):
+            if jd["type"] == "bfs":
+                ref, _ = oracle.bfs(h.m, h.ptr, h.ind, s)
+                np.testing.assert_array_equal(out[i], ref, err_msg=f"bfs {h.name} src {s}")
+            else:
+                ref = oracle.sssp_u32(h.m, h.ptr, h.ind, h.w_u32, s)
+                np.testing.assert_array_equal(out[i].view(np.uint32), ref,
+                                              err_msg=f"sssp {h.name} src {s}")
+
+
+def test_batch_equals_single_source_path(ctx):
+    import apspie_b200 as ap
+    h = ap.gen_rmat(16, 16, seed=9)
+    g = h.to_device()
+    srcs = ap.seeded_sources(h, 64, seed=5)
+    out = ap.batch_run(ctx, [{"type": "bfs", "graph": g, "sources": srcs}])[0].cpu().numpy()
+    for i, s in enumerate(srcs):
+        np.testing.assert_array_equal(out[i], ap.bfs(ctx, g, s).cpu().numpy())
+
+
+def test_batch_forced_push_and_pull(ctx):
+    import apspie_b200 as ap
+    h = ap.gen_rmat(13, 16, seed=11)
+    g = h.to_device()
+    srcs = ap.seeded_sources(h, 30, seed=6)
+    refs = [oracle.bfs(h.m, h.ptr, h.ind, s)[0] for s in srcs]
+    for alpha, beta in ((0, 24), (1 << 20, 1 << 30)):   # never pull / pull early and stay
+        out = ap.batch_run(ctx, [{"type": "bfs", "graph": g, "sources": srcs, "alpha": alpha,
+                                  "beta": beta}])[0].cpu().numpy()
+        for i in range(len(srcs)):
+            np.testing.assert_array_equal(out[i], refs[i])
+
+
+def test_batch_rejects_bad_jobs(ctx):
+    import apspie_b200 as ap
+    a, *_ = _graphs()
+    ga = a.to_device()
+    with pytest.raises(ap.ApspieError):
+        ap.batch_run(ctx, [{"type": "bfs", "graph": ga, "sources": [a.m]}])
+
+
+def test_autotuner_picks_and_caches(ctx):
+    import apspie_b200 as ap
+    h = ap.gen_rmat(16, 16, seed=12)
+    g = h.to_device()
+    srcs = ap.seeded_sources(h, 4, seed=1)
+    first = ap.autotune_bfs(ctx, g, srcs)
+    again = ap.autotune_bfs(ctx, g, srcs)   # cached: same answer
+    assert first == again and first["ms_per_bfs"] > 0
+    ref, _ = oracle.bfs(h.m, h.ptr, h.ind, srcs[0])
+    np.testing.assert_array_equal(ap.bfs(ctx, g, srcs[0]).cpu().numpy(), ref)
+    ap.bfs_set_params(ctx)  # restore defaults for the other tests
+    f = ap.autotune_spmspv(ctx, g)
+    assert f >= 0
+    ap.spmspv_set_params(ctx)
