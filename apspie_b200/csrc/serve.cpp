@@ -236,6 +236,7 @@ int launch_slot(apspie_server *s, Slot &sl) {
         parts += p;
         ++n;
       }
+      if (n == 0) n = 1;  // a single job beyond 64 device jobs: reported as an error below
       st = apspie_batch_run(sl.ctx, (int)n, jobs.data() + first, 0);
       s->launched_jobs += n;
       first += n;

@@ -216,6 +216,106 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def sssp_leg(ctx, steps=20):
+    """SSSP on R-MAT 20 (directed, dedup), uint32 weights in [1, 255] and
+    float weights in (0, 1]: GTEPS = E_R / device time, inputs resident."""
+    import torch
+    import apspie_b200 as ap
+    h = ap.gen_rmat(20, EDGE_FACTOR, seed=SEED, symmetric=False)
+    ap.weights_u32(h, seed=SEED)
+    ap.weights_f32(h, seed=SEED)
+    g = h.to_device()
+    srcs = ap.seeded_sources(h, steps, seed=3)
+    out = {"graph": f"R-MAT 20 directed, m={h.m}, nnz={h.nnz}"}
+    stream = torch.cuda.current_stream()
+    for kind in ("u32", "f32"):
+        e_r = []
+        for s in srcs[:3]:
+            ap.sssp(ctx, g, s, weights=kind)
+        for s in srcs:
+            ap.sssp(ctx, g, s, weights=kind)
+            e_r.append(ap.sssp_stats(ctx))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for s in srcs:
+            ap.sssp(ctx, g, s, weights=kind)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        edges = sum(x["edges_traversed"] for x in e_r)
+        reached = sum(x["vertices_reached"] for x in e_r) / len(e_r)
+        b_alg = 8.0 * edges / len(e_r) + 8.0 * reached + 4.0 * h.m
+        out[kind] = {"gteps": edges / (ms * 1e-3) / 1e9, "ms_per_sssp": ms / len(srcs),
+                     "hbm_gbs_alg": b_alg / (ms / len(srcs) * 1e-3) / 1e9,
+                     "relaxations_per_edge": sum(x["relaxations"] for x in e_r) / max(edges, 1),
+                     "rounds": e_r[-1]["rounds"]}
+    return out
+
+
+def batched_leg(ctx, big):
+    """256 BFS + 64 SSSP (uint32 weights) sources over R-MAT 12/16/20/22
+    (symmetrised) and the 1024x1024 grid, in one batched launch, against the
+    same queries one at a time through the single-source kernels."""
+    import torch
+    import apspie_b200 as ap
+    graphs = {12: ap.gen_rmat(12, 16, seed=SEED), 16: ap.gen_rmat(16, 16, seed=SEED),
+              20: ap.gen_rmat(20, 16, seed=SEED), 22: big, "grid": ap.gen_grid(1024, 1024)}
+    plan_bfs = {22: 64, 20: 64, 16: 64, 12: 32, "grid": 32}
+    plan_sssp = {22: 8, 20: 16, 16: 16, 12: 16, "grid": 8}
+    dev, jobs, plain = {}, [], []
+    for k, h in graphs.items():
+        if h.w_u32 is None:
+            ap.weights_u32(h, seed=SEED)
+        dev[k] = h.to_device()
+        if k == "grid":
+            srcs = list(range(0, h.m, h.m // 64))
+        else:
+            srcs = ap.seeded_sources(h, plan_bfs[k] + plan_sssp[k], seed=7)
+        jobs.append({"type": "bfs", "graph": dev[k], "sources": srcs[:plan_bfs[k]]})
+        jobs.append({"type": "sssp", "graph": dev[k], "sources": srcs[plan_bfs[k]:][:plan_sssp[k]]})
+    # warm-up + reference results of the plain path (E_R from its stats)
+    edges = 0
+    for j in jobs:
+        for s in j["sources"]:
+            if j["type"] == "bfs":
+                ap.bfs(ctx, j["graph"], s)
+                edges += ap.bfs_stats(ctx)["edges_traversed"]
+            else:
+                ap.sssp(ctx, j["graph"], s, weights="u32")
+                edges += ap.sssp_stats(ctx)["edges_traversed"]
+    ap.batch_run(ctx, jobs)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for j in jobs:
+        for s in j["sources"]:
+            if j["type"] == "bfs":
+                ap.bfs(ctx, j["graph"], s)
+            else:
+                ap.sssp(ctx, j["graph"], s, weights="u32")
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    outs = ap.batch_run(ctx, jobs)
+    torch.cuda.synchronize()
+    batch_s = time.perf_counter() - t0
+    st = ap.batch_stats(ctx)
+    # spot check: every batched result equals the single-source path
+    for j, o in zip(jobs, outs):
+        s = j["sources"][0]
+        ref = (ap.bfs(ctx, j["graph"], s) if j["type"] == "bfs"
+               else ap.sssp(ctx, j["graph"], s, weights="u32"))
+        if not torch.equal(o[0], ref):
+            raise RuntimeError("batched result differs from the single-source path")
+    nq = sum(len(j["sources"]) for j in jobs)
+    return {"queries": nq, "bfs": 256, "sssp": 64,
+            "graphs": "R-MAT 12/16/20/22 symmetrised + grid 1024x1024",
+            "batched_gteps": edges / batch_s / 1e9, "plain_gteps": edges / plain_s / 1e9,
+            "speedup_vs_plain": plain_s / batch_s, "batched_ms": batch_s * 1e3,
+            "plain_ms": plain_s * 1e3, "super_steps": st["super_steps"],
+            "timing": "host wall clock around synchronised launches"}
+
+
 def run_ours(args):
     import torch
     rank, world, local = dist_env()
@@ -318,6 +418,11 @@ def run_ours(args):
            "d2h_bytes_per_step": int(depth_h.numel() * 4),
            "note": "graph CSR copied host->device and depths device->host every step"}
 
+    extras = {}
+    if not args.profile_run and rank == 0:
+        extras["sssp"] = sssp_leg(ctx)
+        extras["batched"] = batched_leg(ctx, h)
+
     # ---- reference CPU BFS on a bounded sample (rank 0, N=1) ----
     cpu = None
     if rank == 0 and world == 1 and not args.profile_run:
@@ -350,6 +455,7 @@ def run_ours(args):
         "level_trace": [[t["dir"], t["frontier"], t["frontier_edges"], round(t["us"], 1)]
                         for t in trace],
     }
+    line.update(extras)
     print(json.dumps(line), flush=True)
 
 
