@@ -105,6 +105,8 @@ PROTOS: dict[str, tuple] = {
     "apspie_server_destroy": (c_int, [vp]),
     "apspie_gen_rmat_host": (c_int, [c_int, c_int, c_u64, c_int, c_int, P_int, P_i64, P_vp, P_vp]),
     "apspie_gen_er_host": (c_int, [c_int, c_int, c_u64, P_i64, P_vp, P_vp]),
+    "apspie_gen_rmat_device": (c_int, [vp, c_int, c_int, c_u64, c_int, c_int, C.POINTER(Csr)]),
+    "apspie_gen_er_device": (c_int, [vp, c_int, c_int, c_u64, C.POINTER(Csr)]),
     "apspie_gen_grid_host": (c_int, [c_int, c_int, P_i64, P_vp, P_vp]),
     "apspie_gen_weights_u32_host": (c_int, [c_int, vp, vp, c_u64, c_u32, c_u32, vp]),
     "apspie_gen_weights_f32_host": (c_int, [c_int, vp, vp, c_u64, vp]),

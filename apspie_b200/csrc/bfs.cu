@@ -32,7 +32,8 @@ namespace apspie {
 namespace {
 
 constexpr int kBfsThreads = 512;
-constexpr int kProbe = 4;         // in-neighbours a lane probes alone in a pull level
+constexpr int kProbe = 4;         // in-neighbours a lane probes per round in a pull level
+constexpr int kScanUnroll = 4;    // depth words a warp loads at once when re-queuing a frontier
 constexpr int kTraceLevels = 64;  // levels recorded in the per-run trace
 
 struct LevelTrace {
@@ -114,6 +115,7 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
   __shared__ int s_rank[kBfsThreads / 32][32];
   __shared__ unsigned s_bcnt;
   __shared__ unsigned long long s_bedg;
+  __shared__ unsigned s_next;  // per-block group counter of pull / compaction sweeps
 
   if (blockIdx.x == 0 && threadIdx.x == 0) st->t_start = globaltimer();
   bool pull = false;
@@ -132,6 +134,7 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
       s_edges = __ldcg(&cur->edges);
       s_bcnt = 0;
       s_bedg = 0;
+      s_next = 0;
       if (blockIdx.x == 0) {
         *clr = LevelCounters{0, 0, 0, 0, 0ull};
         st->comp[(L + 1) & 1] = LevelCounters{0, 0, 0, 0, 0ull};
@@ -168,15 +171,36 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
     if (!pull) {
       if (nimpl) {
         // the frontier came from a pull level and exists only as depth == L:
-        // queue it (and chunk its hubs) before expanding
-        for (int base = gwarp * 32; base < m; base += nwarps * 32) {
-          int v = base + lane;
-          bool f[1] = {v < m && __ldcg(depth + v) == L};
-          int u[1] = {v};
-          unsigned fm = __ballot_sync(kFull, f[0]);
-          if (fm) {
-            discover_n<1, false>(f, u, ptr, qin, cin, &st->comp[L & 1]);
-            if (lane == 0 && L < kTraceLevels) atomicAdd(&st->trace[L].queued, (unsigned long long)__popc(fm));
+        // queue it (and chunk its hubs) before expanding.  Each block scans
+        // its own range of 32-vertex groups, kScanUnroll groups per load
+        // batch, taken from a shared counter.
+        const unsigned ngroups = (unsigned)((m + 31) / 32);
+        const unsigned per_block = (ngroups + gridDim.x - 1) / gridDim.x;
+        const unsigned gbeg = blockIdx.x * per_block;
+        const unsigned gend = min(gbeg + per_block, ngroups);
+        for (;;) {
+          unsigned g0 = 0;
+          if (lane == 0) g0 = atomicAdd(&s_next, (unsigned)kScanUnroll);
+          g0 = __shfl_sync(kFull, g0, 0);
+          if (gbeg + g0 >= gend) break;
+          int dv[kScanUnroll];
+#pragma unroll
+          for (int i = 0; i < kScanUnroll; ++i) {
+            unsigned g = gbeg + g0 + i;
+            int v = (int)(g * 32u) + lane;
+            dv[i] = (g < gend && v < m) ? __ldcg(depth + v) : -1;
+          }
+#pragma unroll
+          for (int i = 0; i < kScanUnroll; ++i) {
+            int v = (int)((gbeg + g0 + i) * 32u) + lane;
+            bool f[1] = {dv[i] == L};
+            int u[1] = {v};
+            unsigned fm = __ballot_sync(kFull, f[0]);
+            if (fm) {
+              discover_n<1, false>(f, u, ptr, qin, cin, &st->comp[L & 1]);
+              if (lane == 0 && L < kTraceLevels)
+                atomicAdd(&st->trace[L].queued, (unsigned long long)__popc(fm));
+            }
           }
         }
         if (!grid_barrier(st->bar, &st->err)) return;
@@ -203,12 +227,45 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
       // not queued: the next frontier is depth == L + 1.
       unsigned cnt = 0;
       unsigned long long edg = 0;
-      for (int base = gwarp * 32; base < m; base += nwarps * 32) {
-        int v = base + lane;
+      // Each block owns a contiguous range of 32-vertex groups; its warps
+      // take groups from a shared counter (no warp waits at the level end on
+      // a statically assigned slow group), and the depth word and in-offsets
+      // of the next group are loaded while the current one is probed.
+      const unsigned ngroups = (unsigned)((m + 31) / 32);
+      const unsigned per_block = (ngroups + gridDim.x - 1) / gridDim.x;
+      const unsigned gbeg = blockIdx.x * per_block;
+      const unsigned gend = min(gbeg + per_block, ngroups);
+      auto grab = [&]() {
+        unsigned g = 0;
+        if (lane == 0) g = atomicAdd(&s_next, 1u);
+        return gbeg + __shfl_sync(kFull, g, 0);
+      };
+      unsigned g = grab();
+      int pv = -2, ps = 0, pe = 0;  // prefetched depth and in-range of the next group
+      if (g < gend) {
+        int v = (int)(g * 32u) + lane;
+        if (v < m) {
+          pv = __ldcg(depth + v);
+          ps = __ldg(tptr + v);
+          pe = __ldg(tptr + v + 1);
+        }
+      }
+      while (g < gend) {
+        const int v = (int)(g * 32u) + lane;
         int s = 0, e = 0;
-        if (v < m && __ldcg(depth + v) == -1) {
-          s = __ldg(tptr + v);
-          e = __ldg(tptr + v + 1);
+        if (pv == -1) {
+          s = ps;
+          e = pe;
+        }
+        const unsigned gn = grab();
+        if (gn < gend) {
+          int vn = (int)(gn * 32u) + lane;
+          pv = -2;
+          if (vn < m) {
+            pv = __ldcg(depth + vn);
+            ps = __ldg(tptr + vn);
+            pe = __ldg(tptr + vn + 1);
+          }
         }
         bool found = false;
         unsigned U = __ballot_sync(kFull, s < e);
@@ -249,6 +306,7 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
           ++cnt;
           edg += (unsigned long long)(__ldg(ptr + v + 1) - __ldg(ptr + v));
         }
+        g = gn;
       }
       cnt = warp_sum(cnt);
       edg = warp_sum(edg);

@@ -194,14 +194,14 @@ radix_scatter(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, long
     if (idx < n) {
       unsigned pos = whist[w][dig[i]] + rank[i];
       keys_out[pos] = keys_in[idx];
-      vals_out[pos] = vals_in[idx];
+      if (vals_in) vals_out[pos] = vals_in[idx];  // keys-only sorts pass no values
     }
   }
 }
 
-// Stable sort of n (key, value) pairs on the low `bits` bits of the key.
-// Ping-pongs between (ka, va) and (kb, vb); *result_in_b tells where the
-// sorted data ended up.  Scratch: slots kSlotSortHist (+ kSlotScan).
+// Stable sort of n (key, value) pairs on the low `bits` bits of the key
+// (va == vb == nullptr sorts keys only).  Ping-pongs between (ka, va) and
+// (kb, vb); *result_in_b tells where the sorted data ended up.  Scratch: slots kSlotSortHist (+ kSlotScan).
 template <typename K, typename V>
 int device_radix_sort(apspie_context *ctx, K *ka, V *va, K *kb, V *vb, long long n, int bits,
                       bool *result_in_b) {

@@ -238,6 +238,50 @@ def spgemm(ctx: Context, A, B):
     return ptr, ind[:nnz], val[:nnz]
 
 
+def _take_csr(ctx: Context, c: Csr, with_val: bool):
+    """Copy a library-owned CSR into torch tensors on the context's device,
+    then release it."""
+    import torch
+    nnz = int(c.nnz)
+    try:
+        dev = torch.device("cuda", ctx.device)
+        ptr = torch.empty(c.m + 1, dtype=torch.int32, device=dev)
+        ind = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+        val = torch.empty(max(nnz, 1), dtype=torch.float32, device=dev) if with_val else None
+        check(lib.apspie_csr_copy_out(ctx.handle, C.byref(c), C.c_void_p(ptr.data_ptr()),
+                                      C.c_void_p(ind.data_ptr()),
+                                      C.c_void_p(val.data_ptr() if with_val else 0)),
+              ctx.handle, "apspie_csr_copy_out")
+        ctx.sync()
+    finally:
+        lib.apspie_csr_free(ctx.handle, C.byref(c))
+    return ptr, ind[:nnz], (val[:nnz] if with_val else None)
+
+
+def gen_rmat_device(ctx: Context, scale: int, edge_factor: int = 16, seed: int = 1,
+                    symmetric: bool = True, scramble: bool = True):
+    """The graph of graph.gen_rmat with the same arguments, built on the
+    device (apspie_gen_rmat_device); returns a DeviceGraph."""
+    from .graph import DeviceGraph
+    c = Csr()
+    check(lib.apspie_gen_rmat_device(ctx.handle, scale, edge_factor, seed, int(symmetric),
+                                     int(scramble), C.byref(c)), ctx.handle,
+          "apspie_gen_rmat_device")
+    ptr, ind, _ = _take_csr(ctx, c, False)
+    return DeviceGraph(1 << scale, int(ind.numel()), ptr, ind,
+                       name=f"rmat{scale}{'s' if symmetric else 'd'}", symmetric=symmetric)
+
+
+def gen_er_device(ctx: Context, n: int, mean_degree: int = 8, seed: int = 1):
+    """graph.gen_er built on the device (apspie_gen_er_device)."""
+    from .graph import DeviceGraph
+    c = Csr()
+    check(lib.apspie_gen_er_device(ctx.handle, n, mean_degree, seed, C.byref(c)), ctx.handle,
+          "apspie_gen_er_device")
+    ptr, ind, _ = _take_csr(ctx, c, False)
+    return DeviceGraph(n, int(ind.numel()), ptr, ind, name=f"er{n}", symmetric=True)
+
+
 def tc_prepare(ctx: Context, g):
     """Degree-ordered strict lower triangle of a symmetric graph:
     returns (perm, Lptr, Lind) device tensors."""

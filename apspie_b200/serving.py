@@ -7,7 +7,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._native import ServerStats, check, lib
+from ._native import ApspieError, ServerStats, check, lib
 
 BFS, SSSP, MIS = 0, 1, 2
 
@@ -33,6 +33,8 @@ class Server:
         return gid.value
 
     def submit(self, kind: int, graph: int, source: int = 0, seed: int = 0) -> int:
+        if not 0 <= graph < len(self._graphs):
+            raise ApspieError(2, f"apspie_server_submit: unknown graph {graph}")
         m = self._graphs[graph].m
         out = np.empty(m, dtype=np.int32)
         rid = C.c_uint64()

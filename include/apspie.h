@@ -364,6 +364,17 @@ int apspie_gen_rmat_host(int scale, int edge_factor, uint64_t seed,
 /* Erdos-Renyi: n*mean_degree/2 uniform vertex pairs, symmetrised, deduped. */
 int apspie_gen_er_host(int n, int mean_degree, uint64_t seed, int64_t *nnz_out,
                        int **h_ptr, int **h_ind);
+/* The same R-MAT / Erdos-Renyi graphs built on the device: samples drawn
+ * with the host builders' counter-based hash, packed (row, col) keys radix
+ * sorted, repeats and self-loops dropped, CSR offsets from row counts.  The
+ * result equals apspie_gen_*_host bit for bit; *out is library-owned
+ * (apspie_csr_copy_out / apspie_csr_free).  Scratch: 16 bytes per sample
+ * (x2 when symmetrised) of context workspace.  Synchronises once (for nnz). */
+int apspie_gen_rmat_device(apspie_ctx ctx, int scale, int edge_factor,
+                           uint64_t seed, int symmetric, int scramble,
+                           apspie_csr *out);
+int apspie_gen_er_device(apspie_ctx ctx, int n, int mean_degree, uint64_t seed,
+                         apspie_csr *out);
 /* rows x cols 2-D 5-point grid, vertex id = r*cols + c. */
 int apspie_gen_grid_host(int rows, int cols, int64_t *nnz_out, int **h_ptr,
                          int **h_ind);
