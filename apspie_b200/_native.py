@@ -72,7 +72,7 @@ PROTOS: dict[str, tuple] = {
     "apspie_bfs": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, vp, c_int]),
     "apspie_bfs_noalloc": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, vp, c_int]),
     "apspie_bfs_get_stats": (c_int, [vp, C.POINTER(BfsStats)]),
-    "apspie_bfs_get_trace": (c_int, [vp, c_int, P_int, vp, vp, vp, vp, vp, vp]),
+    "apspie_bfs_get_trace": (c_int, [vp, c_int, P_int, vp, vp, vp, vp, vp, vp, vp, vp]),
     "apspie_bfs_set_params": (c_int, [vp, c_int, c_int, c_int]),
     "apspie_sssp_u32": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, c_int]),
     "apspie_sssp_f32": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, c_int]),
@@ -107,6 +107,8 @@ PROTOS: dict[str, tuple] = {
     "apspie_gen_er_host": (c_int, [c_int, c_int, c_u64, P_i64, P_vp, P_vp]),
     "apspie_gen_rmat_device": (c_int, [vp, c_int, c_int, c_u64, c_int, c_int, C.POINTER(Csr)]),
     "apspie_gen_er_device": (c_int, [vp, c_int, c_int, c_u64, C.POINTER(Csr)]),
+    "apspie_gen_weights_u32_device": (c_int, [vp, c_int, vp, vp, c_u64, c_u32, c_u32, vp]),
+    "apspie_gen_weights_f32_device": (c_int, [vp, c_int, vp, vp, c_u64, vp]),
     "apspie_gen_grid_host": (c_int, [c_int, c_int, P_i64, P_vp, P_vp]),
     "apspie_gen_weights_u32_host": (c_int, [c_int, vp, vp, c_u64, c_u32, c_u32, vp]),
     "apspie_gen_weights_f32_host": (c_int, [c_int, vp, vp, c_u64, vp]),

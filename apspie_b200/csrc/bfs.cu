@@ -43,6 +43,8 @@ struct LevelTrace {
   unsigned long long t_end;      // %globaltimer at the end of the level (ns)
   unsigned long long queued;     // vertices queued from an implicit frontier (== nf when it ran)
   unsigned long long expanded;   // edges the push expansion walked (== mf)
+  unsigned long long t_first;    // %globaltimer when the first block finished its share
+  unsigned long long t_last;     // ... and when the last one did (the rest is barrier wait)
 };
 
 struct BfsState {
@@ -82,10 +84,10 @@ __global__ void bfs_init(int m, int src, int32_t *depth, const int *__restrict__
   if (blockIdx.x == 0) {
     seed_frontier(src, ptr, queue, chunks, &st->c[0]);
     if (threadIdx.x == 0) {
-      st->c[1] = LevelCounters{0, 0, 0, 0, 0ull};
-      st->c[2] = LevelCounters{0, 0, 0, 0, 0ull};
-      st->comp[0] = LevelCounters{0, 0, 0, 0, 0ull};
-      st->comp[1] = LevelCounters{0, 0, 0, 0, 0ull};
+      st->c[1] = LevelCounters{0ull, 0, 0, 0ull};
+      st->c[2] = LevelCounters{0ull, 0, 0, 0ull};
+      st->comp[0] = LevelCounters{0ull, 0, 0, 0ull};
+      st->comp[1] = LevelCounters{0ull, 0, 0, 0ull};
       st->bar[0] = st->bar[1] = 0;
       st->err = 0;
       st->levels = 0;
@@ -96,6 +98,8 @@ __global__ void bfs_init(int m, int src, int32_t *depth, const int *__restrict__
     for (int i = threadIdx.x; i < kTraceLevels; i += blockDim.x) {
       st->trace[i].queued = 0;
       st->trace[i].expanded = 0;
+      st->trace[i].t_first = ~0ull;
+      st->trace[i].t_last = 0;
     }
   }
 }
@@ -127,8 +131,9 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
     LevelCounters *nxt = &st->c[(L + 1) % 3];
     LevelCounters *clr = &st->c[(L + 2) % 3];
     if (threadIdx.x == 0) {
-      s_q = __ldcg(&cur->q);
-      s_chunks = __ldcg(&cur->chunks);
+      const unsigned long long qc = __ldcg(&cur->qc);
+      s_q = qc_queue(qc);
+      s_chunks = qc_chunks(qc);
       s_nbig = __ldcg(&cur->nbig);
       s_nimpl = __ldcg(&cur->nimpl);
       s_edges = __ldcg(&cur->edges);
@@ -136,8 +141,8 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
       s_bedg = 0;
       s_next = 0;
       if (blockIdx.x == 0) {
-        *clr = LevelCounters{0, 0, 0, 0, 0ull};
-        st->comp[(L + 1) & 1] = LevelCounters{0, 0, 0, 0, 0ull};
+        *clr = LevelCounters{0ull, 0, 0, 0ull};
+        st->comp[(L + 1) & 1] = LevelCounters{0ull, 0, 0, 0ull};
       }
     }
     __syncthreads();
@@ -178,6 +183,7 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
         const unsigned per_block = (ngroups + gridDim.x - 1) / gridDim.x;
         const unsigned gbeg = blockIdx.x * per_block;
         const unsigned gend = min(gbeg + per_block, ngroups);
+        DiscoverAcc acc;
         for (;;) {
           unsigned g0 = 0;
           if (lane == 0) g0 = atomicAdd(&s_next, (unsigned)kScanUnroll);
@@ -197,16 +203,18 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
             int u[1] = {v};
             unsigned fm = __ballot_sync(kFull, f[0]);
             if (fm) {
-              discover_n<1, false>(f, u, ptr, qin, cin, &st->comp[L & 1]);
+              discover_n<1, false>(f, u, ptr, qin, cin, &st->comp[L & 1], acc);
               if (lane == 0 && L < kTraceLevels)
                 atomicAdd(&st->trace[L].queued, (unsigned long long)__popc(fm));
             }
           }
         }
+        flush_acc(acc, &st->comp[L & 1]);
         if (!grid_barrier(st->bar, &st->err)) return;
         if (threadIdx.x == 0) {
-          s_q = __ldcg(&st->comp[L & 1].q);
-          s_chunks = __ldcg(&st->comp[L & 1].chunks);
+          const unsigned long long qc = __ldcg(&st->comp[L & 1].qc);
+          s_q = qc_queue(qc);
+          s_chunks = qc_chunks(qc);
         }
         __syncthreads();
         nq = s_q;
@@ -320,6 +328,14 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
         atomicAdd(&nxt->edges, s_bedg);
       }
     }
+    if (L < kTraceLevels) {
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        const unsigned long long t = globaltimer();
+        atomicMin(&st->trace[L].t_first, t);
+        atomicMax(&st->trace[L].t_last, t);
+      }
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0 && L < kTraceLevels) {
       st->trace[L].mode = pull ? 2 : 1;
       st->trace[L].nf = nf;
@@ -429,7 +445,8 @@ int apspie_bfs_set_params(apspie_ctx ctx, int alpha, int beta, int mode) {
 extern "C" int apspie_bfs_get_trace(apspie_ctx ctx, int max_levels, int *n_out,
                                     int32_t *h_mode, int64_t *h_frontier,
                                     int64_t *h_frontier_edges, int64_t *h_ns,
-                                    int64_t *h_queued, int64_t *h_expanded) {
+                                    int64_t *h_queued, int64_t *h_expanded,
+                                    int64_t *h_work_first_ns, int64_t *h_work_last_ns) {
   APSPIE_CHECK_CTX(ctx);
   if (!ctx->bfs_state || max_levels < 0 || !n_out)
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_bfs_get_trace: no BFS has run");
@@ -448,6 +465,8 @@ extern "C" int apspie_bfs_get_trace(apspie_ctx ctx, int max_levels, int *n_out,
     if (h_ns) h_ns[i] = (int64_t)(h->trace[i].t_end - prev);
     if (h_queued) h_queued[i] = (int64_t)h->trace[i].queued;
     if (h_expanded) h_expanded[i] = (int64_t)h->trace[i].expanded;
+    if (h_work_first_ns) h_work_first_ns[i] = (int64_t)(h->trace[i].t_first - prev);
+    if (h_work_last_ns) h_work_last_ns[i] = (int64_t)(h->trace[i].t_last - prev);
     prev = h->trace[i].t_end;
   }
   *n_out = n;

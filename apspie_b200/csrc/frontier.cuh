@@ -15,9 +15,13 @@
 // keeps several independent loads in flight.  A visitor provides
 //   check(payload, k, u, &aux) -> bool   (plain loads only)
 //   commit(payload, k, u, aux) -> bool   (atomics; true = u joins the next frontier)
-// discover() appends joiners (warp-aggregated) to the next queue or, for big
-// vertices, writes their chunk entries cooperatively, and accumulates the
-// next frontier's edge count.
+// discover_n() appends joiners (warp-aggregated) to the next queue or, for
+// big vertices, writes their chunk entries cooperatively.  Every warp of the
+// grid appends to the same counters, and same-address atomics serialise in
+// L2, so an append costs ONE returning atomic: queue and chunk-list lengths
+// share a 64-bit word and are reserved together, while the big-vertex count
+// and the next frontier's edge count are summed in registers and added once
+// per warp per level (flush_acc).
 #pragma once
 #include "common.cuh"
 
@@ -28,12 +32,31 @@ constexpr int kChunk = 128;   // edges per chunk (one unrolled batch of a warp)
 constexpr int kUnroll = 4;    // rounds of 32 edges issued together
 
 struct LevelCounters {
-  unsigned q;       // vertices in the queue (degree <= kBigDeg)
-  unsigned chunks;  // entries in the chunk list
-  unsigned nbig;    // vertices in the chunk list
-  unsigned nimpl;   // vertices of an implicit frontier (BFS pull: depth == level), not queued
+  unsigned long long qc;  // low 32 bits: vertices in the queue (degree <= kBigDeg);
+                          // high 32 bits: entries in the chunk list
+  unsigned nbig;          // vertices in the chunk list
+  unsigned nimpl;         // vertices of an implicit frontier (BFS pull: depth == level), not queued
   unsigned long long edges;  // sum of out-degrees of the frontier
 };
+
+__device__ __forceinline__ unsigned qc_queue(unsigned long long qc) { return (unsigned)qc; }
+__device__ __forceinline__ unsigned qc_chunks(unsigned long long qc) { return (unsigned)(qc >> 32); }
+
+// Per-lane tallies of a warp's appends during one level, flushed once.
+struct DiscoverAcc {
+  unsigned nbig = 0;
+  unsigned long long edges = 0;
+};
+
+__device__ __forceinline__ void flush_acc(DiscoverAcc &acc, LevelCounters *nxt) {
+  const unsigned b = warp_sum(acc.nbig);
+  const unsigned long long e = warp_sum(acc.edges);
+  if (lane_id() == 0) {
+    if (b) atomicAdd(&nxt->nbig, b);
+    if (e) atomicAdd(&nxt->edges, e);
+  }
+  acc = DiscoverAcc{};
+}
 
 // Capacity of a chunk list for a graph with nnz edges: every big vertex has
 // more than kBigDeg edges, so there are fewer than nnz / kBigDeg of them.
@@ -42,12 +65,13 @@ inline size_t chunk_capacity(long long nnz) {
 }
 
 // Called by all 32 lanes with N candidates per lane; candidate r of a lane
-// joins the next frontier when found[r].  One queue append, one chunk
-// reservation and one edge-count update per warp for all N x 32 candidates.
+// joins the next frontier when found[r].  One atomic per warp reserves the
+// queue slots and chunk entries of all N x 32 candidates; the big-vertex and
+// edge tallies go to acc (kCountEdges = false leaves the edge tally alone).
 template <int N, bool kCountEdges = true>
 __device__ __forceinline__ void discover_n(const bool (&found)[N], const int (&u)[N],
                                            const int *__restrict__ ptr, int *qout, int2 *cout,
-                                           LevelCounters *nxt) {
+                                           LevelCounters *nxt, DiscoverAcc &acc) {
   const int lane = lane_id();
   int deg[N];
 #pragma unroll
@@ -62,29 +86,26 @@ __device__ __forceinline__ void discover_n(const bool (&found)[N], const int (&u
     nchunk += big ? (deg[r] + kChunk - 1) / kChunk : 0;
     edges += (unsigned long long)deg[r];
   }
+  acc.nbig += (unsigned)nbig;
+  if (kCountEdges) acc.edges += edges;
+  const int qincl = warp_incl_scan(nsmall);
+  const int cincl = warp_incl_scan(nchunk);
+  const unsigned qtot = (unsigned)__shfl_sync(kFull, qincl, 31);
+  const unsigned ctot = (unsigned)__shfl_sync(kFull, cincl, 31);
+  if ((qtot | ctot) == 0u) return;
+  unsigned long long base = 0;
+  if (lane == 31) base = atomicAdd(&nxt->qc, ((unsigned long long)ctot << 32) | qtot);
+  base = __shfl_sync(kFull, base, 31);
   // queue slots
-  int qincl = warp_incl_scan(nsmall);
-  int qtot = __shfl_sync(kFull, qincl, 31);
   if (qtot) {
-    unsigned qbase = 0;
-    if (lane == 31) qbase = atomicAdd(&nxt->q, (unsigned)qtot);
-    qbase = __shfl_sync(kFull, qbase, 31) + (unsigned)(qincl - nsmall);
+    unsigned qbase = qc_queue(base) + (unsigned)(qincl - nsmall);
 #pragma unroll
     for (int r = 0; r < N; ++r)
       if (found[r] && deg[r] <= kBigDeg) qout[qbase++] = u[r];
   }
   // chunk entries of big vertices, written cooperatively
-  unsigned bmask = __ballot_sync(kFull, nbig > 0);
-  if (bmask) {
-    int cincl = warp_incl_scan(nchunk);
-    int ctot = __shfl_sync(kFull, cincl, 31);
-    int btot = warp_sum(nbig);
-    unsigned cbase = 0;
-    if (lane == 0) {
-      cbase = atomicAdd(&nxt->chunks, (unsigned)ctot);
-      atomicAdd(&nxt->nbig, (unsigned)btot);
-    }
-    cbase = __shfl_sync(kFull, cbase, 0) + (unsigned)(cincl - nchunk);
+  if (ctot) {
+    unsigned cbase = qc_chunks(base) + (unsigned)(cincl - nchunk);
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       bool big = found[r] && deg[r] > kBigDeg;
@@ -101,17 +122,6 @@ __device__ __forceinline__ void discover_n(const bool (&found)[N], const int (&u
       cbase += (unsigned)nch;
     }
   }
-  if (kCountEdges) {
-    edges = warp_sum(edges);
-    if (lane == 0 && edges) atomicAdd(&nxt->edges, edges);
-  }
-}
-
-__device__ __forceinline__ void discover(bool found, int u, const int *__restrict__ ptr,
-                                         int *qout, int2 *cout, LevelCounters *nxt) {
-  bool f[1] = {found};
-  int uu[1] = {u};
-  discover_n<1>(f, uu, ptr, qout, cout, nxt);
 }
 
 // Seeds a frontier of one vertex (used by the init kernels; block-wide).
@@ -121,13 +131,13 @@ __device__ __forceinline__ void seed_frontier(int src, const int *__restrict__ p
   int nch = deg > kBigDeg ? (deg + kChunk - 1) / kChunk : 0;
   for (int j = threadIdx.x; j < nch; j += blockDim.x) chunks[j] = make_int2(src, j);
   if (threadIdx.x == 0) {
-    *c = LevelCounters{0, 0, 0, 0, 0ull};
+    *c = LevelCounters{0ull, 0, 0, 0ull};
     if (nch) {
-      c->chunks = (unsigned)nch;
+      c->qc = (unsigned long long)nch << 32;
       c->nbig = 1;
     } else {
       queue[0] = src;
-      c->q = 1;
+      c->qc = 1ull;
     }
     c->edges = (unsigned long long)deg;
   }
@@ -144,6 +154,7 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
                                             unsigned long long *walked = nullptr) {
   const int lane = lane_id();
   unsigned long long nwalk = 0;
+  DiscoverAcc acc;
   for (unsigned base = (unsigned)gwarp * 32u; base < nq; base += (unsigned)nwarps * 32u) {
     unsigned idx = base + lane;
     int v = idx < nq ? __ldcg(qin + idx) : -1;
@@ -179,7 +190,7 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
       bool f[kUnroll];
 #pragma unroll
       for (int r = 0; r < kUnroll; ++r) f[r] = ok[r] && visit.commit(pp[r], kk[r], uu[r], aux[r]);
-      discover_n<kUnroll>(f, uu, ptr, qout, cout, nxt);
+      discover_n<kUnroll>(f, uu, ptr, qout, cout, nxt, acc);
     }
   }
   for (unsigned c = (unsigned)gwarp; c < nch; c += (unsigned)nwarps) {
@@ -204,9 +215,10 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
 #pragma unroll
       for (int r = 0; r < kUnroll; ++r)
         f[r] = ok[r] && visit.commit(pay, k0 + r * 32 + lane, uu[r], aux[r]);
-      discover_n<kUnroll>(f, uu, ptr, qout, cout, nxt);
+      discover_n<kUnroll>(f, uu, ptr, qout, cout, nxt, acc);
     }
   }
+  flush_acc(acc, nxt);
   if (walked && lane == 0 && nwalk) atomicAdd(walked, nwalk);
 }
 

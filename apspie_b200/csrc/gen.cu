@@ -90,6 +90,25 @@ __global__ void keys_to_csr(const unsigned long long *k, long long n, int bits, 
   }
 }
 
+// edge weights as functions of (row, col, seed): one warp per row
+__global__ void weights_u32_kernel(int m, const int *ptr, const int *ind, uint64_t seed,
+                                   uint32_t lo, uint32_t hi, uint32_t *w) {
+  const int lane = threadIdx.x & 31;
+  for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < m;
+       u += (gridDim.x * blockDim.x) >> 5)
+    for (int k = ptr[u] + lane; k < ptr[u + 1]; k += 32)
+      w[k] = weight_u32(seed, (uint32_t)u, (uint32_t)ind[k], lo, hi);
+}
+
+__global__ void weights_f32_kernel(int m, const int *ptr, const int *ind, uint64_t seed,
+                                   float *w) {
+  const int lane = threadIdx.x & 31;
+  for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < m;
+       u += (gridDim.x * blockDim.x) >> 5)
+    for (int k = ptr[u] + lane; k < ptr[u + 1]; k += 32)
+      w[k] = weight_f32(seed, (uint32_t)u, (uint32_t)ind[k]);
+}
+
 __global__ void fill_int(int n, int v, int *p) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
 }
@@ -189,6 +208,28 @@ int apspie_gen_er_device(apspie_ctx ctx, int n, int mean_degree, uint64_t seed, 
   int rc = check_launch(ctx, "er_keys");
   if (rc) return rc;
   return keys_to_graph(ctx, ka, kb, nk, bits, n, out);
+}
+
+int apspie_gen_weights_u32_device(apspie_ctx ctx, int m, const int *d_ptr, const int *d_ind,
+                                  uint64_t seed, uint32_t lo, uint32_t hi, uint32_t *d_w) {
+  APSPIE_CHECK_CTX(ctx);
+  if (m < 0 || !d_ptr || !d_w || hi < lo)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_gen_weights_u32_device: bad arguments");
+  if (m == 0) return APSPIE_OK;
+  weights_u32_kernel<<<gg(ctx, (long long)m * 32), 256, 0, ctx->stream>>>(m, d_ptr, d_ind, seed, lo,
+                                                                         hi, d_w);
+  return check_launch(ctx, "weights_u32_kernel");
+}
+
+int apspie_gen_weights_f32_device(apspie_ctx ctx, int m, const int *d_ptr, const int *d_ind,
+                                  uint64_t seed, float *d_w) {
+  APSPIE_CHECK_CTX(ctx);
+  if (m < 0 || !d_ptr || !d_w)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_gen_weights_f32_device: bad arguments");
+  if (m == 0) return APSPIE_OK;
+  weights_f32_kernel<<<gg(ctx, (long long)m * 32), 256, 0, ctx->stream>>>(m, d_ptr, d_ind, seed,
+                                                                         d_w);
+  return check_launch(ctx, "weights_f32_kernel");
 }
 
 }  // extern "C"

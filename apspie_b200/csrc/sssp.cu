@@ -87,8 +87,8 @@ __global__ void sssp_init(int m, int src, unsigned *dist, int *stamp, const int 
   if (blockIdx.x == 0) {
     seed_frontier(src, ptr, queue, chunks, &st->c[0]);
     if (threadIdx.x == 0) {
-      st->c[1] = LevelCounters{0, 0, 0, 0, 0ull};
-      st->c[2] = LevelCounters{0, 0, 0, 0, 0ull};
+      st->c[1] = LevelCounters{0ull, 0, 0, 0ull};
+      st->c[2] = LevelCounters{0ull, 0, 0, 0ull};
       st->bar[0] = st->bar[1] = 0;
       st->err = 0;
       st->rounds = 0;
@@ -115,10 +115,11 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
     LevelCounters *nxt = &st->c[(r + 1) % 3];
     LevelCounters *clr = &st->c[(r + 2) % 3];
     if (threadIdx.x == 0) {
-      s_q = __ldcg(&cur->q);
-      s_chunks = __ldcg(&cur->chunks);
+      const unsigned long long qc = __ldcg(&cur->qc);
+      s_q = qc_queue(qc);
+      s_chunks = qc_chunks(qc);
       s_edges = __ldcg(&cur->edges);
-      if (blockIdx.x == 0) *clr = LevelCounters{0, 0, 0, 0, 0ull};
+      if (blockIdx.x == 0) *clr = LevelCounters{0ull, 0, 0, 0ull};
     }
     __syncthreads();
     const unsigned nq = s_q, nch = s_chunks;

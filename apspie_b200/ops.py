@@ -94,15 +94,18 @@ def bfs_trace(ctx: Context, max_levels: int = 64) -> list[dict]:
     ns = np.zeros(max_levels, np.int64)
     qd = np.zeros(max_levels, np.int64)
     ex = np.zeros(max_levels, np.int64)
+    wf = np.zeros(max_levels, np.int64)
+    wl = np.zeros(max_levels, np.int64)
     cnt = C.c_int()
     check(lib.apspie_bfs_get_trace(ctx.handle, max_levels, C.byref(cnt), mode.ctypes.data,
                                    nf.ctypes.data, mf.ctypes.data, ns.ctypes.data,
-                                   qd.ctypes.data, ex.ctypes.data), ctx.handle,
-          "apspie_bfs_get_trace")
+                                   qd.ctypes.data, ex.ctypes.data, wf.ctypes.data,
+                                   wl.ctypes.data), ctx.handle, "apspie_bfs_get_trace")
     n = cnt.value
     return [{"level": i, "dir": "pull" if mode[i] == 2 else "push", "frontier": int(nf[i]),
              "frontier_edges": int(mf[i]), "us": ns[i] / 1e3, "queued": int(qd[i]),
-             "expanded": int(ex[i])} for i in range(n)]
+             "expanded": int(ex[i]), "work_first_us": wf[i] / 1e3, "work_last_us": wl[i] / 1e3}
+            for i in range(n)]
 
 
 def bfs_stats(ctx: Context) -> dict:
@@ -280,6 +283,20 @@ def gen_er_device(ctx: Context, n: int, mean_degree: int = 8, seed: int = 1):
           "apspie_gen_er_device")
     ptr, ind, _ = _take_csr(ctx, c, False)
     return DeviceGraph(n, int(ind.numel()), ptr, ind, name=f"er{n}", symmetric=True)
+
+
+def weights_device(ctx: Context, g, seed: int = 7, lo: int = 1, hi: int = 255):
+    """graph.weights_u32 / weights_f32 computed on the device for a
+    DeviceGraph: sets g.w_u32 (uint32 bits in an int32 tensor) and g.w_f32."""
+    import torch
+    w = torch.empty(max(g.nnz, 1), dtype=torch.int32, device=g.ptr.device)
+    wf = torch.empty(max(g.nnz, 1), dtype=torch.float32, device=g.ptr.device)
+    check(lib.apspie_gen_weights_u32_device(ctx.handle, int(g.m), _p(g.ptr), _p(g.ind), seed, lo,
+                                            hi, _p(w)), ctx.handle, "weights_u32_device")
+    check(lib.apspie_gen_weights_f32_device(ctx.handle, int(g.m), _p(g.ptr), _p(g.ind), seed,
+                                            _p(wf)), ctx.handle, "weights_f32_device")
+    g.w_u32, g.w_f32 = w[:g.nnz], wf[:g.nnz]
+    return g
 
 
 def tc_prepare(ctx: Context, g):

@@ -452,8 +452,11 @@ def run_ours(args):
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "per_step_ms": {"min": min(per), "median": statistics.median(per), "max": max(per)},
-        "level_trace": [[t["dir"], t["frontier"], t["frontier_edges"], round(t["us"], 1)]
+        "level_trace": [[t["dir"], t["frontier"], t["frontier_edges"], round(t["us"], 1),
+                         round(t["work_first_us"], 1), round(t["work_last_us"], 1)]
                         for t in trace],
+        "level_trace_columns": ["dir", "frontier", "frontier_edges", "us", "first_block_done_us",
+                                "last_block_done_us"],
     }
     line.update(extras)
     print(json.dumps(line), flush=True)

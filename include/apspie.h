@@ -88,12 +88,15 @@ int apspie_bfs_get_stats(apspie_ctx ctx, apspie_bfs_stats *out);
  * i < max_levels (at most 64) the direction (1 push, 2 pull), frontier size,
  * frontier out-edges, device time in ns, and two self-checks: vertices
  * queued from an implicit (pull-produced) frontier before a push level, and
- * edges the push expansion walked (== frontier out-edges).  *n_out = levels
+ * edges the push expansion walked (== frontier out-edges); and the ns from
+ * the level's start until the first and the last block finished its share of
+ * the level (the remainder of h_ns is the grid barrier).  *n_out = levels
  * written.  The array outputs may be NULL. */
 int apspie_bfs_get_trace(apspie_ctx ctx, int max_levels, int *n_out,
                          int32_t *h_mode, int64_t *h_frontier,
                          int64_t *h_frontier_edges, int64_t *h_ns,
-                         int64_t *h_queued, int64_t *h_expanded);
+                         int64_t *h_queued, int64_t *h_expanded,
+                         int64_t *h_work_first_ns, int64_t *h_work_last_ns);
 
 /* BFS that allocates no memory: apspie_bfs's traversal (same arguments and
  * result, push/pull chosen automatically, or push only when d_tptr is NULL)
@@ -375,6 +378,12 @@ int apspie_gen_rmat_device(apspie_ctx ctx, int scale, int edge_factor,
                            apspie_csr *out);
 int apspie_gen_er_device(apspie_ctx ctx, int n, int mean_degree, uint64_t seed,
                          apspie_csr *out);
+/* apspie_gen_weights_*_host on device arrays (same values). */
+int apspie_gen_weights_u32_device(apspie_ctx ctx, int m, const int *d_ptr,
+                                  const int *d_ind, uint64_t seed, uint32_t lo,
+                                  uint32_t hi, uint32_t *d_w);
+int apspie_gen_weights_f32_device(apspie_ctx ctx, int m, const int *d_ptr,
+                                  const int *d_ind, uint64_t seed, float *d_w);
 /* rows x cols 2-D 5-point grid, vertex id = r*cols + c. */
 int apspie_gen_grid_host(int rows, int cols, int64_t *nnz_out, int **h_ptr,
                          int **h_ind);

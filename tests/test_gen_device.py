@@ -43,3 +43,13 @@ def test_rmat22_device_properties(ctx):
     assert bool((key[1:] > key[:-1]).all())
     tkey = ind * d.m + rows
     assert int((key * 2654435761 % (1 << 61)).sum()) == int((tkey * 2654435761 % (1 << 61)).sum())
+
+
+@pytest.mark.gpu
+def test_weights_device_match_host(ctx):
+    h = ap.gen_rmat(12, 16, seed=3)
+    wu = ap.weights_u32(h, seed=9)
+    wf = ap.weights_f32(h, seed=9)
+    d = ap.weights_device(ctx, h.to_device(), seed=9)
+    np.testing.assert_array_equal(d.w_u32.cpu().numpy().view(np.uint32), wu)
+    np.testing.assert_array_equal(d.w_f32.cpu().numpy(), wf)
