@@ -32,7 +32,7 @@ class BfsStats(C.Structure):
 
 
 class SsspStats(C.Structure):
-    _fields_ = [("rounds", C.c_int32), ("pad", C.c_int32), ("vertices_reached", C.c_int64),
+    _fields_ = [("rounds", C.c_int32), ("phases", C.c_int32), ("vertices_reached", C.c_int64),
                 ("edges_traversed", C.c_int64), ("relaxations", C.c_int64)]
 
 
@@ -76,6 +76,7 @@ PROTOS: dict[str, tuple] = {
     "apspie_bfs_set_params": (c_int, [vp, c_int, c_int, c_int]),
     "apspie_sssp_u32": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, c_int]),
     "apspie_sssp_f32": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, c_int]),
+    "apspie_sssp_set_params": (c_int, [vp, c_u32, c_f32]),
     "apspie_sssp_get_stats": (c_int, [vp, C.POINTER(SsspStats)]),
     "apspie_mis": (c_int, [vp, c_i64, c_int, vp, vp, vp, vp, c_f32]),
     "apspie_mis_get_rounds": (c_int, [vp, P_int]),
@@ -98,6 +99,9 @@ PROTOS: dict[str, tuple] = {
     "apspie_server_create": (c_int, [c_int, C.c_size_t, c_int, P_vp]),
     "apspie_server_add_graph": (c_int, [vp, c_int, c_i64, vp, vp, vp, vp, vp, c_int, P_int]),
     "apspie_server_submit": (c_int, [vp, c_int, c_int, c_int, c_u32, vp, P_u64]),
+    "apspie_server_submit_device": (c_int, [vp, c_int, c_int, c_int, c_u32, vp, P_u64]),
+    "apspie_server_replay": (c_int, [vp, c_int, vp, vp, C.POINTER(C.c_double)]),
+    "apspie_server_replay_plain": (c_int, [vp, c_int, vp, vp, C.POINTER(C.c_double)]),
     "apspie_server_poll": (c_int, [vp, c_u64, P_int, C.POINTER(C.c_double)]),
     "apspie_server_wait": (c_int, [vp, c_u64, C.POINTER(C.c_double)]),
     "apspie_server_get_stats": (c_int, [vp, C.POINTER(ServerStats)]),

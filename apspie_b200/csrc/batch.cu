@@ -5,13 +5,20 @@
 //     carries 64-bit masks (visited, and the frontier of three consecutive
 //     levels), bit s standing for source s -- the "frontier matrix" of
 //     MS-BFS; or
-//   * a batched uint32 SSSP over up to 64 sources of one graph: frontier
-//     items are (source, vertex) pairs, relaxed with atomicMin on
-//     dist[source][vertex].
+//   * a multi-source uint32 SSSP over up to 32 sources of one graph: the
+//     distances are vertex-major, dist[v][0..sw) one row of sw = 1, 2, 4, 8,
+//     16 or 32 words (the sources rounded up to a power of two), and every
+//     vertex carries a mask of the sources whose distance at it dropped in
+//     the last round.  A warp relaxes 32 / sw edges (v -> u, w) at a time, sw
+//     lanes per edge, one per source (lane s: atomicMin(dist[u][s],
+//     dist[v][s] + w) when s is active at v), so an edge is read once per
+//     round for all sources and a row is one coalesced access; the improved
+//     lanes' bits are OR-ed into u's next mask, and the edge whose OR found
+//     the mask empty appends u to the next frontier.
 // Each super-step advances every unfinished job by one level / round.  The
-// work of a super-step is cut into units (32 frontier vertices, one 128-edge
-// chunk of a hub, 32 vertices of a pull sweep, 32 stale frontier words to
-// clear) and the units of all jobs are dealt round-robin over the warps of
+// work of a super-step is cut into units (BFS: 32 frontier vertices or one
+// 128-edge chunk of a hub; SSSP: 4 frontier vertices or one 64-edge chunk;
+// 32 vertices of a pull sweep; 32 stale frontier words to clear) and the units of all jobs are dealt round-robin over the warps of
 // the grid, so a large graph and a small one share the GPU in the same
 // launch.  Super-steps are separated by the bounded grid barrier; per-job
 // direction switches (push / pull, Beamer's rule with per-job thresholds from
@@ -21,7 +28,7 @@
 // Per source, the results are exactly those of the single-source kernels:
 // BFS levels are set once per (source, vertex) by the thread whose atomicOr
 // on the visited mask first sets the bit; SSSP converges to the same
-// min-plus fixpoint.
+// min-plus fixpoint (the fixpoint is unique, whatever the relaxation order).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -38,9 +45,18 @@ namespace {
 constexpr int kBatchThreads = 512;
 constexpr int kMaxJobs = 64;
 constexpr int kJobBfs = 0, kJobSssp = 1;
+constexpr int kMsbfsWidth = 64;   // sources per BFS device job (one 64-bit mask)
+constexpr int kMssspWidth = 32;   // most sources per SSSP device job (one lane each)
+// SSSP jobs relax a whole distance row per edge, so their units are smaller:
+// 4 queued vertices of degree <= kSsspBigDeg, or kSsspChunk edges of a hub
+constexpr int kSsspBigDeg = 32;
+constexpr int kSsspChunk = 64;
+constexpr int kSsspPerUnit = 4;
+constexpr int kSsspSlots = 4;     // rounds of 32 / sw edges a warp relaxes together
 
 struct JobCounters {
-  unsigned q, chunks, nbig, pad;
+  unsigned long long qc;  // queue length (low 32 bits) | chunk-list length (high 32 bits)
+  unsigned nbig, pad;
   unsigned long long edges;
 };
 
@@ -51,16 +67,17 @@ struct BatchJob {
   const int *ptr, *ind, *tptr, *tind;
   const uint32_t *w;
   const int *src;
-  int32_t *out;  // BFS: vertex-major depth [m][64]; SSSP: dist [nsrc][m]
+  int32_t *out;  // vertex-major results: BFS depth [m][64]; SSSP distance [m][32]
   unsigned long long *visited, *F0, *F1, *F2;
   int *q0, *q1, *q2;
   int2 *c0, *c1, *c2;
-  int *stamp;
+  int big_deg, chunk;  // degree above which a vertex is chunked, edges per chunk
+  int sw, pad1;        // SSSP: distance row width (power of two >= nsrc)
   JobCounters c[3];
 };
 
 struct BatchState {
-  unsigned bar[2];
+  alignas(8) unsigned bar[2];  // grid-barrier arrival counter (64-bit)
   int err;
   int steps;
   unsigned long long edges;  // sum over jobs of frontier edges walked
@@ -81,6 +98,30 @@ __device__ __forceinline__ unsigned long long srcmask(int nsrc) {
 }
 
 // ------------------------------------------------------------------ init ---
+// Queues the distinct sources of job j as its level-0 frontier (one thread).
+__device__ void seed_queue(BatchJob *j) {
+  for (int i = 0; i < 3; ++i) j->c[i] = JobCounters{0ull, 0, 0, 0ull};
+  unsigned q = 0, nch_total = 0;
+  for (int s = 0; s < j->nsrc; ++s) {
+    int v = j->src[s];
+    bool first = true;
+    for (int t = 0; t < s; ++t)
+      if (j->src[t] == v) first = false;
+    if (!first) continue;
+    int deg = __ldg(j->ptr + v + 1) - __ldg(j->ptr + v);
+    if (deg > j->big_deg) {
+      int nch = (deg + j->chunk - 1) / j->chunk;
+      for (int c = 0; c < nch; ++c) j->c0[nch_total + c] = make_int2(v, c);
+      nch_total += (unsigned)nch;
+      j->c[0].nbig += 1;
+    } else {
+      j->q0[q++] = v;
+    }
+    j->c[0].edges += (unsigned long long)deg;
+  }
+  j->c[0].qc = ((unsigned long long)nch_total << 32) | q;
+}
+
 __global__ void batch_init_bfs(BatchJob *jobs, int jid) {
   BatchJob *j = jobs + jid;
   const int m = j->m;
@@ -108,116 +149,96 @@ __global__ void batch_seed_bfs(BatchJob *jobs, int jid) {
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int i = 0; i < 3; ++i) j->c[i] = JobCounters{0, 0, 0, 0, 0ull};
-    // queue the distinct sources (those whose frontier word was set first here)
-    for (int s = 0; s < j->nsrc; ++s) {
-      int v = j->src[s];
-      bool first = true;
-      for (int t = 0; t < s; ++t)
-        if (j->src[t] == v) first = false;
-      if (!first) continue;
-      int deg = __ldg(j->ptr + v + 1) - __ldg(j->ptr + v);
-      if (deg > kBigDeg) {
-        int nch = (deg + kChunk - 1) / kChunk;
-        for (int c = 0; c < nch; ++c) j->c0[j->c[0].chunks + c] = make_int2(v, c);
-        j->c[0].chunks += (unsigned)nch;
-        j->c[0].nbig += 1;
-      } else {
-        j->q0[j->c[0].q++] = v;
-      }
-      j->c[0].edges += (unsigned long long)deg;
-    }
+    seed_queue(j);
   }
 }
 
 __global__ void batch_init_sssp(BatchJob *jobs, int jid) {
   BatchJob *j = jobs + jid;
-  const size_t n = (size_t)j->m * j->nsrc;
+  const size_t n = (size_t)j->m * j->sw;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
+       i += (size_t)gridDim.x * blockDim.x)
     j->out[i] = -1;  // 0xFFFFFFFF: unreached
-    j->stamp[i] = -1;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < j->m; v += gridDim.x * blockDim.x) {
+    j->F0[v] = 0ull;
+    j->F1[v] = 0ull;
+    j->F2[v] = 0ull;
   }
 }
 
 __global__ void batch_seed_sssp(BatchJob *jobs, int jid) {
   BatchJob *j = jobs + jid;
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  for (int i = 0; i < 3; ++i) j->c[i] = JobCounters{0, 0, 0, 0, 0ull};
-  for (int s = 0; s < j->nsrc; ++s) {
+  if (blockIdx.x != 0) return;
+  for (int s = threadIdx.x; s < j->nsrc; s += blockDim.x) {
     int v = j->src[s];
-    int item = s * j->m + v;
-    j->out[item] = 0;
-    int deg = __ldg(j->ptr + v + 1) - __ldg(j->ptr + v);
-    if (deg > kBigDeg) {
-      int nch = (deg + kChunk - 1) / kChunk;
-      for (int c = 0; c < nch; ++c) j->c0[j->c[0].chunks + c] = make_int2(item, c);
-      j->c[0].chunks += (unsigned)nch;
-      j->c[0].nbig += 1;
-    } else {
-      j->q0[j->c[0].q++] = item;
-    }
-    j->c[0].edges += (unsigned long long)deg;
+    j->out[(size_t)v * j->sw + s] = 0;
+    atomicOr(j->F0 + v, 1ull << s);
   }
+  __syncthreads();
+  if (threadIdx.x == 0) seed_queue(j);
 }
 
 // --------------------------------------------------------- append helper ---
-// Appends up to N candidates per lane (an item id u with degree deg, or
-// nothing) to the job's next queue / chunk list.  Warp-collective.
+// Appends up to N candidates per lane (an id u with degree deg, or nothing)
+// to the job's next queue / chunk list: one packed atomic per warp reserves
+// the queue slots and chunk entries, chunk entries are written 32 at a time.
+// Warp-collective.
 template <int N>
-__device__ __forceinline__ void append_n(const bool (&found)[N], const int (&u)[N],
-                                         const int (&deg)[N], int *qout, int2 *cout,
-                                         JobCounters *nxt) {
+__device__ __forceinline__ void append_n(const BatchJob *j, const bool (&found)[N],
+                                         const int (&u)[N], const int (&deg)[N], int *qout,
+                                         int2 *cout, JobCounters *nxt) {
   const int lane = lane_id();
+  const int bd = j->big_deg, ck = j->chunk;
   int nsmall = 0, nbig = 0, nchunk = 0;
   unsigned long long edges = 0;
 #pragma unroll
   for (int r = 0; r < N; ++r) {
-    bool big = found[r] && deg[r] > kBigDeg;
+    bool big = found[r] && deg[r] > bd;
     nsmall += (found[r] && !big) ? 1 : 0;
     nbig += big ? 1 : 0;
-    nchunk += big ? (deg[r] + kChunk - 1) / kChunk : 0;
+    nchunk += big ? (deg[r] + ck - 1) / ck : 0;
     edges += found[r] ? (unsigned long long)deg[r] : 0ull;
   }
-  int qincl = warp_incl_scan(nsmall);
-  int qtot = __shfl_sync(kFull, qincl, 31);
+  const int qincl = warp_incl_scan(nsmall);
+  const int cincl = warp_incl_scan(nchunk);
+  const unsigned qtot = (unsigned)__shfl_sync(kFull, qincl, 31);
+  const unsigned ctot = (unsigned)__shfl_sync(kFull, cincl, 31);
+  if ((qtot | ctot) == 0u) return;
+  unsigned long long base = 0;
+  if (lane == 31) base = atomicAdd(&nxt->qc, ((unsigned long long)ctot << 32) | qtot);
+  base = __shfl_sync(kFull, base, 31);
   if (qtot) {
-    unsigned qbase = 0;
-    if (lane == 31) qbase = atomicAdd(&nxt->q, (unsigned)qtot);
-    qbase = __shfl_sync(kFull, qbase, 31) + (unsigned)(qincl - nsmall);
+    unsigned qb = (unsigned)base + (unsigned)(qincl - nsmall);
 #pragma unroll
     for (int r = 0; r < N; ++r)
-      if (found[r] && deg[r] <= kBigDeg) qout[qbase++] = u[r];
+      if (found[r] && deg[r] <= bd) qout[qb++] = u[r];
   }
-  unsigned bmask = __ballot_sync(kFull, nbig > 0);
-  if (bmask) {
-    int cincl = warp_incl_scan(nchunk);
-    int ctot = __shfl_sync(kFull, cincl, 31);
-    int btot = warp_sum(nbig);
-    unsigned cbase = 0;
-    if (lane == 0) {
-      cbase = atomicAdd(&nxt->chunks, (unsigned)ctot);
-      atomicAdd(&nxt->nbig, (unsigned)btot);
-    }
-    cbase = __shfl_sync(kFull, cbase, 0) + (unsigned)(cincl - nchunk);
+  if (ctot) {
+    unsigned cb = (unsigned)(base >> 32);
 #pragma unroll
     for (int r = 0; r < N; ++r) {
-      bool big = found[r] && deg[r] > kBigDeg;
-      int nch = big ? (deg[r] + kChunk - 1) / kChunk : 0;
-      unsigned rm = __ballot_sync(kFull, big);
-      while (rm) {
-        int jl = __ffs(rm) - 1;
-        rm &= rm - 1;
-        int uj = __shfl_sync(kFull, u[r], jl);
-        unsigned bj = __shfl_sync(kFull, cbase, jl);
-        int nj = __shfl_sync(kFull, nch, jl);
-        for (int c = lane; c < nj; c += 32) cout[bj + c] = make_int2(uj, c);
+      const bool big = found[r] && deg[r] > bd;
+      if (__ballot_sync(kFull, big) == 0u) continue;
+      const int nch = big ? (deg[r] + ck - 1) / ck : 0;
+      const int incl = warp_incl_scan(nch);
+      const int tot = __shfl_sync(kFull, incl, 31);
+      const int excl = incl - nch;
+      for (int c0 = 0; c0 < tot; c0 += 32) {
+        const int e = c0 + lane;
+        const int owner = warp_owner(excl, min(e, tot - 1));
+        const int uj = __shfl_sync(kFull, u[r], owner);
+        const int ej = __shfl_sync(kFull, excl, owner);
+        if (e < tot) cout[cb + (unsigned)e] = make_int2(uj, e - ej);
       }
-      cbase += (unsigned)nch;
+      cb += (unsigned)tot;
     }
   }
+  const unsigned b = warp_sum((unsigned)nbig);
   edges = warp_sum(edges);
-  if (lane == 0 && edges) atomicAdd(&nxt->edges, edges);
+  if (lane == 0) {
+    if (b) atomicAdd(&nxt->nbig, b);
+    if (edges) atomicAdd(&nxt->edges, edges);
+  }
 }
 
 // ------------------------------------------------------------ MS-BFS ---
@@ -268,7 +289,7 @@ __device__ void msbfs_push_queue(BatchJob *j, int L, int unit, unsigned nq) {
       found[0] = msbfs_relax(j, fo, u[0], L + 1, Fn);
       if (found[0]) dg[0] = __ldg(j->ptr + u[0] + 1) - __ldg(j->ptr + u[0]);
     }
-    append_n<1>(found, u, dg, qout, cout, nxt);
+    append_n<1>(j, found, u, dg, qout, cout, nxt);
   }
 }
 
@@ -291,7 +312,7 @@ __device__ void msbfs_push_chunk(BatchJob *j, int L, int unit) {
       found[0] = msbfs_relax(j, f, u[0], L + 1, Fn);
       if (found[0]) dg[0] = __ldg(j->ptr + u[0] + 1) - __ldg(j->ptr + u[0]);
     }
-    append_n<1>(found, u, dg, qout, cout, nxt);
+    append_n<1>(j, found, u, dg, qout, cout, nxt);
   }
 }
 
@@ -354,7 +375,7 @@ __device__ void msbfs_pull(BatchJob *j, int L, int unit, unsigned long long *s_a
     for (unsigned long long b = nb; b; b &= b - 1) row[__ffsll((long long)b) - 1] = L + 1;
     dg[0] = __ldg(j->ptr + v + 1) - __ldg(j->ptr + v);
   }
-  append_n<1>(found, u, dg, qout, cout, nxt);
+  append_n<1>(j, found, u, dg, qout, cout, nxt);
   __syncwarp();
 }
 
@@ -374,85 +395,126 @@ __device__ void msbfs_clear(BatchJob *j, int L, int unit, unsigned prevq, bool c
   }
 }
 
-// ------------------------------------------------------------ SSSP lanes ---
-__device__ __forceinline__ bool sssp_relax(BatchJob *j, int item_base, unsigned du, int k, int u,
-                                           int round) {
-  unsigned nd = du + __ldg(j->w + k);
-  if (nd < du || nd == 0xffffffffu) nd = 0xfffffffeu;
-  unsigned *dist = (unsigned *)j->out;
-  int it = item_base + u;
-  if (nd >= __ldcg(dist + it)) return false;
-  if (nd >= atomicMin(dist + it, nd)) return false;
-  return atomicExch(j->stamp + it, round) != round;
+// ---------------------------------------------------- multi-source SSSP ---
+__device__ __forceinline__ unsigned sat_add(unsigned d, unsigned w) {
+  unsigned t = d + w;
+  return (t < d || t == 0xffffffffu) ? 0xfffffffeu : t;  // saturate below "unreached"
 }
 
-__device__ void sssp_queue(BatchJob *j, int L, int unit, unsigned nq) {
+// Edges per batch of a job with row width sw: kSsspSlots rounds of 32 / sw
+// edges, at most 32 (one per loading lane).
+__device__ __forceinline__ int mssp_batch(int sw) { return min(32, kSsspSlots * (32 / sw)); }
+
+// Relaxes the batch of edges held by lanes 0..nb-1 (ue: target, we: weight,
+// ve: tail, me: the tail's active-source mask; me == 0 for no edge), for every
+// active source.  Lane l of a round works on edge (round * 32/sw + l / sw)
+// and source l % sw.  Returns, on the loading lanes, whether that edge's
+// target entered the next frontier.
+__device__ __forceinline__ bool mssp_relax(BatchJob *j, int ue, unsigned we, int ve, unsigned me,
+                                           unsigned long long *Fn) {
   const int lane = lane_id();
-  const int m = j->m;
-  int *qin = jobQ(j, L % 2), *qout = jobQ(j, (L + 1) % 2);
-  int2 *cout = jobC(j, (L + 1) % 2);
+  const int sw = j->sw;
+  const int per = 32 / sw;                 // edges per round
+  const int src = lane & (sw - 1), eo = lane / sw;
+  const unsigned grp = sw == 32 ? 0xffffffffu : ((1u << sw) - 1u);
+  unsigned *dist = reinterpret_cast<unsigned *>(j->out);
+  unsigned nd[kSsspSlots], cur[kSsspSlots];
+  int uu[kSsspSlots];
+  bool act[kSsspSlots];
+#pragma unroll
+  for (int i = 0; i < kSsspSlots; ++i) {
+    const int el = i * per + eo;           // the edge's loading lane
+    const bool in = el < 32;
+    const unsigned mi = __shfl_sync(kFull, me, el & 31);
+    const int vi = __shfl_sync(kFull, ve, el & 31);
+    const unsigned wi = __shfl_sync(kFull, we, el & 31);
+    uu[i] = __shfl_sync(kFull, ue, el & 31);
+    act[i] = in && ((mi >> src) & 1u);
+    // the tail's distance is read from L2 (it dropped in the last round)
+    nd[i] = act[i] ? sat_add(__ldcg(dist + (size_t)vi * sw + src), wi) : 0u;
+    cur[i] = act[i] ? __ldcg(dist + (size_t)uu[i] * sw + src) : 0u;
+  }
+  unsigned mybal = 0;
+#pragma unroll
+  for (int i = 0; i < kSsspSlots; ++i) {
+    const bool imp = act[i] && nd[i] < cur[i] &&
+                     nd[i] < atomicMin(dist + (size_t)uu[i] * sw + src, nd[i]);
+    const unsigned b = __ballot_sync(kFull, imp);
+    // loading lane i * per + g takes the bits of its edge's group g
+    const int g = lane - i * per;
+    if (g >= 0 && g < per) mybal = (b >> (g * sw)) & grp;
+  }
+  bool first = false;
+  if (mybal) first = atomicOr(Fn + ue, (unsigned long long)mybal) == 0ull;
+  return first;
+}
+
+// kSsspPerUnit queued vertices: their edges laid out flat, a batch at a time
+__device__ void mssp_queue(BatchJob *j, int L, int unit, unsigned nq) {
+  const int lane = lane_id();
+  int *qin = jobQ(j, L % 3), *qout = jobQ(j, (L + 1) % 3);
+  int2 *cout = jobC(j, (L + 1) % 3);
+  unsigned long long *Fc = jobF(j, L % 3), *Fn = jobF(j, (L + 1) % 3);
   JobCounters *nxt = &j->c[(L + 1) % 3];
-  const unsigned *dist = (const unsigned *)j->out;
-  unsigned idx = (unsigned)unit * 32u + lane;
-  int item = idx < nq ? __ldcg(qin + idx) : -1;
-  int s = 0, d = 0, base = 0;
-  unsigned du = 0;
-  if (item >= 0) {
-    int v = item % m;
-    base = item - v;
+  const int nb = mssp_batch(j->sw);
+  const unsigned idx = (unsigned)unit * kSsspPerUnit + (unsigned)lane;
+  int v = -1, s = 0, d = 0;
+  if (lane < kSsspPerUnit && idx < nq) {
+    v = __ldcg(qin + idx);
     s = __ldg(j->ptr + v);
     d = __ldg(j->ptr + v + 1) - s;
-    du = __ldcg(dist + item);
   }
-  int incl = warp_incl_scan(d);
-  int excl = incl - d;
-  int total = __shfl_sync(kFull, incl, 31);
-  for (int e0 = 0; e0 < total; e0 += 32) {
-    int e = e0 + lane;
-    int owner = warp_owner(excl, e);
-    int so = __shfl_sync(kFull, s, owner);
-    int eo = __shfl_sync(kFull, excl, owner);
-    unsigned duo = __shfl_sync(kFull, du, owner);
-    int bo = __shfl_sync(kFull, base, owner);
-    bool found[1] = {false};
-    int u[1] = {-1}, dg[1] = {0};
-    if (e < total) {
-      int k = so + (e - eo);
-      int dst = __ldg(j->ind + k);
-      found[0] = sssp_relax(j, bo, duo, k, dst, L);
-      if (found[0]) {
-        u[0] = bo + dst;
-        dg[0] = __ldg(j->ptr + dst + 1) - __ldg(j->ptr + dst);
-      }
+  const int incl = warp_incl_scan(d);
+  const int excl = incl - d;
+  const int total = __shfl_sync(kFull, incl, 31);
+  for (int e0 = 0; e0 < total; e0 += nb) {
+    const int e = e0 + lane;
+    const int owner = warp_owner(excl, min(e, total - 1));
+    const int so = __shfl_sync(kFull, s, owner);
+    const int eo = __shfl_sync(kFull, excl, owner);
+    const int vo = __shfl_sync(kFull, v, owner);
+    int ue = 0, ve = 0;
+    unsigned we = 0, me = 0;
+    if (lane < nb && e < total) {
+      const int k = so + (e - eo);
+      ue = __ldg(j->ind + k);
+      we = __ldg(j->w + k);
+      ve = vo;
+      me = (unsigned)__ldcg(Fc + vo);
     }
-    append_n<1>(found, u, dg, qout, cout, nxt);
+    bool f[1] = {mssp_relax(j, ue, we, ve, me, Fn)};
+    int u1[1] = {ue}, dg[1] = {0};
+    if (f[0]) dg[0] = __ldg(j->ptr + ue + 1) - __ldg(j->ptr + ue);
+    append_n<1>(j, f, u1, dg, qout, cout, nxt);
   }
 }
 
-__device__ void sssp_chunk(BatchJob *j, int L, int unit) {
+// one kSsspChunk-edge chunk of a hub
+__device__ void mssp_chunk(BatchJob *j, int L, int unit) {
   const int lane = lane_id();
-  const int m = j->m;
-  int2 *cin = jobC(j, L % 2), *cout = jobC(j, (L + 1) % 2);
-  int *qout = jobQ(j, (L + 1) % 2);
+  int2 *cin = jobC(j, L % 3), *cout = jobC(j, (L + 1) % 3);
+  int *qout = jobQ(j, (L + 1) % 3);
+  unsigned long long *Fc = jobF(j, L % 3), *Fn = jobF(j, (L + 1) % 3);
   JobCounters *nxt = &j->c[(L + 1) % 3];
-  int2 ch = __ldcg(cin + unit);
-  int v = ch.x % m, base = ch.x - v;
-  int s = __ldg(j->ptr + v) + ch.y * kChunk;
-  int e = min(s + kChunk, __ldg(j->ptr + v + 1));
-  unsigned du = __ldcg((const unsigned *)j->out + ch.x);
-  for (int k0 = s; k0 < e; k0 += 32) {
-    int k = k0 + lane;
-    bool found[1] = {false};
-    int u[1] = {-1}, dg[1] = {0};
-    if (k < e) {
-      int dst = __ldg(j->ind + k);
-      found[0] = sssp_relax(j, base, du, k, dst, L);
-      if (found[0]) {
-        u[0] = base + dst;
-        dg[0] = __ldg(j->ptr + dst + 1) - __ldg(j->ptr + dst);
-      }
+  const int2 ch = __ldcg(cin + unit);
+  const int v = ch.x;
+  const int s = __ldg(j->ptr + v) + ch.y * kSsspChunk;
+  const int e = min(s + kSsspChunk, __ldg(j->ptr + v + 1));
+  const unsigned mv = (unsigned)__ldcg(Fc + v);
+  const int nb = mssp_batch(j->sw);
+  for (int k0 = s; k0 < e; k0 += nb) {
+    const int k = k0 + lane;
+    int ue = 0;
+    unsigned we = 0, me = 0;
+    if (lane < nb && k < e) {
+      ue = __ldg(j->ind + k);
+      we = __ldg(j->w + k);
+      me = mv;
     }
-    append_n<1>(found, u, dg, qout, cout, nxt);
+    bool f[1] = {mssp_relax(j, ue, we, v, me, Fn)};
+    int u1[1] = {ue}, dg[1] = {0};
+    if (f[0]) dg[0] = __ldg(j->ptr + ue + 1) - __ldg(j->ptr + ue);
+    append_n<1>(j, f, u1, dg, qout, cout, nxt);
   }
 }
 
@@ -482,59 +544,66 @@ batch_persistent(BatchJob *jobs, int njobs, BatchState *st, int max_steps) {
   __syncthreads();
   int step = 0;
   for (;; ++step) {
-    if (threadIdx.x == 0) {
-      unsigned run = 0;
-      for (int jj = 0; jj < njobs; ++jj) {
-        BatchJob *j = jobs + jj;
-        JobCounters *cur = &j->c[step % 3];
-        unsigned q = __ldcg(&cur->q), ch = __ldcg(&cur->chunks), nb = __ldcg(&cur->nbig);
-        unsigned long long ed = __ldcg(&cur->edges);
-        s_q[jj] = q;
-        s_ch[jj] = ch;
-        s_edges[jj] = ed;
-        if (blockIdx.x == 0) j->c[(step + 2) % 3] = JobCounters{0, 0, 0, 0, 0ull};
-        unsigned long long nf = (unsigned long long)q + nb;
-        bool active = !s_done[jj] && nf > 0 && (max_steps <= 0 || step < max_steps);
-        if (!active) s_done[jj] = 1;
-        unsigned u0 = 0, u1 = 0, u2 = 0, u3 = 0;
+    // Step set-up, one thread per job (all blocks compute the same values
+    // from counters nobody writes during this step): the job's frontier,
+    // direction and units.
+    if (threadIdx.x < njobs) {
+      const int jj = threadIdx.x;
+      BatchJob *j = jobs + jj;
+      JobCounters *cur = &j->c[step % 3];
+      const unsigned long long qc = __ldcg(&cur->qc);
+      const unsigned q = (unsigned)qc, ch = (unsigned)(qc >> 32), nb = __ldcg(&cur->nbig);
+      const unsigned long long ed = __ldcg(&cur->edges);
+      s_q[jj] = q;
+      s_ch[jj] = ch;
+      s_edges[jj] = ed;
+      if (blockIdx.x == 0) j->c[(step + 2) % 3] = JobCounters{0ull, 0, 0, 0ull};
+      const unsigned long long nf = (unsigned long long)q + nb;
+      const bool active = !s_done[jj] && nf > 0 && (max_steps <= 0 || step < max_steps);
+      if (!active) s_done[jj] = 1;
+      // clear the frontier words of level step-1 (they are reused at step+1)
+      unsigned u0 = (s_prevq[jj] + 31) / 32, u1 = (s_prevch[jj] + 31) / 32, u2 = 0, u3 = 0;
+      if (active) {
+        s_explored[jj] += ed;
         if (j->type == kJobBfs) {
-          // clear the frontier words of level step-1 (they are reused at step+1)
-          u0 = (s_prevq[jj] + 31) / 32;
-          u1 = (s_prevch[jj] + 31) / 32;
-        }
-        if (active) {
-          s_explored[jj] += ed;
-          if (j->type == kJobBfs) {
-            long long unexplored = j->nnz * (long long)1 - (long long)s_explored[jj];
-            if (!s_pull[jj]) {
-              if ((long long)ed * j->alpha > unexplored) s_pull[jj] = 1;
-            } else if ((long long)nf * j->beta < (long long)j->m) {
-              s_pull[jj] = 0;
-            }
-            if (s_pull[jj]) {
-              u2 = (unsigned)((j->m + 31) / 32);
-            } else {
-              u2 = (q + 31) / 32;
-              u3 = ch;
-            }
+          long long unexplored = j->nnz - (long long)s_explored[jj];
+          if (!s_pull[jj]) {
+            if ((long long)ed * j->alpha > unexplored) s_pull[jj] = 1;
+          } else if ((long long)nf * j->beta < (long long)j->m) {
+            s_pull[jj] = 0;
+          }
+          if (s_pull[jj]) {
+            u2 = (unsigned)((j->m + 31) / 32);
           } else {
             u2 = (q + 31) / 32;
             u3 = ch;
           }
+        } else {
+          u2 = (q + kSsspPerUnit - 1) / kSsspPerUnit;
+          u3 = ch;
         }
-        s_u0[jj] = u0;
-        s_u1[jj] = u1;
-        s_u2[jj] = u2;
-        s_u3[jj] = u3;
-        s_pre[jj] = run;
-        run += u0 + u1 + u2 + u3;
       }
-      s_pre[njobs] = run;
+      s_u0[jj] = u0;
+      s_u1[jj] = u1;
+      s_u2[jj] = u2;
+      s_u3[jj] = u3;
     }
     __syncthreads();
+    // exclusive prefix of the jobs' unit counts (warp 0; at most 64 jobs)
+    if (warp == 0) {
+      const int lane = lane_id();
+      unsigned carry = 0;
+      for (int b = 0; b < njobs; b += 32) {
+        const int jj = b + lane;
+        const unsigned cnt = jj < njobs ? s_u0[jj] + s_u1[jj] + s_u2[jj] + s_u3[jj] : 0u;
+        const unsigned incl = warp_incl_scan(cnt);
+        if (jj < njobs) s_pre[jj] = carry + incl - cnt;
+        carry += __shfl_sync(kFull, incl, 31);
+      }
+      if (lane == 0) s_pre[njobs] = carry;
+    }
+    const bool any_active = __syncthreads_or(threadIdx.x < njobs && !s_done[threadIdx.x]) != 0;
     const unsigned total = s_pre[njobs];
-    bool any_active = false;
-    for (int jj = 0; jj < njobs; ++jj) any_active |= !s_done[jj];
     if (!any_active) break;
     for (unsigned g = (unsigned)gwarp; g < total; g += (unsigned)nwarps) {
       int lo = 0, hi = njobs - 1;
@@ -566,40 +635,36 @@ batch_persistent(BatchJob *jobs, int njobs, BatchState *st, int max_steps) {
         }
       } else {
         if (loc < s_u2[lo])
-          sssp_queue(j, step, (int)loc, s_q[lo]);
+          mssp_queue(j, step, (int)loc, s_q[lo]);
         else
-          sssp_chunk(j, step, (int)(loc - s_u2[lo]));
+          mssp_chunk(j, step, (int)(loc - s_u2[lo]));
       }
     }
-    if (threadIdx.x == 0) {
-      for (int jj = 0; jj < njobs; ++jj) {
-        // the frontier of this step is cleared two steps later
-        bool was_active = s_u2[jj] + s_u3[jj] > 0;
-        s_prevq[jj] = was_active ? s_q[jj] : 0;
-        s_prevch[jj] = was_active ? s_ch[jj] : 0;
-      }
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      unsigned long long ed = 0;
-      for (int jj = 0; jj < njobs; ++jj)
-        if (s_u2[jj] + s_u3[jj] > 0) ed += s_edges[jj];
-      st->edges += ed;
+    __syncthreads();
+    if (threadIdx.x < njobs) {
+      const int jj = threadIdx.x;
+      // the frontier of this step is cleared two steps later
+      const bool was_active = s_u2[jj] + s_u3[jj] > 0;
+      s_prevq[jj] = was_active ? s_q[jj] : 0;
+      s_prevch[jj] = was_active ? s_ch[jj] : 0;
+      if (blockIdx.x == 0 && was_active && s_edges[jj]) atomicAdd(&st->edges, s_edges[jj]);
     }
     if (!grid_barrier(st->bar, &st->err)) return;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) st->steps = step;
 }
 
-// vertex-major depth [m][64] -> source-major out[s][m] for s < nsrc
-__global__ void batch_transpose(const int32_t *vm, int m, int nsrc, int32_t *out) {
+// vertex-major results [m][width] -> source-major out[s][m] for s < nsrc
+// (width 64 or 32)
+__global__ void batch_transpose(const int32_t *vm, int m, int width, int nsrc, int32_t *out) {
   __shared__ int32_t tile[32][65];
   const int v0 = blockIdx.x * 32;
-  for (int t = threadIdx.x; t < 32 * 64; t += blockDim.x) {
-    int vv = t / 64, s = t % 64;
-    tile[vv][s] = (v0 + vv < m) ? vm[(size_t)(v0 + vv) * 64 + s] : -1;
+  for (int t = threadIdx.x; t < 32 * width; t += blockDim.x) {
+    int vv = t / width, s = t % width;
+    tile[vv][s] = (v0 + vv < m) ? vm[(size_t)(v0 + vv) * width + s] : -1;
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < 32 * 64; t += blockDim.x) {
+  for (int t = threadIdx.x; t < 32 * width; t += blockDim.x) {
     int s = t / 32, vv = t % 32;
     if (s < nsrc && v0 + vv < m) out[(size_t)s * m + v0 + vv] = tile[vv][s];
   }
@@ -621,6 +686,19 @@ int batch_grid(apspie_context *ctx) {
 }
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Distance-row width of an SSSP job: the sources rounded up to a power of two.
+int row_width(int nsrc) {
+  int w = 1;
+  while (w < nsrc) w <<= 1;
+  return w;
+}
+
+// Chunk-list capacity of a job: its big vertices have more than big_deg edges.
+size_t job_chunk_capacity(long long nnz, bool bfs) {
+  const long long bd = bfs ? kBigDeg : kSsspBigDeg, ck = bfs ? kChunk : kSsspChunk;
+  return (size_t)(nnz / ck + nnz / bd + 2);
+}
 
 }  // namespace
 }  // namespace apspie
@@ -648,7 +726,9 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
       if (J.h_src[s] < 0 || J.h_src[s] >= J.m)
         return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: job %d source %d out of range",
                          i, J.h_src[s]);
-    for (int f = 0; f < J.nsrc; f += 64) parts.push_back(Part{i, f, std::min(64, J.nsrc - f)});
+    const int width = J.type == APSPIE_JOB_BFS ? kMsbfsWidth : kMssspWidth;
+    for (int f = 0; f < J.nsrc; f += width)
+      parts.push_back(Part{i, f, std::min(width, J.nsrc - f)});
   }
   const int nparts = (int)parts.size();
   if (nparts > kMaxJobs)
@@ -661,22 +741,13 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
   const size_t head = total;
   for (int p = 0; p < nparts; ++p) {
     const apspie_job &J = jobs[parts[p].job];
-    size_t m = (size_t)J.m, cap = chunk_capacity(J.nnz);
+    const bool bfs = J.type == APSPIE_JOB_BFS;
+    const size_t m = (size_t)J.m, cap = job_chunk_capacity(J.nnz, bfs);
     size_t b = 0;
-    if (J.type == APSPIE_JOB_BFS) {
-      b += align_up(8 * m) * 4;           // visited + 3 frontier masks
-      b += align_up(4 * m) * 3;           // queues
-      b += align_up(8 * cap) * 3;         // chunk lists
-      b += align_up(4 * m * 64);          // vertex-major depths
-    } else {
-      size_t items = m * (size_t)parts[p].n;
-      if (items >= (size_t)INT32_MAX)
-        return set_error(ctx, APSPIE_ERR_OVERFLOW, "apspie_batch_run: sources x vertices too large");
-      size_t icap = std::min(items, cap * (size_t)parts[p].n);
-      b += align_up(4 * items) * 2;        // queues (two rotate)
-      b += align_up(8 * icap) * 2;         // chunk lists
-      b += align_up(4 * items);            // stamps
-    }
+    b += align_up(8 * m) * (bfs ? 4 : 3);  // (BFS: visited +) 3 frontier masks
+    b += align_up(4 * m) * 3;              // queues
+    b += align_up(8 * cap) * 3;            // chunk lists
+    b += align_up(4 * m * (bfs ? kMsbfsWidth : row_width(parts[p].n)));  // vertex-major results
     off[p] = total;
     total += b;
   }
@@ -714,31 +785,25 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
     for (int s = 0; s < parts[p].n; ++s) hsrc[p * 64 + s] = J.h_src[parts[p].first + s];
     B.src = dsrc + p * 64;
     unsigned char *b = ws + off[p];
-    size_t m = (size_t)J.m, cap = chunk_capacity(J.nnz);
-    if (B.type == kJobBfs) {
-      B.visited = (unsigned long long *)b; b += align_up(8 * m);
-      B.F0 = (unsigned long long *)b; b += align_up(8 * m);
-      B.F1 = (unsigned long long *)b; b += align_up(8 * m);
-      B.F2 = (unsigned long long *)b; b += align_up(8 * m);
-      B.q0 = (int *)b; b += align_up(4 * m);
-      B.q1 = (int *)b; b += align_up(4 * m);
-      B.q2 = (int *)b; b += align_up(4 * m);
-      B.c0 = (int2 *)b; b += align_up(8 * cap);
-      B.c1 = (int2 *)b; b += align_up(8 * cap);
-      B.c2 = (int2 *)b; b += align_up(8 * cap);
-      B.out = (int32_t *)b;  // vertex-major; transposed into the caller's array after
-    } else {
-      size_t items = m * (size_t)B.nsrc;
-      size_t icap = std::min(items, cap * (size_t)B.nsrc);
-      B.q0 = (int *)b; b += align_up(4 * items);
-      B.q1 = (int *)b; b += align_up(4 * items);
-      B.q2 = B.q0;
-      B.c0 = (int2 *)b; b += align_up(8 * icap);
-      B.c1 = (int2 *)b; b += align_up(8 * icap);
-      B.c2 = B.c0;
-      B.stamp = (int *)b;
-      B.out = (int32_t *)J.d_out + (size_t)parts[p].first * m;
+    const bool bfs = B.type == kJobBfs;
+    const size_t m = (size_t)J.m, cap = job_chunk_capacity(J.nnz, bfs);
+    B.big_deg = bfs ? kBigDeg : kSsspBigDeg;
+    B.sw = bfs ? kMsbfsWidth : row_width(B.nsrc);
+    B.chunk = bfs ? kChunk : kSsspChunk;
+    if (bfs) {
+      B.visited = (unsigned long long *)b;
+      b += align_up(8 * m);
     }
+    B.F0 = (unsigned long long *)b; b += align_up(8 * m);
+    B.F1 = (unsigned long long *)b; b += align_up(8 * m);
+    B.F2 = (unsigned long long *)b; b += align_up(8 * m);
+    B.q0 = (int *)b; b += align_up(4 * m);
+    B.q1 = (int *)b; b += align_up(4 * m);
+    B.q2 = (int *)b; b += align_up(4 * m);
+    B.c0 = (int2 *)b; b += align_up(8 * cap);
+    B.c1 = (int2 *)b; b += align_up(8 * cap);
+    B.c2 = (int2 *)b; b += align_up(8 * cap);
+    B.out = (int32_t *)b;  // vertex-major; transposed into the caller's array after
   }
   cudaStream_t st = ctx->stream;
   cudaMemcpyAsync(djobs, hjobs, host_bytes, cudaMemcpyHostToDevice, st);
@@ -747,9 +812,8 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
   int rc = check_cuda(ctx, cudaGetLastError(), "apspie_batch_run upload");
   if (rc) return rc;
   for (int p = 0; p < nparts; ++p) {
-    const int m = jobs[parts[p].job].m;
-    int g = std::max(1, std::min((m * (hjobs[p].type == kJobBfs ? 64 : hjobs[p].nsrc) + 255) / 256,
-                                 ctx->num_sms * 8));
+    const long long m = jobs[parts[p].job].m;
+    int g = (int)std::max(1ll, std::min((m * hjobs[p].sw + 255) / 256, (long long)ctx->num_sms * 8));
     if (hjobs[p].type == kJobBfs) {
       batch_init_bfs<<<g, 256, 0, st>>>(djobs, p);
       batch_seed_bfs<<<1, 64, 0, st>>>(djobs, p);
@@ -769,9 +833,9 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
   if (e != cudaSuccess) return check_cuda(ctx, e, "batch_persistent");
   ctx->launches += 1;
   for (int p = 0; p < nparts; ++p) {
-    if (hjobs[p].type != kJobBfs) continue;
     const apspie_job &J = jobs[parts[p].job];
-    batch_transpose<<<(J.m + 31) / 32, 256, 0, st>>>(hjobs[p].out, J.m, parts[p].n,
+    const int width = hjobs[p].sw;
+    batch_transpose<<<(J.m + 31) / 32, 256, 0, st>>>(hjobs[p].out, J.m, width, parts[p].n,
                                                      J.d_out + (size_t)parts[p].first * J.m);
   }
   rc = check_launch(ctx, "batch_transpose", nparts);

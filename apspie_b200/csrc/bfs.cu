@@ -54,7 +54,7 @@ struct BfsState {
   // reading those to choose the direction while faster ones already append.
   // Two sets, by level parity; block 0 clears the other one each level.
   LevelCounters comp[2];
-  unsigned bar[2];
+  alignas(8) unsigned bar[2];  // grid-barrier arrival counter (64-bit)
   int err;
   int levels;
   int pull_levels;
@@ -67,6 +67,7 @@ struct BfsState {
 
 // Push visitor: an unvisited destination is claimed with one CAS.
 struct BfsVisit {
+  static constexpr bool kTwoWay = false;
   int next;
   int32_t *depth;
   __device__ __forceinline__ bool check(unsigned, int, int u, unsigned &) const {
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(kBfsThreads, 3)
 bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__restrict__ ind,
                const int *__restrict__ tptr, const int *__restrict__ tind, int32_t *depth,
                int *qa, int *qb, int2 *ca, int2 *cb, BfsState *st, int max_levels, int alpha,
-               int beta, int mode) {
+               int beta, int mode, unsigned *gmask) {
   const int lane = lane_id();
   const int warp = warp_in_block();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -124,6 +125,7 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
   if (blockIdx.x == 0 && threadIdx.x == 0) st->t_start = globaltimer();
   bool pull = false;
   int pull_levels = 0;
+  unsigned long long prev_nf = 0;
   unsigned long long reached = 0, explored = 0;
   int L = 0;
   for (;; ++L) {
@@ -131,10 +133,10 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
     LevelCounters *nxt = &st->c[(L + 1) % 3];
     LevelCounters *clr = &st->c[(L + 2) % 3];
     if (threadIdx.x == 0) {
-      const unsigned long long qc = __ldcg(&cur->qc);
-      s_q = qc_queue(qc);
-      s_chunks = qc_chunks(qc);
-      s_nbig = __ldcg(&cur->nbig);
+      const unsigned long long bc = __ldcg(&cur->bc);
+      s_q = __ldcg(&cur->q);
+      s_chunks = bc_chunks(bc);
+      s_nbig = bc_big(bc);
       s_nimpl = __ldcg(&cur->nimpl);
       s_edges = __ldcg(&cur->edges);
       s_bcnt = 0;
@@ -212,21 +214,29 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
         flush_acc(acc, &st->comp[L & 1]);
         if (!grid_barrier(st->bar, &st->err)) return;
         if (threadIdx.x == 0) {
-          const unsigned long long qc = __ldcg(&st->comp[L & 1].qc);
-          s_q = qc_queue(qc);
-          s_chunks = qc_chunks(qc);
+          const unsigned long long bc = __ldcg(&st->comp[L & 1].bc);
+          s_q = __ldcg(&st->comp[L & 1].q);
+          s_chunks = bc_chunks(bc);
+          s_nbig = bc_big(bc);
         }
         __syncthreads();
         nq = s_q;
         nch = s_chunks;
       }
       BfsVisit vis{next, depth};
-      expand_push(ptr, ind, qin, nq, cin, nch, qout, cout, nxt, gwarp, nwarps,
+      expand_push(ptr, ind, qin, nq, cin, s_nbig, nch, qout, cout, nxt, gwarp, nwarps,
                   [](int) { return 0u; }, vis,
                   L < kTraceLevels ? &st->trace[L].expanded : nullptr);
     } else {
       ++pull_levels;
       // ---- pull: unvisited vertices look for a parent at depth L ----
+      // While the frontier grows the next level will pull again, and its
+      // frontier stays implicit (depth == L + 1, counted only).  Once it
+      // shrinks the next level may push: each group's found-mask is then
+      // kept (gmask) and, when the block has finished its range, the block
+      // appends its discoveries to the next queue, so that level need not
+      // rebuild the queue from the depth array behind a grid barrier.
+      const bool append = nf < prev_nf;
       // The unresolved vertices of a warp share its lanes round-robin: with k
       // of them unresolved, vertex of rank j gets lanes j, j+k, j+2k, ... and
       // each of those lanes probes kProbe in-neighbours (all index loads, then
@@ -309,12 +319,39 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
           found = (fm >> lane) & 1u;
           U = __ballot_sync(kFull, mine && !found && s < e);
         }
-        if (found) {
-          depth[v] = next;
+        if (found) depth[v] = next;
+        if (append) {
+          const unsigned fw = __ballot_sync(kFull, found);
+          if (lane == 0) gmask[g] = fw;
+        } else if (found) {
           ++cnt;
           edg += (unsigned long long)(__ldg(ptr + v + 1) - __ldg(ptr + v));
         }
         g = gn;
+      }
+      if (append) {
+        // block-local append of the discoveries of [gbeg, gend): 32 groups
+        // per warp batch, each round every lane with bits left hands one
+        // vertex to the warp's append
+        __syncthreads();
+        if (threadIdx.x == 0) s_next = 0;
+        __syncthreads();
+        DiscoverAcc pacc;
+        for (;;) {
+          unsigned g0 = 0;
+          if (lane == 0) g0 = atomicAdd(&s_next, 32u);
+          g0 = __shfl_sync(kFull, g0, 0);
+          if (gbeg + g0 >= gend) break;
+          const unsigned gw = gbeg + g0 + lane;
+          unsigned bits = gw < gend ? gmask[gw] : 0u;
+          while (__ballot_sync(kFull, bits != 0u)) {
+            bool f1[1] = {bits != 0u};
+            int u1[1] = {f1[0] ? (int)(gw * 32u) + __ffs(bits) - 1 : 0};
+            bits &= bits - 1u;
+            discover_n<1>(f1, u1, ptr, qout, cout, nxt, pacc);
+          }
+        }
+        flush_acc(pacc, nxt);
       }
       cnt = warp_sum(cnt);
       edg = warp_sum(edg);
@@ -328,6 +365,7 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
         atomicAdd(&nxt->edges, s_bedg);
       }
     }
+    prev_nf = nf;
     if (L < kTraceLevels) {
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -391,7 +429,8 @@ int apspie_bfs(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
   auto *qb = (int *)workspace(ctx, kSlotBfsQueueB, sizeof(int) * (size_t)m);
   auto *ca = (int2 *)workspace(ctx, kSlotBfsChunksA, sizeof(int2) * chunk_cap);
   auto *cb = (int2 *)workspace(ctx, kSlotBfsChunksB, sizeof(int2) * chunk_cap);
-  if (!st || !qa || !qb || !ca || !cb) return APSPIE_ERR_OOM;
+  auto *gmask = (unsigned *)workspace(ctx, kSlotBfsGroupMask, sizeof(unsigned) * ((size_t)m / 32 + 1));
+  if (!st || !qa || !qb || !ca || !cb || !gmask) return APSPIE_ERR_OOM;
   ctx->bfs_state = st;
   int grid = bfs_grid(ctx);
   if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_bfs: occupancy query failed");
@@ -404,7 +443,8 @@ int apspie_bfs(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
   int alpha = ctx->bfs_alpha, beta = ctx->bfs_beta, mode = ctx->bfs_mode;
   if (!d_tptr) mode = 1;  // no in-adjacency: push only
   void *args[] = {&m,  &nnz_ll, (void *)&d_ptr, (void *)&d_ind, (void *)&d_tptr, (void *)&d_tind,
-                  &d_depth, &qa, &qb, &ca, &cb, &st, &max_levels, &alpha, &beta, &mode};
+                  &d_depth, &qa, &qb, &ca, &cb, &st, &max_levels, &alpha, &beta, &mode,
+                  &gmask};
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)bfs_persistent, dim3(grid),
                                               dim3(kBfsThreads), args, 0, ctx->stream);
   if (e != cudaSuccess) return check_cuda(ctx, e, "bfs_persistent");
@@ -498,7 +538,8 @@ constexpr size_t kNaOffQa = align256(sizeof(BfsState));
 constexpr size_t kNaOffQb = kNaOffQa + align256(sizeof(int) * (size_t)kNoAllocMaxVertices);
 constexpr size_t kNaOffCa = kNaOffQb + align256(sizeof(int) * (size_t)kNoAllocMaxVertices);
 constexpr size_t kNaOffCb = kNaOffCa + align256(sizeof(int2) * kNoAllocChunkCap);
-constexpr size_t kNaBytes = kNaOffCb + align256(sizeof(int2) * kNoAllocChunkCap);
+constexpr size_t kNaOffGm = kNaOffCb + align256(sizeof(int2) * kNoAllocChunkCap);
+constexpr size_t kNaBytes = kNaOffGm + align256(sizeof(unsigned) * (kNoAllocMaxVertices / 32 + 1));
 
 static __device__ __align__(256) unsigned char g_bfs_noalloc_scratch[kNaBytes];
 
@@ -561,6 +602,7 @@ extern "C" int apspie_bfs_noalloc(void *stream, int src, int64_t nnz, int m, con
   auto *qb = (int *)(base + kNaOffQb);
   auto *ca = (int2 *)(base + kNaOffCa);
   auto *cb = (int2 *)(base + kNaOffCb);
+  auto *gmask = (unsigned *)(base + kNaOffGm);
   // bfs_init clears every counter and status word the kernel reads, so the
   // contents left by the previous call do not matter
   int init_grid = std::min((m + 255) / 256, grid * 2);
@@ -569,7 +611,8 @@ extern "C" int apspie_bfs_noalloc(void *stream, int src, int64_t nnz, int m, con
   long long nnz_ll = (long long)nnz;
   int alpha = 14, beta = 24, mode = d_tptr ? 0 : 1;
   void *args[] = {&m,  &nnz_ll, (void *)&d_ptr, (void *)&d_ind, (void *)&d_tptr, (void *)&d_tind,
-                  &d_depth, &qa, &qb, &ca, &cb, &state, &max_levels, &alpha, &beta, &mode};
+                  &d_depth, &qa, &qb, &ca, &cb, &state, &max_levels, &alpha, &beta, &mode,
+                  &gmask};
   if (cudaLaunchCooperativeKernel((const void *)bfs_persistent, dim3(grid), dim3(kBfsThreads), args,
                                   0, st) != cudaSuccess) {
     cudaGetLastError();

@@ -72,9 +72,18 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
   return v;
 }
 
-// Sense-counting grid barrier for cooperatively launched kernels.
-// bar[0] = arrival count, bar[1] = generation.  Returns false (and sets
-// *err = APSPIE_ERR_TIMEOUT) if the other blocks do not arrive within
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid barrier for cooperatively launched kernels, on one 64-bit arrival
+// counter that only grows (bar must be 8-byte aligned and zero at launch):
+// the k-th barrier of every block waits until the counter reaches
+// k * nblocks, so the last block to arrive has nothing left to do and the
+// others see the release as soon as its arrival lands.  Returns false (and
+// sets *err = APSPIE_ERR_TIMEOUT) if the other blocks do not arrive within
 // kSpinLimit polls; the caller must then leave the kernel.
 constexpr unsigned kSpinLimit = 1u << 24;
 
@@ -82,25 +91,20 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
-    unsigned gen = ld_acquire(bar + 1);
-    __threadfence();
-    unsigned arrived = atomicAdd(bar, 1u);
+    unsigned long long *ctr = reinterpret_cast<unsigned long long *>(bar);
+    const unsigned long long nblocks = gridDim.x * gridDim.y * gridDim.z;
+    __threadfence();  // this block's writes before its arrival
+    const unsigned long long arrived = atomicAdd(ctr, 1ull);
+    const unsigned long long target = (arrived / nblocks + 1) * nblocks;
     int ok = 1;
-    if (arrived == nblocks - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      unsigned spins = 0;
-      while (ld_acquire(bar + 1) == gen) {
-        if (++spins > kSpinLimit || *(volatile int *)err != 0) {
-          atomicCAS(err, 0, (int)APSPIE_ERR_TIMEOUT);
-          ok = 0;
-          break;
-        }
-        __nanosleep(64);
+    unsigned spins = 0;
+    while (ld_acquire64(ctr) < target) {
+      if (++spins > kSpinLimit || *(volatile int *)err != 0) {
+        atomicCAS(err, 0, (int)APSPIE_ERR_TIMEOUT);
+        ok = 0;
+        break;
       }
+      __nanosleep(32);
     }
     __threadfence();
     s_ok = ok;

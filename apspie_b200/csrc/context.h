@@ -36,6 +36,9 @@ struct apspie_context {
   int bfs_mode = 0;  // 0 auto, 1 push only, 2 pull only
   void *bfs_state = nullptr;  // device pointer into a workspace slot
   void *sssp_state = nullptr;
+  // SSSP near-far step (0: frontier Bellman-Ford)
+  uint32_t sssp_delta_u32 = 0;
+  float sssp_delta_f32 = 0.0f;
   void *mis_state = nullptr;
   void *batch_state = nullptr;
   // SpMSpV: the bitmap path is taken when E * factor > m
@@ -58,12 +61,14 @@ enum SlotId : int {
   kSlotBfsQueueB,
   kSlotBfsChunksA,
   kSlotBfsChunksB,
+  kSlotBfsGroupMask,
   kSlotSsspState,
   kSlotSsspQueueA,
   kSlotSsspQueueB,
   kSlotSsspChunksA,
   kSlotSsspChunksB,
   kSlotSsspStamp,
+  kSlotSsspNearFar,
   kSlotMisState,
   kSlotMisQueueA,
   kSlotMisQueueB,

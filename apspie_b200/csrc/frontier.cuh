@@ -7,21 +7,24 @@
 //     of their degrees lays the warp's edges out flat, each round deals 32
 //     consecutive edges to the lanes (coalesced reads of ind[]), and a 5-step
 //     shuffle search maps an edge back to its owner lane;
-//   * vertices of degree > kBigDeg are split into kChunk-edge chunks, listed
-//     as (vertex, chunk) pairs that every warp of the grid pulls from, so a
-//     small frontier of hubs still spreads over the whole GPU.
+//   * vertices of degree > kBigDeg are split into kChunk-edge chunks that
+//     every warp of the grid takes a share of, so a small frontier of hubs
+//     still spreads over the whole GPU.  They are listed once each, as
+//     (vertex, first chunk index) in a "big list" whose chunk indices grow
+//     with the list position; a warp finds the vertex of its first chunk by
+//     a 32-way search of that list and walks on from there.  (Writing one
+//     entry per chunk at discovery cost more than the expansion of small
+//     levels, and is wasted when the next level pulls.)
 // Rounds are issued kUnroll at a time: all index loads of the batch, then all
 // visitor checks (the random loads), then the atomic commits, so each lane
 // keeps several independent loads in flight.  A visitor provides
 //   check(payload, k, u, &aux) -> bool   (plain loads only)
 //   commit(payload, k, u, aux) -> bool   (atomics; true = u joins the next frontier)
-// discover_n() appends joiners (warp-aggregated) to the next queue or, for
-// big vertices, writes their chunk entries cooperatively.  Every warp of the
-// grid appends to the same counters, and same-address atomics serialise in
-// L2, so an append costs ONE returning atomic: queue and chunk-list lengths
-// share a 64-bit word and are reserved together, while the big-vertex count
-// and the next frontier's edge count are summed in registers and added once
-// per warp per level (flush_acc).
+// discover_n() appends joiners (warp-aggregated) to the next queue or the
+// next big list: one atomic per warp for the queue slots, one for the big
+// list, whose length and chunk total share a 64-bit word so that list order
+// and chunk order agree; the next frontier's edge count is summed in
+// registers and added once per warp per level (flush_acc).
 #pragma once
 #include "common.cuh"
 
@@ -32,30 +35,46 @@ constexpr int kChunk = 128;   // edges per chunk (one unrolled batch of a warp)
 constexpr int kUnroll = 4;    // rounds of 32 edges issued together
 
 struct LevelCounters {
-  unsigned long long qc;  // low 32 bits: vertices in the queue (degree <= kBigDeg);
-                          // high 32 bits: entries in the chunk list
-  unsigned nbig;          // vertices in the chunk list
+  unsigned long long bc;  // low 32 bits: vertices in the big list (degree > kBigDeg);
+                          // high 32 bits: their chunks
+  unsigned q;             // vertices in the queue (degree <= kBigDeg)
   unsigned nimpl;         // vertices of an implicit frontier (BFS pull: depth == level), not queued
   unsigned long long edges;  // sum of out-degrees of the frontier
 };
 
-__device__ __forceinline__ unsigned qc_queue(unsigned long long qc) { return (unsigned)qc; }
-__device__ __forceinline__ unsigned qc_chunks(unsigned long long qc) { return (unsigned)(qc >> 32); }
+__device__ __forceinline__ unsigned bc_big(unsigned long long bc) { return (unsigned)bc; }
+__device__ __forceinline__ unsigned bc_chunks(unsigned long long bc) { return (unsigned)(bc >> 32); }
 
-// Per-lane tallies of a warp's appends during one level, flushed once.
+// Per-lane tally of a warp's appends during one level, flushed once.
 struct DiscoverAcc {
-  unsigned nbig = 0;
   unsigned long long edges = 0;
 };
 
 __device__ __forceinline__ void flush_acc(DiscoverAcc &acc, LevelCounters *nxt) {
-  const unsigned b = warp_sum(acc.nbig);
   const unsigned long long e = warp_sum(acc.edges);
-  if (lane_id() == 0) {
-    if (b) atomicAdd(&nxt->nbig, b);
-    if (e) atomicAdd(&nxt->edges, e);
-  }
+  if (lane_id() == 0 && e) atomicAdd(&nxt->edges, e);
   acc = DiscoverAcc{};
+}
+
+// Position in the big list (entries (vertex, first chunk), first chunks
+// increasing) of the vertex that owns chunk c: the largest i with
+// big[i].y <= c.  Warp-collective: 32 pivots per step, so a list of n
+// entries takes ceil(log32 n) dependent loads.
+__device__ __forceinline__ int big_search(const int2 *big, int nbig, unsigned c) {
+  const int lane = lane_id();
+  int lo = 0, hi = nbig;  // big[lo].y <= c < big[hi].y (big[nbig].y = infinity)
+  while (hi - lo > 1) {
+    const long long span = hi - lo;
+    const int piv = lo + (int)(span * lane / 32);
+    const bool le = (unsigned)__ldcg(&big[piv].y) <= c;
+    const unsigned b = __ballot_sync(kFull, le);  // lane 0 (piv == lo) is always set
+    const int last = 31 - __clz(b);
+    const int nlo = lo + (int)(span * last / 32);
+    const int nhi = last == 31 ? hi : lo + (int)(span * (last + 1) / 32);
+    lo = nlo;
+    hi = max(nhi, nlo + 1);
+  }
+  return lo;
 }
 
 // Capacity of a chunk list for a graph with nnz edges: every big vertex has
@@ -66,11 +85,11 @@ inline size_t chunk_capacity(long long nnz) {
 
 // Called by all 32 lanes with N candidates per lane; candidate r of a lane
 // joins the next frontier when found[r].  One atomic per warp reserves the
-// queue slots and chunk entries of all N x 32 candidates; the big-vertex and
-// edge tallies go to acc (kCountEdges = false leaves the edge tally alone).
+// queue slots of all N x 32 candidates, one the big-list entries and their
+// chunks; the edge tally goes to acc (kCountEdges = false leaves it alone).
 template <int N, bool kCountEdges = true>
 __device__ __forceinline__ void discover_n(const bool (&found)[N], const int (&u)[N],
-                                           const int *__restrict__ ptr, int *qout, int2 *cout,
+                                           const int *__restrict__ ptr, int *qout, int2 *bout,
                                            LevelCounters *nxt, DiscoverAcc &acc) {
   const int lane = lane_id();
   int deg[N];
@@ -86,58 +105,75 @@ __device__ __forceinline__ void discover_n(const bool (&found)[N], const int (&u
     nchunk += big ? (deg[r] + kChunk - 1) / kChunk : 0;
     edges += (unsigned long long)deg[r];
   }
-  acc.nbig += (unsigned)nbig;
   if (kCountEdges) acc.edges += edges;
   const int qincl = warp_incl_scan(nsmall);
-  const int cincl = warp_incl_scan(nchunk);
   const unsigned qtot = (unsigned)__shfl_sync(kFull, qincl, 31);
-  const unsigned ctot = (unsigned)__shfl_sync(kFull, cincl, 31);
-  if ((qtot | ctot) == 0u) return;
-  unsigned long long base = 0;
-  if (lane == 31) base = atomicAdd(&nxt->qc, ((unsigned long long)ctot << 32) | qtot);
-  base = __shfl_sync(kFull, base, 31);
-  // queue slots
+  const unsigned bany = __ballot_sync(kFull, nbig > 0);
+  int bincl = 0, cincl = 0;
+  unsigned btot = 0, ctot = 0;
+  if (bany) {
+    bincl = warp_incl_scan(nbig);
+    cincl = warp_incl_scan(nchunk);
+    btot = (unsigned)__shfl_sync(kFull, bincl, 31);
+    ctot = (unsigned)__shfl_sync(kFull, cincl, 31);
+  }
+  unsigned qbase = 0;
+  unsigned long long bbase = 0;
+  if (lane == 31) {
+    if (qtot) qbase = atomicAdd(&nxt->q, qtot);
+    if (btot) bbase = atomicAdd(&nxt->bc, ((unsigned long long)ctot << 32) | btot);
+  }
   if (qtot) {
-    unsigned qbase = qc_queue(base) + (unsigned)(qincl - nsmall);
+    unsigned qb = __shfl_sync(kFull, qbase, 31) + (unsigned)(qincl - nsmall);
 #pragma unroll
     for (int r = 0; r < N; ++r)
-      if (found[r] && deg[r] <= kBigDeg) qout[qbase++] = u[r];
+      if (found[r] && deg[r] <= kBigDeg) qout[qb++] = u[r];
   }
-  // chunk entries of big vertices, written cooperatively
-  if (ctot) {
-    unsigned cbase = qc_chunks(base) + (unsigned)(cincl - nchunk);
+  if (bany) {
+    bbase = __shfl_sync(kFull, bbase, 31);
+    unsigned bi = bc_big(bbase) + (unsigned)(bincl - nbig);
+    unsigned ci = bc_chunks(bbase) + (unsigned)(cincl - nchunk);
 #pragma unroll
-    for (int r = 0; r < N; ++r) {
-      bool big = found[r] && deg[r] > kBigDeg;
-      int nch = big ? (deg[r] + kChunk - 1) / kChunk : 0;
-      unsigned rm = __ballot_sync(kFull, big);
-      while (rm) {
-        int j = __ffs(rm) - 1;
-        rm &= rm - 1;
-        int uj = __shfl_sync(kFull, u[r], j);
-        unsigned bj = __shfl_sync(kFull, cbase, j);
-        int nj = __shfl_sync(kFull, nch, j);
-        for (int c = lane; c < nj; c += 32) cout[bj + c] = make_int2(uj, c);
+    for (int r = 0; r < N; ++r)
+      if (found[r] && deg[r] > kBigDeg) {
+        bout[bi++] = make_int2(u[r], (int)ci);
+        ci += (unsigned)((deg[r] + kChunk - 1) / kChunk);
       }
-      cbase += (unsigned)nch;
-    }
   }
+}
+
+// Appends up to N candidates per lane to a plain vertex list (no chunking),
+// one atomic per warp.
+template <int N>
+__device__ __forceinline__ void append_plain(const bool (&f)[N], const int (&u)[N], int *list,
+                                             unsigned *count) {
+  const int lane = lane_id();
+  int n = 0;
+#pragma unroll
+  for (int r = 0; r < N; ++r) n += f[r] ? 1 : 0;
+  const int incl = warp_incl_scan(n);
+  const unsigned tot = (unsigned)__shfl_sync(kFull, incl, 31);
+  if (tot == 0u) return;
+  unsigned base = 0;
+  if (lane == 31) base = atomicAdd(count, tot);
+  base = __shfl_sync(kFull, base, 31) + (unsigned)(incl - n);
+#pragma unroll
+  for (int r = 0; r < N; ++r)
+    if (f[r]) list[base++] = u[r];
 }
 
 // Seeds a frontier of one vertex (used by the init kernels; block-wide).
 __device__ __forceinline__ void seed_frontier(int src, const int *__restrict__ ptr, int *queue,
-                                              int2 *chunks, LevelCounters *c) {
-  int deg = __ldg(ptr + src + 1) - __ldg(ptr + src);
-  int nch = deg > kBigDeg ? (deg + kChunk - 1) / kChunk : 0;
-  for (int j = threadIdx.x; j < nch; j += blockDim.x) chunks[j] = make_int2(src, j);
+                                              int2 *big, LevelCounters *c) {
   if (threadIdx.x == 0) {
+    const int deg = __ldg(ptr + src + 1) - __ldg(ptr + src);
     *c = LevelCounters{0ull, 0, 0, 0ull};
-    if (nch) {
-      c->qc = (unsigned long long)nch << 32;
-      c->nbig = 1;
+    if (deg > kBigDeg) {
+      big[0] = make_int2(src, 0);
+      c->bc = ((unsigned long long)((deg + kChunk - 1) / kChunk) << 32) | 1ull;
     } else {
       queue[0] = src;
-      c->qc = 1ull;
+      c->q = 1;
     }
     c->edges = (unsigned long long)deg;
   }
@@ -145,13 +181,18 @@ __device__ __forceinline__ void seed_frontier(int src, const int *__restrict__ p
 
 // Push expansion of (qin[0..nq), cin[0..nch)).  `load(v)` gives the 32-bit
 // payload of a source vertex (e.g. its distance), broadcast to its edges.
+// visit.commit returns a class: 0 = nothing, 1 = joins the next frontier,
+// 2 (visitors with kTwoWay) = goes to the visitor's secondary list
+// (visit.far_list / visit.far_count, appended without chunking), 3 = a
+// secondary-list member already listed; visit.note_far sees the classes
+// and the visitor's aux values of each batch.
 template <typename Load, typename Visit>
 __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
                                             const int *__restrict__ ind, const int *qin,
-                                            unsigned nq, const int2 *cin, unsigned nch,
-                                            int *qout, int2 *cout, LevelCounters *nxt,
-                                            int gwarp, int nwarps, Load load, Visit &visit,
-                                            unsigned long long *walked = nullptr) {
+                                            unsigned nq, const int2 *bin, unsigned nbig,
+                                            unsigned nch, int *qout, int2 *bout,
+                                            LevelCounters *nxt, int gwarp, int nwarps, Load load,
+                                            Visit &visit, unsigned long long *walked = nullptr) {
   const int lane = lane_id();
   unsigned long long nwalk = 0;
   DiscoverAcc acc;
@@ -187,14 +228,39 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
 #pragma unroll
       for (int r = 0; r < kUnroll; ++r)
         ok[r] = uu[r] >= 0 && visit.check(pp[r], kk[r], uu[r], aux[r]);
-      bool f[kUnroll];
+      bool f[kUnroll], g[kUnroll];
+      int cls[kUnroll];
 #pragma unroll
-      for (int r = 0; r < kUnroll; ++r) f[r] = ok[r] && visit.commit(pp[r], kk[r], uu[r], aux[r]);
-      discover_n<kUnroll>(f, uu, ptr, qout, cout, nxt, acc);
+      for (int r = 0; r < kUnroll; ++r) {
+        cls[r] = ok[r] ? (int)visit.commit(pp[r], kk[r], uu[r], aux[r]) : 0;
+        f[r] = cls[r] == 1;
+        g[r] = cls[r] == 2;
+      }
+      discover_n<kUnroll>(f, uu, ptr, qout, bout, nxt, acc);
+      if constexpr (Visit::kTwoWay) {
+        append_plain<kUnroll>(g, uu, visit.far_list, visit.far_count);
+        visit.note_far(cls, aux);
+      }
     }
   }
-  for (unsigned c = (unsigned)gwarp; c < nch; c += (unsigned)nwarps) {
-    int2 ch = __ldcg(cin + c);
+  // chunks of the big vertices: warp w takes the contiguous range
+  // [w * per, (w + 1) * per), finds the vertex of its first chunk and walks on
+  const unsigned per = (nch + (unsigned)nwarps - 1) / (unsigned)nwarps;
+  const unsigned c_beg = (unsigned)gwarp * per, c_end = min(c_beg + per, nch);
+  int bi = c_beg < c_end ? big_search(bin, (int)nbig, c_beg) : 0;
+  int2 bcur = make_int2(0, 0);
+  unsigned bnext = 0;
+  if (c_beg < c_end) {
+    bcur = __ldcg(bin + bi);
+    bnext = bi + 1 < (int)nbig ? (unsigned)__ldcg(&bin[bi + 1].y) : 0xffffffffu;
+  }
+  for (unsigned c = c_beg; c < c_end; ++c) {
+    while (c >= bnext) {
+      ++bi;
+      bcur = __ldcg(bin + bi);
+      bnext = bi + 1 < (int)nbig ? (unsigned)__ldcg(&bin[bi + 1].y) : 0xffffffffu;
+    }
+    const int2 ch = make_int2(bcur.x, (int)(c - (unsigned)bcur.y));
     int s = __ldg(ptr + ch.x) + ch.y * kChunk;
     int e = min(s + kChunk, __ldg(ptr + ch.x + 1));
     nwalk += (unsigned long long)(e - s);
@@ -211,11 +277,19 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
 #pragma unroll
       for (int r = 0; r < kUnroll; ++r)
         ok[r] = uu[r] >= 0 && visit.check(pay, k0 + r * 32 + lane, uu[r], aux[r]);
-      bool f[kUnroll];
+      bool f[kUnroll], g[kUnroll];
+      int cls[kUnroll];
 #pragma unroll
-      for (int r = 0; r < kUnroll; ++r)
-        f[r] = ok[r] && visit.commit(pay, k0 + r * 32 + lane, uu[r], aux[r]);
-      discover_n<kUnroll>(f, uu, ptr, qout, cout, nxt, acc);
+      for (int r = 0; r < kUnroll; ++r) {
+        cls[r] = ok[r] ? (int)visit.commit(pay, k0 + r * 32 + lane, uu[r], aux[r]) : 0;
+        f[r] = cls[r] == 1;
+        g[r] = cls[r] == 2;
+      }
+      discover_n<kUnroll>(f, uu, ptr, qout, bout, nxt, acc);
+      if constexpr (Visit::kTwoWay) {
+        append_plain<kUnroll>(g, uu, visit.far_list, visit.far_count);
+        visit.note_far(cls, aux);
+      }
     }
   }
   flush_acc(acc, nxt);

@@ -35,7 +35,7 @@ constexpr int kUndecided = -1, kOut = 0, kIn = 1, kJoin = 2;
 
 struct MisState {
   unsigned q[3];  // queue lengths, rotating
-  unsigned bar[2];
+  alignas(8) unsigned bar[2];  // grid-barrier arrival counter (64-bit)
   int err;
   int rounds;
 };

@@ -16,8 +16,17 @@
 //     that arrive are admitted into the other slot and launched right away,
 //     so their work is queued behind (and its result copies overlap) the
 //     running batch instead of waiting for it to return to the host.
-// Each query's result row is copied back into the caller's host buffer and
-// its latency (submit -> result in host memory) is recorded.
+// Each query's result row is copied into the caller's host buffer, or into
+// its device buffer (or dropped, for load tests), and its latency (submit ->
+// result in host / device memory) is recorded.  MIS priorities (mt19937 of
+// the query's seed) are generated once per (graph, seed) and kept on the
+// device.
+//
+// apspie_server_replay drives the server with a timed query stream (open
+// loop: each query is submitted at its scheduled arrival time, and its
+// latency counts from that time); apspie_server_replay_plain runs the same
+// stream one query at a time through the single-source kernels, for
+// comparison.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -44,6 +53,7 @@ struct Request {
   int type, graph, source;
   uint32_t seed;
   void *h_result;
+  int32_t *d_result = nullptr;
   Clock::time_point t_submit;
   double latency_ms = 0;
   int status = APSPIE_OK;
@@ -69,8 +79,6 @@ struct Slot {
   size_t d_bytes = 0;
   void *h_stage = nullptr;
   size_t h_bytes = 0;
-  uint32_t *d_prio = nullptr;  // MIS priorities
-  size_t prio_bytes = 0;
   std::vector<Request *> reqs;
   bool busy = false;
   int launch_status = APSPIE_OK;
@@ -93,6 +101,9 @@ struct apspie_server {
   bool stop = false;
   Slot slots[2];
   int max_pending = 1 << 20;
+  // MIS priorities per (graph, seed), on the device
+  std::mutex prio_mu;
+  std::map<std::pair<int, uint32_t>, uint32_t *> prio_cache;
   // statistics
   uint64_t batches = 0, completed = 0, launched_jobs = 0;
   std::vector<double> latencies;
@@ -140,6 +151,39 @@ bool ensure_host(void **p, size_t *have, size_t want) {
   }
   *have = w;
   return true;
+}
+
+// Device priorities of an MIS query: mt19937(seed) for the graph's vertices,
+// generated on the host and uploaded on `stream` the first time.
+int get_prio(apspie_server *s, int graph, uint32_t seed, cudaStream_t stream, uint32_t **out) {
+  std::lock_guard<std::mutex> lock(s->prio_mu);
+  auto key = std::make_pair(graph, seed);
+  auto it = s->prio_cache.find(key);
+  if (it != s->prio_cache.end()) {
+    *out = it->second;
+    return APSPIE_OK;
+  }
+  const size_t m = (size_t)s->graphs[graph].m;
+  uint32_t *d = nullptr, *h = nullptr;
+  if (cudaMalloc(&d, 4 * m) != cudaSuccess || cudaMallocHost(&h, 4 * m) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(d);
+    return APSPIE_ERR_OOM;
+  }
+  int st = apspie_mt19937_fill_host(seed, (int64_t)m, h);
+  if (st == APSPIE_OK && (cudaMemcpyAsync(d, h, 4 * m, cudaMemcpyHostToDevice, stream) != cudaSuccess ||
+                          cudaStreamSynchronize(stream) != cudaSuccess)) {
+    cudaGetLastError();
+    st = APSPIE_ERR_CUDA;
+  }
+  cudaFreeHost(h);
+  if (st != APSPIE_OK) {
+    cudaFree(d);
+    return st;
+  }
+  s->prio_cache[key] = d;
+  *out = d;
+  return APSPIE_OK;
 }
 
 // Completes the requests of a finished slot: results to the callers'
@@ -245,23 +289,26 @@ int launch_slot(apspie_server *s, Slot &sl) {
   for (Request *r : mis) {
     if (st != APSPIE_OK) break;
     const GraphEntry &g = s->graphs[r->graph];
-    size_t pb = 4 * (size_t)g.m;
-    if (!ensure_device((void **)&sl.d_prio, &sl.prio_bytes, pb)) {
-      st = APSPIE_ERR_OOM;
-      break;
-    }
-    // priorities via the host MT19937 into the staging row, then upload
-    uint32_t *h = (uint32_t *)((char *)sl.h_stage + r->offset);
-    cudaStreamSynchronize(sl.stream);  // the staging row may be in a pending copy
-    apspie_mt19937_fill_host(r->seed, g.m, h);
-    cudaMemcpyAsync(sl.d_prio, h, pb, cudaMemcpyHostToDevice, sl.stream);
-    st = apspie_mis(sl.ctx, g.nnz, g.m, g.ptr, g.ind, sl.d_prio,
-                    (int32_t *)((char *)sl.d_out + r->offset), 1.0f);
+    uint32_t *prio = nullptr;
+    st = get_prio(s, r->graph, r->seed, sl.stream, &prio);
+    if (st == APSPIE_OK)
+      st = apspie_mis(sl.ctx, g.nnz, g.m, g.ptr, g.ind, prio,
+                      (int32_t *)((char *)sl.d_out + r->offset), 1.0f);
   }
-  if (st == APSPIE_OK)
-    if (cudaMemcpyAsync(sl.h_stage, sl.d_out, off, cudaMemcpyDeviceToHost, sl.stream) !=
-        cudaSuccess)
-      st = APSPIE_ERR_CUDA;
+  // results to the callers: host rows through the staging buffer, device
+  // rows directly; a query with neither only has its latency recorded
+  for (Request *r : sl.reqs) {
+    if (st != APSPIE_OK) break;
+    const size_t bytes = 4 * (size_t)s->graphs[r->graph].m;
+    cudaError_t e = cudaSuccess;
+    if (r->h_result)
+      e = cudaMemcpyAsync((char *)sl.h_stage + r->offset, (char *)sl.d_out + r->offset, bytes,
+                          cudaMemcpyDeviceToHost, sl.stream);
+    if (e == cudaSuccess && r->d_result)
+      e = cudaMemcpyAsync(r->d_result, (char *)sl.d_out + r->offset, bytes,
+                          cudaMemcpyDeviceToDevice, sl.stream);
+    if (e != cudaSuccess) st = APSPIE_ERR_CUDA;
+  }
   cudaEventRecord(sl.done, sl.stream);
   return st;
 }
@@ -361,15 +408,25 @@ int apspie_server_add_graph(apspie_server_t s, int m, int64_t nnz, const int *d_
   return APSPIE_OK;
 }
 
-int apspie_server_submit(apspie_server_t s, int type, int graph, int source, uint32_t seed,
-                         void *h_result, uint64_t *req_id) {
-  if (!s || !req_id || type < 0 || type > 2) return APSPIE_ERR_INVALID;
-  std::lock_guard<std::mutex> lock(s->mu);
-  if (s->stop) return APSPIE_ERR_INVALID;
+}  // extern "C"
+
+namespace {
+
+int check_query(apspie_server *s, int type, int graph, int source) {
+  if (type < 0 || type > 2) return APSPIE_ERR_INVALID;
   if (graph < 0 || graph >= (int)s->graphs.size()) return APSPIE_ERR_INVALID;
   const GraphEntry &g = s->graphs[graph];
   if (type != 2 && (source < 0 || source >= g.m)) return APSPIE_ERR_INVALID;
   if (type == 1 && !g.w) return APSPIE_ERR_INVALID;
+  return APSPIE_OK;
+}
+
+// Queues one query (caller holds s->mu).
+int enqueue_locked(apspie_server *s, int type, int graph, int source, uint32_t seed,
+                   void *h_result, int32_t *d_result, Clock::time_point t_submit, Request **out) {
+  if (s->stop) return APSPIE_ERR_INVALID;
+  int st = check_query(s, type, graph, source);
+  if (st) return st;
   if ((int)s->pending.size() >= s->max_pending) return APSPIE_ERR_BUSY;
   auto *r = new (std::nothrow) Request();
   if (!r) return APSPIE_ERR_OOM;
@@ -379,13 +436,145 @@ int apspie_server_submit(apspie_server_t s, int type, int graph, int source, uin
   r->source = source;
   r->seed = seed;
   r->h_result = h_result;
-  r->t_submit = Clock::now();
+  r->d_result = d_result;
+  r->t_submit = t_submit;
   r->bytes = request_bytes(s, type, graph);
   s->pending.push_back(r);
   s->reqs[r->id] = r;
-  *req_id = r->id;
+  *out = r;
   s->cv.notify_all();
   return APSPIE_OK;
+}
+
+void spin_until(Clock::time_point t) {
+  while (Clock::now() < t) std::this_thread::yield();
+}
+
+}  // namespace
+
+extern "C" {
+
+int apspie_server_submit(apspie_server_t s, int type, int graph, int source, uint32_t seed,
+                         void *h_result, uint64_t *req_id) {
+  if (!s || !req_id) return APSPIE_ERR_INVALID;
+  std::lock_guard<std::mutex> lock(s->mu);
+  Request *r = nullptr;
+  int st = enqueue_locked(s, type, graph, source, seed, h_result, nullptr, Clock::now(), &r);
+  if (st == APSPIE_OK) *req_id = r->id;
+  return st;
+}
+
+int apspie_server_submit_device(apspie_server_t s, int type, int graph, int source,
+                                uint32_t seed, int32_t *d_result, uint64_t *req_id) {
+  if (!s || !req_id) return APSPIE_ERR_INVALID;
+  std::lock_guard<std::mutex> lock(s->mu);
+  Request *r = nullptr;
+  int st = enqueue_locked(s, type, graph, source, seed, nullptr, d_result, Clock::now(), &r);
+  if (st == APSPIE_OK) *req_id = r->id;
+  return st;
+}
+
+int apspie_server_replay(apspie_server_t s, int n, const apspie_query *q, double *lat_ms,
+                         double *wall_ms) {
+  if (!s || n < 0 || (n > 0 && (!q || !lat_ms))) return APSPIE_ERR_INVALID;
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    for (int i = 0; i < n; ++i)
+      if (check_query(s, q[i].type, q[i].graph, q[i].source) || q[i].t_us < 0 ||
+          (i > 0 && q[i].t_us < q[i - 1].t_us))
+        return APSPIE_ERR_INVALID;
+  }
+  std::vector<Request *> rs((size_t)n, nullptr);
+  const Clock::time_point t0 = Clock::now() + std::chrono::milliseconds(1);
+  int st = APSPIE_OK;
+  for (int i = 0; i < n && st == APSPIE_OK; ++i) {
+    const Clock::time_point at =
+        t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double, std::micro>(q[i].t_us));
+    spin_until(at);
+    std::lock_guard<std::mutex> lock(s->mu);
+    // the pending queue is large; a full one is waited out, the query keeps
+    // its scheduled arrival time
+    while ((st = enqueue_locked(s, q[i].type, q[i].graph, q[i].source, q[i].seed, nullptr,
+                                nullptr, at, &rs[i])) == APSPIE_ERR_BUSY) {
+      s->mu.unlock();
+      std::this_thread::sleep_for(std::chrono::microseconds(100));
+      s->mu.lock();
+    }
+  }
+  double last = 0;
+  std::unique_lock<std::mutex> lock(s->mu);
+  for (int i = 0; i < n; ++i) {
+    Request *r = rs[i];
+    if (!r) {
+      lat_ms[i] = -1;
+      continue;
+    }
+    if (!s->cv.wait_for(lock, std::chrono::seconds(600), [&] { return r->done; })) {
+      st = APSPIE_ERR_TIMEOUT;
+      lat_ms[i] = -1;
+      continue;  // left in the table; the server frees it on destroy
+    }
+    if (r->status != APSPIE_OK && st == APSPIE_OK) st = r->status;
+    lat_ms[i] = r->latency_ms;
+    last = std::max(last, std::chrono::duration<double, std::milli>(r->t_submit - t0).count() +
+                              r->latency_ms);
+    s->reqs.erase(r->id);
+    delete r;
+  }
+  if (wall_ms) *wall_ms = last;
+  return st;
+}
+
+int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q, double *lat_ms,
+                               double *wall_ms) {
+  if (!s || n < 0 || (n > 0 && (!q || !lat_ms))) return APSPIE_ERR_INVALID;
+  int maxm = 0;
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    for (int i = 0; i < n; ++i)
+      if (check_query(s, q[i].type, q[i].graph, q[i].source) || q[i].t_us < 0 ||
+          (i > 0 && q[i].t_us < q[i - 1].t_us))
+        return APSPIE_ERR_INVALID;
+    for (const GraphEntry &g : s->graphs) maxm = std::max(maxm, g.m);
+  }
+  if (cudaSetDevice(s->device) != cudaSuccess) return APSPIE_ERR_CUDA;
+  cudaStream_t stream = nullptr;
+  apspie_ctx ctx = nullptr;
+  int32_t *row = nullptr;
+  if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&row, 4 * (size_t)std::max(maxm, 1)) != cudaSuccess) {
+    cudaGetLastError();
+    if (stream) cudaStreamDestroy(stream);
+    return APSPIE_ERR_OOM;
+  }
+  int st = apspie_ctx_create(s->device, stream, &ctx);
+  const Clock::time_point t0 = Clock::now() + std::chrono::milliseconds(1);
+  double last = 0;
+  for (int i = 0; i < n && st == APSPIE_OK; ++i) {
+    const Clock::time_point at =
+        t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double, std::micro>(q[i].t_us));
+    spin_until(at);  // returns at once when the previous query ran late
+    const GraphEntry &g = s->graphs[q[i].graph];
+    if (q[i].type == 0) {
+      const int *tp = g.symmetric ? g.ptr : g.tptr, *ti = g.symmetric ? g.ind : g.tind;
+      st = apspie_bfs(ctx, q[i].source, g.nnz, g.m, g.ptr, g.ind, tp, ti, row, 0);
+    } else if (q[i].type == 1) {
+      st = apspie_sssp_u32(ctx, q[i].source, g.nnz, g.m, g.ptr, g.ind, g.w, (uint32_t *)row, 0);
+    } else {
+      uint32_t *prio = nullptr;
+      st = get_prio(s, q[i].graph, q[i].seed, stream, &prio);
+      if (st == APSPIE_OK) st = apspie_mis(ctx, g.nnz, g.m, g.ptr, g.ind, prio, row, 1.0f);
+    }
+    if (st == APSPIE_OK && cudaStreamSynchronize(stream) != cudaSuccess) st = APSPIE_ERR_CUDA;
+    const double l = std::chrono::duration<double, std::milli>(Clock::now() - at).count();
+    lat_ms[i] = l;
+    last = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+  }
+  if (ctx) apspie_ctx_destroy(ctx);
+  cudaFree(row);
+  cudaStreamDestroy(stream);
+  if (wall_ms) *wall_ms = last;
+  return st;
 }
 
 int apspie_server_poll(apspie_server_t s, uint64_t req_id, int *done, double *latency_ms) {
@@ -466,9 +655,9 @@ int apspie_server_destroy(apspie_server_t s) {
     if (sl.done) cudaEventDestroy(sl.done);
     if (sl.stream) cudaStreamDestroy(sl.stream);
     cudaFree(sl.d_out);
-    cudaFree(sl.d_prio);
     if (sl.h_stage) cudaFreeHost(sl.h_stage);
   }
+  for (auto &kv : s->prio_cache) cudaFree(kv.second);
   for (auto &kv : s->reqs) delete kv.second;
   delete s;
   return APSPIE_OK;

@@ -10,6 +10,16 @@
 // distance word, so no (row, value) pairs are materialised or sorted.  A
 // vertex enters the next frontier once per round (stamp array).
 //
+// Near-far scheduling (Davidson, Baxter, Garland & Owens, "Work-Efficient
+// Parallel GPU Methods for Single-Source Shortest Paths", IPDPS 2014): with a
+// threshold T, only vertices whose new distance is below T join the next
+// frontier ("near"); the others go to a far list.  When the near frontier
+// runs dry T grows by delta and the far list is split again.  Vertices are
+// then mostly expanded once, with their final distance, instead of once per
+// improvement.  delta = 0 disables it (T = infinity: plain frontier
+// Bellman-Ford, fewer rounds, more relaxations -- better on high-diameter
+// graphs).  The schedule only changes the order of relaxations.
+//
 // Distances are kept as 32-bit words: uint32 sums for integer weights, and
 // the IEEE bit pattern for float weights -- non-negative floats order like
 // their bit patterns, so atomicMin on the word is min on the value.  Each
@@ -20,6 +30,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 
 #include "common.cuh"
 #include "context.h"
@@ -32,9 +43,13 @@ constexpr int kSsspThreads = 512;
 
 struct SsspState {
   LevelCounters c[3];
-  unsigned bar[2];
+  unsigned far_count[3];  // far lists rotate by phase
+  unsigned far_min[3];    // least distance sent to each far list
+  alignas(8) unsigned bar[2];  // grid-barrier arrival counter (64-bit)
   int err;
   int rounds;
+  int phases;
+  int pad;
   unsigned long long relaxations;  // edges scanned over all rounds
   unsigned long long reached;
   unsigned long long edges;        // sum of out-degrees of reached vertices
@@ -50,6 +65,11 @@ struct Arith<uint32_t> {
     unsigned s = d + w;
     return (s < d || s == kInf) ? kInf - 1u : s;  // saturate below "unreached"
   }
+  // threshold + delta (delta given as the weight type's bits), saturating at kInf
+  __device__ __forceinline__ static unsigned step(unsigned t, unsigned delta) {
+    unsigned s = t + delta;
+    return s < t ? kInf : s;
+  }
 };
 
 template <>
@@ -58,40 +78,68 @@ struct Arith<float> {
   __device__ __forceinline__ static unsigned add(unsigned d, float w) {
     return __float_as_uint(__fadd_rn(__uint_as_float(d), w));
   }
+  __device__ __forceinline__ static unsigned step(unsigned t, unsigned delta) {
+    return __float_as_uint(__fadd_rn(__uint_as_float(t), __uint_as_float(delta)));
+  }
 };
 
-// Push visitor: relax (u, w[k]) with the source's distance du as payload.
+// Push visitor: relax (u, w[k]) with the tail's distance du as payload.  An
+// improved target below the threshold joins the next frontier (class 1,
+// once per round by the stamp); one at or above it goes to the far list
+// (class 2, once per phase by the far stamp).
 template <typename W>
 struct SsspVisit {
+  static constexpr bool kTwoWay = true;
   const W *__restrict__ w;
   unsigned *dist;
   int *stamp;
-  int round;
+  int *fstamp;
+  int round, phase;
+  unsigned thresh;
+  int *far_list;
+  unsigned *far_count;
+  unsigned *far_min;
   __device__ __forceinline__ bool check(unsigned du, int k, int u, unsigned &nd) const {
     nd = Arith<W>::add(du, __ldg(w + k));
     return nd < __ldcg(dist + u);
   }
-  __device__ __forceinline__ bool commit(unsigned, int, int u, unsigned nd) const {
-    if (nd >= atomicMin(dist + u, nd)) return false;
-    return atomicExch(stamp + u, round) != round;
+  __device__ __forceinline__ int commit(unsigned, int, int u, unsigned nd) const {
+    if (nd >= atomicMin(dist + u, nd)) return 0;
+    if (nd < thresh) return atomicExch(stamp + u, round) != round ? 1 : 0;
+    return atomicExch(fstamp + u, phase) != phase ? 2 : 3;  // 3: far, already listed
+  }
+  // least distance sent far by this warp's batch (classes 2 and 3), one atomic
+  template <int N>
+  __device__ __forceinline__ void note_far(const int (&cls)[N], const unsigned (&nd)[N]) const {
+    unsigned lo = Arith<W>::kInf;
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+      if (cls[r] >= 2) lo = min(lo, nd[r]);
+    lo = __reduce_min_sync(kFull, lo);
+    if (lo != Arith<W>::kInf && lane_id() == 0) atomicMin(far_min, lo);
   }
 };
 
 template <typename W>
-__global__ void sssp_init(int m, int src, unsigned *dist, int *stamp, const int *__restrict__ ptr,
-                          int *queue, int2 *chunks, SsspState *st) {
+__global__ void sssp_init(int m, int src, unsigned *dist, int *stamp, int *fstamp, unsigned *xd,
+                          const int *__restrict__ ptr, int *queue, int2 *chunks, SsspState *st) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < m; v += gridDim.x * blockDim.x) {
     dist[v] = (v == src) ? 0u : Arith<W>::kInf;
     stamp[v] = -1;
+    fstamp[v] = -1;
+    xd[v] = Arith<W>::kInf;
   }
   if (blockIdx.x == 0) {
     seed_frontier(src, ptr, queue, chunks, &st->c[0]);
     if (threadIdx.x == 0) {
       st->c[1] = LevelCounters{0ull, 0, 0, 0ull};
       st->c[2] = LevelCounters{0ull, 0, 0, 0ull};
+      st->far_count[0] = st->far_count[1] = st->far_count[2] = 0;
+      st->far_min[0] = st->far_min[1] = st->far_min[2] = Arith<W>::kInf;
       st->bar[0] = st->bar[1] = 0;
       st->err = 0;
       st->rounds = 0;
+      st->phases = 0;
       st->relaxations = 0;
       st->reached = 0;
       st->edges = 0;
@@ -103,36 +151,91 @@ template <typename W>
 __global__ void __launch_bounds__(kSsspThreads, 3)
 sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
                 const W *__restrict__ w, unsigned *dist, int *stamp, int *qa, int *qb, int2 *ca,
-                int2 *cb, SsspState *st, int max_rounds) {
+                int2 *cb, SsspState *st, int max_rounds, int *fstamp, unsigned *xd, int *far0,
+                int *far1, int *far2, unsigned delta) {
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
-  __shared__ unsigned s_q, s_chunks;
+  const int lane = lane_id();
+  __shared__ unsigned s_q, s_chunks, s_nbig, s_far;
   __shared__ unsigned long long s_edges;
   unsigned long long relax = 0;
+  // T = infinity without near-far; else the first phase covers [0, delta)
+  unsigned thresh = delta ? delta : Arith<W>::kInf;
+  int phase = 0;
   int r = 0;
   for (;; ++r) {
     LevelCounters *cur = &st->c[r % 3];
     LevelCounters *nxt = &st->c[(r + 1) % 3];
     LevelCounters *clr = &st->c[(r + 2) % 3];
     if (threadIdx.x == 0) {
-      const unsigned long long qc = __ldcg(&cur->qc);
-      s_q = qc_queue(qc);
-      s_chunks = qc_chunks(qc);
+      const unsigned long long bc = __ldcg(&cur->bc);
+      s_q = __ldcg(&cur->q);
+      s_chunks = bc_chunks(bc);
+      s_nbig = bc_big(bc);
       s_edges = __ldcg(&cur->edges);
+      s_far = __ldcg(&st->far_count[phase % 3]);
       if (blockIdx.x == 0) *clr = LevelCounters{0ull, 0, 0, 0ull};
     }
     __syncthreads();
     const unsigned nq = s_q, nch = s_chunks;
-    if (nq == 0 && nch == 0) break;
     if (max_rounds > 0 && r >= max_rounds) break;
+    int *qout = (r & 1) ? qa : qb;
+    int2 *cout = (r & 1) ? ca : cb;
+    if (nq == 0 && nch == 0) {
+      // near frontier empty: done, or open the next phase by splitting the
+      // far list of this one into the next near frontier and the next far list
+      const unsigned nfar = s_far;
+      if (nfar == 0) break;
+      int *fin = phase % 3 == 0 ? far0 : (phase % 3 == 1 ? far1 : far2);
+      // the next threshold: one step up, or one step above the least far
+      // distance when that is higher (skips empty ranges); it always grows
+      const unsigned fmin = __ldcg(&st->far_min[phase % 3]);
+      unsigned nt = Arith<W>::step(thresh, delta);
+      const unsigned nf = Arith<W>::step(fmin, delta);
+      nt = nf > nt ? nf : nt;
+      thresh = nt > thresh ? nt : Arith<W>::kInf;
+      ++phase;
+      int *fout = phase % 3 == 0 ? far0 : (phase % 3 == 1 ? far1 : far2);
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->far_count[(phase + 1) % 3] = 0;
+        st->far_min[(phase + 1) % 3] = Arith<W>::kInf;
+      }
+      DiscoverAcc acc;
+      for (unsigned base = (unsigned)gwarp * 32u; base < nfar; base += (unsigned)nwarps * 32u) {
+        const unsigned idx = base + lane;
+        const int u = idx < nfar ? __ldcg(fin + idx) : 0;
+        bool to_near[1] = {false}, keep[1] = {false};
+        if (idx < nfar) {
+          const unsigned d = __ldcg(dist + u);
+          // below the new threshold and not yet expanded with this distance
+          if (d < thresh) {
+            to_near[0] = d != __ldcg(xd + u) && atomicExch(stamp + u, r) != r;
+          } else {
+            keep[0] = atomicExch(fstamp + u, phase) != phase;
+            if (keep[0]) atomicMin(&st->far_min[phase % 3], d);
+          }
+        }
+        int uu[1] = {u};
+        discover_n<1>(to_near, uu, ptr, qout, cout, nxt, acc);
+        append_plain<1>(keep, uu, fout, &st->far_count[phase % 3]);
+      }
+      flush_acc(acc, nxt);
+      if (!grid_barrier(st->bar, &st->err)) return;
+      continue;
+    }
     relax += s_edges;
     int *qin = (r & 1) ? qb : qa;
-    int *qout = (r & 1) ? qa : qb;
     int2 *cin = (r & 1) ? cb : ca;
-    int2 *cout = (r & 1) ? ca : cb;
-    SsspVisit<W> vis{w, dist, stamp, r};
-    expand_push(ptr, ind, qin, nq, cin, nch, qout, cout, nxt, gwarp, nwarps,
-                [&](int v) { return __ldcg(dist + v); }, vis);
+    int *fout = phase % 3 == 0 ? far0 : (phase % 3 == 1 ? far1 : far2);
+    SsspVisit<W> vis{w,    dist,   stamp, fstamp, r, phase, thresh, fout, &st->far_count[phase % 3],
+                     &st->far_min[phase % 3]};
+    expand_push(ptr, ind, qin, nq, cin, s_nbig, nch, qout, cout, nxt, gwarp, nwarps,
+                [&](int v) {
+                  const unsigned d = __ldcg(dist + v);
+                  xd[v] = d;  // the distance v is expanded with
+                  return d;
+                },
+                vis);
     if (!grid_barrier(st->bar, &st->err)) return;
   }
   // reached vertices and their out-degrees (E_R)
@@ -150,6 +253,7 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->rounds = r;
+    st->phases = phase;
     st->relaxations = relax;
   }
 }
@@ -172,7 +276,7 @@ int sssp_grid(apspie_context *ctx) {
 
 template <typename W>
 int sssp_run(apspie_context *ctx, int src, int64_t nnz, int m, const int *d_ptr, const int *d_ind,
-             const W *d_w, unsigned *d_dist, int max_rounds) {
+             const W *d_w, unsigned *d_dist, int max_rounds, unsigned delta) {
   APSPIE_CHECK_CTX(ctx);
   if (m <= 0 || src < 0 || src >= m)
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_sssp: src %d outside [0,%d)", src, m);
@@ -187,16 +291,23 @@ int sssp_run(apspie_context *ctx, int src, int64_t nnz, int m, const int *d_ptr,
   auto *ca = (int2 *)workspace(ctx, kSlotSsspChunksA, sizeof(int2) * cap);
   auto *cb = (int2 *)workspace(ctx, kSlotSsspChunksB, sizeof(int2) * cap);
   auto *stamp = (int *)workspace(ctx, kSlotSsspStamp, sizeof(int) * (size_t)m);
-  if (!st || !qa || !qb || !ca || !cb || !stamp) return APSPIE_ERR_OOM;
+  // far stamps, expanded distances and three far lists of m entries
+  const size_t mm = ((size_t)m + 63) & ~size_t(63);
+  auto *nf = (int *)workspace(ctx, kSlotSsspNearFar, sizeof(int) * mm * 5);
+  if (!st || !qa || !qb || !ca || !cb || !stamp || !nf) return APSPIE_ERR_OOM;
+  int *fstamp = nf, *far0 = nf + 2 * mm, *far1 = nf + 3 * mm, *far2 = nf + 4 * mm;
+  unsigned *xd = (unsigned *)(nf + mm);
   ctx->sssp_state = st;
   int grid = sssp_grid<W>(ctx);
   if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_sssp: occupancy query failed");
   int init_grid = std::min((m + 255) / 256, ctx->num_sms * 8);
-  sssp_init<W><<<init_grid, 256, 0, ctx->stream>>>(m, src, d_dist, stamp, d_ptr, qa, ca, st);
+  sssp_init<W><<<init_grid, 256, 0, ctx->stream>>>(m, src, d_dist, stamp, fstamp, xd, d_ptr, qa,
+                                                   ca, st);
   int rc = check_launch(ctx, "sssp_init");
   if (rc) return rc;
   void *args[] = {&m,  (void *)&d_ptr, (void *)&d_ind, (void *)&d_w, &d_dist, &stamp,
-                  &qa, &qb,            &ca,            &cb,           &st,     &max_rounds};
+                  &qa, &qb,            &ca,            &cb,           &st,     &max_rounds,
+                  &fstamp, &xd, &far0, &far1, &far2, &delta};
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)sssp_persistent<W>, dim3(grid),
                                               dim3(kSsspThreads), args, 0, ctx->stream);
   if (e != cudaSuccess) return check_cuda(ctx, e, "sssp_persistent");
@@ -213,12 +324,26 @@ extern "C" {
 
 int apspie_sssp_u32(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
                     const int *d_ind, const uint32_t *d_w, uint32_t *d_dist, int max_rounds) {
-  return sssp_run<uint32_t>(ctx, src, nnz, m, d_ptr, d_ind, d_w, d_dist, max_rounds);
+  return sssp_run<uint32_t>(ctx, src, nnz, m, d_ptr, d_ind, d_w, d_dist, max_rounds,
+                            ctx->sssp_delta_u32);
 }
 
 int apspie_sssp_f32(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
                     const int *d_ind, const float *d_w, float *d_dist, int max_rounds) {
-  return sssp_run<float>(ctx, src, nnz, m, d_ptr, d_ind, d_w, (unsigned *)d_dist, max_rounds);
+  float df = ctx->sssp_delta_f32;
+  unsigned bits = 0;
+  std::memcpy(&bits, &df, sizeof(bits));
+  return sssp_run<float>(ctx, src, nnz, m, d_ptr, d_ind, d_w, (unsigned *)d_dist, max_rounds,
+                         df > 0.0f ? bits : 0u);
+}
+
+int apspie_sssp_set_params(apspie_ctx ctx, uint32_t delta_u32, float delta_f32) {
+  APSPIE_CHECK_CTX(ctx);
+  if (!(delta_f32 >= 0.0f) || delta_f32 > 3.0e38f)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_sssp_set_params: bad float delta");
+  ctx->sssp_delta_u32 = delta_u32;
+  ctx->sssp_delta_f32 = delta_f32;
+  return APSPIE_OK;
 }
 
 int apspie_sssp_get_stats(apspie_ctx ctx, apspie_sssp_stats *out) {
@@ -232,6 +357,7 @@ int apspie_sssp_get_stats(apspie_ctx ctx, apspie_sssp_stats *out) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return check_cuda(ctx, e, "apspie_sssp_get_stats");
   out->rounds = h->rounds;
+  out->phases = h->phases;
   out->vertices_reached = (int64_t)h->reached;
   out->edges_traversed = (int64_t)h->edges;
   out->relaxations = (int64_t)h->relaxations;

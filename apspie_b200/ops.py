@@ -146,8 +146,15 @@ def sssp(ctx: Context, g, src: int, dist=None, weights: str = "u32", max_rounds:
 def sssp_stats(ctx: Context) -> dict:
     s = SsspStats()
     check(lib.apspie_sssp_get_stats(ctx.handle, C.byref(s)), ctx.handle, "apspie_sssp_get_stats")
-    return {"rounds": s.rounds, "vertices_reached": s.vertices_reached,
+    return {"rounds": s.rounds, "phases": s.phases, "vertices_reached": s.vertices_reached,
             "edges_traversed": s.edges_traversed, "relaxations": s.relaxations}
+
+
+def sssp_set_params(ctx: Context, delta_u32: int = 0, delta_f32: float = 0.0) -> None:
+    """Near-far step of SSSP (0 = frontier Bellman-Ford); see
+    apspie_sssp_set_params."""
+    check(lib.apspie_sssp_set_params(ctx.handle, int(delta_u32), float(delta_f32)), ctx.handle,
+          "apspie_sssp_set_params")
 
 
 def mis(ctx: Context, g, prio, out=None, delta: float = 1.0):

@@ -11,6 +11,10 @@ from ._native import ApspieError, ServerStats, check, lib
 
 BFS, SSSP, MIS = 0, 1, 2
 
+# apspie_query (include/apspie.h)
+QUERY_DTYPE = np.dtype([("type", np.int32), ("graph", np.int32), ("source", np.int32),
+                        ("seed", np.uint32), ("t_us", np.float64)])
+
 
 class Server:
     def __init__(self, device: int = 0, budget_bytes: int = 120 << 30, max_batch: int = 256):
@@ -43,6 +47,33 @@ class Server:
               what="apspie_server_submit")
         self._live[rid.value] = out
         return rid.value
+
+    def submit_device(self, kind: int, graph: int, source: int = 0, seed: int = 0,
+                      out=None) -> int:
+        """Submit with the result written to the device tensor `out` (int32,
+        m entries), or dropped when out is None."""
+        if not 0 <= graph < len(self._graphs):
+            raise ApspieError(2, f"apspie_server_submit_device: unknown graph {graph}")
+        rid = C.c_uint64()
+        check(lib.apspie_server_submit_device(self._h, int(kind), int(graph), int(source),
+                                              int(seed),
+                                              C.c_void_p(0 if out is None else out.data_ptr()),
+                                              C.byref(rid)), what="apspie_server_submit_device")
+        self._live[rid.value] = out
+        return rid.value
+
+    def replay(self, queries, plain: bool = False):
+        """Open-loop replay of a timed query stream: `queries` is a structured
+        array with fields type, graph, source, seed, t_us (see QUERY_DTYPE).
+        Returns (latencies_ms array, wall_ms).  plain=True runs the stream one
+        query at a time through the single-query kernels instead."""
+        q = np.ascontiguousarray(queries, dtype=QUERY_DTYPE)
+        lat = np.zeros(len(q), dtype=np.float64)
+        wall = C.c_double()
+        fn = lib.apspie_server_replay_plain if plain else lib.apspie_server_replay
+        check(fn(self._h, len(q), C.c_void_p(q.ctypes.data), C.c_void_p(lat.ctypes.data),
+                 C.byref(wall)), what="apspie_server_replay")
+        return lat, wall.value
 
     def wait(self, rid: int):
         lat = C.c_double()

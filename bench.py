@@ -44,6 +44,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--scale", type=int, default=SCALE)
+    p.add_argument("--workload", default="bfs", choices=["bfs", "serving"],
+                   help="serving: only the serving sweep (rates 100 .. 100,000 queries/s), "
+                        "one JSON line")
     p.add_argument("--profile-run", action="store_true",
                    help="only the timed traversals (for ncu captures): no clock extension, "
                         "no end-to-end leg, no CPU baseline")
@@ -285,20 +288,24 @@ def batched_leg(ctx, big):
                 ap.sssp(ctx, j["graph"], s, weights="u32")
                 edges += ap.sssp_stats(ctx)["edges_traversed"]
     ap.batch_run(ctx, jobs)
+    stream = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    ev[0].record(stream)
     for j in jobs:
         for s in j["sources"]:
             if j["type"] == "bfs":
                 ap.bfs(ctx, j["graph"], s)
             else:
                 ap.sssp(ctx, j["graph"], s, weights="u32")
+    ev[1].record(stream)
     torch.cuda.synchronize()
-    plain_s = time.perf_counter() - t0
-    t0 = time.perf_counter()
+    plain_s = ev[0].elapsed_time(ev[1]) * 1e-3
+    ev[2].record(stream)
     outs = ap.batch_run(ctx, jobs)
+    ev[3].record(stream)
     torch.cuda.synchronize()
-    batch_s = time.perf_counter() - t0
+    batch_s = ev[2].elapsed_time(ev[3]) * 1e-3
     st = ap.batch_stats(ctx)
     # spot check: every batched result equals the single-source path
     for j, o in zip(jobs, outs):
@@ -313,7 +320,56 @@ def batched_leg(ctx, big):
             "batched_gteps": edges / batch_s / 1e9, "plain_gteps": edges / plain_s / 1e9,
             "speedup_vs_plain": plain_s / batch_s, "batched_ms": batch_s * 1e3,
             "plain_ms": plain_s * 1e3, "super_steps": st["super_steps"],
-            "timing": "host wall clock around synchronised launches"}
+            "timing": "CUDA events on the launching stream (plain: all single-source calls "
+                      "back to back; batched: one apspie_batch_run, transposes included)"}
+
+
+SERVE_SCALES = (12, 14, 16, 18, 20, 22, 23)
+
+
+def serving_leg(ctx, rates=(1000, 100000), n_queries=600, seed=SEED):
+    """Serving: 8 device-resident graphs (R-MAT 12..23 symmetrised + the
+    1024x1024 grid, uint32 weights in [1, 255]), a Poisson stream of 60% BFS
+    / 30% SSSP / 10% MIS queries, graph chosen in proportion to its vertex
+    count, sources seed-chosen among vertices with edges.  Each rate is
+    replayed open-loop through the server (continuous batching) and through
+    the plain one-query-at-a-time path; latency = arrival -> result on the
+    device."""
+    import torch
+    import apspie_b200 as ap
+    from apspie_b200.serving import QUERY_DTYPE
+    graphs = [ap.gen_rmat_device(ctx, sc, EDGE_FACTOR, seed=seed) for sc in SERVE_SCALES]
+    graphs.append(ap.gen_grid(1024, 1024).to_device())
+    for g in graphs:
+        ap.weights_device(ctx, g, seed=seed)
+    torch.cuda.synchronize()
+    ms = np.array([g.m for g in graphs], dtype=np.float64)
+    degs = [(g.ptr[1:] - g.ptr[:-1]).cpu().numpy() for g in graphs]
+    nonzero = [np.flatnonzero(d > 0) for d in degs]
+    out = {"graphs": [f"rmat{sc}" for sc in SERVE_SCALES] + ["grid1024"],
+           "mix": "60% BFS / 30% SSSP / 10% MIS", "queries_per_rate": n_queries,
+           "budget_gb": 120, "rates": []}
+    with ap.Server(budget_bytes=120 << 30, max_batch=256) as srv:
+        gids = [srv.add_graph(g) for g in graphs]
+        for rate in rates:
+            rng = np.random.default_rng(seed * 1000 + int(rate))
+            q = np.zeros(n_queries, dtype=QUERY_DTYPE)
+            q["type"] = rng.choice([0, 1, 2], size=n_queries, p=[0.6, 0.3, 0.1])
+            gi = rng.choice(len(graphs), size=n_queries, p=ms / ms.sum())
+            q["graph"] = [gids[i] for i in gi]
+            q["source"] = [int(nonzero[i][rng.integers(len(nonzero[i]))]) for i in gi]
+            q["seed"] = 1
+            q["t_us"] = np.cumsum(rng.exponential(1e6 / rate, size=n_queries))
+            row = {"rate_qps": rate}
+            for name, plain in (("batched", False), ("plain", True)):
+                lat, wall = srv.replay(q, plain=plain)
+                row[name] = {"qps": n_queries / (wall * 1e-3),
+                             "p50_ms": float(np.percentile(lat, 50)),
+                             "p99_ms": float(np.percentile(lat, 99)),
+                             "wall_ms": wall}
+            row["throughput_ratio"] = row["batched"]["qps"] / row["plain"]["qps"]
+            out["rates"].append(row)
+    return out
 
 
 def run_ours(args):
@@ -422,6 +478,7 @@ def run_ours(args):
     if not args.profile_run and rank == 0:
         extras["sssp"] = sssp_leg(ctx)
         extras["batched"] = batched_leg(ctx, h)
+        extras["serving"] = serving_leg(ctx)
 
     # ---- reference CPU BFS on a bounded sample (rank 0, N=1) ----
     cpu = None
@@ -462,10 +519,33 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args):
+    """--workload serving: the full arrival-rate sweep of the serving leg."""
+    import torch
+    rank, _, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    import apspie_b200 as ap
+    ctx = ap.Context(local)
+    res = serving_leg(ctx, rates=(100, 1000, 10000, 100000), n_queries=max(args.steps, 200))
+    best = max(res["rates"], key=lambda r: r["batched"]["qps"])
+    line = {"metric": "serving throughput (queries/s), mixed BFS/SSSP/MIS on 8 resident graphs",
+            "value": best["batched"]["qps"], "unit": "queries/s", "n_gpus": 1,
+            "steps": res["queries_per_rate"], "warmup": 0, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32/uint32",
+            "data": "synthetic", "config": {"workload": "serving: " + ", ".join(res["graphs"]),
+                                            "mix": res["mix"], "budget_gb": res["budget_gb"]},
+            "serving": res}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "serving":
+        run_serving(args)
     else:
         run_ours(args)
 

@@ -144,11 +144,18 @@ int apspie_sssp_f32(apspie_ctx ctx, int src, int64_t nnz, int m,
 
 typedef struct {
   int32_t rounds;            /* frontier rounds run */
-  int32_t pad;
+  int32_t phases;            /* near-far phases (0 without near-far) */
   int64_t vertices_reached;  /* |R| */
   int64_t edges_traversed;   /* E_R = sum of out-degrees of reached vertices */
   int64_t relaxations;       /* edges scanned over all rounds (>= E_R) */
 } apspie_sssp_stats;
+
+/* Near-far schedule of apspie_sssp_*: a vertex whose distance drops below
+ * the threshold T joins the next frontier, one at or above it waits in a far
+ * list until the frontier runs dry and T grows by delta.  delta 0 (the
+ * default) = T infinite, i.e. frontier Bellman-Ford.  The distances do not
+ * depend on delta (same fixpoint); the work and the number of rounds do. */
+int apspie_sssp_set_params(apspie_ctx ctx, uint32_t delta_u32, float delta_f32);
 
 /* Statistics of the last SSSP on this context (synchronises). */
 int apspie_sssp_get_stats(apspie_ctx ctx, apspie_sssp_stats *out);
@@ -239,6 +246,29 @@ int apspie_server_add_graph(apspie_server_t s, int m, int64_t nnz,
 /* Non-blocking; APSPIE_ERR_BUSY when the pending queue is full. */
 int apspie_server_submit(apspie_server_t s, int type, int graph, int source,
                          uint32_t seed, void *h_result, uint64_t *req_id);
+/* As apspie_server_submit, with the result row copied into d_result (device
+ * memory, m 32-bit entries) instead; d_result == NULL drops the result once it
+ * is computed (load tests: only the latency is recorded). */
+int apspie_server_submit_device(apspie_server_t s, int type, int graph,
+                                int source, uint32_t seed, int32_t *d_result,
+                                uint64_t *req_id);
+/* One query of a timed stream: kind and arguments as for submit, arrival
+ * time in microseconds from the start of the stream (non-decreasing). */
+typedef struct {
+  int32_t type, graph, source;
+  uint32_t seed;
+  double t_us;
+} apspie_query;
+/* Open-loop replay: submits query i at its arrival time (results dropped) and
+ * waits for all; lat_ms[i] = arrival -> result on the device; *wall_ms =
+ * stream start -> last completion. */
+int apspie_server_replay(apspie_server_t s, int n, const apspie_query *q,
+                         double *lat_ms, double *wall_ms);
+/* The same stream one query at a time, in arrival order, through
+ * apspie_bfs / apspie_sssp_u32 / apspie_mis on a stream of its own (the
+ * plain single-query path); latencies likewise from the arrival times. */
+int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q,
+                               double *lat_ms, double *wall_ms);
 /* *done = 1 once the result is in h_result (the request is then retired and
  * its status returned). */
 int apspie_server_poll(apspie_server_t s, uint64_t req_id, int *done,

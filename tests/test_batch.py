@@ -93,3 +93,29 @@ def test_autotuner_picks_and_caches(ctx):
     f = ap.autotune_spmspv(ctx, g)
     assert f >= 0
     ap.spmspv_set_params(ctx)
+
+
+def test_batch_sssp_multi_source_parts(ctx):
+    """Multi-source SSSP rows: more than 32 sources (two device jobs), a
+    duplicated source, hubs split into chunks, a directed graph and a
+    grid with heavy weights; every row equals the oracle's Dijkstra."""
+    import apspie_b200 as ap
+    r = ap.gen_rmat(13, 16, seed=11)          # hubs of degree >> 32
+    ap.weights_u32(r, seed=5)
+    g = ap.gen_grid(48, 48)
+    ap.weights_u32(g, seed=6, lo=200, hi=255)
+    dd = ap.gen_rmat(12, 8, seed=12, symmetric=False)
+    ap.weights_u32(dd, seed=7)
+    srcs = ap.seeded_sources(r, 45, seed=8)
+    srcs[7] = srcs[3]
+    jobs = [{"type": "sssp", "graph": r.to_device(), "sources": srcs},
+            {"type": "sssp", "graph": g.to_device(), "sources": [0, 2303, 1200]},
+            {"type": "sssp", "graph": dd.to_device(), "sources": list(range(0, 4096, 300))},
+            {"type": "sssp", "graph": r.to_device(), "sources": [srcs[0]]},          # row width 1
+            {"type": "sssp", "graph": g.to_device(), "sources": [5, 77]}]            # row width 2
+    outs = ap.batch_run(ctx, jobs)
+    for jd, out, h in zip(jobs, outs, (r, g, dd, r, g)):
+        out = out.cpu().numpy().view(np.uint32)
+        for i, s in enumerate(jd["sources"]):
+            ref = oracle.sssp_u32(h.m, h.ptr, h.ind, h.w_u32, s)
+            np.testing.assert_array_equal(out[i], ref, err_msg=f"sssp {h.name} src {s}")

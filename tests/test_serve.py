@@ -106,3 +106,42 @@ def test_server_rejects_bad_queries():
             srv.submit(1, gid, 0)            # SSSP on an unweighted graph
         with pytest.raises(ap.ApspieError):
             srv.submit(0, gid + 5, 0)        # unknown graph
+
+
+def test_server_device_results_and_replay(ctx):
+    """Results delivered into device buffers equal the single-query path;
+    the open-loop replay and the plain one-at-a-time replay both finish a
+    timed stream and report one latency per query."""
+    import torch
+    import apspie_b200 as ap
+    from apspie_b200.serving import QUERY_DTYPE
+    hs = _graphs()
+    ds = [h.to_device() for h in hs]
+    rng = np.random.default_rng(2)
+    with ap.Server(budget_bytes=8 << 30) as srv:
+        gids = [srv.add_graph(d) for d in ds]
+        outs, rids, qs = [], [], []
+        for _ in range(40):
+            gi = int(rng.integers(3))
+            kind = int(rng.choice([0, 1, 2]))
+            src, seed = int(rng.integers(hs[gi].m)), int(rng.integers(1 << 31))
+            out = torch.empty(hs[gi].m, dtype=torch.int32, device="cuda")
+            outs.append(out)
+            qs.append((gi, kind, src, seed))
+            rids.append(srv.submit_device(kind, gids[gi], src, seed, out))
+        for r in rids:
+            srv.wait(r)
+        for (gi, kind, src, seed), out in zip(qs, outs):
+            ref = _alone(ctx, hs[gi], ds[gi], kind, src, seed)
+            np.testing.assert_array_equal(out.cpu().numpy(), ref.view(np.int32))
+        n = 120
+        q = np.zeros(n, dtype=QUERY_DTYPE)
+        q["type"] = rng.choice([0, 1, 2], size=n, p=[0.6, 0.3, 0.1])
+        q["graph"] = rng.integers(0, 3, size=n)
+        q["source"] = [int(rng.integers(hs[g].m)) for g in q["graph"]]
+        q["seed"] = 5
+        q["t_us"] = np.cumsum(rng.exponential(1e6 / 2000.0, size=n))   # 2,000 queries / s
+        lat, wall = srv.replay(q)
+        lat_p, wall_p = srv.replay(q, plain=True)
+    assert (lat > 0).all() and (lat_p > 0).all()
+    assert wall >= q["t_us"][-1] / 1e3 and wall_p >= q["t_us"][-1] / 1e3
