@@ -64,6 +64,8 @@ PROTOS: dict[str, tuple] = {
     "apspie_ctx_create": (c_int, [c_int, vp, P_vp]),
     "apspie_ctx_destroy": (c_int, [vp]),
     "apspie_ctx_set_stream": (c_int, [vp, vp]),
+    "apspie_ctx_set_max_grid": (c_int, [vp, c_int]),
+    "apspie_ctx_resident_blocks": (c_int, [vp, P_int]),
     "apspie_ctx_sync": (c_int, [vp]),
     "apspie_ctx_launch_count": (c_int, [vp, P_u64]),
     "apspie_ctx_workspace_bytes": (c_int, [vp, P_size]),
@@ -72,17 +74,20 @@ PROTOS: dict[str, tuple] = {
     "apspie_bfs": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, vp, c_int]),
     "apspie_bfs_noalloc": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, vp, c_int]),
     "apspie_bfs_get_stats": (c_int, [vp, C.POINTER(BfsStats)]),
+    "apspie_bfs_prepare": (c_int, [vp, c_int, c_i64, vp, vp, vp, vp]),
     "apspie_bfs_get_trace": (c_int, [vp, c_int, P_int, vp, vp, vp, vp, vp, vp, vp, vp]),
     "apspie_bfs_set_params": (c_int, [vp, c_int, c_int, c_int]),
     "apspie_sssp_u32": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, c_int]),
     "apspie_sssp_f32": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, c_int]),
     "apspie_sssp_set_params": (c_int, [vp, c_u32, c_f32]),
+    "apspie_sssp_get_trace": (c_int, [vp, c_int, P_int, vp, vp, vp, vp]),
     "apspie_sssp_get_stats": (c_int, [vp, C.POINTER(SsspStats)]),
     "apspie_mis": (c_int, [vp, c_i64, c_int, vp, vp, vp, vp, c_f32]),
     "apspie_mis_get_rounds": (c_int, [vp, P_int]),
     "apspie_neighbor_flags": (c_int, [vp, c_i64, c_int, vp, vp, vp, vp]),
     "apspie_spmspv": (c_int, [vp, c_int, c_int, c_i64, vp, vp, vp, c_int, vp, vp, vp, vp, P_int,
                               P_i64]),
+    "apspie_spmv": (c_int, [vp, c_int, c_int, c_i64, vp, vp, vp, vp, vp]),
     "apspie_mxv_dense": (c_int, [vp, c_int, c_int, c_i64, vp, vp, vp, vp, vp, P_i64]),
     "apspie_spmspv_set_params": (c_int, [vp, C.c_double]),
     "apspie_spgemm": (c_int, [vp, C.POINTER(Csr), C.POINTER(Csr), C.POINTER(Csr)]),
@@ -100,8 +105,8 @@ PROTOS: dict[str, tuple] = {
     "apspie_server_add_graph": (c_int, [vp, c_int, c_i64, vp, vp, vp, vp, vp, c_int, P_int]),
     "apspie_server_submit": (c_int, [vp, c_int, c_int, c_int, c_u32, vp, P_u64]),
     "apspie_server_submit_device": (c_int, [vp, c_int, c_int, c_int, c_u32, vp, P_u64]),
-    "apspie_server_replay": (c_int, [vp, c_int, vp, vp, C.POINTER(C.c_double)]),
-    "apspie_server_replay_plain": (c_int, [vp, c_int, vp, vp, C.POINTER(C.c_double)]),
+    "apspie_server_replay": (c_int, [vp, c_int, vp, c_int, vp, C.POINTER(C.c_double)]),
+    "apspie_server_replay_plain": (c_int, [vp, c_int, vp, c_int, vp, C.POINTER(C.c_double)]),
     "apspie_server_poll": (c_int, [vp, c_u64, P_int, C.POINTER(C.c_double)]),
     "apspie_server_wait": (c_int, [vp, c_u64, C.POINTER(C.c_double)]),
     "apspie_server_get_stats": (c_int, [vp, C.POINTER(ServerStats)]),

@@ -4,7 +4,8 @@
 //   * a multi-source BFS over up to 64 sources of one graph: every vertex
 //     carries 64-bit masks (visited, and the frontier of three consecutive
 //     levels), bit s standing for source s -- the "frontier matrix" of
-//     MS-BFS; or
+//     MS-BFS -- and the depths are vertex-major, one row per vertex of the
+//     sources rounded up to a power of two; or
 //   * a multi-source uint32 SSSP over up to 32 sources of one graph: the
 //     distances are vertex-major, dist[v][0..sw) one row of sw = 1, 2, 4, 8,
 //     16 or 32 words (the sources rounded up to a power of two), and every
@@ -72,7 +73,7 @@ struct BatchJob {
   int *q0, *q1, *q2;
   int2 *c0, *c1, *c2;
   int big_deg, chunk;  // degree above which a vertex is chunked, edges per chunk
-  int sw, pad1;        // SSSP: distance row width (power of two >= nsrc)
+  int sw, pad1;        // result row width (power of two >= nsrc)
   JobCounters c[3];
 };
 
@@ -125,7 +126,7 @@ __device__ void seed_queue(BatchJob *j) {
 __global__ void batch_init_bfs(BatchJob *jobs, int jid) {
   BatchJob *j = jobs + jid;
   const int m = j->m;
-  const size_t n64 = (size_t)m * 64;
+  const size_t n64 = (size_t)m * j->sw;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n64;
        i += (size_t)gridDim.x * blockDim.x)
     j->out[i] = -1;
@@ -145,7 +146,7 @@ __global__ void batch_seed_bfs(BatchJob *jobs, int jid) {
     int v = j->src[s];
     atomicOr(j->visited + v, 1ull << s);
     atomicOr(j->F0 + v, 1ull << s);
-    j->out[(size_t)v * 64 + s] = 0;
+    j->out[(size_t)v * j->sw + s] = 0;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -252,7 +253,7 @@ __device__ __forceinline__ bool msbfs_relax(BatchJob *j, unsigned long long f, i
   unsigned long long old = atomicOr(j->visited + u, nb);
   unsigned long long mine = nb & ~old;
   if (!mine) return false;
-  int32_t *row = j->out + (size_t)u * 64;
+  int32_t *row = j->out + (size_t)u * j->sw;
   for (unsigned long long b = mine; b; b &= b - 1) row[__ffsll((long long)b) - 1] = next;
   return atomicOr(Fn + u, mine) == 0ull;
 }
@@ -371,7 +372,7 @@ __device__ void msbfs_pull(BatchJob *j, int L, int unit, unsigned long long *s_a
   if (found[0]) {
     j->visited[v] |= nb;  // only this lane touches v's masks in a pull step
     Fn[v] = nb;
-    int32_t *row = j->out + (size_t)v * 64;
+    int32_t *row = j->out + (size_t)v * j->sw;
     for (unsigned long long b = nb; b; b &= b - 1) row[__ffsll((long long)b) - 1] = L + 1;
     dg[0] = __ldg(j->ptr + v + 1) - __ldg(j->ptr + v);
   }
@@ -747,7 +748,7 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
     b += align_up(8 * m) * (bfs ? 4 : 3);  // (BFS: visited +) 3 frontier masks
     b += align_up(4 * m) * 3;              // queues
     b += align_up(8 * cap) * 3;            // chunk lists
-    b += align_up(4 * m * (bfs ? kMsbfsWidth : row_width(parts[p].n)));  // vertex-major results
+    b += align_up(4 * m * row_width(parts[p].n));  // vertex-major results
     off[p] = total;
     total += b;
   }
@@ -788,7 +789,7 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
     const bool bfs = B.type == kJobBfs;
     const size_t m = (size_t)J.m, cap = job_chunk_capacity(J.nnz, bfs);
     B.big_deg = bfs ? kBigDeg : kSsspBigDeg;
-    B.sw = bfs ? kMsbfsWidth : row_width(B.nsrc);
+    B.sw = row_width(B.nsrc);  // result row: the sources rounded up to a power of two
     B.chunk = bfs ? kChunk : kSsspChunk;
     if (bfs) {
       B.visited = (unsigned long long *)b;
@@ -824,7 +825,7 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
   }
   rc = check_launch(ctx, "batch init", 2 * nparts);
   if (rc) return rc;
-  int grid = batch_grid(ctx);
+  int grid = clamp_grid(ctx, batch_grid(ctx));
   if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_batch_run: occupancy query failed");
   int np = nparts;
   void *args[] = {&djobs, &np, &dstate, &max_steps};

@@ -224,7 +224,7 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
         nch = s_chunks;
       }
       BfsVisit vis{next, depth};
-      expand_push(ptr, ind, qin, nq, cin, s_nbig, nch, qout, cout, nxt, gwarp, nwarps,
+      expand_push(ptr, ind, qin, nq, cin, s_nbig, nch, qout, cout, nxt, cur, gwarp, nwarps,
                   [](int) { return 0u; }, vis,
                   L < kTraceLevels ? &st->trace[L].expanded : nullptr);
     } else {
@@ -432,7 +432,7 @@ int apspie_bfs(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
   auto *gmask = (unsigned *)workspace(ctx, kSlotBfsGroupMask, sizeof(unsigned) * ((size_t)m / 32 + 1));
   if (!st || !qa || !qb || !ca || !cb || !gmask) return APSPIE_ERR_OOM;
   ctx->bfs_state = st;
-  int grid = bfs_grid(ctx);
+  int grid = clamp_grid(ctx, bfs_grid(ctx));
   if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_bfs: occupancy query failed");
 
   int init_grid = std::min((m + 255) / 256, ctx->num_sms * 8);

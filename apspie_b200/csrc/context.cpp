@@ -114,6 +114,18 @@ int apspie_ctx_destroy(apspie_ctx ctx) {
   return APSPIE_OK;
 }
 
+int apspie_ctx_set_max_grid(apspie_ctx ctx, int blocks) {
+  if (!ctx || blocks < 0) return APSPIE_ERR_INVALID;
+  ctx->max_grid = blocks;
+  return APSPIE_OK;
+}
+
+int apspie_ctx_resident_blocks(apspie_ctx ctx, int *blocks) {
+  if (!ctx || !blocks) return APSPIE_ERR_INVALID;
+  *blocks = 2 * ctx->num_sms;  // 512-thread persistent blocks: two per SM fit every kernel
+  return APSPIE_OK;
+}
+
 int apspie_ctx_set_stream(apspie_ctx ctx, void *stream) {
   if (!ctx) return APSPIE_ERR_INVALID;
   ctx->stream = (cudaStream_t)stream;

@@ -30,6 +30,9 @@ struct apspie_context {
   void *pinned = nullptr;
   size_t pinned_bytes = 0;
 
+  // at most this many blocks per persistent launch (0: as many as fit), so
+  // that two persistent kernels can share the GPU
+  int max_grid = 0;
   // BFS tuning and the device block that holds the last run's statistics
   int bfs_alpha = 14;
   int bfs_beta = 24;
@@ -111,3 +114,11 @@ int check_cuda(apspie_context *ctx, cudaError_t e, const char *what);
     if (_e != cudaSuccess)                                      \
       return apspie::check_cuda((ctx), _e, "cudaSetDevice");    \
   } while (0)
+
+namespace apspie {
+// Grid of a persistent launch: the occupancy-sized grid, capped by the
+// context's max_grid.
+inline int clamp_grid(const apspie_context *ctx, int grid) {
+  return (ctx->max_grid > 0 && ctx->max_grid < grid) ? ctx->max_grid : grid;
+}
+}  // namespace apspie

@@ -30,7 +30,7 @@
 
 namespace apspie {
 
-constexpr int kBigDeg = 64;   // out-degree above which a vertex is chunked
+constexpr int kBigDeg = 32;   // out-degree above which a vertex is chunked
 constexpr int kChunk = 128;   // edges per chunk (one unrolled batch of a warp)
 constexpr int kUnroll = 4;    // rounds of 32 edges issued together
 
@@ -40,6 +40,8 @@ struct LevelCounters {
   unsigned q;             // vertices in the queue (degree <= kBigDeg)
   unsigned nimpl;         // vertices of an implicit frontier (BFS pull: depth == level), not queued
   unsigned long long edges;  // sum of out-degrees of the frontier
+  unsigned grab;          // queue units handed out so far while this level expands
+  unsigned cgrab;         // chunks handed out so far
 };
 
 __device__ __forceinline__ unsigned bc_big(unsigned long long bc) { return (unsigned)bc; }
@@ -179,6 +181,79 @@ __device__ __forceinline__ void seed_frontier(int src, const int *__restrict__ p
   }
 }
 
+// Chunks of the big vertices, in runs of consecutive chunks: the warp finds
+// the vertex of a run's first chunk and walks on.  With at most two chunks
+// per warp every warp takes its own run (no counter traffic: a level's
+// worth of same-address atomics from every warp costs microseconds); larger
+// levels hand runs of about an eighth of a warp's share out on demand from
+// the level's counter, because equal chunk counts are not equal work (a
+// chunk whose targets improve appends and chunks others).
+template <typename Load, typename Visit>
+__device__ __forceinline__ void expand_chunks(const int *__restrict__ ptr,
+                                              const int *__restrict__ ind, const int2 *bin,
+                                              unsigned nbig, unsigned nch, int *qout, int2 *bout,
+                                              LevelCounters *nxt, int gwarp, int nwarps, Load load,
+                                              Visit &visit, DiscoverAcc &acc,
+                                              unsigned long long &nwalk, unsigned *cgrab) {
+  const int lane = lane_id();
+  const bool dynamic = nch > 2u * (unsigned)nwarps;
+  const unsigned run = dynamic ? max(1u, nch / ((unsigned)nwarps * 8u))
+                               : (nch + (unsigned)nwarps - 1) / (unsigned)nwarps;
+  for (int turn = 0;; ++turn) {
+    unsigned c_beg;
+    if (dynamic) {
+      c_beg = 0;
+      if (lane == 0) c_beg = atomicAdd(cgrab, run);
+      c_beg = __shfl_sync(kFull, c_beg, 0);
+    } else {
+      c_beg = turn == 0 ? (unsigned)gwarp * run : nch;
+    }
+    if (c_beg >= nch) break;
+    const unsigned c_end = min(c_beg + run, nch);
+    int bi = big_search(bin, (int)nbig, c_beg);
+    int2 bcur = __ldcg(bin + bi);
+    unsigned bnext = bi + 1 < (int)nbig ? (unsigned)__ldcg(&bin[bi + 1].y) : 0xffffffffu;
+    for (unsigned c = c_beg; c < c_end; ++c) {
+      while (c >= bnext) {
+        ++bi;
+        bcur = __ldcg(bin + bi);
+        bnext = bi + 1 < (int)nbig ? (unsigned)__ldcg(&bin[bi + 1].y) : 0xffffffffu;
+      }
+      const int v = bcur.x;
+      const int s = __ldg(ptr + v) + (int)(c - (unsigned)bcur.y) * kChunk;
+      const int e = min(s + kChunk, __ldg(ptr + v + 1));
+      nwalk += (unsigned long long)(e - s);
+      const unsigned pay = load(v);
+      for (int k0 = s; k0 < e; k0 += 32 * kUnroll) {
+        int uu[kUnroll];
+        unsigned aux[kUnroll];
+        bool ok[kUnroll];
+#pragma unroll
+        for (int r = 0; r < kUnroll; ++r) {
+          int k = k0 + r * 32 + lane;
+          uu[r] = k < e ? __ldg(ind + k) : -1;
+        }
+#pragma unroll
+        for (int r = 0; r < kUnroll; ++r)
+          ok[r] = uu[r] >= 0 && visit.check(pay, k0 + r * 32 + lane, uu[r], aux[r]);
+        bool f[kUnroll], g[kUnroll];
+        int cls[kUnroll];
+#pragma unroll
+        for (int r = 0; r < kUnroll; ++r) {
+          cls[r] = ok[r] ? (int)visit.commit(pay, k0 + r * 32 + lane, uu[r], aux[r]) : 0;
+          f[r] = cls[r] == 1;
+          g[r] = cls[r] == 2;
+        }
+        discover_n<kUnroll>(f, uu, ptr, qout, bout, nxt, acc);
+        if constexpr (Visit::kTwoWay) {
+          append_plain<kUnroll>(g, uu, visit.far_list, visit.far_count);
+          visit.note_far(cls, aux);
+        }
+      }
+    }
+  }
+}
+
 // Push expansion of (qin[0..nq), cin[0..nch)).  `load(v)` gives the 32-bit
 // payload of a source vertex (e.g. its distance), broadcast to its edges.
 // visit.commit returns a class: 0 = nothing, 1 = joins the next frontier,
@@ -191,12 +266,30 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
                                             const int *__restrict__ ind, const int *qin,
                                             unsigned nq, const int2 *bin, unsigned nbig,
                                             unsigned nch, int *qout, int2 *bout,
-                                            LevelCounters *nxt, int gwarp, int nwarps, Load load,
-                                            Visit &visit, unsigned long long *walked = nullptr) {
+                                            LevelCounters *nxt, LevelCounters *cur, int gwarp,
+                                            int nwarps, Load load, Visit &visit,
+                                            unsigned long long *walked = nullptr) {
   const int lane = lane_id();
   unsigned long long nwalk = 0;
   DiscoverAcc acc;
-  for (unsigned base = (unsigned)gwarp * 32u; base < nq; base += (unsigned)nwarps * 32u) {
+  expand_chunks(ptr, ind, bin, nbig, nch, qout, bout, nxt, gwarp, nwarps, load, visit, acc, nwalk,
+                &cur->cgrab);
+  // queue units of 32 vertices (at most 32 x kBigDeg edges): one per warp in
+  // turn on small levels, handed out on demand from the level's counter on
+  // large ones, so a warp that drew heavy units takes fewer of them
+  const unsigned nunits = (nq + 31u) / 32u;
+  const bool dynamic = nunits > 2u * (unsigned)nwarps;
+  for (unsigned turn = 0;; ++turn) {
+    unsigned unit;
+    if (dynamic) {
+      unit = 0;
+      if (lane == 0) unit = atomicAdd(&cur->grab, 1u);
+      unit = __shfl_sync(kFull, unit, 0);
+    } else {
+      unit = (unsigned)gwarp + turn * (unsigned)nwarps;
+    }
+    const unsigned base = unit * 32u;
+    if (base >= nq) break;
     unsigned idx = base + lane;
     int v = idx < nq ? __ldcg(qin + idx) : -1;
     int s = 0, d = 0;
@@ -233,55 +326,6 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
 #pragma unroll
       for (int r = 0; r < kUnroll; ++r) {
         cls[r] = ok[r] ? (int)visit.commit(pp[r], kk[r], uu[r], aux[r]) : 0;
-        f[r] = cls[r] == 1;
-        g[r] = cls[r] == 2;
-      }
-      discover_n<kUnroll>(f, uu, ptr, qout, bout, nxt, acc);
-      if constexpr (Visit::kTwoWay) {
-        append_plain<kUnroll>(g, uu, visit.far_list, visit.far_count);
-        visit.note_far(cls, aux);
-      }
-    }
-  }
-  // chunks of the big vertices: warp w takes the contiguous range
-  // [w * per, (w + 1) * per), finds the vertex of its first chunk and walks on
-  const unsigned per = (nch + (unsigned)nwarps - 1) / (unsigned)nwarps;
-  const unsigned c_beg = (unsigned)gwarp * per, c_end = min(c_beg + per, nch);
-  int bi = c_beg < c_end ? big_search(bin, (int)nbig, c_beg) : 0;
-  int2 bcur = make_int2(0, 0);
-  unsigned bnext = 0;
-  if (c_beg < c_end) {
-    bcur = __ldcg(bin + bi);
-    bnext = bi + 1 < (int)nbig ? (unsigned)__ldcg(&bin[bi + 1].y) : 0xffffffffu;
-  }
-  for (unsigned c = c_beg; c < c_end; ++c) {
-    while (c >= bnext) {
-      ++bi;
-      bcur = __ldcg(bin + bi);
-      bnext = bi + 1 < (int)nbig ? (unsigned)__ldcg(&bin[bi + 1].y) : 0xffffffffu;
-    }
-    const int2 ch = make_int2(bcur.x, (int)(c - (unsigned)bcur.y));
-    int s = __ldg(ptr + ch.x) + ch.y * kChunk;
-    int e = min(s + kChunk, __ldg(ptr + ch.x + 1));
-    nwalk += (unsigned long long)(e - s);
-    unsigned pay = load(ch.x);
-    for (int k0 = s; k0 < e; k0 += 32 * kUnroll) {
-      int uu[kUnroll];
-      unsigned aux[kUnroll];
-      bool ok[kUnroll];
-#pragma unroll
-      for (int r = 0; r < kUnroll; ++r) {
-        int k = k0 + r * 32 + lane;
-        uu[r] = k < e ? __ldg(ind + k) : -1;
-      }
-#pragma unroll
-      for (int r = 0; r < kUnroll; ++r)
-        ok[r] = uu[r] >= 0 && visit.check(pay, k0 + r * 32 + lane, uu[r], aux[r]);
-      bool f[kUnroll], g[kUnroll];
-      int cls[kUnroll];
-#pragma unroll
-      for (int r = 0; r < kUnroll; ++r) {
-        cls[r] = ok[r] ? (int)visit.commit(pay, k0 + r * 32 + lane, uu[r], aux[r]) : 0;
         f[r] = cls[r] == 1;
         g[r] = cls[r] == 2;
       }

@@ -109,6 +109,41 @@ __global__ void weights_f32_kernel(int m, const int *ptr, const int *ind, uint64
       w[k] = weight_f32(seed, (uint32_t)u, (uint32_t)ind[k]);
 }
 
+// key of edge (u -> v) for the pull-ordered in-adjacency: row v, then u's
+// out-degree descending (clamped to dbits bits); value u
+__global__ void pull_keys(int m, const int *ptr, const int *ind, int dbits,
+                          unsigned long long *keys, int *vals) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long dmax = (1ull << dbits) - 1ull;
+  for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < m;
+       u += (gridDim.x * blockDim.x) >> 5) {
+    const int s = ptr[u], e = ptr[u + 1];
+    const unsigned long long d = min((unsigned long long)(e - s), dmax);
+    for (int k = s + lane; k < e; k += 32) {
+      keys[k] = ((unsigned long long)ind[k] << dbits) | (dmax - d);
+      vals[k] = u;
+    }
+  }
+}
+
+// row lengths of the sorted keys (row = key >> dbits), one atomic per run
+__global__ void key_rows(const unsigned long long *k, long long n, int dbits, int *row_count) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
+       base += stride) {
+    const long long i = base + (threadIdx.x & 31);
+    const unsigned row = i < n ? (unsigned)(k[i] >> dbits) : 0xffffffffu;
+    const unsigned peers = __match_any_sync(kFull, row);
+    if (i < n && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&row_count[row], __popc(peers));
+  }
+}
+
+__global__ void copy_int(long long n, const int *in, int *out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = in[i];
+}
+
 __global__ void fill_int(int n, int v, int *p) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
 }
@@ -208,6 +243,38 @@ int apspie_gen_er_device(apspie_ctx ctx, int n, int mean_degree, uint64_t seed, 
   int rc = check_launch(ctx, "er_keys");
   if (rc) return rc;
   return keys_to_graph(ctx, ka, kb, nk, bits, n, out);
+}
+
+int apspie_bfs_prepare(apspie_ctx ctx, int m, int64_t nnz, const int *d_ptr, const int *d_ind,
+                       int *d_tptr, int *d_tind) {
+  APSPIE_CHECK_CTX(ctx);
+  if (m <= 0 || nnz < 0 || nnz >= (int64_t)INT32_MAX || !d_ptr || !d_tptr ||
+      (nnz > 0 && (!d_ind || !d_tind)))
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_bfs_prepare: bad arguments");
+  cudaStream_t st = ctx->stream;
+  fill_int<<<gg(ctx, m + 1), 256, 0, st>>>(m + 1, 0, d_tptr);
+  int rc = check_launch(ctx, "fill_int");
+  if (rc || nnz == 0) return rc;
+  const int vbits = bits_for(m);
+  const int dbits = std::min(24, 63 - vbits);
+  auto *ka = (unsigned long long *)workspace(ctx, kSlotSortKeysA, 8 * (size_t)nnz);
+  auto *kb = (unsigned long long *)workspace(ctx, kSlotSortKeysB, 8 * (size_t)nnz);
+  auto *va = (int *)workspace(ctx, kSlotSortValsA, 4 * (size_t)nnz);
+  auto *vb = (int *)workspace(ctx, kSlotSortValsB, 4 * (size_t)nnz);
+  if (!ka || !kb || !va || !vb) return APSPIE_ERR_OOM;
+  pull_keys<<<gg(ctx, (long long)m * 32), 256, 0, st>>>(m, d_ptr, d_ind, dbits, ka, va);
+  rc = check_launch(ctx, "pull_keys");
+  if (rc) return rc;
+  bool in_b = false;
+  rc = device_radix_sort<unsigned long long, int>(ctx, ka, va, kb, vb, nnz, vbits + dbits, &in_b);
+  if (rc) return rc;
+  const unsigned long long *k = in_b ? kb : ka;
+  const int *v = in_b ? vb : va;
+  key_rows<<<gg(ctx, nnz), 256, 0, st>>>(k, nnz, dbits, d_tptr);
+  copy_int<<<gg(ctx, nnz), 256, 0, st>>>(nnz, v, d_tind);
+  rc = check_launch(ctx, "key_rows", 2);
+  if (rc) return rc;
+  return device_exclusive_scan<int>(ctx, d_tptr, d_tptr, (long long)m + 1, nullptr);
 }
 
 int apspie_gen_weights_u32_device(apspie_ctx ctx, int m, const int *d_ptr, const int *d_ind,

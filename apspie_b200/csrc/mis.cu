@@ -227,7 +227,7 @@ int apspie_mis(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr, const int *
   auto *qb = (int *)workspace(ctx, kSlotMisQueueB, sizeof(int) * (size_t)m);
   if (!st || !qa || !qb) return APSPIE_ERR_OOM;
   ctx->mis_state = st;
-  int grid = mis_grid(ctx);
+  int grid = clamp_grid(ctx, mis_grid(ctx));
   if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_mis: occupancy query failed");
   int init_grid = std::min((m + 255) / 256, ctx->num_sms * 8);
   mis_init<<<init_grid, 256, 0, ctx->stream>>>(m, d_mis, qa, st);

@@ -63,8 +63,8 @@ __global__ void scan_tile_sums(const T *in, long long n, T *sums) {
   if (threadIdx.x == 0) sums[blockIdx.x] = tot;
 }
 
-// Exclusive scan of sums[0..n) in one block (n <= kScanThreads * 64); writes
-// the grand total to *total.
+// Exclusive scan of sums[0..n) in one block, blockDim.x values per pass;
+// writes the grand total to *total.
 template <typename T>
 __global__ void scan_single_block(T *sums, int n, T *total) {
   __shared__ T sw[33];
@@ -112,7 +112,9 @@ template <typename T>
 int device_exclusive_scan(apspie_context *ctx, const T *in, T *out, long long n, T *d_total) {
   long long tiles = (n + kScanTile - 1) / kScanTile;
   if (tiles < 1) tiles = 1;
-  if (tiles > (long long)kScanThreads * 64)
+  // the tile sums are scanned by one block in a loop: fine up to 2^20 tiles
+  // (2^32 elements); T must hold the total
+  if (tiles > (1ll << 20))
     return set_error(ctx, APSPIE_ERR_OVERFLOW, "device scan: %lld elements too many", n);
   T *sums = (T *)workspace(ctx, kSlotScan, sizeof(T) * (size_t)(tiles + 1));
   if (!sums) return APSPIE_ERR_OOM;

@@ -8,14 +8,21 @@
 //   * admission: a query's device state (its result row plus its share of the
 //     traversal scratch) is charged against a byte budget; queries wait in
 //     arrival order until the budget allows them in;
-//   * coalescing: admitted BFS and SSSP queries are grouped by (graph, kind)
-//     into jobs of up to 64 sources and run by apspie_batch_run in ONE
-//     persistent launch; MIS queries run after it on the same stream;
-//   * continuous batching: there are two batch slots, each with its own
-//     context and stream.  While one slot's batch runs on the GPU, queries
-//     that arrive are admitted into the other slot and launched right away,
-//     so their work is queued behind (and its result copies overlap) the
-//     running batch instead of waiting for it to return to the host.
+//   * coalescing: the admitted BFS and SSSP queries of one (graph, kind) form
+//     a group, run by ONE apspie_batch_run (multi-source frontier matrix), or
+//     by the single-source kernel when the group has one query; an MIS query
+//     is a group of its own.  Groups are launched cheapest first
+//     (measured time per group, kept per graph and kind), and each group has
+//     its own completion event, so a quick query is not held back by a slow
+//     one of the same batch;
+//   * lanes: graphs whose traversals take many levels (found when the graph
+//     is added, by one probe BFS) run on a second stream with a small grid,
+//     next to the main lane, so their thousands of short levels do not keep
+//     the whole GPU from the other queries;
+//   * continuous batching: there are two batch slots.  While one slot's
+//     groups run, queries that arrive are admitted into the other slot and
+//     launched right away, queued on the GPU behind (and overlapping the
+//     copies of) the running ones.
 // Each query's result row is copied into the caller's host buffer, or into
 // its device buffer (or dropped, for load tests), and its latency (submit ->
 // result in host / device memory) is recorded.  MIS priorities (mt19937 of
@@ -54,14 +61,20 @@ struct Request {
   uint32_t seed;
   void *h_result;
   int32_t *d_result = nullptr;
+  bool to_stage = false;  // result copied to the slot's pinned staging rows only (replay)
   Clock::time_point t_submit;
   double latency_ms = 0;
   int status = APSPIE_OK;
   bool done = false;
   size_t bytes = 0;
-  // placement in the slot's device / staging buffers
-  size_t offset = 0;
+  size_t dev_off = 0;   // result row in the slot's device buffer
+  size_t host_off = 0;  // ... and in its pinned staging buffer (host results)
 };
+
+// A graph traversal is "deep" when a probe BFS takes more levels than this:
+// its queries go to the small-grid lane.
+constexpr int kDeepLevels = 64;
+constexpr int kDeepBlocks = 32;  // blocks of the deep lane's persistent launches
 
 struct GraphEntry {
   int m;
@@ -69,19 +82,32 @@ struct GraphEntry {
   const int *ptr, *ind, *tptr, *tind;
   const uint32_t *w;
   int symmetric;
+  bool deep;
+  float cost_ms[3];  // running estimate of one group's device time, per kind
+};
+
+struct Group {
+  int kind = 0, graph = 0, lane = 0;
+  std::vector<Request *> reqs;
+  cudaEvent_t start = nullptr, end = nullptr;
+  int status = APSPIE_OK;
+  bool done = false;
+};
+
+struct Lane {
+  apspie_ctx ctx = nullptr;
+  cudaStream_t stream = nullptr;
 };
 
 struct Slot {
-  apspie_ctx ctx = nullptr;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t done = nullptr;
+  Lane lane[2];
   int32_t *d_out = nullptr;
   size_t d_bytes = 0;
   void *h_stage = nullptr;
   size_t h_bytes = 0;
-  std::vector<Request *> reqs;
+  std::vector<Group> groups;
+  std::vector<cudaEvent_t> events;  // pool, two per group
   bool busy = false;
-  int launch_status = APSPIE_OK;
 };
 
 }  // namespace
@@ -90,7 +116,7 @@ struct apspie_server {
   int device = 0;
   size_t budget = 0;
   int max_batch = 256;
-  std::vector<GraphEntry> graphs;
+  std::deque<GraphEntry> graphs;  // stable references while graphs are added
   std::mutex mu;
   std::condition_variable cv;
   std::deque<Request *> pending;
@@ -100,6 +126,7 @@ struct apspie_server {
   std::thread worker;
   bool stop = false;
   Slot slots[2];
+  bool any_deep = false;
   int max_pending = 1 << 20;
   // MIS priorities per (graph, seed), on the device
   std::mutex prio_mu;
@@ -186,18 +213,59 @@ int get_prio(apspie_server *s, int graph, uint32_t seed, cudaStream_t stream, ui
   return APSPIE_OK;
 }
 
-// Completes the requests of a finished slot: results to the callers'
-// buffers, latencies, budget release.
-void finish_slot(apspie_server *s, Slot &sl) {
-  cudaError_t e = cudaEventSynchronize(sl.done);
-  int st = sl.launch_status;
-  if (st == APSPIE_OK && e != cudaSuccess) st = APSPIE_ERR_CUDA;
+// Levels of one BFS of graph g from its first vertex with edges, on a
+// context and stream of its own (the depth of the graph's traversals).
+int probe_levels(int device, const GraphEntry &g, int *levels) {
+  *levels = 0;
+  if (g.nnz == 0) return APSPIE_OK;
+  if (cudaSetDevice(device) != cudaSuccess) return APSPIE_ERR_CUDA;
+  const int nh = std::min(g.m, 4096);
+  std::vector<int> h(nh + 1);
+  if (cudaMemcpy(h.data(), g.ptr, sizeof(int) * (nh + 1), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    return APSPIE_ERR_CUDA;
+  }
+  int src = -1;
+  for (int u = 0; u < nh && src < 0; ++u)
+    if (h[u + 1] > h[u]) src = u;
+  if (src < 0) return APSPIE_OK;  // a sparse prefix: treat as shallow
+  cudaStream_t stream = nullptr;
+  apspie_ctx ctx = nullptr;
+  int32_t *depth = nullptr;
+  int st = APSPIE_ERR_CUDA;
+  if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) == cudaSuccess &&
+      cudaMalloc(&depth, 4 * (size_t)g.m) == cudaSuccess &&
+      apspie_ctx_create(device, stream, &ctx) == APSPIE_OK) {
+    const int *tp = g.tptr ? g.tptr : (g.symmetric ? g.ptr : nullptr);
+    const int *ti = g.tptr ? g.tind : (g.symmetric ? g.ind : nullptr);
+    st = apspie_bfs(ctx, src, g.nnz, g.m, g.ptr, g.ind, tp, ti, depth, 0);
+    apspie_bfs_stats bs;
+    if (st == APSPIE_OK) st = apspie_bfs_get_stats(ctx, &bs);
+    if (st == APSPIE_OK) *levels = bs.levels;
+  }
+  cudaGetLastError();
+  if (ctx) apspie_ctx_destroy(ctx);
+  cudaFree(depth);
+  if (stream) cudaStreamDestroy(stream);
+  return st;
+}
+
+// Completes the requests of a finished group: results to the callers'
+// buffers, latencies, budget release, the group's cost estimate.
+void finish_group(apspie_server *s, Slot &sl, Group &g) {
+  int st = g.status;
+  float ms = 0;
+  if (st == APSPIE_OK && cudaEventElapsedTime(&ms, g.start, g.end) != cudaSuccess) {
+    cudaGetLastError();
+    st = APSPIE_ERR_CUDA;
+  }
   auto now = Clock::now();
   std::lock_guard<std::mutex> lock(s->mu);
-  for (Request *r : sl.reqs) {
-    const GraphEntry &g = s->graphs[r->graph];
+  GraphEntry &ge = s->graphs[g.graph];
+  if (st == APSPIE_OK) ge.cost_ms[g.kind] = 0.5f * ge.cost_ms[g.kind] + 0.5f * ms;
+  for (Request *r : g.reqs) {
     if (st == APSPIE_OK && r->h_result)
-      std::memcpy(r->h_result, (char *)sl.h_stage + r->offset, 4 * (size_t)g.m);
+      std::memcpy(r->h_result, (char *)sl.h_stage + r->host_off, 4 * (size_t)ge.m);
     r->status = st;
     r->latency_ms = std::chrono::duration<double, std::milli>(now - r->t_submit).count();
     r->done = true;
@@ -205,139 +273,223 @@ void finish_slot(apspie_server *s, Slot &sl) {
     if (st == APSPIE_OK) s->latencies.push_back(r->latency_ms);
     ++s->completed;
   }
-  sl.reqs.clear();
-  sl.busy = false;
+  g.done = true;
   s->cv.notify_all();
 }
 
-// Builds and launches one batch on slot sl (requests already admitted).
-int launch_slot(apspie_server *s, Slot &sl) {
-  // layout: one m-row per request in the slot buffers
-  size_t total = 0;
-  for (Request *r : sl.reqs) {
-    r->offset = total;
-    total += 4 * (size_t)s->graphs[r->graph].m;
-  }
-  if (!ensure_device((void **)&sl.d_out, &sl.d_bytes, total) ||
-      !ensure_host(&sl.h_stage, &sl.h_bytes, total))
-    return APSPIE_ERR_OOM;
-  // group BFS / SSSP by (graph, type); consecutive rows in the slot buffer
-  std::map<std::pair<int, int>, std::vector<Request *>> groups;
-  std::vector<Request *> mis;
-  for (Request *r : sl.reqs) {
-    if (r->type == 2)
-      mis.push_back(r);
-    else
-      groups[{r->graph, r->type}].push_back(r);
-  }
-  std::vector<apspie_job> jobs;
-  std::vector<std::vector<int>> srcs;
-  std::vector<int32_t *> outs;
-  // results of a job are contiguous rows: lay the grouped requests out again
-  size_t off = 0;
-  for (auto &kv : groups)
-    for (Request *r : kv.second) {
-      r->offset = off;
-      off += 4 * (size_t)s->graphs[r->graph].m;
+// Completes every group of the slot whose work has finished (all of them,
+// waiting, when `wait`); frees the slot when none is left.
+void poll_slot(apspie_server *s, Slot &sl, bool wait) {
+  bool all = true;
+  for (Group &g : sl.groups) {
+    if (g.done) continue;
+    cudaError_t e = wait ? cudaEventSynchronize(g.end) : cudaEventQuery(g.end);
+    if (e == cudaErrorNotReady) {
+      all = false;
+      continue;
     }
-  for (Request *r : mis) {
-    r->offset = off;
-    off += 4 * (size_t)s->graphs[r->graph].m;
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      if (g.status == APSPIE_OK) g.status = APSPIE_ERR_CUDA;
+    }
+    finish_group(s, sl, g);
   }
-  srcs.reserve(groups.size());
-  for (auto &kv : groups) {
-    const GraphEntry &g = s->graphs[kv.first.first];
-    std::vector<int> sv;
-    for (Request *r : kv.second) sv.push_back(r->source);
-    srcs.push_back(std::move(sv));
+  if (all) {
+    sl.groups.clear();
+    sl.busy = false;
+  }
+}
+
+// Launches one group on its lane: the traversal into the group's rows of the
+// slot buffer, then the copies to the callers, between two timing events.
+int launch_group(apspie_server *s, Slot &sl, Group &g) {
+  const GraphEntry &ge = s->graphs[g.graph];
+  Lane &ln = sl.lane[g.lane];
+  cudaEventRecord(g.start, ln.stream);
+  int st = APSPIE_OK;
+  const size_t row = 4 * (size_t)ge.m;
+  if (g.kind == 2) {
+    Request *r = g.reqs.front();
+    uint32_t *prio = nullptr;
+    st = get_prio(s, g.graph, r->seed, ln.stream, &prio);
+    if (st == APSPIE_OK)
+      st = apspie_mis(ln.ctx, ge.nnz, ge.m, ge.ptr, ge.ind, prio,
+                      (int32_t *)((char *)sl.d_out + r->dev_off), 1.0f);
+  } else if (g.reqs.size() == 1) {
+    // one source: the single-source kernels are the faster path
+    Request *r = g.reqs.front();
+    int32_t *out = (int32_t *)((char *)sl.d_out + r->dev_off);
+    if (g.kind == 0) {
+      const int *tp = ge.tptr ? ge.tptr : (ge.symmetric ? ge.ptr : nullptr);
+      const int *ti = ge.tptr ? ge.tind : (ge.symmetric ? ge.ind : nullptr);
+      st = apspie_bfs(ln.ctx, r->source, ge.nnz, ge.m, ge.ptr, ge.ind, tp, ti, out, 0);
+    } else {
+      st = apspie_sssp_u32(ln.ctx, r->source, ge.nnz, ge.m, ge.ptr, ge.ind, ge.w,
+                           (uint32_t *)out, 0);
+    }
+  } else {
+    std::vector<int> src;
+    for (Request *r : g.reqs) src.push_back(r->source);
     apspie_job j;
     std::memset(&j, 0, sizeof(j));
-    j.type = kv.first.second == 0 ? APSPIE_JOB_BFS : APSPIE_JOB_SSSP_U32;
-    j.m = g.m;
-    j.nnz = g.nnz;
-    j.d_ptr = g.ptr;
-    j.d_ind = g.ind;
-    j.d_tptr = g.tptr;
-    j.d_tind = g.tind;
-    j.d_w = g.w;
-    j.symmetric = g.symmetric;
-    j.nsrc = (int)srcs.back().size();
-    j.h_src = srcs.back().data();
-    j.d_out = (int32_t *)((char *)sl.d_out + kv.second.front()->offset);
+    j.type = g.kind == 0 ? APSPIE_JOB_BFS : APSPIE_JOB_SSSP_U32;
+    j.m = ge.m;
+    j.nnz = ge.nnz;
+    j.d_ptr = ge.ptr;
+    j.d_ind = ge.ind;
+    j.d_tptr = ge.tptr;
+    j.d_tind = ge.tind;
+    j.d_w = ge.w;
+    j.symmetric = ge.symmetric;
+    j.nsrc = (int)src.size();
+    j.h_src = src.data();
+    j.d_out = (int32_t *)((char *)sl.d_out + g.reqs.front()->dev_off);
     j.alpha = -1;
     j.beta = -1;
-    jobs.push_back(j);
-  }
-  int st = APSPIE_OK;
-  if (!jobs.empty()) {
-    // at most 64 device jobs per launch: split the job list if needed
-    size_t first = 0;
-    while (first < jobs.size() && st == APSPIE_OK) {
-      size_t n = 0, parts = 0;
-      while (first + n < jobs.size()) {
-        size_t p = (jobs[first + n].nsrc + 63) / 64;
-        if (parts + p > 64) break;
-        parts += p;
-        ++n;
-      }
-      if (n == 0) n = 1;  // a single job beyond 64 device jobs: reported as an error below
-      st = apspie_batch_run(sl.ctx, (int)n, jobs.data() + first, 0);
-      s->launched_jobs += n;
-      first += n;
-    }
-  }
-  for (Request *r : mis) {
-    if (st != APSPIE_OK) break;
-    const GraphEntry &g = s->graphs[r->graph];
-    uint32_t *prio = nullptr;
-    st = get_prio(s, r->graph, r->seed, sl.stream, &prio);
-    if (st == APSPIE_OK)
-      st = apspie_mis(sl.ctx, g.nnz, g.m, g.ptr, g.ind, prio,
-                      (int32_t *)((char *)sl.d_out + r->offset), 1.0f);
+    st = apspie_batch_run(ln.ctx, 1, &j, 0);
+    ++s->launched_jobs;
   }
   // results to the callers: host rows through the staging buffer, device
   // rows directly; a query with neither only has its latency recorded
-  for (Request *r : sl.reqs) {
+  for (Request *r : g.reqs) {
     if (st != APSPIE_OK) break;
-    const size_t bytes = 4 * (size_t)s->graphs[r->graph].m;
     cudaError_t e = cudaSuccess;
-    if (r->h_result)
-      e = cudaMemcpyAsync((char *)sl.h_stage + r->offset, (char *)sl.d_out + r->offset, bytes,
-                          cudaMemcpyDeviceToHost, sl.stream);
+    if (r->h_result || r->to_stage)
+      e = cudaMemcpyAsync((char *)sl.h_stage + r->host_off, (char *)sl.d_out + r->dev_off, row,
+                          cudaMemcpyDeviceToHost, ln.stream);
     if (e == cudaSuccess && r->d_result)
-      e = cudaMemcpyAsync(r->d_result, (char *)sl.d_out + r->offset, bytes,
-                          cudaMemcpyDeviceToDevice, sl.stream);
+      e = cudaMemcpyAsync(r->d_result, (char *)sl.d_out + r->dev_off, row,
+                          cudaMemcpyDeviceToDevice, ln.stream);
     if (e != cudaSuccess) st = APSPIE_ERR_CUDA;
   }
-  cudaEventRecord(sl.done, sl.stream);
+  cudaEventRecord(g.end, ln.stream);
   return st;
+}
+
+// Builds the groups of a batch on slot sl and launches them, cheapest first.
+void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    // with deep graphs around, the main lane leaves room for the deep lane
+    int resident = 0;
+    apspie_ctx_resident_blocks(sl.lane[0].ctx, &resident);
+    apspie_ctx_set_max_grid(sl.lane[0].ctx, s->any_deep ? std::max(1, resident - kDeepBlocks) : 0);
+  }
+  std::map<std::pair<int, int>, size_t> index;
+  sl.groups.clear();
+  for (Request *r : batch) {
+    if (r->type == 2) {
+      sl.groups.emplace_back();
+      sl.groups.back().kind = 2;
+      sl.groups.back().graph = r->graph;
+      sl.groups.back().reqs.push_back(r);
+      continue;
+    }
+    auto key = std::make_pair(r->graph, r->type);
+    auto it = index.find(key);
+    if (it == index.end()) {
+      index[key] = sl.groups.size();
+      sl.groups.emplace_back();
+      sl.groups.back().kind = r->type;
+      sl.groups.back().graph = r->graph;
+      sl.groups.back().reqs.push_back(r);
+    } else {
+      sl.groups[it->second].reqs.push_back(r);
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    for (Group &g : sl.groups) g.lane = (s->graphs[g.graph].deep && g.kind != 2) ? 1 : 0;
+    std::stable_sort(sl.groups.begin(), sl.groups.end(), [&](const Group &a, const Group &b) {
+      return s->graphs[a.graph].cost_ms[a.kind] < s->graphs[b.graph].cost_ms[b.kind];
+    });
+  }
+  // rows: a group's results are consecutive (a batch job writes [nsrc][m])
+  // (replayed results that only have to reach host memory all land on the
+  // same staging row: the copy is what is measured, not the bytes kept)
+  size_t dev = 0, host = 0, sink = 0;
+  for (Group &g : sl.groups)
+    for (Request *r : g.reqs) {
+      const size_t row = 4 * (size_t)s->graphs[r->graph].m;
+      r->dev_off = dev;
+      dev += row;
+      if (r->h_result) {
+        r->host_off = host;
+        host += row;
+      } else if (r->to_stage) {
+        sink = std::max(sink, row);
+      }
+    }
+  for (Group &g : sl.groups)
+    for (Request *r : g.reqs)
+      if (!r->h_result && r->to_stage) r->host_off = host;
+  host += sink;
+  while (sl.events.size() < 2 * sl.groups.size()) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      cudaGetLastError();
+      break;
+    }
+    sl.events.push_back(e);
+  }
+  const bool buffers = sl.events.size() >= 2 * sl.groups.size() &&
+                       ensure_device((void **)&sl.d_out, &sl.d_bytes, dev) &&
+                       (host == 0 || ensure_host(&sl.h_stage, &sl.h_bytes, host));
+  for (size_t i = 0; i < sl.groups.size(); ++i) {
+    Group &g = sl.groups[i];
+    if (!buffers) {
+      g.status = APSPIE_ERR_OOM;
+      continue;
+    }
+    g.start = sl.events[2 * i];
+    g.end = sl.events[2 * i + 1];
+    g.status = launch_group(s, sl, g);
+  }
+  if (!buffers) {
+    // nothing was launched: complete the groups with the error
+    for (Group &g : sl.groups) {
+      g.start = g.end = nullptr;
+      std::lock_guard<std::mutex> lock(s->mu);
+      for (Request *r : g.reqs) {
+        r->status = APSPIE_ERR_OOM;
+        r->done = true;
+        s->in_flight -= r->bytes;
+        ++s->completed;
+      }
+      g.done = true;
+    }
+    s->cv.notify_all();
+    sl.groups.clear();
+    return;
+  }
+  sl.busy = true;
 }
 
 void worker_main(apspie_server *s) {
   cudaSetDevice(s->device);
   for (;;) {
-    // finish any slot whose batch completed
     for (Slot &sl : s->slots)
-      if (sl.busy && cudaEventQuery(sl.done) != cudaErrorNotReady) finish_slot(s, sl);
+      if (sl.busy) poll_slot(s, sl, false);
     Slot *free_slot = nullptr;
     for (Slot &sl : s->slots)
       if (!sl.busy) free_slot = &sl;
     if (!free_slot) {
-      // both batches in flight: wait for the older one
-      Slot *older = &s->slots[0];
-      finish_slot(s, *older);
+      // both batches in flight: wait for the older slot's next group
+      Slot &older = s->slots[0];
+      for (Group &g : older.groups)
+        if (!g.done) {
+          cudaEventSynchronize(g.end);
+          break;
+        }
       continue;
     }
     std::vector<Request *> batch;
     {
       std::unique_lock<std::mutex> lock(s->mu);
-      if (s->stop && s->pending.empty()) {
-        bool idle = !s->slots[0].busy && !s->slots[1].busy;
-        if (idle) return;
-      }
+      const bool any_busy = s->slots[0].busy || s->slots[1].busy;
+      if (s->stop && s->pending.empty() && !any_busy) return;
       if (s->pending.empty()) {
-        bool any_busy = s->slots[0].busy || s->slots[1].busy;
-        s->cv.wait_for(lock, std::chrono::microseconds(any_busy ? 50 : 2000));
+        s->cv.wait_for(lock, std::chrono::microseconds(any_busy ? 20 : 2000));
         continue;
       }
       // admit in arrival order while the budget allows
@@ -350,17 +502,19 @@ void worker_main(apspie_server *s) {
       }
     }
     if (batch.empty()) {
-      // over budget: wait for a running batch to release memory
+      // over budget: wait for a running group to release memory
       for (Slot &sl : s->slots)
         if (sl.busy) {
-          finish_slot(s, sl);
+          for (Group &g : sl.groups)
+            if (!g.done) {
+              cudaEventSynchronize(g.end);
+              break;
+            }
           break;
         }
       continue;
     }
-    free_slot->reqs = std::move(batch);
-    free_slot->busy = true;
-    free_slot->launch_status = launch_slot(s, *free_slot);
+    launch_slot(s, *free_slot, std::move(batch));
     ++s->batches;
   }
 }
@@ -383,15 +537,17 @@ int apspie_server_create(int device, size_t state_budget_bytes, int max_batch,
     delete s;
     return APSPIE_ERR_INVALID;
   }
-  for (Slot &sl : s->slots) {
-    if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
-        apspie_ctx_create(device, sl.stream, &sl.ctx) != APSPIE_OK) {
-      cudaGetLastError();
-      delete s;
-      return APSPIE_ERR_CUDA;
+  for (Slot &sl : s->slots)
+    for (int l = 0; l < 2; ++l) {
+      Lane &ln = sl.lane[l];
+      if (cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking) != cudaSuccess ||
+          apspie_ctx_create(device, ln.stream, &ln.ctx) != APSPIE_OK) {
+        cudaGetLastError();
+        apspie_server_destroy(s);
+        return APSPIE_ERR_CUDA;
+      }
+      if (l == 1) apspie_ctx_set_max_grid(ln.ctx, kDeepBlocks);
     }
-  }
   s->worker = std::thread(worker_main, s);
   *out = s;
   return APSPIE_OK;
@@ -402,8 +558,18 @@ int apspie_server_add_graph(apspie_server_t s, int m, int64_t nnz, const int *d_
                             const uint32_t *d_w, int symmetric, int *graph_id) {
   if (!s || m <= 0 || nnz < 0 || !d_ptr || (nnz > 0 && !d_ind) || !graph_id)
     return APSPIE_ERR_INVALID;
+  GraphEntry g{m, nnz, d_ptr, d_ind, d_tptr, d_tind, d_w, symmetric, false, {0, 0, 0}};
+  int levels = 0;
+  int st = probe_levels(s->device, g, &levels);
+  if (st != APSPIE_OK) return st;
+  g.deep = levels > kDeepLevels;
+  // first guesses of a group's device time, replaced by measurements
+  g.cost_ms[0] = 1e-6f * (float)nnz * (g.deep ? 100.0f : 1.0f);
+  g.cost_ms[1] = 4.0f * g.cost_ms[0];
+  g.cost_ms[2] = 2.0f * g.cost_ms[0];
   std::lock_guard<std::mutex> lock(s->mu);
-  s->graphs.push_back(GraphEntry{m, nnz, d_ptr, d_ind, d_tptr, d_tind, d_w, symmetric});
+  s->graphs.push_back(g);
+  if (g.deep) s->any_deep = true;
   *graph_id = (int)s->graphs.size() - 1;
   return APSPIE_OK;
 }
@@ -474,8 +640,8 @@ int apspie_server_submit_device(apspie_server_t s, int type, int graph, int sour
   return st;
 }
 
-int apspie_server_replay(apspie_server_t s, int n, const apspie_query *q, double *lat_ms,
-                         double *wall_ms) {
+int apspie_server_replay(apspie_server_t s, int n, const apspie_query *q, int to_host,
+                         double *lat_ms, double *wall_ms) {
   if (!s || n < 0 || (n > 0 && (!q || !lat_ms))) return APSPIE_ERR_INVALID;
   {
     std::lock_guard<std::mutex> lock(s->mu);
@@ -500,6 +666,7 @@ int apspie_server_replay(apspie_server_t s, int n, const apspie_query *q, double
       std::this_thread::sleep_for(std::chrono::microseconds(100));
       s->mu.lock();
     }
+    if (st == APSPIE_OK) rs[i]->to_stage = to_host != 0;
   }
   double last = 0;
   std::unique_lock<std::mutex> lock(s->mu);
@@ -525,8 +692,8 @@ int apspie_server_replay(apspie_server_t s, int n, const apspie_query *q, double
   return st;
 }
 
-int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q, double *lat_ms,
-                               double *wall_ms) {
+int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q, int to_host,
+                               double *lat_ms, double *wall_ms) {
   if (!s || n < 0 || (n > 0 && (!q || !lat_ms))) return APSPIE_ERR_INVALID;
   int maxm = 0;
   {
@@ -541,9 +708,12 @@ int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q, 
   cudaStream_t stream = nullptr;
   apspie_ctx ctx = nullptr;
   int32_t *row = nullptr;
+  void *h_row = nullptr;
   if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc(&row, 4 * (size_t)std::max(maxm, 1)) != cudaSuccess) {
+      cudaMalloc(&row, 4 * (size_t)std::max(maxm, 1)) != cudaSuccess ||
+      (to_host && cudaMallocHost(&h_row, 4 * (size_t)std::max(maxm, 1)) != cudaSuccess)) {
     cudaGetLastError();
+    cudaFree(row);
     if (stream) cudaStreamDestroy(stream);
     return APSPIE_ERR_OOM;
   }
@@ -565,6 +735,9 @@ int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q, 
       st = get_prio(s, q[i].graph, q[i].seed, stream, &prio);
       if (st == APSPIE_OK) st = apspie_mis(ctx, g.nnz, g.m, g.ptr, g.ind, prio, row, 1.0f);
     }
+    if (st == APSPIE_OK && to_host &&
+        cudaMemcpyAsync(h_row, row, 4 * (size_t)g.m, cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+      st = APSPIE_ERR_CUDA;
     if (st == APSPIE_OK && cudaStreamSynchronize(stream) != cudaSuccess) st = APSPIE_ERR_CUDA;
     const double l = std::chrono::duration<double, std::milli>(Clock::now() - at).count();
     lat_ms[i] = l;
@@ -572,6 +745,7 @@ int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q, 
   }
   if (ctx) apspie_ctx_destroy(ctx);
   cudaFree(row);
+  if (h_row) cudaFreeHost(h_row);
   cudaStreamDestroy(stream);
   if (wall_ms) *wall_ms = last;
   return st;
@@ -650,10 +824,12 @@ int apspie_server_destroy(apspie_server_t s) {
   if (s->worker.joinable()) s->worker.join();
   cudaSetDevice(s->device);
   for (Slot &sl : s->slots) {
-    if (sl.stream) cudaStreamSynchronize(sl.stream);
-    if (sl.ctx) apspie_ctx_destroy(sl.ctx);
-    if (sl.done) cudaEventDestroy(sl.done);
-    if (sl.stream) cudaStreamDestroy(sl.stream);
+    for (Lane &ln : sl.lane) {
+      if (ln.stream) cudaStreamSynchronize(ln.stream);
+      if (ln.ctx) apspie_ctx_destroy(ln.ctx);
+      if (ln.stream) cudaStreamDestroy(ln.stream);
+    }
+    for (cudaEvent_t e : sl.events) cudaEventDestroy(e);
     cudaFree(sl.d_out);
     if (sl.h_stage) cudaFreeHost(sl.h_stage);
   }

@@ -41,6 +41,16 @@ namespace {
 
 constexpr int kSsspThreads = 512;
 
+constexpr int kSsspTraceRounds = 64;  // rounds recorded in the per-run trace
+
+struct RoundTrace {
+  unsigned frontier;          // queued vertices + big-list vertices
+  unsigned phase;
+  unsigned long long edges;   // their out-edges
+  unsigned long long t_last;  // %globaltimer when the last block finished its share
+  unsigned long long t_end;   // ... and when the round's barrier released
+};
+
 struct SsspState {
   LevelCounters c[3];
   unsigned far_count[3];  // far lists rotate by phase
@@ -53,6 +63,8 @@ struct SsspState {
   unsigned long long relaxations;  // edges scanned over all rounds
   unsigned long long reached;
   unsigned long long edges;        // sum of out-degrees of reached vertices
+  unsigned long long t_start;
+  RoundTrace trace[kSsspTraceRounds];
 };
 
 template <typename W>
@@ -140,6 +152,7 @@ __global__ void sssp_init(int m, int src, unsigned *dist, int *stamp, int *fstam
       st->err = 0;
       st->rounds = 0;
       st->phases = 0;
+      for (int i = 0; i < kSsspTraceRounds; ++i) st->trace[i] = RoundTrace{0, 0, 0ull, 0ull, 0ull};
       st->relaxations = 0;
       st->reached = 0;
       st->edges = 0;
@@ -160,6 +173,7 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
   __shared__ unsigned long long s_edges;
   unsigned long long relax = 0;
   // T = infinity without near-far; else the first phase covers [0, delta)
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->t_start = globaltimer();
   unsigned thresh = delta ? delta : Arith<W>::kInf;
   int phase = 0;
   int r = 0;
@@ -229,14 +243,25 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
     int *fout = phase % 3 == 0 ? far0 : (phase % 3 == 1 ? far1 : far2);
     SsspVisit<W> vis{w,    dist,   stamp, fstamp, r, phase, thresh, fout, &st->far_count[phase % 3],
                      &st->far_min[phase % 3]};
-    expand_push(ptr, ind, qin, nq, cin, s_nbig, nch, qout, cout, nxt, gwarp, nwarps,
+    expand_push(ptr, ind, qin, nq, cin, s_nbig, nch, qout, cout, nxt, cur, gwarp, nwarps,
                 [&](int v) {
                   const unsigned d = __ldcg(dist + v);
                   xd[v] = d;  // the distance v is expanded with
                   return d;
                 },
                 vis);
+    if (r < kSsspTraceRounds) {
+      __syncthreads();
+      if (threadIdx.x == 0) atomicMax(&st->trace[r].t_last, globaltimer());
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->trace[r].frontier = nq + s_nbig;
+        st->trace[r].phase = (unsigned)phase;
+        st->trace[r].edges = s_edges;
+      }
+    }
     if (!grid_barrier(st->bar, &st->err)) return;
+    if (r < kSsspTraceRounds && blockIdx.x == 0 && threadIdx.x == 0)
+      st->trace[r].t_end = globaltimer();
   }
   // reached vertices and their out-degrees (E_R)
   unsigned long long cnt = 0, edg = 0;
@@ -298,7 +323,7 @@ int sssp_run(apspie_context *ctx, int src, int64_t nnz, int m, const int *d_ptr,
   int *fstamp = nf, *far0 = nf + 2 * mm, *far1 = nf + 3 * mm, *far2 = nf + 4 * mm;
   unsigned *xd = (unsigned *)(nf + mm);
   ctx->sssp_state = st;
-  int grid = sssp_grid<W>(ctx);
+  int grid = clamp_grid(ctx, sssp_grid<W>(ctx));
   if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_sssp: occupancy query failed");
   int init_grid = std::min((m + 255) / 256, ctx->num_sms * 8);
   sssp_init<W><<<init_grid, 256, 0, ctx->stream>>>(m, src, d_dist, stamp, fstamp, xd, d_ptr, qa,
@@ -343,6 +368,33 @@ int apspie_sssp_set_params(apspie_ctx ctx, uint32_t delta_u32, float delta_f32) 
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_sssp_set_params: bad float delta");
   ctx->sssp_delta_u32 = delta_u32;
   ctx->sssp_delta_f32 = delta_f32;
+  return APSPIE_OK;
+}
+
+int apspie_sssp_get_trace(apspie_ctx ctx, int max_rounds, int *n_out, int64_t *h_frontier,
+                          int64_t *h_frontier_edges, int64_t *h_ns, int64_t *h_work_last_ns) {
+  APSPIE_CHECK_CTX(ctx);
+  if (!ctx->sssp_state || max_rounds < 0 || !n_out)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_sssp_get_trace: no SSSP has run");
+  auto *h = (SsspState *)pinned(ctx, sizeof(SsspState));
+  if (!h) return APSPIE_ERR_OOM;
+  cudaError_t e = cudaMemcpyAsync(h, ctx->sssp_state, sizeof(SsspState), cudaMemcpyDeviceToHost,
+                                  ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return check_cuda(ctx, e, "apspie_sssp_get_trace");
+  const int n = std::min(std::min(max_rounds, kSsspTraceRounds), h->rounds);
+  unsigned long long prev = h->t_start;
+  int k = 0;
+  for (int i = 0; i < n; ++i) {
+    if (h->trace[i].t_end == 0) continue;  // a phase change round (no expansion)
+    if (h_frontier) h_frontier[k] = h->trace[i].frontier;
+    if (h_frontier_edges) h_frontier_edges[k] = (int64_t)h->trace[i].edges;
+    if (h_ns) h_ns[k] = (int64_t)(h->trace[i].t_end - prev);
+    if (h_work_last_ns) h_work_last_ns[k] = (int64_t)(h->trace[i].t_last - prev);
+    prev = h->trace[i].t_end;
+    ++k;
+  }
+  *n_out = k;
   return APSPIE_OK;
 }
 

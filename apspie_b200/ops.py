@@ -78,11 +78,27 @@ def bfs(ctx: Context, g, src: int, depth=None, max_levels: int = 0):
     import torch
     if depth is None:
         depth = torch.empty(g.m, dtype=torch.int32, device=g.ptr.device)
-    tptr, tind = (g.ptr, g.ind) if g.symmetric else (g.tptr, g.tind)
+    if getattr(g, "tptr", None) is not None:
+        tptr, tind = g.tptr, g.tind
+    else:
+        tptr, tind = (g.ptr, g.ind) if g.symmetric else (None, None)
     check(lib.apspie_bfs(ctx.handle, int(src), int(g.nnz), int(g.m), _p(g.ptr), _p(g.ind),
                          _p(tptr), _p(tind), _p(depth), int(max_levels)), ctx.handle,
           "apspie_bfs")
     return depth
+
+
+def bfs_prepare(ctx: Context, g):
+    """Pull-ordered in-adjacency of g (apspie_bfs_prepare): sets g.tptr /
+    g.tind, which bfs() then pulls over."""
+    import torch
+    dev = g.ptr.device
+    tptr = torch.empty(g.m + 1, dtype=torch.int32, device=dev)
+    tind = torch.empty(max(g.nnz, 1), dtype=torch.int32, device=dev)
+    check(lib.apspie_bfs_prepare(ctx.handle, int(g.m), int(g.nnz), _p(g.ptr), _p(g.ind),
+                                 _p(tptr), _p(tind)), ctx.handle, "apspie_bfs_prepare")
+    g.tptr, g.tind = tptr, tind[:g.nnz]
+    return g
 
 
 def bfs_trace(ctx: Context, max_levels: int = 64) -> list[dict]:
@@ -148,6 +164,18 @@ def sssp_stats(ctx: Context) -> dict:
     check(lib.apspie_sssp_get_stats(ctx.handle, C.byref(s)), ctx.handle, "apspie_sssp_get_stats")
     return {"rounds": s.rounds, "phases": s.phases, "vertices_reached": s.vertices_reached,
             "edges_traversed": s.edges_traversed, "relaxations": s.relaxations}
+
+
+def sssp_trace(ctx: Context, max_rounds: int = 64) -> list[dict]:
+    """Per-round frontier, out-edges and device us of the last SSSP."""
+    import numpy as np
+    nf, mf, ns, wl = (np.zeros(max_rounds, np.int64) for _ in range(4))
+    cnt = C.c_int()
+    check(lib.apspie_sssp_get_trace(ctx.handle, max_rounds, C.byref(cnt), nf.ctypes.data,
+                                    mf.ctypes.data, ns.ctypes.data, wl.ctypes.data), ctx.handle,
+          "apspie_sssp_get_trace")
+    return [{"round": i, "frontier": int(nf[i]), "frontier_edges": int(mf[i]),
+             "us": ns[i] / 1e3, "work_last_us": wl[i] / 1e3} for i in range(cnt.value)]
 
 
 def sssp_set_params(ctx: Context, delta_u32: int = 0, delta_f32: float = 0.0) -> None:
@@ -222,6 +250,19 @@ def _csr(m, n, ptr, ind, val) -> Csr:
     return Csr(int(m), int(n), int(ind.numel()) if ind is not None else 0,
                C.c_void_p(ptr.data_ptr()), C.c_void_p(0 if ind is None else ind.data_ptr()),
                C.c_void_p(0 if val is None else val.data_ptr()))
+
+
+def spmv(ctx: Context, m: int, ptr, ind, val, x, semiring: int = 0, y=None):
+    """Dense SpMV over every row (apspie_spmv; the reference's spmv() /
+    cuspmv()): y[r] = (+)_k A(r, ind[k]) (x) x[ind[k]].  val may be None
+    (ones)."""
+    import torch
+    if y is None:
+        y = torch.empty(m, dtype=torch.float32, device=ptr.device)
+    nnz = int(ind.numel()) if ind is not None else 0
+    check(lib.apspie_spmv(ctx.handle, int(semiring), int(m), nnz, _p(ptr), _p(ind), _p(val),
+                          _p(x), _p(y)), ctx.handle, "apspie_spmv")
+    return y
 
 
 def spgemm(ctx: Context, A, B):

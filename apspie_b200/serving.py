@@ -62,17 +62,19 @@ class Server:
         self._live[rid.value] = out
         return rid.value
 
-    def replay(self, queries, plain: bool = False):
+    def replay(self, queries, plain: bool = False, to_host: bool = True):
         """Open-loop replay of a timed query stream: `queries` is a structured
         array with fields type, graph, source, seed, t_us (see QUERY_DTYPE).
-        Returns (latencies_ms array, wall_ms).  plain=True runs the stream one
-        query at a time through the single-query kernels instead."""
+        Returns (latencies_ms array, wall_ms); a latency runs from the query's
+        arrival until its result is in host memory (to_host) or on the device.
+        plain=True runs the stream one query at a time through the
+        single-query kernels instead."""
         q = np.ascontiguousarray(queries, dtype=QUERY_DTYPE)
         lat = np.zeros(len(q), dtype=np.float64)
         wall = C.c_double()
         fn = lib.apspie_server_replay_plain if plain else lib.apspie_server_replay
-        check(fn(self._h, len(q), C.c_void_p(q.ctypes.data), C.c_void_p(lat.ctypes.data),
-                 C.byref(wall)), what="apspie_server_replay")
+        check(fn(self._h, len(q), C.c_void_p(q.ctypes.data), int(bool(to_host)),
+                 C.c_void_p(lat.ctypes.data), C.byref(wall)), what="apspie_server_replay")
         return lat, wall.value
 
     def wait(self, rid: int):

@@ -50,6 +50,13 @@ typedef struct apspie_context *apspie_ctx;
 int apspie_ctx_create(int device, void *stream, apspie_ctx *out);
 int apspie_ctx_destroy(apspie_ctx ctx);
 int apspie_ctx_set_stream(apspie_ctx ctx, void *stream);
+/* Caps the blocks of this context's persistent launches (BFS, SSSP, MIS,
+ * batch); 0 = as many as fit (the default).  Two contexts whose caps add up
+ * to at most apspie_ctx_resident_blocks can run persistent kernels at the
+ * same time on different streams. */
+int apspie_ctx_set_max_grid(apspie_ctx ctx, int blocks);
+/* A cap that every persistent kernel of the library fits (2 per SM). */
+int apspie_ctx_resident_blocks(apspie_ctx ctx, int *blocks);
 int apspie_ctx_sync(apspie_ctx ctx);
 /* Number of kernels this context has launched since creation. */
 int apspie_ctx_launch_count(apspie_ctx ctx, uint64_t *out);
@@ -83,6 +90,18 @@ typedef struct {
 /* Statistics of the last apspie_bfs on this context (synchronises). Also
  * reports a device-side timeout of that run as APSPIE_ERR_TIMEOUT. */
 int apspie_bfs_get_stats(apspie_ctx ctx, apspie_bfs_stats *out);
+
+/* Builds the in-adjacency that apspie_bfs pulls over (d_tptr: m + 1
+ * offsets, d_tind: nnz indices, caller-allocated) from the out-adjacency,
+ * each row ordered by the neighbours' out-degree, highest first (ties by
+ * id).  A vertex still unvisited at level L has no neighbour above depth L,
+ * and its best-connected neighbours are the likeliest to be in the level's
+ * frontier, so a pull probe hits sooner.  Depths do not depend on the order.
+ * A one-time graph build step (a radix sort of the edges), like building
+ * the transpose; pass the result as d_tptr / d_tind (also for an undirected
+ * graph, instead of repeating d_ptr / d_ind). */
+int apspie_bfs_prepare(apspie_ctx ctx, int m, int64_t nnz, const int *d_ptr,
+                       const int *d_ind, int *d_tptr, int *d_tind);
 
 /* Per-level trace of the last apspie_bfs (synchronises): for each level
  * i < max_levels (at most 64) the direction (1 push, 2 pull), frontier size,
@@ -156,6 +175,14 @@ typedef struct {
  * default) = T infinite, i.e. frontier Bellman-Ford.  The distances do not
  * depend on delta (same fixpoint); the work and the number of rounds do. */
 int apspie_sssp_set_params(apspie_ctx ctx, uint32_t delta_u32, float delta_f32);
+
+/* Per-round trace of the last SSSP (synchronises), expansion rounds only
+ * (at most 64): frontier vertices, their out-edges, device ns of the round
+ * and ns until the last block finished its share (the rest is the grid
+ * barrier).  *n_out = rounds written; the arrays may be NULL. */
+int apspie_sssp_get_trace(apspie_ctx ctx, int max_rounds, int *n_out,
+                          int64_t *h_frontier, int64_t *h_frontier_edges,
+                          int64_t *h_ns, int64_t *h_work_last_ns);
 
 /* Statistics of the last SSSP on this context (synchronises). */
 int apspie_sssp_get_stats(apspie_ctx ctx, apspie_sssp_stats *out);
@@ -259,16 +286,18 @@ typedef struct {
   uint32_t seed;
   double t_us;
 } apspie_query;
-/* Open-loop replay: submits query i at its arrival time (results dropped) and
- * waits for all; lat_ms[i] = arrival -> result on the device; *wall_ms =
- * stream start -> last completion. */
+/* Open-loop replay: submits query i at its arrival time and waits for all;
+ * lat_ms[i] = arrival -> result in host memory (to_host != 0: each result
+ * row is copied into the server's pinned staging memory) or on the device
+ * (to_host == 0); results are not kept.  *wall_ms = stream start -> last
+ * completion. */
 int apspie_server_replay(apspie_server_t s, int n, const apspie_query *q,
-                         double *lat_ms, double *wall_ms);
+                         int to_host, double *lat_ms, double *wall_ms);
 /* The same stream one query at a time, in arrival order, through
  * apspie_bfs / apspie_sssp_u32 / apspie_mis on a stream of its own (the
  * plain single-query path); latencies likewise from the arrival times. */
 int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q,
-                               double *lat_ms, double *wall_ms);
+                               int to_host, double *lat_ms, double *wall_ms);
 /* *done = 1 once the result is in h_result (the request is then retired and
  * its status returned). */
 int apspie_server_poll(apspie_server_t s, uint64_t req_id, int *done,
@@ -323,6 +352,16 @@ int apspie_spmspv(apspie_ctx ctx, int semiring, int m, int64_t nnz,
                   const int *d_ptr, const int *d_ind, const float *d_val,
                   int xnnz, const int *d_xind, const float *d_xval, int *d_yind,
                   float *d_yval, int *h_ynnz, int64_t *h_expanded);
+
+/* Dense SpMV over every row: y[r] = (+) over row r's entries k of
+ * A(r, ind[k]) (x) x[ind[k]] (d_val NULL = ones), for all m rows; an empty
+ * row gets the (+) identity (0, or +/-FLT_MAX for MIN_PLUS / MAX_TIMES).
+ * Replaces the dense spmv() (mgpu::SpmvCsrBinary, src/bfs.cuh:12-14) and
+ * cuspmv() (cusparseScsrmv, src/tc.cuh:18-59).  PLUS_TIMES sums in double
+ * and rounds once; each row is reduced in a fixed order.  No sync. */
+int apspie_spmv(apspie_ctx ctx, int semiring, int m, int64_t nnz,
+                const int *d_ptr, const int *d_ind, const float *d_val,
+                const float *d_x, float *d_y);
 
 /* Dense x in, dense y out: the dense mXv<T>() (src/mXv.cuh:111-247) and
  * spmspvSssp (src/spmspvSssp.cuh:92).  The frontier is {j : x[j] > 0.5}

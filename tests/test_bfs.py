@@ -137,3 +137,29 @@ def test_bfs_repeated_runs_with_direction_switches(ctx):
                     if t["queued"]:
                         assert t["queued"] == t["frontier"]
         assert "pull" in dirs and dirs[-1] == "push"
+
+
+@pytest.mark.parametrize("symmetric", [True, False])
+@pytest.mark.parametrize("mode", [0, 2])
+def test_bfs_prepared_in_adjacency(ctx, symmetric, mode):
+    """apspie_bfs_prepare: each in-row is the set of in-neighbours ordered by
+    out-degree (highest first, ties by id), and BFS over it gives the same
+    depths as the oracle."""
+    import apspie_b200 as ap
+    h = ap.gen_rmat(14, 16, seed=21, symmetric=symmetric)
+    g = ap.bfs_prepare(ctx, h.to_device(with_transpose=False))
+    tptr, tind = g.tptr.cpu().numpy(), g.tind.cpu().numpy()
+    tr = h.transpose()
+    deg = np.diff(h.ptr)
+    np.testing.assert_array_equal(tptr, tr.ptr)
+    for v in range(0, h.m, 97):
+        row = tind[tptr[v]:tptr[v + 1]]
+        exp = sorted(tr.ind[tr.ptr[v]:tr.ptr[v + 1]], key=lambda u: (-deg[u], u))
+        np.testing.assert_array_equal(row, exp, err_msg=f"row {v}")
+    ap.bfs_set_params(ctx, mode=mode)
+    try:
+        for s in ap.seeded_sources(h, 6, seed=2):
+            ref, _ = oracle.bfs(h.m, h.ptr, h.ind, s)
+            np.testing.assert_array_equal(ap.bfs(ctx, g, s).cpu().numpy(), ref)
+    finally:
+        ap.bfs_set_params(ctx, mode=0)

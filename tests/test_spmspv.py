@@ -111,3 +111,39 @@ def test_spmspv_bfs_step_matches_bfs(ctx):
     s = int(np.argmax(h.degrees()))
     yi, _, _ = ap.spmspv(ctx, 3, g, torch.tensor([s], dtype=torch.int32, device="cuda"))
     np.testing.assert_array_equal(yi.cpu().numpy(), np.unique(h.ind[h.ptr[s]:h.ptr[s + 1]]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("semiring", [0, 1, 2, 3])
+def test_dense_spmv_all_rows(ctx, semiring):
+    """apspie_spmv against an FP64 / exact restatement: power-law rows with
+    a few hubs above the block threshold (4096) and empty rows."""
+    import torch
+    import apspie_b200 as ap
+    rng = np.random.default_rng(semiring)
+    m = 6000
+    lens = rng.integers(0, 20, m)
+    lens[::997] = 0
+    lens[[5, 1234, 4321]] = [5000, 9000, 4097]
+    ptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ind = rng.integers(0, m, int(ptr[-1])).astype(np.int32)
+    val = rng.uniform(-1, 1, int(ptr[-1])).astype(np.float32)
+    x = rng.uniform(-1, 1, m).astype(np.float32)
+    x[::5] = 0
+    t = lambda a: torch.from_numpy(a).cuda()
+    y = ap.spmv(ctx, m, t(ptr), t(ind), t(val), t(x), semiring).cpu().numpy()
+    for r in range(m):
+        a, xs = val[ptr[r]:ptr[r + 1]], x[ind[ptr[r]:ptr[r + 1]]]
+        if semiring == 0:
+            ref = float(np.sum(a.astype(np.float64) * xs.astype(np.float64)))
+            tol = 1e-6 * max(1.0, float(np.sum(np.abs(a.astype(np.float64) * xs))))
+            assert abs(y[r] - ref) <= tol, (r, y[r], ref)
+        elif semiring == 1:
+            ref = np.float32(np.min(a + xs)) if len(a) else np.finfo(np.float32).max
+            assert y[r] == ref, (r, y[r], ref)
+        elif semiring == 2:
+            ref = np.float32(np.max(a * xs)) if len(a) else -np.finfo(np.float32).max
+            assert y[r] == ref, (r, y[r], ref)
+        else:
+            ref = 1.0 if np.any((a != 0) & (xs != 0)) else 0.0
+            assert y[r] == ref, (r, y[r], ref)
