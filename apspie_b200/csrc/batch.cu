@@ -243,22 +243,37 @@ __device__ __forceinline__ void append_n(const BatchJob *j, const bool (&found)[
 }
 
 // ------------------------------------------------------------ MS-BFS ---
-// Push relaxation of edge (v -> u) carrying frontier mask f at level L:
-// claims the bits of f that u has not seen; returns true when u enters the
-// next frontier for the first time in this level.
-__device__ __forceinline__ bool msbfs_relax(BatchJob *j, unsigned long long f, int u, int next,
-                                            unsigned long long *Fn) {
-  unsigned long long nb = f & ~__ldcg(j->visited + u);
-  if (!nb) return false;
-  unsigned long long old = atomicOr(j->visited + u, nb);
-  unsigned long long mine = nb & ~old;
-  if (!mine) return false;
-  int32_t *row = j->out + (size_t)u * j->sw;
-  for (unsigned long long b = mine; b; b &= b - 1) row[__ffsll((long long)b) - 1] = next;
-  return atomicOr(Fn + u, mine) == 0ull;
+// Push relaxation of K edges per lane (v -> u[r]) carrying the tail's
+// frontier mask f[r] at level L: claims the bits of f that u has not seen
+// (found[r]: u enters the next frontier for the first time in this level).
+// The visited ORs of all K edges are issued together, then the frontier ORs.
+template <int K>
+__device__ __forceinline__ void msbfs_relax_n(BatchJob *j, const unsigned long long (&f)[K],
+                                              const int (&u)[K], int next,
+                                              unsigned long long *Fn, bool (&found)[K]) {
+  unsigned long long nb[K], old[K];
+#pragma unroll
+  for (int r = 0; r < K; ++r) nb[r] = u[r] >= 0 ? f[r] & ~__ldcg(j->visited + u[r]) : 0ull;
+#pragma unroll
+  for (int r = 0; r < K; ++r) old[r] = nb[r] ? atomicOr(j->visited + u[r], nb[r]) : ~0ull;
+  unsigned long long mine[K], fo[K];
+#pragma unroll
+  for (int r = 0; r < K; ++r) {
+    mine[r] = nb[r] & ~old[r];
+    if (mine[r]) {
+      int32_t *row = j->out + (size_t)u[r] * j->sw;
+      for (unsigned long long b = mine[r]; b; b &= b - 1) row[__ffsll((long long)b) - 1] = next;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < K; ++r) fo[r] = mine[r] ? atomicOr(Fn + u[r], mine[r]) : 1ull;
+#pragma unroll
+  for (int r = 0; r < K; ++r) found[r] = mine[r] != 0ull && fo[r] == 0ull;
 }
 
-// 32 queued frontier vertices, edges dealt flat over the warp
+constexpr int kMsbfsUnroll = 4;  // edges per lane per batch
+
+// 32 queued frontier vertices, edges dealt flat over the warp, 4 x 32 a batch
 __device__ void msbfs_push_queue(BatchJob *j, int L, int unit, unsigned nq) {
   const int lane = lane_id();
   int *qin = jobQ(j, L % 3), *qout = jobQ(j, (L + 1) % 3);
@@ -277,23 +292,28 @@ __device__ void msbfs_push_queue(BatchJob *j, int L, int unit, unsigned nq) {
   int incl = warp_incl_scan(d);
   int excl = incl - d;
   int total = __shfl_sync(kFull, incl, 31);
-  for (int e0 = 0; e0 < total; e0 += 32) {
-    int e = e0 + lane;
-    int owner = warp_owner(excl, e);
-    int so = __shfl_sync(kFull, s, owner);
-    int eo = __shfl_sync(kFull, excl, owner);
-    unsigned long long fo = __shfl_sync(kFull, f, owner);
-    bool found[1] = {false};
-    int u[1] = {-1}, dg[1] = {0};
-    if (e < total) {
-      u[0] = __ldg(j->ind + so + (e - eo));
-      found[0] = msbfs_relax(j, fo, u[0], L + 1, Fn);
-      if (found[0]) dg[0] = __ldg(j->ptr + u[0] + 1) - __ldg(j->ptr + u[0]);
+  for (int e0 = 0; e0 < total; e0 += 32 * kMsbfsUnroll) {
+    unsigned long long fo[kMsbfsUnroll];
+    int u[kMsbfsUnroll], dg[kMsbfsUnroll];
+    bool found[kMsbfsUnroll];
+#pragma unroll
+    for (int r = 0; r < kMsbfsUnroll; ++r) {
+      const int e = e0 + r * 32 + lane;
+      const int owner = warp_owner(excl, min(e, total - 1));
+      const int so = __shfl_sync(kFull, s, owner);
+      const int eo = __shfl_sync(kFull, excl, owner);
+      fo[r] = __shfl_sync(kFull, f, owner);
+      u[r] = e < total ? __ldg(j->ind + so + (e - eo)) : -1;
     }
-    append_n<1>(j, found, u, dg, qout, cout, nxt);
+    msbfs_relax_n<kMsbfsUnroll>(j, fo, u, L + 1, Fn, found);
+#pragma unroll
+    for (int r = 0; r < kMsbfsUnroll; ++r)
+      dg[r] = found[r] ? __ldg(j->ptr + u[r] + 1) - __ldg(j->ptr + u[r]) : 0;
+    append_n<kMsbfsUnroll>(j, found, u, dg, qout, cout, nxt);
   }
 }
 
+// one kChunk-edge chunk of a hub, 4 x 32 edges a batch
 __device__ void msbfs_push_chunk(BatchJob *j, int L, int unit) {
   const int lane = lane_id();
   int2 *cin = jobC(j, L % 3), *cout = jobC(j, (L + 1) % 3);
@@ -304,16 +324,21 @@ __device__ void msbfs_push_chunk(BatchJob *j, int L, int unit) {
   int s = __ldg(j->ptr + ch.x) + ch.y * kChunk;
   int e = min(s + kChunk, __ldg(j->ptr + ch.x + 1));
   unsigned long long f = __ldcg(Fc + ch.x);
-  for (int k0 = s; k0 < e; k0 += 32) {
-    int k = k0 + lane;
-    bool found[1] = {false};
-    int u[1] = {-1}, dg[1] = {0};
-    if (k < e) {
-      u[0] = __ldg(j->ind + k);
-      found[0] = msbfs_relax(j, f, u[0], L + 1, Fn);
-      if (found[0]) dg[0] = __ldg(j->ptr + u[0] + 1) - __ldg(j->ptr + u[0]);
+  for (int k0 = s; k0 < e; k0 += 32 * kMsbfsUnroll) {
+    unsigned long long fo[kMsbfsUnroll];
+    int u[kMsbfsUnroll], dg[kMsbfsUnroll];
+    bool found[kMsbfsUnroll];
+#pragma unroll
+    for (int r = 0; r < kMsbfsUnroll; ++r) {
+      const int k = k0 + r * 32 + lane;
+      fo[r] = f;
+      u[r] = k < e ? __ldg(j->ind + k) : -1;
     }
-    append_n<1>(j, found, u, dg, qout, cout, nxt);
+    msbfs_relax_n<kMsbfsUnroll>(j, fo, u, L + 1, Fn, found);
+#pragma unroll
+    for (int r = 0; r < kMsbfsUnroll; ++r)
+      dg[r] = found[r] ? __ldg(j->ptr + u[r] + 1) - __ldg(j->ptr + u[r]) : 0;
+    append_n<kMsbfsUnroll>(j, found, u, dg, qout, cout, nxt);
   }
 }
 
@@ -435,11 +460,16 @@ __device__ __forceinline__ bool mssp_relax(BatchJob *j, int ue, unsigned we, int
     nd[i] = act[i] ? sat_add(__ldcg(dist + (size_t)vi * sw + src), wi) : 0u;
     cur[i] = act[i] ? __ldcg(dist + (size_t)uu[i] * sw + src) : 0u;
   }
+  // all the slots' minima first (independent atomics), then the ballots
+  unsigned old[kSsspSlots];
+#pragma unroll
+  for (int i = 0; i < kSsspSlots; ++i)
+    old[i] = (act[i] && nd[i] < cur[i]) ? atomicMin(dist + (size_t)uu[i] * sw + src, nd[i])
+                                         : 0u;
   unsigned mybal = 0;
 #pragma unroll
   for (int i = 0; i < kSsspSlots; ++i) {
-    const bool imp = act[i] && nd[i] < cur[i] &&
-                     nd[i] < atomicMin(dist + (size_t)uu[i] * sw + src, nd[i]);
+    const bool imp = act[i] && nd[i] < cur[i] && nd[i] < old[i];
     const unsigned b = __ballot_sync(kFull, imp);
     // loading lane i * per + g takes the bits of its edge's group g
     const int g = lane - i * per;

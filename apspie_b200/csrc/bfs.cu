@@ -32,7 +32,7 @@ namespace apspie {
 namespace {
 
 constexpr int kBfsThreads = 512;
-constexpr int kProbe = 4;         // in-neighbours a lane probes per round in a pull level
+constexpr int kProbe = 1;         // in-neighbours a lane probes per round in a pull level
 constexpr int kScanUnroll = 4;    // depth words a warp loads at once when re-queuing a frontier
 constexpr int kTraceLevels = 64;  // levels recorded in the per-run trace
 
@@ -73,8 +73,15 @@ struct BfsVisit {
   __device__ __forceinline__ bool check(unsigned, int, int u, unsigned &) const {
     return __ldcg(depth + u) == -1;
   }
-  __device__ __forceinline__ bool commit(unsigned, int, int u, unsigned) const {
-    return atomicCAS(depth + u, -1, next) == -1;
+  template <int N>
+  __device__ __forceinline__ void commit_n(const unsigned (&)[N], const int (&)[N],
+                                           const int (&u)[N], const unsigned (&)[N],
+                                           const bool (&ok)[N], int (&cls)[N]) const {
+    int old[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) old[r] = ok[r] ? atomicCAS(depth + u[r], -1, next) : 0;
+#pragma unroll
+    for (int r = 0; r < N; ++r) cls[r] = (ok[r] && old[r] == -1) ? 1 : 0;
   }
 };
 

@@ -19,7 +19,11 @@
 // visitor checks (the random loads), then the atomic commits, so each lane
 // keeps several independent loads in flight.  A visitor provides
 //   check(payload, k, u, &aux) -> bool   (plain loads only)
-//   commit(payload, k, u, aux) -> bool   (atomics; true = u joins the next frontier)
+//   commit_n<N>(payload[], k[], u[], aux[], ok[], cls[])   (the atomics of
+//     the N candidates for which ok[r], issued together -- each class of
+//     atomic for all N before the next class -- so a batch waits for one or
+//     two atomic round trips, not N dependent ones; cls[r] = 1 when u joins
+//     the next frontier)
 // discover_n() appends joiners (warp-aggregated) to the next queue or the
 // next big list: one atomic per warp for the queue slots, one for the big
 // list, whose length and chunk total share a 64-bit word so that list order
@@ -237,10 +241,16 @@ __device__ __forceinline__ void expand_chunks(const int *__restrict__ ptr,
         for (int r = 0; r < kUnroll; ++r)
           ok[r] = uu[r] >= 0 && visit.check(pay, k0 + r * 32 + lane, uu[r], aux[r]);
         bool f[kUnroll], g[kUnroll];
-        int cls[kUnroll];
+        int cls[kUnroll], kk[kUnroll];
+        unsigned pp[kUnroll];
 #pragma unroll
         for (int r = 0; r < kUnroll; ++r) {
-          cls[r] = ok[r] ? (int)visit.commit(pay, k0 + r * 32 + lane, uu[r], aux[r]) : 0;
+          kk[r] = k0 + r * 32 + lane;
+          pp[r] = pay;
+        }
+        visit.template commit_n<kUnroll>(pp, kk, uu, aux, ok, cls);
+#pragma unroll
+        for (int r = 0; r < kUnroll; ++r) {
           f[r] = cls[r] == 1;
           g[r] = cls[r] == 2;
         }
@@ -323,9 +333,9 @@ __device__ __forceinline__ void expand_push(const int *__restrict__ ptr,
         ok[r] = uu[r] >= 0 && visit.check(pp[r], kk[r], uu[r], aux[r]);
       bool f[kUnroll], g[kUnroll];
       int cls[kUnroll];
+      visit.template commit_n<kUnroll>(pp, kk, uu, aux, ok, cls);
 #pragma unroll
       for (int r = 0; r < kUnroll; ++r) {
-        cls[r] = ok[r] ? (int)visit.commit(pp[r], kk[r], uu[r], aux[r]) : 0;
         f[r] = cls[r] == 1;
         g[r] = cls[r] == 2;
       }

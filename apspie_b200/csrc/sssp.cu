@@ -115,10 +115,29 @@ struct SsspVisit {
     nd = Arith<W>::add(du, __ldg(w + k));
     return nd < __ldcg(dist + u);
   }
-  __device__ __forceinline__ int commit(unsigned, int, int u, unsigned nd) const {
-    if (nd >= atomicMin(dist + u, nd)) return 0;
-    if (nd < thresh) return atomicExch(stamp + u, round) != round ? 1 : 0;
-    return atomicExch(fstamp + u, phase) != phase ? 2 : 3;  // 3: far, already listed
+  template <int N>
+  __device__ __forceinline__ void commit_n(const unsigned (&)[N], const int (&)[N],
+                                           const int (&u)[N], const unsigned (&nd)[N],
+                                           const bool (&ok)[N], int (&cls)[N]) const {
+    // all distance minima first, then the stamps of the improved targets
+    unsigned old[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) old[r] = ok[r] ? atomicMin(dist + u[r], nd[r]) : 0u;
+    int prev[N];
+    bool imp[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      imp[r] = ok[r] && nd[r] < old[r];
+      prev[r] = 0;
+      if (imp[r])
+        prev[r] = nd[r] < thresh ? atomicExch(stamp + u[r], round) : atomicExch(fstamp + u[r], phase);
+    }
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      cls[r] = 0;
+      if (imp[r]) cls[r] = nd[r] < thresh ? (prev[r] != round ? 1 : 0)
+                                          : (prev[r] != phase ? 2 : 3);  // 3: far, already listed
+    }
   }
   // least distance sent far by this warp's batch (classes 2 and 3), one atomic
   template <int N>
@@ -161,7 +180,7 @@ __global__ void sssp_init(int m, int src, unsigned *dist, int *stamp, int *fstam
 }
 
 template <typename W>
-__global__ void __launch_bounds__(kSsspThreads, 3)
+__global__ void __launch_bounds__(kSsspThreads, 2)
 sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
                 const W *__restrict__ w, unsigned *dist, int *stamp, int *qa, int *qb, int2 *ca,
                 int2 *cb, SsspState *st, int max_rounds, int *fstamp, unsigned *xd, int *far0,

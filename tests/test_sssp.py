@@ -109,3 +109,63 @@ def test_sssp_rmat20_full_size(ctx):
     s = ap.seeded_sources(h, 1, seed=0)[0]
     rel = _check_against_oracle(ctx, h, g, s)
     assert rel <= F32_REL_TOL
+
+
+@pytest.mark.parametrize("delta_u32,delta_f32", [(16, 0.05), (256, 0.5), (1 << 31, 1e30)])
+def test_sssp_near_far_same_fixpoint(ctx, delta_u32, delta_f32):
+    """Near-far schedules give exactly the delta-0 distances (u32 against the
+    oracle's Dijkstra, f32 against the reference's float SSSP), on a directed
+    R-MAT and on a grid, whose many phases exercise the far lists."""
+    import apspie_b200 as ap
+    cases = [ap.gen_rmat(13, 16, seed=31, symmetric=False), ap.gen_grid(40, 60)]
+    try:
+        for h in cases:
+            ap.weights_u32(h, seed=4)
+            ap.weights_f32(h, seed=4)
+            g = h.to_device()
+            ap.sssp_set_params(ctx, delta_u32, delta_f32)
+            for s in ap.seeded_sources(h, 3, seed=5):
+                du = ap.sssp(ctx, g, s, weights="u32").cpu().numpy().view(np.uint32)
+                np.testing.assert_array_equal(du, oracle.sssp_u32(h.m, h.ptr, h.ind, h.w_u32, s))
+                st = ap.sssp_stats(ctx)
+                if delta_u32 < 1 << 20 and h.m == 2400:
+                    assert st["phases"] > 0
+                df = ap.sssp(ctx, g, s, weights="f32").cpu().numpy()
+                ref = oracle.sssp_f32(h.m, h.ptr, h.ind, h.w_f32, s)
+                assert np.array_equal(np.isinf(df), ref == -1)
+                fin = ~np.isinf(df)
+                np.testing.assert_array_equal(df[fin].view(np.uint32), ref[fin].view(np.uint32))
+    finally:
+        ap.sssp_set_params(ctx, 0, 0.0)
+
+
+def test_sssp_trace_accounts_for_every_round(ctx):
+    import apspie_b200 as ap
+    h = ap.gen_rmat(14, 16, seed=32, symmetric=False)
+    ap.weights_u32(h, seed=6)
+    g = h.to_device()
+    ap.sssp(ctx, g, ap.seeded_sources(h, 1, seed=7)[0], weights="u32")
+    st, tr = ap.sssp_stats(ctx), ap.sssp_trace(ctx)
+    assert len(tr) == st["rounds"]
+    assert sum(t["frontier_edges"] for t in tr) == st["relaxations"]
+    assert tr[0]["frontier"] == 1 and all(t["us"] > 0 for t in tr)
+
+
+def test_persistent_kernels_with_a_capped_grid(ctx):
+    """A context whose persistent launches are capped to a few blocks (the
+    server's small-grid lane) gives the same BFS depths and SSSP distances."""
+    import apspie_b200 as ap
+    from apspie_b200._native import lib
+    h = ap.gen_rmat(13, 16, seed=33)
+    ap.weights_u32(h, seed=8)
+    g = h.to_device()
+    srcs = ap.seeded_sources(h, 3, seed=9)
+    full = [(ap.bfs(ctx, g, s).cpu().numpy(), ap.sssp(ctx, g, s, weights="u32").cpu().numpy())
+            for s in srcs]
+    assert lib.apspie_ctx_set_max_grid(ctx.handle, 4) == 0
+    try:
+        for s, (d0, w0) in zip(srcs, full):
+            np.testing.assert_array_equal(ap.bfs(ctx, g, s).cpu().numpy(), d0)
+            np.testing.assert_array_equal(ap.sssp(ctx, g, s, weights="u32").cpu().numpy(), w0)
+    finally:
+        lib.apspie_ctx_set_max_grid(ctx.handle, 0)

@@ -79,3 +79,36 @@ def test_noalloc_rejects_sizes_beyond_the_limit():
                                 _p(ptr), None, None, _p(out), 0)
     assert rc == APSPIE_ERR_TOO_LARGE
     assert lib.apspie_status_string(rc) == b"input exceeds the fixed scratch size"
+
+
+def test_noalloc_bfs_inside_a_cuda_graph():
+    """A caller captures apspie_bfs_noalloc (its init kernel and the
+    cooperative persistent kernel) into a CUDA graph and replays it: the
+    replay writes the same depths as a direct call."""
+    import torch
+
+    import apspie_b200 as ap
+    import oracle
+    from apspie_b200._native import lib
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    h = ap.gen_rmat(14, 16, seed=3)
+    g = h.to_device()
+    src = ap.seeded_sources(h, 1, seed=1)[0]
+    depth = torch.empty(h.m, dtype=torch.int32, device="cuda")
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        assert _noalloc(lib, side, g, src, depth, g.ptr, g.ind) == 0   # first call: outside capture
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=side):
+        assert _noalloc(lib, side, g, src, depth, g.ptr, g.ind) == 0
+    depth.fill_(7)
+    torch.cuda.synchronize()
+    for _ in range(2):
+        graph.replay()
+        torch.cuda.synchronize()
+        ref, _ = oracle.bfs(h.m, h.ptr, h.ind, src)
+        np.testing.assert_array_equal(depth.cpu().numpy(), ref)
+        depth.fill_(7)
