@@ -718,6 +718,49 @@ int batch_grid(apspie_context *ctx) {
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Jobs whose graphs take more levels than this run in their own launch with
+// a small grid next to the others (a grid graph's ~2,000 levels of a few
+// thousand vertices each would otherwise set the step count of the whole
+// batch while the rest of the GPU idles).
+constexpr int kDeepLevels = 64;
+
+// BFS levels of graph J from its first vertex with edges, cached in the
+// context by the graph's fingerprint (one probe BFS per new graph).
+int graph_levels(apspie_context *ctx, const apspie_job &J, int *levels) {
+  *levels = 0;
+  if (J.nnz == 0) return APSPIE_OK;
+  const uint64_t fp = graph_fingerprint(ctx, J.m, J.nnz, J.d_ptr);
+  for (const auto &e : ctx->depth_cache)
+    if (e.fp == fp) {
+      *levels = e.levels;
+      return APSPIE_OK;
+    }
+  const int nh = std::min(J.m, 4096);
+  int *h = (int *)pinned(ctx, sizeof(int) * (nh + 1));
+  if (!h) return APSPIE_ERR_OOM;
+  cudaMemcpyAsync(h, J.d_ptr, sizeof(int) * (nh + 1), cudaMemcpyDeviceToHost, ctx->stream);
+  int rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "graph_levels");
+  if (rc) return rc;
+  int src = -1;
+  for (int u = 0; u < nh && src < 0; ++u)
+    if (h[u + 1] > h[u]) src = u;
+  int lv = 0;
+  if (src >= 0) {
+    auto *depth = (int32_t *)workspace(ctx, kSlotDense, sizeof(int32_t) * (size_t)J.m);
+    if (!depth) return APSPIE_ERR_OOM;
+    const int *tp = J.d_tptr ? J.d_tptr : (J.symmetric ? J.d_ptr : nullptr);
+    const int *ti = J.d_tptr ? J.d_tind : (J.symmetric ? J.d_ind : nullptr);
+    rc = apspie_bfs(ctx, src, J.nnz, J.m, J.d_ptr, J.d_ind, tp, ti, depth, 0);
+    apspie_bfs_stats bs;
+    if (!rc) rc = apspie_bfs_get_stats(ctx, &bs);
+    if (rc) return rc;
+    lv = bs.levels;
+  }
+  ctx->depth_cache.push_back(apspie_context::DepthEntry{fp, lv});
+  *levels = lv;
+  return APSPIE_OK;
+}
+
 // Distance-row width of an SSSP job: the sources rounded up to a power of two.
 int row_width(int nsrc) {
   int w = 1;
@@ -765,9 +808,25 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
   if (nparts > kMaxJobs)
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: %d device jobs > %d", nparts,
                      kMaxJobs);
+  // deep-graph jobs go last and, when others are present, into a launch of
+  // their own on the context's second stream
+  std::vector<char> deep_job(njobs, 0);
+  for (int i = 0; i < njobs && njobs > 1; ++i) {
+    int lv = 0;
+    int rc0 = graph_levels(ctx, jobs[i], &lv);
+    if (rc0) return rc0;
+    deep_job[i] = lv > kDeepLevels;
+  }
+  std::stable_partition(parts.begin(), parts.end(),
+                        [&](const Part &p) { return !deep_job[p.job]; });
+  int nshallow = 0;
+  for (const Part &p : parts) nshallow += deep_job[p.job] ? 0 : 1;
+  const int full = clamp_grid(ctx, batch_grid(ctx));
+  if (full <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_batch_run: occupancy query failed");
+  const bool split = nshallow > 0 && nshallow < nparts && full > 1 && ctx->deep_blocks < full;
   // workspace layout per device job
   std::vector<size_t> off(nparts + 1, 0);
-  size_t total = align_up(sizeof(BatchJob) * kMaxJobs) + align_up(sizeof(BatchState)) +
+  size_t total = align_up(sizeof(BatchJob) * kMaxJobs) + 2 * align_up(sizeof(BatchState)) +
                  align_up(sizeof(int) * 64 * kMaxJobs);
   const size_t head = total;
   for (int p = 0; p < nparts; ++p) {
@@ -786,7 +845,9 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
   if (!ws) return APSPIE_ERR_OOM;
   auto *djobs = (BatchJob *)ws;
   auto *dstate = (BatchState *)(ws + align_up(sizeof(BatchJob) * kMaxJobs));
-  int *dsrc = (int *)(ws + align_up(sizeof(BatchJob) * kMaxJobs) + align_up(sizeof(BatchState)));
+  auto *dstate2 = (BatchState *)(ws + align_up(sizeof(BatchJob) * kMaxJobs) +
+                                 align_up(sizeof(BatchState)));
+  int *dsrc = (int *)(ws + align_up(sizeof(BatchJob) * kMaxJobs) + 2 * align_up(sizeof(BatchState)));
   (void)head;
   // host image of the job table (pinned, copied in one transfer); earlier
   // copies out of the pinned buffer must have completed before it is reused
@@ -839,39 +900,72 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
   cudaStream_t st = ctx->stream;
   cudaMemcpyAsync(djobs, hjobs, host_bytes, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(dsrc, hsrc, sizeof(int) * 64 * nparts, cudaMemcpyHostToDevice, st);
-  cudaMemsetAsync(dstate, 0, sizeof(BatchState), st);
+  cudaMemsetAsync(dstate, 0, 2 * align_up(sizeof(BatchState)), st);
   int rc = check_cuda(ctx, cudaGetLastError(), "apspie_batch_run upload");
   if (rc) return rc;
+  // the deep jobs' stream starts after the uploads
+  cudaStream_t st2 = st;
+  if (split) {
+    if (!ctx->aux_stream &&
+        (cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking) != cudaSuccess ||
+         cudaEventCreateWithFlags(&ctx->aux_done, cudaEventDisableTiming) != cudaSuccess))
+      return check_cuda(ctx, cudaGetLastError(), "apspie_batch_run: second stream");
+    st2 = ctx->aux_stream;
+    cudaEventRecord(ctx->aux_done, st);
+    cudaStreamWaitEvent(st2, ctx->aux_done, 0);
+  }
   for (int p = 0; p < nparts; ++p) {
     const long long m = jobs[parts[p].job].m;
+    cudaStream_t sp = p < nshallow ? st : st2;
     int g = (int)std::max(1ll, std::min((m * hjobs[p].sw + 255) / 256, (long long)ctx->num_sms * 8));
     if (hjobs[p].type == kJobBfs) {
-      batch_init_bfs<<<g, 256, 0, st>>>(djobs, p);
-      batch_seed_bfs<<<1, 64, 0, st>>>(djobs, p);
+      batch_init_bfs<<<g, 256, 0, sp>>>(djobs, p);
+      batch_seed_bfs<<<1, 64, 0, sp>>>(djobs, p);
     } else {
-      batch_init_sssp<<<g, 256, 0, st>>>(djobs, p);
-      batch_seed_sssp<<<1, 32, 0, st>>>(djobs, p);
+      batch_init_sssp<<<g, 256, 0, sp>>>(djobs, p);
+      batch_seed_sssp<<<1, 32, 0, sp>>>(djobs, p);
     }
   }
   rc = check_launch(ctx, "batch init", 2 * nparts);
   if (rc) return rc;
-  int grid = clamp_grid(ctx, batch_grid(ctx));
-  if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_batch_run: occupancy query failed");
-  int np = nparts;
-  void *args[] = {&djobs, &np, &dstate, &max_steps};
-  cudaError_t e = cudaLaunchCooperativeKernel((const void *)batch_persistent, dim3(grid),
-                                              dim3(kBatchThreads), args, 0, st);
+  // one launch for everything, or the shallow jobs here and the deep ones on
+  // the second stream with deep_grid blocks, the two grids sharing the GPU
+  // deep jobs are latency bound per level but carry many levels: by default
+  // they get two thirds of the GPU (measured best on the batched benchmark)
+  const int deep_grid = std::max(1, std::min(full - 1, ctx->deep_blocks > 0 ? ctx->deep_blocks
+                                                                             : 2 * full / 3));
+  const int grid1 = split ? std::max(1, full - deep_grid) : full;
+  int n1 = split ? nshallow : nparts;
+  BatchJob *dj1 = djobs;
+  void *args1[] = {&dj1, &n1, &dstate, &max_steps};
+  cudaError_t e = cudaLaunchCooperativeKernel((const void *)batch_persistent, dim3(grid1),
+                                              dim3(kBatchThreads), args1, 0, st);
   if (e != cudaSuccess) return check_cuda(ctx, e, "batch_persistent");
   ctx->launches += 1;
+  if (split) {
+    int n2 = nparts - nshallow;
+    BatchJob *dj2 = djobs + nshallow;
+    void *args2[] = {&dj2, &n2, &dstate2, &max_steps};
+    e = cudaLaunchCooperativeKernel((const void *)batch_persistent, dim3(deep_grid),
+                                    dim3(kBatchThreads), args2, 0, st2);
+    if (e != cudaSuccess) return check_cuda(ctx, e, "batch_persistent (deep jobs)");
+    ctx->launches += 1;
+  }
   for (int p = 0; p < nparts; ++p) {
     const apspie_job &J = jobs[parts[p].job];
     const int width = hjobs[p].sw;
-    batch_transpose<<<(J.m + 31) / 32, 256, 0, st>>>(hjobs[p].out, J.m, width, parts[p].n,
-                                                     J.d_out + (size_t)parts[p].first * J.m);
+    batch_transpose<<<(J.m + 31) / 32, 256, 0, p < nshallow ? st : st2>>>(
+        hjobs[p].out, J.m, width, parts[p].n, J.d_out + (size_t)parts[p].first * J.m);
   }
   rc = check_launch(ctx, "batch_transpose", nparts);
   if (rc) return rc;
+  if (split) {
+    // the call completes on the context's stream
+    cudaEventRecord(ctx->aux_done, st2);
+    cudaStreamWaitEvent(st, ctx->aux_done, 0);
+  }
   ctx->batch_state = dstate;
+  ctx->batch_state2 = split ? dstate2 : nullptr;
   return APSPIE_OK;
 }
 
@@ -879,14 +973,23 @@ int apspie_batch_get_stats(apspie_ctx ctx, apspie_batch_stats *out) {
   APSPIE_CHECK_CTX(ctx);
   if (!out || !ctx->batch_state)
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_get_stats: no batch has run");
-  auto *h = (BatchState *)pinned(ctx, sizeof(BatchState));
+  auto *h = (BatchState *)pinned(ctx, 2 * sizeof(BatchState));
   if (!h) return APSPIE_ERR_OOM;
   cudaMemcpyAsync(h, ctx->batch_state, sizeof(BatchState), cudaMemcpyDeviceToHost, ctx->stream);
+  if (ctx->batch_state2)
+    cudaMemcpyAsync(h + 1, ctx->batch_state2, sizeof(BatchState), cudaMemcpyDeviceToHost,
+                    ctx->stream);
   int rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "apspie_batch_get_stats");
   if (rc) return rc;
-  out->super_steps = h->steps;
-  out->frontier_edges = (int64_t)h->edges;
-  if (h->err) return set_error(ctx, APSPIE_ERR_TIMEOUT, "apspie_batch_run: grid barrier timed out");
+  out->super_steps = h[0].steps;
+  out->frontier_edges = (int64_t)h[0].edges;
+  int err = h[0].err;
+  if (ctx->batch_state2) {
+    out->super_steps = std::max(out->super_steps, h[1].steps);
+    out->frontier_edges += (int64_t)h[1].edges;
+    err |= h[1].err;
+  }
+  if (err) return set_error(ctx, APSPIE_ERR_TIMEOUT, "apspie_batch_run: grid barrier timed out");
   return APSPIE_OK;
 }
 

@@ -79,6 +79,24 @@ void *pinned(apspie_context *ctx, size_t bytes) {
 
 using namespace apspie;
 
+namespace apspie {
+
+uint64_t graph_fingerprint(apspie_context *ctx, int m, int64_t nnz, const int *d_ptr) {
+  // offsets sampled at 64 evenly spaced rows (plus the last)
+  int *h = (int *)pinned(ctx, sizeof(int) * 65);
+  uint64_t f = 1469598103934665603ull ^ ((uint64_t)m << 32) ^ (uint64_t)nnz;
+  if (!h) return f;
+  for (int i = 0; i <= 64; ++i) {
+    size_t row = (size_t)((int64_t)m * i / 64);
+    cudaMemcpyAsync(h + i, d_ptr + row, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  }
+  cudaStreamSynchronize(ctx->stream);
+  for (int i = 0; i <= 64; ++i) f = (f ^ (uint64_t)(uint32_t)h[i]) * 1099511628211ull;
+  return f;
+}
+
+}  // namespace apspie
+
 extern "C" {
 
 int apspie_ctx_create(int device, void *stream, apspie_ctx *out) {
@@ -107,6 +125,11 @@ int apspie_ctx_destroy(apspie_ctx ctx) {
   if (!ctx) return APSPIE_ERR_INVALID;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->aux_stream) {
+    cudaStreamSynchronize(ctx->aux_stream);
+    cudaStreamDestroy(ctx->aux_stream);
+  }
+  if (ctx->aux_done) cudaEventDestroy(ctx->aux_done);
   for (auto &s : ctx->slots)
     if (s.ptr) cudaFree(s.ptr);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -117,6 +140,12 @@ int apspie_ctx_destroy(apspie_ctx ctx) {
 int apspie_ctx_set_max_grid(apspie_ctx ctx, int blocks) {
   if (!ctx || blocks < 0) return APSPIE_ERR_INVALID;
   ctx->max_grid = blocks;
+  return APSPIE_OK;
+}
+
+int apspie_batch_set_params(apspie_ctx ctx, int deep_blocks) {
+  if (!ctx || deep_blocks < 0) return APSPIE_ERR_INVALID;
+  ctx->deep_blocks = deep_blocks;
   return APSPIE_OK;
 }
 

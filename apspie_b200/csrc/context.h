@@ -46,6 +46,18 @@ struct apspie_context {
   void *batch_state = nullptr;
   // SpMSpV: the bitmap path is taken when E * factor > m
   double spmspv_sort_factor = 4.0;
+  // batched launches: a second stream (and its completion event) for the
+  // jobs of deep graphs, which run next to the others with a small grid;
+  // traversal depth of graphs seen before, by fingerprint
+  cudaStream_t aux_stream = nullptr;
+  int deep_blocks = 0;  // blocks of the deep jobs' launch (0: two thirds of the resident ones)
+  cudaEvent_t aux_done = nullptr;
+  void *batch_state2 = nullptr;
+  struct DepthEntry {
+    uint64_t fp;
+    int levels;
+  };
+  std::vector<DepthEntry> depth_cache;
   // autotuner results by graph fingerprint
   struct TuneEntry {
     uint64_t fp;
@@ -116,6 +128,10 @@ int check_cuda(apspie_context *ctx, cudaError_t e, const char *what);
   } while (0)
 
 namespace apspie {
+// Fingerprint of a graph: m, nnz and its row offsets at 64 evenly spaced rows
+// (synchronises the context's stream).
+uint64_t graph_fingerprint(apspie_context *ctx, int m, int64_t nnz, const int *d_ptr);
+
 // Grid of a persistent launch: the occupancy-sized grid, capped by the
 // context's max_grid.
 inline int clamp_grid(const apspie_context *ctx, int grid) {

@@ -138,6 +138,28 @@ __global__ void key_rows(const unsigned long long *k, long long n, int dbits, in
   }
 }
 
+// key of edge k = (row u -> col ind[k]) for the transpose: (col, row); value k
+__global__ void transpose_keys(int m, const int *ptr, const int *ind, int rbits,
+                               unsigned long long *keys, int *vals) {
+  const int lane = threadIdx.x & 31;
+  for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < m;
+       u += (gridDim.x * blockDim.x) >> 5)
+    for (int k = ptr[u] + lane; k < ptr[u + 1]; k += 32) {
+      keys[k] = ((unsigned long long)ind[k] << rbits) | (unsigned)u;
+      vals[k] = k;
+    }
+}
+
+__global__ void transpose_emit(long long n, int rbits, const unsigned long long *keys,
+                               const int *vals, const float *val, int *tind, float *tval) {
+  const unsigned long long mask = (1ull << rbits) - 1ull;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    tind[i] = (int)(keys[i] & mask);
+    if (tval) tval[i] = val ? val[vals[i]] : 1.0f;
+  }
+}
+
 __global__ void copy_int(long long n, const int *in, int *out) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -275,6 +297,40 @@ int apspie_bfs_prepare(apspie_ctx ctx, int m, int64_t nnz, const int *d_ptr, con
   rc = check_launch(ctx, "key_rows", 2);
   if (rc) return rc;
   return device_exclusive_scan<int>(ctx, d_tptr, d_tptr, (long long)m + 1, nullptr);
+}
+
+int apspie_csr_transpose(apspie_ctx ctx, int m, int n, int64_t nnz, const int *d_ptr,
+                         const int *d_ind, const float *d_val, int *d_tptr, int *d_tind,
+                         float *d_tval) {
+  APSPIE_CHECK_CTX(ctx);
+  if (m <= 0 || n <= 0 || nnz < 0 || nnz >= (int64_t)INT32_MAX || !d_ptr || !d_tptr ||
+      (nnz > 0 && (!d_ind || !d_tind)))
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_csr_transpose: bad arguments");
+  cudaStream_t st = ctx->stream;
+  fill_int<<<gg(ctx, (long long)n + 1), 256, 0, st>>>(n + 1, 0, d_tptr);
+  int rc = check_launch(ctx, "fill_int");
+  if (rc || nnz == 0) return rc;
+  const int rbits = std::max(1, bits_for(m)), cbits = std::max(1, bits_for(n));
+  auto *ka = (unsigned long long *)workspace(ctx, kSlotSortKeysA, 8 * (size_t)nnz);
+  auto *kb = (unsigned long long *)workspace(ctx, kSlotSortKeysB, 8 * (size_t)nnz);
+  auto *va = (int *)workspace(ctx, kSlotSortValsA, 4 * (size_t)nnz);
+  auto *vb = (int *)workspace(ctx, kSlotSortValsB, 4 * (size_t)nnz);
+  if (!ka || !kb || !va || !vb) return APSPIE_ERR_OOM;
+  transpose_keys<<<gg(ctx, (long long)m * 32), 256, 0, st>>>(m, d_ptr, d_ind, rbits, ka, va);
+  rc = check_launch(ctx, "transpose_keys");
+  if (rc) return rc;
+  // rows within a column come out ascending: the keys hold them, and the
+  // sort only needs the column bits above them (stable LSD on all bits)
+  bool in_b = false;
+  rc = device_radix_sort<unsigned long long, int>(ctx, ka, va, kb, vb, nnz, rbits + cbits, &in_b);
+  if (rc) return rc;
+  const unsigned long long *k = in_b ? kb : ka;
+  const int *v = in_b ? vb : va;
+  key_rows<<<gg(ctx, nnz), 256, 0, st>>>(k, nnz, rbits, d_tptr);
+  transpose_emit<<<gg(ctx, nnz), 256, 0, st>>>(nnz, rbits, k, v, d_val, d_tind, d_tval);
+  rc = check_launch(ctx, "transpose_emit", 2);
+  if (rc) return rc;
+  return device_exclusive_scan<int>(ctx, d_tptr, d_tptr, (long long)n + 1, nullptr);
 }
 
 int apspie_gen_weights_u32_device(apspie_ctx ctx, int m, const int *d_ptr, const int *d_ind,

@@ -16,9 +16,10 @@
 //     its own completion event, so a quick query is not held back by a slow
 //     one of the same batch;
 //   * lanes: graphs whose traversals take many levels (found when the graph
-//     is added, by one probe BFS) run on a second stream with a small grid,
-//     next to the main lane, so their thousands of short levels do not keep
-//     the whole GPU from the other queries;
+//     is added, by one probe BFS) run on a second stream with half of the
+//     GPU's persistent blocks, next to the main lane with the other half, so
+//     their thousands of short levels do not keep the whole GPU from the
+//     other queries;
 //   * continuous batching: there are two batch slots.  While one slot's
 //     groups run, queries that arrive are admitted into the other slot and
 //     launched right away, queued on the GPU behind (and overlapping the
@@ -74,7 +75,6 @@ struct Request {
 // A graph traversal is "deep" when a probe BFS takes more levels than this:
 // its queries go to the small-grid lane.
 constexpr int kDeepLevels = 64;
-constexpr int kDeepBlocks = 32;  // blocks of the deep lane's persistent launches
 
 struct GraphEntry {
   int m;
@@ -373,7 +373,7 @@ void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
     // with deep graphs around, the main lane leaves room for the deep lane
     int resident = 0;
     apspie_ctx_resident_blocks(sl.lane[0].ctx, &resident);
-    apspie_ctx_set_max_grid(sl.lane[0].ctx, s->any_deep ? std::max(1, resident - kDeepBlocks) : 0);
+    apspie_ctx_set_max_grid(sl.lane[0].ctx, s->any_deep ? std::max(1, resident - resident / 2) : 0);
   }
   std::map<std::pair<int, int>, size_t> index;
   sl.groups.clear();
@@ -546,7 +546,12 @@ int apspie_server_create(int device, size_t state_budget_bytes, int max_batch,
         apspie_server_destroy(s);
         return APSPIE_ERR_CUDA;
       }
-      if (l == 1) apspie_ctx_set_max_grid(ln.ctx, kDeepBlocks);
+      if (l == 1) {
+        // the deep lane: half of the resident persistent blocks
+        int resident = 0;
+        apspie_ctx_resident_blocks(ln.ctx, &resident);
+        apspie_ctx_set_max_grid(ln.ctx, std::max(1, resident / 2));
+      }
     }
   s->worker = std::thread(worker_main, s);
   *out = s;

@@ -16,8 +16,13 @@
 //   2. symbolic pass counts distinct columns per row (keys only), a scan gives
 //      C's row offsets, C is allocated exactly;
 //   3. numeric pass accumulates the products in double (so the float result is
-//      the correctly rounded exact sum up to double error), bitonic-sorts the
-//      table by column and writes the row straight into C.
+//      the correctly rounded exact sum up to double error) and writes the row
+//      into C in column order: warp rows bitonic-sort their small table; block
+//      rows scatter the occupied entries into C by column bucket (512 buckets
+//      over the column range: counts, a scan, atomic slots) and each thread
+//      insertion-sorts one bucket in place -- linear work instead of sorting
+//      the whole table (a row whose fullest bucket holds more than 128
+//      entries falls back to the bitonic sort).
 // Tables are at most half full, probing is linear and every insert succeeds
 // (nothing is dropped).  Explicit zeros (cancellation) stay in the structure,
 // as the reference's insert keeps every touched key.
@@ -142,12 +147,23 @@ __device__ __forceinline__ void for_each_product(int i, const int *__restrict__ 
     s_av[tid] = av;
     if (WARP) __syncwarp(); else __syncthreads();
     const int n_a = min(width, a1 - c0);
+    // owner of product p: the largest t < n_a with s_off[t] <= p.  A thread's
+    // p grows by `width` per step, so its owner only moves forward: gallop
+    // from the previous one
+    int lo = 0;
     for (int p = tid; p < total; p += width) {
-      // owner: largest t < n_a with s_off[t] <= p
-      int lo = 0, hi = n_a - 1;
-      while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (s_off[mid] <= p) lo = mid; else hi = mid - 1;
+      if (lo + 1 < n_a && s_off[lo + 1] <= p) {
+        int step = 1, hi = lo + 1;
+        while (hi + step < n_a && s_off[hi + step] <= p) {
+          hi += step;
+          step <<= 1;
+        }
+        int l2 = hi, h2 = min(hi + step, n_a) - 1;
+        while (l2 < h2) {
+          int mid = (l2 + h2 + 1) >> 1;
+          if (s_off[mid] <= p) l2 = mid; else h2 = mid - 1;
+        }
+        lo = l2;
       }
       int b = s_bs[lo] + (p - s_off[lo]);
       f(__ldg(Bind + b), (double)s_av[lo] * (double)(Bval ? __ldg(Bval + b) : 1.0f));
@@ -234,13 +250,16 @@ spgemm_warp_rows(const int *list, const Bins *bins, const long long *prod,
 }
 
 // ----------------------------------------------------------- block rows ---
+constexpr int kBuckets = kSpgThreads;  // one per thread of the block
+constexpr int kBucketMax = 128;        // fuller buckets: bitonic sort instead
+
 template <bool NUMERIC>
 __global__ void __launch_bounds__(kSpgThreads)
 spgemm_block_rows(const int *list, const Bins *bins, const long long *prod,
                   const int *__restrict__ Aptr, const int *__restrict__ Aind,
                   const float *__restrict__ Aval, const int *__restrict__ Bptr,
                   const int *__restrict__ Bind, const float *__restrict__ Bval, int *cnt,
-                  const int *Cptr, int *Cind, float *Cval) {
+                  const int *Cptr, int *Cind, float *Cval, int ncols) {
   extern __shared__ __align__(16) unsigned char dyn[];
   double *vals = NUMERIC ? (double *)dyn : nullptr;
   int *keys = (int *)(dyn + (NUMERIC ? sizeof(double) * kBlockTable : 0));
@@ -273,11 +292,55 @@ spgemm_block_rows(const int *list, const Bins *bins, const long long *prod,
       if (threadIdx.x == 0) cnt[i] = s_cnt;
     } else {
       __syncthreads();
-      bitonic_sort<false>(keys, vals, T);
-      int base = Cptr[i], n = Cptr[i + 1] - base;
-      for (int t = threadIdx.x; t < n; t += blockDim.x) {
-        Cind[base + t] = keys[t];
-        Cval[base + t] = (float)vals[t];
+      const int base = Cptr[i], n = Cptr[i + 1] - base;
+      // bucket b holds columns [b * ncols / kBuckets, (b + 1) * ncols / kBuckets)
+      __shared__ int s_bcnt[kBuckets], s_bfill[kBuckets], sw2[33];
+      s_bcnt[threadIdx.x] = 0;
+      s_bfill[threadIdx.x] = 0;
+      __syncthreads();
+      for (int t = threadIdx.x; t < T; t += blockDim.x) {
+        const int j = keys[t];
+        if (j != kEmpty) atomicAdd(&s_bcnt[(int)(((long long)j * kBuckets) / ncols)], 1);
+      }
+      __syncthreads();
+      const int mine = s_bcnt[threadIdx.x];
+      int total;
+      const int start = block_excl_scan(mine, sw2, &total);
+      const int fullest = __syncthreads_or(mine > kBucketMax);
+      if (!fullest) {
+        // the buckets' starts replace their counts, then the scatter
+        s_bcnt[threadIdx.x] = start;
+        __syncthreads();
+        for (int t = threadIdx.x; t < T; t += blockDim.x) {
+          const int j = keys[t];
+          if (j == kEmpty) continue;
+          const int b = (int)(((long long)j * kBuckets) / ncols);
+          const int pos = base + s_bcnt[b] + atomicAdd(&s_bfill[b], 1);
+          Cind[pos] = j;
+          Cval[pos] = (float)vals[t];
+        }
+        __syncthreads();
+        // each thread insertion-sorts its bucket in C (columns are distinct)
+        int *ci = Cind + base + start;
+        float *cv = Cval + base + start;
+        for (int a = 1; a < mine; ++a) {
+          const int kj = ci[a];
+          const float kv = cv[a];
+          int b = a - 1;
+          while (b >= 0 && ci[b] > kj) {
+            ci[b + 1] = ci[b];
+            cv[b + 1] = cv[b];
+            --b;
+          }
+          ci[b + 1] = kj;
+          cv[b + 1] = kv;
+        }
+      } else {
+        bitonic_sort<false>(keys, vals, T);
+        for (int t = threadIdx.x; t < n; t += blockDim.x) {
+          Cind[base + t] = keys[t];
+          Cval[base + t] = (float)vals[t];
+        }
       }
     }
     __syncthreads();
@@ -437,7 +500,7 @@ int apspie_spgemm(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B, apsp
   if (hb.n[1])
     spgemm_block_rows<false><<<gridsz(ctx, hb.n[1], 1, 4), kSpgThreads, dyn_sym, st>>>(
         l1, bins, prod, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind, nullptr, cnt, nullptr,
-        nullptr, nullptr);
+        nullptr, nullptr, n);
   if (hb.n[2])
     spgemm_dense_rows<false><<<dense_blocks, kSpgThreads, 0, st>>>(
         l2, bins, n, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind, nullptr, gbits, gvals, cnt,
@@ -495,7 +558,7 @@ int apspie_spgemm(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B, apsp
   if (hb.n[1])
     spgemm_block_rows<true><<<gridsz(ctx, hb.n[1], 1, 1), kSpgThreads, dyn_num, st>>>(
         l1, bins, prod, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind, B->d_val, cnt, Cptr,
-        Cind, Cval);
+        Cind, Cval, n);
   if (hb.n[2])
     spgemm_dense_rows<true><<<dense_blocks, kSpgThreads, 0, st>>>(
         l2, bins, n, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind, B->d_val, gbits, gvals,

@@ -7,10 +7,14 @@
 // (src/tc.cuh:169-199) and a float mgpu::Reduce.  Here nothing but the count
 // is produced: for each row i of L, L(i,:) goes into a shared-memory hash
 // set, and every wedge j in L(k,:) for k in L(i,:) probes it; a hit is a
-// triangle (i > k > j).  Rows are binned by |L(i,:)|: one warp per row up to
-// 256 entries (table 512), one block per row up to 4096 (table 8192), and a
-// binary-search fallback over the sorted row beyond that.  Per-warp partial
-// counts are summed in 64-bit and added with one atomic per warp.
+// triangle (i > k > j).  Rows of up to 256 entries go one warp per row
+// (table 512).  Longer rows are cut into units of 512 of their k's, one
+// block per unit, so a hub row's wedges spread over many blocks; the unit's
+// set of L(i,:) is a bitmap over all vertex ids in shared memory when the
+// graph has at most kTcBitmapMaxVerts vertices (one bit probe per wedge),
+// else a hash table (rows up to 8192) or a binary search of the sorted row.
+// Per-warp partial counts are summed in 64-bit and added with one atomic per
+// warp.
 //
 // tc_prepare relabels vertices by ascending (degree, id) with the stable
 // radix sort, keeps the edges with new(col) < new(row), sorts them by
@@ -67,22 +71,30 @@ struct TcBins {
   unsigned long long count;
 };
 
-__global__ void tc_bin(int m, const int *__restrict__ Lp, int *lists, TcBins *bins) {
+constexpr int kTcUnitK = 512;                 // k's of a long row per block unit
+constexpr int kTcBitmapMaxVerts = 1 << 20;    // 128 KiB of shared bitmap
+
+// warp rows -> lists[0..); long rows -> units (i, piece) in units[0..)
+__global__ void tc_bin(int m, const int *__restrict__ Lp, int *lists, int2 *units, TcBins *bins) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
     int d = Lp[i + 1] - Lp[i];
     if (d < 2) continue;  // a triangle needs two lower neighbours
-    int b = d <= kTcWarpMax ? 0 : (d <= kTcBlockMax ? 1 : 2);
-    unsigned s = atomicAdd(&bins->n[b], 1u);
-    lists[(size_t)b * m + s] = i;
+    if (d <= kTcWarpMax) {
+      lists[atomicAdd(&bins->n[0], 1u)] = i;
+    } else {
+      const int pieces = (d + kTcUnitK - 1) / kTcUnitK;
+      const unsigned s = atomicAdd(&bins->n[1], (unsigned)pieces);
+      for (int p = 0; p < pieces; ++p) units[s + p] = make_int2(i, p);
+    }
   }
 }
 
-// Wedges of row i dealt over a group (warp or block): visit(j) per wedge.
+// Wedges (k, j) for the k's at positions [a0, a1) of Li, dealt over a group
+// (warp or block): visit(j) per wedge.
 template <bool WARP, typename F>
-__device__ __forceinline__ void for_each_wedge(int i, const int *__restrict__ Lp,
-                                               const int *__restrict__ Li, int *s_off, int *s_bs,
-                                               F visit) {
-  const int a0 = __ldg(Lp + i), a1 = __ldg(Lp + i + 1);
+__device__ __forceinline__ void for_each_wedge_in(int a0, int a1, const int *__restrict__ Lp,
+                                                  const int *__restrict__ Li, int *s_off,
+                                                  int *s_bs, F visit) {
   const int width = WARP ? 32 : (int)blockDim.x;
   const int tid = WARP ? lane_id() : (int)threadIdx.x;
   for (int c0 = a0; c0 < a1; c0 += width) {
@@ -105,16 +117,36 @@ __device__ __forceinline__ void for_each_wedge(int i, const int *__restrict__ Lp
     s_bs[tid] = bs;
     if (WARP) __syncwarp(); else __syncthreads();
     const int n_a = min(width, a1 - c0);
+    // the k owning wedge p: a thread's p grows by `width` per step, so its
+    // owner only moves forward -- gallop from the previous one
+    int lo = 0;
     for (int p = tid; p < total; p += width) {
-      int lo = 0, hi = n_a - 1;
-      while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (s_off[mid] <= p) lo = mid; else hi = mid - 1;
+      if (lo + 1 < n_a && s_off[lo + 1] <= p) {
+        int step = 1, hi = lo + 1;
+        while (hi + step < n_a && s_off[hi + step] <= p) {
+          hi += step;
+          step <<= 1;
+        }
+        // owner in [hi, min(hi + step, n_a) - 1]
+        int l2 = hi, h2 = min(hi + step, n_a) - 1;
+        while (l2 < h2) {
+          int mid = (l2 + h2 + 1) >> 1;
+          if (s_off[mid] <= p) l2 = mid; else h2 = mid - 1;
+        }
+        lo = l2;
       }
       visit(__ldg(Li + s_bs[lo] + (p - s_off[lo])));
     }
     if (WARP) __syncwarp(); else __syncthreads();
   }
+}
+
+// Wedges of row i.
+template <bool WARP, typename F>
+__device__ __forceinline__ void for_each_wedge(int i, const int *__restrict__ Lp,
+                                               const int *__restrict__ Li, int *s_off, int *s_bs,
+                                               F visit) {
+  for_each_wedge_in<WARP>(__ldg(Lp + i), __ldg(Lp + i + 1), Lp, Li, s_off, s_bs, visit);
 }
 
 __global__ void __launch_bounds__(32 * kTcWarps)
@@ -141,45 +173,59 @@ tc_warp_rows(const int *list, TcBins *bins, const int *__restrict__ Lp, const in
   if (lane == 0 && cnt) atomicAdd(&bins->count, cnt);
 }
 
+// One unit = the k's [piece * kTcUnitK, +kTcUnitK) of a long row i, one
+// block per unit.  MODE 0: L(i,:) as a bitmap over all vertex ids (dynamic
+// shared memory, zero between units: set bits are cleared again); MODE 1:
+// hash table (rows up to kTcBlockMax); MODE 2: binary search in the row.
+template <int MODE>
 __global__ void __launch_bounds__(kTcThreads)
-tc_block_rows(const int *list, TcBins *bins, const int *__restrict__ Lp, const int *__restrict__ Li) {
-  __shared__ int keys[kTcBlockTable];
+tc_units(const int2 *units, TcBins *bins, int m, const int *__restrict__ Lp,
+         const int *__restrict__ Li) {
+  extern __shared__ unsigned tc_smem[];
   __shared__ int s_off[kTcThreads], s_bs[kTcThreads];
   unsigned long long cnt = 0;
-  const unsigned nrows = bins->n[1];
-  for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
-    int i = list[r];
-    int a0 = __ldg(Lp + i), d = __ldg(Lp + i + 1) - a0;
-    int bits = tbits(d, 13);
-    for (int t = threadIdx.x; t < (1 << bits); t += blockDim.x) keys[t] = kNone;
-    __syncthreads();
-    for (int t = threadIdx.x; t < d; t += blockDim.x) set_insert(keys, bits, __ldg(Li + a0 + t));
-    __syncthreads();
-    for_each_wedge<false>(i, Lp, Li, s_off, s_bs,
-                          [&](int j) { cnt += set_has(keys, bits, j) ? 1 : 0; });
+  const unsigned nunits = bins->n[1];
+  if (MODE != 2) {
+    const int words = MODE == 0 ? (m + 31) / 32 : kTcBlockTable;
+    for (int t = threadIdx.x; t < words; t += blockDim.x) tc_smem[t] = MODE == 0 ? 0u : (unsigned)kNone;
     __syncthreads();
   }
-  cnt = warp_sum(cnt);
-  if (lane_id() == 0 && cnt) atomicAdd(&bins->count, cnt);
-}
-
-// Rows longer than the block table: binary search in the sorted row.
-__global__ void __launch_bounds__(kTcThreads)
-tc_search_rows(const int *list, TcBins *bins, const int *__restrict__ Lp, const int *__restrict__ Li) {
-  __shared__ int s_off[kTcThreads], s_bs[kTcThreads];
-  unsigned long long cnt = 0;
-  const unsigned nrows = bins->n[2];
-  for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
-    int i = list[r];
-    const int a0 = __ldg(Lp + i), a1 = __ldg(Lp + i + 1);
-    for_each_wedge<false>(i, Lp, Li, s_off, s_bs, [&](int j) {
-      int lo = a0, hi = a1;
-      while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (__ldg(Li + mid) < j) lo = mid + 1; else hi = mid;
+  for (unsigned u = blockIdx.x; u < nunits; u += gridDim.x) {
+    const int2 un = units[u];
+    const int i = un.x;
+    const int a0 = __ldg(Lp + i), a1 = __ldg(Lp + i + 1), d = a1 - a0;
+    const int k0 = a0 + un.y * kTcUnitK, k1 = min(k0 + kTcUnitK, a1);
+    if (MODE == 0) {
+      for (int t = threadIdx.x; t < d; t += blockDim.x) {
+        const int j = __ldg(Li + a0 + t);
+        atomicOr(tc_smem + (j >> 5), 1u << (j & 31));
       }
-      cnt += (lo < a1 && __ldg(Li + lo) == j) ? 1 : 0;
-    });
+      __syncthreads();
+      for_each_wedge_in<false>(k0, k1, Lp, Li, s_off, s_bs,
+                               [&](int j) { cnt += (tc_smem[j >> 5] >> (j & 31)) & 1u; });
+      __syncthreads();
+      for (int t = threadIdx.x; t < d; t += blockDim.x) tc_smem[__ldg(Li + a0 + t) >> 5] = 0u;
+      __syncthreads();
+    } else if (MODE == 1 && d <= kTcBlockMax) {
+      int *keys = reinterpret_cast<int *>(tc_smem);
+      const int bits = tbits(d, 13);
+      for (int t = threadIdx.x; t < (1 << bits); t += blockDim.x) keys[t] = kNone;
+      __syncthreads();
+      for (int t = threadIdx.x; t < d; t += blockDim.x) set_insert(keys, bits, __ldg(Li + a0 + t));
+      __syncthreads();
+      for_each_wedge_in<false>(k0, k1, Lp, Li, s_off, s_bs,
+                               [&](int j) { cnt += set_has(keys, bits, j) ? 1 : 0; });
+      __syncthreads();
+    } else {
+      for_each_wedge_in<false>(k0, k1, Lp, Li, s_off, s_bs, [&](int j) {
+        int lo = a0, hi = a1;
+        while (lo < hi) {
+          int mid = (lo + hi) >> 1;
+          if (__ldg(Li + mid) < j) lo = mid + 1; else hi = mid;
+        }
+        cnt += (lo < a1 && __ldg(Li + lo) == j) ? 1 : 0;
+      });
+    }
   }
   cnt = warp_sum(cnt);
   if (lane_id() == 0 && cnt) atomicAdd(&bins->count, cnt);
@@ -319,16 +365,24 @@ int apspie_tc(apspie_ctx ctx, int m, int64_t lnnz, const int *d_Lptr, const int 
   if (m <= 0 || lnnz < 0 || !d_Lptr || (lnnz > 0 && !d_Lind) || !h_count)
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_tc: bad arguments");
   cudaStream_t st = ctx->stream;
-  auto *lists = (int *)workspace(ctx, kSlotMisc0, sizeof(int) * 3 * (size_t)m);
+  auto *lists = (int *)workspace(ctx, kSlotMisc0, sizeof(int) * (size_t)m);
+  // units: at most lnnz / kTcUnitK + (rows longer than kTcWarpMax) pieces
+  auto *units = (int2 *)workspace(
+      ctx, kSlotMisc1, sizeof(int2) * ((size_t)lnnz / kTcUnitK + (size_t)lnnz / kTcWarpMax + 2));
   auto *bins = (TcBins *)workspace(ctx, kSlotSmall, sizeof(TcBins));
-  if (!lists || !bins) return APSPIE_ERR_OOM;
+  if (!lists || !units || !bins) return APSPIE_ERR_OOM;
   cudaMemsetAsync(bins, 0, sizeof(TcBins), st);
-  tc_bin<<<tgrid(ctx, m, 256), 256, 0, st>>>(m, d_Lptr, lists, bins);
+  tc_bin<<<tgrid(ctx, m, 256), 256, 0, st>>>(m, d_Lptr, lists, units, bins);
   tc_warp_rows<<<ctx->num_sms * 16, 32 * kTcWarps, 0, st>>>(lists, bins, d_Lptr, d_Lind);
-  tc_block_rows<<<ctx->num_sms * 4, kTcThreads, 0, st>>>(lists + m, bins, d_Lptr, d_Lind);
-  tc_search_rows<<<ctx->num_sms * 2, kTcThreads, 0, st>>>(lists + 2 * (size_t)m, bins, d_Lptr,
-                                                          d_Lind);
-  int rc = check_launch(ctx, "apspie_tc", 4);
+  if (m <= kTcBitmapMaxVerts) {
+    const int smem = (int)(sizeof(unsigned) * (size_t)((m + 31) / 32));
+    cudaFuncSetAttribute(tc_units<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    tc_units<0><<<ctx->num_sms * 2, kTcThreads, smem, st>>>(units, bins, m, d_Lptr, d_Lind);
+  } else {
+    const int smem = (int)(sizeof(int) * kTcBlockTable);
+    tc_units<1><<<ctx->num_sms * 4, kTcThreads, smem, st>>>(units, bins, m, d_Lptr, d_Lind);
+  }
+  int rc = check_launch(ctx, "apspie_tc", 3);
   if (rc) return rc;
   auto *h = (TcBins *)pinned(ctx, sizeof(TcBins));
   if (!h) return APSPIE_ERR_OOM;

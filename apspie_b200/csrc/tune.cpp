@@ -22,20 +22,6 @@
 namespace apspie {
 namespace {
 
-uint64_t fingerprint(apspie_context *ctx, int m, int64_t nnz, const int *d_ptr) {
-  // offsets sampled at 64 evenly spaced rows (plus the last)
-  int *h = (int *)pinned(ctx, sizeof(int) * 65);
-  uint64_t f = 1469598103934665603ull ^ ((uint64_t)m << 32) ^ (uint64_t)nnz;
-  if (!h) return f;
-  for (int i = 0; i <= 64; ++i) {
-    size_t row = (size_t)((int64_t)m * i / 64);
-    cudaMemcpyAsync(h + i, d_ptr + row, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-  }
-  cudaStreamSynchronize(ctx->stream);
-  for (int i = 0; i <= 64; ++i) f = (f ^ (uint64_t)(uint32_t)h[i]) * 1099511628211ull;
-  return f;
-}
-
 float time_bfs(apspie_context *ctx, int nsrc, const int *src, int64_t nnz, int m, const int *ptr,
                const int *ind, const int *tptr, const int *tind, int32_t *depth, int *rc) {
   cudaEvent_t a, b;
@@ -69,7 +55,7 @@ int apspie_autotune_bfs(apspie_ctx ctx, int nsrc, const int *h_src, int64_t nnz,
   APSPIE_CHECK_CTX(ctx);
   if (nsrc <= 0 || !h_src || !d_depth_scratch || !alpha_out || !beta_out)
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_bfs: bad arguments");
-  const uint64_t fp = fingerprint(ctx, m, nnz, d_ptr);
+  const uint64_t fp = graph_fingerprint(ctx, m, nnz, d_ptr);
   for (auto &e : ctx->tune_cache)
     if (e.fp == fp) {
       *alpha_out = e.alpha;

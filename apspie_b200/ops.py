@@ -88,6 +88,21 @@ def bfs(ctx: Context, g, src: int, depth=None, max_levels: int = 0):
     return depth
 
 
+def csr_transpose(ctx: Context, m: int, n: int, ptr, ind, val=None):
+    """CSC of an m x n CSR on the device (apspie_csr_transpose): returns
+    (tptr, tind, tval) tensors, row ids ascending within each column."""
+    import torch
+    dev = ptr.device
+    nnz = int(ind.numel())
+    tptr = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    tind = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+    tval = torch.empty(max(nnz, 1), dtype=torch.float32, device=dev)
+    check(lib.apspie_csr_transpose(ctx.handle, int(m), int(n), nnz, _p(ptr), _p(ind), _p(val),
+                                   _p(tptr), _p(tind), _p(tval)), ctx.handle,
+          "apspie_csr_transpose")
+    return tptr, tind[:nnz], tval[:nnz]
+
+
 def bfs_prepare(ctx: Context, g):
     """Pull-ordered in-adjacency of g (apspie_bfs_prepare): sets g.tptr /
     g.tind, which bfs() then pulls over."""

@@ -91,6 +91,15 @@ typedef struct {
  * reports a device-side timeout of that run as APSPIE_ERR_TIMEOUT. */
 int apspie_bfs_get_stats(apspie_ctx ctx, apspie_bfs_stats *out);
 
+/* Transpose of an m x n CSR (the CSC of the matrix; csr2csc,
+ * src/util.cuh:474, extract_csr2csc, src/matrix.cpp:230): d_tptr n + 1
+ * offsets, d_tind nnz row ids ascending within each column, d_tval nnz values
+ * (may be NULL; d_val NULL = ones).  Caller-allocated outputs; a stable radix
+ * sort of the edges on the device. */
+int apspie_csr_transpose(apspie_ctx ctx, int m, int n, int64_t nnz,
+                         const int *d_ptr, const int *d_ind, const float *d_val,
+                         int *d_tptr, int *d_tind, float *d_tval);
+
 /* Builds the in-adjacency that apspie_bfs pulls over (d_tptr: m + 1
  * offsets, d_tind: nnz indices, caller-allocated) from the out-adjacency,
  * each row ordered by the neighbours' out-degree, highest first (ties by
@@ -242,6 +251,12 @@ typedef struct {
 
 int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs,
                      int max_steps);
+/* Jobs on graphs whose BFS takes more than 64 levels (found by one probe BFS
+ * per new graph, cached by fingerprint) run in a second launch on a second
+ * stream next to the others when both kinds are present; deep_blocks = its
+ * grid (0: two thirds of the resident blocks, the default; at least the
+ * resident blocks: no second launch, every job in one). */
+int apspie_batch_set_params(apspie_ctx ctx, int deep_blocks);
 /* Statistics of the last batch (synchronises; reports a barrier timeout). */
 int apspie_batch_get_stats(apspie_ctx ctx, apspie_batch_stats *out);
 

@@ -14,7 +14,9 @@
 //   * spmspvMis takes any order-preserving 32-bit priority: float priorities
 //     in (0, 1] (the reference's cuRAND draws) are used through their bit
 //     patterns, uint32 priorities (mt19937) directly;
-//   * spgemm ignores partSize / partNum (no 2-D tiling is needed).
+//   * spgemm ignores partSize / partNum (no 2-D tiling is needed);
+//   * csr2csc takes the context as a last argument (the reference creates
+//     a cuSPARSE handle inside; here the context carries the stream).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -249,6 +251,30 @@ void mXv(const int *d_randVecInd, const T *d_randVecVal, const int edge, const i
                               &out, nullptr),
                 context.handle(), "mXv");
   nnz = out;
+}
+
+// Dense SpMV spmv<T>() (src/bfs.cuh:11-14, mgpu::SpmvCsrBinary): y = A x over
+// every row of the CSR (plus-times; the sum is taken in double).
+template <typename T>
+void spmv(const T *d_inputVector, const int edge, const int m, const T *d_csrValA,
+          const int *d_csrRowPtrA, const int *d_csrColIndA, T *d_spmvResult,
+          mgpu::CudaContext &context) {
+  apspie::check(apspie_spmv(context.handle(), APSPIE_PLUS_TIMES, m, edge, d_csrRowPtrA,
+                            d_csrColIndA, (const float *)d_csrValA, (const float *)d_inputVector,
+                            (float *)d_spmvResult),
+                context.handle(), "spmv");
+}
+
+// csr2csc<T>() (src/util.cuh:473-488): transpose of a square CSR, values
+// carried along, row ids ascending within each column.
+template <typename typeVal>
+void csr2csc(const int m, const int edge, const typeVal *d_csrValA, const int *d_csrRowPtrA,
+             const int *d_csrColIndA, typeVal *d_cscValA, int *d_cscRowIndA, int *d_cscColPtrA,
+             mgpu::CudaContext &context) {
+  apspie::check(apspie_csr_transpose(context.handle(), m, m, edge, d_csrRowPtrA, d_csrColIndA,
+                                     (const float *)d_csrValA, d_cscColPtrA, d_cscRowIndA,
+                                     (float *)d_cscValA),
+                context.handle(), "csr2csc");
 }
 
 // -------------------------------------------------------------- SpGEMM ---

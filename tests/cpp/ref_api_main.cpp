@@ -5,7 +5,7 @@
 // routine through the reference's signatures (include/apspie_ref.hpp), then
 // verify() / unverify().  Exit status 0 means CORRECT.
 //
-//   ref_api_main <bfs|spmspvbfs|sssp|mis|mxv|spgemm|tc> file.mtx [-source N] [-undirected]
+//   ref_api_main <bfs|spmspvbfs|sssp|mis|mxv|spmv|csr2csc|spgemm|tc> file.mtx [-source N] [-undirected]
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -150,6 +150,51 @@ int main(int argc, char **argv) {
       delete d;
       cudaFree(d_x);
       cudaFree(d_y);
+    } else if (algo == "spmv") {
+      // dense SpMV over every row: y = A x, x[j] = j + 1
+      std::vector<float> x(m);
+      for (int j = 0; j < m; ++j) x[j] = (float)(j + 1);
+      float *d_x = nullptr, *d_y = nullptr;
+      cudaMalloc(&d_x, sizeof(float) * m);
+      cudaMalloc(&d_y, sizeof(float) * m);
+      cudaMemcpy(d_x, x.data(), sizeof(float) * m, cudaMemcpyHostToDevice);
+      spmv<float>(d_x, edge, m, A.d_cscVal, A.d_cscColPtr, A.d_cscRowInd, d_y, *context);
+      std::vector<float> expect(m, 0.0f);
+      for (int r = 0; r < m; ++r) {
+        double acc = 0;
+        for (int k = g.ptr[r]; k < g.ptr[r + 1]; ++k) acc += (double)g.val[k] * x[g.ind[k]];
+        expect[r] = (float)acc;
+      }
+      errors = verify(m, download(d_y, m).data(), expect.data());
+      cudaFree(d_x);
+      cudaFree(d_y);
+    } else if (algo == "csr2csc") {
+      float *d_tv = nullptr;
+      int *d_tp = nullptr, *d_ti = nullptr;
+      cudaMalloc(&d_tv, sizeof(float) * (edge > 0 ? edge : 1));
+      cudaMalloc(&d_ti, sizeof(int) * (edge > 0 ? edge : 1));
+      cudaMalloc(&d_tp, sizeof(int) * (m + 1));
+      csr2csc<float>(m, edge, A.d_cscVal, A.d_cscColPtr, A.d_cscRowInd, d_tv, d_ti, d_tp,
+                     *context);
+      // host transpose: column-major counting sort of the same arrays
+      std::vector<int> tp(m + 1, 0), ti(edge), fill;
+      std::vector<float> tv(edge);
+      for (int k = 0; k < edge; ++k) ++tp[g.ind[k] + 1];
+      for (int j = 0; j < m; ++j) tp[j + 1] += tp[j];
+      fill.assign(tp.begin(), tp.end() - 1);
+      for (int r = 0; r < m; ++r)
+        for (int k = g.ptr[r]; k < g.ptr[r + 1]; ++k) {
+          ti[fill[g.ind[k]]] = r;
+          tv[fill[g.ind[k]]++] = g.val[k];
+        }
+      errors = verify(m + 1, download(d_tp, m + 1).data(), tp.data());
+      if (edge > 0) {
+        errors += verify(edge, download(d_ti, edge).data(), ti.data());
+        errors += verify(edge, download(d_tv, edge).data(), tv.data());
+      }
+      cudaFree(d_tv);
+      cudaFree(d_ti);
+      cudaFree(d_tp);
     } else if (algo == "spgemm") {
       d_matrix C;
       spgemm(&C, &A, &A, 0, 0, *context);

@@ -53,3 +53,23 @@ def test_weights_device_match_host(ctx):
     d = ap.weights_device(ctx, h.to_device(), seed=9)
     np.testing.assert_array_equal(d.w_u32.cpu().numpy().view(np.uint32), wu)
     np.testing.assert_array_equal(d.w_f32.cpu().numpy(), wf)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("m,n", [(1000, 1000), (700, 1500), (3000, 40)])
+def test_csr_transpose_matches_host(ctx, m, n):
+    """apspie_csr_transpose = the CSC: offsets, row ids ascending within a
+    column, values carried along (scipy's csr -> csc as the reference)."""
+    import scipy.sparse as sp
+    import torch
+    rng = np.random.default_rng(m + n)
+    a = sp.random(m, n, density=0.01, format="csr", random_state=rng, dtype=np.float32)
+    a.sort_indices()
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    tp, ti, tv = ap.csr_transpose(ctx, m, n, t(a.indptr.astype(np.int32)),
+                                  t(a.indices.astype(np.int32)), t(a.data))
+    c = a.tocsc()
+    c.sort_indices()
+    np.testing.assert_array_equal(tp.cpu().numpy(), c.indptr)
+    np.testing.assert_array_equal(ti.cpu().numpy(), c.indices)
+    np.testing.assert_array_equal(tv.cpu().numpy(), c.data)

@@ -119,3 +119,30 @@ def test_tc_rmat(ctx, scale):
     import apspie_b200 as ap
     count = _tc(ctx, ap.gen_rmat(scale, 16, seed=1))
     assert count > 0
+
+
+def _sym(m, pairs):
+    import apspie_b200 as ap
+    e = np.asarray(pairs, dtype=np.int64)
+    rows = np.concatenate([e[:, 0], e[:, 1]])
+    cols = np.concatenate([e[:, 1], e[:, 0]])
+    order = np.lexsort((cols, rows))
+    return ap.from_edges(m, rows[order], cols[order])
+
+
+@pytest.mark.parametrize("m", [6000, 1_200_000])
+def test_tc_long_rows_both_set_forms(ctx, m):
+    """A hub whose lower row has 5,000 entries (more than the hash-table bound
+    of 4,096) and R-MAT 12 edges, spread over m vertex ids: m = 6,000 uses
+    the shared-memory bitmap, m = 1.2 M (more than 2^20) the hash table and
+    the binary search; the count matches the oracle either way."""
+    import apspie_b200 as ap
+    stride = (m - 1) // 5200
+    hub, path = 0, [stride * (t + 1) for t in range(5000)]
+    pairs = [(hub, p) for p in path] + [(path[t], path[t + 1]) for t in range(4999)]
+    assert _tc(ctx, _sym(m, pairs)) == 4999
+    r = ap.gen_rmat(12, 16, seed=3)
+    src = np.repeat(np.arange(r.m), np.diff(r.ptr))
+    keep = src < r.ind
+    spread = lambda v: v.astype(np.int64) * ((m - 1) // r.m)
+    _tc(ctx, _sym(m, np.stack([spread(src[keep]), spread(r.ind[keep])], axis=1)))
