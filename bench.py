@@ -471,7 +471,8 @@ def run_ours(args):
     g = h.to_device(local)
     deg = h.degrees()
     nsrc = max(args.steps, 1)
-    sources = ap.seeded_sources(h, nsrc + args.warmup, seed=rank)
+    from apspie_b200.replicas import replica_sources
+    sources = replica_sources(h, nsrc + args.warmup, rank)
     ctx = ap.Context(local)
     stream = torch.cuda.current_stream(local)
     depth = torch.empty(h.m, dtype=torch.int32, device=g.ptr.device)
@@ -531,15 +532,8 @@ def run_ours(args):
             torch.cuda.synchronize()
     per = [a.elapsed_time(b) for a, b in ev]
     ms = total_ms
-    if dist:
-        t = torch.tensor([ms], device=g.ptr.device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        et = torch.tensor([float(sum(e_r))], device=g.ptr.device, dtype=torch.float64)
-        dist.all_reduce(et)
-        edges_all = float(et.item())
-    else:
-        edges_all = float(sum(e_r))
+    from apspie_b200.replicas import aggregate
+    ms, edges_all = aggregate(ms, float(sum(e_r)), device=g.ptr.device)
     value = edges_all / (ms * 1e-3) / 1e9
 
     # ---- roofline of the traversal kernel (bfs_init + bfs_persistent per launch) ----
