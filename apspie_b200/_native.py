@@ -92,6 +92,8 @@ PROTOS: dict[str, tuple] = {
     "apspie_mxv_dense": (c_int, [vp, c_int, c_int, c_i64, vp, vp, vp, vp, vp, P_i64]),
     "apspie_spmspv_set_params": (c_int, [vp, C.c_double]),
     "apspie_spgemm": (c_int, [vp, C.POINTER(Csr), C.POINTER(Csr), C.POINTER(Csr)]),
+    "apspie_spgemm_symbolic": (c_int, [vp, C.POINTER(Csr), C.POINTER(Csr), vp, P_i64]),
+    "apspie_spgemm_numeric": (c_int, [vp, C.POINTER(Csr), C.POINTER(Csr), vp, vp, vp]),
     "apspie_csr_free": (c_int, [vp, C.POINTER(Csr)]),
     "apspie_csr_copy_out": (c_int, [vp, C.POINTER(Csr), vp, vp, vp]),
     "apspie_tc_prepare": (c_int, [vp, c_i64, c_int, vp, vp, vp, vp, vp, P_i64]),

@@ -58,6 +58,11 @@ struct apspie_context {
     int levels;
   };
   std::vector<DepthEntry> depth_cache;
+  // SpGEMM plan left by apspie_spgemm_symbolic for apspie_spgemm_numeric
+  bool spgemm_plan_valid = false;
+  const void *spgemm_plan_A = nullptr, *spgemm_plan_B = nullptr;
+  int spgemm_plan_m = 0, spgemm_plan_n = 0;
+  unsigned spgemm_plan_bins[3] = {0, 0, 0};
   // autotuner results by graph fingerprint
   struct TuneEntry {
     uint64_t fp;
@@ -104,6 +109,13 @@ enum SlotId : int {
   kSlotMxvFlags,
   kSlotSmall,
   kSlotBatch,
+  // SpGEMM plan: kept from the symbolic phase for repeated numeric phases
+  kSlotSpgProd,
+  kSlotSpgLists,
+  kSlotSpgCnt,
+  kSlotSpgBins,
+  kSlotSpgBits,
+  kSlotSpgVals,
   kSlotCount
 };
 

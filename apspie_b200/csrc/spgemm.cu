@@ -433,24 +433,20 @@ using namespace apspie;
 
 extern "C" {
 
-int apspie_spgemm(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B, apspie_csr *C) {
+int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B,
+                           int *d_Cptr, int64_t *h_nnz) {
   APSPIE_CHECK_CTX(ctx);
-  if (!A || !B || !C || A->m < 0 || A->n < 0 || B->m != A->n || B->n < 0 || !A->d_ptr ||
-      !B->d_ptr || (A->nnz > 0 && !A->d_ind) || (B->nnz > 0 && !B->d_ind))
-    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_spgemm: bad matrices");
+  if (!A || !B || !d_Cptr || !h_nnz || A->m < 0 || A->n < 0 || B->m != A->n || B->n < 0 ||
+      !A->d_ptr || !B->d_ptr || (A->nnz > 0 && !A->d_ind) || (B->nnz > 0 && !B->d_ind))
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_spgemm_symbolic: bad matrices");
+  ctx->spgemm_plan_valid = false;
   const int m = A->m, n = B->n;
   cudaStream_t st = ctx->stream;
-  C->m = m;
-  C->n = n;
-  C->nnz = 0;
-  C->d_ptr = nullptr;
-  C->d_ind = nullptr;
-  C->d_val = nullptr;
-  auto *prod = (long long *)workspace(ctx, kSlotMisc0, sizeof(long long) * ((size_t)m + 1));
-  auto *lists = (int *)workspace(ctx, kSlotMisc1, sizeof(int) * 3 * ((size_t)m + 1));
-  auto *cnt = (int *)workspace(ctx, kSlotMisc2, sizeof(int) * ((size_t)m + 1));
+  auto *prod = (long long *)workspace(ctx, kSlotSpgProd, sizeof(long long) * ((size_t)m + 1));
+  auto *lists = (int *)workspace(ctx, kSlotSpgLists, sizeof(int) * 3 * ((size_t)m + 1));
+  auto *cnt = (int *)workspace(ctx, kSlotSpgCnt, sizeof(int) * ((size_t)m + 1));
   auto *offs = (long long *)workspace(ctx, kSlotMisc3, sizeof(long long) * ((size_t)m + 2));
-  auto *bins = (Bins *)workspace(ctx, kSlotSmall, sizeof(Bins) + 64);
+  auto *bins = (Bins *)workspace(ctx, kSlotSpgBins, sizeof(Bins) + 64);
   if (!prod || !lists || !cnt || !offs || !bins) return APSPIE_ERR_OOM;
   long long *d_total = (long long *)(bins + 1);
   cudaMemsetAsync(bins, 0, sizeof(Bins), st);
@@ -481,8 +477,8 @@ int apspie_spgemm(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B, apsp
   unsigned *gbits = nullptr;
   double *gvals = nullptr;
   if (dense_blocks > 0) {
-    gbits = (unsigned *)workspace(ctx, kSlotBitmap, sizeof(unsigned) * (size_t)words * dense_blocks);
-    gvals = (double *)workspace(ctx, kSlotDense, sizeof(double) * (size_t)n * dense_blocks);
+    gbits = (unsigned *)workspace(ctx, kSlotSpgBits, sizeof(unsigned) * (size_t)words * dense_blocks);
+    gvals = (double *)workspace(ctx, kSlotSpgVals, sizeof(double) * (size_t)n * dense_blocks);
     if (!gbits || !gvals) return APSPIE_ERR_OOM;
     zero_words<<<gridsz(ctx, (long long)words * dense_blocks, 256), 256, 0, st>>>(
         (size_t)words * dense_blocks, gbits);
@@ -529,26 +525,60 @@ int apspie_spgemm(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B, apsp
   if (nnzC >= (long long)INT32_MAX)
     return set_error(ctx, APSPIE_ERR_OVERFLOW, "apspie_spgemm: nnz(C) = %lld exceeds int32",
                      nnzC);
-  // C is allocated by the library, as the reference's spgemm does
-  // (src/spgemmKernel.cuh:669-681); release it with apspie_csr_free.
-  int *Cptr = nullptr, *Cind = nullptr;
-  float *Cval = nullptr;
-  cudaError_t e = cudaMalloc(&Cptr, sizeof(int) * ((size_t)m + 1));
-  if (e == cudaSuccess) e = cudaMalloc(&Cind, sizeof(int) * (size_t)std::max(1ll, nnzC));
-  if (e == cudaSuccess) e = cudaMalloc(&Cval, sizeof(float) * (size_t)std::max(1ll, nnzC));
-  if (e != cudaSuccess) {
-    cudaFree(Cptr);
-    cudaFree(Cind);
-    cudaFree(Cval);
-    return check_cuda(ctx, e, "apspie_spgemm: allocating C");
-  }
   if (m > 0) {
     // offs[m] = total after the scan wrote offs[0..m); set the last entry
     cudaMemcpyAsync(offs + m, d_total, sizeof(long long), cudaMemcpyDeviceToDevice, st);
-    to_int32_offsets<<<gridsz(ctx, m + 1, 256), 256, 0, st>>>(m, offs, Cptr);
+    to_int32_offsets<<<gridsz(ctx, m + 1, 256), 256, 0, st>>>(m, offs, d_Cptr);
   } else {
-    cudaMemsetAsync(Cptr, 0, sizeof(int), st);
+    cudaMemsetAsync(d_Cptr, 0, sizeof(int), st);
   }
+  rc = check_launch(ctx, "to_int32_offsets");
+  if (rc) return rc;
+  // the bins, lists, counts and dense accumulators stay in the workspace for
+  // the numeric phase
+  ctx->spgemm_plan_valid = true;
+  ctx->spgemm_plan_A = A->d_ptr;
+  ctx->spgemm_plan_B = B->d_ptr;
+  ctx->spgemm_plan_m = m;
+  ctx->spgemm_plan_n = n;
+  for (int b = 0; b < 3; ++b) ctx->spgemm_plan_bins[b] = hb.n[b];
+  *h_nnz = nnzC;
+  return APSPIE_OK;
+}
+
+int apspie_spgemm_numeric(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B,
+                          const int *d_Cptr, int *d_Cind, float *d_Cval) {
+  APSPIE_CHECK_CTX(ctx);
+  if (!A || !B || !d_Cptr || !ctx->spgemm_plan_valid || ctx->spgemm_plan_A != A->d_ptr ||
+      ctx->spgemm_plan_B != B->d_ptr || ctx->spgemm_plan_m != A->m || ctx->spgemm_plan_n != B->n)
+    return set_error(ctx, APSPIE_ERR_INVALID,
+                     "apspie_spgemm_numeric: no matching apspie_spgemm_symbolic before it");
+  const int m = A->m, n = B->n;
+  cudaStream_t st = ctx->stream;
+  Bins hb;
+  for (int b = 0; b < 3; ++b) hb.n[b] = ctx->spgemm_plan_bins[b];
+  // the symbolic phase's buffers (own slots, same sizes: no reallocation;
+  // the dense accumulators are left cleared by every dense-row pass)
+  auto *prod = (long long *)workspace(ctx, kSlotSpgProd, sizeof(long long) * ((size_t)m + 1));
+  auto *lists = (int *)workspace(ctx, kSlotSpgLists, sizeof(int) * 3 * ((size_t)m + 1));
+  auto *cnt = (int *)workspace(ctx, kSlotSpgCnt, sizeof(int) * ((size_t)m + 1));
+  auto *bins = (Bins *)workspace(ctx, kSlotSpgBins, sizeof(Bins) + 64);
+  if (!prod || !lists || !cnt || !bins) return APSPIE_ERR_OOM;
+  const size_t dyn_num = sizeof(double) * kBlockTable + sizeof(int) * kBlockTable;
+  const int dense_blocks = (int)std::min<unsigned>(hb.n[2], (unsigned)ctx->num_sms * 2);
+  const int words = (n + 31) / 32;
+  unsigned *gbits = nullptr;
+  double *gvals = nullptr;
+  if (dense_blocks > 0) {
+    gbits = (unsigned *)workspace(ctx, kSlotSpgBits, sizeof(unsigned) * (size_t)words * dense_blocks);
+    gvals = (double *)workspace(ctx, kSlotSpgVals, sizeof(double) * (size_t)n * dense_blocks);
+    if (!gbits || !gvals) return APSPIE_ERR_OOM;
+  }
+  const int *l0 = lists, *l1 = lists + (size_t)m, *l2 = lists + 2 * (size_t)m;
+  const int *Cptr = d_Cptr;
+  int *Cind = d_Cind;
+  float *Cval = d_Cval;
+  int rc;
   // ---- numeric ----
   if (hb.n[0])
     spgemm_warp_rows<true><<<gridsz(ctx, hb.n[0], kWarpsPerBlockSmall, 32),
@@ -563,7 +593,41 @@ int apspie_spgemm(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B, apsp
     spgemm_dense_rows<true><<<dense_blocks, kSpgThreads, 0, st>>>(
         l2, bins, n, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind, B->d_val, gbits, gvals,
         cnt, Cptr, Cind, Cval);
-  rc = check_launch(ctx, "spgemm numeric", 4);
+  return check_launch(ctx, "spgemm numeric", 3);
+}
+
+int apspie_spgemm(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B, apspie_csr *C) {
+  APSPIE_CHECK_CTX(ctx);
+  if (!C) return set_error(ctx, APSPIE_ERR_INVALID, "apspie_spgemm: bad matrices");
+  C->m = A ? A->m : 0;
+  C->n = B ? B->n : 0;
+  C->nnz = 0;
+  C->d_ptr = nullptr;
+  C->d_ind = nullptr;
+  C->d_val = nullptr;
+  if (!A || !B || A->m < 0)
+    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_spgemm: bad matrices");
+  // C is allocated by the library, as the reference's spgemm does
+  // (src/spgemmKernel.cuh:669-681); release it with apspie_csr_free.
+  int *Cptr = nullptr, *Cind = nullptr;
+  float *Cval = nullptr;
+  cudaError_t e = cudaMalloc(&Cptr, sizeof(int) * ((size_t)A->m + 1));
+  if (e != cudaSuccess) return check_cuda(ctx, e, "apspie_spgemm: allocating C");
+  int64_t nnzC = 0;
+  int rc = apspie_spgemm_symbolic(ctx, A, B, Cptr, &nnzC);
+  if (rc) {
+    cudaFree(Cptr);
+    return rc;
+  }
+  e = cudaMalloc(&Cind, sizeof(int) * (size_t)std::max<int64_t>(1, nnzC));
+  if (e == cudaSuccess) e = cudaMalloc(&Cval, sizeof(float) * (size_t)std::max<int64_t>(1, nnzC));
+  if (e != cudaSuccess) {
+    cudaFree(Cptr);
+    cudaFree(Cind);
+    cudaFree(Cval);
+    return check_cuda(ctx, e, "apspie_spgemm: allocating C");
+  }
+  rc = apspie_spgemm_numeric(ctx, A, B, Cptr, Cind, Cval);
   if (rc) {
     cudaFree(Cptr);
     cudaFree(Cind);

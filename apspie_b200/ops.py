@@ -280,27 +280,36 @@ def spmv(ctx: Context, m: int, ptr, ind, val, x, semiring: int = 0, y=None):
     return y
 
 
+def spgemm_symbolic(ctx: Context, A, B):
+    """Symbolic phase of C = A * B: returns (ptr, nnz) with ptr C's m + 1
+    row offsets on the device.  The numeric phase (spgemm_numeric) must
+    follow on the same context with the same A and B."""
+    import torch
+    a, b = _csr(*A), _csr(*B)
+    ptr = torch.empty(a.m + 1, dtype=torch.int32, device=A[2].device)
+    nnz = C.c_int64(0)
+    check(lib.apspie_spgemm_symbolic(ctx.handle, C.byref(a), C.byref(b), _p(ptr), C.byref(nnz)),
+          ctx.handle, "apspie_spgemm_symbolic")
+    return ptr, int(nnz.value)
+
+
+def spgemm_numeric(ctx: Context, A, B, ptr, ind, val):
+    """Numeric phase of C = A * B into caller buffers ind / val (nnz(C)
+    entries each), stream-ordered, no synchronisation."""
+    a, b = _csr(*A), _csr(*B)
+    check(lib.apspie_spgemm_numeric(ctx.handle, C.byref(a), C.byref(b), _p(ptr), _p(ind),
+                                    _p(val)), ctx.handle, "apspie_spgemm_numeric")
+
+
 def spgemm(ctx: Context, A, B):
     """C = A * B (spgemm(d_matrix*...), src/spgemm.cuh:132).  A and B are
     (m, n, ptr, ind, val) tuples of device tensors (val may be None = ones);
     returns (ptr, ind, val) tensors of C (columns ascending per row)."""
     import torch
-    a, b = _csr(*A), _csr(*B)
-    c = Csr()
-    check(lib.apspie_spgemm(ctx.handle, C.byref(a), C.byref(b), C.byref(c)), ctx.handle,
-          "apspie_spgemm")
-    nnz = int(c.nnz)
-    try:
-        dev = A[2].device
-        ptr = torch.empty(c.m + 1, dtype=torch.int32, device=dev)
-        ind = torch.empty(max(c.nnz, 1), dtype=torch.int32, device=dev)
-        val = torch.empty(max(c.nnz, 1), dtype=torch.float32, device=dev)
-        check(lib.apspie_csr_copy_out(ctx.handle, C.byref(c), C.c_void_p(ptr.data_ptr()),
-                                      C.c_void_p(ind.data_ptr()), C.c_void_p(val.data_ptr())),
-              ctx.handle, "apspie_csr_copy_out")
-        ctx.sync()
-    finally:
-        lib.apspie_csr_free(ctx.handle, C.byref(c))
+    ptr, nnz = spgemm_symbolic(ctx, A, B)
+    ind = torch.empty(max(nnz, 1), dtype=torch.int32, device=ptr.device)
+    val = torch.empty(max(nnz, 1), dtype=torch.float32, device=ptr.device)
+    spgemm_numeric(ctx, A, B, ptr, ind, val)
     return ptr, ind[:nnz], val[:nnz]
 
 

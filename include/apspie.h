@@ -414,6 +414,21 @@ typedef struct {
  * release them with apspie_csr_free.  Synchronises. */
 int apspie_spgemm(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B,
                   apspie_csr *C);
+/* The two phases of apspie_spgemm with caller-owned C (the reference's
+ * spgemm does both inside one call, src/spgemm.cuh:132-342).
+ * apspie_spgemm_symbolic writes C's m + 1 row offsets into d_Cptr and nnz(C)
+ * into *h_nnz (synchronises once to read it); apspie_spgemm_numeric then
+ * fills d_Cind / d_Cval (nnz(C) entries each) for the same A and B on the
+ * same context, stream-ordered and without synchronising.  The row bins
+ * and accumulators of the symbolic phase stay in the context's workspace
+ * (slots of their own), so the numeric phase may be repeated for new
+ * values of A and B as long as their structure is unchanged; the next
+ * symbolic phase, or apspie_spgemm, replaces the plan (a numeric call for
+ * other matrices then returns APSPIE_ERR_INVALID). */
+int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B,
+                           int *d_Cptr, int64_t *h_nnz);
+int apspie_spgemm_numeric(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B,
+                          const int *d_Cptr, int *d_Cind, float *d_Cval);
 int apspie_csr_free(apspie_ctx ctx, apspie_csr *C);
 /* Stream-ordered device-to-device copy of a library-owned CSR into caller
  * buffers (m + 1 offsets, nnz indices, nnz values; d_ind / d_val may be

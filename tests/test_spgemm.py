@@ -74,6 +74,31 @@ def test_spgemm_all_bins_rectangular(ctx):
     _check_product(ctx, A, B)
 
 
+def test_spgemm_two_phase_reuse(ctx):
+    """Symbolic once, numeric into caller buffers; the numeric phase repeats
+    for new values on the same structure; a numeric call for other matrices
+    is refused."""
+    import torch
+    import apspie_b200 as ap
+    A = ap.gen_powerlaw(1 << 12, 1 << 11, max_deg=1024, seed=2)
+    B = ap.gen_powerlaw(1 << 11, 1 << 12, max_deg=1024, seed=3)
+    dA, dB = _dev_csr(A), _dev_csr(B)
+    ptr, nnz = ap.spgemm_symbolic(ctx, dA, dB)
+    ind = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    val = torch.empty(nnz, dtype=torch.float32, device="cuda")
+    rp, ri, _ = oracle.spgemm(A.m, B.ncols, A.ptr, A.ind, A.w_f32, B.ptr, B.ind, B.w_f32)
+    np.testing.assert_array_equal(ptr.cpu().numpy(), rp.astype(np.int32))
+    for scale in (1.0, -2.5):
+        dA[4].copy_(torch.from_numpy(A.w_f32 * np.float32(scale)))
+        ap.spgemm_numeric(ctx, dA, dB, ptr, ind, val)
+        _, _, rv = oracle.spgemm(A.m, B.ncols, A.ptr, A.ind, A.w_f32 * np.float32(scale),
+                                 B.ptr, B.ind, B.w_f32)
+        np.testing.assert_array_equal(ind.cpu().numpy(), ri)
+        np.testing.assert_allclose(val.cpu().numpy(), rv, rtol=1e-4, atol=1e-6)
+    with pytest.raises(ap.ApspieError):
+        ap.spgemm_numeric(ctx, dB, dA, ptr, ind, val)
+
+
 def test_spgemm_powerlaw_full_config(ctx):
     """2^18 x 2^18, row nnz power law (alpha 2.1, mean 16, max 4096): A * A."""
     import apspie_b200 as ap
