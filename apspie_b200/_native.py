@@ -94,6 +94,7 @@ PROTOS: dict[str, tuple] = {
     "apspie_spgemm": (c_int, [vp, C.POINTER(Csr), C.POINTER(Csr), C.POINTER(Csr)]),
     "apspie_spgemm_symbolic": (c_int, [vp, C.POINTER(Csr), C.POINTER(Csr), vp, P_i64]),
     "apspie_spgemm_numeric": (c_int, [vp, C.POINTER(Csr), C.POINTER(Csr), vp, vp, vp]),
+    "apspie_spgemm_set_params": (c_int, [vp, c_i64]),
     "apspie_csr_free": (c_int, [vp, C.POINTER(Csr)]),
     "apspie_csr_copy_out": (c_int, [vp, C.POINTER(Csr), vp, vp, vp]),
     "apspie_tc_prepare": (c_int, [vp, c_i64, c_int, vp, vp, vp, vp, vp, P_i64]),

@@ -149,6 +149,12 @@ int apspie_batch_set_params(apspie_ctx ctx, int deep_blocks) {
   return APSPIE_OK;
 }
 
+int apspie_spgemm_set_params(apspie_ctx ctx, int64_t bitmap_max_cols) {
+  if (!ctx || bitmap_max_cols < 0) return APSPIE_ERR_INVALID;
+  ctx->spgemm_bitmap_max_cols = bitmap_max_cols;
+  return APSPIE_OK;
+}
+
 int apspie_ctx_resident_blocks(apspie_ctx ctx, int *blocks) {
   if (!ctx || !blocks) return APSPIE_ERR_INVALID;
   *blocks = 2 * ctx->num_sms;  // 512-thread persistent blocks: two per SM fit every kernel

@@ -62,7 +62,11 @@ struct apspie_context {
   bool spgemm_plan_valid = false;
   const void *spgemm_plan_A = nullptr, *spgemm_plan_B = nullptr;
   int spgemm_plan_m = 0, spgemm_plan_n = 0;
-  unsigned spgemm_plan_bins[3] = {0, 0, 0};
+  // row counts of the SpGEMM bins (symbolic and numeric) and, last, the
+  // largest output row staged in global memory
+  unsigned spgemm_plan_bins[16] = {};
+  int spgemm_plan_words = 0;  // bitmap words per row (0: hash tables)
+  long long spgemm_bitmap_max_cols = 1 << 18;
   // autotuner results by graph fingerprint
   struct TuneEntry {
     uint64_t fp;

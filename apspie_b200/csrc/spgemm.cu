@@ -75,44 +75,97 @@ __device__ __forceinline__ int table_insert(int *keys, int bits, int j, bool *fr
 }
 
 // ---------------------------------------------------------- row products ---
+// Eight lanes per row (four rows per warp in flight): most rows of A are
+// short, so a whole warp per row would leave most lanes idle.
 __global__ void row_products(int m, const int *__restrict__ Aptr, const int *__restrict__ Aind,
                              const int *__restrict__ Bptr, long long *prod) {
-  const int lane = lane_id();
-  const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
-  for (int i = gwarp; i < m; i += nwarps) {
+  const int sub = threadIdx.x & 7;
+  const int g = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 3);
+  const int ng = (int)((gridDim.x * blockDim.x) >> 3);
+  const int rounds = (m + ng - 1) / ng;  // the same for every lane: shuffles stay converged
+  for (int rr = 0; rr < rounds; ++rr) {
+    const int i = g + rr * ng;
     long long acc = 0;
-    for (int a = __ldg(Aptr + i) + lane; a < __ldg(Aptr + i + 1); a += 32) {
-      int k = __ldg(Aind + a);
-      acc += __ldg(Bptr + k + 1) - __ldg(Bptr + k);
+    if (i < m) {
+      const int a1 = __ldg(Aptr + i + 1);
+      for (int a = __ldg(Aptr + i) + sub; a < a1; a += 8) {
+        const int k = __ldg(Aind + a);
+        acc += __ldg(Bptr + k + 1) - __ldg(Bptr + k);
+      }
     }
-    acc = warp_sum(acc);
-    if (lane == 0) prod[i] = acc;
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+    if (i < m && sub == 0) prod[i] = acc;
   }
 }
 
-struct Bins {
-  unsigned n[3];
+// Row bins.  Symbolic phase, by products: warp rows, two sizes of
+// mid rows (hash tables of 2048 / 8192 keys), block rows (bitmap or a
+// 16384-key table), dense rows (hash mode only).  Numeric phase, by the
+// exact output size of the non-warp rows: three mid sizes (tables of
+// 1024 / 2048 / 4096 entries), block rows, bitmap rows staged in global
+// memory.  Bin b's rows are lists[b * m ...].
+enum {
+  kBinWarp = 0,
+  kBinMid1,
+  kBinMid2,
+  kBinBlock,
+  kBinDense,
+  kBinN1,
+  kBinN2,
+  kBinN3,
+  kBinN4,
+  kBinN5,
+  kNumBins
+};
+constexpr int kMid1MaxProd = 1024;
+constexpr int kMid2MaxProd = 4096;
+constexpr int kN1MaxNnz = 512, kN2MaxNnz = 1024, kN3MaxNnz = 2048;
+
+// Device-side counters of one SpGEMM, read back by the host in one copy.
+struct SpgState {
+  unsigned n[kNumBins];
+  unsigned maxc;  // largest output row of bin kBinN5
   unsigned pad;
+  long long total;  // nnz(C)
 };
 
-__global__ void bin_rows(int m, const long long *prod, int *lists, Bins *bins, int *cnt) {
+// Slot of this lane's row in bin b: one atomic per distinct bin of the
+// active lanes (the bins' counters are few and hot).
+__device__ __forceinline__ unsigned warp_bin_slot(unsigned *counters, int b) {
+  const unsigned peers = __match_any_sync(__activemask(), b);
+  const int leader = __ffs(peers) - 1;
+  unsigned base = 0;
+  if (lane_id() == leader) base = atomicAdd(counters + b, (unsigned)__popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + __popc(peers & ((1u << lane_id()) - 1u));
+}
+
+__global__ void bin_rows(int m, const long long *prod, int *lists, SpgState *st, int *cnt,
+                         bool bitmap) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
     long long p = prod[i];
     if (p == 0) {
       cnt[i] = 0;
       continue;
     }
-    int b = p <= kWarpRowMaxProd ? 0 : (p <= kBlockRowMaxProd ? 1 : 2);
-    unsigned s = atomicAdd(&bins->n[b], 1u);
-    lists[(size_t)b * m + s] = i;
+    int b = p <= kWarpRowMaxProd ? kBinWarp
+            : p <= kMid1MaxProd  ? kBinMid1
+            : p <= kMid2MaxProd  ? kBinMid2
+            : (bitmap || p <= kBlockRowMaxProd) ? kBinBlock
+                                                : kBinDense;
+    lists[(size_t)b * m + warp_bin_slot(st->n, b)] = i;
   }
 }
 
 // Deals the products of row i over `nthreads` threads of a group (a warp or
 // a block): f(j, value) is called once per product.  Group-level scan-based
-// gather over the row's A entries, up to `width` A entries per step.
-template <bool WARP, typename F>
+// gather over the row's A entries, up to `width` A entries per step.  RUNS
+// (blocks only): each thread takes runs of consecutive products (one owner
+// search per run; measured faster for the symbolic passes), otherwise the
+// threads stride the products (coalesced loads of B; measured faster for
+// the numeric passes, which load two arrays of B per product).
+template <bool WARP, bool RUNS = false, typename F>
 __device__ __forceinline__ void for_each_product(int i, const int *__restrict__ Aptr,
                                                  const int *__restrict__ Aind,
                                                  const float *__restrict__ Aval,
@@ -147,9 +200,34 @@ __device__ __forceinline__ void for_each_product(int i, const int *__restrict__ 
     s_av[tid] = av;
     if (WARP) __syncwarp(); else __syncthreads();
     const int n_a = min(width, a1 - c0);
-    // owner of product p: the largest t < n_a with s_off[t] <= p.  A thread's
-    // p grows by `width` per step, so its owner only moves forward: gallop
-    // from the previous one
+    if (!WARP && RUNS) {
+      // block: each thread takes runs of vt consecutive products (vt grows
+      // with the chunk's products, up to 8): one binary search for a run's
+      // first owner (the largest t with s_off[t] <= p), then a linear walk
+      const int vt = max(1, min(8, total / width));
+      for (int p0 = tid * vt; p0 < total; p0 += width * vt) {
+        int lo = 0, hi = n_a - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (s_off[mid] <= p0) lo = mid; else hi = mid - 1;
+        }
+        int nxt = lo + 1 < n_a ? s_off[lo + 1] : INT_MAX;
+        const int pend = min(p0 + vt, total);
+        for (int p = p0; p < pend; ++p) {
+          while (p >= nxt) {
+            ++lo;
+            nxt = lo + 1 < n_a ? s_off[lo + 1] : INT_MAX;
+          }
+          const int b = s_bs[lo] + (p - s_off[lo]);
+          f(__ldg(Bind + b), (double)s_av[lo] * (double)(Bval ? __ldg(Bval + b) : 1.0f));
+        }
+      }
+      __syncthreads();
+      continue;
+    }
+    // strided: owner of product p, the largest t < n_a with s_off[t] <= p.
+    // A thread's p grows by `width` per step, so its owner only moves
+    // forward: gallop from the previous one
     int lo = 0;
     for (int p = tid; p < total; p += width) {
       if (lo + 1 < n_a && s_off[lo + 1] <= p) {
@@ -169,6 +247,101 @@ __device__ __forceinline__ void for_each_product(int i, const int *__restrict__ 
       f(__ldg(Bind + b), (double)s_av[lo] * (double)(Bval ? __ldg(Bval + b) : 1.0f));
     }
     if (WARP) __syncwarp(); else __syncthreads();
+  }
+}
+
+// Block-wide exclusive max-scan of one int per thread (identity -1).
+template <int TPB>
+__device__ __forceinline__ int block_excl_max(int v, int *sw) {
+  const int lane = lane_id(), w = warp_in_block();
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl = max(incl, y);
+  }
+  if (lane == 31) sw[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    int x = lane < TPB / 32 ? sw[lane] : -1;
+    int xi = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, xi, o);
+      if (lane >= o) xi = max(xi, y);
+    }
+    const int prev = __shfl_up_sync(kFull, xi, 1);
+    if (lane < TPB / 32) sw[lane] = lane ? prev : -1;
+  }
+  __syncthreads();
+  const int before = sw[w];
+  const int ex = __shfl_up_sync(kFull, incl, 1);
+  const int res = max(before, lane ? ex : -1);
+  __syncthreads();
+  return res;
+}
+
+// Block version of for_each_product by load-balanced search: the chunk's
+// products are taken in windows of 2 * TPB; each A entry marks the window
+// position of its first product with its index (the entry running into the
+// window marks position 0), an inclusive max-scan turns the marks into the
+// owner of every position, and thread t handles positions t and t + TPB --
+// one shared-memory read for the owner, and the loads of B's rows coalesced.
+template <int TPB, typename F>
+__device__ __forceinline__ void for_each_product_lbs(int i, const int *__restrict__ Aptr,
+                                                     const int *__restrict__ Aind,
+                                                     const float *__restrict__ Aval,
+                                                     const int *__restrict__ Bptr,
+                                                     const int *__restrict__ Bind,
+                                                     const float *__restrict__ Bval, int *s_off,
+                                                     int *s_bs, float *s_av, F f) {
+  constexpr int CAP = 2 * TPB;
+  __shared__ int s_om[CAP];
+  __shared__ int sw[33];
+  const int a0 = __ldg(Aptr + i), a1 = __ldg(Aptr + i + 1);
+  const int tid = threadIdx.x;
+  for (int c0 = a0; c0 < a1; c0 += TPB) {
+    const int a = c0 + tid;
+    int bs = 0, d = 0;
+    float av = 0.f;
+    if (a < a1) {
+      const int k = __ldg(Aind + a);
+      bs = __ldg(Bptr + k);
+      d = __ldg(Bptr + k + 1) - bs;
+      av = Aval ? __ldg(Aval + a) : 1.0f;
+    }
+    int total;
+    const int excl = block_excl_scan(d, sw, &total);
+    s_off[tid] = excl;
+    s_bs[tid] = bs;
+    s_av[tid] = av;
+    for (int w0 = 0; w0 < total; w0 += CAP) {
+      const int wn = min(CAP, total - w0);
+      s_om[tid] = -1;
+      s_om[tid + TPB] = -1;
+      __syncthreads();
+      if (d > 0) {
+        if (excl >= w0 && excl < w0 + wn) s_om[excl - w0] = tid;
+        else if (excl < w0 && excl + d > w0) s_om[0] = tid;
+      }
+      __syncthreads();
+      const int v0 = s_om[2 * tid], v1 = max(v0, s_om[2 * tid + 1]);
+      const int pre = block_excl_max<TPB>(v1, sw);
+      s_om[2 * tid] = max(pre, v0);
+      s_om[2 * tid + 1] = max(pre, v1);
+      __syncthreads();
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int q = tid + h * TPB;
+        if (q < wn) {
+          const int o = s_om[q];
+          const int b = s_bs[o] + (w0 + q - s_off[o]);
+          f(__ldg(Bind + b), (double)s_av[o] * (double)(Bval ? __ldg(Bval + b) : 1.0f));
+        }
+      }
+      __syncthreads();
+    }
+    __syncthreads();
   }
 }
 
@@ -200,9 +373,41 @@ __device__ __forceinline__ void bitonic_sort(int *keys, double *vals, int n) {
 }
 
 // ------------------------------------------------------------ warp rows ---
+// Writes the warp's compacted row (keys[0..fill) distinct, keys[fill..fill4)
+// padded with kEmpty) to C in column order: lane l holds entries l, l + 32,
+// ..., (P of them) and counts, over the whole row read four keys at a time
+// (broadcast loads), the keys below each; that count is the entry's place.
+template <int P>
+__device__ __forceinline__ void rank_emit(const int *keys, const double *vals, int fill,
+                                          int fill4, int n, int *ci, float *cv) {
+  const int lane = lane_id();
+  int myk[P], rk[P];
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    const int e = lane + 32 * q;
+    myk[q] = e < fill ? keys[e] : kEmpty;
+    rk[q] = 0;
+  }
+  const int4 *k4 = reinterpret_cast<const int4 *>(keys);
+  for (int f = 0; f < (fill4 >> 2); ++f) {
+    const int4 x = k4[f];
+#pragma unroll
+    for (int q = 0; q < P; ++q)
+      rk[q] += (x.x < myk[q]) + (x.y < myk[q]) + (x.z < myk[q]) + (x.w < myk[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    const int e = lane + 32 * q;
+    if (e < fill && rk[q] < n) {
+      ci[rk[q]] = myk[q];
+      cv[rk[q]] = (float)vals[e];
+    }
+  }
+}
+
 template <bool NUMERIC>
 __global__ void __launch_bounds__(32 * kWarpsPerBlockSmall)
-spgemm_warp_rows(const int *list, const Bins *bins, const long long *prod,
+spgemm_warp_rows(const int *list, const unsigned *nlist, const long long *prod,
                  const int *__restrict__ Aptr, const int *__restrict__ Aind,
                  const float *__restrict__ Aval, const int *__restrict__ Bptr,
                  const int *__restrict__ Bind, const float *__restrict__ Bval, int *cnt,
@@ -214,7 +419,7 @@ spgemm_warp_rows(const int *list, const Bins *bins, const long long *prod,
   const int w = warp_in_block(), lane = lane_id();
   int *keys = s_keys[w];
   double *vals = NUMERIC ? s_vals[w] : nullptr;
-  const unsigned nrows = bins->n[0];
+  const unsigned nrows = *nlist;
   for (unsigned r = blockIdx.x * kWarpsPerBlockSmall + w; r < nrows;
        r += gridDim.x * kWarpsPerBlockSmall) {
     int i = list[r];
@@ -238,12 +443,34 @@ spgemm_warp_rows(const int *list, const Bins *bins, const long long *prod,
       int c = warp_sum(fresh_count);
       if (lane == 0) cnt[i] = c;
     } else {
-      bitonic_sort<true>(keys, vals, T);
+      // compact the occupied slots to the front (in place: a slot moves
+      // only left, and each chunk of 32 is read before it is written), pad
+      // to a power of two and sort that instead of the whole table
       int base = Cptr[i], n = Cptr[i + 1] - base;
-      for (int t = lane; t < n; t += 32) {
-        Cind[base + t] = keys[t];
-        Cval[base + t] = (float)vals[t];
+      int fill = 0;
+      for (int t0 = 0; t0 < T; t0 += 32) {
+        const int k = keys[t0 + lane];
+        const double v = vals[t0 + lane];
+        const unsigned occ = __ballot_sync(kFull, k != kEmpty);
+        __syncwarp();
+        if (k != kEmpty) {
+          const int d = fill + __popc(occ & ((1u << lane) - 1u));
+          keys[d] = k;
+          vals[d] = v;
+        }
+        fill += __popc(occ);
+        __syncwarp();
       }
+      // pad to a multiple of four with keys that compare above every column
+      const int fill4 = (fill + 3) & ~3;
+      if (fill + lane < fill4) keys[fill + lane] = kEmpty;
+      __syncwarp();
+      // each entry's rank among the row's (distinct) columns is its place in C
+      const int per = (fill + 31) >> 5;
+      if (per <= 1) rank_emit<1>(keys, vals, fill, fill4, n, Cind + base, Cval + base);
+      else if (per <= 2) rank_emit<2>(keys, vals, fill, fill4, n, Cind + base, Cval + base);
+      else if (per <= 4) rank_emit<4>(keys, vals, fill, fill4, n, Cind + base, Cval + base);
+      else rank_emit<8>(keys, vals, fill, fill4, n, Cind + base, Cval + base);
     }
     __syncwarp();
   }
@@ -255,7 +482,7 @@ constexpr int kBucketMax = 128;        // fuller buckets: bitonic sort instead
 
 template <bool NUMERIC>
 __global__ void __launch_bounds__(kSpgThreads)
-spgemm_block_rows(const int *list, const Bins *bins, const long long *prod,
+spgemm_block_rows(const int *list, const unsigned *nlist, const long long *prod,
                   const int *__restrict__ Aptr, const int *__restrict__ Aind,
                   const float *__restrict__ Aval, const int *__restrict__ Bptr,
                   const int *__restrict__ Bind, const float *__restrict__ Bval, int *cnt,
@@ -266,7 +493,7 @@ spgemm_block_rows(const int *list, const Bins *bins, const long long *prod,
   __shared__ int s_off[kSpgThreads], s_bs[kSpgThreads];
   __shared__ float s_av[kSpgThreads];
   __shared__ int s_cnt;
-  const unsigned nrows = bins->n[1];
+  const unsigned nrows = *nlist;
   for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
     int i = list[r];
     int bits = table_bits(prod[i], 14);
@@ -278,7 +505,7 @@ spgemm_block_rows(const int *list, const Bins *bins, const long long *prod,
     if (threadIdx.x == 0) s_cnt = 0;
     __syncthreads();
     int fresh_count = 0;
-    for_each_product<false>(i, Aptr, Aind, Aval, Bptr, Bind, Bval, s_off, s_bs, s_av,
+    for_each_product_lbs<kSpgThreads>(i, Aptr, Aind, Aval, Bptr, Bind, Bval, s_off, s_bs, s_av,
                             [&](int j, double v) {
                               bool fresh;
                               int h = table_insert(keys, bits, j, &fresh);
@@ -347,12 +574,134 @@ spgemm_block_rows(const int *list, const Bins *bins, const long long *prod,
   }
 }
 
+// ------------------------------------------------------------- mid rows ---
+// One block of TPB threads per row, a hash table of up to 2^TBITS slots in
+// dynamic shared memory sized to the row (products for the symbolic pass,
+// the exact output size for the numeric pass, so at most half full).  The
+// numeric pass then sorts the row in shared memory: the occupied entries are
+// scattered by column range into TPB buckets (counts, a scan, atomic slots),
+// each thread insertion-sorts one bucket, and the row is written to C
+// coalesced.  A row whose fullest bucket holds more than kMidBucketMax
+// entries bitonic-sorts its table instead.  Several rows per SM are in
+// flight, which is what hides the L2 latency of gathering B's rows.
+constexpr int kMidBucketMax = 64;
+
+template <int TPB, int TBITS, bool NUMERIC>
+constexpr size_t mid_smem() {
+  return NUMERIC ? (size_t)16 << TBITS : (size_t)4 << TBITS;
+}
+
+template <bool NUMERIC, int TPB, int TBITS>
+__global__ void __launch_bounds__(TPB)
+spgemm_mid_rows(const int *list, const unsigned *nlist, const long long *prod,
+                const int *__restrict__ Aptr, const int *__restrict__ Aind,
+                const float *__restrict__ Aval, const int *__restrict__ Bptr,
+                const int *__restrict__ Bind, const float *__restrict__ Bval, int *cnt,
+                const int *Cptr, int *Cind, float *Cval, int ncols) {
+  constexpr int T = 1 << TBITS;
+  extern __shared__ __align__(16) unsigned char dyn[];
+  // numeric: vals double[T] | keys int[T] | skeys int[T/2] | svals float[T/2]
+  double *vals = NUMERIC ? (double *)dyn : nullptr;
+  int *keys = (int *)(dyn + (NUMERIC ? sizeof(double) * T : 0));
+  int *skeys = keys + T;
+  float *svals = (float *)(skeys + T / 2);
+  __shared__ int s_off[TPB], s_bs[TPB];
+  __shared__ float s_av[TPB];
+  __shared__ int s_bstart[TPB], s_bfill[TPB], sw[33];
+  __shared__ int s_cnt;
+  const int tid = threadIdx.x;
+  const unsigned nrows = *nlist;
+  for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
+    const int i = list[r];
+    const int base = NUMERIC ? Cptr[i] : 0;
+    const int n = NUMERIC ? Cptr[i + 1] - base : 0;
+    const int bits = table_bits(NUMERIC ? (long long)n : prod[i], TBITS);
+    const int Tn = 1 << bits;
+    for (int t = tid; t < Tn; t += TPB) {
+      keys[t] = kEmpty;
+      if (NUMERIC) vals[t] = 0.0;
+    }
+    s_bstart[tid] = 0;
+    s_bfill[tid] = 0;
+    if (tid == 0) s_cnt = 0;
+    __syncthreads();
+    int fresh_count = 0;
+    for_each_product_lbs<TPB>(i, Aptr, Aind, Aval, Bptr, Bind, Bval, s_off, s_bs, s_av,
+                            [&](int j, double v) {
+                              bool fresh;
+                              const int h = table_insert(keys, bits, j, &fresh);
+                              fresh_count += fresh;
+                              if (NUMERIC) atomicAdd(vals + h, v);
+                            });
+    if (!NUMERIC) {
+      const int c = warp_sum(fresh_count);
+      if (lane_id() == 0 && c) atomicAdd(&s_cnt, c);
+      __syncthreads();
+      if (tid == 0) cnt[i] = s_cnt;
+      __syncthreads();
+      continue;
+    }
+    // bucket b holds columns [b * ncols / TPB, (b + 1) * ncols / TPB)
+    for (int t = tid; t < Tn; t += TPB) {
+      const int j = keys[t];
+      if (j != kEmpty) atomicAdd(&s_bstart[(int)(((long long)j * TPB) / ncols)], 1);
+    }
+    __syncthreads();
+    const int mine = s_bstart[tid];
+    int total;
+    const int start = block_excl_scan(mine, sw, &total);
+    if (!__syncthreads_or(mine > kMidBucketMax)) {
+      s_bstart[tid] = start;
+      __syncthreads();
+      for (int t = tid; t < Tn; t += TPB) {
+        const int j = keys[t];
+        if (j == kEmpty) continue;
+        const int b = (int)(((long long)j * TPB) / ncols);
+        const int pos = s_bstart[b] + atomicAdd(&s_bfill[b], 1);
+        if (pos < T / 2) {
+          skeys[pos] = j;
+          svals[pos] = (float)vals[t];
+        }
+      }
+      __syncthreads();
+      int *ck = skeys + start;
+      float *cv = svals + start;
+      const int len = min(mine, T / 2 - start);
+      for (int a = 1; a < len; ++a) {
+        const int kj = ck[a];
+        const float kv = cv[a];
+        int b = a - 1;
+        while (b >= 0 && ck[b] > kj) {
+          ck[b + 1] = ck[b];
+          cv[b + 1] = cv[b];
+          --b;
+        }
+        ck[b + 1] = kj;
+        cv[b + 1] = kv;
+      }
+      __syncthreads();
+      const int nw = min(n, T / 2);
+      for (int t = tid; t < nw; t += TPB) {
+        Cind[base + t] = skeys[t];
+        Cval[base + t] = svals[t];
+      }
+    } else {
+      bitonic_sort<false>(keys, vals, Tn);
+      for (int t = tid; t < n && t < Tn; t += TPB) {
+        Cind[base + t] = keys[t];
+        Cval[base + t] = (float)vals[t];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // ----------------------------------------------------- dense accumulator ---
 // One block per row; each resident block owns a bitmap of n bits and n
 // doubles in global memory, cleared as the row is emitted.
 template <bool NUMERIC>
 __global__ void __launch_bounds__(kSpgThreads)
-spgemm_dense_rows(const int *list, const Bins *bins, int n,
+spgemm_dense_rows(const int *list, const unsigned *nlist, int n,
                   const int *__restrict__ Aptr, const int *__restrict__ Aind,
                   const float *__restrict__ Aval, const int *__restrict__ Bptr,
                   const int *__restrict__ Bind, const float *__restrict__ Bval,
@@ -364,10 +713,10 @@ spgemm_dense_rows(const int *list, const Bins *bins, int n,
   const int words = (n + 31) / 32;
   unsigned *bits = gbits + (size_t)blockIdx.x * words;
   double *vals = NUMERIC ? gvals + (size_t)blockIdx.x * n : nullptr;
-  const unsigned nrows = bins->n[2];
+  const unsigned nrows = *nlist;
   for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
     int i = list[r];
-    for_each_product<false>(i, Aptr, Aind, Aval, Bptr, Bind, Bval, s_off, s_bs, s_av,
+    for_each_product_lbs<kSpgThreads>(i, Aptr, Aind, Aval, Bptr, Bind, Bval, s_off, s_bs, s_av,
                             [&](int j, double v) {
                               unsigned bit = 1u << (j & 31);
                               if (!(__ldcg(bits + (j >> 5)) & bit)) atomicOr(bits + (j >> 5), bit);
@@ -397,6 +746,147 @@ spgemm_dense_rows(const int *list, const Bins *bins, int n,
     }
     if (!NUMERIC && threadIdx.x == 0) cnt[i] = run;
     __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------- bitmap rows ---
+// One block per row over a bitmap of the W = ceil(ncols / 32) words of C's
+// columns in shared memory.  MODE 0 (symbolic): set a bit per product, the
+// row's size is the popcount.  MODE 1 (numeric): set the bits, then
+// woff[w] = popcount of words [0, w) (a scan over the words), so the product
+// in column j lands at woff[j / 32] + popcount(word & bits below j) of the
+// column-ordered row; its value is added there in a double staging row of
+// scap entries in shared memory and the row is emitted word by word.  A row
+// longer than scap is done in windows of scap positions, one pass over its
+// products per window (products outside the window are skipped), so no
+// value ever goes through a global atomic.  Staging values are cleared as
+// they are emitted and the bits after the last window, so each row starts
+// clean.
+constexpr int kStageSmem = 4096;     // 512-thread numeric rows: nnz(C(i,:)) <= this
+constexpr int kStageBig = 16384;     // 1024-thread numeric rows: window of this many
+constexpr int kBitmapMaxWords = 8192;
+
+template <int MODE, int TPB>
+__global__ void __launch_bounds__(TPB, TPB <= 512 ? 2 : 1)
+spgemm_bitmap_rows(const int *list, const unsigned *nlist, int W,
+                   const int *__restrict__ Aptr, const int *__restrict__ Aind,
+                   const float *__restrict__ Aval, const int *__restrict__ Bptr,
+                   const int *__restrict__ Bind, const float *__restrict__ Bval, int *cnt,
+                   const int *Cptr, int *Cind, float *Cval, int scap) {
+  extern __shared__ __align__(16) unsigned char dyn[];
+  unsigned *bits = (unsigned *)dyn;
+  int *woff = (int *)(bits + W);
+  double *stage = (double *)(dyn + (size_t)8 * ((W + 1) & ~1));
+  __shared__ int s_off[TPB], s_bs[TPB];
+  __shared__ float s_av[TPB];
+  __shared__ int s_wt[33];
+  const int tid = threadIdx.x, lane = lane_id(), wi = warp_in_block();
+  constexpr int nw = TPB / 32;
+  for (int t = tid; t < W; t += TPB) bits[t] = 0u;
+  if (MODE == 1)
+    for (int t = tid; t < scap; t += TPB) stage[t] = 0.0;
+  __syncthreads();
+  // warp wi scans words [ws, we)
+  const int seg = ((W + nw - 1) / nw + 31) & ~31;
+  const int ws = min(W, wi * seg), we = min(W, ws + seg);
+  const unsigned nrows = *nlist;
+  for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
+    const int i = list[r];
+    for_each_product_lbs<TPB>(i, Aptr, Aind, nullptr, Bptr, Bind, nullptr, s_off, s_bs, s_av,
+                            [&](int j, double) {
+                              const unsigned bit = 1u << (j & 31);
+                              if (!(bits[j >> 5] & bit)) atomicOr(bits + (j >> 5), bit);
+                            });
+    __syncthreads();
+    if (MODE == 0) {
+      int c = 0;
+      for (int w = tid; w < W; w += TPB) {
+        c += __popc(bits[w]);
+        bits[w] = 0u;
+      }
+      c = warp_sum(c);
+      if (lane == 0) s_wt[wi] = c;
+      __syncthreads();
+      if (tid == 0) {
+        int tot = 0;
+        for (int k = 0; k < nw; ++k) tot += s_wt[k];
+        cnt[i] = tot;
+      }
+      __syncthreads();
+      continue;
+    }
+    int carry = 0;
+    for (int w0 = ws; w0 < we; w0 += 32) {
+      const int w = w0 + lane;
+      const int c = w < we ? __popc(bits[w]) : 0;
+      const int incl = warp_incl_scan(c);
+      if (w < we) woff[w] = carry + incl - c;
+      carry += __shfl_sync(kFull, incl, 31);
+    }
+    if (lane == 0) s_wt[wi] = carry;
+    __syncthreads();
+    if (wi == 0) {
+      const int x = lane < nw ? s_wt[lane] : 0;
+      const int xi = warp_incl_scan(x);
+      if (lane < nw) s_wt[lane] = xi - x;
+    }
+    __syncthreads();
+    const int add = s_wt[wi];
+    for (int w = ws + lane; w < we; w += 32) woff[w] += add;
+    __syncthreads();
+    // the row's length from the symbolic phase bounds every position (it
+    // equals the popcount unless A or B changed structure in between)
+    const int base = Cptr[i];
+    const int len = Cptr[i + 1] - base;
+    for (int p0 = 0; p0 < len; p0 += scap) {
+      const int p1 = min(len, p0 + scap);
+      for_each_product_lbs<TPB>(i, Aptr, Aind, Aval, Bptr, Bind, Bval, s_off, s_bs, s_av,
+                              [&](int j, double v) {
+                                const int w = j >> 5;
+                                const int pos =
+                                    woff[w] + __popc(bits[w] & ((1u << (j & 31)) - 1u));
+                                if (pos >= p0 && pos < p1) atomicAdd(stage + (pos - p0), v);
+                              });
+      __syncthreads();
+      for (int w = tid; w < W; w += TPB) {
+        unsigned b = bits[w];
+        int k = woff[w];
+        if (!b || k >= p1 || k + __popc(b) <= p0) continue;
+        while (b && k < p1) {
+          const int t = __ffs(b) - 1;
+          b &= b - 1;
+          if (k >= p0) {
+            Cind[base + k] = w * 32 + t;
+            Cval[base + k] = (float)stage[k - p0];
+            stage[k - p0] = 0.0;
+          }
+          ++k;
+        }
+      }
+      __syncthreads();
+    }
+    for (int w = tid; w < W; w += TPB) bits[w] = 0u;
+    __syncthreads();
+  }
+}
+
+// Re-bins the rows of the mid and block bins for the numeric phase by
+// their exact output size (cnt, from the symbolic phase).
+__global__ void rebin_rows(int m, int *lists, SpgState *st, const int *cnt, bool bitmap) {
+  const unsigned n1 = st->n[kBinMid1], n2 = st->n[kBinMid2], n3 = st->n[kBinBlock];
+  const unsigned n = n1 + n2 + n3;
+  for (unsigned r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int src = r < n1 ? kBinMid1 : (r < n1 + n2 ? kBinMid2 : kBinBlock);
+    const unsigned k = r < n1 ? r : (r < n1 + n2 ? r - n1 : r - n1 - n2);
+    const int i = lists[(size_t)src * m + k];
+    const int c = cnt[i];
+    const int b = c <= kN1MaxNnz ? kBinN1
+                  : c <= kN2MaxNnz ? kBinN2
+                  : c <= kN3MaxNnz ? kBinN3
+                  : (!bitmap || c <= kStageSmem) ? kBinN4
+                                                 : kBinN5;
+    lists[(size_t)b * m + warp_bin_slot(st->n, b)] = i;
+    if (b == kBinN5) atomicMax(&st->maxc, (unsigned)c);
   }
 }
 
@@ -443,36 +933,44 @@ int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr
   const int m = A->m, n = B->n;
   cudaStream_t st = ctx->stream;
   auto *prod = (long long *)workspace(ctx, kSlotSpgProd, sizeof(long long) * ((size_t)m + 1));
-  auto *lists = (int *)workspace(ctx, kSlotSpgLists, sizeof(int) * 3 * ((size_t)m + 1));
+  auto *lists = (int *)workspace(ctx, kSlotSpgLists, sizeof(int) * kNumBins * ((size_t)m + 1));
   auto *cnt = (int *)workspace(ctx, kSlotSpgCnt, sizeof(int) * ((size_t)m + 1));
   auto *offs = (long long *)workspace(ctx, kSlotMisc3, sizeof(long long) * ((size_t)m + 2));
-  auto *bins = (Bins *)workspace(ctx, kSlotSpgBins, sizeof(Bins) + 64);
-  if (!prod || !lists || !cnt || !offs || !bins) return APSPIE_ERR_OOM;
-  long long *d_total = (long long *)(bins + 1);
-  cudaMemsetAsync(bins, 0, sizeof(Bins), st);
+  auto *sst = (SpgState *)workspace(ctx, kSlotSpgBins, sizeof(SpgState));
+  if (!prod || !lists || !cnt || !offs || !sst) return APSPIE_ERR_OOM;
+  long long *d_total = &sst->total;
+  // block rows over a column bitmap when C's columns fit shared memory
+  const int bwords = (n + 31) / 32;
+  const bool bitmap = n > 0 && (long long)n <= ctx->spgemm_bitmap_max_cols &&
+                      bwords <= kBitmapMaxWords;
+  auto L = [&](int b) { return lists + (size_t)b * m; };
+  cudaMemsetAsync(sst, 0, sizeof(SpgState), st);
   if (m > 0) {
     row_products<<<gridsz(ctx, (long long)m * 32, 256), 256, 0, st>>>(m, A->d_ptr, A->d_ind,
                                                                       B->d_ptr, prod);
-    bin_rows<<<gridsz(ctx, m, 256), 256, 0, st>>>(m, prod, lists, bins, cnt);
+    bin_rows<<<gridsz(ctx, m, 256), 256, 0, st>>>(m, prod, lists, sst, cnt, bitmap);
     int rc = check_launch(ctx, "spgemm bin", 2);
     if (rc) return rc;
   }
-  Bins hb;
+  SpgState hb{};
   {
-    auto *h = (Bins *)pinned(ctx, sizeof(Bins));
+    auto *h = (SpgState *)pinned(ctx, sizeof(SpgState));
     if (!h) return APSPIE_ERR_OOM;
-    cudaMemcpyAsync(h, bins, sizeof(Bins), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h, sst, sizeof(SpgState), cudaMemcpyDeviceToHost, st);
     int rc = check_cuda(ctx, cudaStreamSynchronize(st), "spgemm bins");
     if (rc) return rc;
     hb = *h;
   }
-  const size_t dyn_num = sizeof(double) * kBlockTable + sizeof(int) * kBlockTable;
   const size_t dyn_sym = sizeof(int) * kBlockTable;
-  cudaFuncSetAttribute(spgemm_block_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)dyn_num);
   cudaFuncSetAttribute(spgemm_block_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)dyn_sym);
-  const int dense_blocks = (int)std::min<unsigned>(hb.n[2], (unsigned)ctx->num_sms * 2);
+  cudaFuncSetAttribute(spgemm_bitmap_rows<0, kSpgThreads>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * kBitmapMaxWords));
+  cudaFuncSetAttribute(spgemm_mid_rows<false, 256, 13>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)mid_smem<256, 13, false>());
+  const unsigned nd = hb.n[kBinDense];
+  const int dense_blocks = (int)std::min<unsigned>(nd, (unsigned)ctx->num_sms * 2);
   const int words = (n + 31) / 32;
   unsigned *gbits = nullptr;
   double *gvals = nullptr;
@@ -485,23 +983,49 @@ int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr
     zero_doubles<<<gridsz(ctx, (long long)n * dense_blocks, 256), 256, 0, st>>>(
         (size_t)n * dense_blocks, gvals);
   }
-  // bin b's rows are lists[b * m ...] (bin_rows)
-  const int *l0 = lists, *l1 = lists + (size_t)m, *l2 = lists + 2 * (size_t)m;
   // ---- symbolic ----
-  if (hb.n[0])
-    spgemm_warp_rows<false><<<gridsz(ctx, hb.n[0], kWarpsPerBlockSmall, 64),
+  const unsigned *nb = sst->n;
+  int launches = 0;
+  if (hb.n[kBinWarp]) {
+    spgemm_warp_rows<false><<<gridsz(ctx, hb.n[kBinWarp], kWarpsPerBlockSmall, 64),
                               32 * kWarpsPerBlockSmall, 0, st>>>(
-        l0, bins, prod, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind, nullptr, cnt, nullptr,
-        nullptr, nullptr);
-  if (hb.n[1])
-    spgemm_block_rows<false><<<gridsz(ctx, hb.n[1], 1, 4), kSpgThreads, dyn_sym, st>>>(
-        l1, bins, prod, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind, nullptr, cnt, nullptr,
-        nullptr, nullptr, n);
-  if (hb.n[2])
+        L(kBinWarp), nb + kBinWarp, prod, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind,
+        nullptr, cnt, nullptr, nullptr, nullptr);
+    ++launches;
+  }
+  if (hb.n[kBinMid1]) {
+    spgemm_mid_rows<false, 128, 11><<<gridsz(ctx, hb.n[kBinMid1], 1, 16), 128,
+                                      mid_smem<128, 11, false>(), st>>>(
+        L(kBinMid1), nb + kBinMid1, prod, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind,
+        nullptr, cnt, nullptr, nullptr, nullptr, n);
+    ++launches;
+  }
+  if (hb.n[kBinMid2]) {
+    spgemm_mid_rows<false, 256, 13><<<gridsz(ctx, hb.n[kBinMid2], 1, 6), 256,
+                                      mid_smem<256, 13, false>(), st>>>(
+        L(kBinMid2), nb + kBinMid2, prod, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind,
+        nullptr, cnt, nullptr, nullptr, nullptr, n);
+    ++launches;
+  }
+  if (hb.n[kBinBlock] && bitmap) {
+    spgemm_bitmap_rows<0, kSpgThreads><<<gridsz(ctx, hb.n[kBinBlock], 1, 4), kSpgThreads,
+                                         (size_t)4 * bwords, st>>>(
+        L(kBinBlock), nb + kBinBlock, bwords, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind,
+        nullptr, cnt, nullptr, nullptr, nullptr, 0);
+    ++launches;
+  } else if (hb.n[kBinBlock]) {
+    spgemm_block_rows<false><<<gridsz(ctx, hb.n[kBinBlock], 1, 4), kSpgThreads, dyn_sym, st>>>(
+        L(kBinBlock), nb + kBinBlock, prod, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind,
+        nullptr, cnt, nullptr, nullptr, nullptr, n);
+    ++launches;
+  }
+  if (nd) {
     spgemm_dense_rows<false><<<dense_blocks, kSpgThreads, 0, st>>>(
-        l2, bins, n, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind, nullptr, gbits, gvals, cnt,
-        nullptr, nullptr, nullptr);
-  int rc = check_launch(ctx, "spgemm symbolic", 3);
+        L(kBinDense), nb + kBinDense, n, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind, nullptr,
+        gbits, gvals, cnt, nullptr, nullptr, nullptr);
+    ++launches;
+  }
+  int rc = check_launch(ctx, "spgemm symbolic", launches);
   if (rc) return rc;
   // ---- row offsets ----
   if (m > 0) {
@@ -511,16 +1035,22 @@ int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr
     rc = device_exclusive_scan<long long>(ctx, offs, offs, m, d_total);
     if (rc) return rc;
   }
+  const unsigned nre = hb.n[kBinMid1] + hb.n[kBinMid2] + hb.n[kBinBlock];
+  if (nre) {
+    rebin_rows<<<gridsz(ctx, nre, 256), 256, 0, st>>>(m, lists, sst, cnt, bitmap);
+    rc = check_launch(ctx, "rebin_rows");
+    if (rc) return rc;
+  }
   long long nnzC = 0;
-  {
-    auto *h = (long long *)pinned(ctx, sizeof(long long));
+  SpgState hs{};
+  if (m > 0) {
+    auto *h = (SpgState *)pinned(ctx, sizeof(SpgState));
     if (!h) return APSPIE_ERR_OOM;
-    if (m > 0) {
-      cudaMemcpyAsync(h, d_total, sizeof(long long), cudaMemcpyDeviceToHost, st);
-      rc = check_cuda(ctx, cudaStreamSynchronize(st), "spgemm nnz");
-      if (rc) return rc;
-      nnzC = *h;
-    }
+    cudaMemcpyAsync(h, sst, sizeof(SpgState), cudaMemcpyDeviceToHost, st);
+    rc = check_cuda(ctx, cudaStreamSynchronize(st), "spgemm nnz");
+    if (rc) return rc;
+    hs = *h;
+    nnzC = hs.total;
   }
   if (nnzC >= (long long)INT32_MAX)
     return set_error(ctx, APSPIE_ERR_OVERFLOW, "apspie_spgemm: nnz(C) = %lld exceeds int32",
@@ -534,14 +1064,16 @@ int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr
   }
   rc = check_launch(ctx, "to_int32_offsets");
   if (rc) return rc;
-  // the bins, lists, counts and dense accumulators stay in the workspace for
-  // the numeric phase
+  // the lists, counts and dense accumulators stay in the workspace for the
+  // numeric phase
   ctx->spgemm_plan_valid = true;
   ctx->spgemm_plan_A = A->d_ptr;
   ctx->spgemm_plan_B = B->d_ptr;
   ctx->spgemm_plan_m = m;
   ctx->spgemm_plan_n = n;
-  for (int b = 0; b < 3; ++b) ctx->spgemm_plan_bins[b] = hb.n[b];
+  for (int b = 0; b < kNumBins; ++b) ctx->spgemm_plan_bins[b] = hs.n[b];
+  ctx->spgemm_plan_bins[kNumBins] = hs.maxc;
+  ctx->spgemm_plan_words = bitmap ? bwords : 0;
   *h_nnz = nnzC;
   return APSPIE_OK;
 }
@@ -555,17 +1087,30 @@ int apspie_spgemm_numeric(apspie_ctx ctx, const apspie_csr *A, const apspie_csr 
                      "apspie_spgemm_numeric: no matching apspie_spgemm_symbolic before it");
   const int m = A->m, n = B->n;
   cudaStream_t st = ctx->stream;
-  Bins hb;
-  for (int b = 0; b < 3; ++b) hb.n[b] = ctx->spgemm_plan_bins[b];
+  const unsigned *hn = ctx->spgemm_plan_bins;
+  const int maxc = (int)hn[kNumBins];
+  const int bwords = ctx->spgemm_plan_words;
   // the symbolic phase's buffers (own slots, same sizes: no reallocation;
   // the dense accumulators are left cleared by every dense-row pass)
   auto *prod = (long long *)workspace(ctx, kSlotSpgProd, sizeof(long long) * ((size_t)m + 1));
-  auto *lists = (int *)workspace(ctx, kSlotSpgLists, sizeof(int) * 3 * ((size_t)m + 1));
+  auto *lists = (int *)workspace(ctx, kSlotSpgLists, sizeof(int) * kNumBins * ((size_t)m + 1));
   auto *cnt = (int *)workspace(ctx, kSlotSpgCnt, sizeof(int) * ((size_t)m + 1));
-  auto *bins = (Bins *)workspace(ctx, kSlotSpgBins, sizeof(Bins) + 64);
-  if (!prod || !lists || !cnt || !bins) return APSPIE_ERR_OOM;
+  auto *sst = (SpgState *)workspace(ctx, kSlotSpgBins, sizeof(SpgState));
+  if (!prod || !lists || !cnt || !sst) return APSPIE_ERR_OOM;
+  auto L = [&](int b) { return lists + (size_t)b * m; };
+  const unsigned *nb = sst->n;
   const size_t dyn_num = sizeof(double) * kBlockTable + sizeof(int) * kBlockTable;
-  const int dense_blocks = (int)std::min<unsigned>(hb.n[2], (unsigned)ctx->num_sms * 2);
+  cudaFuncSetAttribute(spgemm_block_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)dyn_num);
+  cudaFuncSetAttribute(spgemm_bitmap_rows<1, kSpgThreads>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(8 * kBitmapMaxWords + 8 * kStageSmem + 16));
+  cudaFuncSetAttribute(spgemm_bitmap_rows<1, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(8 * kBitmapMaxWords + 8 * kStageBig + 16));
+  cudaFuncSetAttribute(spgemm_mid_rows<true, 256, 12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)mid_smem<256, 12, true>());
+  const unsigned nd = hn[kBinDense];
+  const int dense_blocks = (int)std::min<unsigned>(nd, (unsigned)ctx->num_sms * 2);
   const int words = (n + 31) / 32;
   unsigned *gbits = nullptr;
   double *gvals = nullptr;
@@ -574,26 +1119,67 @@ int apspie_spgemm_numeric(apspie_ctx ctx, const apspie_csr *A, const apspie_csr 
     gvals = (double *)workspace(ctx, kSlotSpgVals, sizeof(double) * (size_t)n * dense_blocks);
     if (!gbits || !gvals) return APSPIE_ERR_OOM;
   }
-  const int *l0 = lists, *l1 = lists + (size_t)m, *l2 = lists + 2 * (size_t)m;
   const int *Cptr = d_Cptr;
   int *Cind = d_Cind;
   float *Cval = d_Cval;
-  int rc;
+  int launches = 0;
   // ---- numeric ----
-  if (hb.n[0])
-    spgemm_warp_rows<true><<<gridsz(ctx, hb.n[0], kWarpsPerBlockSmall, 32),
+  if (hn[kBinWarp]) {
+    spgemm_warp_rows<true><<<gridsz(ctx, hn[kBinWarp], kWarpsPerBlockSmall, 32),
                              32 * kWarpsPerBlockSmall, 0, st>>>(
-        l0, bins, prod, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind, B->d_val, cnt, Cptr,
-        Cind, Cval);
-  if (hb.n[1])
-    spgemm_block_rows<true><<<gridsz(ctx, hb.n[1], 1, 1), kSpgThreads, dyn_num, st>>>(
-        l1, bins, prod, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind, B->d_val, cnt, Cptr,
-        Cind, Cval, n);
-  if (hb.n[2])
+        L(kBinWarp), nb + kBinWarp, prod, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
+        B->d_val, cnt, Cptr, Cind, Cval);
+    ++launches;
+  }
+  if (hn[kBinN1]) {
+    spgemm_mid_rows<true, 128, 10><<<gridsz(ctx, hn[kBinN1], 1, 12), 128,
+                                     mid_smem<128, 10, true>(), st>>>(
+        L(kBinN1), nb + kBinN1, prod, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
+        B->d_val, cnt, Cptr, Cind, Cval, n);
+    ++launches;
+  }
+  if (hn[kBinN2]) {
+    spgemm_mid_rows<true, 128, 11><<<gridsz(ctx, hn[kBinN2], 1, 6), 128,
+                                     mid_smem<128, 11, true>(), st>>>(
+        L(kBinN2), nb + kBinN2, prod, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
+        B->d_val, cnt, Cptr, Cind, Cval, n);
+    ++launches;
+  }
+  if (hn[kBinN3]) {
+    spgemm_mid_rows<true, 256, 12><<<gridsz(ctx, hn[kBinN3], 1, 3), 256,
+                                     mid_smem<256, 12, true>(), st>>>(
+        L(kBinN3), nb + kBinN3, prod, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
+        B->d_val, cnt, Cptr, Cind, Cval, n);
+    ++launches;
+  }
+  if (hn[kBinN4] && bwords) {
+    spgemm_bitmap_rows<1, kSpgThreads><<<gridsz(ctx, hn[kBinN4], 1, 2), kSpgThreads,
+                                         (size_t)8 * ((bwords + 1) & ~1) + 8 * kStageSmem, st>>>(
+        L(kBinN4), nb + kBinN4, bwords, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
+        B->d_val, cnt, Cptr, Cind, Cval, kStageSmem);
+    ++launches;
+  } else if (hn[kBinN4]) {
+    spgemm_block_rows<true><<<gridsz(ctx, hn[kBinN4], 1, 1), kSpgThreads, dyn_num, st>>>(
+        L(kBinN4), nb + kBinN4, prod, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
+        B->d_val, cnt, Cptr, Cind, Cval, n);
+    ++launches;
+  }
+  if (hn[kBinN5]) {
+    // rows longer than kStageSmem: 1024 threads, windows of kStageBig
+    const int scap = std::min(kStageBig, std::max(maxc, 1));
+    spgemm_bitmap_rows<1, 1024><<<gridsz(ctx, hn[kBinN5], 1, 1), 1024,
+                                  (size_t)8 * ((bwords + 1) & ~1) + 8 * (size_t)scap, st>>>(
+        L(kBinN5), nb + kBinN5, bwords, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
+        B->d_val, cnt, Cptr, Cind, Cval, scap);
+    ++launches;
+  }
+  if (nd) {
     spgemm_dense_rows<true><<<dense_blocks, kSpgThreads, 0, st>>>(
-        l2, bins, n, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind, B->d_val, gbits, gvals,
-        cnt, Cptr, Cind, Cval);
-  return check_launch(ctx, "spgemm numeric", 3);
+        L(kBinDense), nb + kBinDense, n, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
+        B->d_val, gbits, gvals, cnt, Cptr, Cind, Cval);
+    ++launches;
+  }
+  return check_launch(ctx, "spgemm numeric", launches);
 }
 
 int apspie_spgemm(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B, apspie_csr *C) {

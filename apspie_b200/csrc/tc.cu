@@ -117,7 +117,31 @@ __device__ __forceinline__ void for_each_wedge_in(int a0, int a1, const int *__r
     s_bs[tid] = bs;
     if (WARP) __syncwarp(); else __syncthreads();
     const int n_a = min(width, a1 - c0);
-    // the k owning wedge p: a thread's p grows by `width` per step, so its
+    if (!WARP) {
+      // block: runs of vt consecutive wedges per thread (vt grows with the
+      // chunk's wedges, up to 8): one binary search for the run's first
+      // owner (the largest t with s_off[t] <= p), then a linear walk
+      const int vt = max(1, min(8, total / width));
+      for (int p0 = tid * vt; p0 < total; p0 += width * vt) {
+        int lo = 0, hi = n_a - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (s_off[mid] <= p0) lo = mid; else hi = mid - 1;
+        }
+        int nxt = lo + 1 < n_a ? s_off[lo + 1] : INT_MAX;
+        const int pend = min(p0 + vt, total);
+        for (int p = p0; p < pend; ++p) {
+          while (p >= nxt) {
+            ++lo;
+            nxt = lo + 1 < n_a ? s_off[lo + 1] : INT_MAX;
+          }
+          visit(__ldg(Li + s_bs[lo] + (p - s_off[lo])));
+        }
+      }
+      __syncthreads();
+      continue;
+    }
+    // warp: the k owning wedge p; a lane's p grows by 32 per step, so its
     // owner only moves forward -- gallop from the previous one
     int lo = 0;
     for (int p = tid; p < total; p += width) {
@@ -374,13 +398,21 @@ int apspie_tc(apspie_ctx ctx, int m, int64_t lnnz, const int *d_Lptr, const int 
   cudaMemsetAsync(bins, 0, sizeof(TcBins), st);
   tc_bin<<<tgrid(ctx, m, 256), 256, 0, st>>>(m, d_Lptr, lists, units, bins);
   tc_warp_rows<<<ctx->num_sms * 16, 32 * kTcWarps, 0, st>>>(lists, bins, d_Lptr, d_Lind);
+  // every resident block: the units are L2-latency bound, so occupancy is
+  // what hides the latency (the bitmap's shared memory sets the limit)
   if (m <= kTcBitmapMaxVerts) {
     const int smem = (int)(sizeof(unsigned) * (size_t)((m + 31) / 32));
     cudaFuncSetAttribute(tc_units<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    tc_units<0><<<ctx->num_sms * 2, kTcThreads, smem, st>>>(units, bins, m, d_Lptr, d_Lind);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc_units<0>, kTcThreads, smem);
+    tc_units<0><<<ctx->num_sms * std::max(1, per_sm), kTcThreads, smem, st>>>(units, bins, m,
+                                                                              d_Lptr, d_Lind);
   } else {
     const int smem = (int)(sizeof(int) * kTcBlockTable);
-    tc_units<1><<<ctx->num_sms * 4, kTcThreads, smem, st>>>(units, bins, m, d_Lptr, d_Lind);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc_units<1>, kTcThreads, smem);
+    tc_units<1><<<ctx->num_sms * std::max(1, per_sm), kTcThreads, smem, st>>>(units, bins, m,
+                                                                              d_Lptr, d_Lind);
   }
   int rc = check_launch(ctx, "apspie_tc", 3);
   if (rc) return rc;

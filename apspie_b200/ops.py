@@ -293,6 +293,13 @@ def spgemm_symbolic(ctx: Context, A, B):
     return ptr, int(nnz.value)
 
 
+def spgemm_set_params(ctx: Context, bitmap_max_cols: int = 1 << 18):
+    """Rows with more than 256 products use a shared-memory column bitmap
+    when B has at most bitmap_max_cols columns (0: always hash tables)."""
+    check(lib.apspie_spgemm_set_params(ctx.handle, int(bitmap_max_cols)), ctx.handle,
+          "apspie_spgemm_set_params")
+
+
 def spgemm_numeric(ctx: Context, A, B, ptr, ind, val):
     """Numeric phase of C = A * B into caller buffers ind / val (nnz(C)
     entries each), stream-ordered, no synchronisation."""

@@ -429,6 +429,12 @@ int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr
                            int *d_Cptr, int64_t *h_nnz);
 int apspie_spgemm_numeric(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B,
                           const int *d_Cptr, int *d_Cind, float *d_Cval);
+/* Rows of A with more than 256 products are accumulated over a
+ * shared-memory bitmap of C's columns (one bit per column of B, the
+ * position of each product in the column-ordered row is a prefix popcount)
+ * when B has at most bitmap_max_cols columns (default 262144, limited to
+ * 262144 by shared memory; 0 = always the hash tables). */
+int apspie_spgemm_set_params(apspie_ctx ctx, int64_t bitmap_max_cols);
 int apspie_csr_free(apspie_ctx ctx, apspie_csr *C);
 /* Stream-ordered device-to-device copy of a library-owned CSR into caller
  * buffers (m + 1 offsets, nnz indices, nnz values; d_ind / d_val may be

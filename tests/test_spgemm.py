@@ -64,14 +64,23 @@ def test_spgemm_keeps_cancellation(ctx):
     assert cp.tolist() == [0, 1] and ci.tolist() == [0] and cv.tolist() == [0.0]
 
 
-def test_spgemm_all_bins_rectangular(ctx):
-    """Power-law rows reach the warp, block and dense-accumulator bins."""
+@pytest.mark.parametrize("bitmap", [True, False])
+def test_spgemm_all_bins_rectangular(ctx, bitmap):
+    """Power-law rows reach the warp, block and dense-accumulator bins (hash
+    tables) or the warp and both bitmap bins (output rows up to 4096 staged
+    in shared memory, larger ones in global memory)."""
     import apspie_b200 as ap
     A = ap.gen_powerlaw(1 << 12, 1 << 11, max_deg=1024, seed=2)
-    B = ap.gen_powerlaw(1 << 11, 1 << 12, max_deg=1024, seed=3)
+    B = ap.gen_powerlaw(1 << 11, 1 << 14, max_deg=1024, seed=3)
     prod = np.array([B.degrees()[A.ind[A.ptr[i]:A.ptr[i + 1]]].sum() for i in range(A.m)])
     assert (prod <= 256).any() and ((prod > 256) & (prod <= 8192)).any() and (prod > 8192).any()
-    _check_product(ctx, A, B)
+    ap.spgemm_set_params(ctx, 1 << 18 if bitmap else 0)
+    try:
+        nnz_rows = np.diff(oracle.spgemm(A.m, B.ncols, A.ptr, A.ind, None, B.ptr, B.ind, None)[0])
+        assert (nnz_rows > 4096).any()
+        _check_product(ctx, A, B)
+    finally:
+        ap.spgemm_set_params(ctx)
 
 
 def test_spgemm_two_phase_reuse(ctx):
