@@ -792,7 +792,9 @@ spgemm_bitmap_rows(const int *list, const unsigned *nlist, int W,
   const unsigned nrows = *nlist;
   for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
     const int i = list[r];
-    for_each_product_lbs<TPB>(i, Aptr, Aind, nullptr, Bptr, Bind, nullptr, s_off, s_bs, s_av,
+    // bits only: runs of consecutive products per thread measured faster
+    // here than the load-balanced search (one array of B per product)
+    for_each_product<false, true>(i, Aptr, Aind, nullptr, Bptr, Bind, nullptr, s_off, s_bs, s_av,
                             [&](int j, double) {
                               const unsigned bit = 1u << (j & 31);
                               if (!(bits[j >> 5] & bit)) atomicOr(bits + (j >> 5), bit);
