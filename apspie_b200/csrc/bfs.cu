@@ -54,11 +54,16 @@ struct BfsState {
   // reading those to choose the direction while faster ones already append.
   // Two sets, by level parity; block 0 clears the other one each level.
   LevelCounters comp[2];
-  alignas(8) unsigned bar[2];  // grid-barrier arrival counter (64-bit)
+  alignas(8) unsigned bar[2];  // grid-barrier arrival counter (64-bit), separate init
   int err;
   int levels;
   int pull_levels;
-  int pad;
+  int par;  // counter set of the last launch with the initialisation fused in
+  // Launches that clear the state themselves alternate between two barrier
+  // counters and error words: a launch resets the set the next one will use
+  // (the previous launch on the stream has finished, so nobody polls it).
+  alignas(8) unsigned barp[2][2];
+  int errp[2];
   unsigned long long reached;
   unsigned long long edges;
   unsigned long long t_start;
@@ -85,8 +90,13 @@ struct BfsVisit {
   }
 };
 
-__global__ void bfs_init(int m, int src, int32_t *depth, const int *__restrict__ ptr,
-                         int *queue, int2 *chunks, BfsState *st) {
+// Clears the depths (the source at 0) and, in block 0, seeds the level-0
+// frontier and resets the counters and the trace.  With reset_bar the
+// separate barrier counter and error word too (bfs_init only: a fused
+// launch polls its own counter set, see BfsState::barp).
+__device__ __forceinline__ void bfs_clear(int m, int src, int32_t *depth,
+                                          const int *__restrict__ ptr, int *queue, int2 *chunks,
+                                          BfsState *st, bool reset_bar) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < m; v += gridDim.x * blockDim.x)
     depth[v] = (v == src) ? 0 : -1;
   if (blockIdx.x == 0) {
@@ -96,7 +106,7 @@ __global__ void bfs_init(int m, int src, int32_t *depth, const int *__restrict__
       st->c[2] = LevelCounters{0ull, 0, 0, 0ull};
       st->comp[0] = LevelCounters{0ull, 0, 0, 0ull};
       st->comp[1] = LevelCounters{0ull, 0, 0, 0ull};
-      st->bar[0] = st->bar[1] = 0;
+      if (reset_bar) st->bar[0] = st->bar[1] = 0;
       st->err = 0;
       st->levels = 0;
       st->pull_levels = 0;
@@ -112,11 +122,17 @@ __global__ void bfs_init(int m, int src, int32_t *depth, const int *__restrict__
   }
 }
 
+__global__ void bfs_init(int m, int src, int32_t *depth, const int *__restrict__ ptr,
+                         int *queue, int2 *chunks, BfsState *st) {
+  bfs_clear(m, src, depth, ptr, queue, chunks, st, true);
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->par = -1;
+}
+
 __global__ void __launch_bounds__(kBfsThreads, 3)
 bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__restrict__ ind,
                const int *__restrict__ tptr, const int *__restrict__ tind, int32_t *depth,
                int *qa, int *qb, int2 *ca, int2 *cb, BfsState *st, int max_levels, int alpha,
-               int beta, int mode, unsigned *gmask) {
+               int beta, int mode, unsigned *gmask, int src, int init_par) {
   const int lane = lane_id();
   const int warp = warp_in_block();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -129,6 +145,19 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
   __shared__ unsigned long long s_bedg;
   __shared__ unsigned s_next;  // per-block group counter of pull / compaction sweeps
 
+  // init_par >= 0: the launch clears the state itself (no bfs_init before
+  // it) and uses barrier counter set init_par
+  unsigned *bar = init_par < 0 ? st->bar : st->barp[init_par];
+  int *err = init_par < 0 ? &st->err : &st->errp[init_par];
+  if (init_par >= 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      *reinterpret_cast<unsigned long long *>(st->barp[init_par ^ 1]) = 0ull;
+      st->errp[init_par ^ 1] = 0;
+      st->par = init_par;
+    }
+    bfs_clear(m, src, depth, ptr, qa, ca, st, false);
+    if (!grid_barrier(bar, err)) return;
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) st->t_start = globaltimer();
   bool pull = false;
   int pull_levels = 0;
@@ -184,10 +213,13 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
 
     if (!pull) {
       if (nimpl) {
-        // the frontier came from a pull level and exists only as depth == L:
-        // queue it (and chunk its hubs) before expanding.  Each block scans
-        // its own range of 32-vertex groups, kScanUnroll groups per load
-        // batch, taken from a shared counter.
+        // the frontier came from a pull level and exists only implicitly:
+        // queue it (and chunk its hubs) before expanding.  That pull level
+        // left one found-mask word per 32-vertex group (gmask), so this reads
+        // m / 8 bytes rather than the depth array.  Each block takes its own
+        // range of groups, 32 groups per warp batch from a shared counter;
+        // each round every lane with bits left hands one vertex to the
+        // warp's append.
         const unsigned ngroups = (unsigned)((m + 31) / 32);
         const unsigned per_block = (ngroups + gridDim.x - 1) / gridDim.x;
         const unsigned gbeg = blockIdx.x * per_block;
@@ -195,31 +227,23 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
         DiscoverAcc acc;
         for (;;) {
           unsigned g0 = 0;
-          if (lane == 0) g0 = atomicAdd(&s_next, (unsigned)kScanUnroll);
+          if (lane == 0) g0 = atomicAdd(&s_next, 32u);
           g0 = __shfl_sync(kFull, g0, 0);
           if (gbeg + g0 >= gend) break;
-          int dv[kScanUnroll];
-#pragma unroll
-          for (int i = 0; i < kScanUnroll; ++i) {
-            unsigned g = gbeg + g0 + i;
-            int v = (int)(g * 32u) + lane;
-            dv[i] = (g < gend && v < m) ? __ldcg(depth + v) : -1;
-          }
-#pragma unroll
-          for (int i = 0; i < kScanUnroll; ++i) {
-            int v = (int)((gbeg + g0 + i) * 32u) + lane;
-            bool f[1] = {dv[i] == L};
-            int u[1] = {v};
-            unsigned fm = __ballot_sync(kFull, f[0]);
-            if (fm) {
-              discover_n<1, false>(f, u, ptr, qin, cin, &st->comp[L & 1], acc);
-              if (lane == 0 && L < kTraceLevels)
-                atomicAdd(&st->trace[L].queued, (unsigned long long)__popc(fm));
-            }
+          const unsigned gw = gbeg + g0 + lane;
+          unsigned bits = gw < gend ? __ldcg(gmask + gw) : 0u;
+          unsigned fm;
+          while ((fm = __ballot_sync(kFull, bits != 0u)) != 0u) {
+            bool f[1] = {bits != 0u};
+            int u[1] = {f[0] ? (int)(gw * 32u) + __ffs(bits) - 1 : 0};
+            bits &= bits - 1u;
+            discover_n<1, false>(f, u, ptr, qin, cin, &st->comp[L & 1], acc);
+            if (lane == 0 && L < kTraceLevels)
+              atomicAdd(&st->trace[L].queued, (unsigned long long)__popc(fm));
           }
         }
         flush_acc(acc, &st->comp[L & 1]);
-        if (!grid_barrier(st->bar, &st->err)) return;
+        if (!grid_barrier(bar, err)) return;
         if (threadIdx.x == 0) {
           const unsigned long long bc = __ldcg(&st->comp[L & 1].bc);
           s_q = __ldcg(&st->comp[L & 1].q);
@@ -327,10 +351,11 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
           U = __ballot_sync(kFull, mine && !found && s < e);
         }
         if (found) depth[v] = next;
-        if (append) {
-          const unsigned fw = __ballot_sync(kFull, found);
-          if (lane == 0) gmask[g] = fw;
-        } else if (found) {
+        // the found-mask of every group, also when the discoveries are only
+        // counted: a push level after this one rebuilds its queue from it
+        const unsigned fw = __ballot_sync(kFull, found);
+        if (lane == 0) gmask[g] = fw;
+        if (!append && found) {
           ++cnt;
           edg += (unsigned long long)(__ldg(ptr + v + 1) - __ldg(ptr + v));
         }
@@ -386,7 +411,7 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
       st->trace[L].nf = nf;
       st->trace[L].mf = mf;
     }
-    if (!grid_barrier(st->bar, &st->err)) return;
+    if (!grid_barrier(bar, err)) return;
     if (blockIdx.x == 0 && threadIdx.x == 0 && L < kTraceLevels) st->trace[L].t_end = globaltimer();
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -442,19 +467,26 @@ int apspie_bfs(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
   int grid = clamp_grid(ctx, bfs_grid(ctx));
   if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_bfs: occupancy query failed");
 
-  int init_grid = std::min((m + 255) / 256, ctx->num_sms * 8);
-  bfs_init<<<init_grid, 256, 0, ctx->stream>>>(m, src, d_depth, d_ptr, qa, ca, st);
-  int rc = check_launch(ctx, "bfs_init");
-  if (rc) return rc;
+  // the kernel clears the depths and its state itself (one grid barrier
+  // instead of a separate launch); a state buffer it has not seen yet is
+  // zeroed once, so both barrier counter sets start at 0
+  if (ctx->bfs_state_zeroed != st) {
+    cudaError_t ez = cudaMemsetAsync(st, 0, sizeof(BfsState), ctx->stream);
+    if (ez != cudaSuccess) return check_cuda(ctx, ez, "apspie_bfs: state");
+    ctx->bfs_state_zeroed = st;
+    ctx->bfs_par = 0;
+  }
   long long nnz_ll = (long long)nnz;
   int alpha = ctx->bfs_alpha, beta = ctx->bfs_beta, mode = ctx->bfs_mode;
   if (!d_tptr) mode = 1;  // no in-adjacency: push only
+  int par = ctx->bfs_par;
   void *args[] = {&m,  &nnz_ll, (void *)&d_ptr, (void *)&d_ind, (void *)&d_tptr, (void *)&d_tind,
                   &d_depth, &qa, &qb, &ca, &cb, &st, &max_levels, &alpha, &beta, &mode,
-                  &gmask};
+                  &gmask, &src, &par};
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)bfs_persistent, dim3(grid),
                                               dim3(kBfsThreads), args, 0, ctx->stream);
   if (e != cudaSuccess) return check_cuda(ctx, e, "bfs_persistent");
+  ctx->bfs_par ^= 1;
   ctx->launches += 1;
   return APSPIE_OK;
 }
@@ -473,9 +505,10 @@ int apspie_bfs_get_stats(apspie_ctx ctx, apspie_bfs_stats *out) {
   out->pull_levels = h->pull_levels;
   out->vertices_reached = (int64_t)h->reached;
   out->edges_traversed = (int64_t)h->edges;
-  if (h->err)
+  const int kerr = h->err ? h->err : (h->par >= 0 && h->par < 2 ? h->errp[h->par] : 0);
+  if (kerr)
     return set_error(ctx, APSPIE_ERR_TIMEOUT, "apspie_bfs: grid barrier timed out (status %d)",
-                     h->err);
+                     kerr);
   return APSPIE_OK;
 }
 
@@ -617,9 +650,10 @@ extern "C" int apspie_bfs_noalloc(void *stream, int src, int64_t nnz, int m, con
   if (cudaGetLastError() != cudaSuccess) return APSPIE_ERR_CUDA;
   long long nnz_ll = (long long)nnz;
   int alpha = 14, beta = 24, mode = d_tptr ? 0 : 1;
+  int no_fused = -1;
   void *args[] = {&m,  &nnz_ll, (void *)&d_ptr, (void *)&d_ind, (void *)&d_tptr, (void *)&d_tind,
                   &d_depth, &qa, &qb, &ca, &cb, &state, &max_levels, &alpha, &beta, &mode,
-                  &gmask};
+                  &gmask, &src, &no_fused};
   if (cudaLaunchCooperativeKernel((const void *)bfs_persistent, dim3(grid), dim3(kBfsThreads), args,
                                   0, st) != cudaSuccess) {
     cudaGetLastError();

@@ -38,6 +38,8 @@ struct apspie_context {
   int bfs_beta = 24;
   int bfs_mode = 0;  // 0 auto, 1 push only, 2 pull only
   void *bfs_state = nullptr;  // device pointer into a workspace slot
+  void *bfs_state_zeroed = nullptr;  // BFS state buffer zeroed once for the fused init
+  int bfs_par = 0;                   // barrier counter set of the next BFS launch
   void *sssp_state = nullptr;
   // SSSP near-far step (0: frontier Bellman-Ford)
   uint32_t sssp_delta_u32 = 0;
