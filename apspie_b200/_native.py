@@ -101,6 +101,7 @@ PROTOS: dict[str, tuple] = {
     "apspie_tc": (c_int, [vp, c_int, c_i64, vp, vp, P_i64]),
     "apspie_batch_run": (c_int, [vp, c_int, C.POINTER(Job), c_int]),
     "apspie_batch_set_params": (c_int, [vp, c_int]),
+    "apspie_batch_set_deep_mode": (c_int, [vp, c_int]),
     "apspie_batch_get_stats": (c_int, [vp, C.POINTER(BatchStats)]),
     "apspie_autotune_bfs": (c_int, [vp, c_int, P_int, c_i64, c_int, vp, vp, vp, vp, vp, P_int,
                                     P_int, C.POINTER(C.c_float)]),

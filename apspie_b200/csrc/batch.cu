@@ -774,6 +774,94 @@ size_t job_chunk_capacity(long long nnz, bool bfs) {
   return (size_t)(nnz / ck + nnz / bd + 2);
 }
 
+// The deep jobs' sources as single-source traversals, spread over up to
+// batch_deep_subs sub-contexts (each its own stream and workspace) and run
+// concurrently next to whatever is already queued on the context's stream
+// (which waits for them at the end).  Sources go to the least loaded
+// sub-context, SSSP first; each traversal gets budget / K blocks.  SSSP
+// runs near-far (the context's step, else kDeepDelta): on a deep weighted
+// graph frontier Bellman-Ford re-relaxes every edge dozens of times (211 M
+// relaxations for 4.2 M edges on the 1024 x 1024 grid, weights 1..255),
+// which needs a large grid per source, while near-far does 7 M over 40 %
+// more rounds and runs on a few blocks.  Results are written straight into
+// the caller's rows.
+constexpr unsigned kDeepDelta = 1024;
+int ensure_subs(apspie_context *ctx, int k) {
+  while ((int)ctx->subs.size() < k) {
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+      if (s) cudaStreamDestroy(s);
+      return check_cuda(ctx, cudaGetLastError(), "apspie_batch_run: sub-context stream");
+    }
+    apspie_ctx sub = nullptr;
+    int rc = apspie_ctx_create(ctx->device, s, &sub);
+    if (rc) {
+      cudaStreamDestroy(s);
+      cudaEventDestroy(ev);
+      return set_error(ctx, rc, "apspie_batch_run: sub-context");
+    }
+    sub->owns_stream = true;
+    ctx->subs.push_back(sub);
+    ctx->sub_done.push_back(ev);
+  }
+  return APSPIE_OK;
+}
+
+int run_deep_sources(apspie_context *ctx, int njobs, const apspie_job *jobs,
+                     const std::vector<char> &deep_job, int budget) {
+  int nsrc = 0;
+  for (int i = 0; i < njobs; ++i)
+    if (deep_job[i]) nsrc += jobs[i].nsrc;
+  const int K = std::max(1, std::min(nsrc, ctx->batch_deep_subs));
+  int rc = ensure_subs(ctx, K);
+  if (rc) return rc;
+  if (!ctx->aux_done &&
+      cudaEventCreateWithFlags(&ctx->aux_done, cudaEventDisableTiming) != cudaSuccess)
+    return check_cuda(ctx, cudaGetLastError(), "apspie_batch_run: event");
+  // the sub-streams start after everything queued so far (inputs, uploads)
+  cudaEventRecord(ctx->aux_done, ctx->stream);
+  const int grid = std::max(1, budget / K);
+  for (int k = 0; k < K; ++k) {
+    apspie_context *sub = ctx->subs[k];
+    cudaStreamWaitEvent(sub->stream, ctx->aux_done, 0);
+    sub->max_grid = grid;
+    sub->bfs_alpha = ctx->bfs_alpha;
+    sub->bfs_beta = ctx->bfs_beta;
+    sub->bfs_mode = ctx->bfs_mode;
+    sub->sssp_delta_u32 = ctx->sssp_delta_u32 ? ctx->sssp_delta_u32 : kDeepDelta;
+  }
+  std::vector<double> load(K, 0.0);
+  for (int pass = 0; pass < 2; ++pass)  // SSSP sources first, then BFS
+    for (int i = 0; i < njobs; ++i) {
+      const apspie_job &J = jobs[i];
+      const bool bfs = J.type == APSPIE_JOB_BFS;
+      if (!deep_job[i] || bfs != (pass == 1)) continue;
+      const int *tp = J.d_tptr ? J.d_tptr : (J.symmetric ? J.d_ptr : nullptr);
+      const int *ti = J.d_tptr ? J.d_tind : (J.symmetric ? J.d_ind : nullptr);
+      for (int s = 0; s < J.nsrc; ++s) {
+        const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[k] += 1.0;
+        apspie_context *sub = ctx->subs[k];
+        int32_t *out = J.d_out + (size_t)s * J.m;
+        rc = bfs ? apspie_bfs(sub, J.h_src[s], J.nnz, J.m, J.d_ptr, J.d_ind, tp, ti, out, 0)
+                 : apspie_sssp_u32(sub, J.h_src[s], J.nnz, J.m, J.d_ptr, J.d_ind, J.d_w,
+                                   reinterpret_cast<uint32_t *>(out), 0);
+        if (rc) return set_error(ctx, rc, "apspie_batch_run: deep source: %s",
+                                 sub->last_error.c_str());
+      }
+    }
+  for (int k = 0; k < K; ++k) {
+    ctx->launches += ctx->subs[k]->launches;
+    ctx->subs[k]->launches = 0;
+    cudaEventRecord(ctx->sub_done[k], ctx->subs[k]->stream);
+    cudaStreamWaitEvent(ctx->stream, ctx->sub_done[k], 0);
+  }
+  ctx->batch_subs_used = K;
+  return check_cuda(ctx, cudaGetLastError(), "apspie_batch_run: deep sources");
+}
+
 }  // namespace
 }  // namespace apspie
 
@@ -785,11 +873,6 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
   APSPIE_CHECK_CTX(ctx);
   if (njobs <= 0 || !jobs)
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: no jobs");
-  // split jobs into device jobs of at most 64 sources
-  struct Part {
-    int job, first, n;
-  };
-  std::vector<Part> parts;
   for (int i = 0; i < njobs; ++i) {
     const apspie_job &J = jobs[i];
     if ((J.type != APSPIE_JOB_BFS && J.type != APSPIE_JOB_SSSP_U32) || J.m <= 0 || J.nnz < 0 ||
@@ -800,6 +883,32 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
       if (J.h_src[s] < 0 || J.h_src[s] >= J.m)
         return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: job %d source %d out of range",
                          i, J.h_src[s]);
+  }
+  // Jobs on deep graphs (a BFS of more than kDeepLevels levels, probed once
+  // per graph) are latency bound per level and gain little from sharing
+  // their levels: their sources run as independent single-source traversals,
+  // concurrently on sub-contexts with small grids.  The others are split
+  // into device jobs of at most 64 (BFS) / 32 (SSSP) sources for one
+  // multi-source launch.
+  std::vector<char> deep_job(njobs, 0);
+  if (max_steps <= 0 && ctx->batch_deep_subs > 0)
+    for (int i = 0; i < njobs; ++i) {
+      int lv = 0;
+      int rc0 = graph_levels(ctx, jobs[i], &lv);
+      if (rc0) return rc0;
+      deep_job[i] = lv > kDeepLevels;
+    }
+  struct Part {
+    int job, first, n;
+  };
+  std::vector<Part> parts;
+  int ndeep_src = 0;
+  for (int i = 0; i < njobs; ++i) {
+    const apspie_job &J = jobs[i];
+    if (deep_job[i]) {
+      ndeep_src += J.nsrc;
+      continue;
+    }
     const int width = J.type == APSPIE_JOB_BFS ? kMsbfsWidth : kMssspWidth;
     for (int f = 0; f < J.nsrc; f += width)
       parts.push_back(Part{i, f, std::min(width, J.nsrc - f)});
@@ -808,186 +917,163 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
   if (nparts > kMaxJobs)
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: %d device jobs > %d", nparts,
                      kMaxJobs);
-  // deep-graph jobs go last and, when others are present, into a launch of
-  // their own on the context's second stream
-  std::vector<char> deep_job(njobs, 0);
-  for (int i = 0; i < njobs && njobs > 1; ++i) {
-    int lv = 0;
-    int rc0 = graph_levels(ctx, jobs[i], &lv);
-    if (rc0) return rc0;
-    deep_job[i] = lv > kDeepLevels;
-  }
-  std::stable_partition(parts.begin(), parts.end(),
-                        [&](const Part &p) { return !deep_job[p.job]; });
-  int nshallow = 0;
-  for (const Part &p : parts) nshallow += deep_job[p.job] ? 0 : 1;
   const int full = clamp_grid(ctx, batch_grid(ctx));
   if (full <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_batch_run: occupancy query failed");
-  const bool split = nshallow > 0 && nshallow < nparts && full > 1 && ctx->deep_blocks < full;
-  // workspace layout per device job
-  std::vector<size_t> off(nparts + 1, 0);
-  size_t total = align_up(sizeof(BatchJob) * kMaxJobs) + 2 * align_up(sizeof(BatchState)) +
-                 align_up(sizeof(int) * 64 * kMaxJobs);
-  const size_t head = total;
-  for (int p = 0; p < nparts; ++p) {
-    const apspie_job &J = jobs[parts[p].job];
-    const bool bfs = J.type == APSPIE_JOB_BFS;
-    const size_t m = (size_t)J.m, cap = job_chunk_capacity(J.nnz, bfs);
-    size_t b = 0;
-    b += align_up(8 * m) * (bfs ? 4 : 3);  // (BFS: visited +) 3 frontier masks
-    b += align_up(4 * m) * 3;              // queues
-    b += align_up(8 * cap) * 3;            // chunk lists
-    b += align_up(4 * m * row_width(parts[p].n));  // vertex-major results
-    off[p] = total;
-    total += b;
-  }
-  unsigned char *ws = (unsigned char *)workspace(ctx, kSlotBatch, total);
-  if (!ws) return APSPIE_ERR_OOM;
-  auto *djobs = (BatchJob *)ws;
-  auto *dstate = (BatchState *)(ws + align_up(sizeof(BatchJob) * kMaxJobs));
-  auto *dstate2 = (BatchState *)(ws + align_up(sizeof(BatchJob) * kMaxJobs) +
-                                 align_up(sizeof(BatchState)));
-  int *dsrc = (int *)(ws + align_up(sizeof(BatchJob) * kMaxJobs) + 2 * align_up(sizeof(BatchState)));
-  (void)head;
-  // host image of the job table (pinned, copied in one transfer); earlier
-  // copies out of the pinned buffer must have completed before it is reused
-  int src_rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "apspie_batch_run");
-  if (src_rc) return src_rc;
-  size_t host_bytes = sizeof(BatchJob) * nparts + sizeof(int) * 64 * nparts;
-  auto *hjobs = (BatchJob *)pinned(ctx, host_bytes);
-  if (!hjobs) return APSPIE_ERR_OOM;
-  int *hsrc = (int *)(hjobs + nparts);
-  for (int p = 0; p < nparts; ++p) {
-    const apspie_job &J = jobs[parts[p].job];
-    BatchJob &B = hjobs[p];
-    std::memset(&B, 0, sizeof(B));
-    B.type = J.type == APSPIE_JOB_BFS ? kJobBfs : kJobSssp;
-    B.m = J.m;
-    B.nnz = J.nnz;
-    B.nsrc = parts[p].n;
-    B.ptr = J.d_ptr;
-    B.ind = J.d_ind;
-    B.tptr = J.d_tptr ? J.d_tptr : J.d_ptr;
-    B.tind = J.d_tptr ? J.d_tind : J.d_ind;
-    B.w = J.d_w;
-    B.alpha = J.alpha >= 0 ? J.alpha : ctx->bfs_alpha;
-    B.beta = J.beta >= 0 ? J.beta : ctx->bfs_beta;
-    // no in-adjacency for a directed graph: never pull (alpha 0)
-    if (!J.d_tptr && !J.symmetric) B.alpha = 0;
-    for (int s = 0; s < parts[p].n; ++s) hsrc[p * 64 + s] = J.h_src[parts[p].first + s];
-    B.src = dsrc + p * 64;
-    unsigned char *b = ws + off[p];
-    const bool bfs = B.type == kJobBfs;
-    const size_t m = (size_t)J.m, cap = job_chunk_capacity(J.nnz, bfs);
-    B.big_deg = bfs ? kBigDeg : kSsspBigDeg;
-    B.sw = row_width(B.nsrc);  // result row: the sources rounded up to a power of two
-    B.chunk = bfs ? kChunk : kSsspChunk;
-    if (bfs) {
-      B.visited = (unsigned long long *)b;
-      b += align_up(8 * m);
-    }
-    B.F0 = (unsigned long long *)b; b += align_up(8 * m);
-    B.F1 = (unsigned long long *)b; b += align_up(8 * m);
-    B.F2 = (unsigned long long *)b; b += align_up(8 * m);
-    B.q0 = (int *)b; b += align_up(4 * m);
-    B.q1 = (int *)b; b += align_up(4 * m);
-    B.q2 = (int *)b; b += align_up(4 * m);
-    B.c0 = (int2 *)b; b += align_up(8 * cap);
-    B.c1 = (int2 *)b; b += align_up(8 * cap);
-    B.c2 = (int2 *)b; b += align_up(8 * cap);
-    B.out = (int32_t *)b;  // vertex-major; transposed into the caller's array after
-  }
+  // the deep sources get deep_blocks in all (default two thirds of the
+  // resident blocks: their traversals are latency bound, and a grid filled
+  // to the last block slowed them down, measured)
+  const int deep_budget =
+      ndeep_src == 0 ? 0
+                     : std::max(1, std::min(full - (nparts > 0 ? 1 : 0),
+                                            ctx->deep_blocks > 0 ? ctx->deep_blocks
+                                                                 : 2 * full / 3));
+  const int grid1 = std::max(1, full - (nparts > 0 ? deep_budget : 0));
   cudaStream_t st = ctx->stream;
-  cudaMemcpyAsync(djobs, hjobs, host_bytes, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(dsrc, hsrc, sizeof(int) * 64 * nparts, cudaMemcpyHostToDevice, st);
-  cudaMemsetAsync(dstate, 0, 2 * align_up(sizeof(BatchState)), st);
-  int rc = check_cuda(ctx, cudaGetLastError(), "apspie_batch_run upload");
-  if (rc) return rc;
-  // the deep jobs' stream starts after the uploads
-  cudaStream_t st2 = st;
-  if (split) {
-    if (!ctx->aux_stream &&
-        (cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking) != cudaSuccess ||
-         cudaEventCreateWithFlags(&ctx->aux_done, cudaEventDisableTiming) != cudaSuccess))
-      return check_cuda(ctx, cudaGetLastError(), "apspie_batch_run: second stream");
-    st2 = ctx->aux_stream;
-    cudaEventRecord(ctx->aux_done, st);
-    cudaStreamWaitEvent(st2, ctx->aux_done, 0);
-  }
-  for (int p = 0; p < nparts; ++p) {
-    const long long m = jobs[parts[p].job].m;
-    cudaStream_t sp = p < nshallow ? st : st2;
-    int g = (int)std::max(1ll, std::min((m * hjobs[p].sw + 255) / 256, (long long)ctx->num_sms * 8));
-    if (hjobs[p].type == kJobBfs) {
-      batch_init_bfs<<<g, 256, 0, sp>>>(djobs, p);
-      batch_seed_bfs<<<1, 64, 0, sp>>>(djobs, p);
-    } else {
-      batch_init_sssp<<<g, 256, 0, sp>>>(djobs, p);
-      batch_seed_sssp<<<1, 32, 0, sp>>>(djobs, p);
+  int rc = APSPIE_OK;
+  ctx->batch_state = nullptr;
+  ctx->batch_subs_used = 0;
+  if (nparts > 0) {
+    // workspace layout per device job
+    std::vector<size_t> off(nparts + 1, 0);
+    size_t total = align_up(sizeof(BatchJob) * kMaxJobs) + align_up(sizeof(BatchState)) +
+                   align_up(sizeof(int) * 64 * kMaxJobs);
+    for (int p = 0; p < nparts; ++p) {
+      const apspie_job &J = jobs[parts[p].job];
+      const bool bfs = J.type == APSPIE_JOB_BFS;
+      const size_t m = (size_t)J.m, cap = job_chunk_capacity(J.nnz, bfs);
+      size_t b = 0;
+      b += align_up(8 * m) * (bfs ? 4 : 3);  // (BFS: visited +) 3 frontier masks
+      b += align_up(4 * m) * 3;              // queues
+      b += align_up(8 * cap) * 3;            // chunk lists
+      b += align_up(4 * m * row_width(parts[p].n));  // vertex-major results
+      off[p] = total;
+      total += b;
     }
-  }
-  rc = check_launch(ctx, "batch init", 2 * nparts);
-  if (rc) return rc;
-  // one launch for everything, or the shallow jobs here and the deep ones on
-  // the second stream with deep_grid blocks, the two grids sharing the GPU
-  // deep jobs are latency bound per level but carry many levels: by default
-  // they get two thirds of the GPU (measured best on the batched benchmark)
-  const int deep_grid = std::max(1, std::min(full - 1, ctx->deep_blocks > 0 ? ctx->deep_blocks
-                                                                             : 2 * full / 3));
-  const int grid1 = split ? std::max(1, full - deep_grid) : full;
-  int n1 = split ? nshallow : nparts;
-  BatchJob *dj1 = djobs;
-  void *args1[] = {&dj1, &n1, &dstate, &max_steps};
-  cudaError_t e = cudaLaunchCooperativeKernel((const void *)batch_persistent, dim3(grid1),
-                                              dim3(kBatchThreads), args1, 0, st);
-  if (e != cudaSuccess) return check_cuda(ctx, e, "batch_persistent");
-  ctx->launches += 1;
-  if (split) {
-    int n2 = nparts - nshallow;
-    BatchJob *dj2 = djobs + nshallow;
-    void *args2[] = {&dj2, &n2, &dstate2, &max_steps};
-    e = cudaLaunchCooperativeKernel((const void *)batch_persistent, dim3(deep_grid),
-                                    dim3(kBatchThreads), args2, 0, st2);
-    if (e != cudaSuccess) return check_cuda(ctx, e, "batch_persistent (deep jobs)");
+    unsigned char *ws = (unsigned char *)workspace(ctx, kSlotBatch, total);
+    if (!ws) return APSPIE_ERR_OOM;
+    auto *djobs = (BatchJob *)ws;
+    auto *dstate = (BatchState *)(ws + align_up(sizeof(BatchJob) * kMaxJobs));
+    int *dsrc = (int *)(ws + align_up(sizeof(BatchJob) * kMaxJobs) + align_up(sizeof(BatchState)));
+    // host image of the job table (pinned, copied in one transfer); earlier
+    // copies out of the pinned buffer must have completed before it is reused
+    rc = check_cuda(ctx, cudaStreamSynchronize(st), "apspie_batch_run");
+    if (rc) return rc;
+    size_t host_bytes = sizeof(BatchJob) * nparts + sizeof(int) * 64 * nparts;
+    auto *hjobs = (BatchJob *)pinned(ctx, host_bytes);
+    if (!hjobs) return APSPIE_ERR_OOM;
+    int *hsrc = (int *)(hjobs + nparts);
+    for (int p = 0; p < nparts; ++p) {
+      const apspie_job &J = jobs[parts[p].job];
+      BatchJob &B = hjobs[p];
+      std::memset(&B, 0, sizeof(B));
+      B.type = J.type == APSPIE_JOB_BFS ? kJobBfs : kJobSssp;
+      B.m = J.m;
+      B.nnz = J.nnz;
+      B.nsrc = parts[p].n;
+      B.ptr = J.d_ptr;
+      B.ind = J.d_ind;
+      B.tptr = J.d_tptr ? J.d_tptr : J.d_ptr;
+      B.tind = J.d_tptr ? J.d_tind : J.d_ind;
+      B.w = J.d_w;
+      B.alpha = J.alpha >= 0 ? J.alpha : ctx->bfs_alpha;
+      B.beta = J.beta >= 0 ? J.beta : ctx->bfs_beta;
+      // no in-adjacency for a directed graph: never pull (alpha 0)
+      if (!J.d_tptr && !J.symmetric) B.alpha = 0;
+      for (int s = 0; s < parts[p].n; ++s) hsrc[p * 64 + s] = J.h_src[parts[p].first + s];
+      B.src = dsrc + p * 64;
+      unsigned char *b = ws + off[p];
+      const bool bfs = B.type == kJobBfs;
+      const size_t m = (size_t)J.m, cap = job_chunk_capacity(J.nnz, bfs);
+      B.big_deg = bfs ? kBigDeg : kSsspBigDeg;
+      B.sw = row_width(B.nsrc);  // result row: the sources rounded up to a power of two
+      B.chunk = bfs ? kChunk : kSsspChunk;
+      if (bfs) {
+        B.visited = (unsigned long long *)b;
+        b += align_up(8 * m);
+      }
+      B.F0 = (unsigned long long *)b; b += align_up(8 * m);
+      B.F1 = (unsigned long long *)b; b += align_up(8 * m);
+      B.F2 = (unsigned long long *)b; b += align_up(8 * m);
+      B.q0 = (int *)b; b += align_up(4 * m);
+      B.q1 = (int *)b; b += align_up(4 * m);
+      B.q2 = (int *)b; b += align_up(4 * m);
+      B.c0 = (int2 *)b; b += align_up(8 * cap);
+      B.c1 = (int2 *)b; b += align_up(8 * cap);
+      B.c2 = (int2 *)b; b += align_up(8 * cap);
+      B.out = (int32_t *)b;  // vertex-major; transposed into the caller's array after
+    }
+    cudaMemcpyAsync(djobs, hjobs, host_bytes, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dsrc, hsrc, sizeof(int) * 64 * nparts, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(dstate, 0, align_up(sizeof(BatchState)), st);
+    rc = check_cuda(ctx, cudaGetLastError(), "apspie_batch_run upload");
+    if (rc) return rc;
+    for (int p = 0; p < nparts; ++p) {
+      const long long m = jobs[parts[p].job].m;
+      int g = (int)std::max(1ll, std::min((m * hjobs[p].sw + 255) / 256, (long long)ctx->num_sms * 8));
+      if (hjobs[p].type == kJobBfs) {
+        batch_init_bfs<<<g, 256, 0, st>>>(djobs, p);
+        batch_seed_bfs<<<1, 64, 0, st>>>(djobs, p);
+      } else {
+        batch_init_sssp<<<g, 256, 0, st>>>(djobs, p);
+        batch_seed_sssp<<<1, 32, 0, st>>>(djobs, p);
+      }
+    }
+    rc = check_launch(ctx, "batch init", 2 * nparts);
+    if (rc) return rc;
+    int n1 = nparts;
+    void *args1[] = {&djobs, &n1, &dstate, &max_steps};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *)batch_persistent, dim3(grid1),
+                                                dim3(kBatchThreads), args1, 0, st);
+    if (e != cudaSuccess) return check_cuda(ctx, e, "batch_persistent");
     ctx->launches += 1;
+    for (int p = 0; p < nparts; ++p) {
+      const apspie_job &J = jobs[parts[p].job];
+      batch_transpose<<<(J.m + 31) / 32, 256, 0, st>>>(
+          hjobs[p].out, J.m, hjobs[p].sw, parts[p].n, J.d_out + (size_t)parts[p].first * J.m);
+    }
+    rc = check_launch(ctx, "batch_transpose", nparts);
+    if (rc) return rc;
+    ctx->batch_state = dstate;
   }
-  for (int p = 0; p < nparts; ++p) {
-    const apspie_job &J = jobs[parts[p].job];
-    const int width = hjobs[p].sw;
-    batch_transpose<<<(J.m + 31) / 32, 256, 0, p < nshallow ? st : st2>>>(
-        hjobs[p].out, J.m, width, parts[p].n, J.d_out + (size_t)parts[p].first * J.m);
+  if (ndeep_src > 0) {
+    rc = run_deep_sources(ctx, njobs, jobs, deep_job, deep_budget);
+    if (rc) return rc;
   }
-  rc = check_launch(ctx, "batch_transpose", nparts);
-  if (rc) return rc;
-  if (split) {
-    // the call completes on the context's stream
-    cudaEventRecord(ctx->aux_done, st2);
-    cudaStreamWaitEvent(st, ctx->aux_done, 0);
-  }
-  ctx->batch_state = dstate;
-  ctx->batch_state2 = split ? dstate2 : nullptr;
   return APSPIE_OK;
 }
 
 int apspie_batch_get_stats(apspie_ctx ctx, apspie_batch_stats *out) {
   APSPIE_CHECK_CTX(ctx);
-  if (!out || !ctx->batch_state)
+  if (!out || (!ctx->batch_state && ctx->batch_subs_used == 0))
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_get_stats: no batch has run");
-  auto *h = (BatchState *)pinned(ctx, 2 * sizeof(BatchState));
-  if (!h) return APSPIE_ERR_OOM;
-  cudaMemcpyAsync(h, ctx->batch_state, sizeof(BatchState), cudaMemcpyDeviceToHost, ctx->stream);
-  if (ctx->batch_state2)
-    cudaMemcpyAsync(h + 1, ctx->batch_state2, sizeof(BatchState), cudaMemcpyDeviceToHost,
-                    ctx->stream);
-  int rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "apspie_batch_get_stats");
-  if (rc) return rc;
-  out->super_steps = h[0].steps;
-  out->frontier_edges = (int64_t)h[0].edges;
-  int err = h[0].err;
-  if (ctx->batch_state2) {
-    out->super_steps = std::max(out->super_steps, h[1].steps);
-    out->frontier_edges += (int64_t)h[1].edges;
-    err |= h[1].err;
+  out->super_steps = 0;
+  out->frontier_edges = 0;
+  int err = 0;
+  if (ctx->batch_state) {
+    auto *h = (BatchState *)pinned(ctx, sizeof(BatchState));
+    if (!h) return APSPIE_ERR_OOM;
+    cudaMemcpyAsync(h, ctx->batch_state, sizeof(BatchState), cudaMemcpyDeviceToHost, ctx->stream);
+    int rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "apspie_batch_get_stats");
+    if (rc) return rc;
+    out->super_steps = h->steps;
+    out->frontier_edges = (int64_t)h->edges;
+    err = h->err;
+  }
+  // deep sources: each sub-context's last traversal of each kind (a barrier
+  // timeout leaves its device stuck, so the later runs on it time out too);
+  // super_steps counts their levels / rounds as well
+  for (int k = 0; k < ctx->batch_subs_used; ++k) {
+    apspie_context *sub = ctx->subs[k];
+    if (sub->bfs_state) {
+      apspie_bfs_stats b;
+      if (apspie_bfs_get_stats(sub, &b) == APSPIE_ERR_TIMEOUT) err = 1;
+      else out->super_steps = std::max(out->super_steps, b.levels);
+    }
+    if (sub->sssp_state) {
+      apspie_sssp_stats q;
+      if (apspie_sssp_get_stats(sub, &q) == APSPIE_ERR_TIMEOUT) err = 1;
+      else out->super_steps = std::max(out->super_steps, q.rounds);
+    }
   }
   if (err) return set_error(ctx, APSPIE_ERR_TIMEOUT, "apspie_batch_run: grid barrier timed out");
   return APSPIE_OK;

@@ -82,14 +82,16 @@ using namespace apspie;
 namespace apspie {
 
 uint64_t graph_fingerprint(apspie_context *ctx, int m, int64_t nnz, const int *d_ptr) {
-  // offsets sampled at 64 evenly spaced rows (plus the last)
-  int *h = (int *)pinned(ctx, sizeof(int) * 65);
+  // offsets sampled at 64 evenly spaced rows (plus the last), gathered on
+  // the device and read back in one copy
   uint64_t f = 1469598103934665603ull ^ ((uint64_t)m << 32) ^ (uint64_t)nnz;
-  if (!h) return f;
-  for (int i = 0; i <= 64; ++i) {
-    size_t row = (size_t)((int64_t)m * i / 64);
-    cudaMemcpyAsync(h + i, d_ptr + row, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  int *h = (int *)pinned(ctx, sizeof(int) * 65);
+  int *d = (int *)workspace(ctx, kSlotFingerprint, sizeof(int) * 65);
+  if (!h || !d || gather_offsets(ctx, d_ptr, m, d) != APSPIE_OK) {
+    cudaGetLastError();
+    return f;
   }
+  cudaMemcpyAsync(h, d, sizeof(int) * 65, cudaMemcpyDeviceToHost, ctx->stream);
   cudaStreamSynchronize(ctx->stream);
   for (int i = 0; i <= 64; ++i) f = (f ^ (uint64_t)(uint32_t)h[i]) * 1099511628211ull;
   return f;
@@ -125,14 +127,13 @@ int apspie_ctx_destroy(apspie_ctx ctx) {
   if (!ctx) return APSPIE_ERR_INVALID;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  if (ctx->aux_stream) {
-    cudaStreamSynchronize(ctx->aux_stream);
-    cudaStreamDestroy(ctx->aux_stream);
-  }
+  for (apspie_context *sub : ctx->subs) apspie_ctx_destroy(sub);
+  for (cudaEvent_t ev : ctx->sub_done) cudaEventDestroy(ev);
   if (ctx->aux_done) cudaEventDestroy(ctx->aux_done);
   for (auto &s : ctx->slots)
     if (s.ptr) cudaFree(s.ptr);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  if (ctx->owns_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return APSPIE_OK;
 }
@@ -146,6 +147,12 @@ int apspie_ctx_set_max_grid(apspie_ctx ctx, int blocks) {
 int apspie_batch_set_params(apspie_ctx ctx, int deep_blocks) {
   if (!ctx || deep_blocks < 0) return APSPIE_ERR_INVALID;
   ctx->deep_blocks = deep_blocks;
+  return APSPIE_OK;
+}
+
+int apspie_batch_set_deep_mode(apspie_ctx ctx, int max_concurrent) {
+  if (!ctx || max_concurrent < 0 || max_concurrent > 64) return APSPIE_ERR_INVALID;
+  ctx->batch_deep_subs = max_concurrent;
   return APSPIE_OK;
 }
 

@@ -48,13 +48,19 @@ struct apspie_context {
   void *batch_state = nullptr;
   // SpMSpV: the bitmap path is taken when E * factor > m
   double spmspv_sort_factor = 4.0;
-  // batched launches: a second stream (and its completion event) for the
-  // jobs of deep graphs, which run next to the others with a small grid;
-  // traversal depth of graphs seen before, by fingerprint
-  cudaStream_t aux_stream = nullptr;
-  int deep_blocks = 0;  // blocks of the deep jobs' launch (0: two thirds of the resident ones)
+  // batched launches: the sources of jobs on deep graphs run as
+  // single-source traversals on sub-contexts (own stream and workspace),
+  // concurrently, with deep_blocks blocks in all (0: two thirds of the
+  // resident ones when multi-source jobs run next to them); aux_done orders
+  // their start after the context's stream; traversal depth of graphs seen
+  // before, by fingerprint
+  int batch_deep_subs = 48;  // most concurrent single-source traversals (0: none)
+  int deep_blocks = 0;
   cudaEvent_t aux_done = nullptr;
-  void *batch_state2 = nullptr;
+  std::vector<struct apspie_context *> subs;
+  std::vector<cudaEvent_t> sub_done;
+  int batch_subs_used = 0;  // sub-contexts the last batch ran sources on
+  bool owns_stream = false;  // a sub-context's stream, destroyed with it
   struct DepthEntry {
     uint64_t fp;
     int levels;
@@ -115,6 +121,7 @@ enum SlotId : int {
   kSlotMxvFlags,
   kSlotSmall,
   kSlotBatch,
+  kSlotFingerprint,
   // SpGEMM plan: kept from the symbolic phase for repeated numeric phases
   kSlotSpgProd,
   kSlotSpgLists,
@@ -149,6 +156,8 @@ namespace apspie {
 // Fingerprint of a graph: m, nnz and its row offsets at 64 evenly spaced rows
 // (synchronises the context's stream).
 uint64_t graph_fingerprint(apspie_context *ctx, int m, int64_t nnz, const int *d_ptr);
+// d_out[i] = d_ptr[m * i / 64] for i = 0..64 (one small launch)
+int gather_offsets(apspie_context *ctx, const int *d_ptr, int m, int *d_out);
 
 // Grid of a persistent launch: the occupancy-sized grid, capped by the
 // context's max_grid.

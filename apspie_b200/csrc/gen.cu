@@ -356,3 +356,17 @@ int apspie_gen_weights_f32_device(apspie_ctx ctx, int m, const int *d_ptr, const
 }
 
 }  // extern "C"
+
+namespace apspie {
+namespace {
+__global__ void gather_offsets_kernel(const int *__restrict__ ptr, int m, int *out) {
+  const int i = threadIdx.x;
+  if (i <= 64) out[i] = ptr[(size_t)((int64_t)m * i / 64)];
+}
+}  // namespace
+
+int gather_offsets(apspie_context *ctx, const int *d_ptr, int m, int *d_out) {
+  gather_offsets_kernel<<<1, 96, 0, ctx->stream>>>(d_ptr, m, d_out);
+  return check_launch(ctx, "gather_offsets");
+}
+}  // namespace apspie

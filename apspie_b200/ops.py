@@ -433,6 +433,17 @@ def batch_run(ctx: Context, jobs: list[dict], max_steps: int = 0):
     return outs
 
 
+def batch_set_params(ctx: Context, deep_blocks: int = 0, deep_concurrent: int = 48):
+    """Sources of jobs on deep graphs (BFS of more than 64 levels) run as
+    single-source traversals, up to deep_concurrent at a time on
+    sub-contexts, with deep_blocks blocks in all (0: the default share);
+    deep_concurrent=0 keeps them in the multi-source launch."""
+    check(lib.apspie_batch_set_params(ctx.handle, int(deep_blocks)), ctx.handle,
+          "apspie_batch_set_params")
+    check(lib.apspie_batch_set_deep_mode(ctx.handle, int(deep_concurrent)), ctx.handle,
+          "apspie_batch_set_deep_mode")
+
+
 def batch_stats(ctx: Context) -> dict:
     s = BatchStats()
     check(lib.apspie_batch_get_stats(ctx.handle, C.byref(s)), ctx.handle, "apspie_batch_get_stats")

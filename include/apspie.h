@@ -252,11 +252,17 @@ typedef struct {
 int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs,
                      int max_steps);
 /* Jobs on graphs whose BFS takes more than 64 levels (found by one probe BFS
- * per new graph, cached by fingerprint) run in a second launch on a second
- * stream next to the others when both kinds are present; deep_blocks = its
- * grid (0: two thirds of the resident blocks, the default; at least the
- * resident blocks: no second launch, every job in one). */
+ * per new graph, cached by fingerprint) are latency bound per level and
+ * share little between sources: their sources run as single-source
+ * traversals (apspie_bfs / apspie_sssp_u32, SSSP near-far with the
+ * context's step or 1024), up to max_concurrent (default 48, at most 64)
+ * at a time on sub-contexts of this context (own streams and workspaces),
+ * next to the multi-source launch of the other jobs; deep_blocks = their
+ * blocks in all (0: two thirds of the resident blocks).  The call stays
+ * stream-ordered on the context's stream.  max_concurrent = 0 puts every
+ * job in the multi-source launch instead; max_steps > 0 always does. */
 int apspie_batch_set_params(apspie_ctx ctx, int deep_blocks);
+int apspie_batch_set_deep_mode(apspie_ctx ctx, int max_concurrent);
 /* Statistics of the last batch (synchronises; reports a barrier timeout). */
 int apspie_batch_get_stats(apspie_ctx ctx, apspie_batch_stats *out);
 

@@ -20,7 +20,18 @@ def _graphs():
     return a, b, c, d
 
 
-def test_batch_bfs_and_sssp_mixed(ctx):
+@pytest.fixture(params=[48, 3, 0], ids=["deep-single-source", "deep-3-streams", "deep-multi-source"])
+def deep_mode(ctx, request):
+    """Jobs on the deep grids as concurrent single-source traversals (the
+    default; or fewer sub-contexts than sources) or inside the multi-source
+    launch."""
+    import apspie_b200 as ap
+    ap.batch_set_params(ctx, 0, request.param)
+    yield request.param
+    ap.batch_set_params(ctx)
+
+
+def test_batch_bfs_and_sssp_mixed(ctx, deep_mode):
     import apspie_b200 as ap
     a, b, c, d = _graphs()
     ga, gb, gc, gd = (x.to_device() for x in (a, b, c, d))
@@ -95,7 +106,7 @@ def test_autotuner_picks_and_caches(ctx):
     ap.spmspv_set_params(ctx)
 
 
-def test_batch_sssp_multi_source_parts(ctx):
+def test_batch_sssp_multi_source_parts(ctx, deep_mode):
     """Multi-source SSSP rows: more than 32 sources (two device jobs), a
     duplicated source, hubs split into chunks, a directed graph and a
     grid with heavy weights; every row equals the oracle's Dijkstra."""
