@@ -919,14 +919,14 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
                      kMaxJobs);
   const int full = clamp_grid(ctx, batch_grid(ctx));
   if (full <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_batch_run: occupancy query failed");
-  // the deep sources get deep_blocks in all (default two thirds of the
-  // resident blocks: their traversals are latency bound, and a grid filled
-  // to the last block slowed them down, measured)
+  // the deep sources get deep_blocks in all (default half the resident
+  // blocks: their traversals are latency bound, a grid filled to the last
+  // block slowed them down, and the multi-source launch beside them needs
+  // the rest; measured on the batched benchmark)
   const int deep_budget =
       ndeep_src == 0 ? 0
                      : std::max(1, std::min(full - (nparts > 0 ? 1 : 0),
-                                            ctx->deep_blocks > 0 ? ctx->deep_blocks
-                                                                 : 2 * full / 3));
+                                            ctx->deep_blocks > 0 ? ctx->deep_blocks : full / 2));
   const int grid1 = std::max(1, full - (nparts > 0 ? deep_budget : 0));
   cudaStream_t st = ctx->stream;
   int rc = APSPIE_OK;

@@ -503,7 +503,7 @@ def run_ours(args):
     # edges traversed per source (and warm-up)
     tune = {"alpha": None, "beta": None}
     if not args.no_tune:
-        tune_src = ap.seeded_sources(h, 8, seed=1000 + rank)
+        tune_src = ap.seeded_sources(h, 16, seed=1000 + rank)
         tune = ap.autotune_bfs(ctx, g, tune_src)
     e_r = []
     for s in sources[:nsrc]:
@@ -621,7 +621,7 @@ def run_ours(args):
                                       % prep_ms),
                    "switch_points": {"alpha": tune.get("alpha"), "beta": tune.get("beta"),
                                      "picked_by": "defaults" if args.no_tune else
-                                     "autotuner on 8 untimed sources"}},
+                                     "autotuner on 16 untimed sources (21 switch-point candidates, two sweeps)"}},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "per_step_ms": {"min": min(per), "median": statistics.median(per), "max": max(per)},

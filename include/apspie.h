@@ -258,7 +258,7 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs,
  * context's step or 1024), up to max_concurrent (default 48, at most 64)
  * at a time on sub-contexts of this context (own streams and workspaces),
  * next to the multi-source launch of the other jobs; deep_blocks = their
- * blocks in all (0: two thirds of the resident blocks).  The call stays
+ * blocks in all (0: half the resident blocks).  The call stays
  * stream-ordered on the context's stream.  max_concurrent = 0 puts every
  * job in the multi-source launch instead; max_steps > 0 always does. */
 int apspie_batch_set_params(apspie_ctx ctx, int deep_blocks);
