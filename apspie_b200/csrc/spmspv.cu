@@ -33,11 +33,15 @@ constexpr int kPlusTimes = 0, kMinPlus = 1, kMaxTimes = 2, kOrAnd = 3;
 
 struct SpmspvSmall {  // device-side scalars of one call
   long long total;    // expanded size E
-  unsigned nbig;      // columns handed to expand_big
+  unsigned nbig;      // columns of more than kBigDeg edges (a warp each)
   int ynnz;           // nnz(y)
   unsigned cnt;       // frontier size of the dense form
-  unsigned pad;
+  unsigned nhub;      // columns of more than kHubDeg edges (the whole grid each)
 };
+
+// Columns longer than this are spread over every block; between kBigDeg and
+// this a warp takes one column
+constexpr int kHubDeg = 1024;
 constexpr int kExpandThreads = 256;
 
 __device__ __forceinline__ float sr_term(int sr, float a, float x) {
@@ -61,7 +65,7 @@ __global__ void __launch_bounds__(kExpandThreads)
 expand_pairs(int sr, int xnnz, const int *__restrict__ xind, const float *__restrict__ xval,
              const int *__restrict__ ptr, const int *__restrict__ ind,
              const float *__restrict__ val, const long long *__restrict__ offs, int *keys,
-             float *vals, int *big, unsigned *nbig) {
+             float *vals, int *big, unsigned *nbig, int *hub, unsigned *nhub) {
   const int lane = lane_id();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
@@ -75,13 +79,15 @@ expand_pairs(int sr, int xnnz, const int *__restrict__ xind, const float *__rest
       s = __ldg(ptr + c);
       d = __ldg(ptr + c + 1) - s;
       xv = xval ? xval[j] : 1.0f;
-      if (d > kBigDeg) {
-        isbig = true;
-        d = 0;
-      }
+      if (d > kBigDeg) isbig = true;
     }
-    unsigned slot = warp_append(isbig, nbig);
-    if (isbig) big[slot] = j;
+    const bool ishub = isbig && d > kHubDeg;
+    const bool ismid = isbig && !ishub;
+    unsigned slot = warp_append(ismid, nbig);
+    if (ismid) big[slot] = j;
+    slot = warp_append(ishub, nhub);
+    if (ishub) hub[slot] = j;
+    if (isbig) d = 0;
     int incl = warp_incl_scan(d);
     int excl = incl - d;
     int total = __shfl_sync(kFull, incl, 31);
@@ -102,18 +108,37 @@ expand_pairs(int sr, int xnnz, const int *__restrict__ xind, const float *__rest
   }
 }
 
+// The listed columns: a warp per column of the medium list, then every
+// thread of the grid strides every hub (a hub's edges spread over all SMs).
 __global__ void expand_big(int sr, const int *__restrict__ xind, const float *__restrict__ xval,
                            const int *__restrict__ ptr, const int *__restrict__ ind,
                            const float *__restrict__ val, const long long *__restrict__ offs,
-                           const int *big, const unsigned *nbig, int *keys, float *vals) {
-  unsigned nb = *nbig;
-  for (unsigned b = blockIdx.x; b < nb; b += gridDim.x) {
-    int j = big[b];
-    int c = xind[j];
-    int s = __ldg(ptr + c), e = __ldg(ptr + c + 1);
-    float xv = xval ? xval[j] : 1.0f;
-    long long o = offs[j] - s;
-    for (int k = s + threadIdx.x; k < e; k += blockDim.x) {
+                           const int *big, const unsigned *nbig, const int *hub,
+                           const unsigned *nhub, int *keys, float *vals) {
+  const int lane = lane_id();
+  const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  const unsigned nb = *nbig;
+  for (unsigned b = gwarp; b < nb; b += nwarps) {
+    const int j = big[b];
+    const int c = xind[j];
+    const int s = __ldg(ptr + c), e = __ldg(ptr + c + 1);
+    const float xv = xval ? xval[j] : 1.0f;
+    const long long o = offs[j] - s;
+    for (int k = s + lane; k < e; k += 32) {
+      keys[o + k] = __ldg(ind + k);
+      vals[o + k] = sr_term(sr, val ? __ldg(val + k) : 1.0f, xv);
+    }
+  }
+  const unsigned nh = *nhub;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  for (unsigned b = 0; b < nh; ++b) {
+    const int j = hub[b];
+    const int c = xind[j];
+    const int s = __ldg(ptr + c), e = __ldg(ptr + c + 1);
+    const float xv = xval ? xval[j] : 1.0f;
+    const long long o = offs[j] - s;
+    for (int k = s + tid; k < e; k += nthreads) {
       keys[o + k] = __ldg(ind + k);
       vals[o + k] = sr_term(sr, val ? __ldg(val + k) : 1.0f, xv);
     }
@@ -181,30 +206,113 @@ __device__ __forceinline__ void atomic_max_double(double *p, double v) {
   }
 }
 
+// Bitmap path expansion.  32 consecutive frontier entries per warp: their
+// edges are dealt over the lanes by an inclusive warp scan of the degrees
+// (coalesced over each column, no lane idles on a short column).  Columns
+// of more than kBigDeg edges are listed instead: up to kHubDeg edges a warp
+// takes one in expand_accumulate_big, longer ones (hubs) are strided by
+// every thread of that grid.  Each product is folded into acc[row] with the
+// semiring's atomic and marks the row's bit.
+__device__ __forceinline__ void accumulate_one(int sr, int r, float t, double *acc,
+                                               unsigned *bits) {
+  switch (sr) {
+    case kPlusTimes: atomicAdd(acc + r, (double)t); break;
+    case kMinPlus: atomic_min_double(acc + r, (double)t); break;
+    case kMaxTimes: atomic_max_double(acc + r, (double)t); break;
+    default: break;
+  }
+  const unsigned bit = 1u << (r & 31);
+  if (!(__ldcg(bits + (r >> 5)) & bit)) atomicOr(bits + (r >> 5), bit);
+}
+
 __global__ void __launch_bounds__(kExpandThreads)
 expand_accumulate(int sr, int xnnz, const int *__restrict__ xind, const float *__restrict__ xval,
                   const int *__restrict__ ptr, const int *__restrict__ ind,
-                  const float *__restrict__ val, double *acc, unsigned *bits) {
-  // warp per frontier entry, coalesced over its column; lanes combine into acc
+                  const float *__restrict__ val, double *acc, unsigned *bits, int *big,
+                  unsigned *nbig, int *hub, unsigned *nhub) {
   const int lane = lane_id();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
-  for (int j = gwarp; j < xnnz; j += nwarps) {
-    int c = xind[j];
-    int s = __ldg(ptr + c), e = __ldg(ptr + c + 1);
-    float xv = xval ? xval[j] : 1.0f;
-    for (int k = s + lane; k < e; k += 32) {
-      int r = __ldg(ind + k);
-      float t = sr_term(sr, val ? __ldg(val + k) : 1.0f, xv);
-      switch (sr) {
-        case kPlusTimes: atomicAdd(acc + r, (double)t); break;
-        case kMinPlus: atomic_min_double(acc + r, (double)t); break;
-        case kMaxTimes: atomic_max_double(acc + r, (double)t); break;
-        default: break;
-      }
-      unsigned bit = 1u << (r & 31);
-      if (!(__ldcg(bits + (r >> 5)) & bit)) atomicOr(bits + (r >> 5), bit);
+  for (int base = gwarp * 32; base < xnnz; base += nwarps * 32) {
+    const int j = base + lane;
+    int s = 0, d = 0;
+    float xv = 0.f;
+    bool isbig = false;
+    if (j < xnnz) {
+      const int c = xind[j];
+      s = __ldg(ptr + c);
+      d = __ldg(ptr + c + 1) - s;
+      xv = xval ? xval[j] : 1.0f;
+      if (d > kBigDeg) isbig = true;
     }
+    const bool ishub = isbig && d > kHubDeg;
+    const bool ismid = isbig && !ishub;
+    unsigned slot = warp_append(ismid, nbig);
+    if (ismid) big[slot] = j;
+    slot = warp_append(ishub, nhub);
+    if (ishub) hub[slot] = j;
+    if (isbig) d = 0;
+    const int incl = warp_incl_scan(d);
+    const int excl = incl - d;
+    const int total = __shfl_sync(kFull, incl, 31);
+    for (int e0 = 0; e0 < total; e0 += 32) {
+      const int e = e0 + lane;
+      const int owner = warp_owner(excl, e);
+      const int so = __shfl_sync(kFull, s, owner);
+      const int eo = __shfl_sync(kFull, excl, owner);
+      const float xo = __shfl_sync(kFull, xv, owner);
+      if (e < total) {
+        const int k = so + (e - eo);
+        accumulate_one(sr, __ldg(ind + k), sr_term(sr, val ? __ldg(val + k) : 1.0f, xo), acc,
+                       bits);
+      }
+    }
+  }
+}
+
+// The listed long columns: a warp per column of the medium list, then every
+// thread of the grid strides every hub (a hub's edges spread over all SMs).
+__global__ void __launch_bounds__(kExpandThreads)
+expand_accumulate_big(int sr, const int *__restrict__ xind, const float *__restrict__ xval,
+                      const int *__restrict__ ptr, const int *__restrict__ ind,
+                      const float *__restrict__ val, const int *big, const unsigned *nbig,
+                      const int *hub, const unsigned *nhub, double *acc, unsigned *bits) {
+  const int lane = lane_id();
+  const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  const unsigned nb = *nbig;
+  for (unsigned b = gwarp; b < nb; b += nwarps) {
+    const int j = big[b];
+    const int c = xind[j];
+    const int s = __ldg(ptr + c), e = __ldg(ptr + c + 1);
+    const float xv = xval ? xval[j] : 1.0f;
+    // four index / value loads in flight per lane before their atomics
+    int k = s + lane;
+    for (; k + 96 < e; k += 128) {
+      int r[4];
+      float a[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        r[q] = __ldg(ind + k + 32 * q);
+        a[q] = val ? __ldg(val + k + 32 * q) : 1.0f;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) accumulate_one(sr, r[q], sr_term(sr, a[q], xv), acc, bits);
+    }
+    for (; k < e; k += 32)
+      accumulate_one(sr, __ldg(ind + k), sr_term(sr, val ? __ldg(val + k) : 1.0f, xv), acc,
+                     bits);
+  }
+  const unsigned nh = *nhub;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  for (unsigned b = 0; b < nh; ++b) {
+    const int j = hub[b];
+    const int c = xind[j];
+    const int s = __ldg(ptr + c), e = __ldg(ptr + c + 1);
+    const float xv = xval ? xval[j] : 1.0f;
+    for (int k = s + tid; k < e; k += nthreads)
+      accumulate_one(sr, __ldg(ind + k), sr_term(sr, val ? __ldg(val + k) : 1.0f, xv), acc,
+                     bits);
   }
 }
 
@@ -306,11 +414,19 @@ int spmspv_core(apspie_context *ctx, int sr, int m, const int *ptr, const int *i
     unsigned *bits = (unsigned *)workspace(ctx, kSlotBitmap, sizeof(unsigned) * (size_t)(2 * words + 2));
     if (!acc || !bits) return APSPIE_ERR_OOM;
     unsigned *woffs = bits + words + 1;
+    int *big = (int *)workspace(ctx, kSlotMisc2, sizeof(int) * 2 * (size_t)(xnnz + 1));
+    if (!big) return APSPIE_ERR_OOM;
+    int *hub = big + xnnz + 1;
+    cudaMemsetAsync(&sm->nbig, 0, sizeof(unsigned), st);
+    cudaMemsetAsync(&sm->nhub, 0, sizeof(unsigned), st);
     acc_init<<<grid_for(ctx, m, 256), 256, 0, st>>>(sr, m, acc, bits);
-    expand_accumulate<<<ctx->num_sms * 8, kExpandThreads, 0, st>>>(sr, xnnz, xind, xval, ptr, ind,
-                                                                   val, acc, bits);
+    expand_accumulate<<<grid_for(ctx, (long long)xnnz * 32, kExpandThreads), kExpandThreads, 0,
+                        st>>>(sr, xnnz, xind, xval, ptr, ind, val, acc, bits, big, &sm->nbig,
+                              hub, &sm->nhub);
+    expand_accumulate_big<<<ctx->num_sms * 4, kExpandThreads, 0, st>>>(
+        sr, xind, xval, ptr, ind, val, big, &sm->nbig, hub, &sm->nhub, acc, bits);
     bitmap_counts<<<grid_for(ctx, words, 256), 256, 0, st>>>(bits, words, woffs);
-    int rc = check_launch(ctx, "spmspv bitmap", 3);
+    int rc = check_launch(ctx, "spmspv bitmap", 4);
     if (rc) return rc;
     rc = device_exclusive_scan<unsigned>(ctx, woffs, woffs, words, (unsigned *)d_ynnz);
     if (rc) return rc;
@@ -322,14 +438,16 @@ int spmspv_core(apspie_context *ctx, int sr, int m, const int *ptr, const int *i
   int *kb = (int *)workspace(ctx, kSlotSortKeysB, sizeof(int) * (size_t)E);
   float *va = (float *)workspace(ctx, kSlotSortValsA, sizeof(float) * (size_t)E);
   float *vb = (float *)workspace(ctx, kSlotSortValsB, sizeof(float) * (size_t)E);
-  int *big = (int *)workspace(ctx, kSlotMisc2, sizeof(int) * (size_t)(xnnz + 1));
+  int *big = (int *)workspace(ctx, kSlotMisc2, sizeof(int) * 2 * (size_t)(xnnz + 1));
   unsigned *nbig = &sm->nbig;
   if (!ka || !kb || !va || !vb || !big) return APSPIE_ERR_OOM;
+  int *hub = big + xnnz + 1;
   cudaMemsetAsync(nbig, 0, sizeof(unsigned), st);
+  cudaMemsetAsync(&sm->nhub, 0, sizeof(unsigned), st);
   expand_pairs<<<grid_for(ctx, (long long)xnnz * 32, kExpandThreads), kExpandThreads, 0, st>>>(
-      sr, xnnz, xind, xval, ptr, ind, val, offs, ka, va, big, nbig);
-  expand_big<<<ctx->num_sms * 2, 512, 0, st>>>(sr, xind, xval, ptr, ind, val, offs, big, nbig, ka,
-                                               va);
+      sr, xnnz, xind, xval, ptr, ind, val, offs, ka, va, big, nbig, hub, &sm->nhub);
+  expand_big<<<ctx->num_sms * 4, kExpandThreads, 0, st>>>(sr, xind, xval, ptr, ind, val, offs,
+                                                          big, nbig, hub, &sm->nhub, ka, va);
   int rc = check_launch(ctx, "expand_pairs", 2);
   if (rc) return rc;
   bool in_b = false;
