@@ -8,16 +8,24 @@
 // joins when its priority beats that maximum (updateMis :64), and the
 // neighbours of joiners leave (updateNeighbor :71) -- with a full D->H copy of
 // the candidate vector every round (:240).  Here one persistent kernel runs
-// the rounds with two phases each, separated by a bounded grid barrier:
-//   A: every candidate v scans its neighbours; it is beaten by an undecided
-//      neighbour of larger key; unbeaten candidates mark themselves JOIN.
-//      (This is the max-priority SpMSpV with the comparison fused in.)
-//   B: undecided vertices next to a JOIN or IN vertex leave (OUT); JOIN
-//      vertices become IN; survivors are compacted into the next queue.
+// the rounds, one pass and one bounded grid barrier each: every undecided
+// vertex v scans its neighbours' states (the max-priority SpMSpV with the
+// comparison fused in) and
+//   * leaves (OUT) when a neighbour is IN;
+//   * else joins (IN), if it is a candidate of the round, when no
+//     neighbour of larger key is still undecided, and at once marks its
+//     undecided neighbours OUT (they would leave next round anyway; doing
+//     it now lets their other neighbours decide a round earlier);
+//   * else stays, and is compacted into the next round's queue (a queued
+//     vertex marked OUT meanwhile is dropped next round).
+// States change in place during the pass, so a neighbour's state may be
+// read before or after its own update in the same pass; the stale value is
+// always "undecided" (IN and OUT are final), which only delays a decision.
+// v is IN exactly when no neighbour of larger key is IN, so the set is the
+// greedy MIS in descending key order for any delta, whatever the timing.
 // key(v) = (prio[v] << 32) | v, so ties in priority go to the larger id and
-// every round admits at least the undecided vertex of largest key.  The set
-// is the greedy MIS in descending key order for any delta.  Self-loops are
-// ignored.  Work per round is spread over warps with the same scan-based
+// every round decides at least the undecided vertex of largest key.
+// Self-loops are ignored.  Work per round is spread over warps with the same scan-based
 // edge dealing as the traversal kernels; a per-warp shared flag array
 // collects the per-vertex OR of the edge predicates.
 #include <cuda_runtime.h>
@@ -31,7 +39,7 @@ namespace apspie {
 namespace {
 
 constexpr int kMisThreads = 512;
-constexpr int kUndecided = -1, kOut = 0, kIn = 1, kJoin = 2;
+constexpr int kUndecided = -1, kOut = 0, kIn = 1;
 
 struct MisState {
   unsigned q[3];  // queue lengths, rotating
@@ -58,14 +66,14 @@ __global__ void mis_init(int m, int32_t *state, int *queue, MisState *st) {
   }
 }
 
-// Deals the edges of 32 queued vertices to the lanes of a warp.  pred(v, u)
-// is evaluated per edge (v = owner vertex, u = neighbour); the returned mask
-// has bit j set when pred held for some edge of the warp's j-th vertex.
-template <typename Pred>
-__device__ __forceinline__ unsigned warp_any_edge(int v, int s, int d, const int *__restrict__ ind,
-                                                  volatile unsigned *flags, Pred pred) {
+// Deals the edges of 32 queued vertices to the lanes of a warp.  code(v, u)
+// is evaluated per edge (v = owner vertex, u = neighbour); lane j gets the
+// OR of the codes over the edges of the warp's j-th vertex.
+template <typename Code>
+__device__ __forceinline__ unsigned warp_or_edges(int v, int s, int d, const int *__restrict__ ind,
+                                                  unsigned *flags, Code code) {
   const int lane = lane_id();
-  flags[lane] = 0;
+  flags[lane] = 0u;
   __syncwarp();
   int incl = warp_incl_scan(d);
   int excl = incl - d;
@@ -77,13 +85,15 @@ __device__ __forceinline__ unsigned warp_any_edge(int v, int s, int d, const int
     int eo = __shfl_sync(kFull, excl, owner);
     int vo = __shfl_sync(kFull, v, owner);
     if (e < total) {
-      int u = __ldg(ind + so + (e - eo));
-      if (pred(vo, u)) flags[owner] = 1u;
+      const unsigned c = code(vo, __ldg(ind + so + (e - eo)));
+      if (c) atomicOr(flags + owner, c);
     }
   }
   __syncwarp();
-  return __ballot_sync(kFull, flags[lane] != 0);
+  return flags[lane];
 }
+
+constexpr unsigned kHitIn = 1u, kHitLarger = 2u;
 
 __global__ void __launch_bounds__(kMisThreads)
 mis_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
@@ -92,9 +102,9 @@ mis_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
   const int lane = lane_id();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
-  __shared__ volatile unsigned s_flags[kMisThreads];
+  __shared__ unsigned s_flags[kMisThreads];
   __shared__ unsigned s_q;
-  volatile unsigned *flags = s_flags + 32 * warp_in_block();
+  unsigned *flags = s_flags + 32 * warp_in_block();
   int r = 0;
   for (;; ++r) {
     if (threadIdx.x == 0) {
@@ -109,55 +119,41 @@ mis_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
     unsigned long long thr = level <= 0.0 ? 0ull : (unsigned long long)(level * 4294967296.0);
     const int *qin = (r & 1) ? qb : qa;
     int *qout = (r & 1) ? qa : qb;
-
-    // ---- phase A: unbeaten candidates mark JOIN ----
     for (unsigned base = (unsigned)gwarp * 32u; base < nq; base += (unsigned)nwarps * 32u) {
-      unsigned idx = base + lane;
+      const unsigned idx = base + lane;
       int v = -1, s = 0, d = 0;
-      bool cand = false;
       if (idx < nq) {
         v = __ldcg(qin + idx);
-        cand = (thr == 0ull) || ((unsigned long long)__ldg(prio + v) >= thr);
-        if (cand) {
+        if (__ldcg(state + v) == kUndecided) {
           s = __ldg(ptr + v);
           d = __ldg(ptr + v + 1) - s;
+        } else {
+          v = -1;  // marked OUT by a neighbour that joined after it was queued
         }
       }
-      unsigned beaten = warp_any_edge(v, s, d, ind, flags, [&](int vo, int u) {
-        if (u == vo) return false;
-        int su = __ldcg(state + u);
-        return (su == kUndecided || su == kJoin) && mis_key(prio, u) > mis_key(prio, vo);
+      const unsigned hit = warp_or_edges(v, s, d, ind, flags, [&](int vo, int u) -> unsigned {
+        if (u == vo) return 0u;
+        const int su = __ldcg(state + u);
+        if (su == kIn) return kHitIn;
+        return (su == kUndecided && mis_key(prio, u) > mis_key(prio, vo)) ? kHitLarger : 0u;
       });
-      if (cand && !((beaten >> lane) & 1u)) state[v] = kJoin;
-    }
-    if (!grid_barrier(st->bar, &st->err)) return;
-
-    // ---- phase B: neighbours of joiners leave, joiners enter ----
-    for (unsigned base = (unsigned)gwarp * 32u; base < nq; base += (unsigned)nwarps * 32u) {
-      unsigned idx = base + lane;
-      int v = -1, s = 0, d = 0, sv = kOut;
-      if (idx < nq) {
-        v = __ldcg(qin + idx);
-        sv = __ldcg(state + v);
-        if (sv == kUndecided) {
-          s = __ldg(ptr + v);
-          d = __ldg(ptr + v + 1) - s;
-        }
-      }
-      unsigned hit = warp_any_edge(v, s, d, ind, flags, [&](int vo, int u) {
-        return u != vo && __ldcg(state + u) >= kIn;
-      });
-      bool survive = false;
+      bool survive = false, joined = false;
       if (v >= 0) {
-        if (sv == kJoin) {
+        const bool cand = (thr == 0ull) || ((unsigned long long)__ldg(prio + v) >= thr);
+        if (hit & kHitIn) {
+          state[v] = kOut;
+        } else if (cand && !(hit & kHitLarger)) {
           state[v] = kIn;
-        } else if (sv == kUndecided) {
-          if ((hit >> lane) & 1u)
-            state[v] = kOut;
-          else
-            survive = true;
+          joined = true;
+        } else {
+          survive = true;
         }
       }
+      if (__ballot_sync(kFull, joined))
+        warp_or_edges(v, s, joined ? d : 0, ind, flags, [&](int vo, int u) -> unsigned {
+          if (u != vo && __ldcg(state + u) == kUndecided) state[u] = kOut;
+          return 0u;
+        });
       unsigned slot = warp_append(survive, &st->q[(r + 1) % 3]);
       if (survive) qout[slot] = v;
     }
