@@ -83,6 +83,9 @@ PROTOS: dict[str, tuple] = {
     "apspie_sssp_set_params": (c_int, [vp, c_u32, c_f32]),
     "apspie_sssp_get_trace": (c_int, [vp, c_int, P_int, vp, vp, vp, vp]),
     "apspie_sssp_get_stats": (c_int, [vp, C.POINTER(SsspStats)]),
+    "apspie_sssp_u32_pull": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, vp, vp, vp, c_int]),
+    "apspie_sssp_f32_pull": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, vp, vp, vp, c_int]),
+    "apspie_sssp_set_pull": (c_int, [vp, c_int]),
     "apspie_mis": (c_int, [vp, c_i64, c_int, vp, vp, vp, vp, c_f32]),
     "apspie_mis_get_rounds": (c_int, [vp, P_int]),
     "apspie_neighbor_flags": (c_int, [vp, c_i64, c_int, vp, vp, vp, vp]),
@@ -109,6 +112,7 @@ PROTOS: dict[str, tuple] = {
                                        C.POINTER(C.c_double)]),
     "apspie_server_create": (c_int, [c_int, C.c_size_t, c_int, P_vp]),
     "apspie_server_add_graph": (c_int, [vp, c_int, c_i64, vp, vp, vp, vp, vp, c_int, P_int]),
+    "apspie_server_set_sssp_in": (c_int, [vp, c_int, vp, vp, vp]),
     "apspie_server_submit": (c_int, [vp, c_int, c_int, c_int, c_u32, vp, P_u64]),
     "apspie_server_submit_device": (c_int, [vp, c_int, c_int, c_int, c_u32, vp, P_u64]),
     "apspie_server_replay": (c_int, [vp, c_int, vp, c_int, vp, C.POINTER(C.c_double)]),

@@ -84,7 +84,25 @@ struct GraphEntry {
   int symmetric;
   bool deep;
   float cost_ms[3];  // running estimate of one group's device time, per kind
+  // in-adjacency with its weights for push/pull SSSP (apspie_server_set_sssp_in)
+  const int *stptr = nullptr, *stind = nullptr;
+  const uint32_t *stw = nullptr;
 };
+
+// SSSP groups on graphs with more edges than this run their queries one by
+// one through the single-source kernel: the multi-source rows share little
+// there (R-MAT 22, 8 sources: 56 ms batched, 37 ms one by one with pull
+// rounds, measured), while on smaller graphs the batch wins.
+constexpr int64_t kSsspBatchMaxNnz = 64ll << 20;
+
+// One SSSP query through the single-source kernel, push/pull when the
+// graph's in-adjacency with weights was registered.
+int sssp_one(apspie_ctx ctx, const GraphEntry &ge, int src, uint32_t *out) {
+  if (ge.stptr)
+    return apspie_sssp_u32_pull(ctx, src, ge.nnz, ge.m, ge.ptr, ge.ind, ge.w, ge.stptr, ge.stind,
+                                ge.stw, out, 0);
+  return apspie_sssp_u32(ctx, src, ge.nnz, ge.m, ge.ptr, ge.ind, ge.w, out, 0);
+}
 
 struct Group {
   int kind = 0, graph = 0, lane = 0;
@@ -324,8 +342,12 @@ int launch_group(apspie_server *s, Slot &sl, Group &g) {
       const int *ti = ge.tptr ? ge.tind : (ge.symmetric ? ge.ind : nullptr);
       st = apspie_bfs(ln.ctx, r->source, ge.nnz, ge.m, ge.ptr, ge.ind, tp, ti, out, 0);
     } else {
-      st = apspie_sssp_u32(ln.ctx, r->source, ge.nnz, ge.m, ge.ptr, ge.ind, ge.w,
-                           (uint32_t *)out, 0);
+      st = sssp_one(ln.ctx, ge, r->source, (uint32_t *)out);
+    }
+  } else if (g.kind == 1 && ge.nnz > kSsspBatchMaxNnz) {
+    for (Request *r : g.reqs) {
+      st = sssp_one(ln.ctx, ge, r->source, (uint32_t *)((char *)sl.d_out + r->dev_off));
+      if (st != APSPIE_OK) break;
     }
   } else {
     std::vector<int> src;
@@ -564,6 +586,7 @@ int apspie_server_add_graph(apspie_server_t s, int m, int64_t nnz, const int *d_
   if (!s || m <= 0 || nnz < 0 || !d_ptr || (nnz > 0 && !d_ind) || !graph_id)
     return APSPIE_ERR_INVALID;
   GraphEntry g{m, nnz, d_ptr, d_ind, d_tptr, d_tind, d_w, symmetric, false, {0, 0, 0}};
+  g.stptr = nullptr;
   int levels = 0;
   int st = probe_levels(s->device, g, &levels);
   if (st != APSPIE_OK) return st;
@@ -576,6 +599,19 @@ int apspie_server_add_graph(apspie_server_t s, int m, int64_t nnz, const int *d_
   s->graphs.push_back(g);
   if (g.deep) s->any_deep = true;
   *graph_id = (int)s->graphs.size() - 1;
+  return APSPIE_OK;
+}
+
+int apspie_server_set_sssp_in(apspie_server_t s, int graph, const int *d_tptr,
+                              const int *d_tind, const uint32_t *d_tw) {
+  if (!s || !d_tptr) return APSPIE_ERR_INVALID;
+  std::lock_guard<std::mutex> lock(s->mu);
+  if (graph < 0 || graph >= (int)s->graphs.size()) return APSPIE_ERR_INVALID;
+  GraphEntry &g = s->graphs[graph];
+  if (g.nnz > 0 && (!d_tind || !d_tw)) return APSPIE_ERR_INVALID;
+  g.stptr = d_tptr;
+  g.stind = d_tind;
+  g.stw = d_tw;
   return APSPIE_OK;
 }
 
@@ -734,7 +770,7 @@ int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q, 
       const int *tp = g.symmetric ? g.ptr : g.tptr, *ti = g.symmetric ? g.ind : g.tind;
       st = apspie_bfs(ctx, q[i].source, g.nnz, g.m, g.ptr, g.ind, tp, ti, row, 0);
     } else if (q[i].type == 1) {
-      st = apspie_sssp_u32(ctx, q[i].source, g.nnz, g.m, g.ptr, g.ind, g.w, (uint32_t *)row, 0);
+      st = sssp_one(ctx, g, q[i].source, (uint32_t *)row);
     } else {
       uint32_t *prio = nullptr;
       st = get_prio(s, q[i].graph, q[i].seed, stream, &prio);

@@ -20,6 +20,16 @@
 // Bellman-Ford, fewer rounds, more relaxations -- better on high-diameter
 // graphs).  The schedule only changes the order of relaxations.
 //
+// Pull rounds (apspie_sssp_*_pull, given the in-adjacency with its weights,
+// near-far off): a round whose frontier's out-edges exceed nnz / alpha
+// scans every in-edge instead -- each vertex takes the minimum of
+// d[u] + w(u,v) over its in-neighbours u in the frontier (stamp of the
+// previous round or this one) and writes its own distance, with no
+// atomics; vertices of more than kHubIn in-edges are split into chunks of
+// kPullChunk edges whose minima go through atomicMin.  Improved vertices
+// are queued as in a push round, so either direction may follow.  The
+// relaxations are the same min-plus steps, so the fixpoint is the same.
+//
 // Distances are kept as 32-bit words: uint32 sums for integer weights, and
 // the IEEE bit pattern for float weights -- non-negative floats order like
 // their bit patterns, so atomicMin on the word is min on the value.  Each
@@ -40,6 +50,8 @@ namespace apspie {
 namespace {
 
 constexpr int kSsspThreads = 512;
+constexpr int kHubIn = 1024;      // in-degree above which a pull round splits a vertex
+constexpr int kPullChunk = 1024;  // in-edges per chunk of such a vertex
 
 constexpr int kSsspTraceRounds = 64;  // rounds recorded in the per-run trace
 
@@ -59,7 +71,7 @@ struct SsspState {
   int err;
   int rounds;
   int phases;
-  int pad;
+  unsigned nhc;  // chunks of the high in-degree vertices (pull rounds)
   unsigned long long relaxations;  // edges scanned over all rounds
   unsigned long long reached;
   unsigned long long edges;        // sum of out-degrees of reached vertices
@@ -171,10 +183,24 @@ __global__ void sssp_init(int m, int src, unsigned *dist, int *stamp, int *fstam
       st->err = 0;
       st->rounds = 0;
       st->phases = 0;
+      st->nhc = 0;
       for (int i = 0; i < kSsspTraceRounds; ++i) st->trace[i] = RoundTrace{0, 0, 0ull, 0ull, 0ull};
       st->relaxations = 0;
       st->reached = 0;
       st->edges = 0;
+    }
+  }
+}
+
+// Lists the (vertex, chunk) units of the vertices with more than kHubIn
+// in-edges for the pull rounds (runs after sssp_init, which zeroes nhc).
+__global__ void sssp_hub_chunks(int m, const int *__restrict__ tptr, int2 *hubc, SsspState *st) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < m; v += gridDim.x * blockDim.x) {
+    const int d = __ldg(tptr + v + 1) - __ldg(tptr + v);
+    if (d > kHubIn) {
+      const unsigned nc = (unsigned)((d + kPullChunk - 1) / kPullChunk);
+      const unsigned at = atomicAdd(&st->nhc, nc);
+      for (unsigned c = 0; c < nc; ++c) hubc[at + c] = make_int2(v, (int)c);
     }
   }
 }
@@ -184,12 +210,15 @@ __global__ void __launch_bounds__(kSsspThreads, 2)
 sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
                 const W *__restrict__ w, unsigned *dist, int *stamp, int *qa, int *qb, int2 *ca,
                 int2 *cb, SsspState *st, int max_rounds, int *fstamp, unsigned *xd, int *far0,
-                int *far1, int *far2, unsigned delta) {
+                int *far1, int *far2, unsigned delta, long long nnz, const int *__restrict__ tptr,
+                const int *__restrict__ tind, const W *__restrict__ tw, const int2 *hubc,
+                int alpha) {
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
   const int lane = lane_id();
   __shared__ unsigned s_q, s_chunks, s_nbig, s_far;
   __shared__ unsigned long long s_edges;
+  __shared__ unsigned s_best[kSsspThreads / 32][32];
   unsigned long long relax = 0;
   // T = infinity without near-far; else the first phase covers [0, delta)
   if (blockIdx.x == 0 && threadIdx.x == 0) st->t_start = globaltimer();
@@ -256,6 +285,99 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
       if (!grid_barrier(st->bar, &st->err)) return;
       continue;
     }
+    if (tptr && delta == 0u && r > 0 && alpha > 0 &&
+        (long long)s_edges * alpha > nnz) {
+      // ---- pull round: every vertex takes the least d[u] + w over its
+      // in-neighbours in the frontier; hub chunks and 32-vertex groups are
+      // handed out by the round's counter ----
+      relax += (unsigned long long)nnz;
+      LevelCounters *nx = nxt;
+      DiscoverAcc acc;
+      const int warp = warp_in_block();
+      const unsigned ngroups = (unsigned)((m + 31) / 32);
+      const unsigned nhc = __ldcg(&st->nhc);
+      for (;;) {
+        unsigned unit = 0;
+        if (lane == 0) unit = atomicAdd(&cur->grab, 1u);
+        unit = __shfl_sync(kFull, unit, 0);
+        if (unit >= nhc + ngroups) break;
+        if (unit < nhc) {
+          const int2 hc = hubc[unit];
+          const int v = hc.x;
+          const int a0 = __ldg(tptr + v) + hc.y * kPullChunk;
+          const int a1 = min(__ldg(tptr + v + 1), a0 + kPullChunk);
+          unsigned best = Arith<W>::kInf;
+          for (int k = a0 + lane; k < a1; k += 32) {
+            const int u = __ldg(tind + k);
+            if (__ldcg(stamp + u) >= r - 1) {
+              const unsigned du = __ldcg(dist + u);
+              if (du != Arith<W>::kInf) best = min(best, Arith<W>::add(du, __ldg(tw + k)));
+            }
+          }
+          best = __reduce_min_sync(kFull, best);
+          bool f[1] = {false};
+          if (lane == 0 && best < __ldcg(dist + v)) {
+            const unsigned old = atomicMin(dist + v, best);
+            if (best < old) f[0] = atomicExch(stamp + v, r) != r;
+          }
+          int uu[1] = {v};
+          discover_n<1>(f, uu, ptr, qout, cout, nx, acc);
+        } else {
+          const int v = (int)((unit - nhc) * 32u) + lane;
+          int s = 0, d = 0;
+          if (v < m) {
+            s = __ldg(tptr + v);
+            d = __ldg(tptr + v + 1) - s;
+            if (d > kHubIn) d = 0;  // its chunks are separate units
+          }
+          s_best[warp][lane] = Arith<W>::kInf;
+          __syncwarp();
+          const int incl = warp_incl_scan(d);
+          const int excl = incl - d;
+          const int total = __shfl_sync(kFull, incl, 31);
+          for (int e0 = 0; e0 < total; e0 += 32) {
+            const int e = e0 + lane;
+            const int owner = warp_owner(excl, e);
+            const int so = __shfl_sync(kFull, s, owner);
+            const int eo = __shfl_sync(kFull, excl, owner);
+            if (e < total) {
+              const int k = so + (e - eo);
+              const int u = __ldg(tind + k);
+              if (__ldcg(stamp + u) >= r - 1) {
+                const unsigned du = __ldcg(dist + u);
+                if (du != Arith<W>::kInf)
+                  atomicMin(&s_best[warp][owner], Arith<W>::add(du, __ldg(tw + k)));
+              }
+            }
+          }
+          __syncwarp();
+          const unsigned best = s_best[warp][lane];
+          bool f[1] = {false};
+          if (v < m && d > 0 && best < __ldcg(dist + v)) {
+            // only this lane writes v in a pull round (hubs are the chunk units)
+            dist[v] = best;
+            stamp[v] = r;
+            f[0] = true;
+          }
+          int uu[1] = {v < m ? v : 0};
+          discover_n<1>(f, uu, ptr, qout, cout, nx, acc);
+        }
+      }
+      flush_acc(acc, nx);
+      if (r < kSsspTraceRounds) {
+        __syncthreads();
+        if (threadIdx.x == 0) atomicMax(&st->trace[r].t_last, globaltimer());
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+          st->trace[r].frontier = nq + s_nbig;
+          st->trace[r].phase = 0xffffffffu;  // marks a pull round
+          st->trace[r].edges = s_edges;
+        }
+      }
+      if (!grid_barrier(st->bar, &st->err)) return;
+      if (r < kSsspTraceRounds && blockIdx.x == 0 && threadIdx.x == 0)
+        st->trace[r].t_end = globaltimer();
+      continue;
+    }
     relax += s_edges;
     int *qin = (r & 1) ? qb : qa;
     int2 *cin = (r & 1) ? cb : ca;
@@ -320,13 +442,15 @@ int sssp_grid(apspie_context *ctx) {
 
 template <typename W>
 int sssp_run(apspie_context *ctx, int src, int64_t nnz, int m, const int *d_ptr, const int *d_ind,
-             const W *d_w, unsigned *d_dist, int max_rounds, unsigned delta) {
+             const W *d_w, unsigned *d_dist, int max_rounds, unsigned delta,
+             const int *d_tptr = nullptr, const int *d_tind = nullptr, const W *d_tw = nullptr) {
   APSPIE_CHECK_CTX(ctx);
   if (m <= 0 || src < 0 || src >= m)
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_sssp: src %d outside [0,%d)", src, m);
   if (nnz < 0 || nnz >= (int64_t)INT32_MAX)
     return set_error(ctx, APSPIE_ERR_OVERFLOW, "apspie_sssp: nnz exceeds int32 offsets");
-  if (!d_ptr || !d_dist || (nnz > 0 && (!d_ind || !d_w)))
+  if (!d_ptr || !d_dist || (nnz > 0 && (!d_ind || !d_w)) ||
+      (d_tptr && nnz > 0 && (!d_tind || !d_tw)))
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_sssp: null pointer");
   size_t cap = chunk_capacity(nnz);
   auto *st = (SsspState *)workspace(ctx, kSlotSsspState, sizeof(SsspState));
@@ -349,9 +473,21 @@ int sssp_run(apspie_context *ctx, int src, int64_t nnz, int m, const int *d_ptr,
                                                    ca, st);
   int rc = check_launch(ctx, "sssp_init");
   if (rc) return rc;
+  int2 *hubc = nullptr;
+  if (d_tptr) {
+    hubc = (int2 *)workspace(ctx, kSlotSsspHubs,
+                             sizeof(int2) * ((size_t)nnz / kPullChunk + (size_t)nnz / kHubIn + 1));
+    if (!hubc) return APSPIE_ERR_OOM;
+    sssp_hub_chunks<<<init_grid, 256, 0, ctx->stream>>>(m, d_tptr, hubc, st);
+    rc = check_launch(ctx, "sssp_hub_chunks");
+    if (rc) return rc;
+  }
+  long long nnz_ll = nnz;
+  int alpha = d_tptr ? ctx->sssp_pull_alpha : 0;
   void *args[] = {&m,  (void *)&d_ptr, (void *)&d_ind, (void *)&d_w, &d_dist, &stamp,
                   &qa, &qb,            &ca,            &cb,           &st,     &max_rounds,
-                  &fstamp, &xd, &far0, &far1, &far2, &delta};
+                  &fstamp, &xd, &far0, &far1, &far2, &delta, &nnz_ll, (void *)&d_tptr,
+                  (void *)&d_tind, (void *)&d_tw, &hubc, &alpha};
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)sssp_persistent<W>, dim3(grid),
                                               dim3(kSsspThreads), args, 0, ctx->stream);
   if (e != cudaSuccess) return check_cuda(ctx, e, "sssp_persistent");
@@ -379,6 +515,33 @@ int apspie_sssp_f32(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_pt
   std::memcpy(&bits, &df, sizeof(bits));
   return sssp_run<float>(ctx, src, nnz, m, d_ptr, d_ind, d_w, (unsigned *)d_dist, max_rounds,
                          df > 0.0f ? bits : 0u);
+}
+
+int apspie_sssp_u32_pull(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
+                         const int *d_ind, const uint32_t *d_w, const int *d_tptr,
+                         const int *d_tind, const uint32_t *d_tw, uint32_t *d_dist,
+                         int max_rounds) {
+  if (!d_tptr) return set_error(ctx, APSPIE_ERR_INVALID, "apspie_sssp_u32_pull: no in-adjacency");
+  return sssp_run<uint32_t>(ctx, src, nnz, m, d_ptr, d_ind, d_w, d_dist, max_rounds,
+                            ctx->sssp_delta_u32, d_tptr, d_tind, d_tw);
+}
+
+int apspie_sssp_f32_pull(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
+                         const int *d_ind, const float *d_w, const int *d_tptr,
+                         const int *d_tind, const float *d_tw, float *d_dist, int max_rounds) {
+  if (!d_tptr) return set_error(ctx, APSPIE_ERR_INVALID, "apspie_sssp_f32_pull: no in-adjacency");
+  float df = ctx->sssp_delta_f32;
+  unsigned bits = 0;
+  std::memcpy(&bits, &df, sizeof(bits));
+  return sssp_run<float>(ctx, src, nnz, m, d_ptr, d_ind, d_w, (unsigned *)d_dist, max_rounds,
+                         df > 0.0f ? bits : 0u, d_tptr, d_tind, d_tw);
+}
+
+int apspie_sssp_set_pull(apspie_ctx ctx, int alpha) {
+  APSPIE_CHECK_CTX(ctx);
+  if (alpha < 0) return set_error(ctx, APSPIE_ERR_INVALID, "apspie_sssp_set_pull: alpha < 0");
+  ctx->sssp_pull_alpha = alpha;
+  return APSPIE_OK;
 }
 
 int apspie_sssp_set_params(apspie_ctx ctx, uint32_t delta_u32, float delta_f32) {

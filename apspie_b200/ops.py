@@ -169,9 +169,38 @@ def sssp(ctx: Context, g, src: int, dist=None, weights: str = "u32", max_rounds:
         raise ValueError(weights)
     if w is None:
         raise ValueError(f"graph has no {weights} weights")
+    tin = g.extra.get("sssp_in", {}).get(weights)
+    if tin is not None:
+        # in-adjacency with its weights from sssp_prepare: push/pull rounds
+        tptr, tind, tw = tin
+        pfn = lib.apspie_sssp_u32_pull if weights == "u32" else lib.apspie_sssp_f32_pull
+        check(pfn(ctx.handle, int(src), int(g.nnz), int(g.m), _p(g.ptr), _p(g.ind), _p(w),
+                  _p(tptr), _p(tind), _p(tw), _p(dist), int(max_rounds)), ctx.handle,
+              "apspie_sssp_pull")
+        return dist
     check(fn(ctx.handle, int(src), int(g.nnz), int(g.m), _p(g.ptr), _p(g.ind), _p(w), _p(dist),
              int(max_rounds)), ctx.handle, "apspie_sssp")
     return dist
+
+
+def sssp_prepare(ctx: Context, g):
+    """In-adjacency of g with its edge weights (apspie_csr_transpose, one sort
+    per weight array present), kept on g; sssp() then runs push/pull rounds
+    over it (apspie_sssp_*_pull)."""
+    import torch
+    g.extra["sssp_in"] = {}
+    for kind, w in (("u32", g.w_u32), ("f32", g.w_f32)):
+        if w is None:
+            continue
+        # the transpose moves 32-bit words: uint32 weights travel as float bits
+        tptr, tind, tw = csr_transpose(ctx, g.m, g.m, g.ptr, g.ind, w.view(torch.float32))
+        g.extra["sssp_in"][kind] = (tptr, tind, tw.view(torch.int32) if kind == "u32" else tw)
+    return g
+
+
+def sssp_set_pull(ctx: Context, alpha: int = 3) -> None:
+    """Pull rounds when the frontier's out-edges * alpha exceed nnz (0: never)."""
+    check(lib.apspie_sssp_set_pull(ctx.handle, int(alpha)), ctx.handle, "apspie_sssp_set_pull")
 
 
 def sssp_stats(ctx: Context) -> dict:

@@ -33,6 +33,11 @@ class Server:
         check(lib.apspie_server_add_graph(self._h, int(g.m), int(g.nnz), p(g.ptr), p(g.ind),
                                           p(tptr), p(tind), p(g.w_u32), int(sym), C.byref(gid)),
               what="apspie_server_add_graph")
+        sin = getattr(g, "extra", {}).get("sssp_in", {}).get("u32")
+        if sin is not None:
+            # in-adjacency with weights from sssp_prepare: push/pull SSSP queries
+            check(lib.apspie_server_set_sssp_in(self._h, gid.value, p(sin[0]), p(sin[1]),
+                                                p(sin[2])), what="apspie_server_set_sssp_in")
         self._graphs.append(g)
         return gid.value
 

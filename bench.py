@@ -422,6 +422,10 @@ def serving_leg(ctx, rates=(1000, 100000), n_queries=600, seed=SEED):
     graphs.append(ap.gen_grid(1024, 1024).to_device())
     for g in graphs:
         ap.weights_device(ctx, g, seed=seed)
+        # graph build step: the in-adjacency with its weights for push/pull
+        # SSSP on the large R-MAT graphs (one transpose each)
+        if g.nnz > (16 << 20):
+            ap.sssp_prepare(ctx, g)
     torch.cuda.synchronize()
     ms = np.array([g.m for g in graphs], dtype=np.float64)
     degs = [(g.ptr[1:] - g.ptr[:-1]).cpu().numpy() for g in graphs]
@@ -429,7 +433,9 @@ def serving_leg(ctx, rates=(1000, 100000), n_queries=600, seed=SEED):
     out = {"graphs": [f"rmat{sc}" for sc in SERVE_SCALES] + ["grid1024"],
            "mix": "60% BFS / 30% SSSP / 10% MIS", "queries_per_rate": n_queries,
            "latency": "arrival -> result row in host memory (device -> pinned host copy included)",
-           "budget_gb": 120, "rates": []}
+           "budget_gb": 120, "rates": [],
+           "sssp_pull_graphs": [n for n, g in zip([f"rmat{sc}" for sc in SERVE_SCALES] + ["grid1024"],
+                                                  graphs) if "sssp_in" in g.extra]}
     with ap.Server(budget_bytes=120 << 30, max_batch=256) as srv:
         gids = [srv.add_graph(g) for g in graphs]
         # untimed warm-up of both paths: every (graph, kind) alone and in

@@ -169,6 +169,25 @@ int apspie_sssp_u32(apspie_ctx ctx, int src, int64_t nnz, int m,
 int apspie_sssp_f32(apspie_ctx ctx, int src, int64_t nnz, int m,
                     const int *d_ptr, const int *d_ind, const float *d_w,
                     float *d_dist, int max_rounds);
+/* The same, direction-optimising: given the in-adjacency with its weights
+ * (d_tptr / d_tind / d_tw, e.g. from apspie_csr_transpose with the weights
+ * as the values), a round whose frontier's out-edges times alpha exceed nnz
+ * (apspie_sssp_set_pull, default 3; 0 = never) scans every in-edge
+ * instead: each vertex takes the least d[u] + w(u,v) over its in-neighbours
+ * in the frontier and writes its own distance, without atomics.  Same
+ * results as apspie_sssp_u32 / _f32 (the same min-plus fixpoint); pull
+ * rounds are only taken with the near-far step at 0.  Replaces the same
+ * reference calls (src/sssp.cuh:28-115), whose every iteration scans all
+ * finite vertices' edges. */
+int apspie_sssp_u32_pull(apspie_ctx ctx, int src, int64_t nnz, int m,
+                         const int *d_ptr, const int *d_ind, const uint32_t *d_w,
+                         const int *d_tptr, const int *d_tind, const uint32_t *d_tw,
+                         uint32_t *d_dist, int max_rounds);
+int apspie_sssp_f32_pull(apspie_ctx ctx, int src, int64_t nnz, int m,
+                         const int *d_ptr, const int *d_ind, const float *d_w,
+                         const int *d_tptr, const int *d_tind, const float *d_tw,
+                         float *d_dist, int max_rounds);
+int apspie_sssp_set_pull(apspie_ctx ctx, int alpha);
 
 typedef struct {
   int32_t rounds;            /* frontier rounds run */
@@ -291,6 +310,11 @@ int apspie_server_add_graph(apspie_server_t s, int m, int64_t nnz,
                             const int *d_ptr, const int *d_ind,
                             const int *d_tptr, const int *d_tind,
                             const uint32_t *d_w, int symmetric, int *graph_id);
+/* Registers graph's in-adjacency with its uint32 weights (e.g. from
+ * apspie_csr_transpose): its SSSP queries then run push/pull rounds
+ * (apspie_sssp_u32_pull).  Call before submitting queries on the graph. */
+int apspie_server_set_sssp_in(apspie_server_t s, int graph, const int *d_tptr,
+                              const int *d_tind, const uint32_t *d_tw);
 /* Non-blocking; APSPIE_ERR_BUSY when the pending queue is full. */
 int apspie_server_submit(apspie_server_t s, int type, int graph, int source,
                          uint32_t seed, void *h_result, uint64_t *req_id);

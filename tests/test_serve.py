@@ -56,6 +56,25 @@ def test_server_mix_equals_alone(ctx):
         assert lat > 0
 
 
+def test_server_push_pull_sssp_large_graph(ctx):
+    """A graph above the batched-SSSP size limit with its in-adjacency and
+    weights registered: SSSP queries, alone and in a group (run one by one
+    through the push/pull kernel), equal the push-only single-query path."""
+    import torch
+    import apspie_b200 as ap
+    g = ap.gen_rmat_device(ctx, 22, 16, seed=5)
+    ap.weights_device(ctx, g, seed=5)
+    srcs = [int(x) for x in torch.nonzero(g.ptr[1:] - g.ptr[:-1]).flatten()[:4:1].cpu()]
+    refs = [ap.sssp(ctx, g, s, weights="u32").cpu().numpy() for s in srcs]   # push rounds only
+    ap.sssp_prepare(ctx, g)
+    with ap.Server(budget_bytes=16 << 30, max_batch=64) as srv:
+        gid = srv.add_graph(g)
+        rids = [srv.submit(1, gid, s) for s in srcs]
+        outs = [srv.wait(r)[0] for r in rids]
+    for s, out, ref in zip(srcs, outs, refs):
+        np.testing.assert_array_equal(out, ref.view(np.int32), err_msg=f"sssp src {s}")
+
+
 def test_server_budget_admits_one_at_a_time(ctx):
     import apspie_b200 as ap
     h = ap.gen_rmat(12, 16, seed=4)

@@ -79,6 +79,27 @@ def test_sssp_rmat_vs_oracle(ctx, scale, symmetric):
         _check_against_oracle(ctx, h, g, s)
 
 
+@pytest.mark.parametrize("scale,symmetric", [(12, False), (14, True)])
+@pytest.mark.parametrize("alpha", [3, 1 << 20])
+def test_sssp_pull_rounds_same_fixpoint(ctx, scale, symmetric, alpha):
+    """Push/pull SSSP over the in-adjacency (default switch point, and pull
+    in every round after the first): same distances as the oracle, and the
+    pull rounds did run (each scans all nnz in-edges)."""
+    import apspie_b200 as ap
+    h = ap.gen_rmat(scale, 16, seed=scale + 7, symmetric=symmetric)
+    ap.weights_u32(h, seed=6)
+    ap.weights_f32(h, seed=6)
+    g = ap.sssp_prepare(ctx, h.to_device())
+    ap.sssp_set_pull(ctx, alpha)
+    try:
+        for s in ap.seeded_sources(h, 3, seed=4) + [int(np.argmax(h.degrees()))]:
+            _check_against_oracle(ctx, h, g, s)
+            if alpha > 3:
+                assert ap.sssp_stats(ctx)["relaxations"] >= h.nnz
+    finally:
+        ap.sssp_set_pull(ctx)
+
+
 def test_sssp_edge_cases(ctx):
     import apspie_b200 as ap
     h = ap.HostGraph(4, np.array([0, 2, 2, 3, 3], np.int32), np.array([1, 2, 1], np.int32))
