@@ -36,12 +36,13 @@ struct SpmspvSmall {  // device-side scalars of one call
   unsigned nbig;      // columns of more than kBigDeg edges (a warp each)
   int ynnz;           // nnz(y)
   unsigned cnt;       // frontier size of the dense form
-  unsigned nhub;      // columns of more than kHubDeg edges (the whole grid each)
+  unsigned nhub;      // chunks of the columns of more than kHubDeg edges
 };
 
-// Columns longer than this are spread over every block; between kBigDeg and
-// this a warp takes one column
+// Columns longer than this are cut into kHubChunk-edge chunks, a warp each;
+// between kBigDeg and this a warp takes one column
 constexpr int kHubDeg = 1024;
+constexpr int kHubChunk = 2048;
 constexpr int kExpandThreads = 256;
 
 __device__ __forceinline__ float sr_term(int sr, float a, float x) {
@@ -65,7 +66,7 @@ __global__ void __launch_bounds__(kExpandThreads)
 expand_pairs(int sr, int xnnz, const int *__restrict__ xind, const float *__restrict__ xval,
              const int *__restrict__ ptr, const int *__restrict__ ind,
              const float *__restrict__ val, const long long *__restrict__ offs, int *keys,
-             float *vals, int *big, unsigned *nbig, int *hub, unsigned *nhub) {
+             float *vals, int *big, unsigned *nbig, int2 *hub, unsigned *nhub) {
   const int lane = lane_id();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
@@ -85,8 +86,11 @@ expand_pairs(int sr, int xnnz, const int *__restrict__ xind, const float *__rest
     const bool ismid = isbig && !ishub;
     unsigned slot = warp_append(ismid, nbig);
     if (ismid) big[slot] = j;
-    slot = warp_append(ishub, nhub);
-    if (ishub) hub[slot] = j;
+    if (ishub) {
+      const int nc = (d + kHubChunk - 1) / kHubChunk;
+      const unsigned at = atomicAdd(nhub, (unsigned)nc);
+      for (int c = 0; c < nc; ++c) hub[at + c] = make_int2(j, c);
+    }
     if (isbig) d = 0;
     int incl = warp_incl_scan(d);
     int excl = incl - d;
@@ -108,12 +112,12 @@ expand_pairs(int sr, int xnnz, const int *__restrict__ xind, const float *__rest
   }
 }
 
-// The listed columns: a warp per column of the medium list, then every
-// thread of the grid strides every hub (a hub's edges spread over all SMs).
+// The listed columns: a warp per column of the medium list, then a warp per
+// hub chunk (a hub's edges spread over all SMs).
 __global__ void expand_big(int sr, const int *__restrict__ xind, const float *__restrict__ xval,
                            const int *__restrict__ ptr, const int *__restrict__ ind,
                            const float *__restrict__ val, const long long *__restrict__ offs,
-                           const int *big, const unsigned *nbig, const int *hub,
+                           const int *big, const unsigned *nbig, const int2 *hub,
                            const unsigned *nhub, int *keys, float *vals) {
   const int lane = lane_id();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -131,14 +135,15 @@ __global__ void expand_big(int sr, const int *__restrict__ xind, const float *__
     }
   }
   const unsigned nh = *nhub;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
-  for (unsigned b = 0; b < nh; ++b) {
-    const int j = hub[b];
+  for (unsigned b = gwarp; b < nh; b += nwarps) {
+    const int2 hc = hub[b];
+    const int j = hc.x;
     const int c = xind[j];
-    const int s = __ldg(ptr + c), e = __ldg(ptr + c + 1);
+    const int s0 = __ldg(ptr + c);
+    const int s = s0 + hc.y * kHubChunk, e = min(__ldg(ptr + c + 1), s + kHubChunk);
     const float xv = xval ? xval[j] : 1.0f;
-    const long long o = offs[j] - s;
-    for (int k = s + tid; k < e; k += nthreads) {
+    const long long o = offs[j] - s0;
+    for (int k = s + lane; k < e; k += 32) {
       keys[o + k] = __ldg(ind + k);
       vals[o + k] = sr_term(sr, val ? __ldg(val + k) : 1.0f, xv);
     }
@@ -210,8 +215,8 @@ __device__ __forceinline__ void atomic_max_double(double *p, double v) {
 // edges are dealt over the lanes by an inclusive warp scan of the degrees
 // (coalesced over each column, no lane idles on a short column).  Columns
 // of more than kBigDeg edges are listed instead: up to kHubDeg edges a warp
-// takes one in expand_accumulate_big, longer ones (hubs) are strided by
-// every thread of that grid.  Each product is folded into acc[row] with the
+// takes one in expand_accumulate_big, longer ones (hubs) are cut into
+// kHubChunk-edge chunks that warps take one by one.  Each product is folded into acc[row] with the
 // semiring's atomic and marks the row's bit.
 __device__ __forceinline__ void accumulate_one(int sr, int r, float t, double *acc,
                                                unsigned *bits) {
@@ -229,7 +234,7 @@ __global__ void __launch_bounds__(kExpandThreads)
 expand_accumulate(int sr, int xnnz, const int *__restrict__ xind, const float *__restrict__ xval,
                   const int *__restrict__ ptr, const int *__restrict__ ind,
                   const float *__restrict__ val, double *acc, unsigned *bits, int *big,
-                  unsigned *nbig, int *hub, unsigned *nhub) {
+                  unsigned *nbig, int2 *hub, unsigned *nhub) {
   const int lane = lane_id();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
@@ -249,8 +254,11 @@ expand_accumulate(int sr, int xnnz, const int *__restrict__ xind, const float *_
     const bool ismid = isbig && !ishub;
     unsigned slot = warp_append(ismid, nbig);
     if (ismid) big[slot] = j;
-    slot = warp_append(ishub, nhub);
-    if (ishub) hub[slot] = j;
+    if (ishub) {
+      const int nc = (d + kHubChunk - 1) / kHubChunk;
+      const unsigned at = atomicAdd(nhub, (unsigned)nc);
+      for (int c = 0; c < nc; ++c) hub[at + c] = make_int2(j, c);
+    }
     if (isbig) d = 0;
     const int incl = warp_incl_scan(d);
     const int excl = incl - d;
@@ -270,13 +278,13 @@ expand_accumulate(int sr, int xnnz, const int *__restrict__ xind, const float *_
   }
 }
 
-// The listed long columns: a warp per column of the medium list, then every
-// thread of the grid strides every hub (a hub's edges spread over all SMs).
+// The listed long columns: a warp per column of the medium list, then a warp
+// per hub chunk (a hub's edges spread over all SMs).
 __global__ void __launch_bounds__(kExpandThreads)
 expand_accumulate_big(int sr, const int *__restrict__ xind, const float *__restrict__ xval,
                       const int *__restrict__ ptr, const int *__restrict__ ind,
                       const float *__restrict__ val, const int *big, const unsigned *nbig,
-                      const int *hub, const unsigned *nhub, double *acc, unsigned *bits) {
+                      const int2 *hub, const unsigned *nhub, double *acc, unsigned *bits) {
   const int lane = lane_id();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
@@ -304,13 +312,26 @@ expand_accumulate_big(int sr, const int *__restrict__ xind, const float *__restr
                      bits);
   }
   const unsigned nh = *nhub;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
-  for (unsigned b = 0; b < nh; ++b) {
-    const int j = hub[b];
+  for (unsigned b = gwarp; b < nh; b += nwarps) {
+    const int2 hc = hub[b];
+    const int j = hc.x;
     const int c = xind[j];
-    const int s = __ldg(ptr + c), e = __ldg(ptr + c + 1);
+    const int s = __ldg(ptr + c) + hc.y * kHubChunk;
+    const int e = min(__ldg(ptr + c + 1), s + kHubChunk);
     const float xv = xval ? xval[j] : 1.0f;
-    for (int k = s + tid; k < e; k += nthreads)
+    int k = s + lane;
+    for (; k + 96 < e; k += 128) {
+      int r[4];
+      float a[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        r[q] = __ldg(ind + k + 32 * q);
+        a[q] = val ? __ldg(val + k + 32 * q) : 1.0f;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) accumulate_one(sr, r[q], sr_term(sr, a[q], xv), acc, bits);
+    }
+    for (; k < e; k += 32)
       accumulate_one(sr, __ldg(ind + k), sr_term(sr, val ? __ldg(val + k) : 1.0f, xv), acc,
                      bits);
   }
@@ -414,9 +435,12 @@ int spmspv_core(apspie_context *ctx, int sr, int m, const int *ptr, const int *i
     unsigned *bits = (unsigned *)workspace(ctx, kSlotBitmap, sizeof(unsigned) * (size_t)(2 * words + 2));
     if (!acc || !bits) return APSPIE_ERR_OOM;
     unsigned *woffs = bits + words + 1;
-    int *big = (int *)workspace(ctx, kSlotMisc2, sizeof(int) * 2 * (size_t)(xnnz + 1));
+    const size_t nbig_cap = ((size_t)xnnz + 2) & ~size_t(1);  // keeps the chunk list 8-aligned
+    int *big = (int *)workspace(ctx, kSlotMisc2,
+                                sizeof(int) * nbig_cap +
+                                    sizeof(int2) * ((size_t)E / kHubChunk + (size_t)xnnz + 1));
     if (!big) return APSPIE_ERR_OOM;
-    int *hub = big + xnnz + 1;
+    int2 *hub = (int2 *)(big + nbig_cap);
     cudaMemsetAsync(&sm->nbig, 0, sizeof(unsigned), st);
     cudaMemsetAsync(&sm->nhub, 0, sizeof(unsigned), st);
     acc_init<<<grid_for(ctx, m, 256), 256, 0, st>>>(sr, m, acc, bits);
@@ -438,10 +462,13 @@ int spmspv_core(apspie_context *ctx, int sr, int m, const int *ptr, const int *i
   int *kb = (int *)workspace(ctx, kSlotSortKeysB, sizeof(int) * (size_t)E);
   float *va = (float *)workspace(ctx, kSlotSortValsA, sizeof(float) * (size_t)E);
   float *vb = (float *)workspace(ctx, kSlotSortValsB, sizeof(float) * (size_t)E);
-  int *big = (int *)workspace(ctx, kSlotMisc2, sizeof(int) * 2 * (size_t)(xnnz + 1));
+  const size_t nbig_cap = ((size_t)xnnz + 2) & ~size_t(1);  // keeps the chunk list 8-aligned
+  int *big = (int *)workspace(ctx, kSlotMisc2,
+                              sizeof(int) * nbig_cap +
+                                  sizeof(int2) * ((size_t)E / kHubChunk + (size_t)xnnz + 1));
   unsigned *nbig = &sm->nbig;
   if (!ka || !kb || !va || !vb || !big) return APSPIE_ERR_OOM;
-  int *hub = big + xnnz + 1;
+  int2 *hub = (int2 *)(big + nbig_cap);
   cudaMemsetAsync(nbig, 0, sizeof(unsigned), st);
   cudaMemsetAsync(&sm->nhub, 0, sizeof(unsigned), st);
   expand_pairs<<<grid_for(ctx, (long long)xnnz * 32, kExpandThreads), kExpandThreads, 0, st>>>(

@@ -45,7 +45,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--scale", type=int, default=SCALE)
     p.add_argument("--profile-case", default=None,
-                   choices=["mis_er", "mis_grid", "tc", "spgemm", "batch", "spmspv", "spmv"],
+                   choices=["mis_er", "mis_grid", "tc", "spgemm", "batch", "spmspv", "spmv",
+                            "sssp_pull"],
                    help="run one workload three times for an ncu capture, print nothing else")
     p.add_argument("--no-prepare", action="store_true",
                    help="pull over the CSR as given instead of the degree-ordered in-adjacency")
@@ -672,8 +673,9 @@ def run_serving(args):
 
 def run_profile_case(args):
     """--profile-case NAME: run one workload of the MIS / TC / SpGEMM / batched
-    / SpMSpV / SpMV configurations three times and exit, for ncu captures of
-    its kernels (no timing, no JSON)."""
+    / SpMSpV / SpMV / push-pull SSSP (R-MAT 22, two sources) configurations
+    three times and exit, for ncu captures of its kernels (no timing, no
+    JSON)."""
     import torch
     import apspie_b200 as ap
     ctx = ap.Context(0)
@@ -700,6 +702,13 @@ def run_profile_case(args):
         jobs = [{"type": "bfs", "graph": g, "sources": srcs[:64]},
                 {"type": "sssp", "graph": g, "sources": srcs[64:]}]
         run = lambda: ap.batch_run(ctx, jobs)
+    elif case == "sssp_pull":
+        h = ap.gen_rmat(22, EDGE_FACTOR, seed=SEED)
+        ap.weights_u32(h, seed=SEED)
+        g = ap.sssp_prepare(ctx, h.to_device())
+        ap.sssp_set_pull(ctx, 2)
+        srcs = ap.seeded_sources(h, 2, seed=3)
+        run = lambda: [ap.sssp(ctx, g, s, weights="u32") for s in srcs]
     elif case in ("spmspv", "spmv"):
         h = ap.gen_rmat(20, EDGE_FACTOR, seed=SEED)
         g = h.to_device()
