@@ -46,7 +46,8 @@ class Job(C.Structure):
                 ("d_ind", C.c_void_p), ("d_tptr", C.c_void_p), ("d_tind", C.c_void_p),
                 ("d_w", C.c_void_p), ("symmetric", C.c_int), ("nsrc", C.c_int),
                 ("h_src", C.POINTER(C.c_int)), ("d_out", C.c_void_p), ("alpha", C.c_int),
-                ("beta", C.c_int)]
+                ("beta", C.c_int), ("d_stptr", C.c_void_p), ("d_stind", C.c_void_p),
+                ("d_stw", C.c_void_p)]
 
 
 class BatchStats(C.Structure):
@@ -105,6 +106,7 @@ PROTOS: dict[str, tuple] = {
     "apspie_batch_run": (c_int, [vp, c_int, C.POINTER(Job), c_int]),
     "apspie_batch_set_params": (c_int, [vp, c_int]),
     "apspie_batch_set_deep_mode": (c_int, [vp, c_int]),
+    "apspie_batch_set_sssp_pull": (c_int, [vp, c_int]),
     "apspie_batch_get_stats": (c_int, [vp, C.POINTER(BatchStats)]),
     "apspie_autotune_bfs": (c_int, [vp, c_int, P_int, c_i64, c_int, vp, vp, vp, vp, vp, P_int,
                                     P_int, C.POINTER(C.c_float)]),

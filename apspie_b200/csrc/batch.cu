@@ -54,6 +54,11 @@ constexpr int kSsspBigDeg = 32;
 constexpr int kSsspChunk = 64;
 constexpr int kSsspPerUnit = 4;
 constexpr int kSsspSlots = 4;     // rounds of 32 / sw edges a warp relaxes together
+// SSSP pull steps: in-degree above which a vertex is split into chunks of
+// kMsPullChunk in-edges, and vertices per pull unit
+constexpr int kMsHubIn = 1024;
+constexpr int kMsPullChunk = 1024;
+constexpr int kMsPullVerts = 8;
 
 struct JobCounters {
   unsigned long long qc;  // queue length (low 32 bits) | chunk-list length (high 32 bits)
@@ -73,7 +78,13 @@ struct BatchJob {
   int *q0, *q1, *q2;
   int2 *c0, *c1, *c2;
   int big_deg, chunk;  // degree above which a vertex is chunked, edges per chunk
-  int sw, pad1;        // result row width (power of two >= nsrc)
+  int sw, salpha;      // result row width (power of two >= nsrc); SSSP pull switch
+  // SSSP pull steps: in-adjacency with its weights, and the chunks of the
+  // vertices of more than kMsHubIn in-edges
+  const int *stptr, *stind;
+  const uint32_t *stw;
+  int2 *hubc;
+  unsigned nhc, pad2;
   JobCounters c[3];
 };
 
@@ -549,6 +560,116 @@ __device__ void mssp_chunk(BatchJob *j, int L, int unit) {
   }
 }
 
+// ------------------------------------------------------- SSSP pull steps ---
+// Lists the (vertex, chunk) pull units of an SSSP job's vertices with more
+// than kMsHubIn in-edges (after the job table upload, which zeroes nhc).
+__global__ void batch_hub_chunks(BatchJob *jobs, int jid) {
+  BatchJob *j = jobs + jid;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < j->m; v += gridDim.x * blockDim.x) {
+    const int d = __ldg(j->stptr + v + 1) - __ldg(j->stptr + v);
+    if (d > kMsHubIn) {
+      const unsigned nc = (unsigned)((d + kMsPullChunk - 1) / kMsPullChunk);
+      const unsigned at = atomicAdd(&j->nhc, nc);
+      for (unsigned c = 0; c < nc; ++c) j->hubc[at + c] = make_int2(v, (int)c);
+    }
+  }
+}
+
+// Least d[u][s] + w(u, v) over in-edges [a0, a1) of v whose tail u changed
+// for source s in the last step, for every source s at once: lane =
+// (edge slot, source) with 32 / sw edge slots, the slots' minima combined
+// by xor shuffles; lanes 0 .. sw-1 return the source's minimum.
+__device__ __forceinline__ unsigned mssp_pull_min(const BatchJob *j, int a0, int a1,
+                                                  const unsigned long long *Fc) {
+  const int lane = lane_id();
+  const int sw = j->sw, per = 32 / sw;
+  const int src = lane & (sw - 1), eo = lane / sw;
+  const unsigned *dist = reinterpret_cast<const unsigned *>(j->out);
+  unsigned best = 0xffffffffu;
+  // four in-edges per lane in flight: their indices, then their frontier
+  // words, then the distances (each lane's k stays below a1: the loops
+  // may run different counts per lane and meet again before the shuffles)
+  int k = a0 + eo;
+  if (src < j->nsrc) {
+    for (; k + 3 * per < a1; k += 4 * per) {
+      int u[4];
+      unsigned fm[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) u[q] = __ldg(j->stind + k + q * per);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) fm[q] = (unsigned)__ldcg(Fc + u[q]);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if ((fm[q] >> src) & 1u)
+          best = min(best, sat_add(__ldcg(dist + (size_t)u[q] * sw + src),
+                                   __ldg(j->stw + k + q * per)));
+    }
+    for (; k < a1; k += per) {
+      const int u = __ldg(j->stind + k);
+      const unsigned fm = (unsigned)__ldcg(Fc + u);
+      if ((fm >> src) & 1u) best = min(best, sat_add(__ldcg(dist + (size_t)u * sw + src),
+                                                     __ldg(j->stw + k)));
+    }
+  }
+  for (int o = sw; o < 32; o <<= 1) best = min(best, __shfl_xor_sync(kFull, best, o));
+  return best;
+}
+
+// One pull unit of an SSSP job: a hub chunk (minima through atomicMin, the
+// hub's other chunks run elsewhere) or kMsPullVerts vertices, each taken
+// by the whole warp and written by it alone (no atomics).  Improved
+// vertices get their next-frontier bits and are queued, as in a push step.
+__device__ void mssp_pull(BatchJob *j, int L, int unit) {
+  const int lane = lane_id();
+  const int sw = j->sw;
+  unsigned *dist = reinterpret_cast<unsigned *>(j->out);
+  const unsigned long long *Fc = jobF(j, L % 3);
+  unsigned long long *Fn = jobF(j, (L + 1) % 3);
+  int *qout = jobQ(j, (L + 1) % 3);
+  int2 *cout = jobC(j, (L + 1) % 3);
+  JobCounters *nxt = &j->c[(L + 1) % 3];
+  const unsigned low = sw == 32 ? 0xffffffffu : ((1u << sw) - 1u);
+  const bool mine = lane < sw && lane < j->nsrc;  // this lane's source after the reduction
+  if ((unsigned)unit < j->nhc) {
+    const int2 hc = j->hubc[unit];
+    const int v = hc.x;
+    const int a0 = __ldg(j->stptr + v) + hc.y * kMsPullChunk;
+    const int a1 = min(__ldg(j->stptr + v + 1), a0 + kMsPullChunk);
+    const unsigned best = mssp_pull_min(j, a0, a1, Fc);
+    bool imp = false;
+    if (mine && best < __ldcg(dist + (size_t)v * sw + lane)) {
+      const unsigned old = atomicMin(dist + (size_t)v * sw + lane, best);
+      imp = best < old;
+    }
+    const unsigned b = __ballot_sync(kFull, imp) & low;
+    bool f[1] = {false};
+    if (lane == 0 && b) f[0] = atomicOr(Fn + v, (unsigned long long)b) == 0ull;
+    int u1[1] = {v}, dg[1] = {0};
+    if (f[0]) dg[0] = __ldg(j->ptr + v + 1) - __ldg(j->ptr + v);
+    append_n<1>(j, f, u1, dg, qout, cout, nxt);
+    return;
+  }
+  const int v0 = (unit - (int)j->nhc) * kMsPullVerts;
+  for (int i = 0; i < kMsPullVerts; ++i) {
+    const int v = v0 + i;
+    if (v >= j->m) break;
+    const int a0 = __ldg(j->stptr + v), a1 = __ldg(j->stptr + v + 1);
+    if (a1 - a0 > kMsHubIn || a1 == a0) continue;  // a hub's chunks are units of their own
+    const unsigned best = mssp_pull_min(j, a0, a1, Fc);
+    bool imp = false;
+    if (mine && best < __ldcg(dist + (size_t)v * sw + lane)) {
+      dist[(size_t)v * sw + lane] = best;  // only this warp writes v in a pull step
+      imp = true;
+    }
+    const unsigned b = __ballot_sync(kFull, imp) & low;
+    bool f[1] = {lane == 0 && b != 0u};
+    if (f[0]) Fn[v] = (unsigned long long)b;
+    int u1[1] = {v}, dg[1] = {0};
+    if (f[0]) dg[0] = __ldg(j->ptr + v + 1) - __ldg(j->ptr + v);
+    append_n<1>(j, f, u1, dg, qout, cout, nxt);
+  }
+}
+
 // ---------------------------------------------------------------- kernel ---
 __global__ void __launch_bounds__(kBatchThreads, 2)
 batch_persistent(BatchJob *jobs, int njobs, BatchState *st, int max_steps) {
@@ -609,7 +730,12 @@ batch_persistent(BatchJob *jobs, int njobs, BatchState *st, int max_steps) {
             u2 = (q + 31) / 32;
             u3 = ch;
           }
+        } else if (j->stptr && j->salpha > 0 && (long long)ed * j->salpha > j->nnz) {
+          // pull step: hub chunks, then units of kMsPullVerts vertices
+          s_pull[jj] = 1;
+          u2 = j->nhc + (unsigned)((j->m + kMsPullVerts - 1) / kMsPullVerts);
         } else {
+          s_pull[jj] = 0;
           u2 = (q + kSsspPerUnit - 1) / kSsspPerUnit;
           u3 = ch;
         }
@@ -664,6 +790,8 @@ batch_persistent(BatchJob *jobs, int njobs, BatchState *st, int max_steps) {
         } else {
           msbfs_push_chunk(j, step, (int)(loc - s_u2[lo]));
         }
+      } else if (s_pull[lo]) {
+        mssp_pull(j, step, (int)loc);
       } else {
         if (loc < s_u2[lo])
           mssp_queue(j, step, (int)loc, s_q[lo]);
@@ -877,7 +1005,8 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
     const apspie_job &J = jobs[i];
     if ((J.type != APSPIE_JOB_BFS && J.type != APSPIE_JOB_SSSP_U32) || J.m <= 0 || J.nnz < 0 ||
         J.nnz >= (int64_t)INT32_MAX || J.nsrc <= 0 || !J.h_src || !J.d_ptr || !J.d_out ||
-        (J.nnz > 0 && !J.d_ind) || (J.type == APSPIE_JOB_SSSP_U32 && J.nnz > 0 && !J.d_w))
+        (J.nnz > 0 && !J.d_ind) || (J.type == APSPIE_JOB_SSSP_U32 && J.nnz > 0 && !J.d_w) ||
+        (J.d_stptr && J.nnz > 0 && (!J.d_stind || !J.d_stw)))
       return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: bad job %d", i);
     for (int s = 0; s < J.nsrc; ++s)
       if (J.h_src[s] < 0 || J.h_src[s] >= J.m)
@@ -946,6 +1075,8 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
       b += align_up(4 * m) * 3;              // queues
       b += align_up(8 * cap) * 3;            // chunk lists
       b += align_up(4 * m * row_width(parts[p].n));  // vertex-major results
+      if (!bfs && J.d_stptr)  // hub chunks of the SSSP pull steps
+        b += align_up(8 * ((size_t)J.nnz / kMsPullChunk + (size_t)J.nnz / kMsHubIn + 1));
       off[p] = total;
       total += b;
     }
@@ -1001,12 +1132,21 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
       B.c1 = (int2 *)b; b += align_up(8 * cap);
       B.c2 = (int2 *)b; b += align_up(8 * cap);
       B.out = (int32_t *)b;  // vertex-major; transposed into the caller's array after
+      b += align_up(4 * m * B.sw);
+      if (!bfs && J.d_stptr) {
+        B.stptr = J.d_stptr;
+        B.stind = J.d_stind;
+        B.stw = J.d_stw;
+        B.salpha = ctx->sssp_pull_alpha_batch;
+        B.hubc = (int2 *)b;
+      }
     }
     cudaMemcpyAsync(djobs, hjobs, host_bytes, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(dsrc, hsrc, sizeof(int) * 64 * nparts, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(dstate, 0, align_up(sizeof(BatchState)), st);
     rc = check_cuda(ctx, cudaGetLastError(), "apspie_batch_run upload");
     if (rc) return rc;
+    int nhub_launches = 0;
     for (int p = 0; p < nparts; ++p) {
       const long long m = jobs[parts[p].job].m;
       int g = (int)std::max(1ll, std::min((m * hjobs[p].sw + 255) / 256, (long long)ctx->num_sms * 8));
@@ -1016,9 +1156,13 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
       } else {
         batch_init_sssp<<<g, 256, 0, st>>>(djobs, p);
         batch_seed_sssp<<<1, 32, 0, st>>>(djobs, p);
+        if (hjobs[p].stptr) {
+          batch_hub_chunks<<<std::min(g, ctx->num_sms * 4), 256, 0, st>>>(djobs, p);
+          ++nhub_launches;
+        }
       }
     }
-    rc = check_launch(ctx, "batch init", 2 * nparts);
+    rc = check_launch(ctx, "batch init", 2 * nparts + nhub_launches);
     if (rc) return rc;
     int n1 = nparts;
     void *args1[] = {&djobs, &n1, &dstate, &max_steps};

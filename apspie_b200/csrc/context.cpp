@@ -150,6 +150,12 @@ int apspie_batch_set_params(apspie_ctx ctx, int deep_blocks) {
   return APSPIE_OK;
 }
 
+int apspie_batch_set_sssp_pull(apspie_ctx ctx, int alpha) {
+  if (!ctx || alpha < 0) return APSPIE_ERR_INVALID;
+  ctx->sssp_pull_alpha_batch = alpha;
+  return APSPIE_OK;
+}
+
 int apspie_batch_set_deep_mode(apspie_ctx ctx, int max_concurrent) {
   if (!ctx || max_concurrent < 0 || max_concurrent > 64) return APSPIE_ERR_INVALID;
   ctx->batch_deep_subs = max_concurrent;

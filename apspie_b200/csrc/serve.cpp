@@ -89,11 +89,13 @@ struct GraphEntry {
   const uint32_t *stw = nullptr;
 };
 
-// SSSP groups on graphs with more edges than this run their queries one by
-// one through the single-source kernel: the multi-source rows share little
-// there (R-MAT 22, 8 sources: 56 ms batched, 37 ms one by one with pull
-// rounds, measured), while on smaller graphs the batch wins.
+// SSSP groups of fewer than kSsspBatchMinGroup queries on graphs with more
+// edges than kSsspBatchMaxNnz run their queries one by one through the
+// single-source kernel: on R-MAT 22 the multi-source rows share little
+// (8 sources: 44 ms batched, 37 ms one by one with pull rounds; 16: 59 vs
+// 75 ms; 32: 92 vs 152 ms, measured), while on smaller graphs the batch wins.
 constexpr int64_t kSsspBatchMaxNnz = 64ll << 20;
+constexpr size_t kSsspBatchMinGroup = 12;
 
 // One SSSP query through the single-source kernel, push/pull when the
 // graph's in-adjacency with weights was registered.
@@ -344,7 +346,7 @@ int launch_group(apspie_server *s, Slot &sl, Group &g) {
     } else {
       st = sssp_one(ln.ctx, ge, r->source, (uint32_t *)out);
     }
-  } else if (g.kind == 1 && ge.nnz > kSsspBatchMaxNnz) {
+  } else if (g.kind == 1 && ge.nnz > kSsspBatchMaxNnz && g.reqs.size() < kSsspBatchMinGroup) {
     for (Request *r : g.reqs) {
       st = sssp_one(ln.ctx, ge, r->source, (uint32_t *)((char *)sl.d_out + r->dev_off));
       if (st != APSPIE_OK) break;
@@ -368,6 +370,9 @@ int launch_group(apspie_server *s, Slot &sl, Group &g) {
     j.d_out = (int32_t *)((char *)sl.d_out + g.reqs.front()->dev_off);
     j.alpha = -1;
     j.beta = -1;
+    j.d_stptr = ge.stptr;
+    j.d_stind = ge.stind;
+    j.d_stw = ge.stw;
     st = apspie_batch_run(ln.ctx, 1, &j, 0);
     ++s->launched_jobs;
   }

@@ -457,6 +457,12 @@ def batch_run(ctx: Context, jobs: list[dict], max_steps: int = 0):
                      C.c_void_p(0 if g.w_u32 is None else g.w_u32.data_ptr()), int(sym),
                      len(jd["sources"]), src, C.c_void_p(out.data_ptr()),
                      int(jd.get("alpha", -1)), int(jd.get("beta", -1)))
+        sin = g.extra.get("sssp_in", {}).get("u32") if jd["type"] == "sssp" else None
+        if sin is not None:
+            # in-adjacency with weights from sssp_prepare: pull steps
+            arr[i].d_stptr = C.c_void_p(sin[0].data_ptr())
+            arr[i].d_stind = C.c_void_p(sin[1].data_ptr())
+            arr[i].d_stw = C.c_void_p(sin[2].data_ptr())
     check(lib.apspie_batch_run(ctx.handle, len(jobs), arr, int(max_steps)), ctx.handle,
           "apspie_batch_run")
     return outs
@@ -471,6 +477,12 @@ def batch_set_params(ctx: Context, deep_blocks: int = 0, deep_concurrent: int = 
           "apspie_batch_set_params")
     check(lib.apspie_batch_set_deep_mode(ctx.handle, int(deep_concurrent)), ctx.handle,
           "apspie_batch_set_deep_mode")
+
+
+def batch_set_sssp_pull(ctx: Context, alpha: int = 0) -> None:
+    """Pull switch of the multi-source SSSP steps (0 = never pull, the default)."""
+    check(lib.apspie_batch_set_sssp_pull(ctx.handle, int(alpha)), ctx.handle,
+          "apspie_batch_set_sssp_pull")
 
 
 def batch_stats(ctx: Context) -> dict:

@@ -261,6 +261,12 @@ typedef struct {
   const int *h_src;            /* host array of nsrc sources */
   int32_t *d_out;              /* nsrc x m results */
   int alpha, beta;             /* BFS direction thresholds, < 0 = default */
+  /* SSSP only, may be NULL: the in-adjacency with its weights; then steps
+   * whose frontier out-edges times the context's batch pull switch
+   * (apspie_batch_set_sssp_pull; default 0 = never) exceed nnz are pull
+   * steps */
+  const int *d_stptr, *d_stind;
+  const uint32_t *d_stw;
 } apspie_job;
 typedef struct {
   int32_t super_steps;
@@ -282,6 +288,10 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs,
  * job in the multi-source launch instead; max_steps > 0 always does. */
 int apspie_batch_set_params(apspie_ctx ctx, int deep_blocks);
 int apspie_batch_set_deep_mode(apspie_ctx ctx, int max_concurrent);
+/* Pull switch of the multi-source SSSP steps (0 = never pull, the
+ * default: on R-MAT 20 / 22 with 8 .. 32 sources the pull steps were 3 - 30 %
+ * slower than the push steps, each reading a distance row per in-edge). */
+int apspie_batch_set_sssp_pull(apspie_ctx ctx, int alpha);
 /* Statistics of the last batch (synchronises; reports a barrier timeout). */
 int apspie_batch_get_stats(apspie_ctx ctx, apspie_batch_stats *out);
 

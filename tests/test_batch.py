@@ -82,6 +82,35 @@ def test_batch_forced_push_and_pull(ctx):
             np.testing.assert_array_equal(out[i], refs[i])
 
 
+@pytest.mark.parametrize("alpha", [2, 1 << 20])
+def test_batch_sssp_pull_steps(ctx, alpha):
+    """Multi-source SSSP with the in-adjacency and weights: pull steps when the
+    frontier's out-edges pass nnz / 2 and in every step after the first, on a symmetric
+    R-MAT with hubs of more than 1024 in-edges (chunked) and on a directed
+    one; every row equals the oracle's Dijkstra."""
+    import apspie_b200 as ap
+    r = ap.gen_rmat(15, 16, seed=21)
+    ap.weights_u32(r, seed=8)
+    assert (r.degrees() > 1024).any()
+    dd = ap.gen_rmat(12, 8, seed=22, symmetric=False)
+    ap.weights_u32(dd, seed=9)
+    gr = ap.sssp_prepare(ctx, r.to_device())
+    gd = ap.sssp_prepare(ctx, dd.to_device())
+    jobs = [{"type": "sssp", "graph": gr, "sources": ap.seeded_sources(r, 40, seed=3)},
+            {"type": "sssp", "graph": gd, "sources": list(range(0, 4096, 500))},
+            {"type": "sssp", "graph": gr, "sources": [int(np.argmax(r.degrees()))]}]
+    ap.batch_set_sssp_pull(ctx, alpha)
+    try:
+        outs = ap.batch_run(ctx, jobs)
+    finally:
+        ap.batch_set_sssp_pull(ctx)
+    for jd, out, h in zip(jobs, outs, (r, dd, r)):
+        out = out.cpu().numpy().view(np.uint32)
+        for i, s in enumerate(jd["sources"]):
+            ref = oracle.sssp_u32(h.m, h.ptr, h.ind, h.w_u32, s)
+            np.testing.assert_array_equal(out[i], ref, err_msg=f"sssp {h.name} src {s}")
+
+
 def test_batch_rejects_bad_jobs(ctx):
     import apspie_b200 as ap
     a, *_ = _graphs()
