@@ -205,8 +205,12 @@ __global__ void sssp_hub_chunks(int m, const int *__restrict__ tptr, int2 *hubc,
   }
 }
 
-template <typename W>
-__global__ void __launch_bounds__(kSsspThreads, 2)
+// MINB blocks per SM: 2 for the push-only entry points; 3 when pull rounds
+// are possible (their loops carry no atomics and gain from the extra warps:
+// R-MAT 22 push/pull 4.0 vs 4.7 ms per source, while push-only ran 12 %
+// slower at 3 blocks, which costs spills at 40 registers; measured).
+template <typename W, int MINB>
+__global__ void __launch_bounds__(kSsspThreads, MINB)
 sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
                 const W *__restrict__ w, unsigned *dist, int *stamp, int *qa, int *qb, int2 *ca,
                 int2 *cb, SsspState *st, int max_rounds, int *fstamp, unsigned *xd, int *far0,
@@ -424,12 +428,13 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
   }
 }
 
-template <typename W>
+template <typename W, int MINB>
 int sssp_grid(apspie_context *ctx) {
   static int cached_dev = -1, cached_grid = 0;
   if (cached_dev == ctx->device && cached_grid > 0) return cached_grid;
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sssp_persistent<W>, kSsspThreads, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sssp_persistent<W, MINB>, kSsspThreads,
+                                                    0) !=
           cudaSuccess ||
       occ < 1) {
     cudaGetLastError();
@@ -466,7 +471,8 @@ int sssp_run(apspie_context *ctx, int src, int64_t nnz, int m, const int *d_ptr,
   int *fstamp = nf, *far0 = nf + 2 * mm, *far1 = nf + 3 * mm, *far2 = nf + 4 * mm;
   unsigned *xd = (unsigned *)(nf + mm);
   ctx->sssp_state = st;
-  int grid = clamp_grid(ctx, sssp_grid<W>(ctx));
+  const bool pull3 = d_tptr != nullptr;
+  int grid = clamp_grid(ctx, pull3 ? sssp_grid<W, 3>(ctx) : sssp_grid<W, 2>(ctx));
   if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_sssp: occupancy query failed");
   int init_grid = std::min((m + 255) / 256, ctx->num_sms * 8);
   sssp_init<W><<<init_grid, 256, 0, ctx->stream>>>(m, src, d_dist, stamp, fstamp, xd, d_ptr, qa,
@@ -488,7 +494,9 @@ int sssp_run(apspie_context *ctx, int src, int64_t nnz, int m, const int *d_ptr,
                   &qa, &qb,            &ca,            &cb,           &st,     &max_rounds,
                   &fstamp, &xd, &far0, &far1, &far2, &delta, &nnz_ll, (void *)&d_tptr,
                   (void *)&d_tind, (void *)&d_tw, &hubc, &alpha};
-  cudaError_t e = cudaLaunchCooperativeKernel((const void *)sssp_persistent<W>, dim3(grid),
+  const void *kern =
+      pull3 ? (const void *)sssp_persistent<W, 3> : (const void *)sssp_persistent<W, 2>;
+  cudaError_t e = cudaLaunchCooperativeKernel(kern, dim3(grid),
                                               dim3(kSsspThreads), args, 0, ctx->stream);
   if (e != cudaSuccess) return check_cuda(ctx, e, "sssp_persistent");
   ctx->launches += 1;
