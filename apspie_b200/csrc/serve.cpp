@@ -16,8 +16,8 @@
 //     its own completion event, so a quick query is not held back by a slow
 //     one of the same batch;
 //   * lanes: graphs whose traversals take many levels (found when the graph
-//     is added, by one probe BFS) run on a second stream with half of the
-//     GPU's persistent blocks, next to the main lane with the other half, so
+//     is added, by one probe BFS) run on a second stream with a quarter of
+//     the GPU's persistent blocks, next to the main lane with the rest, so
 //     their thousands of short levels do not keep the whole GPU from the
 //     other queries;
 //   * continuous batching: there are two batch slots.  While one slot's
@@ -400,7 +400,7 @@ void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
     // with deep graphs around, the main lane leaves room for the deep lane
     int resident = 0;
     apspie_ctx_resident_blocks(sl.lane[0].ctx, &resident);
-    apspie_ctx_set_max_grid(sl.lane[0].ctx, s->any_deep ? std::max(1, resident - resident / 2) : 0);
+    apspie_ctx_set_max_grid(sl.lane[0].ctx, s->any_deep ? std::max(1, resident - resident / 4) : 0);
   }
   std::map<std::pair<int, int>, size_t> index;
   sl.groups.clear();
@@ -574,10 +574,12 @@ int apspie_server_create(int device, size_t state_budget_bytes, int max_batch,
         return APSPIE_ERR_CUDA;
       }
       if (l == 1) {
-        // the deep lane: half of the resident persistent blocks
+        // the deep lane: a quarter of the resident persistent blocks (its
+        // traversals are latency bound per level; the main lane's large
+        // graphs need the blocks)
         int resident = 0;
         apspie_ctx_resident_blocks(ln.ctx, &resident);
-        apspie_ctx_set_max_grid(ln.ctx, std::max(1, resident / 2));
+        apspie_ctx_set_max_grid(ln.ctx, std::max(1, resident / 4));
       }
     }
   s->worker = std::thread(worker_main, s);
