@@ -213,14 +213,34 @@ __device__ __forceinline__ void for_each_product(int i, const int *__restrict__ 
         }
         int nxt = lo + 1 < n_a ? s_off[lo + 1] : INT_MAX;
         const int pend = min(p0 + vt, total);
-        for (int p = p0; p < pend; ++p) {
-          while (p >= nxt) {
-            ++lo;
-            nxt = lo + 1 < n_a ? s_off[lo + 1] : INT_MAX;
+        // the run's product positions first, then all its loads, then the
+        // calls: up to 8 independent loads in flight per thread
+        int pos[8];
+        float av[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int p = p0 + q;
+          pos[q] = -1;
+          av[q] = 0.f;
+          if (p < pend) {
+            while (p >= nxt) {
+              ++lo;
+              nxt = lo + 1 < n_a ? s_off[lo + 1] : INT_MAX;
+            }
+            pos[q] = s_bs[lo] + (p - s_off[lo]);
+            av[q] = s_av[lo];
           }
-          const int b = s_bs[lo] + (p - s_off[lo]);
-          f(__ldg(Bind + b), (double)s_av[lo] * (double)(Bval ? __ldg(Bval + b) : 1.0f));
         }
+        int jb[8];
+        float bv[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          jb[q] = pos[q] >= 0 ? __ldg(Bind + pos[q]) : -1;
+          bv[q] = (pos[q] >= 0 && Bval) ? __ldg(Bval + pos[q]) : 1.0f;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (jb[q] >= 0) f(jb[q], (double)av[q] * (double)bv[q]);
       }
       __syncthreads();
       continue;

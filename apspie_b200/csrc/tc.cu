@@ -130,13 +130,27 @@ __device__ __forceinline__ void for_each_wedge_in(int a0, int a1, const int *__r
         }
         int nxt = lo + 1 < n_a ? s_off[lo + 1] : INT_MAX;
         const int pend = min(p0 + vt, total);
-        for (int p = p0; p < pend; ++p) {
-          while (p >= nxt) {
-            ++lo;
-            nxt = lo + 1 < n_a ? s_off[lo + 1] : INT_MAX;
+        // the run's wedge positions first, then all its loads, then the
+        // visits: up to 8 independent loads in flight per thread
+        int pos[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int p = p0 + q;
+          pos[q] = -1;
+          if (p < pend) {
+            while (p >= nxt) {
+              ++lo;
+              nxt = lo + 1 < n_a ? s_off[lo + 1] : INT_MAX;
+            }
+            pos[q] = s_bs[lo] + (p - s_off[lo]);
           }
-          visit(__ldg(Li + s_bs[lo] + (p - s_off[lo])));
         }
+        int jv[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) jv[q] = pos[q] >= 0 ? __ldg(Li + pos[q]) : -1;
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (jv[q] >= 0) visit(jv[q]);
       }
       __syncthreads();
       continue;
