@@ -126,106 +126,211 @@ int device_exclusive_scan(apspie_context *ctx, const T *in, T *out, long long n,
 }
 
 // ------------------------------------------------------------ radix sort ---
+// Onesweep LSD radix sort (Adinets & Merrill, "Onesweep: A Faster Least
+// Significant Digit Radix Sort for GPUs", 2022): one read of the keys
+// counts every pass's digits, then one kernel per 8-bit pass.  A pass's
+// tiles take ids from a counter (so a tile only waits on tiles that are
+// already running), rank their keys locally (match_any per warp, a prefix
+// over the warps), publish their per-digit counts, and find their digit
+// offsets by decoupled look-back over the tiles before them: each status
+// word holds a flag (aggregate of this tile / inclusive of all before and
+// this one), the pass's tag and the count.  Stable.
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
+constexpr int kMaxPasses = 8;
+constexpr unsigned long long kStAgg = 1ull << 62, kStIncl = 2ull << 62;
+constexpr unsigned long long kStCountMask = (1ull << 40) - 1;
 
+// all passes' digit counts in one read of the keys
 template <typename K>
-__global__ void radix_count(const K *keys, long long n, int shift, unsigned *counts,
-                            unsigned ntiles) {
-  __shared__ unsigned hist[kRadix];
-  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) hist[d] = 0;
+__global__ void __launch_bounds__(kSortThreads)
+radix_histograms(const K *keys, long long n, int npass, unsigned long long *ghist) {
+  __shared__ unsigned hist[kMaxPasses][kRadix];
+  for (int t = threadIdx.x; t < kMaxPasses * kRadix; t += blockDim.x) hist[t / kRadix][t % kRadix] = 0;
   __syncthreads();
-  long long base = (long long)blockIdx.x * kSortTile;
-  for (int i = threadIdx.x; i < kSortTile; i += blockDim.x) {
-    long long idx = base + i;
-    if (idx < n) atomicAdd(&hist[(unsigned)(keys[idx] >> shift) & (kRadix - 1)], 1u);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const K k = keys[i];
+    for (int p = 0; p < npass; ++p)
+      atomicAdd(&hist[p][(unsigned)(k >> (p * kRadixBits)) & (kRadix - 1)], 1u);
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < kRadix; d += blockDim.x)
-    counts[(size_t)d * ntiles + blockIdx.x] = hist[d];
+  for (int t = threadIdx.x; t < npass * kRadix; t += blockDim.x) {
+    const unsigned c = hist[t / kRadix][t % kRadix];
+    if (c) atomicAdd(ghist + t, (unsigned long long)c);
+  }
+}
+
+// per pass, exclusive prefix of the digit counts (one block of kRadix)
+template <int R = kRadix>
+__global__ void radix_digit_offsets(unsigned long long *ghist, int npass) {
+  __shared__ unsigned long long sw[33];
+  for (int p = 0; p < npass; ++p) {
+    const unsigned long long c = ghist[p * R + threadIdx.x];
+    unsigned long long total;
+    const unsigned long long ex = block_excl_scan(c, sw, &total);
+    ghist[p * R + threadIdx.x] = ex;
+    __syncthreads();
+  }
 }
 
 template <typename K, typename V>
 __global__ void __launch_bounds__(kSortThreads)
-radix_scatter(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, long long n, int shift,
-              const unsigned *offsets, unsigned ntiles) {
+radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, long long n,
+               int pass, const unsigned long long *goff, unsigned long long *status,
+               unsigned *tile_counter, int *err) {
   constexpr int kWarps = kSortThreads / 32;
+  static_assert(sizeof(V) <= sizeof(K), "values are staged in the keys' shared array");
+  // the tile in digit order (keys, then values), each key's digit, per-warp
+  // digit counts, and per digit the output position of the tile's run minus
+  // its start within the tile
+  __shared__ __align__(16) K skeys[kSortTile];
+  __shared__ unsigned char sdig[kSortTile];
   __shared__ unsigned whist[kWarps][kRadix];
+  __shared__ unsigned long long gbase[kRadix];
+  __shared__ unsigned long long s_scan[33];
+  __shared__ unsigned s_tile;
   const int lane = lane_id(), w = warp_in_block();
+  const int shift = pass * kRadixBits;
+  const unsigned long long tag = (unsigned long long)(pass + 1) << 40;
+  if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
   for (int d = lane; d < kRadix; d += 32) whist[w][d] = 0;
-  __syncwarp();
-  // this warp's slice: kSortItems rounds of 32 consecutive keys
-  long long wbase = (long long)blockIdx.x * kSortTile + (long long)w * 32 * kSortItems;
-  unsigned rank[kSortItems];
-  unsigned dig[kSortItems];
+  __syncthreads();
+  const unsigned tile = s_tile;
+  const long long tbase = (long long)tile * kSortTile;
+  const int tlen = (int)min((long long)kSortTile, n - tbase);
+  // this warp's slice of the tile: kSortItems rounds of 32 consecutive keys
+  const int wofs = w * 32 * kSortItems;
+  unsigned pos[kSortItems], dig[kSortItems];
+  K kv[kSortItems];
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
-    long long idx = wbase + i * 32 + lane;
-    bool valid = idx < n;
-    unsigned d = valid ? (unsigned)(keys_in[idx] >> shift) & (kRadix - 1) : (unsigned)kRadix;
-    unsigned peers = __match_any_sync(kFull, d);
-    unsigned lower = peers & ((1u << lane) - 1u);
-    int leader = __ffs(peers) - 1;
+    const int t = wofs + i * 32 + lane;
+    kv[i] = t < tlen ? keys_in[tbase + t] : K(0);
+  }
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const bool valid = wofs + i * 32 + lane < tlen;
+    const unsigned d = valid ? (unsigned)(kv[i] >> shift) & (kRadix - 1) : (unsigned)kRadix;
+    const unsigned peers = __match_any_sync(kFull, d);
+    const int leader = __ffs(peers) - 1;
     unsigned prev = 0;
     if (valid && lane == leader) {
       prev = whist[w][d];
       whist[w][d] = prev + __popc(peers);
     }
     prev = __shfl_sync(kFull, prev, leader);
-    rank[i] = prev + __popc(lower);
+    pos[i] = prev + __popc(peers & ((1u << lane) - 1u));
     dig[i] = d;
     __syncwarp();
   }
   __syncthreads();
-  // exclusive prefix over warps per digit, plus the tile's global base
-  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
-    unsigned run = offsets[(size_t)d * ntiles + blockIdx.x];
-    for (int ww = 0; ww < kWarps; ++ww) {
-      unsigned c = whist[ww][d];
-      whist[ww][d] = run;
-      run += c;
+  // per digit (one per thread): prefix over the warps, the tile's count,
+  // its start within the tile, then the look-back for its output offset
+  const int d = threadIdx.x;
+  unsigned run = 0;
+  for (int ww = 0; ww < kWarps; ++ww) {
+    const unsigned c = whist[ww][d];
+    whist[ww][d] = run;
+    run += c;
+  }
+  unsigned long long tot;
+  const unsigned long long loc = block_excl_scan((unsigned long long)run, s_scan, &tot);
+  unsigned long long *mine = status + (size_t)tile * kRadix + d;
+  unsigned long long excl = 0;
+  if (tile == 0) {
+    __stcg(mine, kStIncl | tag | (unsigned long long)run);
+  } else {
+    __stcg(mine, kStAgg | tag | (unsigned long long)run);
+    long long t = (long long)tile - 1;
+    unsigned spins = 0;
+    while (t >= 0) {
+      const unsigned long long sv = ld_acquire64(status + (size_t)t * kRadix + d);
+      if ((sv & (0x3FFFFFull << 40)) != tag || (sv >> 62) == 0ull) {
+        if (++spins > kSpinLimit) {  // a predecessor never published: give up
+          atomicExch(err, 1);
+          break;
+        }
+        continue;
+      }
+      excl += sv & kStCountMask;
+      if ((sv >> 62) == 2ull) break;  // inclusive: everything before is in it
+      --t;
+    }
+    __stcg(mine, kStIncl | tag | (excl + run));
+  }
+  gbase[d] = goff[pass * kRadix + d] + excl - loc;
+  for (int ww = 0; ww < kWarps; ++ww) whist[ww][d] += (unsigned)loc;
+  __syncthreads();
+  // tile position of every key: its digit's start + the warps before it + its rank
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    if (wofs + i * 32 + lane < tlen) {
+      const unsigned dd = dig[i];
+      pos[i] += whist[w][dd];
+      skeys[pos[i]] = kv[i];
+      sdig[pos[i]] = (unsigned char)dd;
     }
   }
   __syncthreads();
+  for (int t = threadIdx.x; t < tlen; t += kSortThreads)
+    keys_out[gbase[sdig[t]] + t] = skeys[t];
+  if (vals_in) {  // keys-only sorts pass no values
+    __syncthreads();
+    V *svals = reinterpret_cast<V *>(skeys);
 #pragma unroll
-  for (int i = 0; i < kSortItems; ++i) {
-    long long idx = wbase + i * 32 + lane;
-    if (idx < n) {
-      unsigned pos = whist[w][dig[i]] + rank[i];
-      keys_out[pos] = keys_in[idx];
-      if (vals_in) vals_out[pos] = vals_in[idx];  // keys-only sorts pass no values
+    for (int i = 0; i < kSortItems; ++i) {
+      const int t = wofs + i * 32 + lane;
+      if (t < tlen) svals[pos[i]] = vals_in[tbase + t];
     }
+    __syncthreads();
+    for (int t = threadIdx.x; t < tlen; t += kSortThreads)
+      vals_out[gbase[sdig[t]] + t] = svals[t];
   }
 }
 
 // Stable sort of n (key, value) pairs on the low `bits` bits of the key
 // (va == vb == nullptr sorts keys only).  Ping-pongs between (ka, va) and
-// (kb, vb); *result_in_b tells where the sorted data ended up.  Scratch: slots kSlotSortHist (+ kSlotScan).
+// (kb, vb); *result_in_b tells where the sorted data ended up.  Scratch:
+// slot kSlotSortHist (histograms, tile counters, status words).
 template <typename K, typename V>
 int device_radix_sort(apspie_context *ctx, K *ka, V *va, K *kb, V *vb, long long n, int bits,
                       bool *result_in_b) {
   *result_in_b = false;
   if (n <= 1 || bits <= 0) return APSPIE_OK;
-  long long tiles = (n + kSortTile - 1) / kSortTile;
-  if (tiles * kRadix >= (1ll << 31))
-    return set_error(ctx, APSPIE_ERR_OVERFLOW, "radix sort: %lld keys too many", n);
-  unsigned nt = (unsigned)tiles;
-  auto *counts = (unsigned *)workspace(ctx, kSlotSortHist, sizeof(unsigned) * (size_t)nt * kRadix);
-  if (!counts) return APSPIE_ERR_OOM;
+  const int npass = (bits + kRadixBits - 1) / kRadixBits;
+  if (npass > kMaxPasses || n >= (1ll << 40))
+    return set_error(ctx, APSPIE_ERR_OVERFLOW, "radix sort: %lld keys of %d bits", n, bits);
+  const long long tiles = (n + kSortTile - 1) / kSortTile;
+  // [histograms: npass x 256 u64][tile counters: 8 x u32, padded][err][status: tiles x 256 u64]
+  const size_t hist_bytes = sizeof(unsigned long long) * kMaxPasses * kRadix;
+  const size_t head = hist_bytes + 64;
+  const size_t bytes = head + sizeof(unsigned long long) * (size_t)tiles * kRadix;
+  auto *ws = (unsigned char *)workspace(ctx, kSlotSortHist, bytes);
+  if (!ws) return APSPIE_ERR_OOM;
+  auto *ghist = (unsigned long long *)ws;
+  auto *counters = (unsigned *)(ws + hist_bytes);
+  int *err = (int *)(ws + hist_bytes + 48);
+  auto *status = (unsigned long long *)(ws + head);
+  cudaStream_t st = ctx->stream;
+  // zero the histograms, counters, error word and every status word
+  cudaMemsetAsync(ws, 0, bytes, st);
+  const int hgrid = (int)std::max(1ll, std::min((n + kSortThreads * 8 - 1) / (kSortThreads * 8),
+                                                (long long)ctx->num_sms * 4));
+  radix_histograms<K><<<hgrid, kSortThreads, 0, st>>>(ka, n, npass, ghist);
+  radix_digit_offsets<kRadix><<<1, kRadix, 0, st>>>(ghist, npass);
+  int rc = check_launch(ctx, "radix_histograms", 2);
+  if (rc) return rc;
   K *kin = ka, *kout = kb;
   V *vin = va, *vout = vb;
-  for (int shift = 0; shift < bits; shift += kRadixBits) {
-    radix_count<K><<<nt, kSortThreads, 0, ctx->stream>>>(kin, n, shift, counts, nt);
-    int rc = check_launch(ctx, "radix_count");
-    if (rc) return rc;
-    rc = device_exclusive_scan<unsigned>(ctx, counts, counts, (long long)nt * kRadix, nullptr);
-    if (rc) return rc;
-    radix_scatter<K, V><<<nt, kSortThreads, 0, ctx->stream>>>(kin, vin, kout, vout, n, shift,
-                                                              counts, nt);
-    rc = check_launch(ctx, "radix_scatter");
+  for (int p = 0; p < npass; ++p) {
+    radix_onesweep<K, V><<<(unsigned)tiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, p,
+                                                                   ghist, status, counters + p,
+                                                                   err);
+    rc = check_launch(ctx, "radix_onesweep");
     if (rc) return rc;
     std::swap(kin, kout);
     std::swap(vin, vout);
