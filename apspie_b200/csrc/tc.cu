@@ -289,38 +289,58 @@ __global__ void rank_to_perm(int m, const int *order, int *perm) {
     perm[order[r]] = r;
 }
 
-__global__ void lower_edges(int m, int cbits, const int *__restrict__ ptr,
-                            const int *__restrict__ ind, const int *__restrict__ perm,
-                            unsigned long long *keys, unsigned *count) {
+// Per vertex v of new id r: how many neighbours rank below r (the length
+// of L's row r) and how many above (v's entries in L's columns).  A warp
+// per vertex, both counts from one read of the row.
+__global__ void split_counts(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
+                            const int *__restrict__ perm, int *lcnt, int *ucnt) {
   const int lane = lane_id();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
-  for (int u = gwarp; u < m; u += nwarps) {
-    const int pu = __ldg(perm + u);
-    const int s = __ldg(ptr + u), e = __ldg(ptr + u + 1);
-    for (int k0 = s; k0 < e; k0 += 32) {
-      int k = k0 + lane;
-      int pv = k < e ? __ldg(perm + __ldg(ind + k)) : INT_MAX;
-      bool keep = pv < pu;
-      unsigned slot = warp_append(keep, count);
-      if (keep) keys[slot] = ((unsigned long long)pu << cbits) | (unsigned)pv;
+  for (int v = gwarp; v < m; v += nwarps) {
+    const int r = __ldg(perm + v);
+    const int s = __ldg(ptr + v), e = __ldg(ptr + v + 1);
+    int lo = 0, hi = 0;
+    for (int k = s + lane; k < e; k += 32) {
+      const int pu = __ldg(perm + __ldg(ind + k));
+      lo += pu < r;
+      hi += pu > r;
+    }
+    lo = warp_sum(lo);
+    hi = warp_sum(hi);
+    if (lane == 0) {
+      lcnt[r] = lo;
+      ucnt[r] = hi;
     }
   }
 }
 
-__global__ void unpack_lower(long long n, int cbits, const unsigned long long *keys, int *Li,
-                             int *rowcnt) {
-  const unsigned long long mask = (1ull << cbits) - 1ull;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x) {
-    unsigned long long k = keys[t];
-    Li[t] = (int)(k & mask);
-    atomicAdd(rowcnt + (int)(k >> cbits), 1);
+// L's entries as (row new(u), column r) pairs, grouped by column r in
+// ascending order (segment uoff[r]): a stable sort by row then leaves each
+// row's columns ascending.  A warp per vertex, lanes compacted by ballot.
+__global__ void upper_pairs(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
+                            const int *__restrict__ perm, const int *__restrict__ uoff,
+                            unsigned *rows, int *cols) {
+  const int lane = lane_id();
+  const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  for (int v = gwarp; v < m; v += nwarps) {
+    const int r = __ldg(perm + v);
+    const int s = __ldg(ptr + v), e = __ldg(ptr + v + 1);
+    int out = __ldg(uoff + r);
+    for (int k0 = s; k0 < e; k0 += 32) {
+      const int k = k0 + lane;
+      const int pu = k < e ? __ldg(perm + __ldg(ind + k)) : -1;
+      const bool keep = pu > r;
+      const unsigned mask = __ballot_sync(kFull, keep);
+      if (keep) {
+        const int at = out + __popc(mask & ((1u << lane) - 1u));
+        rows[at] = (unsigned)pu;
+        cols[at] = r;
+      }
+      out += __popc(mask);
+    }
   }
-}
-
-__global__ void zero_ints(int n, int *p) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0;
 }
 
 int tgrid(apspie_context *ctx, long long n, int threads, int per_sm = 16) {
@@ -365,34 +385,52 @@ int apspie_tc_prepare(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr, cons
   rc = device_radix_sort<unsigned, int>(ctx, dk, ids, dk2, ids2, m, dbits, &in_b);
   if (rc) return rc;
   rank_to_perm<<<tgrid(ctx, m, 256), 256, 0, st>>>(m, in_b ? ids2 : ids, d_perm);
-  // 2. keep new(v) < new(u), packed (new(u) << cbits | new(v))
-  size_t cap = (size_t)std::max<int64_t>(1, nnz);
-  auto *ka = (unsigned long long *)workspace(ctx, kSlotMisc0, sizeof(unsigned long long) * cap);
-  auto *kb = (unsigned long long *)workspace(ctx, kSlotMisc1, sizeof(unsigned long long) * cap);
-  auto *va = (int *)workspace(ctx, kSlotMisc2, sizeof(int) * cap);
-  auto *vb = (int *)workspace(ctx, kSlotMisc3, sizeof(int) * cap);
-  if (!ka || !kb || !va || !vb) return APSPIE_ERR_OOM;
-  lower_edges<<<tgrid(ctx, (long long)m * 32, 256), 256, 0, st>>>(m, cbits, d_ptr, d_ind, d_perm,
-                                                                  ka, small + 2);
-  rc = check_launch(ctx, "lower_edges", 2);
+  // 2. row lengths of L (indexed by new id) and each vertex's count above it
+  auto *lcnt = d_Lptr;
+  auto *uoff = (int *)workspace(ctx, kSlotMisc0, sizeof(int) * ((size_t)m + 1));
+  if (!uoff) return APSPIE_ERR_OOM;
+  cudaMemsetAsync(lcnt + m, 0, sizeof(int), st);
+  cudaMemsetAsync(uoff + m, 0, sizeof(int), st);
+  split_counts<<<tgrid(ctx, (long long)m * 32, 256), 256, 0, st>>>(m, d_ptr, d_ind, d_perm, lcnt,
+                                                                   uoff);
+  rc = check_launch(ctx, "split_counts");
   if (rc) return rc;
-  cudaMemcpyAsync(hs, small + 2, 4, cudaMemcpyDeviceToHost, st);
-  rc = check_cuda(ctx, cudaStreamSynchronize(st), "tc_prepare count");
+  // exclusive scans of the m + 1 entries (entry m is 0): offsets + totals
+  rc = device_exclusive_scan<int>(ctx, lcnt, d_Lptr, (long long)m + 1, nullptr);
+  if (rc) return rc;
+  rc = device_exclusive_scan<int>(ctx, uoff, uoff, (long long)m + 1, nullptr);
+  if (rc) return rc;
+  cudaMemcpyAsync(hs, d_Lptr + m, 4, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(hs + 1, uoff + m, 4, cudaMemcpyDeviceToHost, st);
+  rc = check_cuda(ctx, cudaStreamSynchronize(st), "tc_prepare counts");
   if (rc) return rc;
   const long long lnnz = hs[0];
-  // 3. sort by (row, col); values are unused
-  rc = device_radix_sort<unsigned long long, int>(ctx, ka, va, kb, vb, lnnz, 2 * cbits, &in_b);
-  if (rc) return rc;
-  // 4. columns and row offsets
-  zero_ints<<<tgrid(ctx, m + 1, 256), 256, 0, st>>>(m + 1, d_Lptr);
-  unpack_lower<<<tgrid(ctx, lnnz, 256), 256, 0, st>>>(lnnz, cbits, in_b ? kb : ka, d_Lind,
-                                                      d_Lptr);
-  rc = check_launch(ctx, "unpack_lower", 2);
-  if (rc) return rc;
-  // d_Lptr[i] holds row i's count and d_Lptr[m] = 0: the exclusive scan of
-  // the m + 1 entries is the offset array
-  rc = device_exclusive_scan<int>(ctx, d_Lptr, d_Lptr, (long long)m + 1, nullptr);
-  if (rc) return rc;
+  // every edge below one end is above the other only when the graph is symmetric
+  if (hs[1] != hs[0] || lnnz > nnz / 2)
+    return set_error(ctx, APSPIE_ERR_INVALID,
+                     "apspie_tc_prepare: the graph is not symmetric (%u entries below, %u above)",
+                     hs[0], hs[1]);
+  if (lnnz > 0) {
+    // 3. (row, column) pairs grouped by ascending column, stable-sorted by row:
+    //    the columns come out in d_Lind (or in the other buffer, then copied)
+    auto *ka = (unsigned *)workspace(ctx, kSlotMisc1, sizeof(unsigned) * (size_t)lnnz);
+    auto *kb = (unsigned *)workspace(ctx, kSlotMisc2, sizeof(unsigned) * (size_t)lnnz);
+    auto *va = (int *)workspace(ctx, kSlotMisc3, sizeof(int) * (size_t)lnnz);
+    if (!ka || !kb || !va) return APSPIE_ERR_OOM;
+    upper_pairs<<<tgrid(ctx, (long long)m * 32, 256), 256, 0, st>>>(m, d_ptr, d_ind, d_perm,
+                                                                    uoff, ka, va);
+    rc = check_launch(ctx, "upper_pairs");
+    if (rc) return rc;
+    in_b = false;
+    rc = device_radix_sort<unsigned, int>(ctx, ka, va, kb, d_Lind, lnnz, cbits, &in_b);
+    if (rc) return rc;
+    if (!in_b) {
+      rc = check_cuda(ctx, cudaMemcpyAsync(d_Lind, va, sizeof(int) * (size_t)lnnz,
+                                           cudaMemcpyDeviceToDevice, st),
+                      "tc_prepare copy");
+      if (rc) return rc;
+    }
+  }
   *h_lnnz = lnnz;
   return APSPIE_OK;
 }

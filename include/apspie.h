@@ -487,7 +487,9 @@ int apspie_csr_copy_out(apspie_ctx ctx, const apspie_csr *C, int *d_ptr,
  * ascending (degree, id) -- d_perm[v] = new id -- and L(new(u), :) = the new
  * ids of u's neighbours below new(u), rows sorted.  test/tc/main.cu:40-55,
  * 172-175 builds the strict triangles on the host.  d_Lptr holds m + 1
- * entries, d_Lind at least nnz / 2; *h_lnnz = nnz(L).  Synchronises. */
+ * entries, d_Lind at least nnz / 2; *h_lnnz = nnz(L).  A graph with more
+ * entries below the new order than above it (or the reverse) is not
+ * symmetric and is refused with APSPIE_ERR_INVALID.  Synchronises. */
 int apspie_tc_prepare(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr,
                       const int *d_ind, int *d_perm, int *d_Lptr, int *d_Lind,
                       int64_t *h_lnnz);

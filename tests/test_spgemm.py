@@ -147,6 +147,15 @@ def test_tc_fixtures(ctx, golden, fixture_names):
         _tc(ctx, h)
 
 
+def test_tc_prepare_rejects_a_directed_graph(ctx):
+    """L is read from both ends of every edge, so the input must be
+    symmetric: a directed R-MAT graph is refused, not miscounted."""
+    import apspie_b200 as ap
+    g = ap.gen_rmat(12, 16, seed=1, symmetric=False).to_device(with_transpose=False)
+    with pytest.raises(ap.ApspieError, match="not symmetric"):
+        ap.tc_prepare(ctx, g)
+
+
 @pytest.mark.parametrize("scale", [12, 18])
 def test_tc_rmat(ctx, scale):
     """R-MAT scale 18, edge factor 16, symmetrised: the TC configuration."""
