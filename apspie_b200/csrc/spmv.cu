@@ -4,14 +4,17 @@
 //
 // Replaces the reference's dense SpMV calls: mgpu::SpmvCsrBinary behind
 // spmv() (src/bfs.cuh:12-14) and cusparseScsrmv behind cuspmv()
-// (src/tc.cuh:18-59).  Three tiers: rows of at most kMidRow entries go to
-// groups of L lanes (L = 4 .. 32 from the mean row length, 32 / L rows per
-// warp in flight, so that short rows do not leave a warp with one chain of
-// dependent loads); rows of at most kLongRow entries are listed and go one
-// warp per row; longer rows (hubs) are listed and split into chunks that
-// are spread over all blocks.  Each row is reduced in a fixed
-// order (per-lane partials, then a fixed butterfly / tree, then the chunks
-// in order), so the result does not depend on scheduling.
+// (src/tc.cuh:18-59).  Merge-path partition (Merrill & Garland, "Merge-based
+// parallel sparse matrix-vector multiplication", SC'16): the row ends
+// (ptr[1..m]) and the nonzeros form one merged list of m + nnz items, cut
+// into tiles of kMpTile items, so a tile's work is fixed whatever the row
+// lengths (hubs, empty rows).  A block stages its tile's terms and row
+// offsets in shared memory (coalesced loads of ind / val, gathers of x),
+// then reduces each row's segment: short segments a thread each, long ones
+// a warp each.  Rows that end in the tile are written; a row that runs on
+// past the tile leaves its partial (carry) and the tile where it ends its
+// head partial, which spmv_merge_fixup adds in tile order.  Every sum is
+// taken in a fixed order, so the result does not depend on scheduling.
 // PLUS_TIMES accumulates in double and rounds once.
 #include <cuda_runtime.h>
 
@@ -25,14 +28,10 @@ namespace apspie {
 namespace {
 
 constexpr int kSr_PlusTimes = 0, kSr_MinPlus = 1, kSr_MaxTimes = 2, kSr_OrAnd = 3;
-constexpr int kMidRow = 256;
-constexpr int kLongRow = 4096;
-constexpr int kLongThreads = 512;
-
-struct SpmvSmall {
-  unsigned nlong;
-  unsigned nmid;
-};
+constexpr int kMpThreads = 256;
+constexpr int kMpItems = 8;                     // merged items per thread
+constexpr int kMpTile = kMpThreads * kMpItems;  // row ends + nonzeros per tile
+constexpr int kMpWarpSeg = 32;                  // longer segments are reduced by a warp
 
 // the semiring's (+) identity and one (x) term, as float (double for plus)
 __device__ __forceinline__ double sr_identity(int sr) {
@@ -66,168 +65,115 @@ __device__ __forceinline__ float sr_out(int sr, double v) {
   return (float)v;
 }
 
-// Sum of the terms of entries k0, k0 + stride, ... < k1 in a fixed order:
-// four index loads, then four x loads, in flight per step (the loads of a
-// lane's entries are independent; a plain loop would wait for each x
-// before issuing the next index load).
-__device__ __forceinline__ double row_part(int sr, int k0, int k1, int stride,
-                                           const int *__restrict__ ind,
-                                           const float *__restrict__ val,
-                                           const float *__restrict__ x) {
-  double acc = sr_identity(sr);
-  int k = k0;
-  for (; k + 3 * stride < k1; k += 4 * stride) {
-    int c[4];
-    float a[4], xv[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      c[q] = __ldg(ind + k + q * stride);
-      a[q] = val ? __ldg(val + k + q * stride) : 1.0f;
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) xv[q] = __ldg(x + c[q]);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) acc = sr_add(sr, acc, sr_term(sr, a[q], xv[q]));
+// Merge-path coordinate of diagonal d of the merged list: (i, j) = row ends
+// and nonzeros before it.  Row end i (ptr[i + 1]) precedes nonzero j iff
+// ptr[i + 1] <= j.
+__device__ __forceinline__ int2 merge_coord(long long d, int m, int nnz,
+                                           const int *__restrict__ ptr) {
+  int lo = (int)max(0ll, d - nnz), hi = (int)min(d, (long long)m);
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if ((long long)__ldg(ptr + mid + 1) <= d - mid - 1) lo = mid + 1; else hi = mid;
   }
-  for (; k < k1; k += stride) {
-    const float a = val ? __ldg(val + k) : 1.0f;
-    acc = sr_add(sr, acc, sr_term(sr, a, __ldg(x + __ldg(ind + k))));
-  }
-  return acc;
+  return make_int2(lo, (int)(d - lo));
 }
 
-// Groups of L lanes, one row each; rows longer than kMidRow are listed for
-// spmv_warp_rows.  The row loop is warp-uniform (every lane runs the same
-// number of batches), so the group reductions stay converged.
-template <int L>
-__global__ void spmv_group_rows(int sr, int m, const int *__restrict__ ptr,
-                                const int *__restrict__ ind, const float *__restrict__ val,
-                                const float *__restrict__ x, float *y, unsigned *nmid,
-                                int *mid_rows) {
-  constexpr int G = 32 / L;
-  const int lane = lane_id(), sub = lane & (L - 1), grp = lane / L;
-  const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
-  for (int base = gwarp * G; base < m; base += nwarps * G) {
-    const int r = base + grp;
-    int s = 0, e = 0;
-    if (r < m) {
-      s = __ldg(ptr + r);
-      e = __ldg(ptr + r + 1);
-    }
-    const bool mid = e - s > kMidRow;
-    if (mid && sub == 0) mid_rows[atomicAdd(nmid, 1u)] = r;
-    double acc = mid ? sr_identity(sr) : row_part(sr, s + sub, e, L, ind, val, x);
-#pragma unroll
-    for (int o = L / 2; o > 0; o >>= 1) acc = sr_add(sr, acc, __shfl_xor_sync(kFull, acc, o));
-    if (sub == 0 && r < m && !mid) y[r] = sr_out(sr, acc);
-  }
+// coordinates of the ntiles + 1 tile boundaries
+__global__ void spmv_merge_plan(int m, int nnz, int ntiles, const int *__restrict__ ptr,
+                                int2 *coord) {
+  const long long total = (long long)m + nnz;
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= ntiles; b += gridDim.x * blockDim.x)
+    coord[b] = merge_coord(min((long long)b * kMpTile, total), m, nnz, ptr);
 }
 
-// One warp per row, over every row (list == nullptr) or the listed ones;
-// rows longer than kLongRow are listed for the hub chunks (spmv_long_plan,
-// spmv_long_chunks, spmv_long_finish).
-__global__ void spmv_warp_rows(int sr, int m, const int *__restrict__ ptr,
-                               const int *__restrict__ ind, const float *__restrict__ val,
-                               const float *__restrict__ x, float *y, unsigned *nlong,
-                               int *long_rows, const unsigned *nlist, const int *list) {
-  const int lane = lane_id();
-  const int n = list ? (int)*nlist : m;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
-       i += (gridDim.x * blockDim.x) >> 5) {
-    const int r = list ? list[i] : i;
-    const int s = __ldg(ptr + r), e = __ldg(ptr + r + 1);
-    if (e - s > kLongRow) {
-      if (lane == 0) long_rows[atomicAdd(nlong, 1u)] = r;
+// One tile per block.  Tile b holds the row ends [i0, i1) and the nonzeros
+// [j0, j1); it touches rows i0 .. min(i1, m - 1).  Row i1 (when < m) is
+// open at the tile's end: its partial goes to carry_val[b].  Row i0, when
+// it has nonzeros before j0 and ends in this tile, goes to head_val[b].
+__global__ void __launch_bounds__(kMpThreads)
+spmv_merge_tiles(int sr, int m, const int *__restrict__ ptr, const int *__restrict__ ind,
+                 const float *__restrict__ val, const float *__restrict__ x, float *y,
+                 const int2 *__restrict__ coord, int *carry_row, double *carry_val,
+                 int *head_row, double *head_val) {
+  __shared__ double s_term[kMpTile];
+  __shared__ int s_ptr[kMpTile + 2];
+  __shared__ int s_long[kMpTile / (kMpWarpSeg + 1) + 1];
+  __shared__ unsigned s_nlong;
+  const int b = blockIdx.x, t = threadIdx.x;
+  const int2 c0 = coord[b], c1 = coord[b + 1];
+  const int i0 = c0.x, j0 = c0.y, i1 = c1.x, j1 = c1.y;
+  const int nr = min(i1, m - 1) - i0 + 1;  // rows touched (i0 < m in every tile)
+  const int nz = j1 - j0;
+  if (t == 0) s_nlong = 0;
+  for (int q = t; q <= nr; q += kMpThreads) s_ptr[q] = __ldg(ptr + i0 + q);
+  // the tile's terms: all index / value loads, then all x loads, in flight
+  {
+    int c[kMpItems];
+    float a[kMpItems], xv[kMpItems];
+#pragma unroll
+    for (int u = 0; u < kMpItems; ++u) {
+      const int q = t + u * kMpThreads;
+      c[u] = q < nz ? __ldg(ind + j0 + q) : 0;
+      a[u] = q < nz ? (val ? __ldg(val + j0 + q) : 1.0f) : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < kMpItems; ++u) xv[u] = t + u * kMpThreads < nz ? __ldg(x + c[u]) : 0.0f;
+#pragma unroll
+    for (int u = 0; u < kMpItems; ++u) {
+      const int q = t + u * kMpThreads;
+      if (q < nz) s_term[q] = sr_term(sr, a[u], xv[u]);
+    }
+  }
+  if (t == 0) {
+    carry_row[b] = i1 < m ? i1 : -1;
+    head_row[b] = (i0 < i1 && s_ptr[0] < j0) ? i0 : -1;
+  }
+  __syncthreads();
+  auto emit = [&](int q, double acc) {
+    const int i = i0 + q;
+    if (i == i1) carry_val[b] = acc;                     // open at the tile's end
+    else if (q == 0 && s_ptr[0] < j0) head_val[b] = acc;  // began in an earlier tile
+    else y[i] = sr_out(sr, acc);
+  };
+  // short segments a thread each; long ones listed for the warps
+  for (int q = t; q < nr; q += kMpThreads) {
+    const int s = max(s_ptr[q], j0) - j0, e = min(s_ptr[q + 1], j1) - j0;
+    if (e - s > kMpWarpSeg) {
+      s_long[atomicAdd(&s_nlong, 1u)] = q;
       continue;
     }
-    double acc = row_part(sr, s + lane, e, 32, ind, val, x);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc = sr_add(sr, acc, __shfl_xor_sync(kFull, acc, o));
-    if (lane == 0) y[r] = sr_out(sr, acc);
+    double acc = sr_identity(sr);
+    for (int k = s; k < e; ++k) acc = sr_add(sr, acc, s_term[k]);
+    emit(q, acc);
   }
-}
-
-// Rows longer than kLongRow (hubs) in chunks of kLongChunk entries spread
-// over all blocks.  spmv_long_plan (one block) numbers the listed rows'
-// chunks in list order (first_chunk, an exclusive scan; the total after the
-// last row); chunk g goes to block g mod gridDim.x, which finds its row by
-// binary search and reduces it in a fixed order into partial[g];
-// spmv_long_finish adds each row's partials in chunk order, so the result
-// does not depend on scheduling.
-constexpr int kLongChunk = 8192;
-
-__global__ void __launch_bounds__(1024)
-spmv_long_plan(const int *__restrict__ ptr, const unsigned *nlong, const int *long_rows,
-               unsigned *first_chunk) {
-  __shared__ unsigned sw[33];
-  const unsigned n = *nlong;
-  unsigned carry = 0;
-  for (unsigned b = 0; b < n; b += blockDim.x) {
-    const unsigned i = b + threadIdx.x;
-    unsigned nc = 0;
-    if (i < n) {
-      const int r = long_rows[i];
-      nc = (unsigned)((__ldg(ptr + r + 1) - __ldg(ptr + r) + kLongChunk - 1) / kLongChunk);
-    }
-    const unsigned lane = lane_id(), w = warp_in_block(), nw = blockDim.x >> 5;
-    const unsigned incl = warp_incl_scan(nc);
-    if (lane == 31) sw[w] = incl;
-    __syncthreads();
-    if (w == 0) {
-      const unsigned v = lane < nw ? sw[lane] : 0u;
-      const unsigned vi = warp_incl_scan(v);
-      if (lane < nw) sw[lane] = vi - v;
-      if (lane == nw - 1) sw[32] = vi;
-    }
-    __syncthreads();
-    if (i < n) first_chunk[i] = carry + sw[w] + incl - nc;
-    carry += sw[32];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) first_chunk[n] = carry;
-}
-
-__global__ void __launch_bounds__(kLongThreads)
-spmv_long_chunks(int sr, const int *__restrict__ ptr, const int *__restrict__ ind,
-                 const float *__restrict__ val, const float *__restrict__ x,
-                 const unsigned *nlong, const int *long_rows, const unsigned *first_chunk,
-                 double *partial) {
-  __shared__ double part[kLongThreads / 32];
+  __syncthreads();
   const int lane = lane_id(), w = warp_in_block();
-  const unsigned n = *nlong;
-  const unsigned total = n ? first_chunk[n] : 0u;
-  for (unsigned g = blockIdx.x; g < total; g += gridDim.x) {
-    unsigned lo = 0, hi = n - 1;
-    while (lo < hi) {
-      const unsigned mid = (lo + hi + 1) >> 1;
-      if (first_chunk[mid] <= g) lo = mid; else hi = mid - 1;
-    }
-    const int r = long_rows[lo];
-    const int s = __ldg(ptr + r), e = __ldg(ptr + r + 1);
-    const int k0 = s + (int)(g - first_chunk[lo]) * kLongChunk, k1 = min(e, k0 + kLongChunk);
-    double acc = row_part(sr, k0 + (int)threadIdx.x, k1, kLongThreads, ind, val, x);
+  for (unsigned l = w; l < s_nlong; l += kMpThreads / 32) {
+    const int q = s_long[l];
+    const int s = max(s_ptr[q], j0) - j0, e = min(s_ptr[q + 1], j1) - j0;
+    double acc = sr_identity(sr);
+    for (int k = s + lane; k < e; k += 32) acc = sr_add(sr, acc, s_term[k]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc = sr_add(sr, acc, __shfl_xor_sync(kFull, acc, o));
-    if (lane == 0) part[w] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = part[0];
-      for (int j = 1; j < kLongThreads / 32; ++j) t = sr_add(sr, t, part[j]);
-      partial[g] = t;
-    }
-    __syncthreads();
+    if (lane == 0) emit(q, acc);
   }
 }
 
-__global__ void spmv_long_finish(int sr, const unsigned *nlong, const int *long_rows,
-                                 const double *partial, const unsigned *first_chunk, float *y) {
-  const unsigned n = *nlong;
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const unsigned c0 = first_chunk[i], c1 = first_chunk[i + 1];
-    double t = partial[c0];
-    for (unsigned c = c0 + 1; c < c1; ++c) t = sr_add(sr, t, partial[c]);
-    y[long_rows[i]] = sr_out(sr, t);
+// Rows that span tiles: the tile where row r ends (head_row[b] == r) adds,
+// in tile order, the carries of the tiles before it that were open on r,
+// then its own head partial.
+__global__ void spmv_merge_fixup(int sr, int ntiles, const int *__restrict__ carry_row,
+                                 const double *__restrict__ carry_val,
+                                 const int *__restrict__ head_row,
+                                 const double *__restrict__ head_val, float *y) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < ntiles; b += gridDim.x * blockDim.x) {
+    const int r = head_row[b];
+    if (r < 0) continue;
+    int first = b - 1;  // carry_row[b - 1] == r: row r is i0 of tile b
+    while (first > 0 && carry_row[first - 1] == r) --first;
+    double acc = carry_val[first];
+    for (int u = first + 1; u < b; ++u) acc = sr_add(sr, acc, carry_val[u]);
+    y[r] = sr_out(sr, sr_add(sr, acc, head_val[b]));
   }
 }
 
@@ -242,44 +188,19 @@ extern "C" int apspie_spmv(apspie_ctx ctx, int semiring, int m, int64_t nnz, con
   if (semiring < 0 || semiring > 3 || m <= 0 || nnz < 0 || nnz >= (int64_t)INT32_MAX || !d_ptr ||
       (nnz > 0 && !d_ind) || !d_x || !d_y)
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_spmv: bad arguments");
-  auto *sm = (SpmvSmall *)workspace(ctx, kSlotSmall, sizeof(SpmvSmall));
-  auto *rows = (int *)workspace(ctx, kSlotMisc0, sizeof(int) * ((size_t)nnz / kLongRow + 1));
-  auto *mid = (int *)workspace(ctx, kSlotMisc1, sizeof(int) * ((size_t)nnz / kMidRow + 1));
-  // chunks of the long rows: at most nnz / kLongChunk full ones plus one
-  // partial per row; each row's first chunk number
-  const size_t max_long = (size_t)nnz / kLongRow + 1;
-  auto *partial = (double *)workspace(ctx, kSlotMisc2,
-                                      sizeof(double) * ((size_t)nnz / kLongChunk + max_long + 1));
-  auto *first = (unsigned *)workspace(ctx, kSlotMisc3, sizeof(unsigned) * (max_long + 1));
-  if (!sm || !rows || !mid || !partial || !first) return APSPIE_ERR_OOM;
+  const long long items = (long long)m + nnz;
+  const int ntiles = (int)((items + kMpTile - 1) / kMpTile);
+  auto *coord = (int2 *)workspace(ctx, kSlotMisc0, sizeof(int2) * ((size_t)ntiles + 1));
+  auto *rows = (int *)workspace(ctx, kSlotMisc1, sizeof(int) * 2 * (size_t)ntiles);
+  auto *vals = (double *)workspace(ctx, kSlotMisc2, sizeof(double) * 2 * (size_t)ntiles);
+  if (!coord || !rows || !vals) return APSPIE_ERR_OOM;
   cudaStream_t st = ctx->stream;
-  cudaMemsetAsync(sm, 0, sizeof(SpmvSmall), st);
-  // lanes per short row from the mean row length
-  const double mean = (double)nnz / m;
-  const int L = mean <= 6 ? 4 : (mean <= 20 ? 8 : (mean <= 48 ? 16 : 32));
-  const long long warps = std::min((long long)m, (long long)ctx->num_sms * 64);
-  const unsigned blocks = (unsigned)((warps * 32 + 255) / 256);
-  int launches = 2;
-  if (L == 32) {
-    spmv_warp_rows<<<blocks, 256, 0, st>>>(semiring, m, d_ptr, d_ind, d_val, d_x, d_y, &sm->nlong,
-                                           rows, nullptr, nullptr);
-  } else {
-    if (L == 4)
-      spmv_group_rows<4><<<blocks, 256, 0, st>>>(semiring, m, d_ptr, d_ind, d_val, d_x, d_y,
-                                                 &sm->nmid, mid);
-    else if (L == 8)
-      spmv_group_rows<8><<<blocks, 256, 0, st>>>(semiring, m, d_ptr, d_ind, d_val, d_x, d_y,
-                                                 &sm->nmid, mid);
-    else
-      spmv_group_rows<16><<<blocks, 256, 0, st>>>(semiring, m, d_ptr, d_ind, d_val, d_x, d_y,
-                                                  &sm->nmid, mid);
-    spmv_warp_rows<<<ctx->num_sms * 8, 256, 0, st>>>(semiring, m, d_ptr, d_ind, d_val, d_x, d_y,
-                                                    &sm->nlong, rows, &sm->nmid, mid);
-    ++launches;
-  }
-  spmv_long_plan<<<1, 1024, 0, st>>>(d_ptr, &sm->nlong, rows, first);
-  spmv_long_chunks<<<ctx->num_sms * 2, kLongThreads, 0, st>>>(
-      semiring, d_ptr, d_ind, d_val, d_x, &sm->nlong, rows, first, partial);
-  spmv_long_finish<<<4, 256, 0, st>>>(semiring, &sm->nlong, rows, partial, first, d_y);
-  return check_launch(ctx, "apspie_spmv", launches + 2);
+  const int pgrid = (ntiles + 1 + 255) / 256;
+  spmv_merge_plan<<<pgrid, 256, 0, st>>>(m, (int)nnz, ntiles, d_ptr, coord);
+  spmv_merge_tiles<<<ntiles, kMpThreads, 0, st>>>(semiring, m, d_ptr, d_ind, d_val, d_x, d_y,
+                                                  coord, rows, vals, rows + ntiles,
+                                                  vals + ntiles);
+  spmv_merge_fixup<<<(ntiles + 255) / 256, 256, 0, st>>>(semiring, ntiles, rows, vals,
+                                                         rows + ntiles, vals + ntiles, d_y);
+  return check_launch(ctx, "apspie_spmv", 3);
 }
