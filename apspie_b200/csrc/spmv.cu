@@ -65,25 +65,31 @@ __device__ __forceinline__ float sr_out(int sr, double v) {
   return (float)v;
 }
 
-// Merge-path coordinate of diagonal d of the merged list: (i, j) = row ends
-// and nonzeros before it.  Row end i (ptr[i + 1]) precedes nonzero j iff
-// ptr[i + 1] <= j.
-__device__ __forceinline__ int2 merge_coord(long long d, int m, int nnz,
-                                           const int *__restrict__ ptr) {
-  int lo = (int)max(0ll, d - nnz), hi = (int)min(d, (long long)m);
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if ((long long)__ldg(ptr + mid + 1) <= d - mid - 1) lo = mid + 1; else hi = mid;
-  }
-  return make_int2(lo, (int)(d - lo));
-}
-
-// coordinates of the ntiles + 1 tile boundaries
+// coordinates of the ntiles + 1 tile boundaries, a warp each: a 32-way
+// search (each round probes 32 evenly spaced rows and keeps the interval
+// between the last probe that precedes the diagonal and the first that
+// does not), then one round over the last <= 32 candidates
 __global__ void spmv_merge_plan(int m, int nnz, int ntiles, const int *__restrict__ ptr,
                                 int2 *coord) {
   const long long total = (long long)m + nnz;
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= ntiles; b += gridDim.x * blockDim.x)
-    coord[b] = merge_coord(min((long long)b * kMpTile, total), m, nnz, ptr);
+  const int lane = lane_id();
+  for (int b = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); b <= ntiles;
+       b += (int)((gridDim.x * blockDim.x) >> 5)) {
+    const long long d = min((long long)b * kMpTile, total);
+    // C(i): row end i precedes the diagonal's nonzero, true below the answer
+    auto before = [&](long long i) { return (long long)__ldg(ptr + i + 1) <= d - i - 1; };
+    long long lo = max(0ll, d - nnz), hi = min(d, (long long)m);
+    while (hi - lo > 32) {
+      const long long step = (hi - lo + 31) / 32;
+      const long long p = lo + lane * step;
+      const int k = __popc(__ballot_sync(kFull, p < hi && before(p)));
+      const long long nlo = k == 0 ? lo : lo + (k - 1) * step + 1;
+      hi = k < 32 ? min(hi, lo + k * step) : hi;
+      lo = nlo;
+    }
+    const int k = __popc(__ballot_sync(kFull, lo + lane < hi && before(lo + lane)));
+    if (lane == 0) coord[b] = make_int2((int)(lo + k), (int)(d - lo - k));
+  }
 }
 
 // One tile per block.  Tile b holds the row ends [i0, i1) and the nonzeros
@@ -195,7 +201,7 @@ extern "C" int apspie_spmv(apspie_ctx ctx, int semiring, int m, int64_t nnz, con
   auto *vals = (double *)workspace(ctx, kSlotMisc2, sizeof(double) * 2 * (size_t)ntiles);
   if (!coord || !rows || !vals) return APSPIE_ERR_OOM;
   cudaStream_t st = ctx->stream;
-  const int pgrid = (ntiles + 1 + 255) / 256;
+  const int pgrid = (int)std::min<long long>((32ll * (ntiles + 1) + 255) / 256, ctx->num_sms * 16ll);
   spmv_merge_plan<<<pgrid, 256, 0, st>>>(m, (int)nnz, ntiles, d_ptr, coord);
   spmv_merge_tiles<<<ntiles, kMpThreads, 0, st>>>(semiring, m, d_ptr, d_ind, d_val, d_x, d_y,
                                                   coord, rows, vals, rows + ntiles,
