@@ -21,9 +21,11 @@
 //     their thousands of short levels do not keep the whole GPU from the
 //     other queries;
 //   * continuous batching: there are two batch slots.  While one slot's
-//     groups run, queries that arrive are admitted into the other slot and
-//     launched right away, queued on the GPU behind (and overlapping the
-//     copies of) the running ones.
+//     groups run, queries that arrive are admitted into the other slot,
+//     which is launched, queued on the GPU behind (and overlapping the
+//     copies of) the running groups, once the running slot's main lane is
+//     down to its last group; until then the queries keep gathering, so
+//     under load the groups grow instead of the batches multiplying.
 // Each query's result row is copied into the caller's host buffer, or into
 // its device buffer (or dropped, for load tests), and its latency (submit ->
 // result in host / device memory) is recorded.  MIS priorities (mt19937 of
@@ -508,6 +510,26 @@ void worker_main(apspie_server *s) {
           cudaEventSynchronize(g.end);
           break;
         }
+      continue;
+    }
+    // One slot free, the other running: while its main lane still has two
+    // or more groups queued the GPU has work, so the next batch waits and
+    // gathers the queries that arrive meanwhile (larger groups share more
+    // of each traversal); it forms once the last main-lane group runs.
+    Group *queued = nullptr;
+    for (Slot &sl : s->slots) {
+      if (!sl.busy) continue;
+      int left = 0;
+      for (Group &g : sl.groups)
+        if (!g.done && g.lane == 0 && g.end) {
+          if (!queued) queued = &g;
+          ++left;
+        }
+      if (left < 2) queued = nullptr;
+      if (queued) break;
+    }
+    if (queued) {
+      cudaEventSynchronize(queued->end);
       continue;
     }
     std::vector<Request *> batch;
