@@ -40,6 +40,7 @@ struct apspie_context {
   void *bfs_state = nullptr;  // device pointer into a workspace slot
   void *bfs_state_zeroed = nullptr;  // BFS state buffer zeroed once for the fused init
   int bfs_par = 0;                   // barrier counter set of the next BFS launch
+  void *sort_err_zeroed = nullptr;   // radix sort give-up word, zeroed once when allocated
   void *sssp_state = nullptr;
   // SSSP near-far step (0: frontier Bellman-Ford)
   uint32_t sssp_delta_u32 = 0;
@@ -112,7 +113,7 @@ enum SlotId : int {
   kSlotSortValsA,
   kSlotSortValsB,
   kSlotSortHist,
-  kSlotSortTiles,
+  kSlotSortErr,  // radix sort: sticky give-up word of the look-back waits
   kSlotScan,
   kSlotDense,
   kSlotBitmap,

@@ -183,6 +183,8 @@ int keys_to_graph(apspie_context *ctx, unsigned long long *ka, unsigned long lon
   int rc = device_radix_sort<unsigned long long, int>(ctx, ka, nullptr, kb, nullptr, n,
                                                       2 * bits + 1, &in_b);
   if (rc) return rc;
+  rc = radix_sort_check(ctx);
+  if (rc) return rc;
   unsigned long long *k = in_b ? kb : ka;
   unsigned *flag = (unsigned *)workspace(ctx, kSlotMisc2, sizeof(unsigned) * (size_t)n);
   unsigned *rank = (unsigned *)workspace(ctx, kSlotMisc3, sizeof(unsigned) * (size_t)n);

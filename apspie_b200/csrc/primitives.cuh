@@ -292,6 +292,37 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
   }
 }
 
+// The context's radix-sort give-up word: set by a tile whose look-back
+// waited kSpinLimit polls for a predecessor (the output is then in bounds
+// but not sorted).  Sticky: zeroed when first allocated and by
+// radix_sort_check, not by each sort, so a caller that synchronises only
+// at its end still sees a give-up of any sort it ran.  Stream-ordered
+// callers that never synchronise (apspie_bfs_prepare, apspie_csr_transpose)
+// leave it to the next call on the context that reads it back (the device
+// graph build, apspie_tc_prepare, apspie_spmspv).
+inline int *radix_sort_err(apspie_context *ctx) {
+  auto *e = (int *)workspace(ctx, kSlotSortErr, 16);
+  if (e && ctx->sort_err_zeroed != e) {
+    cudaMemsetAsync(e, 0, 16, ctx->stream);
+    ctx->sort_err_zeroed = e;
+  }
+  return e;
+}
+
+// Reads the give-up word back (synchronises the stream): APSPIE_ERR_TIMEOUT
+// when a sort since the last check gave up, clearing the word.
+inline int radix_sort_check(apspie_context *ctx) {
+  int *e = radix_sort_err(ctx);
+  int *h = (int *)pinned(ctx, sizeof(int));
+  if (!e || !h) return APSPIE_ERR_OOM;
+  cudaMemcpyAsync(h, e, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  const cudaError_t ce = cudaStreamSynchronize(ctx->stream);
+  if (ce != cudaSuccess) return check_cuda(ctx, ce, "radix sort check");
+  if (*h == 0) return APSPIE_OK;
+  cudaMemsetAsync(e, 0, sizeof(int), ctx->stream);
+  return set_error(ctx, APSPIE_ERR_TIMEOUT, "radix sort: a look-back wait gave up");
+}
+
 // Stable sort of n (key, value) pairs on the low `bits` bits of the key
 // (va == vb == nullptr sorts keys only).  Ping-pongs between (ka, va) and
 // (kb, vb); *result_in_b tells where the sorted data ended up.  Scratch:
@@ -305,18 +336,18 @@ int device_radix_sort(apspie_context *ctx, K *ka, V *va, K *kb, V *vb, long long
   if (npass > kMaxPasses || n >= (1ll << 40))
     return set_error(ctx, APSPIE_ERR_OVERFLOW, "radix sort: %lld keys of %d bits", n, bits);
   const long long tiles = (n + kSortTile - 1) / kSortTile;
-  // [histograms: npass x 256 u64][tile counters: 8 x u32, padded][err][status: tiles x 256 u64]
+  // [histograms: npass x 256 u64][tile counters: 8 x u32, padded][status: tiles x 256 u64]
   const size_t hist_bytes = sizeof(unsigned long long) * kMaxPasses * kRadix;
   const size_t head = hist_bytes + 64;
   const size_t bytes = head + sizeof(unsigned long long) * (size_t)tiles * kRadix;
+  int *err = radix_sort_err(ctx);
   auto *ws = (unsigned char *)workspace(ctx, kSlotSortHist, bytes);
-  if (!ws) return APSPIE_ERR_OOM;
+  if (!ws || !err) return APSPIE_ERR_OOM;
   auto *ghist = (unsigned long long *)ws;
   auto *counters = (unsigned *)(ws + hist_bytes);
-  int *err = (int *)(ws + hist_bytes + 48);
   auto *status = (unsigned long long *)(ws + head);
   cudaStream_t st = ctx->stream;
-  // zero the histograms, counters, error word and every status word
+  // zero the histograms, counters and every status word
   cudaMemsetAsync(ws, 0, bytes, st);
   const int hgrid = (int)std::max(1ll, std::min((n + kSortThreads * 8 - 1) / (kSortThreads * 8),
                                                 (long long)ctx->num_sms * 4));

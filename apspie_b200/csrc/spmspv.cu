@@ -516,10 +516,16 @@ int apspie_spmspv(apspie_ctx ctx, int semiring, int m, int64_t nnz, const int *d
                        d_ynnz, &E);
   if (rc) return rc;
   int *h = (int *)pinned(ctx, sizeof(long long));
-  if (!h) return APSPIE_ERR_OOM;
+  int *sort_err = radix_sort_err(ctx);
+  if (!h || !sort_err) return APSPIE_ERR_OOM;
   cudaMemcpyAsync(h, d_ynnz, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(h + 1, sort_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
   rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "apspie_spmspv");
   if (rc) return rc;
+  if (h[1]) {  // the sort path's look-back gave up: the output is not sorted
+    cudaMemsetAsync(sort_err, 0, sizeof(int), ctx->stream);
+    return set_error(ctx, APSPIE_ERR_TIMEOUT, "apspie_spmspv: radix sort look-back gave up");
+  }
   *h_ynnz = *h;
   if (h_expanded) *h_expanded = E;
   return APSPIE_OK;

@@ -431,6 +431,8 @@ int apspie_tc_prepare(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr, cons
       if (rc) return rc;
     }
   }
+  rc = radix_sort_check(ctx);  // both sorts; synchronises
+  if (rc) return rc;
   *h_lnnz = lnnz;
   return APSPIE_OK;
 }
