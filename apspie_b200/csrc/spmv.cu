@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <type_traits>
 
 #include "common.cuh"
 #include "context.h"
@@ -96,8 +97,9 @@ __global__ void spmv_merge_plan(int m, int nnz, int ntiles, const int *__restric
 // [j0, j1); it touches rows i0 .. min(i1, m - 1).  Row i1 (when < m) is
 // open at the tile's end: its partial goes to carry_val[b].  Row i0, when
 // it has nonzeros before j0 and ends in this tile, goes to head_val[b].
+template <int SR>
 __global__ void __launch_bounds__(kMpThreads)
-spmv_merge_tiles(int sr, int m, const int *__restrict__ ptr, const int *__restrict__ ind,
+spmv_merge_tiles(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
                  const float *__restrict__ val, const float *__restrict__ x, float *y,
                  const int2 *__restrict__ coord, int *carry_row, double *carry_val,
                  int *head_row, double *head_val) {
@@ -105,6 +107,7 @@ spmv_merge_tiles(int sr, int m, const int *__restrict__ ptr, const int *__restri
   __shared__ int s_ptr[kMpTile + 2];
   __shared__ int s_long[kMpTile / (kMpWarpSeg + 1) + 1];
   __shared__ unsigned s_nlong;
+  constexpr int sr = SR;  // the semiring, fixed per instantiation
   const int b = blockIdx.x, t = threadIdx.x;
   const int2 c0 = coord[b], c1 = coord[b + 1];
   const int i0 = c0.x, j0 = c0.y, i1 = c1.x, j1 = c1.y;
@@ -148,9 +151,17 @@ spmv_merge_tiles(int sr, int m, const int *__restrict__ ptr, const int *__restri
       s_long[atomicAdd(&s_nlong, 1u)] = q;
       continue;
     }
-    double acc = sr_identity(sr);
-    for (int k = s; k < e; ++k) acc = sr_add(sr, acc, s_term[k]);
-    emit(q, acc);
+    // four partial sums, combined in a fixed order
+    double a0 = sr_identity(sr), a1 = a0, a2 = a0, a3 = a0;
+    int k = s;
+    for (; k + 3 < e; k += 4) {
+      a0 = sr_add(sr, a0, s_term[k]);
+      a1 = sr_add(sr, a1, s_term[k + 1]);
+      a2 = sr_add(sr, a2, s_term[k + 2]);
+      a3 = sr_add(sr, a3, s_term[k + 3]);
+    }
+    for (; k < e; ++k) a0 = sr_add(sr, a0, s_term[k]);
+    emit(q, sr_add(sr, sr_add(sr, a0, a1), sr_add(sr, a2, a3)));
   }
   __syncthreads();
   const int lane = lane_id(), w = warp_in_block();
@@ -168,10 +179,12 @@ spmv_merge_tiles(int sr, int m, const int *__restrict__ ptr, const int *__restri
 // Rows that span tiles: the tile where row r ends (head_row[b] == r) adds,
 // in tile order, the carries of the tiles before it that were open on r,
 // then its own head partial.
-__global__ void spmv_merge_fixup(int sr, int ntiles, const int *__restrict__ carry_row,
+template <int SR>
+__global__ void spmv_merge_fixup(int ntiles, const int *__restrict__ carry_row,
                                  const double *__restrict__ carry_val,
                                  const int *__restrict__ head_row,
                                  const double *__restrict__ head_val, float *y) {
+  constexpr int sr = SR;
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < ntiles; b += gridDim.x * blockDim.x) {
     const int r = head_row[b];
     if (r < 0) continue;
@@ -203,10 +216,19 @@ extern "C" int apspie_spmv(apspie_ctx ctx, int semiring, int m, int64_t nnz, con
   cudaStream_t st = ctx->stream;
   const int pgrid = (int)std::min<long long>((32ll * (ntiles + 1) + 255) / 256, ctx->num_sms * 16ll);
   spmv_merge_plan<<<pgrid, 256, 0, st>>>(m, (int)nnz, ntiles, d_ptr, coord);
-  spmv_merge_tiles<<<ntiles, kMpThreads, 0, st>>>(semiring, m, d_ptr, d_ind, d_val, d_x, d_y,
-                                                  coord, rows, vals, rows + ntiles,
-                                                  vals + ntiles);
-  spmv_merge_fixup<<<(ntiles + 255) / 256, 256, 0, st>>>(semiring, ntiles, rows, vals,
-                                                         rows + ntiles, vals + ntiles, d_y);
+  const unsigned fgrid = (unsigned)((ntiles + 255) / 256);
+  auto launch = [&](auto sr_tag) {
+    constexpr int SR = decltype(sr_tag)::value;
+    spmv_merge_tiles<SR><<<ntiles, kMpThreads, 0, st>>>(m, d_ptr, d_ind, d_val, d_x, d_y, coord,
+                                                        rows, vals, rows + ntiles, vals + ntiles);
+    spmv_merge_fixup<SR><<<fgrid, 256, 0, st>>>(ntiles, rows, vals, rows + ntiles, vals + ntiles,
+                                                d_y);
+  };
+  switch (semiring) {
+    case kSr_MinPlus: launch(std::integral_constant<int, kSr_MinPlus>{}); break;
+    case kSr_MaxTimes: launch(std::integral_constant<int, kSr_MaxTimes>{}); break;
+    case kSr_OrAnd: launch(std::integral_constant<int, kSr_OrAnd>{}); break;
+    default: launch(std::integral_constant<int, kSr_PlusTimes>{}); break;
+  }
   return check_launch(ctx, "apspie_spmv", 3);
 }
