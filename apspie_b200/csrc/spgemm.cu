@@ -7,22 +7,27 @@
 // host, inserts every product into a global-memory open-addressing table of
 // TABLE_SIZE slots per tile (atomicCAS key (row<<16|col), atomicAdd float,
 // entries DROPPED after 25 probes), then radix-sorts the whole tables and
-// converts COO to CSR.  Here:
+// converts COO to CSR.  Here, in two phases (apspie_spgemm_symbolic /
+// apspie_spgemm_numeric, the plan kept in the context between them):
 //   0. prod[i] = sum over A(i,k) of nnz(B(k,:)) (an upper bound of nnz(C(i,:)));
-//   1. rows are binned: prod <= 256 -> one warp per row, table of
-//      next_pow2(2*prod) slots in shared memory; prod <= 8192 -> one block per
-//      row, table up to 16384 slots; larger -> one block per row with a dense
-//      accumulator (bitmap + values) in global memory;
-//   2. symbolic pass counts distinct columns per row (keys only), a scan gives
-//      C's row offsets, C is allocated exactly;
-//   3. numeric pass accumulates the products in double (so the float result is
-//      the correctly rounded exact sum up to double error) and writes the row
-//      into C in column order: warp rows bitonic-sort their small table; block
-//      rows scatter the occupied entries into C by column bucket (512 buckets
-//      over the column range: counts, a scan, atomic slots) and each thread
-//      insertion-sorts one bucket in place -- linear work instead of sorting
-//      the whole table (a row whose fullest bucket holds more than 128
-//      entries falls back to the bitonic sort).
+//   1. symbolic rows are binned by prod: <= 256 one warp per row (shared hash
+//      table); <= 1024 / <= 4096 one block per row on a 2048 / 8192-key
+//      shared table (spgemm_mid_rows); longer rows over a shared-memory
+//      bitmap of C's columns when B has at most bitmap_max_cols columns
+//      (spgemm_bitmap_rows<0>), else a 16384-key table (<= 8192 products) or
+//      a dense accumulator in global memory; the distinct columns per row
+//      give nnz(C(i,:)), a scan gives C's row offsets;
+//   2. the block-row bins are re-binned by that exact output size
+//      (rebin_rows): <= 512 / 1024 / 2048 outputs on mid tables of 1024 /
+//      2048 / 4096 slots whose entries are put in column order by an
+//      in-shared bucket sort; longer rows (bitmap case) on the column bitmap,
+//      where a product's position in the column-ordered row is the prefix
+//      popcount of the bitmap up to its column (no sort), values staged in
+//      shared memory (rows of up to 4096 outputs at 512 threads, windows of
+//      16384 positions at 1024 threads for longer ones);
+//   3. the numeric pass accumulates in double (so the float result is the
+//      correctly rounded exact sum up to double error); warp rows compact
+//      their table and emit by rank in column order.
 // Tables are at most half full, probing is linear and every insert succeeds
 // (nothing is dropped).  Explicit zeros (cancellation) stay in the structure,
 // as the reference's insert keeps every touched key.

@@ -56,6 +56,10 @@ if _r is not None:
     _r.ref_sssp_cpu.argtypes = [ci, ci, vp, vp, vp, vp, ci]
     _r.ref_sssp_cpu.restype = ci
     _r.ref_mt_fill.argtypes = [C.c_ulong, C.c_longlong, vp]
+    _r.ref_tc_ewise.argtypes = [ci, i64, vp, vp, vp, vp, vp, vp, vp]
+    _r.ref_tc_ewise.restype = None
+    _r.ref_mis.argtypes = [ci, vp, vp, vp, C.c_float, vp]
+    _r.ref_mis.restype = ci
 
 PLUS_TIMES, MIN_PLUS, MAX_TIMES, OR_AND = 0, 1, 2, 3
 
@@ -200,3 +204,53 @@ def ref_mt_fill(seed, n):
     out = np.empty(n, dtype=np.uint32)
     _r.ref_mt_fill(seed, n, _d(out))
     return out
+
+
+def ref_tc(m, ptr, ind) -> int:
+    """Triangles of a symmetric graph by the reference's own
+    intersection kernel ewiseMultTc (src/tc.cuh:168-199, built host-side in
+    oracle/_ref), fed as test/tc/main.cu:172-175,241-244 feed it: C = the
+    strictly upper part and B = the strictly lower part in CSC (self-loops
+    fall in neither, as in buildLower, test/tc/main.cu:40-55), D = the
+    product that cuSPARSE csrgemm forms from C's and B's arrays (computed
+    here by the oracle's Gustavson SpGEMM), then the per-thread counts summed
+    (mgpu::Reduce, test/tc/main.cu:247) in int64."""
+    ptr, ind = _a(ptr, np.int64), _a(ind, np.int64)
+    rows = np.repeat(np.arange(m, dtype=np.int64), np.diff(ptr))
+
+    def part(keep):
+        r, c = rows[keep], ind[keep]
+        order = np.lexsort((c, r))
+        p = np.zeros(m + 1, np.int64)
+        np.add.at(p, r + 1, 1)
+        return np.cumsum(p).astype(np.int32), c[order].astype(np.int32)
+
+    cp, ci_ = part(ind < rows)   # column i of C (CSC): rows j < i
+    bp, bi = part(ind > rows)    # column i of B (CSC): rows j > i
+    dp, di, dv = spgemm(m, m, cp, ci_, None, bp, bi, None)
+    dp32 = dp.astype(np.int32)
+    # one readable entry past the end of each row index array (the kernel
+    # reads it when a column is exhausted, src/tc.cuh:190,194)
+    di_pad = np.append(di.astype(np.int32), np.int32(0))
+    ci_pad = np.append(ci_, np.int32(0))
+    dv = _a(dv, np.float64)
+    cv = np.ones(max(1, ci_.size), np.float64)
+    nthreads = ((m + 511) // 512) * 512
+    out = np.zeros(max(1, nthreads), np.float64)
+    _r.ref_tc_ewise(m, int(di.size), _d(dv), _d(dp32), _d(di_pad), _d(cv), _d(cp), _d(ci_pad),
+                    _d(out))
+    return int(np.sum(out[:m].astype(np.int64)))
+
+
+def ref_mis(m, ptr, ind, prio_u32, delta: float):
+    """MIS by the reference's own round kernels (src/spmspvMis.cuh:10-78,
+    built host-side in oracle/_ref) driven by its round loop
+    (src/spmspvMis.cuh:232-318), with the uint32 priorities mapped to
+    prio / 2^32 in double (same order, every value below 1 as the
+    reference's fillUniform draws are).  Returns (membership 1 / 0 / -1,
+    rounds)."""
+    ptr, ind = _a(ptr, np.int32), _a(ind, np.int32)
+    pr = _a(prio_u32, np.uint32).astype(np.float64) / 4294967296.0
+    out = np.empty(m, dtype=np.int32)
+    rounds = _r.ref_mis(m, _d(ptr), _d(ind), _d(pr), float(delta), _d(out))
+    return out, int(rounds)

@@ -1,8 +1,8 @@
 """Generate tests/golden/golden.npz from the reference's own CPU code.
 
-Runs in a checkout that has the reference tree (REF_ROOT, default
-/root/reference) and the compiled reference routines (oracle/_ref, built by
-`make -C oracle`).  The output is committed; tests read only the .npz.
+Runs in a checkout that has the reference tree (the environment variable
+REF_ROOT, required, names its root) and the compiled reference routines
+(oracle/_ref, built by `make -C oracle REF_SRC=$REF_ROOT/src`).  The output is committed; tests read only the .npz.
 
 Contents
   mtx/<name>/{dir,und}_{ptr,ind}   CSR of each dataset/small/*.mtx file, parsed
@@ -17,6 +17,17 @@ Contents
   rmat10/*                         BFS / SSSP of the reference on R-MAT scale 10
                                    graphs from the package's generator, plus a
                                    SHA-256 of each CSR (pins the generator)
+  tc/<name>                        triangle count of each undirected fixture and
+                                   of R-MAT 10 / 12 (symmetrised, seed 3) by the
+                                   reference's ewiseMultTc built host-side
+                                   (oracle.ref_tc)
+  mis/<name>/ptr, ind              self-loop-free symmetric graphs (the
+                                   undirected fixtures, R-MAT 10, ER 2^10 mean
+                                   degree 8, a 24x24 grid)
+  mis/<name>/d<delta>, rounds_*    MIS membership (1 / 0) and rounds from the
+                                   reference's round kernels and loop
+                                   (oracle.ref_mis) with mt19937(5489)
+                                   priorities, delta 0.1 and 1
 """
 from __future__ import annotations
 
@@ -31,7 +42,9 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 import oracle  # noqa: E402
 
-REF_ROOT = Path(os.environ.get("REF_ROOT", "/root/reference"))
+if "REF_ROOT" not in os.environ:
+    raise SystemExit("make_golden.py: set REF_ROOT to the root of the apspie source tree")
+REF_ROOT = Path(os.environ["REF_ROOT"])
 FIXTURES = ["test_cc", "test_bc", "test_pr", "test_spgemm", "test_mis", "test_mesh", "chesapeake"]
 
 
@@ -115,6 +128,37 @@ def main() -> None:
         [oracle.ref_sssp(gd.m, gd.ptr, gd.ind, wu.astype(np.float32), int(s)) for s in srcs])
     out["rmat10/dir_sssp_f32"] = np.stack(
         [oracle.ref_sssp(gd.m, gd.ptr, gd.ind, wf, int(s)) for s in srcs])
+    # triangle counts by the reference's intersection kernel
+    for name in FIXTURES:
+        ptr, ind = out[f"mtx/{name}/und_ptr"], out[f"mtx/{name}/und_ind"]
+        out[f"tc/{name}"] = np.array([oracle.ref_tc(len(ptr) - 1, ptr, ind)], np.int64)
+    for sc in (10, 12):
+        gt = ap.gen_rmat(sc, 16, seed=3, symmetric=True)
+        out[f"tc/rmat{sc}"] = np.array([oracle.ref_tc(gt.m, gt.ptr, gt.ind)], np.int64)
+    # MIS by the reference's round kernels, on graphs without self-loops
+    # (a self-looped vertex never joins the reference's set)
+    mis_graphs = {}
+    for name in FIXTURES:
+        ptr, ind = out[f"mtx/{name}/und_ptr"], out[f"mtx/{name}/und_ind"]
+        m = len(ptr) - 1
+        rows = np.repeat(np.arange(m), np.diff(ptr))
+        mis_graphs[name] = csr(m, rows[rows != ind], ind[rows != ind].astype(np.int64))
+    gm = ap.gen_rmat(10, 16, seed=3, symmetric=True)
+    mis_graphs["rmat10"] = (gm.ptr, gm.ind)
+    ge = ap.gen_er(1 << 10, 8, seed=3)
+    mis_graphs["er10"] = (ge.ptr, ge.ind)
+    gg = ap.gen_grid(24, 24)
+    mis_graphs["grid24"] = (gg.ptr, gg.ind)
+    for name, (ptr, ind) in mis_graphs.items():
+        m = len(ptr) - 1
+        prio = oracle.ref_mt_fill(5489, m)
+        out[f"mis/{name}/ptr"] = np.asarray(ptr, np.int32)
+        out[f"mis/{name}/ind"] = np.asarray(ind, np.int32)
+        for delta in (0.1, 1.0):
+            mis, rounds = oracle.ref_mis(m, ptr, ind, prio, delta)
+            assert np.all(mis >= 0), f"{name}: undecided vertices"
+            out[f"mis/{name}/d{delta}"] = mis.astype(np.int8)
+            out[f"mis/{name}/rounds_d{delta}"] = np.array([rounds], np.int32)
     np.savez_compressed(Path(__file__).with_name("golden.npz"), **out)
     print(f"wrote {len(out)} arrays")
 

@@ -43,6 +43,22 @@ def test_mis_fixtures(ctx, golden, fixture_names):
             assert oracle.mis_check(h.m, ptr, ind, got) == 0 or name == "test_spgemm"
 
 
+def test_mis_matches_reference_kernel_goldens(ctx, golden):
+    """apspie_mis against the membership that the reference's own round
+    kernels and loop (src/spmspvMis.cuh:10-78, 232-318) produced with the
+    same mt19937(5489) priorities, stored in the goldens, at both of their
+    step sizes."""
+    import apspie_b200 as ap
+    names = sorted({k.split("/")[1] for k in golden if k.startswith("mis/")})
+    for name in names:
+        ptr, ind = golden[f"mis/{name}/ptr"], golden[f"mis/{name}/ind"]
+        h = ap.HostGraph(len(ptr) - 1, ptr, ind, symmetric=True)
+        for delta in (0.1, 1.0):
+            got, _, _ = _run(ctx, h, ap.mt19937(5489, h.m), delta)
+            np.testing.assert_array_equal(got, golden[f"mis/{name}/d{delta}"].astype(np.int32),
+                                          err_msg=f"{name} delta {delta}")
+
+
 @pytest.mark.parametrize("delta", [1.0, 0.5, 0.1])
 def test_mis_er_and_grid_any_delta(ctx, delta):
     import apspie_b200 as ap

@@ -111,3 +111,58 @@ def test_oracle_spgemm_structure_keeps_cancellation():
     # A = [[1, -1]], B = [[1],[1]] -> C = [[0]] must stay as an explicit entry
     cp, ci, cv = oracle.spgemm(1, 1, [0, 2], [0, 1], [1.0, -1.0], [0, 1, 2], [0, 0], [1.0, 1.0])
     assert list(cp) == [0, 1] and list(ci) == [0] and cv[0] == 0.0
+
+
+def test_oracle_tc_matches_reference_kernel_goldens(golden, fixture_names):
+    """Triangle counts of the reference's own intersection kernel
+    (ewiseMultTc, src/tc.cuh:168-199, run host-side on the U*L product as
+    test/tc/main.cu:241-247 runs it) pin the oracle's L-masked count."""
+    import apspie_b200 as ap
+    graphs = {n: (golden[f"mtx/{n}/und_ptr"], golden[f"mtx/{n}/und_ind"]) for n in fixture_names}
+    for sc in (10, 12):
+        g = ap.gen_rmat(sc, 16, seed=3, symmetric=True)
+        graphs[f"rmat{sc}"] = (g.ptr, g.ind)
+    for name, (ptr, ind) in graphs.items():
+        m = len(ptr) - 1
+        _, lp, li = oracle.tc_build_lower(m, ptr, ind)
+        assert oracle.tc_lower(m, lp, li) == int(golden[f"tc/{name}"][0]), name
+
+
+def test_oracle_mis_matches_reference_kernel_goldens(golden):
+    """MIS of the reference's own round kernels and loop (src/spmspvMis.cuh:
+    10-78, 232-318) at two step sizes pins the oracle's greedy MIS: with
+    distinct priorities both are the greedy set in descending priority."""
+    names = sorted({k.split("/")[1] for k in golden if k.startswith("mis/")})
+    assert len(names) >= 9
+    for name in names:
+        ptr, ind = golden[f"mis/{name}/ptr"], golden[f"mis/{name}/ind"]
+        m = len(ptr) - 1
+        got = oracle.mis(m, ptr, ind, oracle.mt_fill(5489, m))
+        for delta in (0.1, 1.0):
+            np.testing.assert_array_equal(got, golden[f"mis/{name}/d{delta}"].astype(np.int32),
+                                          err_msg=f"{name} delta {delta}")
+
+
+@pytest.mark.skipif(not oracle.have_reference(), reason="oracle/_ref not built")
+def test_oracle_tc_live_against_reference_kernel():
+    import apspie_b200 as ap
+    for g in (ap.gen_rmat(12, 16, seed=1), ap.gen_rmat(11, 16, seed=2), ap.gen_er(3000, 12, seed=4),
+              ap.gen_grid(20, 30)):
+        _, lp, li = oracle.tc_build_lower(g.m, g.ptr, g.ind)
+        assert oracle.ref_tc(g.m, g.ptr, g.ind) == oracle.tc_lower(g.m, lp, li)
+
+
+@pytest.mark.skipif(not oracle.have_reference(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("delta", [0.05, 0.1, 1.0])
+def test_oracle_mis_live_against_reference_kernels(delta):
+    import apspie_b200 as ap
+    for seed, g in ((5489, ap.gen_rmat(12, 16, seed=2)), (42, ap.gen_er(1 << 12, 8, seed=4)),
+                    (7, ap.gen_grid(48, 48))):
+        prio = oracle.mt_fill(seed, g.m)
+        ref, rounds = oracle.ref_mis(g.m, g.ptr, g.ind, prio, delta)
+        assert rounds > 0 and np.all(ref >= 0)
+        np.testing.assert_array_equal(oracle.mis(g.m, g.ptr, g.ind, prio), ref)
+    # a planted mistake in the oracle's answer is seen by the comparison
+    bad = oracle.mis(g.m, g.ptr, g.ind, prio)
+    bad[int(np.flatnonzero(bad == 1)[0])] = 0
+    assert not np.array_equal(bad, ref)

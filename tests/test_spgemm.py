@@ -147,6 +147,25 @@ def test_tc_fixtures(ctx, golden, fixture_names):
         _tc(ctx, h)
 
 
+def test_tc_matches_reference_kernel_goldens(ctx, golden, fixture_names):
+    """apspie_tc against the counts of the reference's own intersection
+    kernel (ewiseMultTc, src/tc.cuh:168-199, run host-side on U*L) stored in
+    the goldens: every undirected fixture and R-MAT 10 / 12."""
+    import apspie_b200 as ap
+    graphs = {}
+    for name in fixture_names:
+        ptr, ind = golden[f"mtx/{name}/und_ptr"], golden[f"mtx/{name}/und_ind"]
+        src = np.repeat(np.arange(len(ptr) - 1), np.diff(ptr))
+        keep = src != ind
+        graphs[name] = ap.from_edges(len(ptr) - 1, src[keep], ind[keep])
+    for sc in (10, 12):
+        graphs[f"rmat{sc}"] = ap.gen_rmat(sc, 16, seed=3, symmetric=True)
+    for name, h in graphs.items():
+        g = h.to_device(with_transpose=False)
+        _, lp, li = ap.tc_prepare(ctx, g)
+        assert ap.triangle_count(ctx, h.m, lp, li) == int(golden[f"tc/{name}"][0]), name
+
+
 def test_tc_prepare_rejects_a_directed_graph(ctx):
     """L is read from both ends of every edge, so the input must be
     symmetric: a directed R-MAT graph is refused, not miscounted."""
