@@ -54,16 +54,16 @@ struct BfsState {
   // reading those to choose the direction while faster ones already append.
   // Two sets, by level parity; block 0 clears the other one each level.
   LevelCounters comp[2];
-  alignas(8) unsigned bar[2];  // grid-barrier arrival counter (64-bit), separate init
-  int err;
+  alignas(128) unsigned bar[2];  // grid-barrier arrival counter (64-bit), separate init
+  alignas(128) int err;
   int levels;
   int pull_levels;
   int par;  // counter set of the last launch with the initialisation fused in
   // Launches that clear the state themselves alternate between two barrier
   // counters and error words: a launch resets the set the next one will use
   // (the previous launch on the stream has finished, so nobody polls it).
-  alignas(8) unsigned barp[2][2];
-  int errp[2];
+  alignas(128) unsigned barp[2][2];
+  alignas(128) int errp[2];
   unsigned long long reached;
   unsigned long long edges;
   unsigned long long t_start;
@@ -75,6 +75,7 @@ struct BfsVisit {
   static constexpr bool kTwoWay = false;
   int next;
   int32_t *depth;
+  __device__ __forceinline__ bool two_way() const { return false; }
   __device__ __forceinline__ bool check(unsigned, int, int u, unsigned &) const {
     return __ldcg(depth + u) == -1;
   }
@@ -255,9 +256,9 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
         nch = s_chunks;
       }
       BfsVisit vis{next, depth};
-      expand_push(ptr, ind, qin, nq, cin, s_nbig, nch, qout, cout, nxt, cur, gwarp, nwarps,
-                  [](int) { return 0u; }, vis,
-                  L < kTraceLevels ? &st->trace[L].expanded : nullptr);
+      expand_push_direct(ptr, ind, qin, nq, cin, s_nbig, nch, qout, cout, nxt, cur, gwarp,
+                         nwarps, [](int, bool, bool &) { return 0u; }, vis,
+                         L < kTraceLevels ? &st->trace[L].expanded : nullptr);
     } else {
       ++pull_levels;
       // ---- pull: unvisited vertices look for a parent at depth L ----

@@ -67,12 +67,12 @@ struct SsspState {
   LevelCounters c[3];
   unsigned far_count[3];  // far lists rotate by phase
   unsigned far_min[3];    // least distance sent to each far list
-  alignas(8) unsigned bar[2];  // grid-barrier arrival counter (64-bit)
-  int err;
+  alignas(128) unsigned bar[2];  // grid-barrier arrival counter (64-bit), its own line
+  alignas(128) int err;
   int rounds;
   int phases;
   unsigned nhc;  // chunks of the high in-degree vertices (pull rounds)
-  unsigned long long relaxations;  // edges scanned over all rounds
+  unsigned long long relaxations;  // edges walked over all rounds (pull rounds: nnz each)
   unsigned long long reached;
   unsigned long long edges;        // sum of out-degrees of reached vertices
   unsigned long long t_start;
@@ -123,6 +123,8 @@ struct SsspVisit {
   int *far_list;
   unsigned *far_count;
   unsigned *far_min;
+  // far lists only exist under a finite threshold (near-far schedule)
+  __device__ __forceinline__ bool two_way() const { return thresh != Arith<W>::kInf; }
   __device__ __forceinline__ bool check(unsigned du, int k, int u, unsigned &nd) const {
     nd = Arith<W>::add(du, __ldg(w + k));
     return nd < __ldcg(dist + u);
@@ -223,7 +225,6 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
   __shared__ unsigned s_q, s_chunks, s_nbig, s_far;
   __shared__ unsigned long long s_edges;
   __shared__ unsigned s_best[kSsspThreads / 32][32];
-  unsigned long long relax = 0;
   // T = infinity without near-far; else the first phase covers [0, delta)
   if (blockIdx.x == 0 && threadIdx.x == 0) st->t_start = globaltimer();
   unsigned thresh = delta ? delta : Arith<W>::kInf;
@@ -294,7 +295,8 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
       // ---- pull round: every vertex takes the least d[u] + w over its
       // in-neighbours in the frontier; hub chunks and 32-vertex groups are
       // handed out by the round's counter ----
-      relax += (unsigned long long)nnz;
+      if (blockIdx.x == 0 && threadIdx.x == 0)
+        atomicAdd(&st->relaxations, (unsigned long long)nnz);
       LevelCounters *nx = nxt;
       DiscoverAcc acc;
       const int warp = warp_in_block();
@@ -382,19 +384,26 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
         st->trace[r].t_end = globaltimer();
       continue;
     }
-    relax += s_edges;
     int *qin = (r & 1) ? qb : qa;
     int2 *cin = (r & 1) ? cb : ca;
     int *fout = phase % 3 == 0 ? far0 : (phase % 3 == 1 ? far1 : far2);
     SsspVisit<W> vis{w,    dist,   stamp, fstamp, r, phase, thresh, fout, &st->far_count[phase % 3],
                      &st->far_min[phase % 3]};
+    // A queued vertex whose distance still equals the one it was last
+    // expanded with (it improved again in the round that expanded it, so it
+    // was queued once more) has nothing new to relax: skipped.  Hub chunks
+    // are expanded by several warps and are not skipped.
     expand_push(ptr, ind, qin, nq, cin, s_nbig, nch, qout, cout, nxt, cur, gwarp, nwarps,
-                [&](int v) {
+                [&](int v, bool whole, bool &skip) {
                   const unsigned d = __ldcg(dist + v);
+                  if (whole && __ldcg(xd + v) == d) {
+                    skip = true;
+                    return d;
+                  }
                   xd[v] = d;  // the distance v is expanded with
                   return d;
                 },
-                vis);
+                vis, &st->relaxations);
     if (r < kSsspTraceRounds) {
       __syncthreads();
       if (threadIdx.x == 0) atomicMax(&st->trace[r].t_last, globaltimer());
@@ -424,7 +433,6 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->rounds = r;
     st->phases = phase;
-    st->relaxations = relax;
   }
 }
 
