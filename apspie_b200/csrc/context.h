@@ -45,7 +45,7 @@ struct apspie_context {
   // SSSP near-far step (0: frontier Bellman-Ford)
   uint32_t sssp_delta_u32 = 0;
   float sssp_delta_f32 = 0.0f;
-  int sssp_pull_alpha = 2;  // pull round when frontier out-edges * alpha > nnz (0: never)
+  int sssp_pull_alpha = 0;  // pull round when frontier out-edges * alpha > nnz (0: never)
   int sssp_pull_alpha_batch = 0;  // the same for the multi-source SSSP steps (off: measured slower)
   void *mis_state = nullptr;
   void *batch_state = nullptr;
@@ -105,6 +105,7 @@ enum SlotId : int {
   kSlotSsspStamp,
   kSlotSsspNearFar,
   kSlotSsspHubs,
+  kSlotSsspHubWord,
   kSlotMisState,
   kSlotMisQueueA,
   kSlotMisQueueB,

@@ -300,7 +300,8 @@ __device__ __forceinline__ void seed_frontier(int src, const int *__restrict__ p
 }
 
 // Chunks of the big vertices, in runs of consecutive chunks: the warp finds
-// the vertex of a run's first chunk and walks on.  With at most two chunks
+// the vertex of a run's first chunk and walks on; when load() skips the
+// vertex, the rest of its chunks in the run are passed over.  With at most two chunks
 // per warp every warp takes its own run (no counter traffic); larger levels
 // hand runs of about a quarter of a warp's share (at least two chunks) out
 // on demand from the level's counter, because equal chunk counts are not
@@ -339,10 +340,15 @@ __device__ __forceinline__ void expand_chunks(const int *__restrict__ ptr,
         bnext = bi + 1 < (int)nbig ? (unsigned)__ldcg(&bin[bi + 1].y) : 0xffffffffu;
       }
       const int v = bcur.x;
-      const int s = __ldg(ptr + v) + (int)(c - (unsigned)bcur.y) * kChunk;
-      const int e = min(s + kChunk, __ldg(ptr + v + 1));
       bool skip = false;
       const unsigned pay = load(v, false, skip);
+      if (skip) {
+        // the loader skips the vertex: none of its chunks in this run
+        c = min(bnext, c_end) - 1u;
+        continue;
+      }
+      const int s = __ldg(ptr + v) + (int)(c - (unsigned)bcur.y) * kChunk;
+      const int e = min(s + kChunk, __ldg(ptr + v + 1));
       nwalk += (unsigned long long)(e - s);
       for (int k0 = s; k0 < e; k0 += 32 * kUnroll) {
         int uu[kUnroll];
@@ -386,8 +392,9 @@ __device__ __forceinline__ void expand_chunks(const int *__restrict__ ptr,
 // calls it (it synchronises the block).  `load(v, whole, skip)` gives the
 // 32-bit payload of a source vertex (e.g. its distance), broadcast to its
 // edges; whole is true when the call covers all of v's edges (a queued
-// vertex), and the loader may then set skip to leave v unexpanded (e.g. when
-// v was already expanded with the same distance).  visit.commit returns a
+// vertex) and false for one chunk of a big vertex; the loader may set skip
+// to leave v (or this chunk and the rest of the vertex's chunks in the run)
+// unexpanded, e.g. when v was already expanded with the same distance.  visit.commit returns a
 // class: 0 = nothing, 1 = joins the next frontier, 2 (visitors with kTwoWay,
 // when visit.two_way()) = goes to the visitor's secondary list
 // (visit.far_list / visit.far_count, appended without chunking), 3 = a

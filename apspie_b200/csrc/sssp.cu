@@ -54,6 +54,12 @@ constexpr int kHubIn = 1024;      // in-degree above which a pull round splits a
 constexpr int kPullChunk = 1024;  // in-edges per chunk of such a vertex
 
 constexpr int kSsspTraceRounds = 64;  // rounds recorded in the per-run trace
+// out-degree from which a hub's chunks may skip a re-expansion with an
+// unchanged distance (CAS-decided per round; measured on R-MAT 20 / 22 / 23:
+// 4 % faster on the symmetric graphs at 256 - 1024, 1 - 2 % slower on the
+// directed one when every hub takes part)
+constexpr int kHubSkipMinDeg = 512;
+
 
 struct RoundTrace {
   unsigned frontier;          // queued vertices + big-list vertices
@@ -167,12 +173,15 @@ struct SsspVisit {
 
 template <typename W>
 __global__ void sssp_init(int m, int src, unsigned *dist, int *stamp, int *fstamp, unsigned *xd,
-                          const int *__restrict__ ptr, int *queue, int2 *chunks, SsspState *st) {
+                          unsigned long long *xw, const int *__restrict__ ptr, int *queue,
+                          int2 *chunks, SsspState *st) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < m; v += gridDim.x * blockDim.x) {
     dist[v] = (v == src) ? 0u : Arith<W>::kInf;
     stamp[v] = -1;
     fstamp[v] = -1;
     xd[v] = Arith<W>::kInf;
+    // no round yet (tag all ones), no distance recorded
+    xw[v] = (0x7fffffffull << 33) | Arith<W>::kInf;
   }
   if (blockIdx.x == 0) {
     seed_frontier(src, ptr, queue, chunks, &st->c[0]);
@@ -218,7 +227,7 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
                 int2 *cb, SsspState *st, int max_rounds, int *fstamp, unsigned *xd, int *far0,
                 int *far1, int *far2, unsigned delta, long long nnz, const int *__restrict__ tptr,
                 const int *__restrict__ tind, const W *__restrict__ tw, const int2 *hubc,
-                int alpha) {
+                int alpha, unsigned long long *xw) {
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
   const int lane = lane_id();
@@ -391,12 +400,42 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
                      &st->far_min[phase % 3]};
     // A queued vertex whose distance still equals the one it was last
     // expanded with (it improved again in the round that expanded it, so it
-    // was queued once more) has nothing new to relax: skipped.  Hub chunks
-    // are expanded by several warps and are not skipped.
+    // was queued once more) has nothing new to relax: skipped.  A hub's
+    // chunks are expanded by several warps with the distance each reads; the
+    // first chunk of the hub to run in a round decides for all of them, by
+    // one CAS on the hub's word xw = (round, skip, distance): skip when the
+    // recorded distance equals the current one, else record the current one.
+    // Every chunk of the round relaxes with at most the recorded distance
+    // (its own read, or the recorded value when its read is older), so a
+    // later round that finds the distance unchanged knows every chunk
+    // relaxed with it.
     expand_push(ptr, ind, qin, nq, cin, s_nbig, nch, qout, cout, nxt, cur, gwarp, nwarps,
                 [&](int v, bool whole, bool &skip) {
                   const unsigned d = __ldcg(dist + v);
-                  if (whole && __ldcg(xd + v) == d) {
+                  if (!whole && __ldg(ptr + v + 1) - __ldg(ptr + v) < kHubSkipMinDeg) {
+                    // a hub of a few chunks: the decision's CAS would cost
+                    // more than the skip saves; expanded, and its recorded
+                    // distance voided
+                    xd[v] = Arith<W>::kInf;
+                    return d;
+                  }
+                  if (!whole) {
+                    unsigned long long xv = __ldcg(xw + v);
+                    if ((unsigned)(xv >> 33) != (unsigned)r) {
+                      const unsigned rec = (unsigned)xv;
+                      const bool sk = rec == d;
+                      const unsigned long long nv = ((unsigned long long)(unsigned)r << 33) |
+                                                    ((unsigned long long)sk << 32) | d;
+                      const unsigned long long pv = atomicCAS(xw + v, xv, nv);
+                      xv = pv == xv ? nv : pv;  // lost the race: follow the winner
+                    }
+                    skip = (xv >> 32) & 1ull;
+                    // this read may predate the recorded one: relax with at
+                    // most the recorded distance, so that it stays the
+                    // largest distance any chunk of the round used
+                    return min(d, (unsigned)xv);
+                  }
+                  if (__ldcg(xd + v) == d) {
                     skip = true;
                     return d;
                   }
@@ -475,7 +514,10 @@ int sssp_run(apspie_context *ctx, int src, int64_t nnz, int m, const int *d_ptr,
   // far stamps, expanded distances and three far lists of m entries
   const size_t mm = ((size_t)m + 63) & ~size_t(63);
   auto *nf = (int *)workspace(ctx, kSlotSsspNearFar, sizeof(int) * mm * 5);
-  if (!st || !qa || !qb || !ca || !cb || !stamp || !nf) return APSPIE_ERR_OOM;
+  // per-vertex (round, skip, distance) words of the hubs' chunked expansions
+  auto *xw = (unsigned long long *)workspace(ctx, kSlotSsspHubWord,
+                                             sizeof(unsigned long long) * (size_t)m);
+  if (!st || !qa || !qb || !ca || !cb || !stamp || !nf || !xw) return APSPIE_ERR_OOM;
   int *fstamp = nf, *far0 = nf + 2 * mm, *far1 = nf + 3 * mm, *far2 = nf + 4 * mm;
   unsigned *xd = (unsigned *)(nf + mm);
   ctx->sssp_state = st;
@@ -483,8 +525,8 @@ int sssp_run(apspie_context *ctx, int src, int64_t nnz, int m, const int *d_ptr,
   int grid = clamp_grid(ctx, pull3 ? sssp_grid<W, 3>(ctx) : sssp_grid<W, 2>(ctx));
   if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_sssp: occupancy query failed");
   int init_grid = std::min((m + 255) / 256, ctx->num_sms * 8);
-  sssp_init<W><<<init_grid, 256, 0, ctx->stream>>>(m, src, d_dist, stamp, fstamp, xd, d_ptr, qa,
-                                                   ca, st);
+  sssp_init<W><<<init_grid, 256, 0, ctx->stream>>>(m, src, d_dist, stamp, fstamp, xd, xw, d_ptr,
+                                                   qa, ca, st);
   int rc = check_launch(ctx, "sssp_init");
   if (rc) return rc;
   int2 *hubc = nullptr;
@@ -501,7 +543,7 @@ int sssp_run(apspie_context *ctx, int src, int64_t nnz, int m, const int *d_ptr,
   void *args[] = {&m,  (void *)&d_ptr, (void *)&d_ind, (void *)&d_w, &d_dist, &stamp,
                   &qa, &qb,            &ca,            &cb,           &st,     &max_rounds,
                   &fstamp, &xd, &far0, &far1, &far2, &delta, &nnz_ll, (void *)&d_tptr,
-                  (void *)&d_tind, (void *)&d_tw, &hubc, &alpha};
+                  (void *)&d_tind, (void *)&d_tw, &hubc, &alpha, &xw};
   const void *kern =
       pull3 ? (const void *)sssp_persistent<W, 3> : (const void *)sssp_persistent<W, 2>;
   cudaError_t e = cudaLaunchCooperativeKernel(kern, dim3(grid),

@@ -198,8 +198,9 @@ def sssp_prepare(ctx: Context, g):
     return g
 
 
-def sssp_set_pull(ctx: Context, alpha: int = 2) -> None:
-    """Pull rounds when the frontier's out-edges * alpha exceed nnz (0: never)."""
+def sssp_set_pull(ctx: Context, alpha: int = 0) -> None:
+    """Pull rounds when the frontier's out-edges * alpha exceed nnz (0: never,
+    the default)."""
     check(lib.apspie_sssp_set_pull(ctx.handle, int(alpha)), ctx.handle, "apspie_sssp_set_pull")
 
 

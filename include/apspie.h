@@ -172,7 +172,9 @@ int apspie_sssp_f32(apspie_ctx ctx, int src, int64_t nnz, int m,
 /* The same, direction-optimising: given the in-adjacency with its weights
  * (d_tptr / d_tind / d_tw, e.g. from apspie_csr_transpose with the weights
  * as the values), a round whose frontier's out-edges times alpha exceed nnz
- * (apspie_sssp_set_pull, default 2, the best of 2 .. 10 on R-MAT 22; 0 = never) scans every in-edge
+ * (apspie_sssp_set_pull; default 0 = never: with the staged push rounds,
+ * push-only measured 3.1 ms per source on R-MAT 22 symmetrised against 3.7
+ * at alpha 2, and 6.2 against 7.3 ms on R-MAT 23) scans every in-edge
  * instead: each vertex takes the least d[u] + w(u,v) over its in-neighbours
  * in the frontier and writes its own distance, without atomics.  Same
  * results as apspie_sssp_u32 / _f32 (the same min-plus fixpoint); pull
