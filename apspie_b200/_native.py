@@ -119,6 +119,7 @@ PROTOS: dict[str, tuple] = {
     "apspie_server_submit_device": (c_int, [vp, c_int, c_int, c_int, c_u32, vp, P_u64]),
     "apspie_server_replay": (c_int, [vp, c_int, vp, c_int, vp, C.POINTER(C.c_double)]),
     "apspie_server_replay_plain": (c_int, [vp, c_int, vp, c_int, vp, C.POINTER(C.c_double)]),
+    "apspie_server_replay_keep": (c_int, [vp, c_int, vp, c_int, vp, vp, C.POINTER(C.c_double)]),
     "apspie_server_poll": (c_int, [vp, c_u64, P_int, C.POINTER(C.c_double)]),
     "apspie_server_wait": (c_int, [vp, c_u64, C.POINTER(C.c_double)]),
     "apspie_server_get_stats": (c_int, [vp, C.POINTER(ServerStats)]),

@@ -712,6 +712,11 @@ int apspie_server_submit_device(apspie_server_t s, int type, int graph, int sour
 
 int apspie_server_replay(apspie_server_t s, int n, const apspie_query *q, int to_host,
                          double *lat_ms, double *wall_ms) {
+  return apspie_server_replay_keep(s, n, q, to_host, nullptr, lat_ms, wall_ms);
+}
+
+int apspie_server_replay_keep(apspie_server_t s, int n, const apspie_query *q, int to_host,
+                              int32_t *const *d_keep, double *lat_ms, double *wall_ms) {
   if (!s || n < 0 || (n > 0 && (!q || !lat_ms))) return APSPIE_ERR_INVALID;
   {
     std::lock_guard<std::mutex> lock(s->mu);
@@ -730,8 +735,9 @@ int apspie_server_replay(apspie_server_t s, int n, const apspie_query *q, int to
     std::lock_guard<std::mutex> lock(s->mu);
     // the pending queue is large; a full one is waited out, the query keeps
     // its scheduled arrival time
-    while ((st = enqueue_locked(s, q[i].type, q[i].graph, q[i].source, q[i].seed, nullptr,
-                                nullptr, at, &rs[i])) == APSPIE_ERR_BUSY) {
+    int32_t *keep = d_keep ? d_keep[i] : nullptr;
+    while ((st = enqueue_locked(s, q[i].type, q[i].graph, q[i].source, q[i].seed, nullptr, keep,
+                                at, &rs[i])) == APSPIE_ERR_BUSY) {
       s->mu.unlock();
       std::this_thread::sleep_for(std::chrono::microseconds(100));
       s->mu.lock();

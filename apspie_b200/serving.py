@@ -67,16 +67,32 @@ class Server:
         self._live[rid.value] = out
         return rid.value
 
-    def replay(self, queries, plain: bool = False, to_host: bool = True):
+    def replay(self, queries, plain: bool = False, to_host: bool = True, keep=None):
         """Open-loop replay of a timed query stream: `queries` is a structured
         array with fields type, graph, source, seed, t_us (see QUERY_DTYPE).
         Returns (latencies_ms array, wall_ms); a latency runs from the query's
         arrival until its result is in host memory (to_host) or on the device.
         plain=True runs the stream one query at a time through the
-        single-query kernels instead."""
+        single-query kernels instead.  keep (batched replay only): a dict
+        {query index: int32 device tensor of the graph's m entries} that
+        receives those queries' answers (apspie_server_replay_keep)."""
         q = np.ascontiguousarray(queries, dtype=QUERY_DTYPE)
         lat = np.zeros(len(q), dtype=np.float64)
         wall = C.c_double()
+        if keep:
+            if plain:
+                raise ValueError("keep is for the batched replay")
+            rows = (C.c_void_p * len(q))()
+            for i, t in keep.items():
+                m = self._graphs[int(q["graph"][i])].m
+                if t.numel() < m or t.dtype.itemsize != 4 or not t.is_cuda:
+                    raise ValueError(f"keep[{i}]: needs a device row of {m} 32-bit entries")
+                rows[i] = t.data_ptr()
+            check(lib.apspie_server_replay_keep(self._h, len(q), C.c_void_p(q.ctypes.data),
+                                                int(bool(to_host)), rows,
+                                                C.c_void_p(lat.ctypes.data), C.byref(wall)),
+                  what="apspie_server_replay_keep")
+            return lat, wall.value
         fn = lib.apspie_server_replay_plain if plain else lib.apspie_server_replay
         check(fn(self._h, len(q), C.c_void_p(q.ctypes.data), int(bool(to_host)),
                  C.c_void_p(lat.ctypes.data), C.byref(wall)), what="apspie_server_replay")

@@ -152,88 +152,145 @@ def build_graph(scale):
     return h
 
 
-def cpu_reference_bfs(h, sources, threads, budget_s, stop=1 << 30):
-    """The reference's SimpleReferenceBfs (oracle/_ref) on `threads` host
-    threads, one source each per round, until the sources or the time budget
-    run out.  Returns (edges, seconds, bfs_count)."""
+def cpu_reference_bfs(h, sources, budget_s):
+    """The reference's SimpleReferenceBfs (oracle/_ref) on one host thread,
+    one source after another until the sources or the time budget run out.
+    Returns (edges, seconds, traversals)."""
     import oracle
     deg = h.degrees()
-    results = []
-    lock = threading.Lock()
-    it = iter(sources)
-    t_end = time.perf_counter() + budget_s
-
-    def worker():
-        while time.perf_counter() < t_end:
-            with lock:
-                s = next(it, None)
-            if s is None:
-                return
-            d = np.empty(h.m, np.int32)
-            t0 = time.perf_counter()
-            oracle._r.ref_bfs_cpu(int(s), h.m, h.ptr.ctypes.data, h.ind.ctypes.data,
-                                  d.ctypes.data, stop)
-            dt = time.perf_counter() - t0
-            e = int(deg[d >= 0].sum())
-            with lock:
-                results.append((e, dt))
-
-    import ctypes
-    sys.stdout.flush()
-    ctypes.CDLL(None).fflush(None)
-    saved = os.dup(1)
-    devnull = os.open(os.devnull, os.O_WRONLY)
-    os.dup2(devnull, 1)
-    try:
+    edges, n = 0, 0
+    with quiet_stdout():
         t0 = time.perf_counter()
-        th = [threading.Thread(target=worker) for _ in range(threads)]
-        for t in th:
-            t.start()
-        for t in th:
-            t.join()
+        for s in sources:
+            if time.perf_counter() - t0 > budget_s:
+                break
+            d = np.empty(h.m, np.int32)
+            oracle._r.ref_bfs_cpu(int(s), h.m, h.ptr.ctypes.data, h.ind.ctypes.data,
+                                  d.ctypes.data, 1 << 30)
+            edges += int(deg[d >= 0].sum())
+            n += 1
         wall = time.perf_counter() - t0
-    finally:
+    return edges, wall, n
+
+
+class quiet_stdout:
+    """The reference routines print timings to stdout; keep them off the
+    single JSON line this script prints."""
+
+    def __enter__(self):
+        import ctypes
+        sys.stdout.flush()
         ctypes.CDLL(None).fflush(None)
-        os.dup2(saved, 1)
-        os.close(saved)
-        os.close(devnull)
-    edges = sum(e for e, _ in results)
-    return edges, wall, len(results), sum(dt for _, dt in results)
+        self.saved = os.dup(1)
+        self.devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.devnull, 1)
+        return self
+
+    def __exit__(self, *exc):
+        import ctypes
+        ctypes.CDLL(None).fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.devnull)
+
+
+def shared_config(scale, m, nnz, world):
+    """The `config` object both arms print (same workload, same graph)."""
+    return {"workload": WORKLOAD, "scale": scale, "m": int(m), "nnz": int(nnz),
+            "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (CSR %.0f MB), no flush" % ((4 * (m + 1) + 4 * nnz) / 1e6)}
 
 
 def run_reference(args):
+    """The reference's own CPU BFS (SimpleReferenceBfs, src/testBfs.cpp:7-72,
+    compiled into oracle/_ref) on all host threads: a step is one round of
+    concurrent single-threaded traversals, one per host thread, each from its
+    own source.  The graph and sources come from oracle.inputs (a NumPy
+    restatement of the library's builder), so this arm loads none of the
+    product's code."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
     import oracle
+    import oracle.inputs as oi
     kind = "reference" if oracle.have_reference() else "port"
-    h = build_graph(args.scale)
-    import apspie_b200 as ap
+    m, ptr, ind = oi.gen_rmat(args.scale, EDGE_FACTOR, seed=SEED, symmetric=True)
     threads = os.cpu_count() or 1
-    sources = ap.seeded_sources(h, max(args.steps, 1) * threads, seed=0)
-    # warm-up: a depth-limited traversal per thread
-    cpu_reference_bfs(h, sources[:threads], threads, 30.0, stop=1)
-    edges, wall, n, _ = cpu_reference_bfs(h, sources, threads, 120.0)
+    K, W = max(args.steps, 1), max(args.warmup, 0)
+    sources = oi.seeded_sources(m, ptr, ind, (K + W) * threads, seed=0)
+    deg = np.diff(ptr).astype(np.int64)
+
+    def one_round(srcs):
+        edges = [0] * len(srcs)
+
+        def work(i):
+            d = np.empty(m, np.int32)
+            oracle._r.ref_bfs_cpu(int(srcs[i]), m, ptr.ctypes.data, ind.ctypes.data,
+                                  d.ctypes.data, 1 << 30)
+            edges[i] = int(deg[d >= 0].sum())
+        th = [threading.Thread(target=work, args=(i,)) for i in range(len(srcs))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        return sum(edges)
+
+    with quiet_stdout():
+        for st in range(W):
+            one_round(sources[st * threads:(st + 1) * threads])
+        t0 = time.perf_counter()
+        edges = 0
+        for st in range(W, W + K):
+            edges += one_round(sources[st * threads:(st + 1) * threads])
+        wall = time.perf_counter() - t0
     gteps = edges / wall / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": gteps, "unit": "GTEPS",
-        "n_gpus": args.gpus, "steps": n, "warmup": args.warmup,
-        "ms_per_step": 1e3 * wall / max(n, 1), "higher_is_better": True, "scaling": "weak",
+        "n_gpus": args.gpus, "steps": K, "warmup": W,
+        "ms_per_step": 1e3 * wall / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "scale": args.scale},
+        "config": shared_config(args.scale, m, len(ind), world),
         "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": threads, "kind": kind,
-                         "sample": f"{n} full BFS traversals of R-MAT {args.scale}, "
-                                   f"{threads} concurrent single-threaded SimpleReferenceBfs "
-                                   f"(src/testBfs.cpp:7-72), 120 s budget"},
+                         "sample": f"{K} steps of {threads} concurrent single-threaded "
+                                   f"SimpleReferenceBfs (src/testBfs.cpp:7-72, -O3) traversals "
+                                   f"of R-MAT {args.scale}, one source each ({K * threads} "
+                                   f"traversals), after {W} untimed steps"},
         "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def sssp_leg(ctx, steps=20):
-    """SSSP on R-MAT 20 (directed, dedup), uint32 weights in [1, 255] and
-    float weights in (0, 1]: GTEPS = E_R / device time, inputs resident."""
+def _sssp_block(ctx, g, srcs, kind, m):
+    """Mean device ms per SSSP over srcs (CUDA events), GTEPS, algorithmic
+    GB/s (8 E_R + 8 |R| + 4 m per traversal), edges walked per reached edge."""
     import torch
+    import apspie_b200 as ap
+    st = []
+    for s in srcs:
+        ap.sssp(ctx, g, s, weights=kind)
+        st.append(ap.sssp_stats(ctx))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(torch.cuda.current_stream())
+    for s in srcs:
+        ap.sssp(ctx, g, s, weights=kind)
+    b.record(torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / len(srcs)
+    edges = sum(x["edges_traversed"] for x in st) / len(st)
+    reached = sum(x["vertices_reached"] for x in st) / len(st)
+    b_alg = 8.0 * edges + 8.0 * reached + 4.0 * m
+    return {"ms_per_sssp": ms, "gteps": edges / (ms * 1e-3) / 1e9,
+            "hbm_gbs_alg": b_alg / (ms * 1e-3) / 1e9,
+            "relaxations_per_edge": sum(x["relaxations"] for x in st) / max(1.0, edges * len(st)),
+            "rounds": st[-1]["rounds"], "sources": len(srcs)}
+
+
+def sssp_leg(ctx, big, steps=20):
+    """SSSP on R-MAT 20 (directed, dedup) with uint32 weights in [1, 255]
+    and float weights in (0, 1], and on the symmetrised R-MAT 22 / 23 of the
+    serving workload with uint32 weights (push rounds, one source at a time):
+    device time per traversal, inputs resident."""
     import apspie_b200 as ap
     h = ap.gen_rmat(20, EDGE_FACTOR, seed=SEED, symmetric=False)
     ap.weights_u32(h, seed=SEED)
@@ -241,29 +298,24 @@ def sssp_leg(ctx, steps=20):
     g = h.to_device()
     srcs = ap.seeded_sources(h, steps, seed=3)
     out = {"graph": f"R-MAT 20 directed, m={h.m}, nnz={h.nnz}"}
-    stream = torch.cuda.current_stream()
     for kind in ("u32", "f32"):
-        e_r = []
         for s in srcs[:3]:
             ap.sssp(ctx, g, s, weights=kind)
-        for s in srcs:
-            ap.sssp(ctx, g, s, weights=kind)
-            e_r.append(ap.sssp_stats(ctx))
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        a.record(stream)
-        for s in srcs:
-            ap.sssp(ctx, g, s, weights=kind)
-        b.record(stream)
-        torch.cuda.synchronize()
-        ms = a.elapsed_time(b)
-        edges = sum(x["edges_traversed"] for x in e_r)
-        reached = sum(x["vertices_reached"] for x in e_r) / len(e_r)
-        b_alg = 8.0 * edges / len(e_r) + 8.0 * reached + 4.0 * h.m
-        out[kind] = {"gteps": edges / (ms * 1e-3) / 1e9, "ms_per_sssp": ms / len(srcs),
-                     "hbm_gbs_alg": b_alg / (ms / len(srcs) * 1e-3) / 1e9,
-                     "relaxations_per_edge": sum(x["relaxations"] for x in e_r) / max(edges, 1),
-                     "rounds": e_r[-1]["rounds"]}
+        out[kind] = _sssp_block(ctx, g, srcs, kind, h.m)
+    del g
+    if big.w_u32 is None:
+        ap.weights_u32(big, seed=SEED)
+    g22 = big.to_device()
+    out["rmat22_sym_u32"] = _sssp_block(ctx, g22, ap.seeded_sources(big, 8, seed=3), "u32", big.m)
+    del g22
+    g23 = ap.gen_rmat_device(ctx, 23, EDGE_FACTOR, seed=SEED)
+    ap.weights_device(ctx, g23, seed=SEED)
+    deg = (g23.ptr[1:] - g23.ptr[:-1]).cpu().numpy()
+    cand = np.flatnonzero(deg > 0)
+    rng = np.random.default_rng(3)
+    s23 = [int(x) for x in cand[rng.integers(len(cand), size=6)]]
+    ap.sssp(ctx, g23, s23[0], weights="u32")
+    out["rmat23_sym_u32"] = _sssp_block(ctx, g23, s23, "u32", g23.m)
     return out
 
 
@@ -340,107 +392,106 @@ def mis_tc_spgemm_leg(ctx):
 def batched_leg(ctx, big):
     """256 BFS + 64 SSSP (uint32 weights) sources over R-MAT 12/16/20/22
     (symmetrised) and the 1024x1024 grid, in one batched launch, against the
-    same queries one at a time through the single-source kernels."""
+    same queries one at a time through the single-source kernels.  Every one
+    of the 320 batched rows is compared with its single-source result (bit
+    for bit; a mismatch raises).  Per graph: its sources one at a time and
+    its two jobs in a batched launch of their own."""
     import torch
     import apspie_b200 as ap
-    graphs = {12: ap.gen_rmat(12, 16, seed=SEED), 16: ap.gen_rmat(16, 16, seed=SEED),
-              20: ap.gen_rmat(20, 16, seed=SEED), 22: big, "grid": ap.gen_grid(1024, 1024)}
-    plan_bfs = {22: 64, 20: 64, 16: 64, 12: 32, "grid": 32}
-    plan_sssp = {22: 8, 20: 16, 16: 16, 12: 16, "grid": 8}
-    dev, jobs, plain = {}, [], []
-    for k, h in graphs.items():
-        if h.w_u32 is None:
-            ap.weights_u32(h, seed=SEED)
-        dev[k] = h.to_device()
-        if k == "grid":
-            srcs = list(range(0, h.m, h.m // 64))
-        else:
-            srcs = ap.seeded_sources(h, plan_bfs[k] + plan_sssp[k], seed=7)
-        jobs.append({"type": "bfs", "graph": dev[k], "sources": srcs[:plan_bfs[k]]})
-        jobs.append({"type": "sssp", "graph": dev[k], "sources": srcs[plan_bfs[k]:][:plan_sssp[k]]})
-    # warm-up + reference results of the plain path (E_R from its stats)
-    edges = 0
-    for j in jobs:
-        for s in j["sources"]:
-            if j["type"] == "bfs":
-                ap.bfs(ctx, j["graph"], s)
-                edges += ap.bfs_stats(ctx)["edges_traversed"]
-            else:
-                ap.sssp(ctx, j["graph"], s, weights="u32")
-                edges += ap.sssp_stats(ctx)["edges_traversed"]
-    ap.batch_run(ctx, jobs)
+    from apspie_b200 import workloads as wl
+    hosts = wl.batched_graphs(seed=SEED, big=big)
+    devs = {k: h.to_device() for k, h in hosts.items()}
+    jobs = wl.batched_jobs(hosts, devs)
     stream = torch.cuda.current_stream()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    torch.cuda.synchronize()
-    ev[0].record(stream)
-    for j in jobs:
-        for s in j["sources"]:
-            if j["type"] == "bfs":
-                ap.bfs(ctx, j["graph"], s)
-            else:
-                ap.sssp(ctx, j["graph"], s, weights="u32")
-    ev[1].record(stream)
-    torch.cuda.synchronize()
-    plain_s = ev[0].elapsed_time(ev[1]) * 1e-3
-    ev[2].record(stream)
-    outs = ap.batch_run(ctx, jobs)
-    ev[3].record(stream)
-    torch.cuda.synchronize()
-    batch_s = ev[2].elapsed_time(ev[3]) * 1e-3
+
+    def plain_run(js, keep=None):
+        edges = 0
+        for j in js:
+            for s in j["sources"]:
+                if j["type"] == "bfs":
+                    r = ap.bfs(ctx, j["graph"], s)
+                else:
+                    r = ap.sssp(ctx, j["graph"], s, weights="u32")
+                if keep is not None:
+                    edges += (ap.bfs_stats(ctx) if j["type"] == "bfs"
+                              else ap.sssp_stats(ctx))["edges_traversed"]
+                    keep.append(r)
+        return edges
+
+    def timed(fn):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        out = fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]), out
+
+    # warm-up (workspaces, autotuner / depth caches) and the reference rows
+    refs = []
+    edges = plain_run(jobs, refs)
+    ap.batch_run(ctx, jobs)
+    plain_ms, _ = timed(lambda: plain_run(jobs))
+    batch_ms, outs = timed(lambda: ap.batch_run(ctx, jobs))
     st = ap.batch_stats(ctx)
-    # spot check: every batched result equals the single-source path
+    verified = 0
+    it = iter(refs)
     for j, o in zip(jobs, outs):
-        s = j["sources"][0]
-        ref = (ap.bfs(ctx, j["graph"], s) if j["type"] == "bfs"
-               else ap.sssp(ctx, j["graph"], s, weights="u32"))
-        if not torch.equal(o[0], ref):
-            raise RuntimeError("batched result differs from the single-source path")
+        for i, s in enumerate(j["sources"]):
+            if not torch.equal(o[i], next(it)):
+                raise RuntimeError(f"batched {j['type']} row of source {s} on {j['key']} "
+                                   "differs from the single-source path")
+            verified += 1
+    per_graph = {}
+    for k in hosts:
+        js = [j for j in jobs if j["key"] == k]
+        pm, _ = timed(lambda: plain_run(js))
+        ap.batch_run(ctx, js)
+        bm, _ = timed(lambda: ap.batch_run(ctx, js))
+        per_graph["grid1024" if k == "grid" else f"rmat{k}"] = {
+            "bfs": len(js[0]["sources"]), "sssp": len(js[1]["sources"]),
+            "plain_ms": pm, "batched_alone_ms": bm, "speedup": pm / bm}
     nq = sum(len(j["sources"]) for j in jobs)
     return {"queries": nq, "bfs": 256, "sssp": 64,
             "graphs": "R-MAT 12/16/20/22 symmetrised + grid 1024x1024",
-            "batched_gteps": edges / batch_s / 1e9, "plain_gteps": edges / plain_s / 1e9,
-            "speedup_vs_plain": plain_s / batch_s, "batched_ms": batch_s * 1e3,
-            "plain_ms": plain_s * 1e3, "super_steps": st["super_steps"],
+            "batched_gteps": edges / (batch_ms * 1e-3) / 1e9,
+            "plain_gteps": edges / (plain_ms * 1e-3) / 1e9,
+            "speedup_vs_plain": plain_ms / batch_ms, "batched_ms": batch_ms,
+            "plain_ms": plain_ms, "super_steps": st["super_steps"], "verified": verified,
+            "per_graph": per_graph,
             "timing": "CUDA events on the launching stream (plain: all single-source calls "
-                      "back to back; batched: one apspie_batch_run, transposes included)"}
+                      "back to back; batched: one apspie_batch_run, transposes included); "
+                      "per_graph: each graph's two jobs in a launch of their own"}
 
 
-SERVE_SCALES = (12, 14, 16, 18, 20, 22, 23)
-
-
-def serving_leg(ctx, rates=(1000, 100000), n_queries=600, seed=SEED):
+def serving_leg(ctx, rates=(100, 1000, 10000, 100000), n_queries=600, seed=SEED, n_verify=120):
     """Serving: 8 device-resident graphs (R-MAT 12..23 symmetrised + the
     1024x1024 grid, uint32 weights in [1, 255]), a Poisson stream of 60% BFS
     / 30% SSSP / 10% MIS queries, graph chosen in proportion to its vertex
-    count, sources seed-chosen among vertices with edges.  Each rate is
-    replayed open-loop through the server (continuous batching) and through
-    the plain one-query-at-a-time path; latency = arrival -> result row in
-    (pinned) host memory."""
+    count (the first 24 queries are one of every (graph, kind) pair), sources
+    seed-chosen among vertices with edges.  Each rate is replayed open-loop
+    through the server (continuous batching) and through the plain
+    one-query-at-a-time path; latency = arrival -> result row in (pinned) host
+    memory.  During the server's replay the answers of a seeded sample of
+    n_verify queries (every pair in the stream among them) are kept on the
+    device and compared with the single-query path afterwards; a mismatch
+    raises."""
     import torch
     import apspie_b200 as ap
+    from apspie_b200 import workloads as wl
     from apspie_b200.serving import QUERY_DTYPE
-    graphs = [ap.gen_rmat_device(ctx, sc, EDGE_FACTOR, seed=seed) for sc in SERVE_SCALES]
-    graphs.append(ap.gen_grid(1024, 1024).to_device())
-    for g in graphs:
-        ap.weights_device(ctx, g, seed=seed)
-        # graph build step: the in-adjacency with its weights for push/pull
-        # SSSP on the large R-MAT graphs (one transpose each)
-        if g.nnz > (16 << 20):
-            ap.sssp_prepare(ctx, g)
+    graphs = wl.serving_graphs(ctx, seed=seed)
+    names = wl.serving_names()
     torch.cuda.synchronize()
-    ms = np.array([g.m for g in graphs], dtype=np.float64)
-    degs = [(g.ptr[1:] - g.ptr[:-1]).cpu().numpy() for g in graphs]
-    nonzero = [np.flatnonzero(d > 0) for d in degs]
-    out = {"graphs": [f"rmat{sc}" for sc in SERVE_SCALES] + ["grid1024"],
-           "mix": "60% BFS / 30% SSSP / 10% MIS", "queries_per_rate": n_queries,
+    out = {"graphs": names, "mix": "60% BFS / 30% SSSP / 10% MIS", "queries_per_rate": n_queries,
            "latency": "arrival -> result row in host memory (device -> pinned host copy included)",
-           "budget_gb": 120, "rates": [],
-           "sssp_pull_graphs": [n for n, g in zip([f"rmat{sc}" for sc in SERVE_SCALES] + ["grid1024"],
-                                                  graphs) if "sssp_in" in g.extra]}
+           "budget_gb": 120, "rates": []}
+    kinds = ("bfs", "sssp", "mis")
     with ap.Server(budget_bytes=120 << 30, max_batch=256) as srv:
         gids = [srv.add_graph(g) for g in graphs]
         # untimed warm-up of both paths: every (graph, kind) alone and in
         # groups, so workspaces, result buffers and MIS priorities exist
+        nonzero = [np.flatnonzero((g.ptr[1:] - g.ptr[:-1]).cpu().numpy() > 0) for g in graphs]
         wq = []
         for gi, g in enumerate(graphs):
             for kind in (0, 1, 2):
@@ -456,23 +507,47 @@ def serving_leg(ctx, rates=(1000, 100000), n_queries=600, seed=SEED):
         srv.replay(warm)
         srv.replay(warm[::7], plain=True)
         for rate in rates:
-            rng = np.random.default_rng(seed * 1000 + int(rate))
-            q = np.zeros(n_queries, dtype=QUERY_DTYPE)
-            q["type"] = rng.choice([0, 1, 2], size=n_queries, p=[0.6, 0.3, 0.1])
-            gi = rng.choice(len(graphs), size=n_queries, p=ms / ms.sum())
-            q["graph"] = [gids[i] for i in gi]
-            q["source"] = [int(nonzero[i][rng.integers(len(nonzero[i]))]) for i in gi]
-            q["seed"] = 1
-            q["t_us"] = np.cumsum(rng.exponential(1e6 / rate, size=n_queries))
+            q, gi = wl.poisson_stream(graphs, gids, n_queries, float(rate), seed * 1000 + int(rate),
+                                      cover=True)
+            rng = np.random.default_rng(seed * 7 + int(rate))
+            pick = {}
+            for i in range(len(q)):   # the first query of every (graph, kind) pair
+                pick.setdefault((int(gi[i]), int(q["type"][i])), i)
+            sample = set(pick.values())
+            for i in rng.permutation(len(q)):
+                if len(sample) >= n_verify:
+                    break
+                sample.add(int(i))
+            keep = {i: torch.empty(graphs[int(gi[i])].m, dtype=torch.int32, device="cuda")
+                    for i in sorted(sample)}
             row = {"rate_qps": rate}
+            lats = {}
             for name, plain in (("batched", False), ("plain", True)):
-                lat, wall = srv.replay(q, plain=plain)
+                lat, wall = srv.replay(q, plain=plain, keep=None if plain else keep)
+                lats[name] = lat
                 row[name] = {"qps": n_queries / (wall * 1e-3),
                              "p50_ms": float(np.percentile(lat, 50)),
                              "p99_ms": float(np.percentile(lat, 99)),
                              "wall_ms": wall}
             row["throughput_ratio"] = row["batched"]["qps"] / row["plain"]["qps"]
+            for i, t in keep.items():
+                ref = wl.plain_answer(ctx, graphs[int(gi[i])], int(q["type"][i]),
+                                      int(q["source"][i]), int(q["seed"][i]))
+                if not torch.equal(t, ref):
+                    raise RuntimeError(f"served answer of query {i} ({kinds[q['type'][i]]} on "
+                                       f"{names[gi[i]]}) differs from the single-query path")
+            row["verified"] = len(keep)
+            row["pairs_in_stream"] = len(pick)
+            table = {}
+            for (g_i, k), _ in sorted(pick.items()):
+                sel = (gi == g_i) & (q["type"] == k)
+                table[f"{names[g_i]}/{kinds[k]}"] = [
+                    int(sel.sum()), round(float(np.median(lats["batched"][sel])), 2),
+                    round(float(np.median(lats["plain"][sel])), 2)]
+            row["by_graph_kind"] = table
+            row["by_graph_kind_columns"] = ["queries", "batched_p50_ms", "plain_p50_ms"]
             out["rates"].append(row)
+            del keep
     return out
 
 
@@ -517,7 +592,7 @@ def run_ours(args):
         ap.bfs_set_params(ctx, sa, sb)
         tune = {"alpha": sa, "beta": sb}
     elif not args.no_tune:
-        tune_src = ap.seeded_sources(h, 16, seed=1000 + rank)
+        tune_src = ap.seeded_sources(h, 64, seed=1000 + rank)
         tune = ap.autotune_bfs(ctx, g, tune_src)
     e_r = []
     for s in sources[:nsrc]:
@@ -598,7 +673,7 @@ def run_ours(args):
 
     extras = {}
     if not args.profile_run and rank == 0:
-        extras["sssp"] = sssp_leg(ctx)
+        extras["sssp"] = sssp_leg(ctx, h)
         extras["mis_tc_spgemm"] = mis_tc_spgemm_leg(ctx)
         extras["batched"] = batched_leg(ctx, h)
         extras["serving"] = serving_leg(ctx)
@@ -608,7 +683,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.profile_run:
         import oracle
         if oracle.have_reference():
-            edges, wall, n, busy = cpu_reference_bfs(h, sources[:8], 1, 20.0)
+            edges, wall, n = cpu_reference_bfs(h, sources[:8], 20.0)
             cpu = {"value": edges / wall / 1e9, "unit": "GTEPS", "cores": 1,
                    "kind": "reference",
                    "sample": f"{n} BFS traversals of the same graph and sources, "
@@ -623,20 +698,19 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": nsrc,
         "warmup": args.warmup, "ms_per_step": ms / nsrc, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "scale": args.scale, "m": h.m, "nnz": h.nnz,
-                   "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (CSR %.0f MB), no flush" %
-                         ((h.ptr.nbytes + h.ind.nbytes) / 1e6),
-                   "edges_traversed_per_step": float(np.mean(e_r)),
-                   "vertices_reached": int(reached),
-                   "pull_adjacency": ("CSR as given" if prep_ms is None else
-                                      "in-adjacency ordered by neighbour out-degree, built once "
-                                      "by apspie_bfs_prepare in %.1f ms outside the timed region"
-                                      % prep_ms),
-                   "switch_points": {"alpha": tune.get("alpha"), "beta": tune.get("beta"),
-                                     "picked_by": "--switch" if args.switch else
-                                     "defaults" if args.no_tune else
-                                     "autotuner on 16 untimed sources (21 switch-point candidates, two sweeps)"}},
+        "config": shared_config(args.scale, h.m, h.nnz, world),
+        "workload_stats": {"edges_traversed_per_step": float(np.mean(e_r)),
+                           "vertices_reached": int(reached),
+                           "pull_adjacency": ("CSR as given" if prep_ms is None else
+                                              "in-adjacency ordered by neighbour out-degree, "
+                                              "built once by apspie_bfs_prepare in %.1f ms "
+                                              "outside the timed region" % prep_ms),
+                           "switch_points": {"alpha": tune.get("alpha"), "beta": tune.get("beta"),
+                                             "picked_by": "--switch" if args.switch else
+                                             "defaults" if args.no_tune else
+                                             "autotuner on 64 untimed sources (21 switch-point "
+                                             "candidates ranked on 32, the best 4 re-timed on "
+                                             "the other 32, two sweeps each)"}},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "per_step_ms": {"min": min(per), "median": statistics.median(per), "max": max(per)},

@@ -350,6 +350,13 @@ typedef struct {
  * completion. */
 int apspie_server_replay(apspie_server_t s, int n, const apspie_query *q,
                          int to_host, double *lat_ms, double *wall_ms);
+/* apspie_server_replay that keeps answers: d_keep (may be NULL) holds one
+ * device pointer per query, NULL or a row of m 32-bit entries on the
+ * server's device into which that query's result is copied (device to
+ * device, on the query's stream, before its completion is recorded), so a
+ * sample of the served answers can be checked after a timed replay. */
+int apspie_server_replay_keep(apspie_server_t s, int n, const apspie_query *q, int to_host,
+                              int32_t *const *d_keep, double *lat_ms, double *wall_ms);
 /* The same stream one query at a time, in arrival order, through
  * apspie_bfs / apspie_sssp_u32 / apspie_mis on a stream of its own (the
  * plain single-query path); latencies likewise from the arrival times. */
@@ -368,8 +375,9 @@ int apspie_server_destroy(apspie_server_t s);
 
 /* ----------------------------------------------------------- autotuner ---
  * Measures the BFS direction thresholds on the given sample sources (a grid
- * of alpha / beta values and push-only, timed with CUDA events), stores the
- * fastest in the context (used by apspie_bfs and, for jobs with alpha / beta
+ * of alpha / beta values and push-only, timed with CUDA events: ranked on
+ * the first half of the sources, the four best timed again on the second
+ * half, the pick by the sum), stores the fastest in the context (used by apspie_bfs and, for jobs with alpha / beta
  * < 0, by apspie_batch_run) and caches it under a fingerprint of the graph
  * (m, nnz, sampled row offsets); a cached graph is not re-measured.
  * d_depth_scratch: m int32.  *ms_out (may be NULL) = mean ms per BFS. */

@@ -128,3 +128,22 @@ def test_transpose_host():
     sym = ap.gen_rmat(10, 8, seed=2)
     st = sym.transpose()
     np.testing.assert_array_equal(st.ind, sym.ind)
+
+
+def test_numpy_rmat_restatement_equals_builder(golden):
+    """oracle.inputs (the reference arm's input builder, which loads none of
+    the library) gives the library's R-MAT graphs and sources bit for bit,
+    and the golden hash of R-MAT 10."""
+    import hashlib
+    import oracle.inputs as oi
+    for scale, sym, seed in ((10, True, 3), (11, False, 5), (13, True, 1)):
+        m, ptr, ind = oi.gen_rmat(scale, 16, seed=seed, symmetric=sym, chunk=1 << 10)
+        g = ap.gen_rmat(scale, 16, seed=seed, symmetric=sym)
+        np.testing.assert_array_equal(ptr, g.ptr)
+        np.testing.assert_array_equal(ind, g.ind)
+        assert oi.seeded_sources(m, ptr, ind, 6, seed=2) == ap.seeded_sources(g, 6, seed=2)
+    m, ptr, ind = oi.gen_rmat(10, 16, seed=3, symmetric=True)
+    h = hashlib.sha256()
+    for a in (ptr, ind):
+        h.update(np.ascontiguousarray(a).tobytes())
+    assert h.hexdigest().encode() == golden["rmat10/sym_sha"].tobytes()
