@@ -60,7 +60,9 @@ constexpr int kMsHubIn = 1024;
 constexpr int kMsPullChunk = 1024;
 constexpr int kMsPullVerts = 8;
 
-struct JobCounters {
+// A level's counters, on a 128-byte line of their own (away from the job's
+// read-mostly fields and from the other levels' counters).
+struct alignas(128) JobCounters {
   unsigned long long qc;  // queue length (low 32 bits) | chunk-list length (high 32 bits)
   unsigned nbig, pad;
   unsigned long long edges;
@@ -191,66 +193,138 @@ __global__ void batch_seed_sssp(BatchJob *jobs, int jid) {
 }
 
 // --------------------------------------------------------- append helper ---
-// Appends up to N candidates per lane (an id u with degree deg, or nothing)
-// to the job's next queue / chunk list: one packed atomic per warp reserves
-// the queue slots and chunk entries, chunk entries are written 32 at a time.
+// A warp's joiners are staged in shared memory (JobStage) and get their
+// slots in the job's next queue / chunk list with one packed atomic per
+// flush, instead of one per warp batch: a reservation is an atomic on a
+// single address, and same-address atomics run at about 1.1 - 1.5 G/s on a
+// B200 (measured), so a pull step that appended per 32-vertex unit waited on
+// them.  The stage holds the entries of one job and one step; it is flushed
+// when the warp moves to a unit of another job and at the end of the step.
+// The next frontier's big-vertex count and edge total are summed per block
+// in shared memory and added once per block and job after the step.
+constexpr int kJStageQ = 256;  // queue entries per warp
+constexpr int kJStageB = 128;  // (vertex, degree) big entries per warp
+// one append call adds at most N x 32 entries of either kind, N <= 4
+// (kMsbfsUnroll): each stage must hold a whole call after a flush
+static_assert(kJStageQ >= 4 * 32 && kJStageB >= 4 * 32, "stage smaller than one append");
+constexpr int kStageWarpsB = kBatchThreads / 32;
+
+struct JobStage {
+  int *q;
+  int2 *b;  // (vertex, degree)
+  int nq, nb;
+  BatchJob *job;  // job of the staged entries, or nullptr
+  int level;      // the step: entries go to the level-(step + 1) lists
+};
+
+// Writes the staged entries of stg.job into its next queue / chunk list.
 // Warp-collective.
-template <int N>
-__device__ __forceinline__ void append_n(const BatchJob *j, const bool (&found)[N],
-                                         const int (&u)[N], const int (&deg)[N], int *qout,
-                                         int2 *cout, JobCounters *nxt) {
+__device__ __noinline__ void stage_flush(JobStage &stg) {
+  if (stg.nq == 0 && stg.nb == 0) return;
+  __syncwarp();
   const int lane = lane_id();
-  const int bd = j->big_deg, ck = j->chunk;
-  int nsmall = 0, nbig = 0, nchunk = 0;
+  BatchJob *j = stg.job;
+  const int L = stg.level;
+  const int ck = j->chunk;
+  int *qout = jobQ(j, (L + 1) % 3);
+  int2 *cout = jobC(j, (L + 1) % 3);
+  JobCounters *nxt = &j->c[(L + 1) % 3];
+  // chunk counts of the big entries and their exclusive prefix
+  int nch[kJStageB / 32], excl[kJStageB / 32];
+  unsigned ctot = 0;
+#pragma unroll
+  for (int i = 0; i < kJStageB / 32; ++i) {
+    const int e = i * 32 + lane;
+    nch[i] = e < stg.nb ? (stg.b[e].y + ck - 1) / ck : 0;
+    const int inc = warp_incl_scan(nch[i]);
+    excl[i] = (int)ctot + inc - nch[i];
+    ctot += (unsigned)__shfl_sync(kFull, inc, 31);
+  }
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(&nxt->qc, ((unsigned long long)ctot << 32) | (unsigned)stg.nq);
+  base = __shfl_sync(kFull, base, 0);
+  const unsigned qb = (unsigned)base, cb = (unsigned)(base >> 32);
+  for (int i = lane; i < stg.nq; i += 32) qout[qb + (unsigned)i] = stg.q[i];
+  // chunk entries (vertex, chunk index), 32 at a time over the flat list
+#pragma unroll
+  for (int i = 0; i < kJStageB / 32; ++i) {
+    const int tot = __shfl_sync(kFull, excl[i] + nch[i], 31) - __shfl_sync(kFull, excl[i], 0);
+    const int first = __shfl_sync(kFull, excl[i], 0);
+    const int rel = excl[i] - first;
+    for (int c0 = 0; c0 < tot; c0 += 32) {
+      const int e = c0 + lane;
+      const int owner = warp_owner(rel, min(e, tot - 1));
+      const int uo = __shfl_sync(kFull, i * 32 + lane < stg.nb ? stg.b[i * 32 + lane].x : 0,
+                                 owner);
+      const int ro = __shfl_sync(kFull, rel, owner);
+      if (e < tot) cout[cb + (unsigned)(first + e)] = make_int2(uo, e - ro);
+    }
+  }
+  __syncwarp();
+  stg.nq = 0;
+  stg.nb = 0;
+}
+
+// Stages up to N joiners per lane (vertex u[r] of degree deg[r] where
+// found[r]) of job j; the next frontier's big count and edges go to the
+// block's tallies.  Warp-collective.
+template <int N>
+__device__ __forceinline__ void append_n(BatchJob *j, const bool (&found)[N], const int (&u)[N],
+                                         const int (&deg)[N], JobStage &stg, unsigned *blk_nbig,
+                                         unsigned long long *blk_edges, int jid) {
+  const int lane = lane_id();
+  const int bd = j->big_deg;
+  int nsmall = 0, nbig = 0;
   unsigned long long edges = 0;
 #pragma unroll
   for (int r = 0; r < N; ++r) {
-    bool big = found[r] && deg[r] > bd;
+    const bool big = found[r] && deg[r] > bd;
     nsmall += (found[r] && !big) ? 1 : 0;
     nbig += big ? 1 : 0;
-    nchunk += big ? (deg[r] + ck - 1) / ck : 0;
     edges += found[r] ? (unsigned long long)deg[r] : 0ull;
   }
   const int qincl = warp_incl_scan(nsmall);
-  const int cincl = warp_incl_scan(nchunk);
-  const unsigned qtot = (unsigned)__shfl_sync(kFull, qincl, 31);
-  const unsigned ctot = (unsigned)__shfl_sync(kFull, cincl, 31);
-  if ((qtot | ctot) == 0u) return;
-  unsigned long long base = 0;
-  if (lane == 31) base = atomicAdd(&nxt->qc, ((unsigned long long)ctot << 32) | qtot);
-  base = __shfl_sync(kFull, base, 31);
-  if (qtot) {
-    unsigned qb = (unsigned)base + (unsigned)(qincl - nsmall);
-#pragma unroll
-    for (int r = 0; r < N; ++r)
-      if (found[r] && deg[r] <= bd) qout[qb++] = u[r];
+  const int bincl = warp_incl_scan(nbig);
+  const int qtot = __shfl_sync(kFull, qincl, 31);
+  const int btot = __shfl_sync(kFull, bincl, 31);
+  if ((qtot | btot) == 0) return;
+  if (stg.job != j) {
+    stage_flush(stg);
+    stg.job = j;
   }
-  if (ctot) {
-    unsigned cb = (unsigned)(base >> 32);
+  if (stg.nq + qtot > kJStageQ || stg.nb + btot > kJStageB) stage_flush(stg);
+  int qa = stg.nq + qincl - nsmall, ba = stg.nb + bincl - nbig;
 #pragma unroll
-    for (int r = 0; r < N; ++r) {
-      const bool big = found[r] && deg[r] > bd;
-      if (__ballot_sync(kFull, big) == 0u) continue;
-      const int nch = big ? (deg[r] + ck - 1) / ck : 0;
-      const int incl = warp_incl_scan(nch);
-      const int tot = __shfl_sync(kFull, incl, 31);
-      const int excl = incl - nch;
-      for (int c0 = 0; c0 < tot; c0 += 32) {
-        const int e = c0 + lane;
-        const int owner = warp_owner(excl, min(e, tot - 1));
-        const int uj = __shfl_sync(kFull, u[r], owner);
-        const int ej = __shfl_sync(kFull, excl, owner);
-        if (e < tot) cout[cb + (unsigned)e] = make_int2(uj, e - ej);
-      }
-      cb += (unsigned)tot;
+  for (int r = 0; r < N; ++r)
+    if (found[r]) {
+      if (deg[r] > bd)
+        stg.b[ba++] = make_int2(u[r], deg[r]);
+      else
+        stg.q[qa++] = u[r];
     }
-  }
+  stg.nq += qtot;
+  stg.nb += btot;
+  __syncwarp();
   const unsigned b = warp_sum((unsigned)nbig);
   edges = warp_sum(edges);
   if (lane == 0) {
-    if (b) atomicAdd(&nxt->nbig, b);
-    if (edges) atomicAdd(&nxt->edges, edges);
+    if (b) atomicAdd(blk_nbig + jid, b);
+    if (edges) atomicAdd(blk_edges + jid, edges);
   }
+}
+
+// What a unit needs to append: the warp's stage and the block's tallies.
+struct AppendCtx {
+  JobStage *stg;
+  unsigned *blk_nbig;
+  unsigned long long *blk_edges;
+  int jid;
+};
+
+template <int N>
+__device__ __forceinline__ void append_n(BatchJob *j, const bool (&found)[N], const int (&u)[N],
+                                         const int (&deg)[N], const AppendCtx &ac) {
+  append_n<N>(j, found, u, deg, *ac.stg, ac.blk_nbig, ac.blk_edges, ac.jid);
 }
 
 // ------------------------------------------------------------ MS-BFS ---
@@ -283,14 +357,14 @@ __device__ __forceinline__ void msbfs_relax_n(BatchJob *j, const unsigned long l
 }
 
 constexpr int kMsbfsUnroll = 4;  // edges per lane per batch
+static_assert(kMsbfsUnroll * 32 <= kJStageB && kMsbfsUnroll * 32 <= kJStageQ,
+              "an MS-BFS batch must fit a flushed stage");
 
 // 32 queued frontier vertices, edges dealt flat over the warp, 4 x 32 a batch
-__device__ void msbfs_push_queue(BatchJob *j, int L, int unit, unsigned nq) {
+__device__ void msbfs_push_queue(BatchJob *j, int L, int unit, unsigned nq, const AppendCtx &ac) {
   const int lane = lane_id();
-  int *qin = jobQ(j, L % 3), *qout = jobQ(j, (L + 1) % 3);
-  int2 *cout = jobC(j, (L + 1) % 3);
+  int *qin = jobQ(j, L % 3);
   unsigned long long *Fc = jobF(j, L % 3), *Fn = jobF(j, (L + 1) % 3);
-  JobCounters *nxt = &j->c[(L + 1) % 3];
   unsigned idx = (unsigned)unit * 32u + lane;
   int v = idx < nq ? __ldcg(qin + idx) : -1;
   int s = 0, d = 0;
@@ -320,17 +394,15 @@ __device__ void msbfs_push_queue(BatchJob *j, int L, int unit, unsigned nq) {
 #pragma unroll
     for (int r = 0; r < kMsbfsUnroll; ++r)
       dg[r] = found[r] ? __ldg(j->ptr + u[r] + 1) - __ldg(j->ptr + u[r]) : 0;
-    append_n<kMsbfsUnroll>(j, found, u, dg, qout, cout, nxt);
+    append_n<kMsbfsUnroll>(j, found, u, dg, ac);
   }
 }
 
 // one kChunk-edge chunk of a hub, 4 x 32 edges a batch
-__device__ void msbfs_push_chunk(BatchJob *j, int L, int unit) {
+__device__ void msbfs_push_chunk(BatchJob *j, int L, int unit, const AppendCtx &ac) {
   const int lane = lane_id();
-  int2 *cin = jobC(j, L % 3), *cout = jobC(j, (L + 1) % 3);
-  int *qout = jobQ(j, (L + 1) % 3);
+  int2 *cin = jobC(j, L % 3);
   unsigned long long *Fc = jobF(j, L % 3), *Fn = jobF(j, (L + 1) % 3);
-  JobCounters *nxt = &j->c[(L + 1) % 3];
   int2 ch = __ldcg(cin + unit);
   int s = __ldg(j->ptr + ch.x) + ch.y * kChunk;
   int e = min(s + kChunk, __ldg(j->ptr + ch.x + 1));
@@ -349,7 +421,7 @@ __device__ void msbfs_push_chunk(BatchJob *j, int L, int unit) {
 #pragma unroll
     for (int r = 0; r < kMsbfsUnroll; ++r)
       dg[r] = found[r] ? __ldg(j->ptr + u[r] + 1) - __ldg(j->ptr + u[r]) : 0;
-    append_n<kMsbfsUnroll>(j, found, u, dg, qout, cout, nxt);
+    append_n<kMsbfsUnroll>(j, found, u, dg, ac);
   }
 }
 
@@ -357,14 +429,11 @@ __device__ void msbfs_push_chunk(BatchJob *j, int L, int unit) {
 // in-neighbours (round-robin over the warp) until every source still missing
 // at the vertex is covered or the list ends
 __device__ void msbfs_pull(BatchJob *j, int L, int unit, unsigned long long *s_acc,
-                           int *s_rank) {
+                           int *s_rank, const AppendCtx &ac) {
   const int lane = lane_id();
   const int m = j->m;
   const unsigned long long all = srcmask(j->nsrc);
   unsigned long long *Fc = jobF(j, L % 3), *Fn = jobF(j, (L + 1) % 3);
-  int *qout = jobQ(j, (L + 1) % 3);
-  int2 *cout = jobC(j, (L + 1) % 3);
-  JobCounters *nxt = &j->c[(L + 1) % 3];
   int v = unit * 32 + lane;
   int s = 0, e = 0;
   unsigned long long want = 0;
@@ -412,7 +481,7 @@ __device__ void msbfs_pull(BatchJob *j, int L, int unit, unsigned long long *s_a
     for (unsigned long long b = nb; b; b &= b - 1) row[__ffsll((long long)b) - 1] = L + 1;
     dg[0] = __ldg(j->ptr + v + 1) - __ldg(j->ptr + v);
   }
-  append_n<1>(j, found, u, dg, qout, cout, nxt);
+  append_n<1>(j, found, u, dg, ac);
   __syncwarp();
 }
 
@@ -492,12 +561,10 @@ __device__ __forceinline__ bool mssp_relax(BatchJob *j, int ue, unsigned we, int
 }
 
 // kSsspPerUnit queued vertices: their edges laid out flat, a batch at a time
-__device__ void mssp_queue(BatchJob *j, int L, int unit, unsigned nq) {
+__device__ void mssp_queue(BatchJob *j, int L, int unit, unsigned nq, const AppendCtx &ac) {
   const int lane = lane_id();
-  int *qin = jobQ(j, L % 3), *qout = jobQ(j, (L + 1) % 3);
-  int2 *cout = jobC(j, (L + 1) % 3);
+  int *qin = jobQ(j, L % 3);
   unsigned long long *Fc = jobF(j, L % 3), *Fn = jobF(j, (L + 1) % 3);
-  JobCounters *nxt = &j->c[(L + 1) % 3];
   const int nb = mssp_batch(j->sw);
   const unsigned idx = (unsigned)unit * kSsspPerUnit + (unsigned)lane;
   int v = -1, s = 0, d = 0;
@@ -527,17 +594,15 @@ __device__ void mssp_queue(BatchJob *j, int L, int unit, unsigned nq) {
     bool f[1] = {mssp_relax(j, ue, we, ve, me, Fn)};
     int u1[1] = {ue}, dg[1] = {0};
     if (f[0]) dg[0] = __ldg(j->ptr + ue + 1) - __ldg(j->ptr + ue);
-    append_n<1>(j, f, u1, dg, qout, cout, nxt);
+    append_n<1>(j, f, u1, dg, ac);
   }
 }
 
 // one kSsspChunk-edge chunk of a hub
-__device__ void mssp_chunk(BatchJob *j, int L, int unit) {
+__device__ void mssp_chunk(BatchJob *j, int L, int unit, const AppendCtx &ac) {
   const int lane = lane_id();
-  int2 *cin = jobC(j, L % 3), *cout = jobC(j, (L + 1) % 3);
-  int *qout = jobQ(j, (L + 1) % 3);
+  int2 *cin = jobC(j, L % 3);
   unsigned long long *Fc = jobF(j, L % 3), *Fn = jobF(j, (L + 1) % 3);
-  JobCounters *nxt = &j->c[(L + 1) % 3];
   const int2 ch = __ldcg(cin + unit);
   const int v = ch.x;
   const int s = __ldg(j->ptr + v) + ch.y * kSsspChunk;
@@ -556,7 +621,7 @@ __device__ void mssp_chunk(BatchJob *j, int L, int unit) {
     bool f[1] = {mssp_relax(j, ue, we, v, me, Fn)};
     int u1[1] = {ue}, dg[1] = {0};
     if (f[0]) dg[0] = __ldg(j->ptr + ue + 1) - __ldg(j->ptr + ue);
-    append_n<1>(j, f, u1, dg, qout, cout, nxt);
+    append_n<1>(j, f, u1, dg, ac);
   }
 }
 
@@ -619,15 +684,12 @@ __device__ __forceinline__ unsigned mssp_pull_min(const BatchJob *j, int a0, int
 // hub's other chunks run elsewhere) or kMsPullVerts vertices, each taken
 // by the whole warp and written by it alone (no atomics).  Improved
 // vertices get their next-frontier bits and are queued, as in a push step.
-__device__ void mssp_pull(BatchJob *j, int L, int unit) {
+__device__ void mssp_pull(BatchJob *j, int L, int unit, const AppendCtx &ac) {
   const int lane = lane_id();
   const int sw = j->sw;
   unsigned *dist = reinterpret_cast<unsigned *>(j->out);
   const unsigned long long *Fc = jobF(j, L % 3);
   unsigned long long *Fn = jobF(j, (L + 1) % 3);
-  int *qout = jobQ(j, (L + 1) % 3);
-  int2 *cout = jobC(j, (L + 1) % 3);
-  JobCounters *nxt = &j->c[(L + 1) % 3];
   const unsigned low = sw == 32 ? 0xffffffffu : ((1u << sw) - 1u);
   const bool mine = lane < sw && lane < j->nsrc;  // this lane's source after the reduction
   if ((unsigned)unit < j->nhc) {
@@ -646,7 +708,7 @@ __device__ void mssp_pull(BatchJob *j, int L, int unit) {
     if (lane == 0 && b) f[0] = atomicOr(Fn + v, (unsigned long long)b) == 0ull;
     int u1[1] = {v}, dg[1] = {0};
     if (f[0]) dg[0] = __ldg(j->ptr + v + 1) - __ldg(j->ptr + v);
-    append_n<1>(j, f, u1, dg, qout, cout, nxt);
+    append_n<1>(j, f, u1, dg, ac);
     return;
   }
   const int v0 = (unit - (int)j->nhc) * kMsPullVerts;
@@ -666,7 +728,7 @@ __device__ void mssp_pull(BatchJob *j, int L, int unit) {
     if (f[0]) Fn[v] = (unsigned long long)b;
     int u1[1] = {v}, dg[1] = {0};
     if (f[0]) dg[0] = __ldg(j->ptr + v + 1) - __ldg(j->ptr + v);
-    append_n<1>(j, f, u1, dg, qout, cout, nxt);
+    append_n<1>(j, f, u1, dg, ac);
   }
 }
 
@@ -685,6 +747,12 @@ batch_persistent(BatchJob *jobs, int njobs, BatchState *st, int max_steps) {
   __shared__ unsigned s_pre[kMaxJobs + 1];
   __shared__ unsigned long long s_acc[kBatchThreads / 32][32];
   __shared__ int s_rank[kBatchThreads / 32][32];
+  // appends: per-warp stages, per-block tallies of the next frontiers
+  __shared__ int s_stq[kStageWarpsB][kJStageQ];
+  __shared__ int2 s_stb[kStageWarpsB][kJStageB];
+  __shared__ unsigned s_nbig_next[kMaxJobs];
+  __shared__ unsigned long long s_edges_next[kMaxJobs];
+  JobStage stg{s_stq[warp], s_stb[warp], 0, 0, nullptr, 0};
 
   for (int jj = threadIdx.x; jj < njobs; jj += blockDim.x) {
     s_explored[jj] = 0;
@@ -744,8 +812,12 @@ batch_persistent(BatchJob *jobs, int njobs, BatchState *st, int max_steps) {
       s_u1[jj] = u1;
       s_u2[jj] = u2;
       s_u3[jj] = u3;
+      s_nbig_next[jj] = 0;
+      s_edges_next[jj] = 0;
     }
     __syncthreads();
+    stg.level = step;
+    stg.job = nullptr;
     // exclusive prefix of the jobs' unit counts (warp 0; at most 64 jobs)
     if (warp == 0) {
       const int lane = lane_id();
@@ -771,6 +843,7 @@ batch_persistent(BatchJob *jobs, int njobs, BatchState *st, int max_steps) {
       // skip empty jobs that share the same prefix
       while (lo + 1 < njobs && s_pre[lo + 1] <= g) ++lo;
       BatchJob *j = jobs + lo;
+      const AppendCtx ac{&stg, s_nbig_next, s_edges_next, lo};
       unsigned loc = g - s_pre[lo];
       if (loc < s_u0[lo]) {
         msbfs_clear(j, step, (int)loc, s_prevq[lo], false);
@@ -784,24 +857,28 @@ batch_persistent(BatchJob *jobs, int njobs, BatchState *st, int max_steps) {
       loc -= s_u1[lo];
       if (j->type == kJobBfs) {
         if (s_pull[lo]) {
-          msbfs_pull(j, step, (int)loc, s_acc[warp], s_rank[warp]);
+          msbfs_pull(j, step, (int)loc, s_acc[warp], s_rank[warp], ac);
         } else if (loc < s_u2[lo]) {
-          msbfs_push_queue(j, step, (int)loc, s_q[lo]);
+          msbfs_push_queue(j, step, (int)loc, s_q[lo], ac);
         } else {
-          msbfs_push_chunk(j, step, (int)(loc - s_u2[lo]));
+          msbfs_push_chunk(j, step, (int)(loc - s_u2[lo]), ac);
         }
       } else if (s_pull[lo]) {
-        mssp_pull(j, step, (int)loc);
+        mssp_pull(j, step, (int)loc, ac);
       } else {
         if (loc < s_u2[lo])
-          mssp_queue(j, step, (int)loc, s_q[lo]);
+          mssp_queue(j, step, (int)loc, s_q[lo], ac);
         else
-          mssp_chunk(j, step, (int)(loc - s_u2[lo]));
+          mssp_chunk(j, step, (int)(loc - s_u2[lo]), ac);
       }
     }
+    stage_flush(stg);
     __syncthreads();
     if (threadIdx.x < njobs) {
       const int jj = threadIdx.x;
+      JobCounters *nx = &jobs[jj].c[(step + 1) % 3];
+      if (s_nbig_next[jj]) atomicAdd(&nx->nbig, s_nbig_next[jj]);
+      if (s_edges_next[jj]) atomicAdd(&nx->edges, s_edges_next[jj]);
       // the frontier of this step is cleared two steps later
       const bool was_active = s_u2[jj] + s_u3[jj] > 0;
       s_prevq[jj] = was_active ? s_q[jj] : 0;

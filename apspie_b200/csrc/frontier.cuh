@@ -185,6 +185,8 @@ __device__ __forceinline__ void append_plain(const bool (&f)[N], const int (&u)[
 constexpr int kStageWarps = 16;  // warps per block of the kernels that call expand_push
 constexpr int kStageQ = 256;     // queue entries per warp (>= kUnroll * 32)
 constexpr int kStageB = 128;     // big-list entries per warp (>= kUnroll * 32)
+static_assert(kStageQ >= kUnroll * 32 && kStageB >= kUnroll * 32,
+              "a batch of joiners must fit a flushed stage");
 
 struct WarpStage {
   int *q;
