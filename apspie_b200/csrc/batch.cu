@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -929,17 +930,34 @@ size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 // batch while the rest of the GPU idles).
 constexpr int kDeepLevels = 64;
 
-// BFS levels of graph J from its first vertex with edges, cached in the
-// context by the graph's fingerprint (one probe BFS per new graph).
+// BFS levels of graph J from its first vertex with edges (one probe BFS per
+// graph), cached for the whole process by (device, row-offset pointer, m,
+// nnz): every context and sub-context reads the same entry without touching
+// the device.  The depth only routes a job (multi-source launch or
+// concurrent single-source traversals); either route gives the same
+// results, so a stale entry (a graph freed and another of the same size
+// built at the same address) can only cost time.
+struct DepthEntry {
+  int dev;
+  const int *ptr;
+  int m;
+  long long nnz;
+  int levels;
+};
+std::mutex g_depth_mu;
+std::vector<DepthEntry> g_depth_cache;
+
 int graph_levels(apspie_context *ctx, const apspie_job &J, int *levels) {
   *levels = 0;
   if (J.nnz == 0) return APSPIE_OK;
-  const uint64_t fp = graph_fingerprint(ctx, J.m, J.nnz, J.d_ptr);
-  for (const auto &e : ctx->depth_cache)
-    if (e.fp == fp) {
-      *levels = e.levels;
-      return APSPIE_OK;
-    }
+  {
+    std::lock_guard<std::mutex> lock(g_depth_mu);
+    for (const auto &e : g_depth_cache)
+      if (e.dev == ctx->device && e.ptr == J.d_ptr && e.m == J.m && e.nnz == J.nnz) {
+        *levels = e.levels;
+        return APSPIE_OK;
+      }
+  }
   const int nh = std::min(J.m, 4096);
   int *h = (int *)pinned(ctx, sizeof(int) * (nh + 1));
   if (!h) return APSPIE_ERR_OOM;
@@ -961,7 +979,8 @@ int graph_levels(apspie_context *ctx, const apspie_job &J, int *levels) {
     if (rc) return rc;
     lv = bs.levels;
   }
-  ctx->depth_cache.push_back(apspie_context::DepthEntry{fp, lv});
+  std::lock_guard<std::mutex> lock(g_depth_mu);
+  g_depth_cache.push_back(DepthEntry{ctx->device, J.d_ptr, J.m, (long long)J.nnz, lv});
   *levels = lv;
   return APSPIE_OK;
 }
@@ -1162,12 +1181,11 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
     auto *djobs = (BatchJob *)ws;
     auto *dstate = (BatchState *)(ws + align_up(sizeof(BatchJob) * kMaxJobs));
     int *dsrc = (int *)(ws + align_up(sizeof(BatchJob) * kMaxJobs) + align_up(sizeof(BatchState)));
-    // host image of the job table (pinned, copied in one transfer); earlier
-    // copies out of the pinned buffer must have completed before it is reused
-    rc = check_cuda(ctx, cudaStreamSynchronize(st), "apspie_batch_run");
-    if (rc) return rc;
+    // host image of the job table (pinned, copied in one transfer), in a
+    // ring of upload buffers: no wait for the stream's earlier kernels
     size_t host_bytes = sizeof(BatchJob) * nparts + sizeof(int) * 64 * nparts;
-    auto *hjobs = (BatchJob *)pinned(ctx, host_bytes);
+    int up_slot = 0;
+    auto *hjobs = (BatchJob *)upload_buffer(ctx, host_bytes, &up_slot);
     if (!hjobs) return APSPIE_ERR_OOM;
     int *hsrc = (int *)(hjobs + nparts);
     for (int p = 0; p < nparts; ++p) {
@@ -1220,6 +1238,8 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
     }
     cudaMemcpyAsync(djobs, hjobs, host_bytes, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(dsrc, hsrc, sizeof(int) * 64 * nparts, cudaMemcpyHostToDevice, st);
+    rc = upload_done(ctx, up_slot);
+    if (rc) return rc;
     cudaMemsetAsync(dstate, 0, align_up(sizeof(BatchState)), st);
     rc = check_cuda(ctx, cudaGetLastError(), "apspie_batch_run upload");
     if (rc) return rc;

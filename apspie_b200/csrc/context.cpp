@@ -97,6 +97,41 @@ uint64_t graph_fingerprint(apspie_context *ctx, int m, int64_t nnz, const int *d
   return f;
 }
 
+void *upload_buffer(apspie_context *ctx, size_t bytes, int *slot) {
+  const int k = ctx->up_next;
+  ctx->up_next = (k + 1) % apspie_context::kUploadRing;
+  if (ctx->up_done[k]) {
+    // the copy that last read this buffer
+    cudaError_t e = cudaEventSynchronize(ctx->up_done[k]);
+    if (e != cudaSuccess) {
+      check_cuda(ctx, e, "upload buffer");
+      return nullptr;
+    }
+  } else if (cudaEventCreateWithFlags(&ctx->up_done[k], cudaEventDisableTiming) != cudaSuccess) {
+    check_cuda(ctx, cudaGetLastError(), "upload buffer event");
+    return nullptr;
+  }
+  if (ctx->up_bytes[k] < bytes) {
+    if (ctx->up_host[k]) cudaFreeHost(ctx->up_host[k]);
+    ctx->up_host[k] = nullptr;
+    ctx->up_bytes[k] = 0;
+    const size_t want = bytes < 4096 ? 4096 : bytes;
+    if (cudaMallocHost(&ctx->up_host[k], want) != cudaSuccess) {
+      cudaGetLastError();
+      ctx->up_host[k] = nullptr;
+      set_error(ctx, APSPIE_ERR_OOM, "cudaMallocHost(%zu) failed", want);
+      return nullptr;
+    }
+    ctx->up_bytes[k] = want;
+  }
+  *slot = k;
+  return ctx->up_host[k];
+}
+
+int upload_done(apspie_context *ctx, int slot) {
+  return check_cuda(ctx, cudaEventRecord(ctx->up_done[slot], ctx->stream), "upload event");
+}
+
 }  // namespace apspie
 
 extern "C" {
@@ -133,6 +168,10 @@ int apspie_ctx_destroy(apspie_ctx ctx) {
   for (auto &s : ctx->slots)
     if (s.ptr) cudaFree(s.ptr);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  for (int k = 0; k < apspie_context::kUploadRing; ++k) {
+    if (ctx->up_host[k]) cudaFreeHost(ctx->up_host[k]);
+    if (ctx->up_done[k]) cudaEventDestroy(ctx->up_done[k]);
+  }
   if (ctx->owns_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return APSPIE_OK;

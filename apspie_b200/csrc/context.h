@@ -29,6 +29,15 @@ struct apspie_context {
   // pinned host scratch for small device->host reads
   void *pinned = nullptr;
   size_t pinned_bytes = 0;
+  // ring of pinned host buffers for tables uploaded to the device (the
+  // batched job table): a buffer is reused once the copy that last read it
+  // has completed (its event), so a call need not wait for the stream's
+  // earlier kernels
+  static constexpr int kUploadRing = 4;
+  void *up_host[kUploadRing] = {};
+  size_t up_bytes[kUploadRing] = {};
+  cudaEvent_t up_done[kUploadRing] = {};
+  int up_next = 0;
 
   // at most this many blocks per persistent launch (0: as many as fit), so
   // that two persistent kernels can share the GPU
@@ -55,8 +64,7 @@ struct apspie_context {
   // single-source traversals on sub-contexts (own stream and workspace),
   // concurrently, with deep_blocks blocks in all (0: two thirds of the
   // resident ones when multi-source jobs run next to them); aux_done orders
-  // their start after the context's stream; traversal depth of graphs seen
-  // before, by fingerprint
+  // their start after the context's stream
   int batch_deep_subs = 48;  // most concurrent single-source traversals (0: none)
   int deep_blocks = 0;
   cudaEvent_t aux_done = nullptr;
@@ -64,11 +72,6 @@ struct apspie_context {
   std::vector<cudaEvent_t> sub_done;
   int batch_subs_used = 0;  // sub-contexts the last batch ran sources on
   bool owns_stream = false;  // a sub-context's stream, destroyed with it
-  struct DepthEntry {
-    uint64_t fp;
-    int levels;
-  };
-  std::vector<DepthEntry> depth_cache;
   // SpGEMM plan left by apspie_spgemm_symbolic for apspie_spgemm_numeric
   bool spgemm_plan_valid = false;
   const void *spgemm_plan_A = nullptr, *spgemm_plan_B = nullptr;
@@ -143,6 +146,12 @@ int set_error(apspie_context *ctx, int status, const char *fmt, ...);
 void *workspace(apspie_context *ctx, int id, size_t bytes);
 // Pinned host buffer of at least `bytes`.
 void *pinned(apspie_context *ctx, size_t bytes);
+// A pinned host buffer of at least `bytes` for a host-to-device upload and
+// its slot: fill it, enqueue the copy, then upload_done(ctx, slot) records
+// the copy's completion.  Waits only for the copy that used the buffer
+// kUploadRing uploads ago.
+void *upload_buffer(apspie_context *ctx, size_t bytes, int *slot);
+int upload_done(apspie_context *ctx, int slot);
 // Checks cudaGetLastError after launches; records the launch count.
 int check_launch(apspie_context *ctx, const char *what, int nlaunches = 1);
 int check_cuda(apspie_context *ctx, cudaError_t e, const char *what);

@@ -10,8 +10,10 @@
 //     arrival order until the budget allows them in;
 //   * coalescing: the admitted BFS and SSSP queries of one (graph, kind) form
 //     a group, run by ONE apspie_batch_run (multi-source frontier matrix), or
-//     by the single-source kernel when the group has one query; an MIS query
-//     is a group of its own.  Groups are launched cheapest first
+//     by the single-source kernel when the group has one query (or, on the
+//     largest graphs, fewer than the group size from which the batch pays);
+//     the MIS queries of one (graph, seed) are one computation whose
+//     membership row is copied to each of them.  Groups are launched cheapest first
 //     (measured time per group, kept per graph and kind), and each group has
 //     its own completion event, so a quick query is not held back by a slow
 //     one of the same batch;
@@ -91,13 +93,16 @@ struct GraphEntry {
   const uint32_t *stw = nullptr;
 };
 
-// SSSP groups of fewer than kSsspBatchMinGroup queries on graphs with more
-// edges than kSsspBatchMaxNnz run their queries one by one through the
-// single-source kernel: on R-MAT 22 the multi-source rows share little
-// (8 sources: 44 ms batched, 37 ms one by one with pull rounds; 16: 59 vs
-// 75 ms; 32: 92 vs 152 ms, measured), while on smaller graphs the batch wins.
-constexpr int64_t kSsspBatchMaxNnz = 64ll << 20;
-constexpr size_t kSsspBatchMinGroup = 12;
+// On graphs with more edges than kLargeNnz, BFS and SSSP groups smaller
+// than these run their queries one by one through the single-source
+// kernels: the multi-source launch shares little there (measured, time per
+// query against one by one: R-MAT 23 BFS 0.72x at 8 sources, 1.29x at 16,
+// 2.9x at 64; SSSP 0.93 - 0.98x at 4 - 8, 1.16x at 16, 1.24x at 32; R-MAT 22
+// BFS 1.5x from 8 sources, SSSP 1.09x at 8 - 16), while on smaller graphs
+// the batch wins from two queries on.
+constexpr int64_t kLargeNnz = 64ll << 20;
+constexpr size_t kBfsBatchMinGroup = 12;
+constexpr size_t kSsspBatchMinGroup = 16;
 
 // One SSSP query through the single-source kernel, push/pull when the
 // graph's in-adjacency with weights was registered.
@@ -112,6 +117,7 @@ struct Group {
   int kind = 0, graph = 0, lane = 0;
   std::vector<Request *> reqs;
   cudaEvent_t start = nullptr, end = nullptr;
+  cudaEvent_t computed = nullptr;  // the traversal's end, which the copies wait for
   int status = APSPIE_OK;
   bool done = false;
 };
@@ -119,6 +125,9 @@ struct Group {
 struct Lane {
   apspie_ctx ctx = nullptr;
   cudaStream_t stream = nullptr;
+  // result copies: on a stream of their own behind each group's traversal,
+  // so the copy engines move a group's rows while the next group computes
+  cudaStream_t copy = nullptr;
 };
 
 struct Slot {
@@ -128,7 +137,7 @@ struct Slot {
   void *h_stage = nullptr;
   size_t h_bytes = 0;
   std::vector<Group> groups;
-  std::vector<cudaEvent_t> events;  // pool, two per group
+  std::vector<cudaEvent_t> events;  // pool, three per group
   bool busy = false;
 };
 
@@ -149,10 +158,19 @@ struct apspie_server {
   bool stop = false;
   Slot slots[2];
   bool any_deep = false;
+  bool warming = false;  // add_graph is warming the lanes: the worker launches nothing
   int max_pending = 1 << 20;
   // MIS priorities per (graph, seed), on the device
   std::mutex prio_mu;
   std::map<std::pair<int, uint32_t>, uint32_t *> prio_cache;
+  // the plain one-query-at-a-time path of apspie_server_replay_plain: its
+  // own stream, context and result rows, kept across calls so a warm-up
+  // replay leaves them warm, as the server's lanes are
+  cudaStream_t plain_stream = nullptr;
+  apspie_ctx plain_ctx = nullptr;
+  int32_t *plain_row = nullptr;
+  void *plain_hrow = nullptr;
+  size_t plain_m = 0;
   // statistics
   uint64_t batches = 0, completed = 0, launched_jobs = 0;
   std::vector<double> latencies;
@@ -174,12 +192,15 @@ size_t request_bytes(const apspie_server *s, int type, int graph) {
   }
 }
 
+// Grows a buffer at least twofold (freeing one synchronises the device, so
+// growth should be rare).
 bool ensure_device(void **p, size_t *have, size_t want) {
   if (*have >= want) return true;
+  const size_t prev = *have;
   if (*p) cudaFree(*p);
   *p = nullptr;
   *have = 0;
-  size_t w = std::max<size_t>(want, 1 << 20);
+  size_t w = std::max<size_t>({want, 2 * prev, (size_t)1 << 20});
   if (cudaMalloc(p, w) != cudaSuccess) {
     cudaGetLastError();
     return false;
@@ -190,10 +211,11 @@ bool ensure_device(void **p, size_t *have, size_t want) {
 
 bool ensure_host(void **p, size_t *have, size_t want) {
   if (*have >= want) return true;
+  const size_t prev = *have;
   if (*p) cudaFreeHost(*p);
   *p = nullptr;
   *have = 0;
-  size_t w = std::max<size_t>(want, 1 << 20);
+  size_t w = std::max<size_t>({want, 2 * prev, (size_t)1 << 20});
   if (cudaMallocHost(p, w) != cudaSuccess) {
     cudaGetLastError();
     return false;
@@ -331,12 +353,17 @@ int launch_group(apspie_server *s, Slot &sl, Group &g) {
   int st = APSPIE_OK;
   const size_t row = 4 * (size_t)ge.m;
   if (g.kind == 2) {
+    // identical queries (same graph and seed): computed once
     Request *r = g.reqs.front();
     uint32_t *prio = nullptr;
     st = get_prio(s, g.graph, r->seed, ln.stream, &prio);
     if (st == APSPIE_OK)
       st = apspie_mis(ln.ctx, ge.nnz, ge.m, ge.ptr, ge.ind, prio,
                       (int32_t *)((char *)sl.d_out + r->dev_off), 1.0f);
+    for (size_t i = 1; i < g.reqs.size() && st == APSPIE_OK; ++i)
+      if (cudaMemcpyAsync((char *)sl.d_out + g.reqs[i]->dev_off, (char *)sl.d_out + r->dev_off,
+                          row, cudaMemcpyDeviceToDevice, ln.stream) != cudaSuccess)
+        st = APSPIE_ERR_CUDA;
   } else if (g.reqs.size() == 1) {
     // one source: the single-source kernels are the faster path
     Request *r = g.reqs.front();
@@ -348,9 +375,14 @@ int launch_group(apspie_server *s, Slot &sl, Group &g) {
     } else {
       st = sssp_one(ln.ctx, ge, r->source, (uint32_t *)out);
     }
-  } else if (g.kind == 1 && ge.nnz > kSsspBatchMaxNnz && g.reqs.size() < kSsspBatchMinGroup) {
+  } else if (ge.nnz > kLargeNnz &&
+             g.reqs.size() < (g.kind == 1 ? kSsspBatchMinGroup : kBfsBatchMinGroup)) {
+    const int *tp = ge.tptr ? ge.tptr : (ge.symmetric ? ge.ptr : nullptr);
+    const int *ti = ge.tptr ? ge.tind : (ge.symmetric ? ge.ind : nullptr);
     for (Request *r : g.reqs) {
-      st = sssp_one(ln.ctx, ge, r->source, (uint32_t *)((char *)sl.d_out + r->dev_off));
+      int32_t *out = (int32_t *)((char *)sl.d_out + r->dev_off);
+      st = g.kind == 1 ? sssp_one(ln.ctx, ge, r->source, (uint32_t *)out)
+                       : apspie_bfs(ln.ctx, r->source, ge.nnz, ge.m, ge.ptr, ge.ind, tp, ti, out, 0);
       if (st != APSPIE_OK) break;
     }
   } else {
@@ -378,20 +410,23 @@ int launch_group(apspie_server *s, Slot &sl, Group &g) {
     st = apspie_batch_run(ln.ctx, 1, &j, 0);
     ++s->launched_jobs;
   }
-  // results to the callers: host rows through the staging buffer, device
-  // rows directly; a query with neither only has its latency recorded
+  // results to the callers, on the lane's copy stream once the traversal
+  // is done: host rows through the staging buffer, device rows directly; a
+  // query with neither only has its latency recorded
+  cudaEventRecord(g.computed, ln.stream);
+  cudaStreamWaitEvent(ln.copy, g.computed, 0);
   for (Request *r : g.reqs) {
     if (st != APSPIE_OK) break;
     cudaError_t e = cudaSuccess;
     if (r->h_result || r->to_stage)
       e = cudaMemcpyAsync((char *)sl.h_stage + r->host_off, (char *)sl.d_out + r->dev_off, row,
-                          cudaMemcpyDeviceToHost, ln.stream);
+                          cudaMemcpyDeviceToHost, ln.copy);
     if (e == cudaSuccess && r->d_result)
       e = cudaMemcpyAsync(r->d_result, (char *)sl.d_out + r->dev_off, row,
-                          cudaMemcpyDeviceToDevice, ln.stream);
+                          cudaMemcpyDeviceToDevice, ln.copy);
     if (e != cudaSuccess) st = APSPIE_ERR_CUDA;
   }
-  cudaEventRecord(g.end, ln.stream);
+  cudaEventRecord(g.end, ln.copy);
   return st;
 }
 
@@ -405,9 +440,18 @@ void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
     apspie_ctx_set_max_grid(sl.lane[0].ctx, s->any_deep ? std::max(1, resident - resident / 4) : 0);
   }
   std::map<std::pair<int, int>, size_t> index;
+  std::map<std::pair<int, uint32_t>, size_t> mis_index;
   sl.groups.clear();
   for (Request *r : batch) {
     if (r->type == 2) {
+      // MIS queries of one graph and seed are the same query: one group
+      auto key = std::make_pair(r->graph, r->seed);
+      auto it = mis_index.find(key);
+      if (it != mis_index.end()) {
+        sl.groups[it->second].reqs.push_back(r);
+        continue;
+      }
+      mis_index[key] = sl.groups.size();
       sl.groups.emplace_back();
       sl.groups.back().kind = 2;
       sl.groups.back().graph = r->graph;
@@ -453,7 +497,7 @@ void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
     for (Request *r : g.reqs)
       if (!r->h_result && r->to_stage) r->host_off = host;
   host += sink;
-  while (sl.events.size() < 2 * sl.groups.size()) {
+  while (sl.events.size() < 3 * sl.groups.size()) {
     cudaEvent_t e = nullptr;
     if (cudaEventCreate(&e) != cudaSuccess) {
       cudaGetLastError();
@@ -461,7 +505,7 @@ void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
     }
     sl.events.push_back(e);
   }
-  const bool buffers = sl.events.size() >= 2 * sl.groups.size() &&
+  const bool buffers = sl.events.size() >= 3 * sl.groups.size() &&
                        ensure_device((void **)&sl.d_out, &sl.d_bytes, dev) &&
                        (host == 0 || ensure_host(&sl.h_stage, &sl.h_bytes, host));
   for (size_t i = 0; i < sl.groups.size(); ++i) {
@@ -470,8 +514,9 @@ void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
       g.status = APSPIE_ERR_OOM;
       continue;
     }
-    g.start = sl.events[2 * i];
-    g.end = sl.events[2 * i + 1];
+    g.start = sl.events[3 * i];
+    g.end = sl.events[3 * i + 1];
+    g.computed = sl.events[3 * i + 2];
     g.status = launch_group(s, sl, g);
   }
   if (!buffers) {
@@ -537,7 +582,7 @@ void worker_main(apspie_server *s) {
       std::unique_lock<std::mutex> lock(s->mu);
       const bool any_busy = s->slots[0].busy || s->slots[1].busy;
       if (s->stop && s->pending.empty() && !any_busy) return;
-      if (s->pending.empty()) {
+      if (s->pending.empty() || s->warming) {
         s->cv.wait_for(lock, std::chrono::microseconds(any_busy ? 20 : 2000));
         continue;
       }
@@ -590,6 +635,7 @@ int apspie_server_create(int device, size_t state_budget_bytes, int max_batch,
     for (int l = 0; l < 2; ++l) {
       Lane &ln = sl.lane[l];
       if (cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaStreamCreateWithFlags(&ln.copy, cudaStreamNonBlocking) != cudaSuccess ||
           apspie_ctx_create(device, ln.stream, &ln.ctx) != APSPIE_OK) {
         cudaGetLastError();
         apspie_server_destroy(s);
@@ -609,6 +655,77 @@ int apspie_server_create(int device, size_t state_budget_bytes, int max_batch,
   return APSPIE_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The first query of a graph on a lane grows that lane's workspaces (and,
+// for a deep graph, creates its sub-contexts: one stream and workspace per
+// concurrent single-source traversal, up to 48); growing frees the old
+// buffer, which synchronises the device, and the first queries took
+// hundreds of ms.  A new graph is therefore run once on every lane that
+// will serve it, at add time: one query of each kind alone and the largest
+// groups (64 BFS, 32 SSSP sources; 48 each on a deep graph) -- only while
+// the server is idle, since a context serves one thread at a time.
+void warm_lanes(apspie_server *s, const GraphEntry &g) {
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (s->in_flight != 0 || !s->pending.empty() || s->slots[0].busy || s->slots[1].busy)
+      return;
+    s->warming = true;
+  }
+  const int kb = g.deep ? 48 : 64, ks = g.deep ? 48 : 32;
+  int32_t *out = nullptr;
+  uint32_t *prio = nullptr;
+  if (cudaMalloc(&out, sizeof(int32_t) * (size_t)g.m * kb) == cudaSuccess &&
+      cudaMalloc(&prio, sizeof(uint32_t) * (size_t)g.m) == cudaSuccess &&
+      cudaMemset(prio, 0, sizeof(uint32_t) * (size_t)g.m) == cudaSuccess) {
+    std::vector<int> src(kb);
+    for (int i = 0; i < kb; ++i) src[i] = (int)((int64_t)g.m * i / kb);
+    apspie_job jobs[2];
+    int nj = 0;
+    for (int kind = 0; kind < 2; ++kind) {
+      if (kind == 1 && !g.w) break;
+      apspie_job &j = jobs[nj++];
+      std::memset(&j, 0, sizeof(j));
+      j.type = kind == 0 ? APSPIE_JOB_BFS : APSPIE_JOB_SSSP_U32;
+      j.m = g.m;
+      j.nnz = g.nnz;
+      j.d_ptr = g.ptr;
+      j.d_ind = g.ind;
+      j.d_tptr = g.tptr;
+      j.d_tind = g.tind;
+      j.d_w = g.w;
+      j.symmetric = g.symmetric;
+      j.nsrc = kind == 0 ? kb : ks;
+      j.h_src = src.data();
+      j.d_out = out;
+      j.alpha = j.beta = -1;
+    }
+    const int *tp = g.tptr ? g.tptr : (g.symmetric ? g.ptr : nullptr);
+    const int *ti = g.tptr ? g.tind : (g.symmetric ? g.ind : nullptr);
+    for (Slot &sl : s->slots) {
+      Lane &ln = sl.lane[g.deep ? 1 : 0];
+      apspie_bfs(ln.ctx, src[0], g.nnz, g.m, g.ptr, g.ind, tp, ti, out, 0);
+      if (g.w) sssp_one(ln.ctx, g, src[0], (uint32_t *)out);
+      if (g.symmetric) apspie_mis(ln.ctx, g.nnz, g.m, g.ptr, g.ind, prio, out, 1.0f);
+      for (int i = 0; i < nj; ++i)
+        if (apspie_batch_run(ln.ctx, 1, &jobs[i], 0) != APSPIE_OK) break;
+      apspie_ctx_sync(ln.ctx);
+    }
+  }
+  cudaFree(out);
+  cudaFree(prio);
+  cudaGetLastError();
+  std::lock_guard<std::mutex> lock(s->mu);
+  s->warming = false;
+  s->cv.notify_all();
+}
+
+}  // namespace
+
+extern "C" {
+
 int apspie_server_add_graph(apspie_server_t s, int m, int64_t nnz, const int *d_ptr,
                             const int *d_ind, const int *d_tptr, const int *d_tind,
                             const uint32_t *d_w, int symmetric, int *graph_id) {
@@ -624,6 +741,7 @@ int apspie_server_add_graph(apspie_server_t s, int m, int64_t nnz, const int *d_
   g.cost_ms[0] = 1e-6f * (float)nnz * (g.deep ? 100.0f : 1.0f);
   g.cost_ms[1] = 4.0f * g.cost_ms[0];
   g.cost_ms[2] = 2.0f * g.cost_ms[0];
+  warm_lanes(s, g);
   std::lock_guard<std::mutex> lock(s->mu);
   s->graphs.push_back(g);
   if (g.deep) s->any_deep = true;
@@ -781,19 +899,34 @@ int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q, 
     for (const GraphEntry &g : s->graphs) maxm = std::max(maxm, g.m);
   }
   if (cudaSetDevice(s->device) != cudaSuccess) return APSPIE_ERR_CUDA;
-  cudaStream_t stream = nullptr;
-  apspie_ctx ctx = nullptr;
-  int32_t *row = nullptr;
-  void *h_row = nullptr;
-  if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc(&row, 4 * (size_t)std::max(maxm, 1)) != cudaSuccess ||
-      (to_host && cudaMallocHost(&h_row, 4 * (size_t)std::max(maxm, 1)) != cudaSuccess)) {
-    cudaGetLastError();
-    cudaFree(row);
-    if (stream) cudaStreamDestroy(stream);
-    return APSPIE_ERR_OOM;
+  int st = APSPIE_OK;
+  if (!s->plain_ctx) {
+    if (cudaStreamCreateWithFlags(&s->plain_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      s->plain_stream = nullptr;
+      return APSPIE_ERR_CUDA;
+    }
+    st = apspie_ctx_create(s->device, s->plain_stream, &s->plain_ctx);
+    if (st != APSPIE_OK) return st;
   }
-  int st = apspie_ctx_create(s->device, stream, &ctx);
+  if (s->plain_m < (size_t)std::max(maxm, 1)) {
+    cudaFree(s->plain_row);
+    if (s->plain_hrow) cudaFreeHost(s->plain_hrow);
+    s->plain_row = nullptr;
+    s->plain_hrow = nullptr;
+    s->plain_m = 0;
+    const size_t mm = (size_t)std::max(maxm, 1);
+    if (cudaMalloc(&s->plain_row, 4 * mm) != cudaSuccess ||
+        cudaMallocHost(&s->plain_hrow, 4 * mm) != cudaSuccess) {
+      cudaGetLastError();
+      return APSPIE_ERR_OOM;
+    }
+    s->plain_m = mm;
+  }
+  cudaStream_t stream = s->plain_stream;
+  apspie_ctx ctx = s->plain_ctx;
+  int32_t *row = s->plain_row;
+  void *h_row = s->plain_hrow;
   const Clock::time_point t0 = Clock::now() + std::chrono::milliseconds(1);
   double last = 0;
   for (int i = 0; i < n && st == APSPIE_OK; ++i) {
@@ -819,10 +952,6 @@ int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q, 
     lat_ms[i] = l;
     last = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
   }
-  if (ctx) apspie_ctx_destroy(ctx);
-  cudaFree(row);
-  if (h_row) cudaFreeHost(h_row);
-  cudaStreamDestroy(stream);
   if (wall_ms) *wall_ms = last;
   return st;
 }
@@ -902,13 +1031,19 @@ int apspie_server_destroy(apspie_server_t s) {
   for (Slot &sl : s->slots) {
     for (Lane &ln : sl.lane) {
       if (ln.stream) cudaStreamSynchronize(ln.stream);
+      if (ln.copy) cudaStreamSynchronize(ln.copy);
       if (ln.ctx) apspie_ctx_destroy(ln.ctx);
       if (ln.stream) cudaStreamDestroy(ln.stream);
+      if (ln.copy) cudaStreamDestroy(ln.copy);
     }
     for (cudaEvent_t e : sl.events) cudaEventDestroy(e);
     cudaFree(sl.d_out);
     if (sl.h_stage) cudaFreeHost(sl.h_stage);
   }
+  if (s->plain_ctx) apspie_ctx_destroy(s->plain_ctx);
+  if (s->plain_stream) cudaStreamDestroy(s->plain_stream);
+  cudaFree(s->plain_row);
+  if (s->plain_hrow) cudaFreeHost(s->plain_hrow);
   for (auto &kv : s->prio_cache) cudaFree(kv.second);
   for (auto &kv : s->reqs) delete kv.second;
   delete s;

@@ -358,8 +358,10 @@ int apspie_server_replay(apspie_server_t s, int n, const apspie_query *q,
 int apspie_server_replay_keep(apspie_server_t s, int n, const apspie_query *q, int to_host,
                               int32_t *const *d_keep, double *lat_ms, double *wall_ms);
 /* The same stream one query at a time, in arrival order, through
- * apspie_bfs / apspie_sssp_u32 / apspie_mis on a stream of its own (the
- * plain single-query path); latencies likewise from the arrival times. */
+ * apspie_bfs / apspie_sssp_u32 / apspie_mis on a stream and context of its
+ * own, kept by the server across calls (the plain single-query path);
+ * latencies likewise from the arrival times.  Not to be called from two
+ * threads at once. */
 int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q,
                                int to_host, double *lat_ms, double *wall_ms);
 /* *done = 1 once the result is in h_result (the request is then retired and
