@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 #include "context.h"
@@ -64,6 +65,9 @@ struct BfsState {
   // (the previous launch on the stream has finished, so nobody polls it).
   alignas(128) unsigned barp[2][2];
   alignas(128) int errp[2];
+  // test hook (apspie_debug_inject): set, the next launch's last block leaves
+  // before its first grid barrier; never cleared by the initialisation
+  int inject;
   unsigned long long reached;
   unsigned long long edges;
   unsigned long long t_start;
@@ -146,6 +150,13 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
   __shared__ unsigned long long s_bedg;
   __shared__ unsigned s_next;  // per-block group counter of pull / compaction sweeps
 
+  // test hook: the last block leaves at once (one-shot), so the others'
+  // first grid barrier waits out its bound and reports APSPIE_ERR_TIMEOUT
+  __shared__ int s_leave;
+  if (threadIdx.x == 0)
+    s_leave = (gridDim.x > 1 && blockIdx.x == gridDim.x - 1) ? atomicExch(&st->inject, 0) : 0;
+  __syncthreads();
+  if (s_leave) return;
   // init_par >= 0: the launch clears the state itself (no bfs_init before
   // it) and uses barrier counter set init_par
   unsigned *bar = init_par < 0 ? st->bar : st->barp[init_par];
@@ -584,45 +595,82 @@ constexpr size_t kNaBytes = kNaOffGm + align256(sizeof(unsigned) * (kNoAllocMaxV
 
 static __device__ __align__(256) unsigned char g_bfs_noalloc_scratch[kNaBytes];
 
-// Device address of the scratch array, looked up once per device.  In host
-// code g_bfs_noalloc_scratch names a host-side stand-in, never the device
-// memory, so it must not be passed to a kernel.
-constexpr int kNaMaxDevices = 64;
+// Device address of the scratch array, looked up once per CUDA context (a
+// __device__ array has an address per context: the device's primary
+// context, or one a caller made with the driver API; after cudaDeviceReset
+// the primary context is new).  In host code g_bfs_noalloc_scratch names a
+// host-side stand-in, never the device memory, so it must not be passed to
+// a kernel.
+struct NaEntry {
+  int dev;
+  void *cu_ctx;  // the CUcontext current at set-up
+  unsigned char *ptr;
+  int grid;
+};
 std::mutex g_na_mutex;
-unsigned char *g_na_ptr[kNaMaxDevices] = {};
-int g_na_grid[kNaMaxDevices] = {};
+std::vector<NaEntry> g_na_cache;
+
+// The current driver context (cuCtxGetCurrent through the runtime's
+// driver entry point, so the library needs no libcuda link); nullptr if
+// the entry point is unavailable.
+void *current_cu_ctx() {
+  using CtxGetCurrent = int (*)(void **);
+  static CtxGetCurrent fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (CtxGetCurrent)f;
+    cudaGetLastError();
+  });
+  void *c = nullptr;
+  if (fn && fn(&c) != 0) c = nullptr;
+  return c;
+}
 
 int noalloc_setup(int dev, unsigned char **ptr, int *grid) {
-  if (dev < 0 || dev >= kNaMaxDevices) return APSPIE_ERR_UNSUPPORTED;
+  void *cu = current_cu_ctx();
   std::lock_guard<std::mutex> lock(g_na_mutex);
-  if (!g_na_ptr[dev]) {
-    void *p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_bfs_noalloc_scratch) != cudaSuccess || !p) {
-      cudaGetLastError();
-      return APSPIE_ERR_CUDA;
+  for (const NaEntry &e : g_na_cache)
+    if (e.dev == dev && e.cu_ctx == cu) {
+      *ptr = e.ptr;
+      *grid = e.grid;
+      return APSPIE_OK;
     }
-    int occ = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bfs_persistent, kBfsThreads, 0) !=
-            cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        occ < 1) {
-      cudaGetLastError();
-      return APSPIE_ERR_CUDA;
-    }
-    g_na_grid[dev] = occ * sms;
-    g_na_ptr[dev] = (unsigned char *)p;
+  void *p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_bfs_noalloc_scratch) != cudaSuccess || !p) {
+    cudaGetLastError();
+    return APSPIE_ERR_CUDA;
   }
-  *ptr = g_na_ptr[dev];
-  *grid = g_na_grid[dev];
+  int occ = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bfs_persistent, kBfsThreads, 0) !=
+          cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      occ < 1) {
+    cudaGetLastError();
+    return APSPIE_ERR_CUDA;
+  }
+  g_na_cache.push_back(NaEntry{dev, cu, (unsigned char *)p, occ * sms});
+  *ptr = (unsigned char *)p;
+  *grid = occ * sms;
   return APSPIE_OK;
 }
+
+// Copies the run's status word (0 or APSPIE_ERR_TIMEOUT) to the caller.
+__global__ void bfs_write_status(const BfsState *st, int32_t *out) {
+  *out = *(const volatile int *)&st->err;
+}
+
+__global__ void set_word(int *p, int v) { *p = v; }
 
 }  // namespace
 }  // namespace apspie
 
 extern "C" int apspie_bfs_noalloc(void *stream, int src, int64_t nnz, int m, const int *d_ptr,
                                   const int *d_ind, const int *d_tptr, const int *d_tind,
-                                  int32_t *d_depth, int max_levels) {
+                                  int32_t *d_depth, int max_levels, int32_t *d_status) {
   using namespace apspie;
   if (m <= 0 || src < 0 || src >= m || nnz < 0) return APSPIE_ERR_INVALID;
   if (m > kNoAllocMaxVertices || nnz > kNoAllocMaxEdges) return APSPIE_ERR_TOO_LARGE;
@@ -660,5 +708,42 @@ extern "C" int apspie_bfs_noalloc(void *stream, int src, int64_t nnz, int m, con
     cudaGetLastError();
     return APSPIE_ERR_CUDA;
   }
+  if (d_status) {
+    bfs_write_status<<<1, 1, 0, st>>>(state, d_status);
+    if (cudaGetLastError() != cudaSuccess) return APSPIE_ERR_CUDA;
+  }
   return APSPIE_OK;
 }
+
+namespace apspie {
+
+// Test hook of apspie_debug_inject for the BFS kernel: the next launch on
+// ctx (ctx NULL: the next apspie_bfs_noalloc on the current device) loses
+// its last block before the first grid barrier.
+int bfs_inject(apspie_context *ctx) {
+  BfsState *st = nullptr;
+  cudaStream_t stream = nullptr;
+  if (ctx) {
+    st = (BfsState *)workspace(ctx, kSlotBfsState, sizeof(BfsState));
+    if (!st) return APSPIE_ERR_OOM;
+    if (ctx->bfs_state_zeroed != st) {
+      cudaError_t ez = cudaMemsetAsync(st, 0, sizeof(BfsState), ctx->stream);
+      if (ez != cudaSuccess) return check_cuda(ctx, ez, "apspie_debug_inject");
+      ctx->bfs_state_zeroed = st;
+      ctx->bfs_par = 0;
+    }
+    stream = ctx->stream;
+  } else {
+    int dev = 0, grid = 0;
+    unsigned char *base = nullptr;
+    if (cudaGetDevice(&dev) != cudaSuccess) return APSPIE_ERR_CUDA;
+    int rc = noalloc_setup(dev, &base, &grid);
+    if (rc) return rc;
+    st = (BfsState *)base;
+  }
+  set_word<<<1, 1, 0, stream>>>(&st->inject, 1);
+  if (cudaGetLastError() != cudaSuccess) return APSPIE_ERR_CUDA;
+  return ctx ? APSPIE_OK : (cudaStreamSynchronize(stream) == cudaSuccess ? APSPIE_OK : APSPIE_ERR_CUDA);
+}
+
+}  // namespace apspie

@@ -35,6 +35,12 @@ void *workspace(apspie_context *ctx, int id, size_t bytes) {
   auto &s = ctx->slots[id];
   if (bytes == 0) bytes = 16;
   if (s.bytes >= bytes) return s.ptr;
+  if (ctx->fail_next_alloc) {
+    // test hook: this growth fails as a cudaMalloc that ran out of memory
+    ctx->fail_next_alloc = false;
+    set_error(ctx, APSPIE_ERR_OOM, "workspace slot %d: allocation failure injected", id);
+    return nullptr;
+  }
   if (s.ptr) {
     // the stream may still use the old buffer
     cudaStreamSynchronize(ctx->stream);

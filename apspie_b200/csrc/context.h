@@ -38,6 +38,8 @@ struct apspie_context {
   size_t up_bytes[kUploadRing] = {};
   cudaEvent_t up_done[kUploadRing] = {};
   int up_next = 0;
+  // test hook (apspie_debug_inject): the next workspace growth fails
+  bool fail_next_alloc = false;
 
   // at most this many blocks per persistent launch (0: as many as fit), so
   // that two persistent kernels can share the GPU

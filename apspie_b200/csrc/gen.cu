@@ -292,6 +292,8 @@ int apspie_bfs_prepare(apspie_ctx ctx, int m, int64_t nnz, const int *d_ptr, con
   bool in_b = false;
   rc = device_radix_sort<unsigned long long, int>(ctx, ka, va, kb, vb, nnz, vbits + dbits, &in_b);
   if (rc) return rc;
+  rc = radix_sort_check(ctx);  // before the sorted keys index anything
+  if (rc) return rc;
   const unsigned long long *k = in_b ? kb : ka;
   const int *v = in_b ? vb : va;
   key_rows<<<gg(ctx, nnz), 256, 0, st>>>(k, nnz, dbits, d_tptr);
@@ -325,6 +327,8 @@ int apspie_csr_transpose(apspie_ctx ctx, int m, int n, int64_t nnz, const int *d
   // sort only needs the column bits above them (stable LSD on all bits)
   bool in_b = false;
   rc = device_radix_sort<unsigned long long, int>(ctx, ka, va, kb, vb, nnz, rbits + cbits, &in_b);
+  if (rc) return rc;
+  rc = radix_sort_check(ctx);  // before the sorted keys index anything
   if (rc) return rc;
   const unsigned long long *k = in_b ? kb : ka;
   const int *v = in_b ? vb : va;

@@ -177,11 +177,15 @@ __global__ void radix_digit_offsets(unsigned long long *ghist, int npass) {
   }
 }
 
+// Polls of a look-back wait before it gives up (a predecessor normally
+// publishes within microseconds; about half a second with the back-off).
+constexpr unsigned kLookbackSpinLimit = 1u << 20;
+
 template <typename K, typename V>
 __global__ void __launch_bounds__(kSortThreads)
 radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, long long n,
                int pass, const unsigned long long *goff, unsigned long long *status,
-               unsigned *tile_counter, int *err) {
+               unsigned *tile_counter, int *err, int *gaveup) {
   constexpr int kWarps = kSortThreads / 32;
   static_assert(sizeof(V) <= sizeof(K), "values are staged in the keys' shared array");
   // the tile in digit order (keys, then values), each key's digit, per-warp
@@ -193,10 +197,17 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
   __shared__ unsigned long long gbase[kRadix];
   __shared__ unsigned long long s_scan[33];
   __shared__ unsigned s_tile;
+  __shared__ int s_withhold;
   const int lane = lane_id(), w = warp_in_block();
   const int shift = pass * kRadixBits;
   const unsigned long long tag = (unsigned long long)(pass + 1) << 40;
-  if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+  if (threadIdx.x == 0) {
+    s_tile = atomicAdd(tile_counter, 1u);
+    // test hook (apspie_debug_inject): err[1] set makes tile 0 of the next
+    // pass withhold its status, so that its successors' bounded look-back
+    // waits run out; one-shot
+    s_withhold = (s_tile == 0u && n > kSortTile) ? atomicExch(err + 1, 0) : 0;
+  }
   for (int d = lane; d < kRadix; d += 32) whist[w][d] = 0;
   __syncthreads();
   const unsigned tile = s_tile;
@@ -242,7 +253,7 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
   unsigned long long *mine = status + (size_t)tile * kRadix + d;
   unsigned long long excl = 0;
   if (tile == 0) {
-    __stcg(mine, kStIncl | tag | (unsigned long long)run);
+    if (!s_withhold) __stcg(mine, kStIncl | tag | (unsigned long long)run);
   } else {
     __stcg(mine, kStAgg | tag | (unsigned long long)run);
     long long t = (long long)tile - 1;
@@ -250,10 +261,16 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
     while (t >= 0) {
       const unsigned long long sv = ld_acquire64(status + (size_t)t * kRadix + d);
       if ((sv & (0x3FFFFFull << 40)) != tag || (sv >> 62) == 0ull) {
-        if (++spins > kSpinLimit) {  // a predecessor never published: give up
+        // a predecessor never published: give up after kLookbackSpinLimit
+        // polls, or at once when another tile of this sort already gave up
+        // (checked every 256; *gaveup is zeroed with the sort's status words)
+        if (++spins > kLookbackSpinLimit ||
+            ((spins & 255u) == 0u && *(volatile int *)gaveup != 0)) {
           atomicExch(err, 1);
+          atomicExch(gaveup, 1);
           break;
         }
+        if ((spins & 15u) == 0u) __nanosleep(64);
         continue;
       }
       excl += sv & kStCountMask;
@@ -276,8 +293,13 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
     }
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < tlen; t += kSortThreads)
-    keys_out[gbase[sdig[t]] + t] = skeys[t];
+  // the bound holds for every sorted pass; it guards a pass after a
+  // look-back give-up, whose input then holds keys the histograms did not
+  // count
+  for (int t = threadIdx.x; t < tlen; t += kSortThreads) {
+    const unsigned long long at = gbase[sdig[t]] + t;
+    if (at < (unsigned long long)n) keys_out[at] = skeys[t];
+  }
   if (vals_in) {  // keys-only sorts pass no values
     __syncthreads();
     V *svals = reinterpret_cast<V *>(skeys);
@@ -287,14 +309,19 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
       if (t < tlen) svals[pos[i]] = vals_in[tbase + t];
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < tlen; t += kSortThreads)
-      vals_out[gbase[sdig[t]] + t] = svals[t];
+    for (int t = threadIdx.x; t < tlen; t += kSortThreads) {
+      const unsigned long long at = gbase[sdig[t]] + t;
+      if (at < (unsigned long long)n) vals_out[at] = svals[t];
+    }
   }
 }
 
 // The context's radix-sort give-up word: set by a tile whose look-back
-// waited kSpinLimit polls for a predecessor (the output is then in bounds
-// but not sorted).  Sticky: zeroed when first allocated and by
+// waited kLookbackSpinLimit polls for a predecessor (the output is then in
+// bounds but neither sorted nor a permutation of the input: some slots keep
+// stale contents).  A caller that uses sorted keys or values as indices must
+// therefore check it (radix_sort_check) before doing so; apspie_spmspv,
+// which only bounds-checks its segment writes, checks it at its end.  Sticky: zeroed when first allocated and by
 // radix_sort_check, not by each sort, so a caller that synchronises only
 // at its end still sees a give-up of any sort it ran.  Stream-ordered
 // callers that never synchronise (apspie_bfs_prepare, apspie_csr_transpose)
@@ -336,7 +363,8 @@ int device_radix_sort(apspie_context *ctx, K *ka, V *va, K *kb, V *vb, long long
   if (npass > kMaxPasses || n >= (1ll << 40))
     return set_error(ctx, APSPIE_ERR_OVERFLOW, "radix sort: %lld keys of %d bits", n, bits);
   const long long tiles = (n + kSortTile - 1) / kSortTile;
-  // [histograms: npass x 256 u64][tile counters: 8 x u32, padded][status: tiles x 256 u64]
+  // [histograms: npass x 256 u64][tile counters: 8 x u32, padded; the
+  // sort's give-up word at u32 15][status: tiles x 256 u64]
   const size_t hist_bytes = sizeof(unsigned long long) * kMaxPasses * kRadix;
   const size_t head = hist_bytes + 64;
   const size_t bytes = head + sizeof(unsigned long long) * (size_t)tiles * kRadix;
@@ -360,7 +388,7 @@ int device_radix_sort(apspie_context *ctx, K *ka, V *va, K *kb, V *vb, long long
   for (int p = 0; p < npass; ++p) {
     radix_onesweep<K, V><<<(unsigned)tiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, p,
                                                                    ghist, status, counters + p,
-                                                                   err);
+                                                                   err, (int *)(counters + 15));
     rc = check_launch(ctx, "radix_onesweep");
     if (rc) return rc;
     std::swap(kin, kout);

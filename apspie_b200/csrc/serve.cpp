@@ -159,6 +159,7 @@ struct apspie_server {
   Slot slots[2];
   bool any_deep = false;
   bool warming = false;  // add_graph is warming the lanes: the worker launches nothing
+  int fail_next_kind = -1;  // test hook: the next group of this kind fails
   int max_pending = 1 << 20;
   // MIS priorities per (graph, seed), on the device
   std::mutex prio_mu;
@@ -352,7 +353,17 @@ int launch_group(apspie_server *s, Slot &sl, Group &g) {
   cudaEventRecord(g.start, ln.stream);
   int st = APSPIE_OK;
   const size_t row = 4 * (size_t)ge.m;
-  if (g.kind == 2) {
+  bool inject = false;
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (s->fail_next_kind == g.kind) {
+      s->fail_next_kind = -1;
+      inject = true;
+    }
+  }
+  if (inject) {
+    st = APSPIE_ERR_CUDA;  // test hook: the group fails without running
+  } else if (g.kind == 2) {
     // identical queries (same graph and seed): computed once
     Request *r = g.reqs.front();
     uint32_t *prio = nullptr;
@@ -954,6 +965,13 @@ int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q, 
   }
   if (wall_ms) *wall_ms = last;
   return st;
+}
+
+int apspie_server_debug_fail_next(apspie_server_t s, int kind) {
+  if (!s || kind < 0 || kind > 2) return APSPIE_ERR_INVALID;
+  std::lock_guard<std::mutex> lock(s->mu);
+  s->fail_next_kind = kind;
+  return APSPIE_OK;
 }
 
 int apspie_server_poll(apspie_server_t s, uint64_t req_id, int *done, double *latency_ms) {

@@ -158,7 +158,7 @@ __global__ void head_flags(const int *keys, long long n, unsigned *flags) {
 }
 
 __global__ void reduce_segments(int sr, const int *keys, const float *vals, long long n,
-                                const unsigned *segid, int *yind, float *yval) {
+                                const unsigned *segid, int *yind, float *yval, int ycap) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     int k = keys[i];
@@ -175,7 +175,10 @@ __global__ void reduce_segments(int sr, const int *keys, const float *vals, long
         default: accf = 1.0f; break;
       }
     }
+    // at most m distinct rows from a sorted run; more only from a sort that
+    // gave up (reported by the caller), whose extra segments are dropped
     unsigned s = segid[i];
+    if (s >= (unsigned)ycap) continue;
     yind[s] = k;
     yval[s] = sr == kPlusTimes ? (float)accd : accf;
   }
@@ -416,15 +419,16 @@ int spmspv_core(apspie_context *ctx, int sr, int m, const int *ptr, const int *i
     if (rc) return rc;
     long long *h = (long long *)pinned(ctx, sizeof(long long));
     if (!h) return APSPIE_ERR_OOM;
-    cudaMemcpyAsync(h, d_tot, sizeof(long long), cudaMemcpyDeviceToHost, st);
+    rc = check_cuda(ctx, cudaMemcpyAsync(h, d_tot, sizeof(long long), cudaMemcpyDeviceToHost, st),
+                    "spmspv total");
+    if (rc) return rc;
     rc = check_cuda(ctx, cudaStreamSynchronize(st), "spmspv total");
     if (rc) return rc;
     E = *h;
   }
   if (h_total) *h_total = E;
   if (E == 0) {
-    cudaMemsetAsync(d_ynnz, 0, sizeof(int), st);
-    return check_cuda(ctx, cudaGetLastError(), "spmspv empty");
+    return check_cuda(ctx, cudaMemsetAsync(d_ynnz, 0, sizeof(int), st), "spmspv empty");
   }
   if (E >= (long long)INT32_MAX)
     return set_error(ctx, APSPIE_ERR_OVERFLOW, "spmspv: %lld expanded pairs", E);
@@ -441,8 +445,10 @@ int spmspv_core(apspie_context *ctx, int sr, int m, const int *ptr, const int *i
                                     sizeof(int2) * ((size_t)E / kHubChunk + (size_t)xnnz + 1));
     if (!big) return APSPIE_ERR_OOM;
     int2 *hub = (int2 *)(big + nbig_cap);
-    cudaMemsetAsync(&sm->nbig, 0, sizeof(unsigned), st);
-    cudaMemsetAsync(&sm->nhub, 0, sizeof(unsigned), st);
+    int rc = check_cuda(ctx, cudaMemsetAsync(&sm->nbig, 0, sizeof(unsigned), st), "spmspv nbig");
+    if (rc) return rc;
+    rc = check_cuda(ctx, cudaMemsetAsync(&sm->nhub, 0, sizeof(unsigned), st), "spmspv nhub");
+    if (rc) return rc;
     acc_init<<<grid_for(ctx, m, 256), 256, 0, st>>>(sr, m, acc, bits);
     expand_accumulate<<<grid_for(ctx, (long long)xnnz * 32, kExpandThreads), kExpandThreads, 0,
                         st>>>(sr, xnnz, xind, xval, ptr, ind, val, acc, bits, big, &sm->nbig,
@@ -450,7 +456,7 @@ int spmspv_core(apspie_context *ctx, int sr, int m, const int *ptr, const int *i
     expand_accumulate_big<<<ctx->num_sms * 4, kExpandThreads, 0, st>>>(
         sr, xind, xval, ptr, ind, val, big, &sm->nbig, hub, &sm->nhub, acc, bits);
     bitmap_counts<<<grid_for(ctx, words, 256), 256, 0, st>>>(bits, words, woffs);
-    int rc = check_launch(ctx, "spmspv bitmap", 4);
+    rc = check_launch(ctx, "spmspv bitmap", 4);
     if (rc) return rc;
     rc = device_exclusive_scan<unsigned>(ctx, woffs, woffs, words, (unsigned *)d_ynnz);
     if (rc) return rc;
@@ -469,13 +475,15 @@ int spmspv_core(apspie_context *ctx, int sr, int m, const int *ptr, const int *i
   unsigned *nbig = &sm->nbig;
   if (!ka || !kb || !va || !vb || !big) return APSPIE_ERR_OOM;
   int2 *hub = (int2 *)(big + nbig_cap);
-  cudaMemsetAsync(nbig, 0, sizeof(unsigned), st);
-  cudaMemsetAsync(&sm->nhub, 0, sizeof(unsigned), st);
+  int rc = check_cuda(ctx, cudaMemsetAsync(nbig, 0, sizeof(unsigned), st), "spmspv nbig");
+  if (rc) return rc;
+  rc = check_cuda(ctx, cudaMemsetAsync(&sm->nhub, 0, sizeof(unsigned), st), "spmspv nhub");
+  if (rc) return rc;
   expand_pairs<<<grid_for(ctx, (long long)xnnz * 32, kExpandThreads), kExpandThreads, 0, st>>>(
       sr, xnnz, xind, xval, ptr, ind, val, offs, ka, va, big, nbig, hub, &sm->nhub);
   expand_big<<<ctx->num_sms * 4, kExpandThreads, 0, st>>>(sr, xind, xval, ptr, ind, val, offs,
                                                           big, nbig, hub, &sm->nhub, ka, va);
-  int rc = check_launch(ctx, "expand_pairs", 2);
+  rc = check_launch(ctx, "expand_pairs", 2);
   if (rc) return rc;
   bool in_b = false;
   rc = device_radix_sort<int, float>(ctx, ka, va, kb, vb, E, bits_for(m), &in_b);
@@ -489,7 +497,7 @@ int spmspv_core(apspie_context *ctx, int sr, int m, const int *ptr, const int *i
   if (rc) return rc;
   rc = device_exclusive_scan<unsigned>(ctx, flags, flags, E, (unsigned *)d_ynnz);
   if (rc) return rc;
-  reduce_segments<<<grid_for(ctx, E, 256), 256, 0, st>>>(sr, ks, vs, E, flags, yind, yval);
+  reduce_segments<<<grid_for(ctx, E, 256), 256, 0, st>>>(sr, ks, vs, E, flags, yind, yval, m);
   return check_launch(ctx, "reduce_segments");
 }
 
@@ -518,12 +526,17 @@ int apspie_spmspv(apspie_ctx ctx, int semiring, int m, int64_t nnz, const int *d
   int *h = (int *)pinned(ctx, sizeof(long long));
   int *sort_err = radix_sort_err(ctx);
   if (!h || !sort_err) return APSPIE_ERR_OOM;
-  cudaMemcpyAsync(h, d_ynnz, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-  cudaMemcpyAsync(h + 1, sort_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  rc = check_cuda(ctx, cudaMemcpyAsync(h, d_ynnz, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream),
+                  "apspie_spmspv");
+  if (rc) return rc;
+  rc = check_cuda(ctx, cudaMemcpyAsync(h + 1, sort_err, sizeof(int), cudaMemcpyDeviceToHost,
+                                       ctx->stream), "apspie_spmspv");
+  if (rc) return rc;
   rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "apspie_spmspv");
   if (rc) return rc;
   if (h[1]) {  // the sort path's look-back gave up: the output is not sorted
-    cudaMemsetAsync(sort_err, 0, sizeof(int), ctx->stream);
+    rc = check_cuda(ctx, cudaMemsetAsync(sort_err, 0, sizeof(int), ctx->stream), "apspie_spmspv");
+    if (rc) return rc;
     return set_error(ctx, APSPIE_ERR_TIMEOUT, "apspie_spmspv: radix sort look-back gave up");
   }
   *h_ynnz = *h;

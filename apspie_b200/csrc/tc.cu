@@ -23,9 +23,11 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstring>
 
 #include "common.cuh"
 #include "context.h"
+#include "gen_common.h"
 #include "primitives.cuh"
 
 namespace apspie {
@@ -291,20 +293,29 @@ __global__ void rank_to_perm(int m, const int *order, int *perm) {
 
 // Per vertex v of new id r: how many neighbours rank below r (the length
 // of L's row r) and how many above (v's entries in L's columns).  A warp
-// per vertex, both counts from one read of the row.
+// per vertex, both counts from one read of the row.  The same pass sums a
+// 64-bit hash of every edge (v, u) and of its reverse (u, v) into hsum[0] and
+// hsum[1] (wrapping): the edge multiset equals its transpose -- the graph is
+// symmetric -- exactly when the multisets of hashed pairs agree, which the two
+// sums confirm up to a 2^-64 chance.
 __global__ void split_counts(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
-                            const int *__restrict__ perm, int *lcnt, int *ucnt) {
+                            const int *__restrict__ perm, int *lcnt, int *ucnt,
+                            unsigned long long *hsum) {
   const int lane = lane_id();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  unsigned long long h_fwd = 0, h_rev = 0;
   for (int v = gwarp; v < m; v += nwarps) {
     const int r = __ldg(perm + v);
     const int s = __ldg(ptr + v), e = __ldg(ptr + v + 1);
     int lo = 0, hi = 0;
     for (int k = s + lane; k < e; k += 32) {
-      const int pu = __ldg(perm + __ldg(ind + k));
+      const int u = __ldg(ind + k);
+      const int pu = __ldg(perm + u);
       lo += pu < r;
       hi += pu > r;
+      h_fwd += apspie_gen::mix64(((unsigned long long)(unsigned)v << 32) | (unsigned)u);
+      h_rev += apspie_gen::mix64(((unsigned long long)(unsigned)u << 32) | (unsigned)v);
     }
     lo = warp_sum(lo);
     hi = warp_sum(hi);
@@ -312,6 +323,12 @@ __global__ void split_counts(int m, const int *__restrict__ ptr, const int *__re
       lcnt[r] = lo;
       ucnt[r] = hi;
     }
+  }
+  h_fwd = warp_sum(h_fwd);
+  h_rev = warp_sum(h_rev);
+  if (lane == 0 && (h_fwd | h_rev)) {
+    atomicAdd(hsum, h_fwd);
+    atomicAdd(hsum + 1, h_rev);
   }
 }
 
@@ -384,6 +401,8 @@ int apspie_tc_prepare(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr, cons
   bool in_b = false;
   rc = device_radix_sort<unsigned, int>(ctx, dk, ids, dk2, ids2, m, dbits, &in_b);
   if (rc) return rc;
+  rc = radix_sort_check(ctx);  // before the sorted ids index anything
+  if (rc) return rc;
   rank_to_perm<<<tgrid(ctx, m, 256), 256, 0, st>>>(m, in_b ? ids2 : ids, d_perm);
   // 2. row lengths of L (indexed by new id) and each vertex's count above it
   auto *lcnt = d_Lptr;
@@ -391,8 +410,10 @@ int apspie_tc_prepare(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr, cons
   if (!uoff) return APSPIE_ERR_OOM;
   cudaMemsetAsync(lcnt + m, 0, sizeof(int), st);
   cudaMemsetAsync(uoff + m, 0, sizeof(int), st);
+  // small[0]: the largest degree; small + 8 bytes .. + 24: the two edge hashes
+  auto *hsum = reinterpret_cast<unsigned long long *>(small) + 1;
   split_counts<<<tgrid(ctx, (long long)m * 32, 256), 256, 0, st>>>(m, d_ptr, d_ind, d_perm, lcnt,
-                                                                   uoff);
+                                                                   uoff, hsum);
   rc = check_launch(ctx, "split_counts");
   if (rc) return rc;
   // exclusive scans of the m + 1 entries (entry m is 0): offsets + totals
@@ -400,16 +421,26 @@ int apspie_tc_prepare(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr, cons
   if (rc) return rc;
   rc = device_exclusive_scan<int>(ctx, uoff, uoff, (long long)m + 1, nullptr);
   if (rc) return rc;
-  cudaMemcpyAsync(hs, d_Lptr + m, 4, cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(hs + 1, uoff + m, 4, cudaMemcpyDeviceToHost, st);
+  rc = check_cuda(ctx, cudaMemcpyAsync(hs, d_Lptr + m, 4, cudaMemcpyDeviceToHost, st),
+                  "tc_prepare counts");
+  if (rc) return rc;
+  rc = check_cuda(ctx, cudaMemcpyAsync(hs + 1, uoff + m, 4, cudaMemcpyDeviceToHost, st),
+                  "tc_prepare counts");
+  if (rc) return rc;
+  rc = check_cuda(ctx, cudaMemcpyAsync(hs + 2, hsum, 16, cudaMemcpyDeviceToHost, st),
+                  "tc_prepare counts");
+  if (rc) return rc;
   rc = check_cuda(ctx, cudaStreamSynchronize(st), "tc_prepare counts");
   if (rc) return rc;
   const long long lnnz = hs[0];
-  // every edge below one end is above the other only when the graph is symmetric
-  if (hs[1] != hs[0] || lnnz > nnz / 2)
+  unsigned long long hh[2];
+  std::memcpy(hh, hs + 2, sizeof(hh));
+  // L is read from both ends of every edge: the graph must be symmetric
+  if (hh[0] != hh[1] || hs[1] != hs[0] || lnnz > nnz / 2)
     return set_error(ctx, APSPIE_ERR_INVALID,
-                     "apspie_tc_prepare: the graph is not symmetric (%u entries below, %u above)",
-                     hs[0], hs[1]);
+                     "apspie_tc_prepare: the graph is not symmetric (%u entries below, %u above, "
+                     "edge hashes %s)",
+                     hs[0], hs[1], hh[0] == hh[1] ? "equal" : "differ");
   if (lnnz > 0) {
     // 3. (row, column) pairs grouped by ascending column, stable-sorted by row:
     //    the columns come out in d_Lind (or in the other buffer, then copied)
@@ -424,6 +455,8 @@ int apspie_tc_prepare(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr, cons
     in_b = false;
     rc = device_radix_sort<unsigned, int>(ctx, ka, va, kb, d_Lind, lnnz, cbits, &in_b);
     if (rc) return rc;
+    rc = radix_sort_check(ctx);
+    if (rc) return rc;
     if (!in_b) {
       rc = check_cuda(ctx, cudaMemcpyAsync(d_Lind, va, sizeof(int) * (size_t)lnnz,
                                            cudaMemcpyDeviceToDevice, st),
@@ -431,8 +464,6 @@ int apspie_tc_prepare(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr, cons
       if (rc) return rc;
     }
   }
-  rc = radix_sort_check(ctx);  // both sorts; synchronises
-  if (rc) return rc;
   *h_lnnz = lnnz;
   return APSPIE_OK;
 }

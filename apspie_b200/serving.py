@@ -100,9 +100,18 @@ class Server:
 
     def wait(self, rid: int):
         lat = C.c_double()
-        check(lib.apspie_server_wait(self._h, C.c_uint64(rid), C.byref(lat)),
-              what="apspie_server_wait")
+        try:
+            check(lib.apspie_server_wait(self._h, C.c_uint64(rid), C.byref(lat)),
+                  what="apspie_server_wait")
+        except ApspieError:
+            self._live.pop(rid, None)
+            raise
         return self._live.pop(rid), lat.value
+
+    def debug_fail_next(self, kind: int) -> None:
+        """Test hook: the next group of this kind fails without running."""
+        check(lib.apspie_server_debug_fail_next(self._h, int(kind)),
+              what="apspie_server_debug_fail_next")
 
     def poll(self, rid: int):
         done, lat = C.c_int(), C.c_double()

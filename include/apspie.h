@@ -139,11 +139,17 @@ int apspie_bfs_get_trace(apspie_ctx ctx, int max_levels, int *n_out,
  * device address (and may load the library's device code); make that first
  * call before any stream capture.  All calls share the one array, so calls
  * that overlap on the GPU (other streams, other host threads) race; run them
- * one after another.  Statistics are not reported.  No counterpart in the
- * reference. */
+ * one after another.  d_status (device memory, may be NULL) receives the
+ * run's status once it has finished, stream-ordered and without a host
+ * synchronisation: 0, or APSPIE_ERR_TIMEOUT when a bounded grid-barrier wait
+ * gave up (the depths are then incomplete).  The array's address is cached
+ * per CUDA context (a driver-API context of the caller's, or the device's
+ * primary context, which cudaDeviceReset replaces).  Statistics are not
+ * reported.  No counterpart in the reference. */
 int apspie_bfs_noalloc(void *stream, int src, int64_t nnz, int m,
                        const int *d_ptr, const int *d_ind, const int *d_tptr,
-                       const int *d_tind, int32_t *d_depth, int max_levels);
+                       const int *d_tind, int32_t *d_depth, int max_levels,
+                       int32_t *d_status);
 
 /* Direction-switch thresholds (Beamer's alpha, beta; defaults 14 and 24):
  * push -> pull when frontier edges * alpha > unexplored edges, pull -> push
@@ -397,6 +403,32 @@ int apspie_autotune_spmspv(apspie_ctx ctx, int m, int64_t nnz, const int *d_ptr,
                            int *d_yind_scratch, float *d_yval_scratch,
                            double *factor_out);
 
+/* --------------------------------------------------------- test hooks ---
+ * For the tests of the timeout paths (no reference counterpart).  Every
+ * device-side wait is bounded and reports APSPIE_ERR_TIMEOUT when it runs
+ * out; a hook makes one run out without a fault or an unbounded wait.
+ * One-shot: APSPIE_INJECT_BFS_BARRIER -- the next BFS launch on ctx (ctx NULL:
+ * the next apspie_bfs_noalloc on the current device) loses its last block
+ * before the first grid barrier; the others' wait gives up (about 1.7 s) and
+ * apspie_bfs_get_stats (or the no-alloc status word) reports the timeout.
+ * APSPIE_INJECT_SORT_LOOKBACK -- the first tile of the next multi-tile radix
+ * sort pass on ctx withholds its look-back status; its successors give up
+ * (about half a second), write their keys in bounds, and the next call that
+ * reads the sort's give-up word (apspie_spmspv, apspie_tc_prepare, the device
+ * graph build) reports the timeout.  APSPIE_INJECT_ALLOC_FAIL -- the next
+ * workspace growth on ctx fails on the host as an exhausted cudaMalloc would:
+ * the call returns APSPIE_ERR_OOM and the context stays usable. */
+enum {
+  APSPIE_INJECT_BFS_BARRIER = 1,
+  APSPIE_INJECT_SORT_LOOKBACK = 2,
+  APSPIE_INJECT_ALLOC_FAIL = 3
+};
+int apspie_debug_inject(apspie_ctx ctx, int what);
+/* The next query group of the given kind (0 BFS, 1 SSSP, 2 MIS) that the
+ * server launches completes with APSPIE_ERR_CUDA without running: its
+ * requests' waits return the error, the other groups are unaffected. */
+int apspie_server_debug_fail_next(apspie_server_t s, int kind);
+
 /* ------------------------------------------------------------- SpMSpV ---
  * Semirings of the reference's three SpMSpV variants. */
 typedef enum {
@@ -499,9 +531,11 @@ int apspie_csr_copy_out(apspie_ctx ctx, const apspie_csr *C, int *d_ptr,
  * ascending (degree, id) -- d_perm[v] = new id -- and L(new(u), :) = the new
  * ids of u's neighbours below new(u), rows sorted.  test/tc/main.cu:40-55,
  * 172-175 builds the strict triangles on the host.  d_Lptr holds m + 1
- * entries, d_Lind at least nnz / 2; *h_lnnz = nnz(L).  A graph with more
- * entries below the new order than above it (or the reverse) is not
- * symmetric and is refused with APSPIE_ERR_INVALID.  Synchronises. */
+ * entries, d_Lind at least nnz / 2; *h_lnnz = nnz(L).  A graph that is not
+ * symmetric is refused with APSPIE_ERR_INVALID: the wrapping sums of a
+ * 64-bit hash of every edge (u, v) and of (v, u) must agree (equal edge
+ * multisets; a different one passes with probability 2^-64), as must the
+ * counts of entries below and above the new order.  Synchronises. */
 int apspie_tc_prepare(apspie_ctx ctx, int64_t nnz, int m, const int *d_ptr,
                       const int *d_ind, int *d_perm, int *d_Lptr, int *d_Lind,
                       int64_t *h_lnnz);

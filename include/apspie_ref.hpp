@@ -297,6 +297,76 @@ inline void spgemm(d_matrix *C, d_matrix *A, d_matrix *B, const int partSize, co
   C->owned_by_library = true;
 }
 
+// spgemm<T>() (src/tc.cuh:63-165): C = A * B on the arrays as given -- the
+// reference hands its "csc" arrays to cusparseXcsrgemmNnz / cusparseScsrgemm,
+// which read them as CSR, so the TC driver's call spgemm(C, B) forms U * L
+// (test/tc/main.cu:241).  C's arrays are allocated here with cudaMalloc, as
+// the reference allocates them (src/tc.cuh:73,120-121); the caller frees them
+// with cudaFree.  `edge` is the reference's nnz argument for both inputs
+// (the TC driver passes the whole graph's edge count for its half
+// matrices); here nnz(A) and nnz(B) are read from the offsets.  The call
+// runs on a context of its own, as the reference creates its own cuSPARSE
+// handle.  Returns nnz(C).
+template <typename T>
+int spgemm(const int edge, const int m, const T *d_cscValA, const int *d_cscColPtrA,
+           const int *d_cscRowIndA, const T *d_cscValB, const int *d_cscColPtrB,
+           const int *d_cscRowIndB, T *&d_cscValC, int *&d_cscColPtrC, int *&d_cscRowIndC) {
+  static_assert(std::is_same<T, float>::value, "spgemm<T>: float values, as cusparseScsrgemm");
+  (void)edge;
+  int dev = 0, na = 0, nb = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaMemcpy(&na, d_cscColPtrA + m, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(&nb, d_cscColPtrB + m, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    throw apspie::Error(APSPIE_ERR_CUDA, "spgemm: reading the offsets");
+  mgpu::CudaContext ctx(dev);
+  apspie_csr a{m, m, na, const_cast<int *>(d_cscColPtrA), const_cast<int *>(d_cscRowIndA),
+               const_cast<float *>((const float *)d_cscValA)};
+  apspie_csr b{m, m, nb, const_cast<int *>(d_cscColPtrB), const_cast<int *>(d_cscRowIndB),
+               const_cast<float *>((const float *)d_cscValB)};
+  apspie_csr c{};
+  apspie::check(apspie_spgemm(ctx.handle(), &a, &b, &c), ctx.handle(), "spgemm");
+  d_cscValC = (T *)c.d_val;
+  d_cscColPtrC = c.d_ptr;
+  d_cscRowIndC = c.d_ind;
+  return (int)c.nnz;
+}
+
+// mXm<T>() (src/tc.cuh:315-375): C(:, i) = A * B(:, i) for every column i of
+// B (the reference runs one sparse mXv per column), i.e. C = A * B on the
+// CSC arrays.  Read as CSR arrays these hold the transposes, so C's arrays
+// are the CSR product of B's arrays and A's (apspie_spgemm(B, A)); each
+// column comes out with its rows ascending, as mXv's ReduceByKey leaves
+// them.  The reference allocates C inside, through its by-value pointer
+// parameters, and so never returns it (src/tc.cuh:318-324); here C is
+// written into the caller's arrays: d_cscColPtrC m + 1 offsets, and
+// d_cscRowIndC / d_cscValC nnz(C) entries, at most the 16 * edge the
+// reference sizes them for (a larger product throws APSPIE_ERR_TOO_LARGE
+// before anything is written but the offsets).  Returns nnz(C).
+template <typename T>
+int mXm(const int edge, const int m, const T *d_cscValA, const int *d_cscColPtrA,
+        const int *d_cscRowIndA, const T *d_cscValB, const int *h_cscColPtrB,
+        const int *d_cscColPtrB, const int *d_cscRowIndB, T *d_cscValC, int *d_cscColPtrC,
+        int *d_cscRowIndC, mgpu::CudaContext &context) {
+  static_assert(std::is_same<T, float>::value, "mXm<T>: float values");
+  int na = 0;
+  if (cudaMemcpy(&na, d_cscColPtrA + m, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    throw apspie::Error(APSPIE_ERR_CUDA, "mXm: reading the offsets");
+  apspie_csr a{m, m, na, const_cast<int *>(d_cscColPtrA), const_cast<int *>(d_cscRowIndA),
+               const_cast<float *>((const float *)d_cscValA)};
+  apspie_csr b{m, m, h_cscColPtrB[m], const_cast<int *>(d_cscColPtrB),
+               const_cast<int *>(d_cscRowIndB), const_cast<float *>((const float *)d_cscValB)};
+  int64_t nnz = 0;
+  apspie::check(apspie_spgemm_symbolic(context.handle(), &b, &a, d_cscColPtrC, &nnz),
+                context.handle(), "mXm");
+  if (nnz > 16ll * edge)
+    throw apspie::Error(APSPIE_ERR_TOO_LARGE, "mXm: nnz(C) exceeds 16 * edge");
+  apspie::check(apspie_spgemm_numeric(context.handle(), &b, &a, d_cscColPtrC, d_cscRowIndC,
+                                      (float *)d_cscValC),
+                context.handle(), "mXm");
+  apspie::check(apspie_ctx_sync(context.handle()), context.handle(), "mXm");
+  return (int)nnz;
+}
+
 // Triangle count of a symmetric graph (the computation of test/tc/main.cu).
 inline long long triangleCount(const int edge, const int m, const int *d_ptr, const int *d_ind,
                                mgpu::CudaContext &context) {

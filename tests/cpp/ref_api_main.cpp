@@ -5,7 +5,8 @@
 // routine through the reference's signatures (include/apspie_ref.hpp), then
 // verify() / unverify().  Exit status 0 means CORRECT.
 //
-//   ref_api_main <bfs|spmspvbfs|sssp|mis|mxv|spmv|csr2csc|spgemm|tc> file.mtx [-source N] [-undirected]
+//   ref_api_main <bfs|spmspvbfs|sssp|mis|mxv|spmv|csr2csc|spgemm|spgemm_csc|mxm|tc> file.mtx
+//                [-source N] [-undirected]
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -217,6 +218,68 @@ int main(int argc, char **argv) {
         errors += verify((int)nnz, gval.data(), cvf.data());
       }
       matrix_delete(&C);
+    } else if (algo == "spgemm_csc" || algo == "mxm") {
+      // the reference's TC-driver SpGEMM (library-allocated C) and its
+      // column-by-column mXm (caller's C), with B = the transpose of A so the
+      // operand order shows: spgemm<T> forms A * B on the arrays, mXm B * A
+      std::vector<int> tp(m + 1, 0), ti(g.nnz);
+      std::vector<float> tv(g.nnz);
+      for (int64_t k = 0; k < g.nnz; ++k) tp[g.ind[k] + 1]++;
+      for (int v = 0; v < m; ++v) tp[v + 1] += tp[v];
+      std::vector<int> at(tp.begin(), tp.end() - 1);
+      for (int u = 0; u < m; ++u)
+        for (int k = g.ptr[u]; k < g.ptr[u + 1]; ++k) {
+          ti[at[g.ind[k]]] = u;
+          tv[at[g.ind[k]]++] = 0.5f * g.val[k] + 1.0f;
+        }
+      int *d_tp = nullptr, *d_ti = nullptr;
+      float *d_tv = nullptr;
+      cudaMalloc(&d_tp, sizeof(int) * (m + 1));
+      cudaMalloc(&d_ti, sizeof(int) * (g.nnz > 0 ? g.nnz : 1));
+      cudaMalloc(&d_tv, sizeof(float) * (g.nnz > 0 ? g.nnz : 1));
+      cudaMemcpy(d_tp, tp.data(), sizeof(int) * (m + 1), cudaMemcpyHostToDevice);
+      cudaMemcpy(d_ti, ti.data(), sizeof(int) * g.nnz, cudaMemcpyHostToDevice);
+      cudaMemcpy(d_tv, tv.data(), sizeof(float) * g.nnz, cudaMemcpyHostToDevice);
+      const bool mxm = algo == "mxm";
+      // the expected product, as CSR arrays: A * B (spgemm) or B * A (mXm)
+      const int *lp = mxm ? tp.data() : g.ptr.data(), *li = mxm ? ti.data() : g.ind.data();
+      const int *rp = mxm ? g.ptr.data() : tp.data(), *ri = mxm ? g.ind.data() : ti.data();
+      const float *lv = mxm ? tv.data() : g.val.data(), *rv = mxm ? g.val.data() : tv.data();
+      std::vector<int64_t> cp(m + 1);
+      int64_t nnz = orc_spgemm_symbolic(m, m, lp, li, rp, ri, cp.data());
+      std::vector<int> ci(nnz > 0 ? nnz : 1);
+      std::vector<double> cv(nnz > 0 ? nnz : 1);
+      orc_spgemm_numeric(m, m, lp, li, lv, rp, ri, rv, cp.data(), ci.data(), cv.data());
+      int *d_cp = nullptr, *d_ci = nullptr;
+      float *d_cv = nullptr;
+      int got = 0;
+      if (mxm) {
+        cudaMalloc(&d_cp, sizeof(int) * (m + 1));
+        cudaMalloc(&d_ci, sizeof(int) * 16 * (size_t)(edge > 0 ? edge : 1));
+        cudaMalloc(&d_cv, sizeof(float) * 16 * (size_t)(edge > 0 ? edge : 1));
+        got = mXm<float>(edge, m, A.d_cscVal, A.d_cscColPtr, A.d_cscRowInd, d_tv, tp.data(), d_tp,
+                         d_ti, d_cv, d_cp, d_ci, *context);
+      } else {
+        got = spgemm<float>(edge, m, A.d_cscVal, A.d_cscColPtr, A.d_cscRowInd, d_tv, d_tp, d_ti,
+                            d_cv, d_cp, d_ci);
+      }
+      errors = (got != nnz);
+      std::vector<int> gptr = download(d_cp, m + 1);
+      std::vector<int> cp32(cp.begin(), cp.end());
+      errors += verify(m + 1, gptr.data(), cp32.data());
+      if (!errors) {
+        std::vector<int> gind = download(d_ci, (size_t)nnz);
+        std::vector<float> gval = download(d_cv, (size_t)nnz);
+        errors += verify((int)nnz, gind.data(), ci.data());
+        std::vector<float> cvf(cv.begin(), cv.end());
+        errors += verify((int)nnz, gval.data(), cvf.data());
+      }
+      cudaFree(d_cp);
+      cudaFree(d_ci);
+      cudaFree(d_cv);
+      cudaFree(d_tp);
+      cudaFree(d_ti);
+      cudaFree(d_tv);
     } else if (algo == "tc") {
       std::vector<int> perm(m), lp(m + 1), li(g.nnz / 2 + 1);
       orc_tc_build_lower(m, g.ptr.data(), g.ind.data(), perm.data(), lp.data(), li.data());

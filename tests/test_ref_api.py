@@ -43,7 +43,7 @@ def _write_mtx(path, ptr, ind):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("algo", ["bfs", "spmspvbfs", "sssp", "mis", "mxv", "spmv", "csr2csc",
-                                  "spgemm", "tc"])
+                                  "spgemm", "spgemm_csc", "mxm", "tc"])
 def test_driver_correct_on_fixtures(driver, golden, fixture_names, tmp_path, algo):
     for name in fixture_names:
         path = tmp_path / f"{name}.mtx"

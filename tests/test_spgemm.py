@@ -175,6 +175,19 @@ def test_tc_prepare_rejects_a_directed_graph(ctx):
         ap.tc_prepare(ctx, g)
 
 
+def test_tc_prepare_rejects_a_directed_graph_with_balanced_counts(ctx):
+    """A directed graph whose entries below and above the degree order are
+    equal in number (3 and 3: 0->1, 3->1, 3->2 below; 1->0, 0->3, 2->3
+    above) is still refused: the hashes of its edges and of their reverses
+    differ."""
+    import apspie_b200 as ap
+    rows = np.array([0, 0, 1, 2, 3, 3])
+    cols = np.array([1, 3, 0, 3, 1, 2])
+    g = ap.from_edges(4, rows, cols).to_device(with_transpose=False)
+    with pytest.raises(ap.ApspieError, match="not symmetric"):
+        ap.tc_prepare(ctx, g)
+
+
 @pytest.mark.parametrize("scale", [12, 18])
 def test_tc_rmat(ctx, scale):
     """R-MAT scale 18, edge factor 16, symmetrised: the TC configuration."""

@@ -7,7 +7,11 @@ fixed device array (at most 2^20 vertices, 2^24 edges).  The test calls it
 through the C ABI and checks it against apspie_bfs, the entry point that
 draws scratch from a context workspace: BFS depths are integers, so the
 tolerance is zero.  Two calls in a row on the same array show that the
-contents left by one call do not leak into the next.
+contents left by one call do not leak into the next.  The optional status
+word reports 0 for a finished traversal and APSPIE_ERR_TIMEOUT when a
+bounded grid-barrier wait gave up (made to happen by a test hook that makes
+one block leave before the barrier; the others' wait runs out, nothing
+faults or hangs).
 
 The file name sorts last so that a run stopping at the first failure has
 already run every other test."""
@@ -18,17 +22,19 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
+APSPIE_ERR_TIMEOUT = 4
 APSPIE_ERR_TOO_LARGE = 8
+INJECT_BFS_BARRIER = 1
 
 
 def _p(t):
     return C.c_void_p(0 if t is None else t.data_ptr())
 
 
-def _noalloc(lib, stream, g, src, out, tptr, tind, max_levels=0):
+def _noalloc(lib, stream, g, src, out, tptr, tind, max_levels=0, status=None):
     return lib.apspie_bfs_noalloc(C.c_void_p(stream.cuda_stream), int(src), int(g.nnz), int(g.m),
                                   _p(g.ptr), _p(g.ind), _p(tptr), _p(tind), _p(out),
-                                  int(max_levels))
+                                  int(max_levels), _p(status))
 
 
 @pytest.mark.parametrize("symmetric", [True, False])
@@ -46,12 +52,14 @@ def test_noalloc_bfs_matches_bfs_twice(symmetric):
     stream = torch.cuda.current_stream()
     with ap.Context(0) as ctx:
         sources = ap.seeded_sources(h, 2, seed=4)
+        status = torch.full((1,), -1, dtype=torch.int32, device="cuda")
         for s in sources:                       # two calls in a row share the scratch array
             ref = ap.bfs(ctx, g, s).cpu().numpy()
             out = torch.full((h.m,), 7, dtype=torch.int32, device="cuda")
-            assert _noalloc(lib, stream, g, s, out, tptr, tind) == 0
+            assert _noalloc(lib, stream, g, s, out, tptr, tind, status=status) == 0
             torch.cuda.synchronize()
             np.testing.assert_array_equal(out.cpu().numpy(), ref)
+            assert int(status.item()) == 0      # finished: no wait gave up
         # the fixed iteration count and the push-only form (no in-adjacency)
         s = sources[0]
         ref = ap.bfs(ctx, g, s, max_levels=3).cpu().numpy()
@@ -73,10 +81,10 @@ def test_noalloc_rejects_sizes_beyond_the_limit():
     out = torch.empty(1, dtype=torch.int32, device="cuda")
     # more vertices than the array holds: refused before anything is launched
     rc = lib.apspie_bfs_noalloc(C.c_void_p(stream.cuda_stream), 0, 0, (1 << 20) + 1, _p(ptr),
-                                None, None, None, _p(out), 0)
+                                None, None, None, _p(out), 0, None)
     assert rc == APSPIE_ERR_TOO_LARGE
     rc = lib.apspie_bfs_noalloc(C.c_void_p(stream.cuda_stream), 0, (1 << 24) + 1, 1, _p(ptr),
-                                _p(ptr), None, None, _p(out), 0)
+                                _p(ptr), None, None, _p(out), 0, None)
     assert rc == APSPIE_ERR_TOO_LARGE
     assert lib.apspie_status_string(rc) == b"input exceeds the fixed scratch size"
 
@@ -112,3 +120,35 @@ def test_noalloc_bfs_inside_a_cuda_graph():
         ref, _ = oracle.bfs(h.m, h.ptr, h.ind, src)
         np.testing.assert_array_equal(depth.cpu().numpy(), ref)
         depth.fill_(7)
+
+
+def test_noalloc_status_reports_a_barrier_timeout():
+    """The status word tells a caller that cannot synchronise whether the
+    depths are complete: a timeout after a one-shot test hook made one block
+    leave before the first grid barrier, then 0 again on the next call, whose
+    depths are right."""
+    import torch
+
+    import apspie_b200 as ap
+    import oracle
+    from apspie_b200._native import lib
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    h = ap.gen_rmat(12, 16, seed=8)
+    g = h.to_device()
+    src = ap.seeded_sources(h, 1, seed=2)[0]
+    ref, _ = oracle.bfs(h.m, h.ptr, h.ind, src)
+    stream = torch.cuda.current_stream()
+    out = torch.empty(h.m, dtype=torch.int32, device="cuda")
+    status = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+    assert _noalloc(lib, stream, g, src, out, g.ptr, g.ind, status=status) == 0   # set-up
+    torch.cuda.synchronize()
+    assert lib.apspie_debug_inject(None, INJECT_BFS_BARRIER) == 0
+    assert _noalloc(lib, stream, g, src, out, g.ptr, g.ind, status=status) == 0
+    torch.cuda.synchronize()
+    assert int(status.item()) == APSPIE_ERR_TIMEOUT
+    assert _noalloc(lib, stream, g, src, out, g.ptr, g.ind, status=status) == 0
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    np.testing.assert_array_equal(out.cpu().numpy(), ref)
