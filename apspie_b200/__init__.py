@@ -13,10 +13,11 @@ from .ops import (Context, bfs, bfs_prepare, bfs_set_params, csr_transpose, bfs_
                   neighbor_flags, sssp, sssp_stats, sssp_set_params, sssp_trace, sssp_prepare, sssp_set_pull, spmspv, spmv, mxv_dense, spmspv_set_params,
                   PLUS_TIMES, MIN_PLUS, MAX_TIMES, OR_AND, spgemm, spgemm_symbolic, spgemm_numeric, spgemm_set_params, tc_prepare,
                   triangle_count, batch_run, batch_stats, batch_set_params, batch_set_sssp_pull, autotune_bfs, autotune_spmspv,
+                  autotune_sssp, autotune_spgemm, autotune_batch, get_tuning, set_tuning, reset_tuning,
                   gen_rmat_device, gen_er_device, weights_device)
 
 __all__ = ["Server",
     "ApspieError", "Context", "DeviceGraph", "HostGraph", "bfs", "bfs_prepare", "bfs_set_params", "csr_transpose", "bfs_stats", "bfs_trace", "from_edges",
-    "sssp", "sssp_set_params", "sssp_stats", "sssp_trace", "sssp_prepare", "sssp_set_pull", "mis", "mis_rounds", "neighbor_flags", "spmspv", "spmv", "mxv_dense", "spmspv_set_params", "spgemm", "spgemm_symbolic", "spgemm_numeric", "spgemm_set_params", "tc_prepare", "triangle_count", "batch_run", "batch_stats", "batch_set_params", "batch_set_sssp_pull", "autotune_bfs", "autotune_spmspv", "gen_er", "gen_er_device", "gen_grid", "gen_powerlaw", "gen_rmat", "gen_rmat_device", "largest_cc_vertex", "mt19937", "read_mtx", "seeded_sources",
+    "sssp", "sssp_set_params", "sssp_stats", "sssp_trace", "sssp_prepare", "sssp_set_pull", "mis", "mis_rounds", "neighbor_flags", "spmspv", "spmv", "mxv_dense", "spmspv_set_params", "spgemm", "spgemm_symbolic", "spgemm_numeric", "spgemm_set_params", "tc_prepare", "triangle_count", "batch_run", "batch_stats", "batch_set_params", "batch_set_sssp_pull", "autotune_bfs", "autotune_spmspv", "autotune_sssp", "autotune_spgemm", "autotune_batch", "get_tuning", "set_tuning", "reset_tuning", "gen_er", "gen_er_device", "gen_grid", "gen_powerlaw", "gen_rmat", "gen_rmat_device", "largest_cc_vertex", "mt19937", "read_mtx", "seeded_sources",
     "weights_device", "weights_f32", "weights_u32",
 ]

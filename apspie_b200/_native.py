@@ -54,6 +54,15 @@ class BatchStats(C.Structure):
     _fields_ = [("super_steps", C.c_int32), ("pad", C.c_int32), ("frontier_edges", C.c_int64)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("bfs_alpha", C.c_int32), ("bfs_beta", C.c_int32),
+                ("bfs_blocks_per_sm", C.c_int32), ("sssp_blocks_per_sm", C.c_int32),
+                ("sssp_pull_alpha", C.c_int32), ("batch_blocks_per_sm", C.c_int32),
+                ("batch_deep_blocks", C.c_int32), ("spgemm_table_load", C.c_int32),
+                ("spgemm_warp_max_prod", C.c_int32), ("spgemm_bitmap_max_cols", C.c_int64),
+                ("spmspv_sort_factor", C.c_double)]
+
+
 class ServerStats(C.Structure):
     _fields_ = [("completed", C.c_uint64), ("batches", C.c_uint64), ("jobs", C.c_uint64),
                 ("pending", C.c_uint64), ("in_flight_bytes", C.c_uint64), ("p50_ms", C.c_double),
@@ -114,6 +123,13 @@ PROTOS: dict[str, tuple] = {
                                     P_int, C.POINTER(C.c_float)]),
     "apspie_autotune_spmspv": (c_int, [vp, c_int, c_i64, vp, vp, vp, vp, vp, vp, vp,
                                        C.POINTER(C.c_double)]),
+    "apspie_autotune_sssp": (c_int, [vp, c_int, P_int, c_i64, c_int, vp, vp, vp, vp, vp, vp, vp,
+                                     C.POINTER(C.c_float), P_int]),
+    "apspie_autotune_spgemm": (c_int, [vp, C.POINTER(Csr), C.POINTER(Csr),
+                                       C.POINTER(C.c_float), P_int]),
+    "apspie_autotune_batch": (c_int, [vp, c_int, C.POINTER(Job), C.POINTER(C.c_float), P_int]),
+    "apspie_ctx_get_tuning": (c_int, [vp, C.POINTER(Tuning)]),
+    "apspie_ctx_set_tuning": (c_int, [vp, C.POINTER(Tuning)]),
     "apspie_server_create": (c_int, [c_int, C.c_size_t, c_int, P_vp]),
     "apspie_server_add_graph": (c_int, [vp, c_int, c_i64, vp, vp, vp, vp, vp, c_int, P_int]),
     "apspie_server_set_sssp_in": (c_int, [vp, c_int, vp, vp, vp]),

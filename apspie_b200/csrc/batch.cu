@@ -1142,7 +1142,7 @@ int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_
   if (nparts > kMaxJobs)
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: %d device jobs > %d", nparts,
                      kMaxJobs);
-  const int full = clamp_grid(ctx, batch_grid(ctx));
+  const int full = persistent_grid(ctx, batch_grid(ctx), ctx->batch_blocks_per_sm);
   if (full <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_batch_run: occupancy query failed");
   // the deep sources get deep_blocks in all (default half the resident
   // blocks: their traversals are latency bound, a grid filled to the last

@@ -476,7 +476,7 @@ int apspie_bfs(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
   auto *gmask = (unsigned *)workspace(ctx, kSlotBfsGroupMask, sizeof(unsigned) * ((size_t)m / 32 + 1));
   if (!st || !qa || !qb || !ca || !cb || !gmask) return APSPIE_ERR_OOM;
   ctx->bfs_state = st;
-  int grid = clamp_grid(ctx, bfs_grid(ctx));
+  int grid = persistent_grid(ctx, bfs_grid(ctx), ctx->bfs_blocks_per_sm);
   if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_bfs: occupancy query failed");
 
   // the kernel clears the depths and its state itself (one grid barrier

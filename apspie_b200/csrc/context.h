@@ -44,6 +44,11 @@ struct apspie_context {
   // at most this many blocks per persistent launch (0: as many as fit), so
   // that two persistent kernels can share the GPU
   int max_grid = 0;
+  // blocks per SM of the persistent BFS / SSSP / batched launches (0: as
+  // many as fit); picked per graph by the autotuners
+  int bfs_blocks_per_sm = 0;
+  int sssp_blocks_per_sm = 0;
+  int batch_blocks_per_sm = 0;
   // BFS tuning and the device block that holds the last run's statistics
   int bfs_alpha = 14;
   int bfs_beta = 24;
@@ -83,13 +88,44 @@ struct apspie_context {
   unsigned spgemm_plan_bins[16] = {};
   int spgemm_plan_words = 0;  // bitmap words per row (0: hash tables)
   long long spgemm_bitmap_max_cols = 1 << 18;
+  // SpGEMM hash tables: every table holds at least table_load x its entries
+  // (2 or 4; each row bin's limit is divided by table_load / 2, so rows move
+  // to the next larger table); rows of at most warp_max_prod products (<= 256)
+  // are one warp's work, longer ones a block's
+  int spgemm_table_load = 2;
+  int spgemm_warp_max_prod = 256;
+  // the plan's table load, fixed by apspie_spgemm_symbolic for numeric
+  int spgemm_plan_load = 2;
+  // the symbolic pass's stored bitmaps (workspace slots), or null
+  void *spgemm_plan_gbm = nullptr;
+  void *spgemm_plan_bslot = nullptr;
   // autotuner results by graph fingerprint
   struct TuneEntry {
     uint64_t fp;
     int alpha, beta;
     float ms;
+    int blocks_per_sm;
   };
   std::vector<TuneEntry> tune_cache;
+  struct SsspTuneEntry {
+    uint64_t fp;
+    int blocks_per_sm, pull_alpha;
+    float ms;
+  };
+  std::vector<SsspTuneEntry> sssp_tune_cache;
+  struct SpgemmTuneEntry {
+    uint64_t fp;
+    int table_load, warp_max_prod;
+    long long bitmap_max_cols;
+    float ms;
+  };
+  std::vector<SpgemmTuneEntry> spgemm_tune_cache;
+  struct BatchTuneEntry {
+    uint64_t fp;
+    int blocks_per_sm, deep_blocks;
+    float ms;
+  };
+  std::vector<BatchTuneEntry> batch_tune_cache;
 };
 
 namespace apspie {
@@ -139,6 +175,10 @@ enum SlotId : int {
   kSlotSpgBins,
   kSlotSpgBits,
   kSlotSpgVals,
+  kSlotSpgStoredBits,  // the symbolic pass's bitmaps of its bitmap rows
+  kSlotSpgBitmapSlot,
+  kSlotSpgSpillPos,    // numeric bitmap rows longer than one window: spilled products
+  kSlotSpgSpillVal,
   kSlotCount
 };
 
@@ -179,5 +219,13 @@ int gather_offsets(apspie_context *ctx, const int *d_ptr, int m, int *d_out);
 // context's max_grid.
 inline int clamp_grid(const apspie_context *ctx, int grid) {
   return (ctx->max_grid > 0 && ctx->max_grid < grid) ? ctx->max_grid : grid;
+}
+
+// Grid of a persistent launch with a blocks-per-SM choice (0: the
+// occupancy-sized grid), capped by the context's max_grid.
+inline int persistent_grid(const apspie_context *ctx, int occ_grid, int blocks_per_sm) {
+  int g = occ_grid;
+  if (blocks_per_sm > 0 && g > blocks_per_sm * ctx->num_sms) g = blocks_per_sm * ctx->num_sms;
+  return clamp_grid(ctx, g);
 }
 }  // namespace apspie

@@ -182,7 +182,7 @@ __global__ void radix_digit_offsets(unsigned long long *ghist, int npass) {
 constexpr unsigned kLookbackSpinLimit = 1u << 20;
 
 template <typename K, typename V>
-__global__ void __launch_bounds__(kSortThreads)
+__global__ void __launch_bounds__(kSortThreads, 3)
 radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, long long n,
                int pass, const unsigned long long *goff, unsigned long long *status,
                unsigned *tile_counter, int *err, int *gaveup) {
@@ -198,6 +198,10 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
   __shared__ unsigned long long s_scan[33];
   __shared__ unsigned s_tile;
   __shared__ int s_withhold;
+  // the tile's values, copied in by cp.async while the keys are ranked
+  // (dynamic: kSortTile values when the sort has values, else none)
+  extern __shared__ __align__(16) unsigned char sort_dyn[];
+  V *svin = reinterpret_cast<V *>(sort_dyn);
   const int lane = lane_id(), w = warp_in_block();
   const int shift = pass * kRadixBits;
   const unsigned long long tag = (unsigned long long)(pass + 1) << 40;
@@ -213,9 +217,26 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
   const unsigned tile = s_tile;
   const long long tbase = (long long)tile * kSortTile;
   const int tlen = (int)min((long long)kSortTile, n - tbase);
+  // Values [0, vdone) of the tile are copied to shared memory in the
+  // background, 16 bytes a copy, when they start on a 16-byte boundary; the
+  // rest (a ragged end, or an unaligned array) are loaded when placed.
+  int vdone = 0;
+  if (vals_in && (reinterpret_cast<uintptr_t>(vals_in + tbase) & 15u) == 0) {
+    constexpr int kPer = 16 / (int)sizeof(V);
+    const int nchunk = tlen / kPer;
+    vdone = nchunk * kPer;
+    const unsigned sbase = (unsigned)__cvta_generic_to_shared(svin);
+    for (int c = threadIdx.x; c < nchunk; c += kSortThreads)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sbase + 16u * c),
+                   "l"(vals_in + tbase + (long long)c * kPer)
+                   : "memory");
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
   // this warp's slice of the tile: kSortItems rounds of 32 consecutive keys
   const int wofs = w * 32 * kSortItems;
-  unsigned pos[kSortItems], dig[kSortItems];
+  // per key its rank (then its tile position); its digit is recomputed
+  // from the key where needed (registers for three blocks per SM)
+  unsigned pos[kSortItems];
   K kv[kSortItems];
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
@@ -235,7 +256,6 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
     }
     prev = __shfl_sync(kFull, prev, leader);
     pos[i] = prev + __popc(peers & ((1u << lane) - 1u));
-    dig[i] = d;
     __syncwarp();
   }
   __syncthreads();
@@ -286,7 +306,7 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
     if (wofs + i * 32 + lane < tlen) {
-      const unsigned dd = dig[i];
+      const unsigned dd = (unsigned)(kv[i] >> shift) & (kRadix - 1);
       pos[i] += whist[w][dd];
       skeys[pos[i]] = kv[i];
       sdig[pos[i]] = (unsigned char)dd;
@@ -301,12 +321,13 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
     if (at < (unsigned long long)n) keys_out[at] = skeys[t];
   }
   if (vals_in) {  // keys-only sorts pass no values
+    if (vdone > 0) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     V *svals = reinterpret_cast<V *>(skeys);
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i) {
       const int t = wofs + i * 32 + lane;
-      if (t < tlen) svals[pos[i]] = vals_in[tbase + t];
+      if (t < tlen) svals[pos[i]] = t < vdone ? svin[t] : vals_in[tbase + t];
     }
     __syncthreads();
     for (int t = threadIdx.x; t < tlen; t += kSortThreads) {
@@ -385,10 +406,14 @@ int device_radix_sort(apspie_context *ctx, K *ka, V *va, K *kb, V *vb, long long
   if (rc) return rc;
   K *kin = ka, *kout = kb;
   V *vin = va, *vout = vb;
+  const size_t vdyn = va ? sizeof(V) * kSortTile : 0;
+  if (vdyn)
+    cudaFuncSetAttribute(radix_onesweep<K, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)vdyn);
   for (int p = 0; p < npass; ++p) {
-    radix_onesweep<K, V><<<(unsigned)tiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, p,
-                                                                   ghist, status, counters + p,
-                                                                   err, (int *)(counters + 15));
+    radix_onesweep<K, V><<<(unsigned)tiles, kSortThreads, vdyn, st>>>(kin, vin, kout, vout, n, p,
+                                                                      ghist, status, counters + p,
+                                                                      err, (int *)(counters + 15));
     rc = check_launch(ctx, "radix_onesweep");
     if (rc) return rc;
     std::swap(kin, kout);

@@ -6,8 +6,10 @@
 // (apspie_server_submit returns at once), and a worker thread turns the queue
 // into batches:
 //   * admission: a query's device state (its result row plus its share of the
-//     traversal scratch) is charged against a byte budget; queries wait in
-//     arrival order until the budget allows them in;
+//     traversal scratch) is charged against a byte budget and against the
+//     device's free memory (read with cudaMemGetInfo when a batch forms and
+//     after each group completes, less a 2 GiB reserve); queries wait in
+//     arrival order until both allow them in;
 //   * coalescing: the admitted BFS and SSSP queries of one (graph, kind) form
 //     a group, run by ONE apspie_batch_run (multi-source frontier matrix), or
 //     by the single-source kernel when the group has one query (or, on the
@@ -159,6 +161,11 @@ struct apspie_server {
   Slot slots[2];
   bool any_deep = false;
   bool warming = false;  // add_graph is warming the lanes: the worker launches nothing
+  // admission also against the device's free memory: the free bytes seen at
+  // the last reading and the bytes admitted since then (their buffers may not
+  // exist yet); re-read when a batch forms and after groups complete
+  size_t free_at_read = 0, admitted_since_read = 0;
+  bool free_known = false;
   int fail_next_kind = -1;  // test hook: the next group of this kind fails
   int max_pending = 1 << 20;
   // MIS priorities per (graph, seed), on the device
@@ -295,6 +302,22 @@ int probe_levels(int device, const GraphEntry &g, int *levels) {
   return st;
 }
 
+// Free device memory kept out of admission for the library's workspaces,
+// result rows and staging (they grow after admission).
+constexpr size_t kFreeReserve = size_t(2) << 30;
+
+// Reads the device's free memory (caller holds s->mu).
+void refresh_free_locked(apspie_server *s) {
+  size_t fr = 0, total = 0;
+  if (cudaMemGetInfo(&fr, &total) == cudaSuccess) {
+    s->free_at_read = fr;
+    s->admitted_since_read = 0;
+    s->free_known = true;
+  } else {
+    cudaGetLastError();
+  }
+}
+
 // Completes the requests of a finished group: results to the callers'
 // buffers, latencies, budget release, the group's cost estimate.
 void finish_group(apspie_server *s, Slot &sl, Group &g) {
@@ -319,6 +342,8 @@ void finish_group(apspie_server *s, Slot &sl, Group &g) {
     ++s->completed;
   }
   g.done = true;
+  // memory the group's work used may be free again
+  refresh_free_locked(s);
   s->cv.notify_all();
 }
 
@@ -597,12 +622,21 @@ void worker_main(apspie_server *s) {
         s->cv.wait_for(lock, std::chrono::microseconds(any_busy ? 20 : 2000));
         continue;
       }
-      // admit in arrival order while the budget allows
+      // admit in arrival order while the state budget and the device's
+      // free memory (less a reserve for the library's own buffers) allow
+      refresh_free_locked(s);
+      const size_t free_cap = s->free_known && s->free_at_read > kFreeReserve
+                                  ? s->free_at_read - kFreeReserve
+                                  : 0;
       while (!s->pending.empty() && (int)batch.size() < s->max_batch) {
         Request *r = s->pending.front();
-        if (s->in_flight + r->bytes > s->budget && !(s->in_flight == 0 && batch.empty())) break;
+        const bool first = s->in_flight == 0 && batch.empty();
+        if (!first && (s->in_flight + r->bytes > s->budget ||
+                       (s->free_known && s->admitted_since_read + r->bytes > free_cap)))
+          break;
         s->pending.pop_front();
         s->in_flight += r->bytes;
+        s->admitted_since_read += r->bytes;
         batch.push_back(r);
       }
     }

@@ -28,7 +28,11 @@
 //   3. the numeric pass accumulates in double (so the float result is the
 //      correctly rounded exact sum up to double error); warp rows compact
 //      their table and emit by rank in column order.
-// Tables are at most half full, probing is linear and every insert succeeds
+// The bin limits above are those of table load 2 (every table at most half
+// full); at load 4 (apspie_ctx_set_tuning, picked per matrix pair by
+// apspie_autotune_spgemm) each limit is halved and tables are sized to four
+// times their entries, and the warp bin's limit can be lowered so that more
+// rows get a 128-thread block.  Probing is linear and every insert succeeds
 // (nothing is dropped).  Explicit zeros (cancellation) stay in the structure,
 // as the reference's insert keeps every touched key.
 #include <cuda_runtime.h>
@@ -50,12 +54,14 @@ constexpr int kBlockTable = 16384;
 constexpr int kSpgThreads = 512;
 constexpr int kWarpsPerBlockSmall = 4;
 constexpr int kEmpty = INT_MAX;
+constexpr int kLbsPer = 4;  // products per thread per step of for_each_product_lbs
 
 __device__ __forceinline__ unsigned hash_col(int j) { return (unsigned)j * 0x9E3779B1u; }
 
-__device__ __forceinline__ int table_bits(long long prod, int cap_bits) {
+// log2 of a table of at least load x n slots (load 2 or 4), at most 2^cap_bits
+__device__ __forceinline__ int table_bits(long long n, int cap_bits, int load) {
   int b = 5;
-  while ((1ll << b) < 2 * prod && b < cap_bits) ++b;
+  while ((1ll << b) < load * n && b < cap_bits) ++b;
   return b;
 }
 
@@ -127,11 +133,28 @@ constexpr int kMid1MaxProd = 1024;
 constexpr int kMid2MaxProd = 4096;
 constexpr int kN1MaxNnz = 512, kN2MaxNnz = 1024, kN3MaxNnz = 2048;
 
+// Row-bin limits of one SpGEMM.  At table load 2 they are the constants
+// above (every table at most half full); at load 4 each is halved, so a row
+// goes to the next larger table and every table is at most a quarter full.
+// The warp bin's limit may be lowered further (rows then go to the 128-thread
+// mid tables).
+struct BinLimits {
+  int warp, mid1, mid2, block;  // symbolic: products per row
+  int n1, n2, n3;               // numeric: outputs per row
+};
+
+BinLimits bin_limits(int load, int warp_max_prod) {
+  const int d = load >= 4 ? 2 : 1;
+  return BinLimits{std::min(warp_max_prod, kWarpRowMaxProd / d), kMid1MaxProd / d,
+                   kMid2MaxProd / d, kBlockRowMaxProd / d, kN1MaxNnz / d, kN2MaxNnz / d,
+                   kN3MaxNnz / d};
+}
+
 // Device-side counters of one SpGEMM, read back by the host in one copy.
 struct SpgState {
   unsigned n[kNumBins];
   unsigned maxc;  // largest output row of bin kBinN5
-  unsigned pad;
+  unsigned maxp;  // most products of a kBinN5 row longer than one staging window
   long long total;  // nnz(C)
 };
 
@@ -147,18 +170,18 @@ __device__ __forceinline__ unsigned warp_bin_slot(unsigned *counters, int b) {
 }
 
 __global__ void bin_rows(int m, const long long *prod, int *lists, SpgState *st, int *cnt,
-                         bool bitmap) {
+                         bool bitmap, BinLimits lim) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
     long long p = prod[i];
     if (p == 0) {
       cnt[i] = 0;
       continue;
     }
-    int b = p <= kWarpRowMaxProd ? kBinWarp
-            : p <= kMid1MaxProd  ? kBinMid1
-            : p <= kMid2MaxProd  ? kBinMid2
-            : (bitmap || p <= kBlockRowMaxProd) ? kBinBlock
-                                                : kBinDense;
+    int b = p <= lim.warp ? kBinWarp
+            : p <= lim.mid1 ? kBinMid1
+            : p <= lim.mid2 ? kBinMid2
+            : (bitmap || p <= lim.block) ? kBinBlock
+                                         : kBinDense;
     lists[(size_t)b * m + warp_bin_slot(st->n, b)] = i;
   }
 }
@@ -320,11 +343,14 @@ __device__ __forceinline__ void for_each_product_lbs(int i, const int *__restric
                                                      const int *__restrict__ Bind,
                                                      const float *__restrict__ Bval, int *s_off,
                                                      int *s_bs, float *s_av, F f) {
-  constexpr int CAP = 2 * TPB;
+  // kLbsPer products per thread per step: the owner map and its max-scan
+  // (five block barriers) are paid once per kLbsPer * TPB products
+  constexpr int CAP = kLbsPer * TPB;
   __shared__ int s_om[CAP];
   __shared__ int sw[33];
   const int a0 = __ldg(Aptr + i), a1 = __ldg(Aptr + i + 1);
   const int tid = threadIdx.x;
+  int pb = 0;  // products of the row before this chunk of A entries
   for (int c0 = a0; c0 < a1; c0 += TPB) {
     const int a = c0 + tid;
     int bs = 0, d = 0;
@@ -342,30 +368,37 @@ __device__ __forceinline__ void for_each_product_lbs(int i, const int *__restric
     s_av[tid] = av;
     for (int w0 = 0; w0 < total; w0 += CAP) {
       const int wn = min(CAP, total - w0);
-      s_om[tid] = -1;
-      s_om[tid + TPB] = -1;
+#pragma unroll
+      for (int h = 0; h < kLbsPer; ++h) s_om[tid + h * TPB] = -1;
       __syncthreads();
       if (d > 0) {
         if (excl >= w0 && excl < w0 + wn) s_om[excl - w0] = tid;
         else if (excl < w0 && excl + d > w0) s_om[0] = tid;
       }
       __syncthreads();
-      const int v0 = s_om[2 * tid], v1 = max(v0, s_om[2 * tid + 1]);
-      const int pre = block_excl_max<TPB>(v1, sw);
-      s_om[2 * tid] = max(pre, v0);
-      s_om[2 * tid + 1] = max(pre, v1);
+      int run[kLbsPer];
+#pragma unroll
+      for (int h = 0; h < kLbsPer; ++h) {
+        run[h] = s_om[kLbsPer * tid + h];
+        if (h) run[h] = max(run[h], run[h - 1]);
+      }
+      const int pre = block_excl_max<TPB>(run[kLbsPer - 1], sw);
+#pragma unroll
+      for (int h = 0; h < kLbsPer; ++h) s_om[kLbsPer * tid + h] = max(pre, run[h]);
       __syncthreads();
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      for (int h = 0; h < kLbsPer; ++h) {
         const int q = tid + h * TPB;
         if (q < wn) {
           const int o = s_om[q];
           const int b = s_bs[o] + (w0 + q - s_off[o]);
-          f(__ldg(Bind + b), (double)s_av[o] * (double)(Bval ? __ldg(Bval + b) : 1.0f));
+          f(__ldg(Bind + b), (double)s_av[o] * (double)(Bval ? __ldg(Bval + b) : 1.0f),
+            pb + w0 + q);
         }
       }
       __syncthreads();
     }
+    pb += total;
     __syncthreads();
   }
 }
@@ -436,7 +469,7 @@ spgemm_warp_rows(const int *list, const unsigned *nlist, const long long *prod,
                  const int *__restrict__ Aptr, const int *__restrict__ Aind,
                  const float *__restrict__ Aval, const int *__restrict__ Bptr,
                  const int *__restrict__ Bind, const float *__restrict__ Bval, int *cnt,
-                 const int *Cptr, int *Cind, float *Cval) {
+                 const int *Cptr, int *Cind, float *Cval, int load) {
   __shared__ int s_keys[kWarpsPerBlockSmall][kWarpTable];
   __shared__ double s_vals[NUMERIC ? kWarpsPerBlockSmall : 1][NUMERIC ? kWarpTable : 1];
   __shared__ int s_off[kWarpsPerBlockSmall][32], s_bs[kWarpsPerBlockSmall][32];
@@ -448,7 +481,7 @@ spgemm_warp_rows(const int *list, const unsigned *nlist, const long long *prod,
   for (unsigned r = blockIdx.x * kWarpsPerBlockSmall + w; r < nrows;
        r += gridDim.x * kWarpsPerBlockSmall) {
     int i = list[r];
-    int bits = table_bits(prod[i], 9);
+    int bits = table_bits(prod[i], 9, load);
     int T = 1 << bits;
     for (int t = lane; t < T; t += 32) {
       keys[t] = kEmpty;
@@ -511,7 +544,7 @@ spgemm_block_rows(const int *list, const unsigned *nlist, const long long *prod,
                   const int *__restrict__ Aptr, const int *__restrict__ Aind,
                   const float *__restrict__ Aval, const int *__restrict__ Bptr,
                   const int *__restrict__ Bind, const float *__restrict__ Bval, int *cnt,
-                  const int *Cptr, int *Cind, float *Cval, int ncols) {
+                  const int *Cptr, int *Cind, float *Cval, int ncols, int load) {
   extern __shared__ __align__(16) unsigned char dyn[];
   double *vals = NUMERIC ? (double *)dyn : nullptr;
   int *keys = (int *)(dyn + (NUMERIC ? sizeof(double) * kBlockTable : 0));
@@ -521,7 +554,7 @@ spgemm_block_rows(const int *list, const unsigned *nlist, const long long *prod,
   const unsigned nrows = *nlist;
   for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
     int i = list[r];
-    int bits = table_bits(prod[i], 14);
+    int bits = table_bits(prod[i], 14, load);
     int T = 1 << bits;
     for (int t = threadIdx.x; t < T; t += blockDim.x) {
       keys[t] = kEmpty;
@@ -531,7 +564,7 @@ spgemm_block_rows(const int *list, const unsigned *nlist, const long long *prod,
     __syncthreads();
     int fresh_count = 0;
     for_each_product_lbs<kSpgThreads>(i, Aptr, Aind, Aval, Bptr, Bind, Bval, s_off, s_bs, s_av,
-                            [&](int j, double v) {
+                            [&](int j, double v, int) {
                               bool fresh;
                               int h = table_insert(keys, bits, j, &fresh);
                               fresh_count += fresh;
@@ -622,7 +655,7 @@ spgemm_mid_rows(const int *list, const unsigned *nlist, const long long *prod,
                 const int *__restrict__ Aptr, const int *__restrict__ Aind,
                 const float *__restrict__ Aval, const int *__restrict__ Bptr,
                 const int *__restrict__ Bind, const float *__restrict__ Bval, int *cnt,
-                const int *Cptr, int *Cind, float *Cval, int ncols) {
+                const int *Cptr, int *Cind, float *Cval, int ncols, int load) {
   constexpr int T = 1 << TBITS;
   extern __shared__ __align__(16) unsigned char dyn[];
   // numeric: vals double[T] | keys int[T] | skeys int[T/2] | svals float[T/2]
@@ -640,7 +673,7 @@ spgemm_mid_rows(const int *list, const unsigned *nlist, const long long *prod,
     const int i = list[r];
     const int base = NUMERIC ? Cptr[i] : 0;
     const int n = NUMERIC ? Cptr[i + 1] - base : 0;
-    const int bits = table_bits(NUMERIC ? (long long)n : prod[i], TBITS);
+    const int bits = table_bits(NUMERIC ? (long long)n : prod[i], TBITS, load);
     const int Tn = 1 << bits;
     for (int t = tid; t < Tn; t += TPB) {
       keys[t] = kEmpty;
@@ -652,7 +685,7 @@ spgemm_mid_rows(const int *list, const unsigned *nlist, const long long *prod,
     __syncthreads();
     int fresh_count = 0;
     for_each_product_lbs<TPB>(i, Aptr, Aind, Aval, Bptr, Bind, Bval, s_off, s_bs, s_av,
-                            [&](int j, double v) {
+                            [&](int j, double v, int) {
                               bool fresh;
                               const int h = table_insert(keys, bits, j, &fresh);
                               fresh_count += fresh;
@@ -742,7 +775,7 @@ spgemm_dense_rows(const int *list, const unsigned *nlist, int n,
   for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
     int i = list[r];
     for_each_product_lbs<kSpgThreads>(i, Aptr, Aind, Aval, Bptr, Bind, Bval, s_off, s_bs, s_av,
-                            [&](int j, double v) {
+                            [&](int j, double v, int) {
                               unsigned bit = 1u << (j & 31);
                               if (!(__ldcg(bits + (j >> 5)) & bit)) atomicOr(bits + (j >> 5), bit);
                               if (NUMERIC) atomicAdd(vals + j, v);
@@ -787,9 +820,21 @@ spgemm_dense_rows(const int *list, const unsigned *nlist, int n,
 // value ever goes through a global atomic.  Staging values are cleared as
 // they are emitted and the bits after the last window, so each row starts
 // clean.
+// With gbm (symbolic: store; numeric: load), the symbolic pass keeps each
+// row's finished bitmap in global memory at slot r of its bin (bslot[i] = r)
+// and the numeric pass of a row of more than kStageSmem outputs (always a
+// bitmap row of the symbolic phase) loads it instead of setting the bits
+// again.  With sp_pos / sp_val (numeric, rows longer than one window), the
+// first window's pass also records every product's position and value in
+// the block's spill region of sp_cap entries, and the later windows stream
+// that list instead of gathering the products again.
 constexpr int kStageSmem = 4096;     // 512-thread numeric rows: nnz(C(i,:)) <= this
 constexpr int kStageBig = 16384;     // 1024-thread numeric rows: window of this many
 constexpr int kBitmapMaxWords = 8192;
+// device memory the symbolic pass may keep its bitmap rows' bitmaps in, and
+// the numeric pass its spilled products in (above: recomputed / re-gathered)
+constexpr size_t kStoredBitmapBudget = size_t(1) << 30;
+constexpr size_t kSpillBudget = size_t(1) << 30;
 
 template <int MODE, int TPB>
 __global__ void __launch_bounds__(TPB, TPB <= 512 ? 2 : 1)
@@ -797,7 +842,8 @@ spgemm_bitmap_rows(const int *list, const unsigned *nlist, int W,
                    const int *__restrict__ Aptr, const int *__restrict__ Aind,
                    const float *__restrict__ Aval, const int *__restrict__ Bptr,
                    const int *__restrict__ Bind, const float *__restrict__ Bval, int *cnt,
-                   const int *Cptr, int *Cind, float *Cval, int scap) {
+                   const int *Cptr, int *Cind, float *Cval, int scap, unsigned *gbm,
+                   int *bslot, const long long *prod, int *sp_pos, double *sp_val, int sp_cap) {
   extern __shared__ __align__(16) unsigned char dyn[];
   unsigned *bits = (unsigned *)dyn;
   int *woff = (int *)(bits + W);
@@ -817,20 +863,29 @@ spgemm_bitmap_rows(const int *list, const unsigned *nlist, int W,
   const unsigned nrows = *nlist;
   for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
     const int i = list[r];
-    // bits only: runs of consecutive products per thread measured faster
-    // here than the load-balanced search (one array of B per product)
-    for_each_product<false, true>(i, Aptr, Aind, nullptr, Bptr, Bind, nullptr, s_off, s_bs, s_av,
-                            [&](int j, double) {
-                              const unsigned bit = 1u << (j & 31);
-                              if (!(bits[j >> 5] & bit)) atomicOr(bits + (j >> 5), bit);
-                            });
+    if (MODE == 1 && gbm) {
+      // the symbolic pass's bitmap of this row
+      const unsigned *src = gbm + (size_t)bslot[i] * W;
+      for (int w = tid; w < W; w += TPB) bits[w] = __ldcg(src + w);
+    } else {
+      // bits only: runs of consecutive products per thread measured faster
+      // here than the load-balanced search (one array of B per product)
+      for_each_product<false, true>(i, Aptr, Aind, nullptr, Bptr, Bind, nullptr, s_off, s_bs,
+                                    s_av, [&](int j, double) {
+                                      const unsigned bit = 1u << (j & 31);
+                                      if (!(bits[j >> 5] & bit)) atomicOr(bits + (j >> 5), bit);
+                                    });
+    }
     __syncthreads();
     if (MODE == 0) {
       int c = 0;
+      unsigned *dst = gbm ? gbm + (size_t)r * W : nullptr;
       for (int w = tid; w < W; w += TPB) {
         c += __popc(bits[w]);
+        if (dst) __stcg(dst + w, bits[w]);
         bits[w] = 0u;
       }
+      if (gbm && tid == 0) bslot[i] = (int)r;
       c = warp_sum(c);
       if (lane == 0) s_wt[wi] = c;
       __syncthreads();
@@ -865,15 +920,31 @@ spgemm_bitmap_rows(const int *list, const unsigned *nlist, int W,
     // equals the popcount unless A or B changed structure in between)
     const int base = Cptr[i];
     const int len = Cptr[i + 1] - base;
+    const int np = (int)prod[i];
+    // later windows stream the first window's spilled (position, value) list
+    const bool spill = sp_pos != nullptr && len > scap && np <= sp_cap;
+    int *my_pos = spill ? sp_pos + (size_t)blockIdx.x * sp_cap : nullptr;
+    double *my_val = spill ? sp_val + (size_t)blockIdx.x * sp_cap : nullptr;
     for (int p0 = 0; p0 < len; p0 += scap) {
       const int p1 = min(len, p0 + scap);
-      for_each_product_lbs<TPB>(i, Aptr, Aind, Aval, Bptr, Bind, Bval, s_off, s_bs, s_av,
-                              [&](int j, double v) {
-                                const int w = j >> 5;
-                                const int pos =
-                                    woff[w] + __popc(bits[w] & ((1u << (j & 31)) - 1u));
-                                if (pos >= p0 && pos < p1) atomicAdd(stage + (pos - p0), v);
-                              });
+      if (p0 == 0 || !spill) {
+        for_each_product_lbs<TPB>(i, Aptr, Aind, Aval, Bptr, Bind, Bval, s_off, s_bs, s_av,
+                                  [&](int j, double v, int q) {
+                                    const int w = j >> 5;
+                                    const int pos =
+                                        woff[w] + __popc(bits[w] & ((1u << (j & 31)) - 1u));
+                                    if (spill) {
+                                      __stcg(my_pos + q, pos);
+                                      __stcg(my_val + q, v);
+                                    }
+                                    if (pos >= p0 && pos < p1) atomicAdd(stage + (pos - p0), v);
+                                  });
+      } else {
+        for (int q = tid; q < np; q += TPB) {
+          const int pos = __ldcg(my_pos + q);
+          if (pos >= p0 && pos < p1) atomicAdd(stage + (pos - p0), __ldcg(my_val + q));
+        }
+      }
       __syncthreads();
       for (int w = tid; w < W; w += TPB) {
         unsigned b = bits[w];
@@ -899,7 +970,8 @@ spgemm_bitmap_rows(const int *list, const unsigned *nlist, int W,
 
 // Re-bins the rows of the mid and block bins for the numeric phase by
 // their exact output size (cnt, from the symbolic phase).
-__global__ void rebin_rows(int m, int *lists, SpgState *st, const int *cnt, bool bitmap) {
+__global__ void rebin_rows(int m, int *lists, SpgState *st, const int *cnt, bool bitmap,
+                           BinLimits lim, const long long *prod) {
   const unsigned n1 = st->n[kBinMid1], n2 = st->n[kBinMid2], n3 = st->n[kBinBlock];
   const unsigned n = n1 + n2 + n3;
   for (unsigned r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
@@ -907,13 +979,16 @@ __global__ void rebin_rows(int m, int *lists, SpgState *st, const int *cnt, bool
     const unsigned k = r < n1 ? r : (r < n1 + n2 ? r - n1 : r - n1 - n2);
     const int i = lists[(size_t)src * m + k];
     const int c = cnt[i];
-    const int b = c <= kN1MaxNnz ? kBinN1
-                  : c <= kN2MaxNnz ? kBinN2
-                  : c <= kN3MaxNnz ? kBinN3
+    const int b = c <= lim.n1   ? kBinN1
+                  : c <= lim.n2 ? kBinN2
+                  : c <= lim.n3 ? kBinN3
                   : (!bitmap || c <= kStageSmem) ? kBinN4
                                                  : kBinN5;
     lists[(size_t)b * m + warp_bin_slot(st->n, b)] = i;
-    if (b == kBinN5) atomicMax(&st->maxc, (unsigned)c);
+    if (b == kBinN5) {
+      atomicMax(&st->maxc, (unsigned)c);
+      if (c > kStageBig) atomicMax(&st->maxp, (unsigned)prod[i]);
+    }
   }
 }
 
@@ -971,11 +1046,14 @@ int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr
   const bool bitmap = n > 0 && (long long)n <= ctx->spgemm_bitmap_max_cols &&
                       bwords <= kBitmapMaxWords;
   auto L = [&](int b) { return lists + (size_t)b * m; };
-  cudaMemsetAsync(sst, 0, sizeof(SpgState), st);
+  const int load = ctx->spgemm_table_load;
+  const BinLimits lim = bin_limits(load, ctx->spgemm_warp_max_prod);
+  int rc0 = check_cuda(ctx, cudaMemsetAsync(sst, 0, sizeof(SpgState), st), "spgemm bins");
+  if (rc0) return rc0;
   if (m > 0) {
     row_products<<<gridsz(ctx, (long long)m * 32, 256), 256, 0, st>>>(m, A->d_ptr, A->d_ind,
                                                                       B->d_ptr, prod);
-    bin_rows<<<gridsz(ctx, m, 256), 256, 0, st>>>(m, prod, lists, sst, cnt, bitmap);
+    bin_rows<<<gridsz(ctx, m, 256), 256, 0, st>>>(m, prod, lists, sst, cnt, bitmap, lim);
     int rc = check_launch(ctx, "spgemm bin", 2);
     if (rc) return rc;
   }
@@ -1010,6 +1088,19 @@ int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr
     zero_doubles<<<gridsz(ctx, (long long)n * dense_blocks, 256), 256, 0, st>>>(
         (size_t)n * dense_blocks, gvals);
   }
+  // the bitmap rows keep their bitmaps for the numeric phase when they fit
+  unsigned *gbm = nullptr;
+  int *bslot = nullptr;
+  if (bitmap && hb.n[kBinBlock] > 0 &&
+      (size_t)hb.n[kBinBlock] * bwords * sizeof(unsigned) <= kStoredBitmapBudget) {
+    gbm = (unsigned *)workspace(ctx, kSlotSpgStoredBits,
+                                (size_t)hb.n[kBinBlock] * bwords * sizeof(unsigned));
+    bslot = (int *)workspace(ctx, kSlotSpgBitmapSlot, sizeof(int) * ((size_t)m + 1));
+    if (!gbm || !bslot) {  // not kept: the numeric phase sets the bits again
+      gbm = nullptr;
+      bslot = nullptr;
+    }
+  }
   // ---- symbolic ----
   const unsigned *nb = sst->n;
   int launches = 0;
@@ -1017,33 +1108,33 @@ int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr
     spgemm_warp_rows<false><<<gridsz(ctx, hb.n[kBinWarp], kWarpsPerBlockSmall, 64),
                               32 * kWarpsPerBlockSmall, 0, st>>>(
         L(kBinWarp), nb + kBinWarp, prod, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind,
-        nullptr, cnt, nullptr, nullptr, nullptr);
+        nullptr, cnt, nullptr, nullptr, nullptr, load);
     ++launches;
   }
   if (hb.n[kBinMid1]) {
     spgemm_mid_rows<false, 128, 11><<<gridsz(ctx, hb.n[kBinMid1], 1, 16), 128,
                                       mid_smem<128, 11, false>(), st>>>(
         L(kBinMid1), nb + kBinMid1, prod, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind,
-        nullptr, cnt, nullptr, nullptr, nullptr, n);
+        nullptr, cnt, nullptr, nullptr, nullptr, n, load);
     ++launches;
   }
   if (hb.n[kBinMid2]) {
     spgemm_mid_rows<false, 256, 13><<<gridsz(ctx, hb.n[kBinMid2], 1, 6), 256,
                                       mid_smem<256, 13, false>(), st>>>(
         L(kBinMid2), nb + kBinMid2, prod, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind,
-        nullptr, cnt, nullptr, nullptr, nullptr, n);
+        nullptr, cnt, nullptr, nullptr, nullptr, n, load);
     ++launches;
   }
   if (hb.n[kBinBlock] && bitmap) {
     spgemm_bitmap_rows<0, kSpgThreads><<<gridsz(ctx, hb.n[kBinBlock], 1, 4), kSpgThreads,
                                          (size_t)4 * bwords, st>>>(
         L(kBinBlock), nb + kBinBlock, bwords, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind,
-        nullptr, cnt, nullptr, nullptr, nullptr, 0);
+        nullptr, cnt, nullptr, nullptr, nullptr, 0, gbm, bslot, prod, nullptr, nullptr, 0);
     ++launches;
   } else if (hb.n[kBinBlock]) {
     spgemm_block_rows<false><<<gridsz(ctx, hb.n[kBinBlock], 1, 4), kSpgThreads, dyn_sym, st>>>(
         L(kBinBlock), nb + kBinBlock, prod, A->d_ptr, A->d_ind, nullptr, B->d_ptr, B->d_ind,
-        nullptr, cnt, nullptr, nullptr, nullptr, n);
+        nullptr, cnt, nullptr, nullptr, nullptr, n, load);
     ++launches;
   }
   if (nd) {
@@ -1064,7 +1155,7 @@ int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr
   }
   const unsigned nre = hb.n[kBinMid1] + hb.n[kBinMid2] + hb.n[kBinBlock];
   if (nre) {
-    rebin_rows<<<gridsz(ctx, nre, 256), 256, 0, st>>>(m, lists, sst, cnt, bitmap);
+    rebin_rows<<<gridsz(ctx, nre, 256), 256, 0, st>>>(m, lists, sst, cnt, bitmap, lim, prod);
     rc = check_launch(ctx, "rebin_rows");
     if (rc) return rc;
   }
@@ -1100,7 +1191,11 @@ int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr
   ctx->spgemm_plan_n = n;
   for (int b = 0; b < kNumBins; ++b) ctx->spgemm_plan_bins[b] = hs.n[b];
   ctx->spgemm_plan_bins[kNumBins] = hs.maxc;
+  ctx->spgemm_plan_bins[kNumBins + 1] = hs.maxp;
+  ctx->spgemm_plan_gbm = gbm;
+  ctx->spgemm_plan_bslot = bslot;
   ctx->spgemm_plan_words = bitmap ? bwords : 0;
+  ctx->spgemm_plan_load = load;
   *h_nnz = nnzC;
   return APSPIE_OK;
 }
@@ -1117,6 +1212,7 @@ int apspie_spgemm_numeric(apspie_ctx ctx, const apspie_csr *A, const apspie_csr 
   const unsigned *hn = ctx->spgemm_plan_bins;
   const int maxc = (int)hn[kNumBins];
   const int bwords = ctx->spgemm_plan_words;
+  const int load = ctx->spgemm_plan_load;
   // the symbolic phase's buffers (own slots, same sizes: no reallocation;
   // the dense accumulators are left cleared by every dense-row pass)
   auto *prod = (long long *)workspace(ctx, kSlotSpgProd, sizeof(long long) * ((size_t)m + 1));
@@ -1155,49 +1251,68 @@ int apspie_spgemm_numeric(apspie_ctx ctx, const apspie_csr *A, const apspie_csr 
     spgemm_warp_rows<true><<<gridsz(ctx, hn[kBinWarp], kWarpsPerBlockSmall, 32),
                              32 * kWarpsPerBlockSmall, 0, st>>>(
         L(kBinWarp), nb + kBinWarp, prod, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
-        B->d_val, cnt, Cptr, Cind, Cval);
+        B->d_val, cnt, Cptr, Cind, Cval, load);
     ++launches;
   }
   if (hn[kBinN1]) {
     spgemm_mid_rows<true, 128, 10><<<gridsz(ctx, hn[kBinN1], 1, 12), 128,
                                      mid_smem<128, 10, true>(), st>>>(
         L(kBinN1), nb + kBinN1, prod, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
-        B->d_val, cnt, Cptr, Cind, Cval, n);
+        B->d_val, cnt, Cptr, Cind, Cval, n, load);
     ++launches;
   }
   if (hn[kBinN2]) {
     spgemm_mid_rows<true, 128, 11><<<gridsz(ctx, hn[kBinN2], 1, 6), 128,
                                      mid_smem<128, 11, true>(), st>>>(
         L(kBinN2), nb + kBinN2, prod, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
-        B->d_val, cnt, Cptr, Cind, Cval, n);
+        B->d_val, cnt, Cptr, Cind, Cval, n, load);
     ++launches;
   }
   if (hn[kBinN3]) {
     spgemm_mid_rows<true, 256, 12><<<gridsz(ctx, hn[kBinN3], 1, 3), 256,
                                      mid_smem<256, 12, true>(), st>>>(
         L(kBinN3), nb + kBinN3, prod, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
-        B->d_val, cnt, Cptr, Cind, Cval, n);
+        B->d_val, cnt, Cptr, Cind, Cval, n, load);
     ++launches;
   }
   if (hn[kBinN4] && bwords) {
     spgemm_bitmap_rows<1, kSpgThreads><<<gridsz(ctx, hn[kBinN4], 1, 2), kSpgThreads,
                                          (size_t)8 * ((bwords + 1) & ~1) + 8 * kStageSmem, st>>>(
         L(kBinN4), nb + kBinN4, bwords, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
-        B->d_val, cnt, Cptr, Cind, Cval, kStageSmem);
+        B->d_val, cnt, Cptr, Cind, Cval, kStageSmem, nullptr, nullptr, prod, nullptr, nullptr,
+        0);
     ++launches;
   } else if (hn[kBinN4]) {
     spgemm_block_rows<true><<<gridsz(ctx, hn[kBinN4], 1, 1), kSpgThreads, dyn_num, st>>>(
         L(kBinN4), nb + kBinN4, prod, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
-        B->d_val, cnt, Cptr, Cind, Cval, n);
+        B->d_val, cnt, Cptr, Cind, Cval, n, load);
     ++launches;
   }
   if (hn[kBinN5]) {
-    // rows longer than kStageSmem: 1024 threads, windows of kStageBig
+    // rows longer than kStageSmem: 1024 threads, windows of kStageBig, the
+    // symbolic pass's bitmaps when it kept them; rows longer than one window
+    // spill their products' positions and values in the first window's pass
     const int scap = std::min(kStageBig, std::max(maxc, 1));
-    spgemm_bitmap_rows<1, 1024><<<gridsz(ctx, hn[kBinN5], 1, 1), 1024,
+    const int g5 = gridsz(ctx, hn[kBinN5], 1, 1);
+    const unsigned maxp = hn[kNumBins + 1];
+    int *sp_pos = nullptr;
+    double *sp_val = nullptr;
+    int sp_cap = 0;
+    if (maxp > 0 && (size_t)g5 * maxp * (sizeof(int) + sizeof(double)) <= kSpillBudget) {
+      sp_pos = (int *)workspace(ctx, kSlotSpgSpillPos, sizeof(int) * (size_t)g5 * maxp);
+      sp_val = (double *)workspace(ctx, kSlotSpgSpillVal, sizeof(double) * (size_t)g5 * maxp);
+      if (sp_pos && sp_val) {
+        sp_cap = (int)maxp;
+      } else {  // not spilled: every window gathers the products again
+        sp_pos = nullptr;
+        sp_val = nullptr;
+      }
+    }
+    spgemm_bitmap_rows<1, 1024><<<g5, 1024,
                                   (size_t)8 * ((bwords + 1) & ~1) + 8 * (size_t)scap, st>>>(
         L(kBinN5), nb + kBinN5, bwords, A->d_ptr, A->d_ind, A->d_val, B->d_ptr, B->d_ind,
-        B->d_val, cnt, Cptr, Cind, Cval, scap);
+        B->d_val, cnt, Cptr, Cind, Cval, scap, (unsigned *)ctx->spgemm_plan_gbm,
+        (int *)ctx->spgemm_plan_bslot, prod, sp_pos, sp_val, sp_cap);
     ++launches;
   }
   if (nd) {

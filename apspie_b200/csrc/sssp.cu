@@ -522,7 +522,8 @@ int sssp_run(apspie_context *ctx, int src, int64_t nnz, int m, const int *d_ptr,
   unsigned *xd = (unsigned *)(nf + mm);
   ctx->sssp_state = st;
   const bool pull3 = d_tptr != nullptr;
-  int grid = clamp_grid(ctx, pull3 ? sssp_grid<W, 3>(ctx) : sssp_grid<W, 2>(ctx));
+  int grid = persistent_grid(ctx, pull3 ? sssp_grid<W, 3>(ctx) : sssp_grid<W, 2>(ctx),
+                             ctx->sssp_blocks_per_sm);
   if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_sssp: occupancy query failed");
   int init_grid = std::min((m + 255) / 256, ctx->num_sms * 8);
   sssp_init<W><<<init_grid, 256, 0, ctx->stream>>>(m, src, d_dist, stamp, fstamp, xd, xw, d_ptr,

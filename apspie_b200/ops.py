@@ -5,7 +5,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-from ._native import BatchStats, BfsStats, Csr, Job, SsspStats, check, lib
+from ._native import BatchStats, BfsStats, Csr, Job, SsspStats, Tuning, check, lib
 
 
 class Context:
@@ -324,8 +324,9 @@ def spgemm_symbolic(ctx: Context, A, B):
 
 
 def spgemm_set_params(ctx: Context, bitmap_max_cols: int = 1 << 18):
-    """Rows with more than 256 products use a shared-memory column bitmap
-    when B has at most bitmap_max_cols columns (0: always hash tables)."""
+    """Rows with more than 4096 products (2048 at table load 4) use a
+    shared-memory column bitmap when B has at most bitmap_max_cols columns
+    (0: always hash tables)."""
     check(lib.apspie_spgemm_set_params(ctx.handle, int(bitmap_max_cols)), ctx.handle,
           "apspie_spgemm_set_params")
 
@@ -439,6 +440,15 @@ def batch_run(ctx: Context, jobs: list[dict], max_steps: int = 0):
     "sources": [...], optional "alpha", "beta"}.  Returns one int32 tensor of
     shape (len(sources), m) per job (SSSP: uint32 bits, 0xFFFFFFFF
     unreached)."""
+    arr, outs, _keep = _job_array(jobs)
+    check(lib.apspie_batch_run(ctx.handle, len(jobs), arr, int(max_steps)), ctx.handle,
+          "apspie_batch_run")
+    return outs
+
+
+def _job_array(jobs: list[dict]):
+    """The apspie_job array of a job list, the output tensors, and the host
+    source arrays the array points into (kept alive by the caller)."""
     import torch
     outs, keep = [], []
     arr = (Job * len(jobs))()
@@ -464,9 +474,7 @@ def batch_run(ctx: Context, jobs: list[dict], max_steps: int = 0):
             arr[i].d_stptr = C.c_void_p(sin[0].data_ptr())
             arr[i].d_stind = C.c_void_p(sin[1].data_ptr())
             arr[i].d_stw = C.c_void_p(sin[2].data_ptr())
-    check(lib.apspie_batch_run(ctx.handle, len(jobs), arr, int(max_steps)), ctx.handle,
-          "apspie_batch_run")
-    return outs
+    return arr, outs, keep
 
 
 def batch_set_params(ctx: Context, deep_blocks: int = 0, deep_concurrent: int = 48):
@@ -492,8 +500,89 @@ def batch_stats(ctx: Context) -> dict:
     return {"super_steps": s.super_steps, "frontier_edges": s.frontier_edges}
 
 
+TUNING_FIELDS = [f for f, _ in Tuning._fields_]
+
+
+def get_tuning(ctx: Context) -> dict:
+    """The context's per-graph choices (apspie_ctx_get_tuning)."""
+    t = Tuning()
+    check(lib.apspie_ctx_get_tuning(ctx.handle, C.byref(t)), ctx.handle, "apspie_ctx_get_tuning")
+    return {f: getattr(t, f) for f in TUNING_FIELDS}
+
+
+def set_tuning(ctx: Context, **kw) -> dict:
+    """Set some of the context's per-graph choices (the others keep their
+    values); returns the whole set."""
+    cur = get_tuning(ctx)
+    bad = set(kw) - set(cur)
+    if bad:
+        raise KeyError(f"unknown tuning fields: {sorted(bad)}")
+    cur.update(kw)
+    t = Tuning(**cur)
+    check(lib.apspie_ctx_set_tuning(ctx.handle, C.byref(t)), ctx.handle, "apspie_ctx_set_tuning")
+    return cur
+
+
+def reset_tuning(ctx: Context) -> dict:
+    """Back to the library defaults."""
+    return set_tuning(ctx, **DEFAULT_TUNING)
+
+
+DEFAULT_TUNING = {"bfs_alpha": 14, "bfs_beta": 24, "bfs_blocks_per_sm": 0,
+                  "sssp_blocks_per_sm": 0, "sssp_pull_alpha": 0, "batch_blocks_per_sm": 0,
+                  "batch_deep_blocks": 0, "spgemm_table_load": 2, "spgemm_warp_max_prod": 256,
+                  "spgemm_bitmap_max_cols": 1 << 18, "spmspv_sort_factor": 4.0}
+
+
+def autotune_sssp(ctx: Context, g, sources) -> dict:
+    """Pick and cache the persistent SSSP launch's blocks per SM and, when g
+    carries its weighted in-adjacency (sssp_prepare), the pull switch, on
+    uint32 weights."""
+    import torch
+    if g.w_u32 is None:
+        raise ValueError("graph has no u32 weights")
+    dist = torch.empty(g.m, dtype=torch.int32, device=g.ptr.device)
+    src = (C.c_int * len(sources))(*[int(s) for s in sources])
+    tin = g.extra.get("sssp_in", {}).get("u32")
+    tptr, tind, tw = tin if tin is not None else (None, None, None)
+    ms, cached = C.c_float(), C.c_int()
+    check(lib.apspie_autotune_sssp(ctx.handle, len(sources), src, int(g.nnz), int(g.m), _p(g.ptr),
+                                   _p(g.ind), _p(g.w_u32), _p(tptr), _p(tind), _p(tw), _p(dist),
+                                   C.byref(ms), C.byref(cached)), ctx.handle,
+          "apspie_autotune_sssp")
+    t = get_tuning(ctx)
+    return {"blocks_per_sm": t["sssp_blocks_per_sm"], "pull_alpha": t["sssp_pull_alpha"],
+            "ms_per_sssp": ms.value, "cached": bool(cached.value)}
+
+
+def autotune_spgemm(ctx: Context, A, B) -> dict:
+    """Pick and cache the SpGEMM table load, warp-row limit and long-row
+    accumulator for A * B ((m, n, ptr, ind, val) tuples as in spgemm)."""
+    a, b = _csr(*A), _csr(*B)
+    ms, cached = C.c_float(), C.c_int()
+    check(lib.apspie_autotune_spgemm(ctx.handle, C.byref(a), C.byref(b), C.byref(ms),
+                                     C.byref(cached)), ctx.handle, "apspie_autotune_spgemm")
+    t = get_tuning(ctx)
+    return {"table_load": t["spgemm_table_load"], "warp_max_prod": t["spgemm_warp_max_prod"],
+            "bitmap_max_cols": t["spgemm_bitmap_max_cols"], "ms": ms.value,
+            "cached": bool(cached.value)}
+
+
+def autotune_batch(ctx: Context, jobs: list[dict]) -> dict:
+    """Pick and cache the batched launch's blocks per SM and the deep-graph
+    sources' block share for this job list (runs batch_run on it)."""
+    arr, _outs, _keep = _job_array(jobs)
+    ms, cached = C.c_float(), C.c_int()
+    check(lib.apspie_autotune_batch(ctx.handle, len(jobs), arr, C.byref(ms), C.byref(cached)),
+          ctx.handle, "apspie_autotune_batch")
+    t = get_tuning(ctx)
+    return {"blocks_per_sm": t["batch_blocks_per_sm"], "deep_blocks": t["batch_deep_blocks"],
+            "ms": ms.value, "cached": bool(cached.value)}
+
+
 def autotune_bfs(ctx: Context, g, sources) -> dict:
-    """Pick and cache the BFS direction thresholds for graph g."""
+    """Pick and cache the BFS direction thresholds and the persistent
+    launch's blocks per SM for graph g."""
     import torch
     depth = torch.empty(g.m, dtype=torch.int32, device=g.ptr.device)
     src = (C.c_int * len(sources))(*[int(s) for s in sources])
@@ -503,7 +592,8 @@ def autotune_bfs(ctx: Context, g, sources) -> dict:
     check(lib.apspie_autotune_bfs(ctx.handle, len(sources), src, int(g.nnz), int(g.m), _p(g.ptr),
                                   _p(g.ind), _p(tptr), _p(tind), _p(depth), C.byref(a),
                                   C.byref(b), C.byref(ms)), ctx.handle, "apspie_autotune_bfs")
-    return {"alpha": a.value, "beta": b.value, "ms_per_bfs": ms.value}
+    return {"alpha": a.value, "beta": b.value, "ms_per_bfs": ms.value,
+            "blocks_per_sm": get_tuning(ctx)["bfs_blocks_per_sm"]}
 
 
 def autotune_spmspv(ctx: Context, g, val=None) -> float:

@@ -297,16 +297,22 @@ def sssp_leg(ctx, big, steps=20):
     ap.weights_f32(h, seed=SEED)
     g = h.to_device()
     srcs = ap.seeded_sources(h, steps, seed=3)
-    out = {"graph": f"R-MAT 20 directed, m={h.m}, nnz={h.nnz}"}
+    out = {"graph": f"R-MAT 20 directed, m={h.m}, nnz={h.nnz}",
+           "tuning": "per graph by apspie_autotune_sssp on 8 untimed sources (u32 weights; "
+                     "blocks per SM, pull switch when the in-adjacency is present)"}
+    tuned = _sssp_tune(ctx, g, ap.seeded_sources(h, 8, seed=77))
     for kind in ("u32", "f32"):
         for s in srcs[:3]:
             ap.sssp(ctx, g, s, weights=kind)
         out[kind] = _sssp_block(ctx, g, srcs, kind, h.m)
+        out[kind]["tuned"] = tuned
     del g
     if big.w_u32 is None:
         ap.weights_u32(big, seed=SEED)
     g22 = big.to_device()
+    tuned = _sssp_tune(ctx, g22, ap.seeded_sources(big, 8, seed=77))
     out["rmat22_sym_u32"] = _sssp_block(ctx, g22, ap.seeded_sources(big, 8, seed=3), "u32", big.m)
+    out["rmat22_sym_u32"]["tuned"] = tuned
     del g22
     g23 = ap.gen_rmat_device(ctx, 23, EDGE_FACTOR, seed=SEED)
     ap.weights_device(ctx, g23, seed=SEED)
@@ -314,9 +320,18 @@ def sssp_leg(ctx, big, steps=20):
     cand = np.flatnonzero(deg > 0)
     rng = np.random.default_rng(3)
     s23 = [int(x) for x in cand[rng.integers(len(cand), size=6)]]
+    tuned = _sssp_tune(ctx, g23, [int(x) for x in cand[rng.integers(len(cand), size=6)]])
     ap.sssp(ctx, g23, s23[0], weights="u32")
     out["rmat23_sym_u32"] = _sssp_block(ctx, g23, s23, "u32", g23.m)
+    out["rmat23_sym_u32"]["tuned"] = tuned
+    ap.set_tuning(ctx, sssp_blocks_per_sm=0, sssp_pull_alpha=0)
     return out
+
+
+def _sssp_tune(ctx, g, srcs):
+    import apspie_b200 as ap
+    t = ap.autotune_sssp(ctx, g, srcs)
+    return {"blocks_per_sm": t["blocks_per_sm"], "pull_alpha": t["pull_alpha"]}
 
 
 def _ev_ms(fn, reps=5):
@@ -368,6 +383,7 @@ def mis_tc_spgemm_leg(ctx):
     a = ap.gen_powerlaw(1 << 18, seed=SEED)
     t = lambda x: torch.from_numpy(x).cuda()
     A = (a.m, a.ncols, t(a.ptr), t(a.ind), t(a.w_f32))
+    tuned = ap.autotune_spgemm(ctx, A, A)
     cp, ci, cv = ap.spgemm(ctx, A, A)
     ms_call = _ev_ms(lambda: ap.spgemm(ctx, A, A), reps=3)
     # the two phases into preallocated C (no allocation inside the timing):
@@ -384,8 +400,13 @@ def mis_tc_spgemm_leg(ctx):
                                 "nnz_C": int(ci.numel()), "xmin": a.xmin,
                                 "hbm_gbs_alg": b_alg / (ms * 1e-3) / 1e9,
                                 "frac": b_alg / (ms * 1e-3) / 1e9 / hbm,
+                                "tuned": {k: tuned[k] for k in ("table_load", "warp_max_prod",
+                                                                "bitmap_max_cols")},
                                 "note": "ms = symbolic + numeric into preallocated C; "
-                                        "ms_call = ap.spgemm with C allocated per call"}
+                                        "ms_call = ap.spgemm with C allocated per call; "
+                                        "tuned = apspie_autotune_spgemm's pick for A * A"}
+    ap.set_tuning(ctx, spgemm_table_load=2, spgemm_warp_max_prod=256,
+                  spgemm_bitmap_max_cols=1 << 18)
     return out
 
 
@@ -431,6 +452,7 @@ def batched_leg(ctx, big):
     refs = []
     edges = plain_run(jobs, refs)
     ap.batch_run(ctx, jobs)
+    tuned = ap.autotune_batch(ctx, jobs)
     plain_ms, _ = timed(lambda: plain_run(jobs))
     batch_ms, outs = timed(lambda: ap.batch_run(ctx, jobs))
     st = ap.batch_stats(ctx)
@@ -459,6 +481,8 @@ def batched_leg(ctx, big):
             "speedup_vs_plain": plain_ms / batch_ms, "batched_ms": batch_ms,
             "plain_ms": plain_ms, "super_steps": st["super_steps"], "verified": verified,
             "per_graph": per_graph,
+            "tuned": {"blocks_per_sm": tuned["blocks_per_sm"], "deep_blocks": tuned["deep_blocks"],
+                      "picked_by": "apspie_autotune_batch on the same job list, untimed"},
             "timing": "CUDA events on the launching stream (plain: all single-source calls "
                       "back to back; batched: one apspie_batch_run, transposes included); "
                       "per_graph: each graph's two jobs in a launch of their own"}
@@ -706,11 +730,14 @@ def run_ours(args):
                                               "built once by apspie_bfs_prepare in %.1f ms "
                                               "outside the timed region" % prep_ms),
                            "switch_points": {"alpha": tune.get("alpha"), "beta": tune.get("beta"),
+                                             "blocks_per_sm": tune.get("blocks_per_sm"),
                                              "picked_by": "--switch" if args.switch else
                                              "defaults" if args.no_tune else
                                              "autotuner on 64 untimed sources (21 switch-point "
-                                             "candidates ranked on 32, the best 4 re-timed on "
-                                             "the other 32, two sweeps each)"}},
+                                             "candidates ranked on 32, the best 4 and the "
+                                             "reference point (32, 128) re-timed on the other "
+                                             "32, two sweeps each; then 3 / 2 / 1 blocks per SM "
+                                             "on all 64)"}},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "per_step_ms": {"min": min(per), "median": statistics.median(per), "max": max(per)},
@@ -747,7 +774,8 @@ def run_serving(args):
 
 def run_profile_case(args):
     """--profile-case NAME: run one workload of the MIS / TC / SpGEMM / batched
-    / SpMSpV / SpMV / push-pull SSSP (R-MAT 22, two sources) configurations
+    / SpMSpV / SpMV / push-pull SSSP (R-MAT 22, two sources) / pull-adjacency
+    sort (R-MAT 22) configurations
     three times and exit, for ncu captures of its kernels (no timing, no
     JSON)."""
     import torch
@@ -768,6 +796,13 @@ def run_profile_case(args):
         a = ap.gen_powerlaw(1 << 18, seed=SEED)
         A = (a.m, a.ncols, t(a.ptr), t(a.ind), t(a.w_f32))
         run = lambda: ap.spgemm(ctx, A, A)
+    elif case == "sort":
+        # the BFS pull-adjacency build of R-MAT 22: a 6-pass radix sort of
+        # 128.3 M (u64 key, i32 value) pairs (graph built on the host, so the
+        # first sort launches are this one's)
+        h = ap.gen_rmat(22, EDGE_FACTOR, seed=SEED)
+        g = h.to_device()
+        run = lambda: ap.bfs_prepare(ctx, g)
     elif case == "batch":
         h = ap.gen_rmat(20, EDGE_FACTOR, seed=SEED)
         ap.weights_u32(h, seed=SEED)

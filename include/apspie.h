@@ -306,7 +306,10 @@ int apspie_batch_get_stats(apspie_ctx ctx, apspie_batch_stats *out);
 /* ------------------------------------------------------------- serving ---
  * A query server over device-resident graphs (no reference counterpart).
  * Queries arrive at any time; a worker thread admits them in arrival order
- * while their device state fits state_budget_bytes, coalesces the admitted
+ * while their device state fits state_budget_bytes and the device's free
+ * memory (read when a batch forms and after each group completes, less a
+ * 2 GiB reserve; the first query of an idle server is always admitted),
+ * coalesces the admitted
  * BFS / SSSP queries by (graph, kind) into one apspie_batch_run launch, runs
  * MIS queries after it, and copies each result row into the caller's host
  * buffer.  Two batch slots (each its own context and stream) keep a new batch
@@ -382,12 +385,39 @@ int apspie_server_reset_stats(apspie_server_t s);
 int apspie_server_destroy(apspie_server_t s);
 
 /* ----------------------------------------------------------- autotuner ---
- * Measures the BFS direction thresholds on the given sample sources (a grid
+ * The reference hard-codes its launch shapes and table sizes (NTHREADS,
+ * TABLE_SIZE, partSize from an "aggro" factor: src/spgemm.cuh:15,
+ * src/spgemmKernel.cuh:9-26, test/spgemm/main.cu:362-377).  Here the
+ * data-dependent choices are context settings, measured per graph by the
+ * autotuners below and cached under a fingerprint of the graph (m, nnz,
+ * sampled row offsets; for SpGEMM of both operands, for a batch of every
+ * job's graph and source count): a graph seen again is not re-measured, the
+ * cached choice is applied to the context again. */
+typedef struct {
+  int32_t bfs_alpha, bfs_beta;     /* BFS switch points (alpha 0: never pull) */
+  int32_t bfs_blocks_per_sm;       /* persistent BFS launch, blocks per SM (0: as many as fit, 3) */
+  int32_t sssp_blocks_per_sm;      /* persistent SSSP launch (0: as many as fit) */
+  int32_t sssp_pull_alpha;         /* SSSP pull rounds (0: push only; see apspie_sssp_set_pull) */
+  int32_t batch_blocks_per_sm;     /* batched multi-source launch (0: as many as fit, 2) */
+  int32_t batch_deep_blocks;       /* blocks of the deep-graph sources in a batch (0: default share) */
+  int32_t spgemm_table_load;       /* SpGEMM hash tables hold >= load x entries: 2 or 4 */
+  int32_t spgemm_warp_max_prod;    /* SpGEMM rows of <= this many products are one warp's (16..256) */
+  int64_t spgemm_bitmap_max_cols;  /* see apspie_spgemm_set_params */
+  double spmspv_sort_factor;       /* see apspie_spmspv_set_params */
+} apspie_tuning;
+int apspie_ctx_get_tuning(apspie_ctx ctx, apspie_tuning *out);
+/* Sets every field (validated: APSPIE_ERR_INVALID when out of range). */
+int apspie_ctx_set_tuning(apspie_ctx ctx, const apspie_tuning *in);
+
+/* Measures the BFS direction thresholds on the given sample sources (a grid
  * of alpha / beta values and push-only, timed with CUDA events: ranked on
  * the first half of the sources, the four best timed again on the second
- * half, the pick by the sum), stores the fastest in the context (used by apspie_bfs and, for jobs with alpha / beta
- * < 0, by apspie_batch_run) and caches it under a fingerprint of the graph
- * (m, nnz, sampled row offsets); a cached graph is not re-measured.
+ * half together with the reference point alpha 32 / beta 128, the pick by
+ * the sum over both halves and kept only if it beats the reference point by
+ * more than 2 %), then the blocks per SM of the persistent launch (3, 2, 1
+ * with the chosen switch points on all sources; fewer blocks kept only when
+ * more than 2 % faster).  Stores the result in the context (used by
+ * apspie_bfs and, for jobs with alpha / beta < 0, by apspie_batch_run).
  * d_depth_scratch: m int32.  *ms_out (may be NULL) = mean ms per BFS. */
 int apspie_autotune_bfs(apspie_ctx ctx, int nsrc, const int *h_src, int64_t nnz,
                         int m, const int *d_ptr, const int *d_ind,
@@ -402,6 +432,27 @@ int apspie_autotune_spmspv(apspie_ctx ctx, int m, int64_t nnz, const int *d_ptr,
                            int *d_xind_scratch, float *d_xval_scratch,
                            int *d_yind_scratch, float *d_yval_scratch,
                            double *factor_out);
+/* Measures the persistent SSSP launch's blocks per SM (as many as fit, then
+ * fewer) and, when the in-adjacency is given (d_tptr / d_tind / d_tw, or
+ * all NULL), the pull-round switch alpha (0, 2, 8), on uint32 weights from
+ * the given sources (two sweeps in opposite orders, each candidate scored by
+ * its better time; a choice other than the current default is kept only
+ * when more than 2 % faster).  d_dist_scratch: m uint32.  *ms_out (may be
+ * NULL) = mean ms per SSSP of the pick; *cached_out (may be NULL) = 1 when
+ * the graph was in the cache. */
+int apspie_autotune_sssp(apspie_ctx ctx, int nsrc, const int *h_src, int64_t nnz, int m,
+                         const int *d_ptr, const int *d_ind, const uint32_t *d_w,
+                         const int *d_tptr, const int *d_tind, const uint32_t *d_tw,
+                         uint32_t *d_dist_scratch, float *ms_out, int *cached_out);
+/* Measures the batched launch's blocks per SM (as many as fit, then one)
+ * and, when some job runs on a deep graph (see apspie_batch_set_params),
+ * the deep sources' block share (a quarter, half, three quarters of the
+ * resident blocks), running apspie_batch_run on the given jobs (their
+ * d_out rows are written).  Same scoring and caching as
+ * apspie_autotune_sssp; the fingerprint covers every job's graph, type and
+ * source count. */
+int apspie_autotune_batch(apspie_ctx ctx, int njobs, const apspie_job *jobs, float *ms_out,
+                          int *cached_out);
 
 /* --------------------------------------------------------- test hooks ---
  * For the tests of the timeout paths (no reference counterpart).  Every
@@ -513,12 +564,21 @@ int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr
                            int *d_Cptr, int64_t *h_nnz);
 int apspie_spgemm_numeric(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B,
                           const int *d_Cptr, int *d_Cind, float *d_Cval);
-/* Rows of A with more than 256 products are accumulated over a
- * shared-memory bitmap of C's columns (one bit per column of B, the
- * position of each product in the column-ordered row is a prefix popcount)
- * when B has at most bitmap_max_cols columns (default 262144, limited to
- * 262144 by shared memory; 0 = always the hash tables). */
+/* Rows of A with more than 4096 products (2048 at table load 4) are
+ * accumulated over a shared-memory bitmap of C's columns (one bit per
+ * column of B, the position of each product in the column-ordered row is a
+ * prefix popcount) when B has at most bitmap_max_cols columns (default
+ * 262144, limited to 262144 by shared memory; 0 = always the hash tables). */
 int apspie_spgemm_set_params(apspie_ctx ctx, int64_t bitmap_max_cols);
+/* Measures the SpGEMM table load (2, 4), the warp-row limit (256, 64
+ * products) and, when B has at most 262144 columns, bitmap versus hash
+ * tables for the long rows, timing apspie_spgemm_symbolic +
+ * apspie_spgemm_numeric of A * B (C is allocated and freed inside); keeps
+ * the fastest (a choice other than the defaults only when more than 2 %
+ * faster) in the context's tuning (apspie_ctx_get_tuning).  Leaves no
+ * SpGEMM plan in the context. */
+int apspie_autotune_spgemm(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B,
+                           float *ms_out, int *cached_out);
 int apspie_csr_free(apspie_ctx ctx, apspie_csr *C);
 /* Stream-ordered device-to-device copy of a library-owned CSR into caller
  * buffers (m + 1 offsets, nnz indices, nnz values; d_ind / d_val may be

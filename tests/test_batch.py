@@ -129,10 +129,9 @@ def test_autotuner_picks_and_caches(ctx):
     assert first == again and first["ms_per_bfs"] > 0
     ref, _ = oracle.bfs(h.m, h.ptr, h.ind, srcs[0])
     np.testing.assert_array_equal(ap.bfs(ctx, g, srcs[0]).cpu().numpy(), ref)
-    ap.bfs_set_params(ctx)  # restore defaults for the other tests
     f = ap.autotune_spmspv(ctx, g)
     assert f >= 0
-    ap.spmspv_set_params(ctx)
+    ap.reset_tuning(ctx)  # restore defaults for the other tests
 
 
 def test_batch_sssp_multi_source_parts(ctx, deep_mode):

@@ -103,7 +103,10 @@ def test_spgemm_two_phase_reuse(ctx):
         _, _, rv = oracle.spgemm(A.m, B.ncols, A.ptr, A.ind, A.w_f32 * np.float32(scale),
                                  B.ptr, B.ind, B.w_f32)
         np.testing.assert_array_equal(ind.cpu().numpy(), ri)
-        np.testing.assert_allclose(val.cpu().numpy(), rv, rtol=1e-4, atol=1e-6)
+        absA = np.abs(A.w_f32 * np.float32(scale))
+        _, _, mag = oracle.spgemm(A.m, B.ncols, A.ptr, A.ind, absA, B.ptr, B.ind, np.abs(B.w_f32))
+        err = np.abs(val.cpu().numpy().astype(np.float64) - rv)
+        assert np.all(err <= VAL_RTOL * np.abs(rv) + 1e-12 * mag + 1e-30), err.max()
     with pytest.raises(ap.ApspieError):
         ap.spgemm_numeric(ctx, dB, dA, ptr, ind, val)
 
