@@ -117,20 +117,32 @@ void *upload_buffer(apspie_context *ctx, size_t bytes, int *slot) {
     check_cuda(ctx, cudaGetLastError(), "upload buffer event");
     return nullptr;
   }
-  if (ctx->up_bytes[k] < bytes) {
+  // the ring's buffers come from one pinned pool, allocated at first use
+  // (pinned allocations are slow: none happens on a later call)
+  if (!ctx->up_pool) {
+    if (cudaMallocHost(&ctx->up_pool, apspie_context::kUploadBytes *
+                                          apspie_context::kUploadRing) != cudaSuccess) {
+      cudaGetLastError();
+      ctx->up_pool = nullptr;
+      set_error(ctx, APSPIE_ERR_OOM, "cudaMallocHost of the upload ring failed");
+      return nullptr;
+    }
+  }
+  *slot = k;
+  if (bytes <= apspie_context::kUploadBytes)
+    return (char *)ctx->up_pool + (size_t)k * apspie_context::kUploadBytes;
+  if (ctx->up_bytes[k] < bytes) {  // larger than a pool buffer: its own
     if (ctx->up_host[k]) cudaFreeHost(ctx->up_host[k]);
     ctx->up_host[k] = nullptr;
     ctx->up_bytes[k] = 0;
-    const size_t want = bytes < 4096 ? 4096 : bytes;
-    if (cudaMallocHost(&ctx->up_host[k], want) != cudaSuccess) {
+    if (cudaMallocHost(&ctx->up_host[k], bytes) != cudaSuccess) {
       cudaGetLastError();
       ctx->up_host[k] = nullptr;
-      set_error(ctx, APSPIE_ERR_OOM, "cudaMallocHost(%zu) failed", want);
+      set_error(ctx, APSPIE_ERR_OOM, "cudaMallocHost(%zu) failed", bytes);
       return nullptr;
     }
-    ctx->up_bytes[k] = want;
+    ctx->up_bytes[k] = bytes;
   }
-  *slot = k;
   return ctx->up_host[k];
 }
 
@@ -178,6 +190,7 @@ int apspie_ctx_destroy(apspie_ctx ctx) {
     if (ctx->up_host[k]) cudaFreeHost(ctx->up_host[k]);
     if (ctx->up_done[k]) cudaEventDestroy(ctx->up_done[k]);
   }
+  if (ctx->up_pool) cudaFreeHost(ctx->up_pool);
   if (ctx->owns_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return APSPIE_OK;
@@ -240,6 +253,9 @@ int apspie_ctx_workspace_bytes(apspie_ctx ctx, size_t *out) {
   if (!ctx || !out) return APSPIE_ERR_INVALID;
   size_t t = 0;
   for (auto &s : ctx->slots) t += s.bytes;
+  for (apspie_context *sub : ctx->subs)
+    if (sub)
+      for (auto &s : sub->slots) t += s.bytes;
   *out = t;
   return APSPIE_OK;
 }

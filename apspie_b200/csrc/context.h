@@ -32,10 +32,15 @@ struct apspie_context {
   // ring of pinned host buffers for tables uploaded to the device (the
   // batched job table): a buffer is reused once the copy that last read it
   // has completed (its event), so a call need not wait for the stream's
-  // earlier kernels
-  static constexpr int kUploadRing = 4;
+  // earlier kernels.  The copy runs when the stream reaches it, so the ring
+  // is as deep as the launches a caller may queue ahead of the GPU (a
+  // server lane queues one batched launch per group: a ring of 4 made the
+  // fifth group's launch wait for the first group's start)
+  static constexpr int kUploadRing = 32;
+  static constexpr size_t kUploadBytes = size_t(64) << 10;  // holds the largest job table
+  void *up_pool = nullptr;  // kUploadRing buffers of kUploadBytes, allocated at first use
   void *up_host[kUploadRing] = {};
-  size_t up_bytes[kUploadRing] = {};
+  size_t up_bytes[kUploadRing] = {};  // a buffer outside the pool when larger
   cudaEvent_t up_done[kUploadRing] = {};
   int up_next = 0;
   // test hook (apspie_debug_inject): the next workspace growth fails

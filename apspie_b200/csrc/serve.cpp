@@ -7,9 +7,10 @@
 // into batches:
 //   * admission: a query's device state (its result row plus its share of the
 //     traversal scratch) is charged against a byte budget and against the
-//     device's free memory (read with cudaMemGetInfo when a batch forms and
-//     after each group completes, less a 2 GiB reserve); queries wait in
-//     arrival order until both allow them in;
+//     device memory the server can use: what its lanes already hold plus the
+//     device's free memory (cudaMemGetInfo, read when a batch forms and after
+//     each group completes), less a 2 GiB reserve; queries wait in arrival
+//     order until both allow them in;
 //   * coalescing: the admitted BFS and SSSP queries of one (graph, kind) form
 //     a group, run by ONE apspie_batch_run (multi-source frontier matrix), or
 //     by the single-source kernel when the group has one query (or, on the
@@ -161,10 +162,11 @@ struct apspie_server {
   Slot slots[2];
   bool any_deep = false;
   bool warming = false;  // add_graph is warming the lanes: the worker launches nothing
-  // admission also against the device's free memory: the free bytes seen at
-  // the last reading and the bytes admitted since then (their buffers may not
-  // exist yet); re-read when a batch forms and after groups complete
-  size_t free_at_read = 0, admitted_since_read = 0;
+  // admission also against device memory: the query state the server may
+  // hold is at most what its lanes already hold (workspaces and result
+  // buffers, which admitted queries reuse) plus what is free on the device,
+  // less a reserve; re-read when a batch forms and after groups complete
+  size_t mem_cap = 0;
   bool free_known = false;
   int fail_next_kind = -1;  // test hook: the next group of this kind fails
   int max_pending = 1 << 20;
@@ -180,7 +182,7 @@ struct apspie_server {
   void *plain_hrow = nullptr;
   size_t plain_m = 0;
   // statistics
-  uint64_t batches = 0, completed = 0, launched_jobs = 0;
+  uint64_t batches = 0, completed = 0, launched_jobs = 0, mem_waits = 0;
   std::vector<double> latencies;
   std::string error;
 };
@@ -306,16 +308,25 @@ int probe_levels(int device, const GraphEntry &g, int *levels) {
 // result rows and staging (they grow after admission).
 constexpr size_t kFreeReserve = size_t(2) << 30;
 
-// Reads the device's free memory (caller holds s->mu).
+// Reads the device's free memory and the server's own holdings (worker
+// thread, caller holds s->mu): queries may fill what the server holds
+// plus what is free, less the reserve.
 void refresh_free_locked(apspie_server *s) {
   size_t fr = 0, total = 0;
-  if (cudaMemGetInfo(&fr, &total) == cudaSuccess) {
-    s->free_at_read = fr;
-    s->admitted_since_read = 0;
-    s->free_known = true;
-  } else {
+  if (cudaMemGetInfo(&fr, &total) != cudaSuccess) {
     cudaGetLastError();
+    return;
   }
+  size_t held = 0;
+  for (Slot &sl : s->slots) {
+    held += sl.d_bytes;
+    for (Lane &ln : sl.lane) {
+      size_t b = 0;
+      if (ln.ctx && apspie_ctx_workspace_bytes(ln.ctx, &b) == APSPIE_OK) held += b;
+    }
+  }
+  s->mem_cap = held + fr > kFreeReserve ? held + fr - kFreeReserve : 0;
+  s->free_known = true;
 }
 
 // Completes the requests of a finished group: results to the callers'
@@ -625,18 +636,16 @@ void worker_main(apspie_server *s) {
       // admit in arrival order while the state budget and the device's
       // free memory (less a reserve for the library's own buffers) allow
       refresh_free_locked(s);
-      const size_t free_cap = s->free_known && s->free_at_read > kFreeReserve
-                                  ? s->free_at_read - kFreeReserve
-                                  : 0;
+      const size_t cap = s->free_known ? std::min(s->budget, s->mem_cap) : s->budget;
       while (!s->pending.empty() && (int)batch.size() < s->max_batch) {
         Request *r = s->pending.front();
         const bool first = s->in_flight == 0 && batch.empty();
-        if (!first && (s->in_flight + r->bytes > s->budget ||
-                       (s->free_known && s->admitted_since_read + r->bytes > free_cap)))
+        if (!first && s->in_flight + r->bytes > cap) {
+          ++s->mem_waits;
           break;
+        }
         s->pending.pop_front();
         s->in_flight += r->bytes;
-        s->admitted_since_read += r->bytes;
         batch.push_back(r);
       }
     }
@@ -1058,6 +1067,8 @@ int apspie_server_get_stats(apspie_server_t s, apspie_server_stats *out) {
   out->p50_ms = q(0.50);
   out->p99_ms = q(0.99);
   out->max_ms = l.empty() ? 0.0 : l.back();
+  out->admission_waits = s->mem_waits;
+  out->memory_cap_bytes = s->mem_cap;
   return APSPIE_OK;
 }
 
@@ -1068,6 +1079,7 @@ int apspie_server_reset_stats(apspie_server_t s) {
   s->completed = 0;
   s->batches = 0;
   s->launched_jobs = 0;
+  s->mem_waits = 0;
   return APSPIE_OK;
 }
 

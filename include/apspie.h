@@ -60,7 +60,8 @@ int apspie_ctx_resident_blocks(apspie_ctx ctx, int *blocks);
 int apspie_ctx_sync(apspie_ctx ctx);
 /* Number of kernels this context has launched since creation. */
 int apspie_ctx_launch_count(apspie_ctx ctx, uint64_t *out);
-/* Bytes of device workspace currently held by the context. */
+/* Bytes of device workspace currently held by the context (its
+ * sub-contexts' included). */
 int apspie_ctx_workspace_bytes(apspie_ctx ctx, size_t *out);
 const char *apspie_last_error(apspie_ctx ctx);
 const char *apspie_status_string(int status);
@@ -306,9 +307,11 @@ int apspie_batch_get_stats(apspie_ctx ctx, apspie_batch_stats *out);
 /* ------------------------------------------------------------- serving ---
  * A query server over device-resident graphs (no reference counterpart).
  * Queries arrive at any time; a worker thread admits them in arrival order
- * while their device state fits state_budget_bytes and the device's free
- * memory (read when a batch forms and after each group completes, less a
- * 2 GiB reserve; the first query of an idle server is always admitted),
+ * while their device state fits state_budget_bytes and the device memory
+ * the server can use: what its lanes' workspaces and result buffers already
+ * hold (admitted queries reuse it) plus the device's free memory, less a
+ * 2 GiB reserve (read when a batch forms and after each group completes; the
+ * first query of an idle server is always admitted),
  * coalesces the admitted
  * BFS / SSSP queries by (graph, kind) into one apspie_batch_run launch, runs
  * MIS queries after it, and copies each result row into the caller's host
@@ -323,6 +326,8 @@ typedef struct {
   uint64_t completed, batches, jobs, pending;
   uint64_t in_flight_bytes;
   double p50_ms, p99_ms, max_ms;  /* submit -> result in host memory */
+  uint64_t admission_waits;  /* times admission stopped at the budget / memory cap */
+  uint64_t memory_cap_bytes; /* held + free device memory less the reserve, last read */
 } apspie_server_stats;
 
 int apspie_server_create(int device, size_t state_budget_bytes, int max_batch,

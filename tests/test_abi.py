@@ -41,3 +41,33 @@ def test_library_is_built_for_sm_100a():
     from apspie_b200 import build
     assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
     assert "-lineinfo" in build.COMMON
+
+def test_ctypes_structs_match_the_header_layout(tmp_path):
+    """The Python binding's struct mirrors have the C header's sizes and
+    field offsets (compiled here with gcc against include/apspie.h)."""
+    import shutil
+    import subprocess
+    import pytest
+    from apspie_b200 import _native as N
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    pairs = {"apspie_tuning": N.Tuning, "apspie_job": N.Job, "apspie_bfs_stats": N.BfsStats,
+             "apspie_sssp_stats": N.SsspStats, "apspie_csr": N.Csr,
+             "apspie_batch_stats": N.BatchStats, "apspie_server_stats": N.ServerStats}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "apspie.h"', "int main(void) {"]
+    for cname, py in pairs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in pairs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
