@@ -9,10 +9,10 @@
 // bits need (ceil(log2 m) bits for row indices), in the onesweep form: one
 // read of the keys counts every pass's digits (radix_histograms), then one
 // kernel per pass (radix_onesweep) whose tiles of 256 threads x 16 keys
-//   * rank their keys: inside a warp, lanes with the same digit are found
-//     with one ballot per digit bit, and a per-warp shared histogram carries
-//     the running count across rounds; a per-digit prefix over the warps of
-//     the tile orders the warps;
+//   * rank their keys: inside a warp, __match_any_sync groups lanes with the
+//     same digit, and a per-warp shared histogram carries the running count
+//     across rounds; a per-digit prefix over the warps of the tile orders
+//     the warps;
 //   * find each digit's output offset by decoupled look-back over the tiles
 //     before them (bounded waits);
 //   * write each digit's run contiguously from a shared-memory copy of the
@@ -184,7 +184,6 @@ __global__ void radix_digit_offsets(unsigned long long *ghist, int npass) {
 // Polls of a look-back wait before it gives up (a predecessor normally
 // publishes within microseconds; about half a second with the back-off).
 constexpr unsigned kLookbackSpinLimit = 1u << 20;
-constexpr int kLookbackWindow = 4;  // predecessors whose status words are loaded at once
 
 template <typename K, typename V>
 __global__ void __launch_bounds__(kSortThreads, 3)
@@ -252,15 +251,7 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
   for (int i = 0; i < kSortItems; ++i) {
     const bool valid = wofs + i * 32 + lane < tlen;
     const unsigned d = valid ? (unsigned)(kv[i] >> shift) & (kRadix - 1) : (unsigned)kRadix;
-    // the lanes holding the same digit: one ballot per digit bit (cheaper
-    // than a match instruction for an 8-bit label), restricted to valid keys
-    unsigned peers = __ballot_sync(kFull, valid);
-#pragma unroll
-    for (int b = 0; b < kRadixBits; ++b) {
-      const unsigned on = __ballot_sync(kFull, (d >> b) & 1u);
-      peers &= ((d >> b) & 1u) ? on : ~on;
-    }
-    if (!valid) peers = 1u << lane;
+    const unsigned peers = __match_any_sync(kFull, d);
     const int leader = __ffs(peers) - 1;
     unsigned prev = 0;
     if (valid && lane == leader) {
@@ -286,36 +277,15 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
   unsigned long long *mine = status + (size_t)tile * kRadix + d;
   unsigned long long excl = 0;
   if (tile == 0) {
-    if (!s_withhold) st_relaxed64(mine, kStIncl | tag | (unsigned long long)run);
+    if (!s_withhold) __stcg(mine, kStIncl | tag | (unsigned long long)run);
   } else {
-    st_relaxed64(mine, kStAgg | tag | (unsigned long long)run);
-    // Look back kLookbackWindow predecessors at a time (their status words
-    // loaded together, relaxed: a word's count is all that is read), adding
-    // counts from the nearest one back until an inclusive word; a word not
-    // yet published stops the window and is polled again.
+    __stcg(mine, kStAgg | tag | (unsigned long long)run);
     long long t = (long long)tile - 1;
     unsigned spins = 0;
     while (t >= 0) {
-      unsigned long long sv[kLookbackWindow];
-#pragma unroll
-      for (int k = 0; k < kLookbackWindow; ++k)
-        sv[k] = t - k >= 0 ? ld_relaxed64(status + (size_t)(t - k) * kRadix + d) : 0ull;
-      bool done = false, stalled = false;
-#pragma unroll
-      for (int k = 0; k < kLookbackWindow; ++k) {
-        if (done || stalled || t < 0) continue;
-        const unsigned long long w = sv[k];
-        if ((w & (0x3FFFFFull << 40)) != tag || (w >> 62) == 0ull) {
-          stalled = true;
-          continue;
-        }
-        excl += w & kStCountMask;
-        if ((w >> 62) == 2ull) done = true;  // inclusive: everything before is in it
-        else --t;
-      }
-      if (done) break;
-      if (stalled) {
-        // a predecessor has not published: give up after kLookbackSpinLimit
+      const unsigned long long sv = ld_acquire64(status + (size_t)t * kRadix + d);
+      if ((sv & (0x3FFFFFull << 40)) != tag || (sv >> 62) == 0ull) {
+        // a predecessor never published: give up after kLookbackSpinLimit
         // polls, or at once when another tile of this sort already gave up
         // (checked every 256; *gaveup is zeroed with the sort's status words)
         if (++spins > kLookbackSpinLimit ||
@@ -325,9 +295,13 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
           break;
         }
         if ((spins & 15u) == 0u) __nanosleep(64);
+        continue;
       }
+      excl += sv & kStCountMask;
+      if ((sv >> 62) == 2ull) break;  // inclusive: everything before is in it
+      --t;
     }
-    st_relaxed64(mine, kStIncl | tag | (excl + run));
+    __stcg(mine, kStIncl | tag | (excl + run));
   }
   gbase[d] = goff[pass * kRadix + d] + excl - loc;
   for (int ww = 0; ww < kWarps; ++ww) whist[ww][d] += (unsigned)loc;

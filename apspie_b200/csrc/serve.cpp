@@ -481,10 +481,21 @@ int launch_group(apspie_server *s, Slot &sl, Group &g) {
 void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
   {
     std::lock_guard<std::mutex> lock(s->mu);
-    // with deep graphs around, the main lane leaves room for the deep lane
+    // The main lane leaves a quarter of the GPU to the deep lane while deep
+    // traversals are in this batch or still running in the other slot;
+    // otherwise it takes the whole GPU (a lone query at a low rate then runs
+    // as fast as on the plain path).  A full-grid launch queued behind a
+    // running deep traversal starts once that ends.
+    bool deep = false;
+    for (Request *r : batch)
+      if (r->type != 2 && s->graphs[r->graph].deep) deep = true;
+    for (Slot &o : s->slots)
+      if (&o != &sl && o.busy)
+        for (Group &g : o.groups)
+          if (!g.done && g.lane == 1) deep = true;
     int resident = 0;
     apspie_ctx_resident_blocks(sl.lane[0].ctx, &resident);
-    apspie_ctx_set_max_grid(sl.lane[0].ctx, s->any_deep ? std::max(1, resident - resident / 4) : 0);
+    apspie_ctx_set_max_grid(sl.lane[0].ctx, deep ? std::max(1, resident - resident / 4) : 0);
   }
   std::map<std::pair<int, int>, size_t> index;
   std::map<std::pair<int, uint32_t>, size_t> mis_index;
