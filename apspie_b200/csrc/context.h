@@ -143,6 +143,7 @@ enum SlotId : int {
   kSlotBfsChunksA,
   kSlotBfsChunksB,
   kSlotBfsGroupMask,
+  kSlotBfsGroupDone,
   kSlotSsspState,
   kSlotSsspQueueA,
   kSlotSsspQueueB,

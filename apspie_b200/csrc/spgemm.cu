@@ -56,6 +56,14 @@ constexpr int kWarpsPerBlockSmall = 4;
 constexpr int kEmpty = INT_MAX;
 constexpr int kLbsPer = 4;  // products per thread per step of for_each_product_lbs
 
+// The smallest s with (ncols - 1) >> s < nb: buckets of 2^s consecutive
+// columns, at most nb of them, in column order.
+__device__ __forceinline__ int bucket_shift(int ncols, int nb) {
+  int s = 0;
+  while (s < 31 && ((ncols - 1) >> s) >= nb) ++s;
+  return s;
+}
+
 __device__ __forceinline__ unsigned hash_col(int j) { return (unsigned)j * 0x9E3779B1u; }
 
 // log2 of a table of at least load x n slots (load 2 or 4), at most 2^cap_bits
@@ -552,6 +560,8 @@ spgemm_block_rows(const int *list, const unsigned *nlist, const long long *prod,
   __shared__ float s_av[kSpgThreads];
   __shared__ int s_cnt;
   const unsigned nrows = *nlist;
+  // column buckets of 2^bshift columns, at most kBuckets of them
+  const int bshift = bucket_shift(ncols, kBuckets);
   for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
     int i = list[r];
     int bits = table_bits(prod[i], 14, load);
@@ -578,14 +588,14 @@ spgemm_block_rows(const int *list, const unsigned *nlist, const long long *prod,
     } else {
       __syncthreads();
       const int base = Cptr[i], n = Cptr[i + 1] - base;
-      // bucket b holds columns [b * ncols / kBuckets, (b + 1) * ncols / kBuckets)
+      // bucket b holds columns [b << bshift, (b + 1) << bshift)
       __shared__ int s_bcnt[kBuckets], s_bfill[kBuckets], sw2[33];
       s_bcnt[threadIdx.x] = 0;
       s_bfill[threadIdx.x] = 0;
       __syncthreads();
       for (int t = threadIdx.x; t < T; t += blockDim.x) {
         const int j = keys[t];
-        if (j != kEmpty) atomicAdd(&s_bcnt[(int)(((long long)j * kBuckets) / ncols)], 1);
+        if (j != kEmpty) atomicAdd(&s_bcnt[j >> bshift], 1);
       }
       __syncthreads();
       const int mine = s_bcnt[threadIdx.x];
@@ -599,7 +609,7 @@ spgemm_block_rows(const int *list, const unsigned *nlist, const long long *prod,
         for (int t = threadIdx.x; t < T; t += blockDim.x) {
           const int j = keys[t];
           if (j == kEmpty) continue;
-          const int b = (int)(((long long)j * kBuckets) / ncols);
+          const int b = j >> bshift;
           const int pos = base + s_bcnt[b] + atomicAdd(&s_bfill[b], 1);
           Cind[pos] = j;
           Cval[pos] = (float)vals[t];
@@ -669,6 +679,9 @@ spgemm_mid_rows(const int *list, const unsigned *nlist, const long long *prod,
   __shared__ int s_cnt;
   const int tid = threadIdx.x;
   const unsigned nrows = *nlist;
+  // column buckets of 2^bshift columns, at most TPB of them (a shift per
+  // key instead of a 64-bit division)
+  const int bshift = bucket_shift(ncols, TPB);
   for (unsigned r = blockIdx.x; r < nrows; r += gridDim.x) {
     const int i = list[r];
     const int base = NUMERIC ? Cptr[i] : 0;
@@ -699,10 +712,10 @@ spgemm_mid_rows(const int *list, const unsigned *nlist, const long long *prod,
       __syncthreads();
       continue;
     }
-    // bucket b holds columns [b * ncols / TPB, (b + 1) * ncols / TPB)
+    // bucket b holds columns [b << bshift, (b + 1) << bshift)
     for (int t = tid; t < Tn; t += TPB) {
       const int j = keys[t];
-      if (j != kEmpty) atomicAdd(&s_bstart[(int)(((long long)j * TPB) / ncols)], 1);
+      if (j != kEmpty) atomicAdd(&s_bstart[j >> bshift], 1);
     }
     __syncthreads();
     const int mine = s_bstart[tid];
@@ -714,7 +727,7 @@ spgemm_mid_rows(const int *list, const unsigned *nlist, const long long *prod,
       for (int t = tid; t < Tn; t += TPB) {
         const int j = keys[t];
         if (j == kEmpty) continue;
-        const int b = (int)(((long long)j * TPB) / ncols);
+        const int b = j >> bshift;
         const int pos = s_bstart[b] + atomicAdd(&s_bfill[b], 1);
         if (pos < T / 2) {
           skeys[pos] = j;

@@ -504,6 +504,13 @@ int sssp_run(apspie_context *ctx, int src, int64_t nnz, int m, const int *d_ptr,
   if (!d_ptr || !d_dist || (nnz > 0 && (!d_ind || !d_w)) ||
       (d_tptr && nnz > 0 && (!d_tind || !d_tw)))
     return set_error(ctx, APSPIE_ERR_INVALID, "apspie_sssp: null pointer");
+  // without a pull switch no round pulls: the in-adjacency is not needed
+  // and the push-only kernel (two blocks per SM, more registers) runs
+  if (ctx->sssp_pull_alpha == 0) {
+    d_tptr = nullptr;
+    d_tind = nullptr;
+    d_tw = nullptr;
+  }
   size_t cap = chunk_capacity(nnz);
   auto *st = (SsspState *)workspace(ctx, kSlotSsspState, sizeof(SsspState));
   auto *qa = (int *)workspace(ctx, kSlotSsspQueueA, sizeof(int) * (size_t)m);

@@ -185,7 +185,9 @@ int apspie_sssp_f32(apspie_ctx ctx, int src, int64_t nnz, int m,
  * instead: each vertex takes the least d[u] + w(u,v) over its in-neighbours
  * in the frontier and writes its own distance, without atomics.  Same
  * results as apspie_sssp_u32 / _f32 (the same min-plus fixpoint); pull
- * rounds are only taken with the near-far step at 0.  Replaces the same
+ * rounds are only taken with the near-far step at 0.  With the switch at 0
+ * the in-adjacency is not read and the call runs as apspie_sssp_u32 / _f32
+ * (the same kernel).  Replaces the same
  * reference calls (src/sssp.cuh:28-115), whose every iteration scans all
  * finite vertices' edges. */
 int apspie_sssp_u32_pull(apspie_ctx ctx, int src, int64_t nnz, int m,
