@@ -26,6 +26,12 @@
 // the autotuner) are decided identically by every block from counters that
 // nobody writes during the step in which they are read.
 //
+// A unit's joiners (vertices that enter a job's next frontier) are staged
+// per warp and job in shared memory and appended with one reservation per
+// flush; the next step's hub and edge tallies are summed per block.  Jobs on
+// deep graphs (a probe BFS of more than 64 levels) run their sources as
+// single-source traversals on sub-contexts beside the launch instead.
+//
 // Per source, the results are exactly those of the single-source kernels:
 // BFS levels are set once per (source, vertex) by the thread whose atomicOr
 // on the visited mask first sets the bit; SSSP converges to the same

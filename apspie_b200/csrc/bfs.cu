@@ -101,14 +101,9 @@ struct BfsVisit {
 // launch polls its own counter set, see BfsState::barp).
 __device__ __forceinline__ void bfs_clear(int m, int src, int32_t *depth,
                                           const int *__restrict__ ptr, int *queue, int2 *chunks,
-                                          BfsState *st, bool reset_bar, unsigned *gdone = nullptr) {
+                                          BfsState *st, bool reset_bar) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < m; v += gridDim.x * blockDim.x)
     depth[v] = (v == src) ? 0 : -1;
-  if (gdone) {
-    const int ndw = (int)((((unsigned)m + 31u) / 32u + 31u) / 32u);
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ndw; t += gridDim.x * blockDim.x)
-      gdone[t] = 0u;
-  }
   if (blockIdx.x == 0) {
     seed_frontier(src, ptr, queue, chunks, &st->c[0]);
     if (threadIdx.x == 0) {
@@ -142,7 +137,7 @@ __global__ void __launch_bounds__(kBfsThreads, 3)
 bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__restrict__ ind,
                const int *__restrict__ tptr, const int *__restrict__ tind, int32_t *depth,
                int *qa, int *qb, int2 *ca, int2 *cb, BfsState *st, int max_levels, int alpha,
-               int beta, int mode, unsigned *gmask, int src, int init_par, unsigned *gdone) {
+               int beta, int mode, unsigned *gmask, int src, int init_par) {
   const int lane = lane_id();
   const int warp = warp_in_block();
   const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -172,7 +167,7 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
       st->errp[init_par ^ 1] = 0;
       st->par = init_par;
     }
-    bfs_clear(m, src, depth, ptr, qa, ca, st, false, gdone);
+    bfs_clear(m, src, depth, ptr, qa, ca, st, false);
     if (!grid_barrier(bar, err)) return;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) st->t_start = globaltimer();
@@ -301,17 +296,10 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
       const unsigned per_block = (ngroups + gridDim.x - 1) / gridDim.x;
       const unsigned gbeg = blockIdx.x * per_block;
       const unsigned gend = min(gbeg + per_block, ngroups);
-      // A group whose vertices are all visited or without in-edges (its
-      // done bit, set by an earlier pull level) is skipped: nothing in it
-      // can be found, so its found-mask word is 0.
       auto grab = [&]() {
-        for (;;) {
-          unsigned g = 0;
-          if (lane == 0) g = atomicAdd(&s_next, 1u);
-          g = gbeg + __shfl_sync(kFull, g, 0);
-          if (g >= gend || !gdone || !((__ldcg(gdone + (g >> 5)) >> (g & 31)) & 1u)) return g;
-          if (lane == 0) gmask[g] = 0u;
-        }
+        unsigned g = 0;
+        if (lane == 0) g = atomicAdd(&s_next, 1u);
+        return gbeg + __shfl_sync(kFull, g, 0);
       };
       unsigned g = grab();
       int pv = -2, ps = 0, pe = 0;  // prefetched depth and in-range of the next group
@@ -341,8 +329,7 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
           }
         }
         bool found = false;
-        const bool open = s < e;  // unvisited, with in-edges to probe
-        unsigned U = __ballot_sync(kFull, open);
+        unsigned U = __ballot_sync(kFull, s < e);
         if (U) {
           if (lane == 0) s_found[warp] = 0u;
           __syncwarp();
@@ -380,9 +367,6 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
         // counted: a push level after this one rebuilds its queue from it
         const unsigned fw = __ballot_sync(kFull, found);
         if (lane == 0) gmask[g] = fw;
-        // every vertex of the group now visited or without in-edges: done
-        if (gdone && __ballot_sync(kFull, !open || found) == kFull && lane == 0)
-          atomicOr(gdone + (g >> 5), 1u << (g & 31));
         if (!append && found) {
           ++cnt;
           edg += (unsigned long long)(__ldg(ptr + v + 1) - __ldg(ptr + v));
@@ -490,10 +474,7 @@ int apspie_bfs(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
   auto *ca = (int2 *)workspace(ctx, kSlotBfsChunksA, sizeof(int2) * chunk_cap);
   auto *cb = (int2 *)workspace(ctx, kSlotBfsChunksB, sizeof(int2) * chunk_cap);
   auto *gmask = (unsigned *)workspace(ctx, kSlotBfsGroupMask, sizeof(unsigned) * ((size_t)m / 32 + 1));
-  // one done bit per 32-vertex group, cleared by the launch
-  auto *gdone = (unsigned *)workspace(ctx, kSlotBfsGroupDone,
-                                      sizeof(unsigned) * (((size_t)m + 31) / 32 / 32 + 1));
-  if (!st || !qa || !qb || !ca || !cb || !gmask || !gdone) return APSPIE_ERR_OOM;
+  if (!st || !qa || !qb || !ca || !cb || !gmask) return APSPIE_ERR_OOM;
   ctx->bfs_state = st;
   int grid = persistent_grid(ctx, bfs_grid(ctx), ctx->bfs_blocks_per_sm);
   if (grid <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_bfs: occupancy query failed");
@@ -513,7 +494,7 @@ int apspie_bfs(apspie_ctx ctx, int src, int64_t nnz, int m, const int *d_ptr,
   int par = ctx->bfs_par;
   void *args[] = {&m,  &nnz_ll, (void *)&d_ptr, (void *)&d_ind, (void *)&d_tptr, (void *)&d_tind,
                   &d_depth, &qa, &qb, &ca, &cb, &st, &max_levels, &alpha, &beta, &mode,
-                  &gmask, &src, &par, &gdone};
+                  &gmask, &src, &par};
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)bfs_persistent, dim3(grid),
                                               dim3(kBfsThreads), args, 0, ctx->stream);
   if (e != cudaSuccess) return check_cuda(ctx, e, "bfs_persistent");
@@ -719,10 +700,9 @@ extern "C" int apspie_bfs_noalloc(void *stream, int src, int64_t nnz, int m, con
   long long nnz_ll = (long long)nnz;
   int alpha = 14, beta = 24, mode = d_tptr ? 0 : 1;
   int no_fused = -1;
-  unsigned *no_done = nullptr;  // no group done bits: every group is scanned
   void *args[] = {&m,  &nnz_ll, (void *)&d_ptr, (void *)&d_ind, (void *)&d_tptr, (void *)&d_tind,
                   &d_depth, &qa, &qb, &ca, &cb, &state, &max_levels, &alpha, &beta, &mode,
-                  &gmask, &src, &no_fused, &no_done};
+                  &gmask, &src, &no_fused};
   if (cudaLaunchCooperativeKernel((const void *)bfs_persistent, dim3(grid), dim3(kBfsThreads), args,
                                   0, st) != cudaSuccess) {
     cudaGetLastError();

@@ -143,7 +143,6 @@ enum SlotId : int {
   kSlotBfsChunksA,
   kSlotBfsChunksB,
   kSlotBfsGroupMask,
-  kSlotBfsGroupDone,
   kSlotSsspState,
   kSlotSsspQueueA,
   kSlotSsspQueueB,

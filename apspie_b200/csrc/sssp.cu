@@ -30,6 +30,14 @@
 // are queued as in a push round, so either direction may follow.  The
 // relaxations are the same min-plus steps, so the fixpoint is the same.
 //
+// Push rounds stage their appends per warp in shared memory (one global
+// reservation per 256 queued vertices or 128 hub entries, frontier.cuh), and
+// skip re-expansions that relax nothing new: a queued vertex whose distance
+// equals the one it was last expanded with was queued again by an
+// improvement that the same expansion already used; a hub of
+// kHubSkipMinDeg+ edges, expanded chunk by chunk, decides the same by one
+// CAS per round on a (round, skip, distance) word.
+//
 // Distances are kept as 32-bit words: uint32 sums for integer weights, and
 // the IEEE bit pattern for float weights -- non-negative floats order like
 // their bit patterns, so atomicMin on the word is min on the value.  Each
