@@ -67,7 +67,7 @@ class ServerStats(C.Structure):
     _fields_ = [("completed", C.c_uint64), ("batches", C.c_uint64), ("jobs", C.c_uint64),
                 ("pending", C.c_uint64), ("in_flight_bytes", C.c_uint64), ("p50_ms", C.c_double),
                 ("p99_ms", C.c_double), ("max_ms", C.c_double), ("admission_waits", C.c_uint64),
-                ("memory_cap_bytes", C.c_uint64)]
+                ("memory_cap_bytes", C.c_uint64), ("max_launch_ms", C.c_double)]
 
 
 # name -> (restype, argtypes); every symbol declared in include/apspie.h

@@ -183,6 +183,8 @@ struct apspie_server {
   size_t plain_m = 0;
   // statistics
   uint64_t batches = 0, completed = 0, launched_jobs = 0, mem_waits = 0;
+  double max_launch_ms = 0.0;  // longest host time of one launch_slot
+  std::vector<void *> retired;  // outgrown staging buffers, freed at destroy
   std::vector<double> latencies;
   std::string error;
 };
@@ -204,10 +206,15 @@ size_t request_bytes(const apspie_server *s, int type, int graph) {
 
 // Grows a buffer at least twofold (freeing one synchronises the device, so
 // growth should be rare).
-bool ensure_device(void **p, size_t *have, size_t want) {
+// Grows a device staging buffer.  The old buffer is kept (released when the
+// server is destroyed) instead of freed: cudaFree waits for all the
+// device's work, the other slot's traversals included (a 335 ms launch was
+// measured at 1,000 q/s).  Growth is at least twofold, so what is kept is
+// at most the size of the current buffer.
+bool ensure_device(void **p, size_t *have, size_t want, std::vector<void *> *retired) {
   if (*have >= want) return true;
   const size_t prev = *have;
-  if (*p) cudaFree(*p);
+  if (*p) retired->push_back(*p);
   *p = nullptr;
   *have = 0;
   size_t w = std::max<size_t>({want, 2 * prev, (size_t)1 << 20});
@@ -564,7 +571,7 @@ void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
     sl.events.push_back(e);
   }
   const bool buffers = sl.events.size() >= 3 * sl.groups.size() &&
-                       ensure_device((void **)&sl.d_out, &sl.d_bytes, dev) &&
+                       ensure_device((void **)&sl.d_out, &sl.d_bytes, dev, &s->retired) &&
                        (host == 0 || ensure_host(&sl.h_stage, &sl.h_bytes, host));
   for (size_t i = 0; i < sl.groups.size(); ++i) {
     Group &g = sl.groups[i];
@@ -597,6 +604,11 @@ void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
   sl.busy = true;
 }
 
+// The worker's pause between polls of the running groups' events (every
+// slot is polled at the top of its loop, so a finished group is reported
+// within about this long whichever slot it is in).
+void pause_briefly() { std::this_thread::sleep_for(std::chrono::microseconds(20)); }
+
 void worker_main(apspie_server *s) {
   cudaSetDevice(s->device);
   for (;;) {
@@ -606,13 +618,10 @@ void worker_main(apspie_server *s) {
     for (Slot &sl : s->slots)
       if (!sl.busy) free_slot = &sl;
     if (!free_slot) {
-      // both batches in flight: wait for the older slot's next group
-      Slot &older = s->slots[0];
-      for (Group &g : older.groups)
-        if (!g.done) {
-          cudaEventSynchronize(g.end);
-          break;
-        }
+      // both batches in flight: poll again shortly.  Waiting on one slot's
+      // group instead left the other slot's finished groups unreported
+      // until that group ended (bursts of 100 - 400 ms latency at 100 q/s).
+      pause_briefly();
       continue;
     }
     // One slot free, the other running: while its main lane still has two
@@ -632,7 +641,7 @@ void worker_main(apspie_server *s) {
       if (queued) break;
     }
     if (queued) {
-      cudaEventSynchronize(queued->end);
+      pause_briefly();
       continue;
     }
     std::vector<Request *> batch;
@@ -661,19 +670,19 @@ void worker_main(apspie_server *s) {
       }
     }
     if (batch.empty()) {
-      // over budget: wait for a running group to release memory
-      for (Slot &sl : s->slots)
-        if (sl.busy) {
-          for (Group &g : sl.groups)
-            if (!g.done) {
-              cudaEventSynchronize(g.end);
-              break;
-            }
-          break;
-        }
+      // over budget: poll again shortly, until a running group releases
+      // its memory
+      pause_briefly();
       continue;
     }
+    const auto t_launch = Clock::now();
     launch_slot(s, *free_slot, std::move(batch));
+    const double launch_ms =
+        std::chrono::duration<double, std::milli>(Clock::now() - t_launch).count();
+    {
+      std::lock_guard<std::mutex> lock(s->mu);
+      s->max_launch_ms = std::max(s->max_launch_ms, launch_ms);
+    }
     ++s->batches;
   }
 }
@@ -1080,6 +1089,7 @@ int apspie_server_get_stats(apspie_server_t s, apspie_server_stats *out) {
   out->max_ms = l.empty() ? 0.0 : l.back();
   out->admission_waits = s->mem_waits;
   out->memory_cap_bytes = s->mem_cap;
+  out->max_launch_ms = s->max_launch_ms;
   return APSPIE_OK;
 }
 
@@ -1091,6 +1101,7 @@ int apspie_server_reset_stats(apspie_server_t s) {
   s->batches = 0;
   s->launched_jobs = 0;
   s->mem_waits = 0;
+  s->max_launch_ms = 0.0;
   return APSPIE_OK;
 }
 
@@ -1119,6 +1130,7 @@ int apspie_server_destroy(apspie_server_t s) {
   if (s->plain_stream) cudaStreamDestroy(s->plain_stream);
   cudaFree(s->plain_row);
   if (s->plain_hrow) cudaFreeHost(s->plain_hrow);
+  for (void *q : s->retired) cudaFree(q);
   for (auto &kv : s->prio_cache) cudaFree(kv.second);
   for (auto &kv : s->reqs) delete kv.second;
   delete s;

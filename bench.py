@@ -574,6 +574,7 @@ def serving_leg(ctx, rates=(100, 1000, 10000, 100000), n_queries=600, seed=SEED,
                         rec["batches"] = int(st["batches"])
                         rec["admission_waits"] = int(st["admission_waits"])
                         rec["memory_cap_gb"] = round(st["memory_cap_bytes"] / 2**30, 1)
+                        rec["max_launch_ms"] = round(st["max_launch_ms"], 2)
                     runs[name].append((rec, lat))
             for name in ("batched", "plain"):
                 order = sorted(range(reps), key=lambda i: runs[name][i][0]["qps"])

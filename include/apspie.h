@@ -330,6 +330,7 @@ typedef struct {
   double p50_ms, p99_ms, max_ms;  /* submit -> result in host memory */
   uint64_t admission_waits;  /* times admission stopped at the budget / memory cap */
   uint64_t memory_cap_bytes; /* held + free device memory less the reserve, last read */
+  double max_launch_ms;      /* longest host time the worker spent launching one batch */
 } apspie_server_stats;
 
 int apspie_server_create(int device, size_t state_budget_bytes, int max_batch,
