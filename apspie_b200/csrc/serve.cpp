@@ -24,13 +24,17 @@
 //     is added, by one probe BFS) run on a second stream with a quarter of
 //     the GPU's persistent blocks, next to the main lane with the rest, so
 //     their thousands of short levels do not keep the whole GPU from the
-//     other queries;
+//     other queries; while no such traversal is in the batch or running in
+//     the other slot, the main lane takes the whole GPU;
 //   * continuous batching: there are two batch slots.  While one slot's
 //     groups run, queries that arrive are admitted into the other slot,
 //     which is launched, queued on the GPU behind (and overlapping the
 //     copies of) the running groups, once the running slot's main lane is
 //     down to its last group; until then the queries keep gathering, so
 //     under load the groups grow instead of the batches multiplying.
+// The worker never blocks on one group: between rounds it pauses briefly
+// and polls every running group's completion event, so a finished query is
+// reported within tens of microseconds whichever slot it ran in.
 // Each query's result row is copied into the caller's host buffer, or into
 // its device buffer (or dropped, for load tests), and its latency (submit ->
 // result in host / device memory) is recorded.  MIS priorities (mt19937 of
@@ -523,9 +527,15 @@ void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
       sl.groups.back().reqs.push_back(r);
       continue;
     }
+    // A group holds at most one multi-source launch's worth of sources
+    // (64 BFS / 32 SSSP), the size every lane was warmed with: a larger one
+    // would run as several device jobs in one launch and need more
+    // workspace than the warm-up gave, and growing a workspace waits for
+    // all device work.  The next query of the pair starts a new group.
+    const size_t cap = s->graphs[r->graph].deep ? SIZE_MAX : (r->type == 0 ? 64u : 32u);
     auto key = std::make_pair(r->graph, r->type);
     auto it = index.find(key);
-    if (it == index.end()) {
+    if (it == index.end() || sl.groups[it->second].reqs.size() >= cap) {
       index[key] = sl.groups.size();
       sl.groups.emplace_back();
       sl.groups.back().kind = r->type;
