@@ -155,11 +155,26 @@ radix_histograms(const K *keys, long long n, int npass, unsigned long long *ghis
   __shared__ unsigned hist[kMaxPasses][kRadix];
   for (int t = threadIdx.x; t < kMaxPasses * kRadix; t += blockDim.x) hist[t / kRadix][t % kRadix] = 0;
   __syncthreads();
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const K k = keys[i];
-    for (int p = 0; p < npass; ++p)
-      atomicAdd(&hist[p][(unsigned)(k >> (p * kRadixBits)) & (kRadix - 1)], 1u);
+  // warp-uniform loop (every lane of a warp takes the same trips; lane 0's
+  // key always exists): keys that arrive grouped (a CSR's rows) share their
+  // high digits across the warp, and then the warp adds once to the digit's
+  // counter instead of 32 times
+  const int lane = (int)(threadIdx.x & 31);
+  for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31u); base < n;
+       base += (long long)gridDim.x * blockDim.x) {
+    const long long i = base + lane;
+    const bool valid = i < n;
+    const K k = valid ? keys[i] : K(0);
+    const unsigned active = __ballot_sync(0xffffffffu, valid);
+    for (int p = 0; p < npass; ++p) {
+      const unsigned d = (unsigned)(k >> (p * kRadixBits)) & (kRadix - 1);
+      const unsigned d0 = __shfl_sync(0xffffffffu, d, 0);
+      if (__all_sync(0xffffffffu, !valid || d == d0)) {
+        if (lane == 0) atomicAdd(&hist[p][d0], (unsigned)__popc(active));
+      } else if (valid) {
+        atomicAdd(&hist[p][d], 1u);
+      }
+    }
   }
   __syncthreads();
   for (int t = threadIdx.x; t < npass * kRadix; t += blockDim.x) {

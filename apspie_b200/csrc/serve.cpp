@@ -8,8 +8,8 @@
 //   * admission: a query's device state (its result row plus its share of the
 //     traversal scratch) is charged against a byte budget and against the
 //     device memory the server can use: what its lanes already hold plus the
-//     device's free memory (cudaMemGetInfo, read when a batch forms and after
-//     each group completes), less a 2 GiB reserve; queries wait in arrival
+//     device's free memory (cudaMemGetInfo, read when a batch forms, at most
+//     every 10 ms), less a 2 GiB reserve; queries wait in arrival
 //     order until both allow them in;
 //   * coalescing: the admitted BFS and SSSP queries of one (graph, kind) form
 //     a group, run by ONE apspie_batch_run (multi-source frontier matrix), or
@@ -169,9 +169,10 @@ struct apspie_server {
   // admission also against device memory: the query state the server may
   // hold is at most what its lanes already hold (workspaces and result
   // buffers, which admitted queries reuse) plus what is free on the device,
-  // less a reserve; re-read when a batch forms and after groups complete
+  // less a reserve; re-read when a batch forms, at most every 10 ms
   size_t mem_cap = 0;
   bool free_known = false;
+  Clock::time_point mem_read_at{};
   int fail_next_kind = -1;  // test hook: the next group of this kind fails
   int max_pending = 1 << 20;
   // MIS priorities per (graph, seed), on the device
@@ -321,8 +322,15 @@ constexpr size_t kFreeReserve = size_t(2) << 30;
 
 // Reads the device's free memory and the server's own holdings (worker
 // thread, caller holds s->mu): queries may fill what the server holds
-// plus what is free, less the reserve.
+// plus what is free, less the reserve.  At most once per kMemReadPeriod:
+// the reading is a driver call, and the cap moves only when the server or
+// another user of the device allocates.
+constexpr auto kMemReadPeriod = std::chrono::milliseconds(10);
+
 void refresh_free_locked(apspie_server *s) {
+  const auto now = Clock::now();
+  if (s->free_known && now - s->mem_read_at < kMemReadPeriod) return;
+  s->mem_read_at = now;
   size_t fr = 0, total = 0;
   if (cudaMemGetInfo(&fr, &total) != cudaSuccess) {
     cudaGetLastError();
@@ -364,8 +372,6 @@ void finish_group(apspie_server *s, Slot &sl, Group &g) {
     ++s->completed;
   }
   g.done = true;
-  // memory the group's work used may be free again
-  refresh_free_locked(s);
   s->cv.notify_all();
 }
 

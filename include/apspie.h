@@ -312,7 +312,7 @@ int apspie_batch_get_stats(apspie_ctx ctx, apspie_batch_stats *out);
  * while their device state fits state_budget_bytes and the device memory
  * the server can use: what its lanes' workspaces and result buffers already
  * hold (admitted queries reuse it) plus the device's free memory, less a
- * 2 GiB reserve (read when a batch forms and after each group completes; the
+ * 2 GiB reserve (read when a batch forms, at most every 10 ms; the
  * first query of an idle server is always admitted),
  * coalesces the admitted
  * BFS / SSSP queries by (graph, kind) into one apspie_batch_run launch, runs
