@@ -78,6 +78,15 @@ __device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long l
   return v;
 }
 
+// Relaxed 64-bit load at gpu scope: several can be in flight at once (an
+// acquire load orders the loads after it), for a word whose value is all
+// the reader needs.
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
 // Grid barrier for cooperatively launched kernels, on one 64-bit arrival
 // counter that only grows (bar must be 8-byte aligned and zero at launch):
 // the k-th barrier of every block waits until the counter reaches

@@ -155,26 +155,11 @@ radix_histograms(const K *keys, long long n, int npass, unsigned long long *ghis
   __shared__ unsigned hist[kMaxPasses][kRadix];
   for (int t = threadIdx.x; t < kMaxPasses * kRadix; t += blockDim.x) hist[t / kRadix][t % kRadix] = 0;
   __syncthreads();
-  // warp-uniform loop (every lane of a warp takes the same trips; lane 0's
-  // key always exists): keys that arrive grouped (a CSR's rows) share their
-  // high digits across the warp, and then the warp adds once to the digit's
-  // counter instead of 32 times
-  const int lane = (int)(threadIdx.x & 31);
-  for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31u); base < n;
-       base += (long long)gridDim.x * blockDim.x) {
-    const long long i = base + lane;
-    const bool valid = i < n;
-    const K k = valid ? keys[i] : K(0);
-    const unsigned active = __ballot_sync(0xffffffffu, valid);
-    for (int p = 0; p < npass; ++p) {
-      const unsigned d = (unsigned)(k >> (p * kRadixBits)) & (kRadix - 1);
-      const unsigned d0 = __shfl_sync(0xffffffffu, d, 0);
-      if (__all_sync(0xffffffffu, !valid || d == d0)) {
-        if (lane == 0) atomicAdd(&hist[p][d0], (unsigned)__popc(active));
-      } else if (valid) {
-        atomicAdd(&hist[p][d], 1u);
-      }
-    }
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const K k = keys[i];
+    for (int p = 0; p < npass; ++p)
+      atomicAdd(&hist[p][(unsigned)(k >> (p * kRadixBits)) & (kRadix - 1)], 1u);
   }
   __syncthreads();
   for (int t = threadIdx.x; t < npass * kRadix; t += blockDim.x) {
@@ -199,6 +184,7 @@ __global__ void radix_digit_offsets(unsigned long long *ghist, int npass) {
 // Polls of a look-back wait before it gives up (a predecessor normally
 // publishes within microseconds; about half a second with the back-off).
 constexpr unsigned kLookbackSpinLimit = 1u << 20;
+constexpr int kLookbackWindow = 4;  // predecessors whose status words are loaded at once
 
 template <typename K, typename V>
 __global__ void __launch_bounds__(kSortThreads, 3)
@@ -295,12 +281,33 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
     if (!s_withhold) __stcg(mine, kStIncl | tag | (unsigned long long)run);
   } else {
     __stcg(mine, kStAgg | tag | (unsigned long long)run);
+    // Look back kLookbackWindow predecessors at a time (their status words
+    // loaded together, relaxed: a word's count is all that is read), adding
+    // counts from the nearest one back until an inclusive word; a word not
+    // yet published stops the window and is polled again.
     long long t = (long long)tile - 1;
     unsigned spins = 0;
     while (t >= 0) {
-      const unsigned long long sv = ld_acquire64(status + (size_t)t * kRadix + d);
-      if ((sv & (0x3FFFFFull << 40)) != tag || (sv >> 62) == 0ull) {
-        // a predecessor never published: give up after kLookbackSpinLimit
+      unsigned long long sv[kLookbackWindow];
+#pragma unroll
+      for (int k = 0; k < kLookbackWindow; ++k)
+        sv[k] = t - k >= 0 ? ld_relaxed64(status + (size_t)(t - k) * kRadix + d) : 0ull;
+      bool done = false, stalled = false;
+#pragma unroll
+      for (int k = 0; k < kLookbackWindow; ++k) {
+        if (done || stalled || t < 0) continue;
+        const unsigned long long w = sv[k];
+        if ((w & (0x3FFFFFull << 40)) != tag || (w >> 62) == 0ull) {
+          stalled = true;
+          continue;
+        }
+        excl += w & kStCountMask;
+        if ((w >> 62) == 2ull) done = true;  // inclusive: everything before is in it
+        else --t;
+      }
+      if (done) break;
+      if (stalled) {
+        // a predecessor has not published: give up after kLookbackSpinLimit
         // polls, or at once when another tile of this sort already gave up
         // (checked every 256; *gaveup is zeroed with the sort's status words)
         if (++spins > kLookbackSpinLimit ||
@@ -310,11 +317,7 @@ radix_onesweep(const K *keys_in, const V *vals_in, K *keys_out, V *vals_out, lon
           break;
         }
         if ((spins & 15u) == 0u) __nanosleep(64);
-        continue;
       }
-      excl += sv & kStCountMask;
-      if ((sv >> 62) == 2ull) break;  // inclusive: everything before is in it
-      --t;
     }
     __stcg(mine, kStIncl | tag | (excl + run));
   }
