@@ -343,7 +343,7 @@ __device__ __forceinline__ int block_excl_max(int v, int *sw) {
 // window marks position 0), an inclusive max-scan turns the marks into the
 // owner of every position, and thread t handles positions t and t + TPB --
 // one shared-memory read for the owner, and the loads of B's rows coalesced.
-template <int TPB, typename F>
+template <int TPB, int PER = kLbsPer, typename F>
 __device__ __forceinline__ void for_each_product_lbs(int i, const int *__restrict__ Aptr,
                                                      const int *__restrict__ Aind,
                                                      const float *__restrict__ Aval,
@@ -351,9 +351,9 @@ __device__ __forceinline__ void for_each_product_lbs(int i, const int *__restric
                                                      const int *__restrict__ Bind,
                                                      const float *__restrict__ Bval, int *s_off,
                                                      int *s_bs, float *s_av, F f) {
-  // kLbsPer products per thread per step: the owner map and its max-scan
-  // (five block barriers) are paid once per kLbsPer * TPB products
-  constexpr int CAP = kLbsPer * TPB;
+  // PER products per thread per step: the owner map and its max-scan
+  // (five block barriers) are paid once per PER * TPB products
+  constexpr int CAP = PER * TPB;
   __shared__ int s_om[CAP];
   __shared__ int sw[33];
   const int a0 = __ldg(Aptr + i), a1 = __ldg(Aptr + i + 1);
@@ -377,25 +377,25 @@ __device__ __forceinline__ void for_each_product_lbs(int i, const int *__restric
     for (int w0 = 0; w0 < total; w0 += CAP) {
       const int wn = min(CAP, total - w0);
 #pragma unroll
-      for (int h = 0; h < kLbsPer; ++h) s_om[tid + h * TPB] = -1;
+      for (int h = 0; h < PER; ++h) s_om[tid + h * TPB] = -1;
       __syncthreads();
       if (d > 0) {
         if (excl >= w0 && excl < w0 + wn) s_om[excl - w0] = tid;
         else if (excl < w0 && excl + d > w0) s_om[0] = tid;
       }
       __syncthreads();
-      int run[kLbsPer];
+      int run[PER];
 #pragma unroll
-      for (int h = 0; h < kLbsPer; ++h) {
-        run[h] = s_om[kLbsPer * tid + h];
+      for (int h = 0; h < PER; ++h) {
+        run[h] = s_om[PER * tid + h];
         if (h) run[h] = max(run[h], run[h - 1]);
       }
-      const int pre = block_excl_max<TPB>(run[kLbsPer - 1], sw);
+      const int pre = block_excl_max<TPB>(run[PER - 1], sw);
 #pragma unroll
-      for (int h = 0; h < kLbsPer; ++h) s_om[kLbsPer * tid + h] = max(pre, run[h]);
+      for (int h = 0; h < PER; ++h) s_om[PER * tid + h] = max(pre, run[h]);
       __syncthreads();
 #pragma unroll
-      for (int h = 0; h < kLbsPer; ++h) {
+      for (int h = 0; h < PER; ++h) {
         const int q = tid + h * TPB;
         if (q < wn) {
           const int o = s_om[q];
