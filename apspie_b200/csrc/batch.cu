@@ -914,18 +914,7 @@ __global__ void batch_transpose(const int32_t *vm, int m, int width, int nsrc, i
 }
 
 int batch_grid(apspie_context *ctx) {
-  static int cached_dev = -1, cached_grid = 0;
-  if (cached_dev == ctx->device && cached_grid > 0) return cached_grid;
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_persistent, kBatchThreads, 0) !=
-          cudaSuccess ||
-      occ < 1) {
-    cudaGetLastError();
-    return 0;
-  }
-  cached_dev = ctx->device;
-  cached_grid = occ * ctx->num_sms;
-  return cached_grid;
+  return occupancy_grid(ctx, (const void *)batch_persistent, kBatchThreads);
 }
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }

@@ -435,18 +435,7 @@ bfs_persistent(int m, long long nnz, const int *__restrict__ ptr, const int *__r
 }
 
 int bfs_grid(apspie_context *ctx) {
-  static int cached_dev = -1, cached_grid = 0;
-  if (cached_dev == ctx->device && cached_grid > 0) return cached_grid;
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bfs_persistent, kBfsThreads, 0) !=
-          cudaSuccess ||
-      occ < 1) {
-    cudaGetLastError();
-    return 0;
-  }
-  cached_dev = ctx->device;
-  cached_grid = occ * ctx->num_sms;
-  return cached_grid;
+  return occupancy_grid(ctx, (const void *)bfs_persistent, kBfsThreads);
 }
 
 }  // namespace

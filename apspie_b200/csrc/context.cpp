@@ -3,6 +3,8 @@
 
 #include <cstdarg>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 
 namespace apspie {
 
@@ -101,6 +103,22 @@ uint64_t graph_fingerprint(apspie_context *ctx, int m, int64_t nnz, const int *d
   cudaStreamSynchronize(ctx->stream);
   for (int i = 0; i <= 64; ++i) f = (f ^ (uint64_t)(uint32_t)h[i]) * 1099511628211ull;
   return f;
+}
+
+int occupancy_grid(apspie_context *ctx, const void *kernel, int threads) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(kernel, ctx->device);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, 0) != cudaSuccess ||
+      occ < 1) {
+    cudaGetLastError();
+    return 0;
+  }
+  return cache[key] = occ * ctx->num_sms;
 }
 
 void *upload_buffer(apspie_context *ctx, size_t bytes, int *slot) {

@@ -220,6 +220,12 @@ uint64_t graph_fingerprint(apspie_context *ctx, int m, int64_t nnz, const int *d
 // d_out[i] = d_ptr[m * i / 64] for i = 0..64 (one small launch)
 int gather_offsets(apspie_context *ctx, const int *d_ptr, int m, int *d_out);
 
+// Blocks of `kernel` (threads per block, no dynamic shared memory) that fit
+// on the context's device at once: the occupancy times the SM count, cached
+// per (kernel, device) under a lock (contexts may be used from several
+// threads).  0 if the occupancy query fails.
+int occupancy_grid(apspie_context *ctx, const void *kernel, int threads);
+
 // Grid of a persistent launch: the occupancy-sized grid, capped by the
 // context's max_grid.
 inline int clamp_grid(const apspie_context *ctx, int grid) {

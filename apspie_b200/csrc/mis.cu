@@ -188,18 +188,7 @@ __global__ void zero_i32(int n, int32_t *p) {
 }
 
 int mis_grid(apspie_context *ctx) {
-  static int cached_dev = -1, cached_grid = 0;
-  if (cached_dev == ctx->device && cached_grid > 0) return cached_grid;
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mis_persistent, kMisThreads, 0) !=
-          cudaSuccess ||
-      occ < 1) {
-    cudaGetLastError();
-    return 0;
-  }
-  cached_dev = ctx->device;
-  cached_grid = occ * ctx->num_sms;
-  return cached_grid;
+  return occupancy_grid(ctx, (const void *)mis_persistent, kMisThreads);
 }
 
 }  // namespace

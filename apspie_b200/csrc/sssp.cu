@@ -485,19 +485,7 @@ sssp_persistent(int m, const int *__restrict__ ptr, const int *__restrict__ ind,
 
 template <typename W, int MINB>
 int sssp_grid(apspie_context *ctx) {
-  static int cached_dev = -1, cached_grid = 0;
-  if (cached_dev == ctx->device && cached_grid > 0) return cached_grid;
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sssp_persistent<W, MINB>, kSsspThreads,
-                                                    0) !=
-          cudaSuccess ||
-      occ < 1) {
-    cudaGetLastError();
-    return 0;
-  }
-  cached_dev = ctx->device;
-  cached_grid = occ * ctx->num_sms;
-  return cached_grid;
+  return occupancy_grid(ctx, (const void *)sssp_persistent<W, MINB>, kSsspThreads);
 }
 
 template <typename W>
