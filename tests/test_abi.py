@@ -71,3 +71,35 @@ def test_ctypes_structs_match_the_header_layout(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for f, _ in py._fields_:
             assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
+
+
+def test_python_constants_match_the_header_enums(tmp_path):
+    """The enum values the Python binding and the tests use (semirings, job
+    types, statuses, test-hook codes) are the header's (compiled with gcc)."""
+    import shutil
+    import subprocess
+    import pytest
+    from apspie_b200 import ops
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    names = ["APSPIE_PLUS_TIMES", "APSPIE_MIN_PLUS", "APSPIE_MAX_TIMES", "APSPIE_OR_AND",
+             "APSPIE_JOB_BFS", "APSPIE_JOB_SSSP_U32", "APSPIE_ERR_OOM", "APSPIE_ERR_CUDA",
+             "APSPIE_ERR_TIMEOUT", "APSPIE_ERR_TOO_LARGE", "APSPIE_INJECT_BFS_BARRIER",
+             "APSPIE_INJECT_SORT_LOOKBACK", "APSPIE_INJECT_ALLOC_FAIL"]
+    src = tmp_path / "enums.c"
+    src.write_text('#include <stdio.h>\n#include "apspie.h"\nint main(void) {\n' +
+                   "".join(f'  printf("{n} %d\\n", (int){n});\n' for n in names) +
+                   "  return 0;\n}\n")
+    exe = tmp_path / "enums"
+    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    got = {l.split()[0]: int(l.split()[1]) for l in out.splitlines() if l.strip()}
+    assert (got["APSPIE_PLUS_TIMES"], got["APSPIE_MIN_PLUS"], got["APSPIE_MAX_TIMES"],
+            got["APSPIE_OR_AND"]) == (ops.PLUS_TIMES, ops.MIN_PLUS, ops.MAX_TIMES, ops.OR_AND)
+    assert (got["APSPIE_JOB_BFS"], got["APSPIE_JOB_SSSP_U32"]) == (ops.JOB_BFS, ops.JOB_SSSP_U32)
+    # the values tests/test_failures.py and tests/test_zz_no_alloc.py spell out
+    assert (got["APSPIE_ERR_OOM"], got["APSPIE_ERR_CUDA"], got["APSPIE_ERR_TIMEOUT"],
+            got["APSPIE_ERR_TOO_LARGE"]) == (2, 3, 4, 8)
+    assert (got["APSPIE_INJECT_BFS_BARRIER"], got["APSPIE_INJECT_SORT_LOOKBACK"],
+            got["APSPIE_INJECT_ALLOC_FAIL"]) == (1, 2, 3)
