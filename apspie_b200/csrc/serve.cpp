@@ -145,7 +145,8 @@ struct Slot {
   size_t h_bytes = 0;
   std::vector<Group> groups;
   std::vector<cudaEvent_t> events;  // pool, three per group
-  bool busy = false;
+  // set and cleared by the worker; read by warm_lanes on the thread adding a graph
+  std::atomic<bool> busy{false};
 };
 
 }  // namespace
@@ -154,7 +155,8 @@ struct apspie_server {
   int device = 0;
   size_t budget = 0;
   int max_batch = 256;
-  std::deque<GraphEntry> graphs;  // stable references while graphs are added
+  // appended by add_graph while the worker runs: read and written under mu
+  std::deque<GraphEntry> graphs;
   std::mutex mu;
   std::condition_variable cv;
   std::deque<Request *> pending;
@@ -189,7 +191,8 @@ struct apspie_server {
   // statistics
   uint64_t batches = 0, completed = 0, launched_jobs = 0, mem_waits = 0;
   double max_launch_ms = 0.0;  // longest host time of one launch_slot
-  std::vector<void *> retired;  // outgrown staging buffers, freed at destroy
+  // outgrown result and staging buffers (device, pinned host), freed at destroy
+  std::vector<void *> retired, retired_host;
   std::vector<double> latencies;
   std::string error;
 };
@@ -209,46 +212,32 @@ size_t request_bytes(const apspie_server *s, int type, int graph) {
   }
 }
 
-// Grows a buffer at least twofold (freeing one synchronises the device, so
-// growth should be rare).
-// Grows a device staging buffer.  The old buffer is kept (released when the
-// server is destroyed) instead of freed: cudaFree waits for all the
+// Grows a slot's device result buffer (host = false) or its pinned staging
+// buffer (host = true).  The old buffer is kept (released when the server is
+// destroyed) instead of freed: cudaFree and cudaFreeHost wait for all the
 // device's work, the other slot's traversals included (a 335 ms launch was
 // measured at 1,000 q/s).  Growth is at least twofold, so what is kept is
 // at most the size of the current buffer.
-bool ensure_device(void **p, size_t *have, size_t want, std::vector<void *> *retired) {
+bool ensure_buffer(void **p, size_t *have, size_t want, bool host, std::vector<void *> *retired) {
   if (*have >= want) return true;
   const size_t prev = *have;
   if (*p) retired->push_back(*p);
   *p = nullptr;
   *have = 0;
   size_t w = std::max<size_t>({want, 2 * prev, (size_t)1 << 20});
-  if (cudaMalloc(p, w) != cudaSuccess) {
+  if ((host ? cudaMallocHost(p, w) : cudaMalloc(p, w)) != cudaSuccess) {
     cudaGetLastError();
+    *p = nullptr;
     return false;
   }
   *have = w;
   return true;
 }
 
-bool ensure_host(void **p, size_t *have, size_t want) {
-  if (*have >= want) return true;
-  const size_t prev = *have;
-  if (*p) cudaFreeHost(*p);
-  *p = nullptr;
-  *have = 0;
-  size_t w = std::max<size_t>({want, 2 * prev, (size_t)1 << 20});
-  if (cudaMallocHost(p, w) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  *have = w;
-  return true;
-}
-
-// Device priorities of an MIS query: mt19937(seed) for the graph's vertices,
-// generated on the host and uploaded on `stream` the first time.
-int get_prio(apspie_server *s, int graph, uint32_t seed, cudaStream_t stream, uint32_t **out) {
+// Device priorities of an MIS query: mt19937(seed) for the graph's m
+// vertices, generated on the host and uploaded on `stream` the first time.
+int get_prio(apspie_server *s, int graph, size_t m, uint32_t seed, cudaStream_t stream,
+             uint32_t **out) {
   std::lock_guard<std::mutex> lock(s->prio_mu);
   auto key = std::make_pair(graph, seed);
   auto it = s->prio_cache.find(key);
@@ -256,7 +245,6 @@ int get_prio(apspie_server *s, int graph, uint32_t seed, cudaStream_t stream, ui
     *out = it->second;
     return APSPIE_OK;
   }
-  const size_t m = (size_t)s->graphs[graph].m;
   uint32_t *d = nullptr, *h = nullptr;
   if (cudaMalloc(&d, 4 * m) != cudaSuccess || cudaMallocHost(&h, 4 * m) != cudaSuccess) {
     cudaGetLastError();
@@ -401,26 +389,29 @@ void poll_slot(apspie_server *s, Slot &sl, bool wait) {
 // Launches one group on its lane: the traversal into the group's rows of the
 // slot buffer, then the copies to the callers, between two timing events.
 int launch_group(apspie_server *s, Slot &sl, Group &g) {
-  const GraphEntry &ge = s->graphs[g.graph];
-  Lane &ln = sl.lane[g.lane];
-  cudaEventRecord(g.start, ln.stream);
-  int st = APSPIE_OK;
-  const size_t row = 4 * (size_t)ge.m;
+  // a copy of the graph's entry: another thread may add a graph (growing the
+  // table) or register its in-adjacency while the group launches
+  GraphEntry ge;
   bool inject = false;
   {
     std::lock_guard<std::mutex> lock(s->mu);
+    ge = s->graphs[g.graph];
     if (s->fail_next_kind == g.kind) {
       s->fail_next_kind = -1;
       inject = true;
     }
   }
+  Lane &ln = sl.lane[g.lane];
+  cudaEventRecord(g.start, ln.stream);
+  int st = APSPIE_OK;
+  const size_t row = 4 * (size_t)ge.m;
   if (inject) {
     st = APSPIE_ERR_CUDA;  // test hook: the group fails without running
   } else if (g.kind == 2) {
     // identical queries (same graph and seed): computed once
     Request *r = g.reqs.front();
     uint32_t *prio = nullptr;
-    st = get_prio(s, g.graph, r->seed, ln.stream, &prio);
+    st = get_prio(s, g.graph, (size_t)ge.m, r->seed, ln.stream, &prio);
     if (st == APSPIE_OK)
       st = apspie_mis(ln.ctx, ge.nnz, ge.m, ge.ptr, ge.ind, prio,
                       (int32_t *)((char *)sl.d_out + r->dev_off), 1.0f);
@@ -472,6 +463,7 @@ int launch_group(apspie_server *s, Slot &sl, Group &g) {
     j.d_stind = ge.stind;
     j.d_stw = ge.stw;
     st = apspie_batch_run(ln.ctx, 1, &j, 0);
+    std::lock_guard<std::mutex> lock(s->mu);
     ++s->launched_jobs;
   }
   // results to the callers, on the lane's copy stream once the traversal
@@ -514,6 +506,9 @@ void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
     apspie_ctx_resident_blocks(sl.lane[0].ctx, &resident);
     apspie_ctx_set_max_grid(sl.lane[0].ctx, deep ? std::max(1, resident - resident / 4) : 0);
   }
+  // the groups, their order and their rows read the graph table: under the
+  // lock, since another thread may add a graph meanwhile
+  std::unique_lock<std::mutex> table_lock(s->mu);
   std::map<std::pair<int, int>, size_t> index;
   std::map<std::pair<int, uint32_t>, size_t> mis_index;
   sl.groups.clear();
@@ -551,13 +546,10 @@ void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
       sl.groups[it->second].reqs.push_back(r);
     }
   }
-  {
-    std::lock_guard<std::mutex> lock(s->mu);
-    for (Group &g : sl.groups) g.lane = (s->graphs[g.graph].deep && g.kind != 2) ? 1 : 0;
-    std::stable_sort(sl.groups.begin(), sl.groups.end(), [&](const Group &a, const Group &b) {
-      return s->graphs[a.graph].cost_ms[a.kind] < s->graphs[b.graph].cost_ms[b.kind];
-    });
-  }
+  for (Group &g : sl.groups) g.lane = (s->graphs[g.graph].deep && g.kind != 2) ? 1 : 0;
+  std::stable_sort(sl.groups.begin(), sl.groups.end(), [&](const Group &a, const Group &b) {
+    return s->graphs[a.graph].cost_ms[a.kind] < s->graphs[b.graph].cost_ms[b.kind];
+  });
   // rows: a group's results are consecutive (a batch job writes [nsrc][m])
   // (replayed results that only have to reach host memory all land on the
   // same staging row: the copy is what is measured, not the bytes kept)
@@ -578,6 +570,7 @@ void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
     for (Request *r : g.reqs)
       if (!r->h_result && r->to_stage) r->host_off = host;
   host += sink;
+  table_lock.unlock();
   while (sl.events.size() < 3 * sl.groups.size()) {
     cudaEvent_t e = nullptr;
     if (cudaEventCreate(&e) != cudaSuccess) {
@@ -586,9 +579,10 @@ void launch_slot(apspie_server *s, Slot &sl, std::vector<Request *> batch) {
     }
     sl.events.push_back(e);
   }
-  const bool buffers = sl.events.size() >= 3 * sl.groups.size() &&
-                       ensure_device((void **)&sl.d_out, &sl.d_bytes, dev, &s->retired) &&
-                       (host == 0 || ensure_host(&sl.h_stage, &sl.h_bytes, host));
+  const bool buffers =
+      sl.events.size() >= 3 * sl.groups.size() &&
+      ensure_buffer((void **)&sl.d_out, &sl.d_bytes, dev, false, &s->retired) &&
+      (host == 0 || ensure_buffer(&sl.h_stage, &sl.h_bytes, host, true, &s->retired_host));
   for (size_t i = 0; i < sl.groups.size(); ++i) {
     Group &g = sl.groups[i];
     if (!buffers) {
@@ -698,8 +692,8 @@ void worker_main(apspie_server *s) {
     {
       std::lock_guard<std::mutex> lock(s->mu);
       s->max_launch_ms = std::max(s->max_launch_ms, launch_ms);
+      ++s->batches;
     }
-    ++s->batches;
   }
 }
 
@@ -1023,7 +1017,11 @@ int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q, 
     const Clock::time_point at =
         t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double, std::micro>(q[i].t_us));
     spin_until(at);  // returns at once when the previous query ran late
-    const GraphEntry &g = s->graphs[q[i].graph];
+    GraphEntry g;
+    {
+      std::lock_guard<std::mutex> lock(s->mu);  // the table may grow meanwhile
+      g = s->graphs[q[i].graph];
+    }
     if (q[i].type == 0) {
       const int *tp = g.symmetric ? g.ptr : g.tptr, *ti = g.symmetric ? g.ind : g.tind;
       st = apspie_bfs(ctx, q[i].source, g.nnz, g.m, g.ptr, g.ind, tp, ti, row, 0);
@@ -1031,7 +1029,7 @@ int apspie_server_replay_plain(apspie_server_t s, int n, const apspie_query *q, 
       st = sssp_one(ctx, g, q[i].source, (uint32_t *)row);
     } else {
       uint32_t *prio = nullptr;
-      st = get_prio(s, q[i].graph, q[i].seed, stream, &prio);
+      st = get_prio(s, q[i].graph, (size_t)g.m, q[i].seed, stream, &prio);
       if (st == APSPIE_OK) st = apspie_mis(ctx, g.nnz, g.m, g.ptr, g.ind, prio, row, 1.0f);
     }
     if (st == APSPIE_OK && to_host &&
@@ -1147,6 +1145,7 @@ int apspie_server_destroy(apspie_server_t s) {
   cudaFree(s->plain_row);
   if (s->plain_hrow) cudaFreeHost(s->plain_hrow);
   for (void *q : s->retired) cudaFree(q);
+  for (void *q : s->retired_host) cudaFreeHost(q);
   for (auto &kv : s->prio_cache) cudaFree(kv.second);
   for (auto &kv : s->reqs) delete kv.second;
   delete s;

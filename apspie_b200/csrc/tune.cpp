@@ -27,25 +27,6 @@
 namespace apspie {
 namespace {
 
-float time_bfs(apspie_context *ctx, int nsrc, const int *src, int64_t nnz, int m, const int *ptr,
-               const int *ind, const int *tptr, const int *tind, int32_t *depth, int *rc) {
-  cudaEvent_t a, b;
-  cudaEventCreate(&a);
-  cudaEventCreate(&b);
-  // one untimed traversal to settle caches and the workspace
-  *rc = apspie_bfs(ctx, src[0], nnz, m, ptr, ind, tptr, tind, depth, 0);
-  cudaEventRecord(a, ctx->stream);
-  for (int i = 0; i < nsrc && *rc == 0; ++i)
-    *rc = apspie_bfs(ctx, src[i], nnz, m, ptr, ind, tptr, tind, depth, 0);
-  cudaEventRecord(b, ctx->stream);
-  cudaEventSynchronize(b);
-  float ms = 0;
-  cudaEventElapsedTime(&ms, a, b);
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
-  return ms;
-}
-
 // Device time of f() on the context's stream, in ms (CUDA events).
 template <typename F>
 int time_stream(apspie_context *ctx, F f, float *ms) {
@@ -55,15 +36,35 @@ int time_stream(apspie_context *ctx, F f, float *ms) {
     cudaEventDestroy(a);
     return check_cuda(ctx, cudaGetLastError(), "event");
   }
-  cudaEventRecord(a, ctx->stream);
-  int rc = f();
-  cudaEventRecord(b, ctx->stream);
-  cudaEventSynchronize(b);
   *ms = 0;
-  cudaEventElapsedTime(ms, a, b);
+  int rc = check_cuda(ctx, cudaEventRecord(a, ctx->stream), "event");
+  if (rc == APSPIE_OK) rc = f();
+  cudaError_t e = cudaEventRecord(b, ctx->stream);
+  if (e == cudaSuccess) e = cudaEventSynchronize(b);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(ms, a, b);
+  if (rc == APSPIE_OK && e != cudaSuccess) rc = check_cuda(ctx, e, "timing a tuner candidate");
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   return rc;
+}
+
+// Device time of BFS from each of the nsrc sources in turn, after one
+// untimed traversal that settles caches and the workspace.
+float time_bfs(apspie_context *ctx, int nsrc, const int *src, int64_t nnz, int m, const int *ptr,
+               const int *ind, const int *tptr, const int *tind, int32_t *depth, int *rc) {
+  float ms = 0;
+  *rc = apspie_bfs(ctx, src[0], nnz, m, ptr, ind, tptr, tind, depth, 0);
+  if (*rc) return ms;
+  *rc = time_stream(
+      ctx,
+      [&]() {
+        int r = APSPIE_OK;
+        for (int i = 0; i < nsrc && r == APSPIE_OK; ++i)
+          r = apspie_bfs(ctx, src[i], nnz, m, ptr, ind, tptr, tind, depth, 0);
+        return r;
+      },
+      &ms);
+  return ms;
 }
 
 // Scores n candidates: apply(k) sets candidate k, run(&ms) times it; two
@@ -123,7 +124,7 @@ int apspie_autotune_bfs(apspie_ctx ctx, int nsrc, const int *h_src, int64_t nnz,
       ctx->bfs_blocks_per_sm = e.blocks_per_sm;
       return APSPIE_OK;
     }
-  const int saved_mode = ctx->bfs_mode;
+  const int saved_mode = ctx->bfs_mode, saved_alpha = ctx->bfs_alpha, saved_beta = ctx->bfs_beta;
   // the switch points are measured on the full persistent grid
   ctx->bfs_blocks_per_sm = 0;
   struct Cand {
@@ -182,7 +183,11 @@ int apspie_autotune_bfs(apspie_ctx ctx, int nsrc, const int *h_src, int64_t nnz,
     sweep_time(top, h_src + n1, n2, score2, rc);
   }
   ctx->bfs_mode = saved_mode;
-  if (rc) return rc;
+  if (rc) {
+    ctx->bfs_alpha = saved_alpha;
+    ctx->bfs_beta = saved_beta;
+    return rc;
+  }
   size_t bi = top[0];
   for (size_t ci : top)
     if (score[ci] + score2[ci] < score[bi] + score2[bi]) bi = ci;
@@ -208,6 +213,8 @@ int apspie_autotune_bfs(apspie_ctx ctx, int nsrc, const int *h_src, int64_t nnz,
       },
       bscore);
   if (rc) {
+    ctx->bfs_alpha = saved_alpha;
+    ctx->bfs_beta = saved_beta;
     ctx->bfs_blocks_per_sm = 0;
     return rc;
   }
@@ -237,29 +244,34 @@ int apspie_autotune_spmspv(apspie_ctx ctx, int m, int64_t nnz, const int *d_ptr,
     int xn = std::max(1, m >> k);
     hx.resize(xn);
     for (int i = 0; i < xn; ++i) hx[i] = (int)((int64_t)i * m / xn);
-    cudaMemcpyAsync(d_xind_scratch, hx.data(), sizeof(int) * xn, cudaMemcpyHostToDevice,
-                    ctx->stream);
+    int crc = check_cuda(ctx,
+                         cudaMemcpyAsync(d_xind_scratch, hx.data(), sizeof(int) * xn,
+                                         cudaMemcpyHostToDevice, ctx->stream),
+                         "apspie_autotune_spmspv: frontier upload");
+    if (crc) {
+      ctx->spmspv_sort_factor = saved;
+      return crc;
+    }
     float t[2] = {0, 0};
     int64_t expanded = 0;
     for (int path = 0; path < 2; ++path) {
       ctx->spmspv_sort_factor = path == 0 ? 0.0 : 1e300;  // 0: sort, 1: bitmap
-      cudaEvent_t a, b;
-      cudaEventCreate(&a);
-      cudaEventCreate(&b);
       int ynnz = 0;
-      int rc = apspie_spmspv(ctx, APSPIE_PLUS_TIMES, m, nnz, d_ptr, d_ind, d_val, xn,
+      auto once = [&]() {
+        return apspie_spmspv(ctx, APSPIE_PLUS_TIMES, m, nnz, d_ptr, d_ind, d_val, xn,
                              d_xind_scratch, nullptr, d_yind_scratch, d_yval_scratch, &ynnz,
                              &expanded);
-      cudaEventRecord(a, ctx->stream);
-      for (int r = 0; r < 3 && rc == 0; ++r)
-        rc = apspie_spmspv(ctx, APSPIE_PLUS_TIMES, m, nnz, d_ptr, d_ind, d_val, xn,
-                           d_xind_scratch, nullptr, d_yind_scratch, d_yval_scratch, &ynnz,
-                           &expanded);
-      cudaEventRecord(b, ctx->stream);
-      cudaEventSynchronize(b);
-      cudaEventElapsedTime(&t[path], a, b);
-      cudaEventDestroy(a);
-      cudaEventDestroy(b);
+      };
+      int rc = once();  // untimed: workspace and caches
+      if (rc == APSPIE_OK)
+        rc = time_stream(
+            ctx,
+            [&]() {
+              int r = APSPIE_OK;
+              for (int k3 = 0; k3 < 3 && r == APSPIE_OK; ++k3) r = once();
+              return r;
+            },
+            &t[path]);
       if (rc) {
         ctx->spmspv_sort_factor = saved;
         return rc;
