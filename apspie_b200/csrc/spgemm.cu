@@ -89,7 +89,10 @@ __device__ __forceinline__ int table_insert(int *keys, int bits, int j, bool *fr
     }
     h = (h + 1) & mask;
   }
-  *fresh = false;  // unreachable: the table is at most half full
+  // unreachable while the tables are sized from this product count (at most
+  // half full); a numeric call after A or B changed structure can fill one,
+  // and the caller then skips the product instead of indexing slot -1
+  *fresh = false;
   return -1;
 }
 
@@ -502,7 +505,7 @@ spgemm_warp_rows(const int *list, const unsigned *nlist, const long long *prod,
                              bool fresh;
                              int h = table_insert(keys, bits, j, &fresh);
                              fresh_count += fresh;
-                             if (NUMERIC) atomicAdd(vals + h, v);
+                             if (NUMERIC && h >= 0) atomicAdd(vals + h, v);
                            });
     __syncwarp();
     if (!NUMERIC) {
@@ -578,7 +581,7 @@ spgemm_block_rows(const int *list, const unsigned *nlist, const long long *prod,
                               bool fresh;
                               int h = table_insert(keys, bits, j, &fresh);
                               fresh_count += fresh;
-                              if (NUMERIC) atomicAdd(vals + h, v);
+                              if (NUMERIC && h >= 0) atomicAdd(vals + h, v);
                             });
     if (!NUMERIC) {
       int c = warp_sum(fresh_count);
@@ -702,7 +705,7 @@ spgemm_mid_rows(const int *list, const unsigned *nlist, const long long *prod,
                               bool fresh;
                               const int h = table_insert(keys, bits, j, &fresh);
                               fresh_count += fresh;
-                              if (NUMERIC) atomicAdd(vals + h, v);
+                              if (NUMERIC && h >= 0) atomicAdd(vals + h, v);
                             });
     if (!NUMERIC) {
       const int c = warp_sum(fresh_count);
@@ -946,7 +949,7 @@ spgemm_bitmap_rows(const int *list, const unsigned *nlist, int W,
                                     const int w = j >> 5;
                                     const int pos =
                                         woff[w] + __popc(bits[w] & ((1u << (j & 31)) - 1u));
-                                    if (spill) {
+                                    if (spill && q < np) {
                                       __stcg(my_pos + q, pos);
                                       __stcg(my_val + q, v);
                                     }
