@@ -567,7 +567,9 @@ int apspie_spgemm(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B,
  * (slots of their own), so the numeric phase may be repeated for new
  * values of A and B as long as their structure is unchanged; the next
  * symbolic phase, or apspie_spgemm, replaces the plan (a numeric call for
- * other matrices then returns APSPIE_ERR_INVALID). */
+ * other matrices then returns APSPIE_ERR_INVALID).  A numeric call after
+ * the structure changed in place (same pointers) is not detected: its C is
+ * wrong, but every write stays inside C's rows and the library's buffers. */
 int apspie_spgemm_symbolic(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B,
                            int *d_Cptr, int64_t *h_nnz);
 int apspie_spgemm_numeric(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B,
