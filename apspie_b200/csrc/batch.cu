@@ -547,16 +547,18 @@ __device__ __forceinline__ bool mssp_relax(BatchJob *j, int ue, unsigned we, int
     nd[i] = act[i] ? sat_add(__ldcg(dist + (size_t)vi * sw + src), wi) : 0u;
     cur[i] = act[i] ? __ldcg(dist + (size_t)uu[i] * sw + src) : 0u;
   }
-  // all the slots' minima first (independent atomics), then the ballots
-  unsigned old[kSsspSlots];
+  // the slots' minima, issued without waiting for their old values: a
+  // (target, source) whose distance read this step is above nd drops this
+  // step, by this minimum or by one that got in between (whose lane sets the
+  // same frontier bit), so the bits set are the same as with the old values
+  // and the ballots need not wait for the atomics
 #pragma unroll
   for (int i = 0; i < kSsspSlots; ++i)
-    old[i] = (act[i] && nd[i] < cur[i]) ? atomicMin(dist + (size_t)uu[i] * sw + src, nd[i])
-                                         : 0u;
+    if (act[i] && nd[i] < cur[i]) atomicMin(dist + (size_t)uu[i] * sw + src, nd[i]);
   unsigned mybal = 0;
 #pragma unroll
   for (int i = 0; i < kSsspSlots; ++i) {
-    const bool imp = act[i] && nd[i] < cur[i] && nd[i] < old[i];
+    const bool imp = act[i] && nd[i] < cur[i];
     const unsigned b = __ballot_sync(kFull, imp);
     // loading lane i * per + g takes the bits of its edge's group g
     const int g = lane - i * per;

@@ -147,24 +147,29 @@ struct SsspVisit {
   __device__ __forceinline__ void commit_n(const unsigned (&)[N], const int (&)[N],
                                            const int (&u)[N], const unsigned (&nd)[N],
                                            const bool (&ok)[N], int (&cls)[N]) const {
-    // all distance minima first, then the stamps of the improved targets
-    unsigned old[N];
+    // The distance minimum and the stamp exchange are issued together, not
+    // one after the other: a target that passed check() (nd below the
+    // distance read this round) is improved this round, by this minimum or
+    // by another that got in between, so it belongs in the next frontier
+    // either way, and the first exchange of the round queues it.  A vertex
+    // queued with a distance it was already expanded with is skipped at
+    // expansion.  (Waiting for the minimum's old value first cost 4 - 6 %:
+    // R-MAT 20 u32 0.556 against 0.533 ms, R-MAT 22 3.13 against 2.93 ms.)
 #pragma unroll
-    for (int r = 0; r < N; ++r) old[r] = ok[r] ? atomicMin(dist + u[r], nd[r]) : 0u;
+    for (int r = 0; r < N; ++r)
+      if (ok[r]) atomicMin(dist + u[r], nd[r]);
     int prev[N];
-    bool imp[N];
 #pragma unroll
     for (int r = 0; r < N; ++r) {
-      imp[r] = ok[r] && nd[r] < old[r];
       prev[r] = 0;
-      if (imp[r])
+      if (ok[r])
         prev[r] = nd[r] < thresh ? atomicExch(stamp + u[r], round) : atomicExch(fstamp + u[r], phase);
     }
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       cls[r] = 0;
-      if (imp[r]) cls[r] = nd[r] < thresh ? (prev[r] != round ? 1 : 0)
-                                          : (prev[r] != phase ? 2 : 3);  // 3: far, already listed
+      if (ok[r]) cls[r] = nd[r] < thresh ? (prev[r] != round ? 1 : 0)
+                                         : (prev[r] != phase ? 2 : 3);  // 3: far, already listed
     }
   }
   // least distance sent far by this warp's batch (classes 2 and 3), one atomic
