@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <new>
 #include <vector>
 
 #include "apspie.h"
@@ -50,27 +51,20 @@ int emit_csr(int m, const std::vector<Entry> &e, int **h_ptr, int **h_ind, float
   return APSPIE_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int apspie_read_mtx_host(const char *path, int undirected, int *m_out, int64_t *nnz_out,
-                         int **h_ptr, int **h_ind, float **h_val, int *weighted_out) {
-  if (!path || !m_out || !nnz_out || !h_ptr || !h_ind) return APSPIE_ERR_INVALID;
-  FILE *f = fopen(path, "r");
-  if (!f) return APSPIE_ERR_INVALID;
+// Parses an opened file (apspie_read_mtx_host opens and closes it).
+int read_mtx(FILE *f, int undirected, int *m_out, int64_t *nnz_out, int **h_ptr, int **h_ind,
+             float **h_val, int *weighted_out) {
   char line[4096];
   long long m = -1, n = -1, nz = -1;
   while (fgets(line, sizeof(line), f)) {
     if (line[0] == '%') continue;
     if (sscanf(line, "%lld %lld %lld", &m, &n, &nz) == 3) break;
   }
-  if (m < 0 || nz < 0 || m >= INT32_MAX || nz >= INT32_MAX) {
-    fclose(f);
-    return APSPIE_ERR_INVALID;
-  }
+  if (m < 0 || nz < 0 || m >= INT32_MAX || nz >= INT32_MAX) return APSPIE_ERR_INVALID;
   std::vector<Entry> e;
-  e.reserve((size_t)nz * (undirected ? 2 : 1));
+  // the header's count is only a hint: a short file must not cost the
+  // memory of a long one
+  e.reserve(std::min<size_t>((size_t)nz * (undirected ? 2 : 1), size_t(1) << 24));
   int weighted = -1;
   for (long long k = 0; k < nz; ++k) {
     if (!fgets(line, sizeof(line), f)) break;  // fewer entries than promised
@@ -83,13 +77,9 @@ int apspie_read_mtx_host(const char *path, int undirected, int *m_out, int64_t *
     }
     if (weighted < 0) weighted = (got == 3);
     if (!weighted) w = 1.0;
-    if (a < 1 || b < 1 || a > m || b > m) {
-      fclose(f);
-      return APSPIE_ERR_INVALID;
-    }
+    if (a < 1 || b < 1 || a > m || b > m) return APSPIE_ERR_INVALID;
     e.push_back(Entry{(int)(b - 1), (int)(a - 1), (float)w});
   }
-  fclose(f);
   if (undirected) {
     size_t n0 = e.size();
     for (size_t i = 0; i < n0; ++i)
@@ -102,10 +92,30 @@ int apspie_read_mtx_host(const char *path, int undirected, int *m_out, int64_t *
       if (w == 0 || e[i].row != e[w - 1].row || e[i].col != e[w - 1].col) e[w++] = e[i];
     e.resize(w);
   }
+  if (e.size() >= (size_t)INT32_MAX) return APSPIE_ERR_OVERFLOW;  // int32 row offsets
   *m_out = (int)m;
   *nnz_out = (int64_t)e.size();
   if (weighted_out) *weighted_out = weighted > 0;
   return emit_csr((int)m, e, h_ptr, h_ind, h_val);
+}
+
+}  // namespace
+
+extern "C" {
+
+int apspie_read_mtx_host(const char *path, int undirected, int *m_out, int64_t *nnz_out,
+                         int **h_ptr, int **h_ind, float **h_val, int *weighted_out) {
+  if (!path || !m_out || !nnz_out || !h_ptr || !h_ind) return APSPIE_ERR_INVALID;
+  FILE *f = fopen(path, "r");
+  if (!f) return APSPIE_ERR_INVALID;
+  int st;
+  try {  // no C++ exception leaves the C ABI
+    st = read_mtx(f, undirected, m_out, nnz_out, h_ptr, h_ind, h_val, weighted_out);
+  } catch (const std::bad_alloc &) {
+    st = APSPIE_ERR_OOM;
+  }
+  fclose(f);
+  return st;
 }
 
 }  // extern "C"

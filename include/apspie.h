@@ -677,7 +677,11 @@ int apspie_mt19937_fill_host(uint32_t seed, int64_t n, uint32_t *h_out);
  * second as the row; buildMatrix (src/matrix.cpp:56-111) keeps file order
  * inside a row.  undirected != 0 symmetrises as makeSymmetric
  * (src/util.cuh:573-643): mirrors added, sorted by (row, col), repeats
- * dropped, self-loops kept.  h_val may be NULL. */
+ * dropped, self-loops kept.  h_val may be NULL.  The header's entry count
+ * is a bound, not a size: a file with fewer entries is read as far as it
+ * goes.  Returns APSPIE_ERR_INVALID for a missing file or an index outside
+ * [1, m], APSPIE_ERR_OVERFLOW past 2^31 - 1 entries, APSPIE_ERR_OOM when host
+ * memory runs out. */
 int apspie_read_mtx_host(const char *path, int undirected, int *m_out,
                          int64_t *nnz_out, int **h_ptr, int **h_ind,
                          float **h_val, int *weighted_out);

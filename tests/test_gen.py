@@ -116,6 +116,16 @@ def test_mtx_weighted_and_malformed(tmp_path):
     bad.write_text("3 3 1\n7 1\n")
     with pytest.raises(ap.ApspieError):
         ap.read_mtx(bad)
+    # a header that promises far more entries than the file holds: the count
+    # is a hint (nothing of its size is allocated); the entries present are read
+    short = tmp_path / "short.mtx"
+    short.write_text("4 4 2000000000\n2 1\n4 3\n")
+    g = ap.read_mtx(short, undirected=True)
+    np.testing.assert_array_equal(g.ptr, [0, 1, 2, 3, 4])
+    np.testing.assert_array_equal(g.ind, [1, 0, 3, 2])
+    missing = tmp_path / "none.mtx"
+    with pytest.raises(ap.ApspieError):
+        ap.read_mtx(missing)
 
 
 def test_transpose_host():
