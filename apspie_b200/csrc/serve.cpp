@@ -56,6 +56,7 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -734,7 +735,12 @@ int apspie_server_create(int device, size_t state_budget_bytes, int max_batch,
         apspie_ctx_set_max_grid(ln.ctx, std::max(1, resident / 4));
       }
     }
-  s->worker = std::thread(worker_main, s);
+  try {
+    s->worker = std::thread(worker_main, s);
+  } catch (const std::exception &) {  // no thread could be started
+    apspie_server_destroy(s);
+    return APSPIE_ERR_OOM;
+  }
   *out = s;
   return APSPIE_OK;
 }
@@ -825,9 +831,19 @@ int apspie_server_add_graph(apspie_server_t s, int m, int64_t nnz, const int *d_
   g.cost_ms[0] = 1e-6f * (float)nnz * (g.deep ? 100.0f : 1.0f);
   g.cost_ms[1] = 4.0f * g.cost_ms[0];
   g.cost_ms[2] = 2.0f * g.cost_ms[0];
-  warm_lanes(s, g);
+  try {
+    warm_lanes(s, g);
+  } catch (const std::exception &) {  // the warm-up is an optimisation only
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->warming = false;
+    s->cv.notify_all();
+  }
   std::lock_guard<std::mutex> lock(s->mu);
-  s->graphs.push_back(g);
+  try {
+    s->graphs.push_back(g);
+  } catch (const std::bad_alloc &) {
+    return APSPIE_ERR_OOM;
+  }
   if (g.deep) s->any_deep = true;
   *graph_id = (int)s->graphs.size() - 1;
   return APSPIE_OK;
@@ -877,8 +893,18 @@ int enqueue_locked(apspie_server *s, int type, int graph, int source, uint32_t s
   r->d_result = d_result;
   r->t_submit = t_submit;
   r->bytes = request_bytes(s, type, graph);
-  s->pending.push_back(r);
-  s->reqs[r->id] = r;
+  try {  // into the table, then the queue; undone if either cannot grow
+    s->reqs[r->id] = r;
+    try {
+      s->pending.push_back(r);
+    } catch (...) {
+      s->reqs.erase(r->id);
+      throw;
+    }
+  } catch (const std::bad_alloc &) {
+    delete r;
+    return APSPIE_ERR_OOM;
+  }
   *out = r;
   s->cv.notify_all();
   return APSPIE_OK;
@@ -927,7 +953,12 @@ int apspie_server_replay_keep(apspie_server_t s, int n, const apspie_query *q, i
           (i > 0 && q[i].t_us < q[i - 1].t_us))
         return APSPIE_ERR_INVALID;
   }
-  std::vector<Request *> rs((size_t)n, nullptr);
+  std::vector<Request *> rs;
+  try {
+    rs.assign((size_t)n, nullptr);
+  } catch (const std::bad_alloc &) {
+    return APSPIE_ERR_OOM;
+  }
   const Clock::time_point t0 = Clock::now() + std::chrono::milliseconds(1);
   int st = APSPIE_OK;
   for (int i = 0; i < n && st == APSPIE_OK; ++i) {
@@ -1091,7 +1122,12 @@ int apspie_server_get_stats(apspie_server_t s, apspie_server_stats *out) {
   out->jobs = s->launched_jobs;
   out->pending = s->pending.size();
   out->in_flight_bytes = s->in_flight;
-  std::vector<double> l = s->latencies;
+  std::vector<double> l;
+  try {
+    l = s->latencies;
+  } catch (const std::bad_alloc &) {
+    return APSPIE_ERR_OOM;
+  }
   std::sort(l.begin(), l.end());
   auto q = [&](double p) {
     if (l.empty()) return 0.0;
