@@ -1091,193 +1091,195 @@ using namespace apspie;
 extern "C" {
 
 int apspie_batch_run(apspie_ctx ctx, int njobs, const apspie_job *jobs, int max_steps) {
-  APSPIE_CHECK_CTX(ctx);
-  if (njobs <= 0 || !jobs)
-    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: no jobs");
-  for (int i = 0; i < njobs; ++i) {
-    const apspie_job &J = jobs[i];
-    if ((J.type != APSPIE_JOB_BFS && J.type != APSPIE_JOB_SSSP_U32) || J.m <= 0 || J.nnz < 0 ||
-        J.nnz >= (int64_t)INT32_MAX || J.nsrc <= 0 || !J.h_src || !J.d_ptr || !J.d_out ||
-        (J.nnz > 0 && !J.d_ind) || (J.type == APSPIE_JOB_SSSP_U32 && J.nnz > 0 && !J.d_w) ||
-        (J.d_stptr && J.nnz > 0 && (!J.d_stind || !J.d_stw)))
-      return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: bad job %d", i);
-    for (int s = 0; s < J.nsrc; ++s)
-      if (J.h_src[s] < 0 || J.h_src[s] >= J.m)
-        return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: job %d source %d out of range",
-                         i, J.h_src[s]);
-  }
-  // Jobs on deep graphs (a BFS of more than kDeepLevels levels, probed once
-  // per graph) are latency bound per level and gain little from sharing
-  // their levels: their sources run as independent single-source traversals,
-  // concurrently on sub-contexts with small grids.  The others are split
-  // into device jobs of at most 64 (BFS) / 32 (SSSP) sources for one
-  // multi-source launch.
-  std::vector<char> deep_job(njobs, 0);
-  if (max_steps <= 0 && ctx->batch_deep_subs > 0)
+  return api_guard([&]() -> int {
+    APSPIE_CHECK_CTX(ctx);
+    if (njobs <= 0 || !jobs)
+      return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: no jobs");
     for (int i = 0; i < njobs; ++i) {
-      int lv = 0;
-      int rc0 = graph_levels(ctx, jobs[i], &lv);
-      if (rc0) return rc0;
-      deep_job[i] = lv > kDeepLevels;
+      const apspie_job &J = jobs[i];
+      if ((J.type != APSPIE_JOB_BFS && J.type != APSPIE_JOB_SSSP_U32) || J.m <= 0 || J.nnz < 0 ||
+          J.nnz >= (int64_t)INT32_MAX || J.nsrc <= 0 || !J.h_src || !J.d_ptr || !J.d_out ||
+          (J.nnz > 0 && !J.d_ind) || (J.type == APSPIE_JOB_SSSP_U32 && J.nnz > 0 && !J.d_w) ||
+          (J.d_stptr && J.nnz > 0 && (!J.d_stind || !J.d_stw)))
+        return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: bad job %d", i);
+      for (int s = 0; s < J.nsrc; ++s)
+        if (J.h_src[s] < 0 || J.h_src[s] >= J.m)
+          return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: job %d source %d out of range",
+                           i, J.h_src[s]);
     }
-  struct Part {
-    int job, first, n;
-  };
-  std::vector<Part> parts;
-  int ndeep_src = 0;
-  for (int i = 0; i < njobs; ++i) {
-    const apspie_job &J = jobs[i];
-    if (deep_job[i]) {
-      ndeep_src += J.nsrc;
-      continue;
-    }
-    const int width = J.type == APSPIE_JOB_BFS ? kMsbfsWidth : kMssspWidth;
-    for (int f = 0; f < J.nsrc; f += width)
-      parts.push_back(Part{i, f, std::min(width, J.nsrc - f)});
-  }
-  const int nparts = (int)parts.size();
-  if (nparts > kMaxJobs)
-    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: %d device jobs > %d", nparts,
-                     kMaxJobs);
-  const int full = persistent_grid(ctx, batch_grid(ctx), ctx->batch_blocks_per_sm);
-  if (full <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_batch_run: occupancy query failed");
-  // the deep sources get deep_blocks in all (default half the resident
-  // blocks: their traversals are latency bound, a grid filled to the last
-  // block slowed them down, and the multi-source launch beside them needs
-  // the rest; measured on the batched benchmark)
-  const int deep_budget =
-      ndeep_src == 0 ? 0
-                     : std::max(1, std::min(full - (nparts > 0 ? 1 : 0),
-                                            ctx->deep_blocks > 0 ? ctx->deep_blocks : full / 2));
-  const int grid1 = std::max(1, full - (nparts > 0 ? deep_budget : 0));
-  cudaStream_t st = ctx->stream;
-  int rc = APSPIE_OK;
-  ctx->batch_state = nullptr;
-  ctx->batch_subs_used = 0;
-  if (nparts > 0) {
-    // workspace layout per device job
-    std::vector<size_t> off(nparts + 1, 0);
-    size_t total = align_up(sizeof(BatchJob) * kMaxJobs) + align_up(sizeof(BatchState)) +
-                   align_up(sizeof(int) * 64 * kMaxJobs);
-    for (int p = 0; p < nparts; ++p) {
-      const apspie_job &J = jobs[parts[p].job];
-      const bool bfs = J.type == APSPIE_JOB_BFS;
-      const size_t m = (size_t)J.m, cap = job_chunk_capacity(J.nnz, bfs);
-      size_t b = 0;
-      b += align_up(8 * m) * (bfs ? 4 : 3);  // (BFS: visited +) 3 frontier masks
-      b += align_up(4 * m) * 3;              // queues
-      b += align_up(8 * cap) * 3;            // chunk lists
-      b += align_up(4 * m * row_width(parts[p].n));  // vertex-major results
-      if (!bfs && J.d_stptr)  // hub chunks of the SSSP pull steps
-        b += align_up(8 * ((size_t)J.nnz / kMsPullChunk + (size_t)J.nnz / kMsHubIn + 1));
-      off[p] = total;
-      total += b;
-    }
-    unsigned char *ws = (unsigned char *)workspace(ctx, kSlotBatch, total);
-    if (!ws) return APSPIE_ERR_OOM;
-    auto *djobs = (BatchJob *)ws;
-    auto *dstate = (BatchState *)(ws + align_up(sizeof(BatchJob) * kMaxJobs));
-    int *dsrc = (int *)(ws + align_up(sizeof(BatchJob) * kMaxJobs) + align_up(sizeof(BatchState)));
-    // host image of the job table (pinned, copied in one transfer), in a
-    // ring of upload buffers: no wait for the stream's earlier kernels
-    size_t host_bytes = sizeof(BatchJob) * nparts + sizeof(int) * 64 * nparts;
-    int up_slot = 0;
-    auto *hjobs = (BatchJob *)upload_buffer(ctx, host_bytes, &up_slot);
-    if (!hjobs) return APSPIE_ERR_OOM;
-    int *hsrc = (int *)(hjobs + nparts);
-    for (int p = 0; p < nparts; ++p) {
-      const apspie_job &J = jobs[parts[p].job];
-      BatchJob &B = hjobs[p];
-      std::memset(&B, 0, sizeof(B));
-      B.type = J.type == APSPIE_JOB_BFS ? kJobBfs : kJobSssp;
-      B.m = J.m;
-      B.nnz = J.nnz;
-      B.nsrc = parts[p].n;
-      B.ptr = J.d_ptr;
-      B.ind = J.d_ind;
-      B.tptr = J.d_tptr ? J.d_tptr : J.d_ptr;
-      B.tind = J.d_tptr ? J.d_tind : J.d_ind;
-      B.w = J.d_w;
-      B.alpha = J.alpha >= 0 ? J.alpha : ctx->bfs_alpha;
-      B.beta = J.beta >= 0 ? J.beta : ctx->bfs_beta;
-      // no in-adjacency for a directed graph: never pull (alpha 0)
-      if (!J.d_tptr && !J.symmetric) B.alpha = 0;
-      for (int s = 0; s < parts[p].n; ++s) hsrc[p * 64 + s] = J.h_src[parts[p].first + s];
-      B.src = dsrc + p * 64;
-      unsigned char *b = ws + off[p];
-      const bool bfs = B.type == kJobBfs;
-      const size_t m = (size_t)J.m, cap = job_chunk_capacity(J.nnz, bfs);
-      B.big_deg = bfs ? kBigDeg : kSsspBigDeg;
-      B.sw = row_width(B.nsrc);  // result row: the sources rounded up to a power of two
-      B.chunk = bfs ? kChunk : kSsspChunk;
-      if (bfs) {
-        B.visited = (unsigned long long *)b;
-        b += align_up(8 * m);
+    // Jobs on deep graphs (a BFS of more than kDeepLevels levels, probed once
+    // per graph) are latency bound per level and gain little from sharing
+    // their levels: their sources run as independent single-source traversals,
+    // concurrently on sub-contexts with small grids.  The others are split
+    // into device jobs of at most 64 (BFS) / 32 (SSSP) sources for one
+    // multi-source launch.
+    std::vector<char> deep_job(njobs, 0);
+    if (max_steps <= 0 && ctx->batch_deep_subs > 0)
+      for (int i = 0; i < njobs; ++i) {
+        int lv = 0;
+        int rc0 = graph_levels(ctx, jobs[i], &lv);
+        if (rc0) return rc0;
+        deep_job[i] = lv > kDeepLevels;
       }
-      B.F0 = (unsigned long long *)b; b += align_up(8 * m);
-      B.F1 = (unsigned long long *)b; b += align_up(8 * m);
-      B.F2 = (unsigned long long *)b; b += align_up(8 * m);
-      B.q0 = (int *)b; b += align_up(4 * m);
-      B.q1 = (int *)b; b += align_up(4 * m);
-      B.q2 = (int *)b; b += align_up(4 * m);
-      B.c0 = (int2 *)b; b += align_up(8 * cap);
-      B.c1 = (int2 *)b; b += align_up(8 * cap);
-      B.c2 = (int2 *)b; b += align_up(8 * cap);
-      B.out = (int32_t *)b;  // vertex-major; transposed into the caller's array after
-      b += align_up(4 * m * B.sw);
-      if (!bfs && J.d_stptr) {
-        B.stptr = J.d_stptr;
-        B.stind = J.d_stind;
-        B.stw = J.d_stw;
-        B.salpha = ctx->sssp_pull_alpha_batch;
-        B.hubc = (int2 *)b;
+    struct Part {
+      int job, first, n;
+    };
+    std::vector<Part> parts;
+    int ndeep_src = 0;
+    for (int i = 0; i < njobs; ++i) {
+      const apspie_job &J = jobs[i];
+      if (deep_job[i]) {
+        ndeep_src += J.nsrc;
+        continue;
       }
+      const int width = J.type == APSPIE_JOB_BFS ? kMsbfsWidth : kMssspWidth;
+      for (int f = 0; f < J.nsrc; f += width)
+        parts.push_back(Part{i, f, std::min(width, J.nsrc - f)});
     }
-    cudaMemcpyAsync(djobs, hjobs, host_bytes, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(dsrc, hsrc, sizeof(int) * 64 * nparts, cudaMemcpyHostToDevice, st);
-    rc = upload_done(ctx, up_slot);
-    if (rc) return rc;
-    cudaMemsetAsync(dstate, 0, align_up(sizeof(BatchState)), st);
-    rc = check_cuda(ctx, cudaGetLastError(), "apspie_batch_run upload");
-    if (rc) return rc;
-    int nhub_launches = 0;
-    for (int p = 0; p < nparts; ++p) {
-      const long long m = jobs[parts[p].job].m;
-      int g = (int)std::max(1ll, std::min((m * hjobs[p].sw + 255) / 256, (long long)ctx->num_sms * 8));
-      if (hjobs[p].type == kJobBfs) {
-        batch_init_bfs<<<g, 256, 0, st>>>(djobs, p);
-        batch_seed_bfs<<<1, 64, 0, st>>>(djobs, p);
-      } else {
-        batch_init_sssp<<<g, 256, 0, st>>>(djobs, p);
-        batch_seed_sssp<<<1, 32, 0, st>>>(djobs, p);
-        if (hjobs[p].stptr) {
-          batch_hub_chunks<<<std::min(g, ctx->num_sms * 4), 256, 0, st>>>(djobs, p);
-          ++nhub_launches;
+    const int nparts = (int)parts.size();
+    if (nparts > kMaxJobs)
+      return set_error(ctx, APSPIE_ERR_INVALID, "apspie_batch_run: %d device jobs > %d", nparts,
+                       kMaxJobs);
+    const int full = persistent_grid(ctx, batch_grid(ctx), ctx->batch_blocks_per_sm);
+    if (full <= 0) return set_error(ctx, APSPIE_ERR_CUDA, "apspie_batch_run: occupancy query failed");
+    // the deep sources get deep_blocks in all (default half the resident
+    // blocks: their traversals are latency bound, a grid filled to the last
+    // block slowed them down, and the multi-source launch beside them needs
+    // the rest; measured on the batched benchmark)
+    const int deep_budget =
+        ndeep_src == 0 ? 0
+                       : std::max(1, std::min(full - (nparts > 0 ? 1 : 0),
+                                              ctx->deep_blocks > 0 ? ctx->deep_blocks : full / 2));
+    const int grid1 = std::max(1, full - (nparts > 0 ? deep_budget : 0));
+    cudaStream_t st = ctx->stream;
+    int rc = APSPIE_OK;
+    ctx->batch_state = nullptr;
+    ctx->batch_subs_used = 0;
+    if (nparts > 0) {
+      // workspace layout per device job
+      std::vector<size_t> off(nparts + 1, 0);
+      size_t total = align_up(sizeof(BatchJob) * kMaxJobs) + align_up(sizeof(BatchState)) +
+                     align_up(sizeof(int) * 64 * kMaxJobs);
+      for (int p = 0; p < nparts; ++p) {
+        const apspie_job &J = jobs[parts[p].job];
+        const bool bfs = J.type == APSPIE_JOB_BFS;
+        const size_t m = (size_t)J.m, cap = job_chunk_capacity(J.nnz, bfs);
+        size_t b = 0;
+        b += align_up(8 * m) * (bfs ? 4 : 3);  // (BFS: visited +) 3 frontier masks
+        b += align_up(4 * m) * 3;              // queues
+        b += align_up(8 * cap) * 3;            // chunk lists
+        b += align_up(4 * m * row_width(parts[p].n));  // vertex-major results
+        if (!bfs && J.d_stptr)  // hub chunks of the SSSP pull steps
+          b += align_up(8 * ((size_t)J.nnz / kMsPullChunk + (size_t)J.nnz / kMsHubIn + 1));
+        off[p] = total;
+        total += b;
+      }
+      unsigned char *ws = (unsigned char *)workspace(ctx, kSlotBatch, total);
+      if (!ws) return APSPIE_ERR_OOM;
+      auto *djobs = (BatchJob *)ws;
+      auto *dstate = (BatchState *)(ws + align_up(sizeof(BatchJob) * kMaxJobs));
+      int *dsrc = (int *)(ws + align_up(sizeof(BatchJob) * kMaxJobs) + align_up(sizeof(BatchState)));
+      // host image of the job table (pinned, copied in one transfer), in a
+      // ring of upload buffers: no wait for the stream's earlier kernels
+      size_t host_bytes = sizeof(BatchJob) * nparts + sizeof(int) * 64 * nparts;
+      int up_slot = 0;
+      auto *hjobs = (BatchJob *)upload_buffer(ctx, host_bytes, &up_slot);
+      if (!hjobs) return APSPIE_ERR_OOM;
+      int *hsrc = (int *)(hjobs + nparts);
+      for (int p = 0; p < nparts; ++p) {
+        const apspie_job &J = jobs[parts[p].job];
+        BatchJob &B = hjobs[p];
+        std::memset(&B, 0, sizeof(B));
+        B.type = J.type == APSPIE_JOB_BFS ? kJobBfs : kJobSssp;
+        B.m = J.m;
+        B.nnz = J.nnz;
+        B.nsrc = parts[p].n;
+        B.ptr = J.d_ptr;
+        B.ind = J.d_ind;
+        B.tptr = J.d_tptr ? J.d_tptr : J.d_ptr;
+        B.tind = J.d_tptr ? J.d_tind : J.d_ind;
+        B.w = J.d_w;
+        B.alpha = J.alpha >= 0 ? J.alpha : ctx->bfs_alpha;
+        B.beta = J.beta >= 0 ? J.beta : ctx->bfs_beta;
+        // no in-adjacency for a directed graph: never pull (alpha 0)
+        if (!J.d_tptr && !J.symmetric) B.alpha = 0;
+        for (int s = 0; s < parts[p].n; ++s) hsrc[p * 64 + s] = J.h_src[parts[p].first + s];
+        B.src = dsrc + p * 64;
+        unsigned char *b = ws + off[p];
+        const bool bfs = B.type == kJobBfs;
+        const size_t m = (size_t)J.m, cap = job_chunk_capacity(J.nnz, bfs);
+        B.big_deg = bfs ? kBigDeg : kSsspBigDeg;
+        B.sw = row_width(B.nsrc);  // result row: the sources rounded up to a power of two
+        B.chunk = bfs ? kChunk : kSsspChunk;
+        if (bfs) {
+          B.visited = (unsigned long long *)b;
+          b += align_up(8 * m);
+        }
+        B.F0 = (unsigned long long *)b; b += align_up(8 * m);
+        B.F1 = (unsigned long long *)b; b += align_up(8 * m);
+        B.F2 = (unsigned long long *)b; b += align_up(8 * m);
+        B.q0 = (int *)b; b += align_up(4 * m);
+        B.q1 = (int *)b; b += align_up(4 * m);
+        B.q2 = (int *)b; b += align_up(4 * m);
+        B.c0 = (int2 *)b; b += align_up(8 * cap);
+        B.c1 = (int2 *)b; b += align_up(8 * cap);
+        B.c2 = (int2 *)b; b += align_up(8 * cap);
+        B.out = (int32_t *)b;  // vertex-major; transposed into the caller's array after
+        b += align_up(4 * m * B.sw);
+        if (!bfs && J.d_stptr) {
+          B.stptr = J.d_stptr;
+          B.stind = J.d_stind;
+          B.stw = J.d_stw;
+          B.salpha = ctx->sssp_pull_alpha_batch;
+          B.hubc = (int2 *)b;
         }
       }
+      cudaMemcpyAsync(djobs, hjobs, host_bytes, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(dsrc, hsrc, sizeof(int) * 64 * nparts, cudaMemcpyHostToDevice, st);
+      rc = upload_done(ctx, up_slot);
+      if (rc) return rc;
+      cudaMemsetAsync(dstate, 0, align_up(sizeof(BatchState)), st);
+      rc = check_cuda(ctx, cudaGetLastError(), "apspie_batch_run upload");
+      if (rc) return rc;
+      int nhub_launches = 0;
+      for (int p = 0; p < nparts; ++p) {
+        const long long m = jobs[parts[p].job].m;
+        int g = (int)std::max(1ll, std::min((m * hjobs[p].sw + 255) / 256, (long long)ctx->num_sms * 8));
+        if (hjobs[p].type == kJobBfs) {
+          batch_init_bfs<<<g, 256, 0, st>>>(djobs, p);
+          batch_seed_bfs<<<1, 64, 0, st>>>(djobs, p);
+        } else {
+          batch_init_sssp<<<g, 256, 0, st>>>(djobs, p);
+          batch_seed_sssp<<<1, 32, 0, st>>>(djobs, p);
+          if (hjobs[p].stptr) {
+            batch_hub_chunks<<<std::min(g, ctx->num_sms * 4), 256, 0, st>>>(djobs, p);
+            ++nhub_launches;
+          }
+        }
+      }
+      rc = check_launch(ctx, "batch init", 2 * nparts + nhub_launches);
+      if (rc) return rc;
+      int n1 = nparts;
+      void *args1[] = {&djobs, &n1, &dstate, &max_steps};
+      cudaError_t e = cudaLaunchCooperativeKernel((const void *)batch_persistent, dim3(grid1),
+                                                  dim3(kBatchThreads), args1, 0, st);
+      if (e != cudaSuccess) return check_cuda(ctx, e, "batch_persistent");
+      ctx->launches += 1;
+      for (int p = 0; p < nparts; ++p) {
+        const apspie_job &J = jobs[parts[p].job];
+        batch_transpose<<<(J.m + 31) / 32, 256, 0, st>>>(
+            hjobs[p].out, J.m, hjobs[p].sw, parts[p].n, J.d_out + (size_t)parts[p].first * J.m);
+      }
+      rc = check_launch(ctx, "batch_transpose", nparts);
+      if (rc) return rc;
+      ctx->batch_state = dstate;
     }
-    rc = check_launch(ctx, "batch init", 2 * nparts + nhub_launches);
-    if (rc) return rc;
-    int n1 = nparts;
-    void *args1[] = {&djobs, &n1, &dstate, &max_steps};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void *)batch_persistent, dim3(grid1),
-                                                dim3(kBatchThreads), args1, 0, st);
-    if (e != cudaSuccess) return check_cuda(ctx, e, "batch_persistent");
-    ctx->launches += 1;
-    for (int p = 0; p < nparts; ++p) {
-      const apspie_job &J = jobs[parts[p].job];
-      batch_transpose<<<(J.m + 31) / 32, 256, 0, st>>>(
-          hjobs[p].out, J.m, hjobs[p].sw, parts[p].n, J.d_out + (size_t)parts[p].first * J.m);
+    if (ndeep_src > 0) {
+      rc = run_deep_sources(ctx, njobs, jobs, deep_job, deep_budget);
+      if (rc) return rc;
     }
-    rc = check_launch(ctx, "batch_transpose", nparts);
-    if (rc) return rc;
-    ctx->batch_state = dstate;
-  }
-  if (ndeep_src > 0) {
-    rc = run_deep_sources(ctx, njobs, jobs, deep_job, deep_budget);
-    if (rc) return rc;
-  }
-  return APSPIE_OK;
+    return APSPIE_OK;
+  });
 }
 
 int apspie_batch_get_stats(apspie_ctx ctx, apspie_batch_stats *out) {

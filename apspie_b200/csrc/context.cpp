@@ -173,25 +173,27 @@ int upload_done(apspie_context *ctx, int slot) {
 extern "C" {
 
 int apspie_ctx_create(int device, void *stream, apspie_ctx *out) {
-  if (!out) return APSPIE_ERR_INVALID;
-  *out = nullptr;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
-    cudaGetLastError();
-    return APSPIE_ERR_INVALID;
-  }
-  if (cudaSetDevice(device) != cudaSuccess) {
-    cudaGetLastError();
-    return APSPIE_ERR_CUDA;
-  }
-  auto *ctx = new (std::nothrow) apspie_context();
-  if (!ctx) return APSPIE_ERR_OOM;
-  ctx->device = device;
-  ctx->stream = (cudaStream_t)stream;
-  cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
-  ctx->slots.resize(kSlotCount);
-  *out = ctx;
-  return APSPIE_OK;
+  return api_guard([&]() -> int {
+    if (!out) return APSPIE_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+      cudaGetLastError();
+      return APSPIE_ERR_INVALID;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) {
+      cudaGetLastError();
+      return APSPIE_ERR_CUDA;
+    }
+    auto *ctx = new (std::nothrow) apspie_context();
+    if (!ctx) return APSPIE_ERR_OOM;
+    ctx->device = device;
+    ctx->stream = (cudaStream_t)stream;
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    ctx->slots.resize(kSlotCount);
+    *out = ctx;
+    return APSPIE_OK;
+  });
 }
 
 int apspie_ctx_destroy(apspie_ctx ctx) {

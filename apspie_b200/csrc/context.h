@@ -8,6 +8,8 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <exception>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -202,6 +204,20 @@ int upload_done(apspie_context *ctx, int slot);
 // Checks cudaGetLastError after launches; records the launch count.
 int check_launch(apspie_context *ctx, const char *what, int nlaunches = 1);
 int check_cuda(apspie_context *ctx, cudaError_t e, const char *what);
+
+// Runs an entry point's body: a failure of its host bookkeeping
+// (std::bad_alloc from a container, or another standard-library exception)
+// becomes a status, so no C++ exception crosses the C ABI.
+template <typename F>
+int api_guard(F f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc &) {
+    return APSPIE_ERR_OOM;
+  } catch (const std::exception &) {
+    return APSPIE_ERR_INVALID;
+  }
+}
 
 }  // namespace apspie
 

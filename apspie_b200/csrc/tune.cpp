@@ -110,182 +110,187 @@ int apspie_autotune_bfs(apspie_ctx ctx, int nsrc, const int *h_src, int64_t nnz,
                         const int *d_ptr, const int *d_ind, const int *d_tptr, const int *d_tind,
                         int32_t *d_depth_scratch, int *alpha_out, int *beta_out,
                         float *ms_out) {
-  APSPIE_CHECK_CTX(ctx);
-  if (nsrc <= 0 || !h_src || !d_depth_scratch || !alpha_out || !beta_out)
-    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_bfs: bad arguments");
-  const uint64_t fp = graph_fingerprint(ctx, m, nnz, d_ptr);
-  for (auto &e : ctx->tune_cache)
-    if (e.fp == fp) {
-      *alpha_out = e.alpha;
-      *beta_out = e.beta;
-      if (ms_out) *ms_out = e.ms;
-      ctx->bfs_alpha = e.alpha;
-      ctx->bfs_beta = e.beta;
-      ctx->bfs_blocks_per_sm = e.blocks_per_sm;
-      return APSPIE_OK;
-    }
-  const int saved_mode = ctx->bfs_mode, saved_alpha = ctx->bfs_alpha, saved_beta = ctx->bfs_beta;
-  // the switch points are measured on the full persistent grid
-  ctx->bfs_blocks_per_sm = 0;
-  struct Cand {
-    int alpha, beta, mode;
-  };
-  // a grid of switch points plus "never pull"; two sweeps in opposite
-  // orders, each candidate scored by its better time, so that clock ramps
-  // and one-off stalls do not decide the pick (a single sweep on 8 sources
-  // picked points that were 13 % slower on other sources, measured)
-  std::vector<Cand> cands;
-  for (int a : {4, 8, 14, 32, 64})
-    for (int b : {8, 24, 64, 128}) cands.push_back(Cand{a, b, 0});
-  cands.push_back(Cand{14, 24, 1});
-  if (!d_tptr) cands = {{14, 24, 1}};
-  // The candidates are ranked on the first half of the sources; the four
-  // best are timed again on the second half and the pick is the best sum
-  // over both halves.  Ranking on one sample alone has a winner's curse: on
-  // R-MAT 22 a point that left 7 M-edge levels in push (a few sources 2x
-  // slower) won on 16 sources and lost 10 % on 200 others (measured).
-  const int n1 = nsrc >= 2 ? nsrc / 2 : nsrc;
-  const int n2 = nsrc - n1;
-  auto sweep_time = [&](const std::vector<size_t> &which, const int *src, int ns,
-                        std::vector<float> &score, int &rc) {
-    for (int sweep = 0; sweep < 2 && rc == 0; ++sweep)
-      for (size_t k = 0; k < which.size() && rc == 0; ++k) {
-        const size_t ci = which[sweep == 0 ? k : which.size() - 1 - k];
-        const Cand &c = cands[ci];
-        ctx->bfs_alpha = c.alpha;
-        ctx->bfs_beta = c.beta;
-        ctx->bfs_mode = c.mode;
-        float ms = time_bfs(ctx, ns, src, nnz, m, d_ptr, d_ind, d_tptr, d_tind,
-                            d_depth_scratch, &rc);
-        if (rc == 0) score[ci] = std::min(score[ci], ms);
+  return api_guard([&]() -> int {
+    APSPIE_CHECK_CTX(ctx);
+    if (nsrc <= 0 || !h_src || !d_depth_scratch || !alpha_out || !beta_out)
+      return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_bfs: bad arguments");
+    const uint64_t fp = graph_fingerprint(ctx, m, nnz, d_ptr);
+    for (auto &e : ctx->tune_cache)
+      if (e.fp == fp) {
+        *alpha_out = e.alpha;
+        *beta_out = e.beta;
+        if (ms_out) *ms_out = e.ms;
+        ctx->bfs_alpha = e.alpha;
+        ctx->bfs_beta = e.beta;
+        ctx->bfs_blocks_per_sm = e.blocks_per_sm;
+        return APSPIE_OK;
       }
-  };
-  std::vector<size_t> all(cands.size());
-  for (size_t k = 0; k < cands.size(); ++k) all[k] = k;
-  std::vector<float> score(cands.size(), 1e30f), score2(cands.size(), 0.0f);
-  int rc = 0;
-  sweep_time(all, h_src, n1, score, rc);
-  std::vector<size_t> top = all;
-  std::sort(top.begin(), top.end(), [&](size_t a, size_t b) { return score[a] < score[b]; });
-  if (top.size() > 4) top.resize(4);
-  // the reference point (alpha 32, beta 128; the best over 200 sources on
-  // R-MAT 22, measured) is always re-timed, and a pick must beat it by more
-  // than 2 %: differences smaller than that are within the sampling noise of
-  // a few dozen sources, while a switch point a little too low leaves a
-  // 7 M-edge level in push on some sources (2x slower there)
-  size_t ref = cands.size();
-  for (size_t k = 0; k < cands.size(); ++k)
-    if (cands[k].alpha == 32 && cands[k].beta == 128 && cands[k].mode == 0) ref = k;
-  if (ref < cands.size() && std::find(top.begin(), top.end(), ref) == top.end())
-    top.push_back(ref);
-  if (n2 > 0 && top.size() > 1) {
-    std::fill(score2.begin(), score2.end(), 1e30f);
-    sweep_time(top, h_src + n1, n2, score2, rc);
-  }
-  ctx->bfs_mode = saved_mode;
-  if (rc) {
-    ctx->bfs_alpha = saved_alpha;
-    ctx->bfs_beta = saved_beta;
-    return rc;
-  }
-  size_t bi = top[0];
-  for (size_t ci : top)
-    if (score[ci] + score2[ci] < score[bi] + score2[bi]) bi = ci;
-  if (ref < cands.size() && bi != ref &&
-      score[bi] + score2[bi] > 0.98f * (score[ref] + score2[ref]))
-    bi = ref;
-  const Cand pick = cands[bi];
-  // "never pull" is alpha 0: no frontier satisfies edges * 0 > unexplored
-  int alpha = pick.mode == 1 ? 0 : pick.alpha;
-  ctx->bfs_alpha = alpha;
-  ctx->bfs_beta = pick.beta;
-  // then the persistent grid: as many blocks per SM as fit (3), 2 or 1,
-  // with the chosen switch points, on all the sources
-  const int bps[3] = {0, 2, 1};
-  std::vector<float> bscore;
-  rc = sweep_scores(
-      3, [&](size_t k) { ctx->bfs_blocks_per_sm = bps[k]; },
-      [&](float *ms) {
-        int r = 0;
-        *ms = time_bfs(ctx, nsrc, h_src, nnz, m, d_ptr, d_ind, d_tptr, d_tind, d_depth_scratch,
-                       &r);
-        return r;
-      },
-      bscore);
-  if (rc) {
-    ctx->bfs_alpha = saved_alpha;
-    ctx->bfs_beta = saved_beta;
+    const int saved_mode = ctx->bfs_mode;
+    const int saved_alpha = ctx->bfs_alpha, saved_beta = ctx->bfs_beta;
+    // the switch points are measured on the full persistent grid
     ctx->bfs_blocks_per_sm = 0;
-    return rc;
-  }
-  const size_t bb = pick_with_margin(bscore);
-  ctx->bfs_blocks_per_sm = bps[bb];
-  const float per = bscore[bb] / nsrc;
-  ctx->tune_cache.push_back(apspie_context::TuneEntry{fp, alpha, pick.beta, per, bps[bb]});
-  *alpha_out = alpha;
-  *beta_out = pick.beta;
-  if (ms_out) *ms_out = per;
-  return APSPIE_OK;
+    struct Cand {
+      int alpha, beta, mode;
+    };
+    // a grid of switch points plus "never pull"; two sweeps in opposite
+    // orders, each candidate scored by its better time, so that clock ramps
+    // and one-off stalls do not decide the pick (a single sweep on 8 sources
+    // picked points that were 13 % slower on other sources, measured)
+    std::vector<Cand> cands;
+    for (int a : {4, 8, 14, 32, 64})
+      for (int b : {8, 24, 64, 128}) cands.push_back(Cand{a, b, 0});
+    cands.push_back(Cand{14, 24, 1});
+    if (!d_tptr) cands = {{14, 24, 1}};
+    // The candidates are ranked on the first half of the sources; the four
+    // best are timed again on the second half and the pick is the best sum
+    // over both halves.  Ranking on one sample alone has a winner's curse: on
+    // R-MAT 22 a point that left 7 M-edge levels in push (a few sources 2x
+    // slower) won on 16 sources and lost 10 % on 200 others (measured).
+    const int n1 = nsrc >= 2 ? nsrc / 2 : nsrc;
+    const int n2 = nsrc - n1;
+    auto sweep_time = [&](const std::vector<size_t> &which, const int *src, int ns,
+                          std::vector<float> &score, int &rc) {
+      for (int sweep = 0; sweep < 2 && rc == 0; ++sweep)
+        for (size_t k = 0; k < which.size() && rc == 0; ++k) {
+          const size_t ci = which[sweep == 0 ? k : which.size() - 1 - k];
+          const Cand &c = cands[ci];
+          ctx->bfs_alpha = c.alpha;
+          ctx->bfs_beta = c.beta;
+          ctx->bfs_mode = c.mode;
+          float ms = time_bfs(ctx, ns, src, nnz, m, d_ptr, d_ind, d_tptr, d_tind,
+                              d_depth_scratch, &rc);
+          if (rc == 0) score[ci] = std::min(score[ci], ms);
+        }
+    };
+    std::vector<size_t> all(cands.size());
+    for (size_t k = 0; k < cands.size(); ++k) all[k] = k;
+    std::vector<float> score(cands.size(), 1e30f), score2(cands.size(), 0.0f);
+    int rc = 0;
+    sweep_time(all, h_src, n1, score, rc);
+    std::vector<size_t> top = all;
+    std::sort(top.begin(), top.end(), [&](size_t a, size_t b) { return score[a] < score[b]; });
+    if (top.size() > 4) top.resize(4);
+    // the reference point (alpha 32, beta 128; the best over 200 sources on
+    // R-MAT 22, measured) is always re-timed, and a pick must beat it by more
+    // than 2 %: differences smaller than that are within the sampling noise of
+    // a few dozen sources, while a switch point a little too low leaves a
+    // 7 M-edge level in push on some sources (2x slower there)
+    size_t ref = cands.size();
+    for (size_t k = 0; k < cands.size(); ++k)
+      if (cands[k].alpha == 32 && cands[k].beta == 128 && cands[k].mode == 0) ref = k;
+    if (ref < cands.size() && std::find(top.begin(), top.end(), ref) == top.end())
+      top.push_back(ref);
+    if (n2 > 0 && top.size() > 1) {
+      std::fill(score2.begin(), score2.end(), 1e30f);
+      sweep_time(top, h_src + n1, n2, score2, rc);
+    }
+    ctx->bfs_mode = saved_mode;
+    if (rc) {
+      ctx->bfs_alpha = saved_alpha;
+      ctx->bfs_beta = saved_beta;
+      return rc;
+    }
+    size_t bi = top[0];
+    for (size_t ci : top)
+      if (score[ci] + score2[ci] < score[bi] + score2[bi]) bi = ci;
+    if (ref < cands.size() && bi != ref &&
+        score[bi] + score2[bi] > 0.98f * (score[ref] + score2[ref]))
+      bi = ref;
+    const Cand pick = cands[bi];
+    // "never pull" is alpha 0: no frontier satisfies edges * 0 > unexplored
+    int alpha = pick.mode == 1 ? 0 : pick.alpha;
+    ctx->bfs_alpha = alpha;
+    ctx->bfs_beta = pick.beta;
+    // then the persistent grid: as many blocks per SM as fit (3), 2 or 1,
+    // with the chosen switch points, on all the sources
+    const int bps[3] = {0, 2, 1};
+    std::vector<float> bscore;
+    rc = sweep_scores(
+        3, [&](size_t k) { ctx->bfs_blocks_per_sm = bps[k]; },
+        [&](float *ms) {
+          int r = 0;
+          *ms = time_bfs(ctx, nsrc, h_src, nnz, m, d_ptr, d_ind, d_tptr, d_tind, d_depth_scratch,
+                         &r);
+          return r;
+        },
+        bscore);
+    if (rc) {
+      ctx->bfs_alpha = saved_alpha;
+      ctx->bfs_beta = saved_beta;
+      ctx->bfs_blocks_per_sm = 0;
+      return rc;
+    }
+    const size_t bb = pick_with_margin(bscore);
+    ctx->bfs_blocks_per_sm = bps[bb];
+    const float per = bscore[bb] / nsrc;
+    ctx->tune_cache.push_back(apspie_context::TuneEntry{fp, alpha, pick.beta, per, bps[bb]});
+    *alpha_out = alpha;
+    *beta_out = pick.beta;
+    if (ms_out) *ms_out = per;
+    return APSPIE_OK;
+  });
 }
 
 int apspie_autotune_spmspv(apspie_ctx ctx, int m, int64_t nnz, const int *d_ptr, const int *d_ind,
                            const float *d_val, int *d_xind_scratch, float *d_xval_scratch,
                            int *d_yind_scratch, float *d_yval_scratch, double *factor_out) {
-  APSPIE_CHECK_CTX(ctx);
-  if (m <= 0 || !d_xind_scratch || !d_yind_scratch || !d_yval_scratch || !factor_out)
-    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_spmspv: bad arguments");
-  // frontiers of m / 2^k evenly spaced vertices; for each, time both paths
-  // and find the density where the bitmap path starts to win
-  std::vector<int> hx;
-  const double saved = ctx->spmspv_sort_factor;
-  double cross = saved;
-  bool found = false;
-  for (int k = 12; k >= 1 && !found; --k) {
-    int xn = std::max(1, m >> k);
-    hx.resize(xn);
-    for (int i = 0; i < xn; ++i) hx[i] = (int)((int64_t)i * m / xn);
-    int crc = check_cuda(ctx,
-                         cudaMemcpyAsync(d_xind_scratch, hx.data(), sizeof(int) * xn,
-                                         cudaMemcpyHostToDevice, ctx->stream),
-                         "apspie_autotune_spmspv: frontier upload");
-    if (crc) {
-      ctx->spmspv_sort_factor = saved;
-      return crc;
-    }
-    float t[2] = {0, 0};
-    int64_t expanded = 0;
-    for (int path = 0; path < 2; ++path) {
-      ctx->spmspv_sort_factor = path == 0 ? 0.0 : 1e300;  // 0: sort, 1: bitmap
-      int ynnz = 0;
-      auto once = [&]() {
-        return apspie_spmspv(ctx, APSPIE_PLUS_TIMES, m, nnz, d_ptr, d_ind, d_val, xn,
-                             d_xind_scratch, nullptr, d_yind_scratch, d_yval_scratch, &ynnz,
-                             &expanded);
-      };
-      int rc = once();  // untimed: workspace and caches
-      if (rc == APSPIE_OK)
-        rc = time_stream(
-            ctx,
-            [&]() {
-              int r = APSPIE_OK;
-              for (int k3 = 0; k3 < 3 && r == APSPIE_OK; ++k3) r = once();
-              return r;
-            },
-            &t[path]);
-      if (rc) {
+  return api_guard([&]() -> int {
+    APSPIE_CHECK_CTX(ctx);
+    if (m <= 0 || !d_xind_scratch || !d_yind_scratch || !d_yval_scratch || !factor_out)
+      return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_spmspv: bad arguments");
+    // frontiers of m / 2^k evenly spaced vertices; for each, time both paths
+    // and find the density where the bitmap path starts to win
+    std::vector<int> hx;
+    const double saved = ctx->spmspv_sort_factor;
+    double cross = saved;
+    bool found = false;
+    for (int k = 12; k >= 1 && !found; --k) {
+      int xn = std::max(1, m >> k);
+      hx.resize(xn);
+      for (int i = 0; i < xn; ++i) hx[i] = (int)((int64_t)i * m / xn);
+      int crc = check_cuda(ctx,
+                           cudaMemcpyAsync(d_xind_scratch, hx.data(), sizeof(int) * xn,
+                                           cudaMemcpyHostToDevice, ctx->stream),
+                           "apspie_autotune_spmspv: frontier upload");
+      if (crc) {
         ctx->spmspv_sort_factor = saved;
-        return rc;
+        return crc;
+      }
+      float t[2] = {0, 0};
+      int64_t expanded = 0;
+      for (int path = 0; path < 2; ++path) {
+        ctx->spmspv_sort_factor = path == 0 ? 0.0 : 1e300;  // 0: sort, 1: bitmap
+        int ynnz = 0;
+        auto once = [&]() {
+          return apspie_spmspv(ctx, APSPIE_PLUS_TIMES, m, nnz, d_ptr, d_ind, d_val, xn,
+                               d_xind_scratch, nullptr, d_yind_scratch, d_yval_scratch, &ynnz,
+                               &expanded);
+        };
+        int rc = once();  // untimed: workspace and caches
+        if (rc == APSPIE_OK)
+          rc = time_stream(
+              ctx,
+              [&]() {
+                int r = APSPIE_OK;
+                for (int k3 = 0; k3 < 3 && r == APSPIE_OK; ++k3) r = once();
+                return r;
+              },
+              &t[path]);
+        if (rc) {
+          ctx->spmspv_sort_factor = saved;
+          return rc;
+        }
+      }
+      if (t[1] < t[0] && expanded > 0) {
+        // bitmap wins from this density on: E * factor > m  <=>  factor > m / E
+        cross = (double)m / (double)expanded;
+        found = true;
       }
     }
-    if (t[1] < t[0] && expanded > 0) {
-      // bitmap wins from this density on: E * factor > m  <=>  factor > m / E
-      cross = (double)m / (double)expanded;
-      found = true;
-    }
-  }
-  ctx->spmspv_sort_factor = found ? cross : saved;
-  *factor_out = ctx->spmspv_sort_factor;
-  return APSPIE_OK;
+    ctx->spmspv_sort_factor = found ? cross : saved;
+    *factor_out = ctx->spmspv_sort_factor;
+    return APSPIE_OK;
+  });
 }
 
 int apspie_ctx_get_tuning(apspie_ctx ctx, apspie_tuning *out) {
@@ -331,206 +336,212 @@ int apspie_autotune_sssp(apspie_ctx ctx, int nsrc, const int *h_src, int64_t nnz
                          const int *d_ptr, const int *d_ind, const uint32_t *d_w,
                          const int *d_tptr, const int *d_tind, const uint32_t *d_tw,
                          uint32_t *d_dist_scratch, float *ms_out, int *cached_out) {
-  APSPIE_CHECK_CTX(ctx);
-  const bool pull = d_tptr && d_tind && d_tw;
-  if (nsrc <= 0 || !h_src || !d_w || !d_dist_scratch || m <= 0 ||
-      (!pull && (d_tptr || d_tind || d_tw)))
-    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_sssp: bad arguments");
-  const uint64_t fp = mix_fp(graph_fingerprint(ctx, m, nnz, d_ptr), pull ? 0x5353503ull : 0x5353ull);
-  if (cached_out) *cached_out = 0;
-  for (auto &e : ctx->sssp_tune_cache)
-    if (e.fp == fp) {
-      ctx->sssp_blocks_per_sm = e.blocks_per_sm;
-      ctx->sssp_pull_alpha = e.pull_alpha;
-      if (ms_out) *ms_out = e.ms;
-      if (cached_out) *cached_out = 1;
-      return APSPIE_OK;
-    }
-  struct Cand {
-    int bps, alpha;
-  };
-  // candidate 0 is the default (all resident blocks, push only)
-  std::vector<Cand> cands = {{0, 0}, {1, 0}};
-  if (pull)
-    for (int a : {2, 8}) {
-      cands.push_back(Cand{0, a});
-      cands.push_back(Cand{1, a});
-    }
-  auto run = [&](float *ms) {
-    return time_stream(
-        ctx,
-        [&]() {
-          int rc = APSPIE_OK;
-          for (int i = 0; i < nsrc && rc == APSPIE_OK; ++i)
-            rc = pull ? apspie_sssp_u32_pull(ctx, h_src[i], nnz, m, d_ptr, d_ind, d_w, d_tptr,
-                                             d_tind, d_tw, d_dist_scratch, 0)
-                      : apspie_sssp_u32(ctx, h_src[i], nnz, m, d_ptr, d_ind, d_w,
-                                        d_dist_scratch, 0);
-          return rc;
-        },
-        ms);
-  };
-  auto apply = [&](size_t k) {
-    ctx->sssp_blocks_per_sm = cands[k].bps;
-    ctx->sssp_pull_alpha = cands[k].alpha;
-  };
-  apply(0);
-  float warm = 0;
-  int rc = run(&warm);  // workspace growth and caches settle
-  std::vector<float> score;
-  if (rc == APSPIE_OK) rc = sweep_scores(cands.size(), apply, run, score);
-  if (rc) {
+  return api_guard([&]() -> int {
+    APSPIE_CHECK_CTX(ctx);
+    const bool pull = d_tptr && d_tind && d_tw;
+    if (nsrc <= 0 || !h_src || !d_w || !d_dist_scratch || m <= 0 ||
+        (!pull && (d_tptr || d_tind || d_tw)))
+      return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_sssp: bad arguments");
+    const uint64_t fp = mix_fp(graph_fingerprint(ctx, m, nnz, d_ptr), pull ? 0x5353503ull : 0x5353ull);
+    if (cached_out) *cached_out = 0;
+    for (auto &e : ctx->sssp_tune_cache)
+      if (e.fp == fp) {
+        ctx->sssp_blocks_per_sm = e.blocks_per_sm;
+        ctx->sssp_pull_alpha = e.pull_alpha;
+        if (ms_out) *ms_out = e.ms;
+        if (cached_out) *cached_out = 1;
+        return APSPIE_OK;
+      }
+    struct Cand {
+      int bps, alpha;
+    };
+    // candidate 0 is the default (all resident blocks, push only)
+    std::vector<Cand> cands = {{0, 0}, {1, 0}};
+    if (pull)
+      for (int a : {2, 8}) {
+        cands.push_back(Cand{0, a});
+        cands.push_back(Cand{1, a});
+      }
+    auto run = [&](float *ms) {
+      return time_stream(
+          ctx,
+          [&]() {
+            int rc = APSPIE_OK;
+            for (int i = 0; i < nsrc && rc == APSPIE_OK; ++i)
+              rc = pull ? apspie_sssp_u32_pull(ctx, h_src[i], nnz, m, d_ptr, d_ind, d_w, d_tptr,
+                                               d_tind, d_tw, d_dist_scratch, 0)
+                        : apspie_sssp_u32(ctx, h_src[i], nnz, m, d_ptr, d_ind, d_w,
+                                          d_dist_scratch, 0);
+            return rc;
+          },
+          ms);
+    };
+    auto apply = [&](size_t k) {
+      ctx->sssp_blocks_per_sm = cands[k].bps;
+      ctx->sssp_pull_alpha = cands[k].alpha;
+    };
     apply(0);
-    return rc;
-  }
-  const size_t bi = pick_with_margin(score);
-  apply(bi);
-  const float per = score[bi] / nsrc;
-  ctx->sssp_tune_cache.push_back(
-      apspie_context::SsspTuneEntry{fp, cands[bi].bps, cands[bi].alpha, per});
-  if (ms_out) *ms_out = per;
-  return APSPIE_OK;
+    float warm = 0;
+    int rc = run(&warm);  // workspace growth and caches settle
+    std::vector<float> score;
+    if (rc == APSPIE_OK) rc = sweep_scores(cands.size(), apply, run, score);
+    if (rc) {
+      apply(0);
+      return rc;
+    }
+    const size_t bi = pick_with_margin(score);
+    apply(bi);
+    const float per = score[bi] / nsrc;
+    ctx->sssp_tune_cache.push_back(
+        apspie_context::SsspTuneEntry{fp, cands[bi].bps, cands[bi].alpha, per});
+    if (ms_out) *ms_out = per;
+    return APSPIE_OK;
+  });
 }
 
 int apspie_autotune_spgemm(apspie_ctx ctx, const apspie_csr *A, const apspie_csr *B,
                            float *ms_out, int *cached_out) {
-  APSPIE_CHECK_CTX(ctx);
-  if (!A || !B || A->m < 0 || B->m != A->n || !A->d_ptr || !B->d_ptr)
-    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_spgemm: bad matrices");
-  const uint64_t fp = mix_fp(graph_fingerprint(ctx, A->m, A->nnz, A->d_ptr),
-                             mix_fp(graph_fingerprint(ctx, B->m, B->nnz, B->d_ptr),
-                                    ((uint64_t)A->n << 32) ^ (uint64_t)B->n));
-  if (cached_out) *cached_out = 0;
-  for (auto &e : ctx->spgemm_tune_cache)
-    if (e.fp == fp) {
-      ctx->spgemm_table_load = e.table_load;
-      ctx->spgemm_warp_max_prod = e.warp_max_prod;
-      ctx->spgemm_bitmap_max_cols = e.bitmap_max_cols;
-      if (ms_out) *ms_out = e.ms;
-      if (cached_out) *cached_out = 1;
-      return APSPIE_OK;
+  return api_guard([&]() -> int {
+    APSPIE_CHECK_CTX(ctx);
+    if (!A || !B || A->m < 0 || B->m != A->n || !A->d_ptr || !B->d_ptr)
+      return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_spgemm: bad matrices");
+    const uint64_t fp = mix_fp(graph_fingerprint(ctx, A->m, A->nnz, A->d_ptr),
+                               mix_fp(graph_fingerprint(ctx, B->m, B->nnz, B->d_ptr),
+                                      ((uint64_t)A->n << 32) ^ (uint64_t)B->n));
+    if (cached_out) *cached_out = 0;
+    for (auto &e : ctx->spgemm_tune_cache)
+      if (e.fp == fp) {
+        ctx->spgemm_table_load = e.table_load;
+        ctx->spgemm_warp_max_prod = e.warp_max_prod;
+        ctx->spgemm_bitmap_max_cols = e.bitmap_max_cols;
+        if (ms_out) *ms_out = e.ms;
+        if (cached_out) *cached_out = 1;
+        return APSPIE_OK;
+      }
+    struct Cand {
+      int load, warp;
+      long long bitmap;
+    };
+    const long long kBitmapCols = 1 << 18;
+    // candidate 0 is the default
+    std::vector<Cand> cands;
+    for (long long bm : {kBitmapCols, 0ll}) {
+      if (bm == 0 && B->n > kBitmapCols) continue;  // the same as the default
+      for (int load : {2, 4})
+        for (int warp : {256, 64}) cands.push_back(Cand{load, warp, bm});
     }
-  struct Cand {
-    int load, warp;
-    long long bitmap;
-  };
-  const long long kBitmapCols = 1 << 18;
-  // candidate 0 is the default
-  std::vector<Cand> cands;
-  for (long long bm : {kBitmapCols, 0ll}) {
-    if (bm == 0 && B->n > kBitmapCols) continue;  // the same as the default
-    for (int load : {2, 4})
-      for (int warp : {256, 64}) cands.push_back(Cand{load, warp, bm});
-  }
-  auto apply = [&](size_t k) {
-    ctx->spgemm_table_load = cands[k].load;
-    ctx->spgemm_warp_max_prod = cands[k].warp;
-    ctx->spgemm_bitmap_max_cols = cands[k].bitmap;
-  };
-  apply(0);
-  // C's structure does not depend on the choices: allocated once
-  int *Cptr = nullptr, *Cind = nullptr;
-  float *Cval = nullptr;
-  int64_t nnzC = 0;
-  int rc = check_cuda(ctx, cudaMalloc(&Cptr, sizeof(int) * ((size_t)A->m + 1)),
-                      "apspie_autotune_spgemm: allocating C");
-  if (rc == APSPIE_OK) rc = apspie_spgemm_symbolic(ctx, A, B, Cptr, &nnzC);
-  if (rc == APSPIE_OK)
-    rc = check_cuda(ctx, cudaMalloc(&Cind, sizeof(int) * (size_t)std::max<int64_t>(1, nnzC)),
-                    "apspie_autotune_spgemm: allocating C");
-  if (rc == APSPIE_OK)
-    rc = check_cuda(ctx, cudaMalloc(&Cval, sizeof(float) * (size_t)std::max<int64_t>(1, nnzC)),
-                    "apspie_autotune_spgemm: allocating C");
-  auto run = [&](float *ms) {
-    return time_stream(
-        ctx,
-        [&]() {
-          int64_t nz = 0;
-          int r = apspie_spgemm_symbolic(ctx, A, B, Cptr, &nz);
-          if (r == APSPIE_OK && nz != nnzC)
-            r = set_error(ctx, APSPIE_ERR_CUDA, "apspie_autotune_spgemm: nnz(C) changed");
-          if (r == APSPIE_OK) r = apspie_spgemm_numeric(ctx, A, B, Cptr, Cind, Cval);
-          return r;
-        },
-        ms);
-  };
-  float warm = 0;
-  if (rc == APSPIE_OK) rc = run(&warm);
-  std::vector<float> score;
-  if (rc == APSPIE_OK) rc = sweep_scores(cands.size(), apply, run, score);
-  cudaStreamSynchronize(ctx->stream);
-  cudaFree(Cptr);
-  cudaFree(Cind);
-  cudaFree(Cval);
-  ctx->spgemm_plan_valid = false;
-  if (rc) {
+    auto apply = [&](size_t k) {
+      ctx->spgemm_table_load = cands[k].load;
+      ctx->spgemm_warp_max_prod = cands[k].warp;
+      ctx->spgemm_bitmap_max_cols = cands[k].bitmap;
+    };
     apply(0);
-    return rc;
-  }
-  const size_t bi = pick_with_margin(score);
-  apply(bi);
-  ctx->spgemm_tune_cache.push_back(apspie_context::SpgemmTuneEntry{
-      fp, cands[bi].load, cands[bi].warp, cands[bi].bitmap, score[bi]});
-  if (ms_out) *ms_out = score[bi];
-  return APSPIE_OK;
+    // C's structure does not depend on the choices: allocated once
+    int *Cptr = nullptr, *Cind = nullptr;
+    float *Cval = nullptr;
+    int64_t nnzC = 0;
+    int rc = check_cuda(ctx, cudaMalloc(&Cptr, sizeof(int) * ((size_t)A->m + 1)),
+                        "apspie_autotune_spgemm: allocating C");
+    if (rc == APSPIE_OK) rc = apspie_spgemm_symbolic(ctx, A, B, Cptr, &nnzC);
+    if (rc == APSPIE_OK)
+      rc = check_cuda(ctx, cudaMalloc(&Cind, sizeof(int) * (size_t)std::max<int64_t>(1, nnzC)),
+                      "apspie_autotune_spgemm: allocating C");
+    if (rc == APSPIE_OK)
+      rc = check_cuda(ctx, cudaMalloc(&Cval, sizeof(float) * (size_t)std::max<int64_t>(1, nnzC)),
+                      "apspie_autotune_spgemm: allocating C");
+    auto run = [&](float *ms) {
+      return time_stream(
+          ctx,
+          [&]() {
+            int64_t nz = 0;
+            int r = apspie_spgemm_symbolic(ctx, A, B, Cptr, &nz);
+            if (r == APSPIE_OK && nz != nnzC)
+              r = set_error(ctx, APSPIE_ERR_CUDA, "apspie_autotune_spgemm: nnz(C) changed");
+            if (r == APSPIE_OK) r = apspie_spgemm_numeric(ctx, A, B, Cptr, Cind, Cval);
+            return r;
+          },
+          ms);
+    };
+    float warm = 0;
+    if (rc == APSPIE_OK) rc = run(&warm);
+    std::vector<float> score;
+    if (rc == APSPIE_OK) rc = sweep_scores(cands.size(), apply, run, score);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(Cptr);
+    cudaFree(Cind);
+    cudaFree(Cval);
+    ctx->spgemm_plan_valid = false;
+    if (rc) {
+      apply(0);
+      return rc;
+    }
+    const size_t bi = pick_with_margin(score);
+    apply(bi);
+    ctx->spgemm_tune_cache.push_back(apspie_context::SpgemmTuneEntry{
+        fp, cands[bi].load, cands[bi].warp, cands[bi].bitmap, score[bi]});
+    if (ms_out) *ms_out = score[bi];
+    return APSPIE_OK;
+  });
 }
 
 int apspie_autotune_batch(apspie_ctx ctx, int njobs, const apspie_job *jobs, float *ms_out,
                           int *cached_out) {
-  APSPIE_CHECK_CTX(ctx);
-  if (njobs <= 0 || !jobs)
-    return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_batch: no jobs");
-  uint64_t fp = 0x42415443ull;
-  for (int j = 0; j < njobs; ++j) {
-    if (jobs[j].m <= 0 || !jobs[j].d_ptr)
-      return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_batch: bad job %d", j);
-    fp = mix_fp(fp, graph_fingerprint(ctx, jobs[j].m, jobs[j].nnz, jobs[j].d_ptr));
-    fp = mix_fp(fp, ((uint64_t)jobs[j].type << 32) ^ (uint64_t)(uint32_t)jobs[j].nsrc);
-  }
-  if (cached_out) *cached_out = 0;
-  for (auto &e : ctx->batch_tune_cache)
-    if (e.fp == fp) {
-      ctx->batch_blocks_per_sm = e.blocks_per_sm;
-      ctx->deep_blocks = e.deep_blocks;
-      if (ms_out) *ms_out = e.ms;
-      if (cached_out) *cached_out = 1;
-      return APSPIE_OK;
+  return api_guard([&]() -> int {
+    APSPIE_CHECK_CTX(ctx);
+    if (njobs <= 0 || !jobs)
+      return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_batch: no jobs");
+    uint64_t fp = 0x42415443ull;
+    for (int j = 0; j < njobs; ++j) {
+      if (jobs[j].m <= 0 || !jobs[j].d_ptr)
+        return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_batch: bad job %d", j);
+      fp = mix_fp(fp, graph_fingerprint(ctx, jobs[j].m, jobs[j].nnz, jobs[j].d_ptr));
+      fp = mix_fp(fp, ((uint64_t)jobs[j].type << 32) ^ (uint64_t)(uint32_t)jobs[j].nsrc);
     }
-  auto run = [&](float *ms) {
-    return time_stream(ctx, [&]() { return apspie_batch_run(ctx, njobs, jobs, 0); }, ms);
-  };
-  struct Cand {
-    int bps, deep;
-  };
-  std::vector<Cand> cands = {{0, 0}, {1, 0}};
-  auto apply = [&](size_t k) {
-    ctx->batch_blocks_per_sm = cands[k].bps;
-    ctx->deep_blocks = cands[k].deep;
-  };
-  apply(0);
-  float warm = 0;
-  int rc = run(&warm);  // workspaces, depth probes of new graphs
-  if (rc == APSPIE_OK && ctx->batch_subs_used > 0) {
-    // deep-graph sources ran beside the multi-source launch: their share of
-    // the resident blocks (0 = half) is a choice too
-    int occ = 0;
-    int full = 0;
-    if (apspie_ctx_resident_blocks(ctx, &occ) == APSPIE_OK) full = occ;
-    if (full >= 4)
-      for (int d : {full / 4, (3 * full) / 4}) cands.push_back(Cand{0, d});
-  }
-  std::vector<float> score;
-  if (rc == APSPIE_OK) rc = sweep_scores(cands.size(), apply, run, score);
-  if (rc) {
+    if (cached_out) *cached_out = 0;
+    for (auto &e : ctx->batch_tune_cache)
+      if (e.fp == fp) {
+        ctx->batch_blocks_per_sm = e.blocks_per_sm;
+        ctx->deep_blocks = e.deep_blocks;
+        if (ms_out) *ms_out = e.ms;
+        if (cached_out) *cached_out = 1;
+        return APSPIE_OK;
+      }
+    auto run = [&](float *ms) {
+      return time_stream(ctx, [&]() { return apspie_batch_run(ctx, njobs, jobs, 0); }, ms);
+    };
+    struct Cand {
+      int bps, deep;
+    };
+    std::vector<Cand> cands = {{0, 0}, {1, 0}};
+    auto apply = [&](size_t k) {
+      ctx->batch_blocks_per_sm = cands[k].bps;
+      ctx->deep_blocks = cands[k].deep;
+    };
     apply(0);
-    return rc;
-  }
-  const size_t bi = pick_with_margin(score);
-  apply(bi);
-  ctx->batch_tune_cache.push_back(
-      apspie_context::BatchTuneEntry{fp, cands[bi].bps, cands[bi].deep, score[bi]});
-  if (ms_out) *ms_out = score[bi];
-  return APSPIE_OK;
+    float warm = 0;
+    int rc = run(&warm);  // workspaces, depth probes of new graphs
+    if (rc == APSPIE_OK && ctx->batch_subs_used > 0) {
+      // deep-graph sources ran beside the multi-source launch: their share of
+      // the resident blocks (0 = half) is a choice too
+      int occ = 0;
+      int full = 0;
+      if (apspie_ctx_resident_blocks(ctx, &occ) == APSPIE_OK) full = occ;
+      if (full >= 4)
+        for (int d : {full / 4, (3 * full) / 4}) cands.push_back(Cand{0, d});
+    }
+    std::vector<float> score;
+    if (rc == APSPIE_OK) rc = sweep_scores(cands.size(), apply, run, score);
+    if (rc) {
+      apply(0);
+      return rc;
+    }
+    const size_t bi = pick_with_margin(score);
+    apply(bi);
+    ctx->batch_tune_cache.push_back(
+        apspie_context::BatchTuneEntry{fp, cands[bi].bps, cands[bi].deep, score[bi]});
+    if (ms_out) *ms_out = score[bi];
+    return APSPIE_OK;
+  });
 }
 
 }  // extern "C"
