@@ -67,7 +67,34 @@ class Context:
 
 
 def _p(t) -> C.c_void_p:
-    return C.c_void_p(0 if t is None else t.data_ptr())
+    """Device pointer of a tensor for the C ABI (0 for None).  The kernels
+    read a tensor's storage as one dense array in device memory, so a host
+    tensor or a strided view is refused here, before anything is launched."""
+    if t is None:
+        return C.c_void_p(0)
+    if not t.is_cuda:
+        raise ValueError(f"apspie_b200: expected a CUDA tensor, got one on {t.device}")
+    if not t.is_contiguous():
+        raise ValueError("apspie_b200: expected a contiguous tensor, got a strided view")
+    return C.c_void_p(t.data_ptr())
+
+
+def _row(t, n: int, what: str):
+    """A caller's per-vertex tensor: at least n entries of 32 bits (the
+    kernels read or write n of them)."""
+    if t is not None and (t.numel() < n or t.element_size() != 4):
+        raise ValueError(f"{what}: needs {n} 32-bit entries, got {t.numel()} of "
+                         f"{t.element_size()} bytes")
+    return t
+
+
+def _graph(g):
+    """A device graph's arrays hold what m and nnz promise (m + 1 offsets,
+    nnz indices, 32-bit entries)."""
+    _row(g.ptr, g.m + 1, "graph row offsets")
+    if g.nnz > 0:
+        _row(g.ind, g.nnz, "graph column indices")
+    return g
 
 
 def bfs(ctx: Context, g, src: int, depth=None, max_levels: int = 0):
@@ -76,8 +103,10 @@ def bfs(ctx: Context, g, src: int, depth=None, max_levels: int = 0):
     for a symmetric graph; a directed graph without them is traversed by
     push only."""
     import torch
+    _graph(g)
     if depth is None:
         depth = torch.empty(g.m, dtype=torch.int32, device=g.ptr.device)
+    _row(depth, g.m, "depth")
     if getattr(g, "tptr", None) is not None:
         tptr, tind = g.tptr, g.tind
     else:
@@ -169,6 +198,9 @@ def sssp(ctx: Context, g, src: int, dist=None, weights: str = "u32", max_rounds:
         raise ValueError(weights)
     if w is None:
         raise ValueError(f"graph has no {weights} weights")
+    _graph(g)
+    _row(dist, g.m, "dist")
+    _row(w, g.nnz, f"{weights} weights")
     tin = g.extra.get("sssp_in", {}).get(weights)
     if tin is not None:
         # in-adjacency with its weights from sssp_prepare: push/pull rounds
@@ -234,8 +266,11 @@ def mis(ctx: Context, g, prio, out=None, delta: float = 1.0):
     """spmspvMis<V>() (src/spmspvMis.cuh:150): int32 membership (1 / 0).
     prio: device tensor of uint32 priorities (int32 view)."""
     import torch
+    _graph(g)
+    _row(prio, g.m, "prio")
     if out is None:
         out = torch.empty(g.m, dtype=torch.int32, device=g.ptr.device)
+    _row(out, g.m, "out")
     check(lib.apspie_mis(ctx.handle, int(g.nnz), int(g.m), _p(g.ptr), _p(g.ind), _p(prio),
                          _p(out), float(delta)), ctx.handle, "apspie_mis")
     return out
@@ -250,8 +285,11 @@ def mis_rounds(ctx: Context) -> int:
 def neighbor_flags(ctx: Context, g, flags, out=None):
     """spmspvCsr() (src/spmspvMis.cuh:81): 1 for out-neighbours of flagged vertices."""
     import torch
+    _graph(g)
+    _row(flags, g.m, "flags")
     if out is None:
         out = torch.empty(g.m, dtype=torch.int32, device=g.ptr.device)
+    _row(out, g.m, "out")
     check(lib.apspie_neighbor_flags(ctx.handle, int(g.nnz), int(g.m), _p(g.ptr), _p(g.ind),
                                     _p(flags), _p(out)), ctx.handle, "apspie_neighbor_flags")
     return out
@@ -264,6 +302,9 @@ def spmspv(ctx: Context, semiring: int, g, xind, xval=None, val=None):
     """Sparse mXv<T>() (src/mXv.cuh:250): returns (yind, yval, expanded).
     g.ptr / g.ind list the columns of A; val (float32 tensor, nnz) or None."""
     import torch
+    _graph(g)
+    _row(val, g.nnz, "val")
+    _row(xval, xind.numel(), "xval")
     dev = g.ptr.device
     yind = torch.empty(max(g.m, 1), dtype=torch.int32, device=dev)
     yval = torch.empty(max(g.m, 1), dtype=torch.float32, device=dev)
@@ -278,8 +319,12 @@ def spmspv(ctx: Context, semiring: int, g, xind, xval=None, val=None):
 def mxv_dense(ctx: Context, semiring: int, g, x, val=None, y=None):
     """Dense mXv<T>() (src/mXv.cuh:111): returns (y, total)."""
     import torch
+    _graph(g)
+    _row(val, g.nnz, "val")
+    _row(x, g.m, "x")
     if y is None:
         y = torch.empty(g.m, dtype=torch.float32, device=g.ptr.device)
+    _row(y, g.m, "y")
     e = C.c_int64()
     check(lib.apspie_mxv_dense(ctx.handle, int(semiring), int(g.m), int(g.nnz), _p(g.ptr),
                                _p(g.ind), _p(val), _p(x), _p(y), C.byref(e)), ctx.handle,
@@ -293,8 +338,8 @@ def spmspv_set_params(ctx: Context, sort_factor: float = 4.0) -> None:
 
 def _csr(m, n, ptr, ind, val) -> Csr:
     return Csr(int(m), int(n), int(ind.numel()) if ind is not None else 0,
-               C.c_void_p(ptr.data_ptr()), C.c_void_p(0 if ind is None else ind.data_ptr()),
-               C.c_void_p(0 if val is None else val.data_ptr()))
+               _p(ptr), _p(ind),
+               _p(val))
 
 
 def spmv(ctx: Context, m: int, ptr, ind, val, x, semiring: int = 0, y=None):
@@ -361,9 +406,9 @@ def _take_csr(ctx: Context, c: Csr, with_val: bool):
         ptr = torch.empty(c.m + 1, dtype=torch.int32, device=dev)
         ind = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
         val = torch.empty(max(nnz, 1), dtype=torch.float32, device=dev) if with_val else None
-        check(lib.apspie_csr_copy_out(ctx.handle, C.byref(c), C.c_void_p(ptr.data_ptr()),
-                                      C.c_void_p(ind.data_ptr()),
-                                      C.c_void_p(val.data_ptr() if with_val else 0)),
+        check(lib.apspie_csr_copy_out(ctx.handle, C.byref(c), _p(ptr),
+                                      _p(ind),
+                                      _p(val if with_val else None)),
               ctx.handle, "apspie_csr_copy_out")
         ctx.sync()
     finally:
@@ -462,18 +507,18 @@ def _job_array(jobs: list[dict]):
         tptr = None if sym else getattr(g, "tptr", None)
         tind = None if sym else getattr(g, "tind", None)
         arr[i] = Job(JOB_BFS if jd["type"] == "bfs" else JOB_SSSP_U32, int(g.m), int(g.nnz),
-                     C.c_void_p(g.ptr.data_ptr()), C.c_void_p(g.ind.data_ptr()),
-                     C.c_void_p(0 if tptr is None else tptr.data_ptr()),
-                     C.c_void_p(0 if tind is None else tind.data_ptr()),
-                     C.c_void_p(0 if g.w_u32 is None else g.w_u32.data_ptr()), int(sym),
-                     len(jd["sources"]), src, C.c_void_p(out.data_ptr()),
+                     _p(g.ptr), _p(g.ind),
+                     _p(tptr),
+                     _p(tind),
+                     _p(g.w_u32), int(sym),
+                     len(jd["sources"]), src, _p(out),
                      int(jd.get("alpha", -1)), int(jd.get("beta", -1)))
         sin = g.extra.get("sssp_in", {}).get("u32") if jd["type"] == "sssp" else None
         if sin is not None:
             # in-adjacency with weights from sssp_prepare: pull steps
-            arr[i].d_stptr = C.c_void_p(sin[0].data_ptr())
-            arr[i].d_stind = C.c_void_p(sin[1].data_ptr())
-            arr[i].d_stw = C.c_void_p(sin[2].data_ptr())
+            arr[i].d_stptr = _p(sin[0])
+            arr[i].d_stind = _p(sin[1])
+            arr[i].d_stw = _p(sin[2])
     return arr, outs, keep
 
 

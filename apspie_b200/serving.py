@@ -8,6 +8,7 @@ import ctypes as C
 import numpy as np
 
 from ._native import ApspieError, ServerStats, check, lib
+from .ops import _p
 
 BFS, SSSP, MIS = 0, 1, 2
 
@@ -29,7 +30,7 @@ class Server:
         sym = bool(getattr(g, "symmetric", False))
         tptr = None if sym else getattr(g, "tptr", None)
         tind = None if sym else getattr(g, "tind", None)
-        p = lambda t: C.c_void_p(0 if t is None else t.data_ptr())
+        p = _p
         check(lib.apspie_server_add_graph(self._h, int(g.m), int(g.nnz), p(g.ptr), p(g.ind),
                                           p(tptr), p(tind), p(g.w_u32), int(sym), C.byref(gid)),
               what="apspie_server_add_graph")
@@ -59,11 +60,13 @@ class Server:
         m entries), or dropped when out is None."""
         if not 0 <= graph < len(self._graphs):
             raise ApspieError(2, f"apspie_server_submit_device: unknown graph {graph}")
+        m = self._graphs[graph].m
+        if out is not None and (out.numel() < m or out.dtype.itemsize != 4):
+            raise ValueError(f"out: needs a device row of {m} 32-bit entries")
         rid = C.c_uint64()
         check(lib.apspie_server_submit_device(self._h, int(kind), int(graph), int(source),
-                                              int(seed),
-                                              C.c_void_p(0 if out is None else out.data_ptr()),
-                                              C.byref(rid)), what="apspie_server_submit_device")
+                                              int(seed), _p(out), C.byref(rid)),
+              what="apspie_server_submit_device")
         self._live[rid.value] = out
         return rid.value
 
@@ -85,9 +88,9 @@ class Server:
             rows = (C.c_void_p * len(q))()
             for i, t in keep.items():
                 m = self._graphs[int(q["graph"][i])].m
-                if t.numel() < m or t.dtype.itemsize != 4 or not t.is_cuda:
+                if t.numel() < m or t.dtype.itemsize != 4:
                     raise ValueError(f"keep[{i}]: needs a device row of {m} 32-bit entries")
-                rows[i] = t.data_ptr()
+                rows[i] = _p(t).value  # a contiguous CUDA tensor, or ValueError
             check(lib.apspie_server_replay_keep(self._h, len(q), C.c_void_p(q.ctypes.data),
                                                 int(bool(to_host)), rows,
                                                 C.c_void_p(lat.ctypes.data), C.byref(wall)),
