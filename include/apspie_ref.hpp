@@ -51,7 +51,7 @@ inline void check(int st, apspie_ctx ctx, const char *what) {
 namespace mgpu {
 class CudaContext {
  public:
-  explicit CudaContext(int device = 0, cudaStream_t stream = nullptr) {
+  explicit CudaContext(int device = 0, cudaStream_t stream = nullptr) : stream_(stream) {
     apspie::check(apspie_ctx_create(device, stream, &h_), nullptr, "apspie_ctx_create");
   }
   ~CudaContext() { apspie_ctx_destroy(h_); }
@@ -103,7 +103,7 @@ inline void matrix_new(d_matrix *A, int m, int n) {
   A->n = n;
   A->nnz = 0;
   A->h_cscColPtr = (int *)calloc((size_t)m + 1, sizeof(int));
-  if (cudaMalloc(&A->d_cscColPtr, sizeof(int) * ((size_t)m + 1)) != cudaSuccess)
+  if (!A->h_cscColPtr || cudaMalloc(&A->d_cscColPtr, sizeof(int) * ((size_t)m + 1)) != cudaSuccess)
     throw apspie::Error(APSPIE_ERR_OOM, "matrix_new");
 }
 
@@ -112,9 +112,17 @@ inline void matrix_new(d_matrix *A, int m, int n) {
 template <typename typeVal>
 void buildMatrix(d_matrix *A, int numEdge, int *h_cooRowInd, int *h_cooColInd,
                  typeVal *h_cooVal) {
+  // the COO entries index host arrays here: checked first (the reference
+  // trusts them)
+  for (int i = 0; i < numEdge; ++i)
+    if (h_cooRowInd[i] < 0 || h_cooRowInd[i] >= A->m || h_cooColInd[i] < 0 ||
+        h_cooColInd[i] >= A->n)
+      throw apspie::Error(APSPIE_ERR_INVALID, "buildMatrix: entry " + std::to_string(i) +
+                                                  " outside the matrix");
   A->nnz = numEdge;
   A->h_cscRowInd = (int *)malloc(sizeof(int) * (size_t)(numEdge > 0 ? numEdge : 1));
   A->h_cscVal = (float *)malloc(sizeof(float) * (size_t)(numEdge > 0 ? numEdge : 1));
+  if (!A->h_cscRowInd || !A->h_cscVal) throw apspie::Error(APSPIE_ERR_OOM, "buildMatrix");
   std::vector<int> cnt((size_t)A->m + 1, 0);
   for (int i = 0; i < numEdge; ++i) cnt[(size_t)h_cooRowInd[i] + 1]++;
   for (int i = 0; i < A->m; ++i) cnt[(size_t)i + 1] += cnt[(size_t)i];
@@ -128,10 +136,13 @@ void buildMatrix(d_matrix *A, int numEdge, int *h_cooRowInd, int *h_cooColInd,
   if (cudaMalloc(&A->d_cscRowInd, sizeof(int) * nb) != cudaSuccess ||
       cudaMalloc(&A->d_cscVal, sizeof(float) * nb) != cudaSuccess)
     throw apspie::Error(APSPIE_ERR_OOM, "buildMatrix");
-  cudaMemcpy(A->d_cscColPtr, A->h_cscColPtr, sizeof(int) * ((size_t)A->m + 1),
-             cudaMemcpyHostToDevice);
-  cudaMemcpy(A->d_cscRowInd, A->h_cscRowInd, sizeof(int) * nb, cudaMemcpyHostToDevice);
-  cudaMemcpy(A->d_cscVal, A->h_cscVal, sizeof(float) * nb, cudaMemcpyHostToDevice);
+  if (cudaMemcpy(A->d_cscColPtr, A->h_cscColPtr, sizeof(int) * ((size_t)A->m + 1),
+                 cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(A->d_cscRowInd, A->h_cscRowInd, sizeof(int) * nb, cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMemcpy(A->d_cscVal, A->h_cscVal, sizeof(float) * nb, cudaMemcpyHostToDevice) !=
+          cudaSuccess)
+    throw apspie::Error(APSPIE_ERR_CUDA, "buildMatrix: upload");
 }
 
 inline void matrix_delete(d_matrix *A) {
@@ -195,6 +206,7 @@ template <typename Value>
 void spmspvSssp(const Value *d_randVec, const int edge, const int m, const Value *d_csrVal,
                 const int *d_csrRowPtr, const int *d_csrColInd, Value *d_misResult,
                 mgpu::CudaContext &context) {
+  static_assert(std::is_same<Value, float>::value, "spmspvSssp: float values");
   apspie::check(apspie_mxv_dense(context.handle(), APSPIE_MIN_PLUS, m, edge, d_csrRowPtr,
                                  d_csrColInd, (const float *)d_csrVal, (const float *)d_randVec,
                                  (float *)d_misResult, nullptr),
@@ -229,6 +241,7 @@ template <typename T>
 int mXv(const T *d_randVec, const int edge, const int m, const T *d_cscVal,
         const int *d_cscColPtr, const int *d_cscRowInd, T *d_mmResult, d_scratch *d,
         mgpu::CudaContext &context) {
+  static_assert(std::is_same<T, float>::value, "mXv: float values (the kernels compute in float)");
   (void)d;
   int64_t total = 0;
   apspie::check(apspie_mxv_dense(context.handle(), APSPIE_PLUS_TIMES, m, edge, d_cscColPtr,
@@ -243,6 +256,7 @@ template <typename T>
 void mXv(const int *d_randVecInd, const T *d_randVecVal, const int edge, const int m, int &nnz,
          const T *d_cscVal, const int *d_cscColPtr, const int *d_cscRowInd, int *d_resultInd,
          T *d_resultVal, d_scratch *d, mgpu::CudaContext &context) {
+  static_assert(std::is_same<T, float>::value, "mXv: float values (the kernels compute in float)");
   (void)d;
   int out = 0;
   apspie::check(apspie_spmspv(context.handle(), APSPIE_PLUS_TIMES, m, edge, d_cscColPtr,
@@ -259,6 +273,7 @@ template <typename T>
 void spmv(const T *d_inputVector, const int edge, const int m, const T *d_csrValA,
           const int *d_csrRowPtrA, const int *d_csrColIndA, T *d_spmvResult,
           mgpu::CudaContext &context) {
+  static_assert(std::is_same<T, float>::value, "spmv: float values");
   apspie::check(apspie_spmv(context.handle(), APSPIE_PLUS_TIMES, m, edge, d_csrRowPtrA,
                             d_csrColIndA, (const float *)d_csrValA, (const float *)d_inputVector,
                             (float *)d_spmvResult),
@@ -271,6 +286,7 @@ template <typename typeVal>
 void csr2csc(const int m, const int edge, const typeVal *d_csrValA, const int *d_csrRowPtrA,
              const int *d_csrColIndA, typeVal *d_cscValA, int *d_cscRowIndA, int *d_cscColPtrA,
              mgpu::CudaContext &context) {
+  static_assert(std::is_same<typeVal, float>::value, "csr2csc: float values");
   apspie::check(apspie_csr_transpose(context.handle(), m, m, edge, d_csrRowPtrA, d_csrColIndA,
                                      (const float *)d_csrValA, d_cscColPtrA, d_cscRowIndA,
                                      (float *)d_cscValA),
@@ -371,11 +387,16 @@ int mXm(const int edge, const int m, const T *d_cscValA, const int *d_cscColPtrA
 inline long long triangleCount(const int edge, const int m, const int *d_ptr, const int *d_ind,
                                mgpu::CudaContext &context) {
   int *perm = nullptr, *lp = nullptr, *li = nullptr;
-  cudaMalloc(&perm, sizeof(int) * (size_t)m);
-  cudaMalloc(&lp, sizeof(int) * ((size_t)m + 1));
-  cudaMalloc(&li, sizeof(int) * (size_t)(edge / 2 + 1));
   int64_t lnnz = 0, count = 0;
-  int st = apspie_tc_prepare(context.handle(), edge, m, d_ptr, d_ind, perm, lp, li, &lnnz);
+  int st = APSPIE_OK;
+  if (cudaMalloc(&perm, sizeof(int) * (size_t)m) != cudaSuccess ||
+      cudaMalloc(&lp, sizeof(int) * ((size_t)m + 1)) != cudaSuccess ||
+      cudaMalloc(&li, sizeof(int) * (size_t)(edge / 2 + 1)) != cudaSuccess) {
+    cudaGetLastError();
+    st = APSPIE_ERR_OOM;
+  }
+  if (st == APSPIE_OK)
+    st = apspie_tc_prepare(context.handle(), edge, m, d_ptr, d_ind, perm, lp, li, &lnnz);
   if (st == APSPIE_OK) st = apspie_tc(context.handle(), m, lnnz, lp, li, &count);
   cudaFree(perm);
   cudaFree(lp);
