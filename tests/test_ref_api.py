@@ -56,3 +56,52 @@ def test_driver_correct_on_fixtures(driver, golden, fixture_names, tmp_path, alg
         res = subprocess.run(args, capture_output=True, text=True, timeout=120)
         assert res.returncode == 0, f"{name}: {res.stdout}\n{res.stderr}"
         assert "CORRECT" in res.stdout and "INCORRECT" not in res.stdout
+
+
+CHECKS_SRC = r"""
+#include <cstdio>
+#include <cstdlib>
+#include "apspie_ref.hpp"
+// buildMatrix refuses COO entries outside the matrix before it writes a host
+// array or touches the device (so this runs without a GPU).
+static int expect_invalid(d_matrix *A, int n, int *r, int *c, float *v) {
+  try {
+    buildMatrix<float>(A, n, r, c, v);
+  } catch (const apspie::Error &e) {
+    return e.status == APSPIE_ERR_INVALID ? 0 : 1;
+  }
+  return 1;
+}
+int main() {
+  d_matrix A;
+  A.m = 3;
+  A.n = 3;
+  A.h_cscColPtr = (int *)calloc(4, sizeof(int));
+  int r0[2] = {0, 3}, c0[2] = {1, 1};     // row 3 of 3
+  int r1[1] = {0}, c1[1] = {-1};          // column -1
+  int r2[1] = {-2}, c2[1] = {0};          // row -2
+  int r3[1] = {2}, c3[1] = {3};           // column 3 of 3
+  float v[2] = {1.0f, 1.0f};
+  int bad = expect_invalid(&A, 2, r0, c0, v) + expect_invalid(&A, 1, r1, c1, v) +
+            expect_invalid(&A, 1, r2, c2, v) + expect_invalid(&A, 1, r3, c3, v);
+  free(A.h_cscColPtr);
+  printf(bad ? "FAILED\n" : "ok\n");
+  return bad;
+}
+"""
+
+
+def test_build_matrix_refuses_entries_outside_the_matrix(tmp_path):
+    """The shim's buildMatrix indexes host arrays by the caller's COO rows;
+    entries outside [0, m) x [0, n) raise apspie::Error(APSPIE_ERR_INVALID)
+    instead of writing past them."""
+    src = tmp_path / "checks.cpp"
+    src.write_text(CHECKS_SRC)
+    out = tmp_path / "checks"
+    cmd = ["g++", "-O1", "-std=c++17", f"-I{ROOT / 'include'}", f"-I{CUDA / 'include'}",
+           str(src), "-o", str(out), f"-L{CUDA / 'lib64'}", "-lcudart",
+           f"-Wl,-rpath,{CUDA / 'lib64'}"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+    run = subprocess.run([str(out)], capture_output=True, text=True, timeout=60)
+    assert run.returncode == 0 and run.stdout.strip() == "ok", run.stdout + run.stderr
