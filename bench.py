@@ -724,7 +724,11 @@ def run_ours(args):
            "note": "graph CSR copied host->device and depths device->host every step"}
 
     extras = {}
-    if not args.profile_run and rank == 0:
+    # The other legs are single-GPU measurements of their own configurations.
+    # They run at N=1 only: under torchrun the other ranks would wait at the
+    # closing barrier for minutes, past the process group's timeout, while
+    # holding their GPUs idle.
+    if not args.profile_run and rank == 0 and world == 1:
         extras["sssp"] = sssp_leg(ctx, h)
         extras["mis_tc_spgemm"] = mis_tc_spgemm_leg(ctx)
         extras["batched"] = batched_leg(ctx, h)
