@@ -83,7 +83,8 @@ PROTOS: dict[str, tuple] = {
     "apspie_last_error": (C.c_char_p, [vp]),
     "apspie_status_string": (C.c_char_p, [c_int]),
     "apspie_bfs": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, vp, c_int]),
-    "apspie_bfs_noalloc": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, vp, c_int, vp]),
+    "apspie_bfs_noalloc": (c_int, [vp, c_int, c_i64, c_int, vp, vp, vp, vp, vp, c_int]),
+    "apspie_bfs_noalloc_status": (c_int, [vp, vp]),
     "apspie_debug_inject": (c_int, [vp, c_int]),
     "apspie_server_debug_fail_next": (c_int, [vp, c_int]),
     "apspie_bfs_get_stats": (c_int, [vp, C.POINTER(BfsStats)]),

@@ -659,7 +659,7 @@ __global__ void set_word(int *p, int v) { *p = v; }
 
 extern "C" int apspie_bfs_noalloc(void *stream, int src, int64_t nnz, int m, const int *d_ptr,
                                   const int *d_ind, const int *d_tptr, const int *d_tind,
-                                  int32_t *d_depth, int max_levels, int32_t *d_status) {
+                                  int32_t *d_depth, int max_levels) {
   using namespace apspie;
   if (m <= 0 || src < 0 || src >= m || nnz < 0) return APSPIE_ERR_INVALID;
   if (m > kNoAllocMaxVertices || nnz > kNoAllocMaxEdges) return APSPIE_ERR_TOO_LARGE;
@@ -697,10 +697,25 @@ extern "C" int apspie_bfs_noalloc(void *stream, int src, int64_t nnz, int m, con
     cudaGetLastError();
     return APSPIE_ERR_CUDA;
   }
-  if (d_status) {
-    bfs_write_status<<<1, 1, 0, st>>>(state, d_status);
-    if (cudaGetLastError() != cudaSuccess) return APSPIE_ERR_CUDA;
+  return APSPIE_OK;
+}
+
+extern "C" int apspie_bfs_noalloc_status(void *stream, int32_t *d_status) {
+  using namespace apspie;
+  if (!d_status) return APSPIE_ERR_INVALID;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return APSPIE_ERR_CUDA;
   }
+  unsigned char *base = nullptr;
+  int grid = 0;
+  int rc = noalloc_setup(dev, &base, &grid);
+  if (rc) return rc;
+  // the status word of the one scratch array's BfsState, read after the
+  // traversals queued before it on this stream
+  bfs_write_status<<<1, 1, 0, (cudaStream_t)stream>>>((const BfsState *)base, d_status);
+  if (cudaGetLastError() != cudaSuccess) return APSPIE_ERR_CUDA;
   return APSPIE_OK;
 }
 

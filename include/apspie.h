@@ -140,17 +140,21 @@ int apspie_bfs_get_trace(apspie_ctx ctx, int max_levels, int *n_out,
  * device address (and may load the library's device code); make that first
  * call before any stream capture.  All calls share the one array, so calls
  * that overlap on the GPU (other streams, other host threads) race; run them
- * one after another.  d_status (device memory, may be NULL) receives the
- * run's status once it has finished, stream-ordered and without a host
- * synchronisation: 0, or APSPIE_ERR_TIMEOUT when a bounded grid-barrier wait
- * gave up (the depths are then incomplete).  The array's address is cached
- * per CUDA context (a driver-API context of the caller's, or the device's
- * primary context, which cudaDeviceReset replaces).  Statistics are not
- * reported.  No counterpart in the reference. */
+ * one after another.  The array's address is cached per CUDA context (a
+ * driver-API context of the caller's, or the device's primary context, which
+ * cudaDeviceReset replaces).  Statistics are not reported; the run's status
+ * is read with apspie_bfs_noalloc_status.  No counterpart in the reference. */
 int apspie_bfs_noalloc(void *stream, int src, int64_t nnz, int m,
                        const int *d_ptr, const int *d_ind, const int *d_tptr,
-                       const int *d_tind, int32_t *d_depth, int max_levels,
-                       int32_t *d_status);
+                       const int *d_tind, int32_t *d_depth, int max_levels);
+/* Status of the last apspie_bfs_noalloc on the current device: enqueues on
+ * `stream` a copy of its status word into d_status (one int of device
+ * memory), stream-ordered and without a host synchronisation -- 0, or
+ * APSPIE_ERR_TIMEOUT when a bounded grid-barrier wait gave up (the depths are
+ * then incomplete).  Enqueue it on the traversal's stream, after the
+ * traversal and before the next apspie_bfs_noalloc on the device: every call
+ * shares the one status word.  Allocates nothing. */
+int apspie_bfs_noalloc_status(void *stream, int32_t *d_status);
 
 /* Direction-switch thresholds (Beamer's alpha, beta; defaults 14 and 24):
  * push -> pull when frontier edges * alpha > unexplored edges, pull -> push

@@ -7,11 +7,11 @@ fixed device array (at most 2^20 vertices, 2^24 edges).  The test calls it
 through the C ABI and checks it against apspie_bfs, the entry point that
 draws scratch from a context workspace: BFS depths are integers, so the
 tolerance is zero.  Two calls in a row on the same array show that the
-contents left by one call do not leak into the next.  The optional status
-word reports 0 for a finished traversal and APSPIE_ERR_TIMEOUT when a
-bounded grid-barrier wait gave up (made to happen by a test hook that makes
-one block leave before the barrier; the others' wait runs out, nothing
-faults or hangs).
+contents left by one call do not leak into the next.  The status word,
+copied out by apspie_bfs_noalloc_status after a traversal, reports 0 for a
+finished traversal and APSPIE_ERR_TIMEOUT when a bounded grid-barrier wait
+gave up (made to happen by a test hook that makes one block leave before
+the barrier; the others' wait runs out, nothing faults or hangs).
 
 The file name sorts last so that a run stopping at the first failure has
 already run every other test."""
@@ -32,9 +32,14 @@ def _p(t):
 
 
 def _noalloc(lib, stream, g, src, out, tptr, tind, max_levels=0, status=None):
-    return lib.apspie_bfs_noalloc(C.c_void_p(stream.cuda_stream), int(src), int(g.nnz), int(g.m),
-                                  _p(g.ptr), _p(g.ind), _p(tptr), _p(tind), _p(out),
-                                  int(max_levels), _p(status))
+    """The traversal, then (status given) its status word copied to `status`
+    on the same stream."""
+    rc = lib.apspie_bfs_noalloc(C.c_void_p(stream.cuda_stream), int(src), int(g.nnz), int(g.m),
+                                _p(g.ptr), _p(g.ind), _p(tptr), _p(tind), _p(out),
+                                int(max_levels))
+    if rc == 0 and status is not None:
+        rc = lib.apspie_bfs_noalloc_status(C.c_void_p(stream.cuda_stream), _p(status))
+    return rc
 
 
 @pytest.mark.parametrize("symmetric", [True, False])
@@ -81,12 +86,14 @@ def test_noalloc_rejects_sizes_beyond_the_limit():
     out = torch.empty(1, dtype=torch.int32, device="cuda")
     # more vertices than the array holds: refused before anything is launched
     rc = lib.apspie_bfs_noalloc(C.c_void_p(stream.cuda_stream), 0, 0, (1 << 20) + 1, _p(ptr),
-                                None, None, None, _p(out), 0, None)
+                                None, None, None, _p(out), 0)
     assert rc == APSPIE_ERR_TOO_LARGE
     rc = lib.apspie_bfs_noalloc(C.c_void_p(stream.cuda_stream), 0, (1 << 24) + 1, 1, _p(ptr),
-                                _p(ptr), None, None, _p(out), 0, None)
+                                _p(ptr), None, None, _p(out), 0)
     assert rc == APSPIE_ERR_TOO_LARGE
     assert lib.apspie_status_string(rc) == b"input exceeds the fixed scratch size"
+    # the status copy needs somewhere to write: refused, nothing launched
+    assert lib.apspie_bfs_noalloc_status(C.c_void_p(stream.cuda_stream), None) == 1
 
 
 def test_noalloc_bfs_inside_a_cuda_graph():
