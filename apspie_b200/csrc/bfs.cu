@@ -34,7 +34,6 @@ namespace {
 
 constexpr int kBfsThreads = 512;
 constexpr int kProbe = 1;         // in-neighbours a lane probes per round in a pull level
-constexpr int kScanUnroll = 4;    // depth words a warp loads at once when re-queuing a frontier
 constexpr int kTraceLevels = 64;  // levels recorded in the per-run trace
 
 struct LevelTrace {

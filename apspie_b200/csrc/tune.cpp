@@ -235,6 +235,7 @@ int apspie_autotune_spmspv(apspie_ctx ctx, int m, int64_t nnz, const int *d_ptr,
                            const float *d_val, int *d_xind_scratch, float *d_xval_scratch,
                            int *d_yind_scratch, float *d_yval_scratch, double *factor_out) {
   return api_guard([&]() -> int {
+    (void)d_xval_scratch;  // the frontiers are timed with unit values: not written
     APSPIE_CHECK_CTX(ctx);
     if (m <= 0 || !d_xind_scratch || !d_yind_scratch || !d_yval_scratch || !factor_out)
       return set_error(ctx, APSPIE_ERR_INVALID, "apspie_autotune_spmspv: bad arguments");

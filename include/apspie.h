@@ -438,7 +438,9 @@ int apspie_autotune_bfs(apspie_ctx ctx, int nsrc, const int *h_src, int64_t nnz,
                         float *ms_out);
 /* Finds the frontier density at which the SpMSpV bitmap path beats the
  * radix-sort path on this matrix and sets the context's sort factor (see
- * apspie_spmspv_set_params).  Scratch: m ints (x), m ints + m floats (y). */
+ * apspie_spmspv_set_params).  Scratch: m ints (x), m ints + m floats (y);
+ * the frontiers are timed with unit values, so d_xval_scratch is not
+ * written and may be NULL. */
 int apspie_autotune_spmspv(apspie_ctx ctx, int m, int64_t nnz, const int *d_ptr,
                            const int *d_ind, const float *d_val,
                            int *d_xind_scratch, float *d_xval_scratch,
