@@ -123,6 +123,8 @@ def csr_transpose(ctx: Context, m: int, n: int, ptr, ind, val=None):
     import torch
     dev = ptr.device
     nnz = int(ind.numel())
+    _row(ptr, m + 1, "row offsets")
+    _row(val, nnz, "values")
     tptr = torch.empty(n + 1, dtype=torch.int32, device=dev)
     tind = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
     tval = torch.empty(max(nnz, 1), dtype=torch.float32, device=dev)
@@ -136,6 +138,7 @@ def bfs_prepare(ctx: Context, g):
     """Pull-ordered in-adjacency of g (apspie_bfs_prepare): sets g.tptr /
     g.tind, which bfs() then pulls over."""
     import torch
+    _graph(g)
     dev = g.ptr.device
     tptr = torch.empty(g.m + 1, dtype=torch.int32, device=dev)
     tind = torch.empty(max(g.nnz, 1), dtype=torch.int32, device=dev)
@@ -220,6 +223,7 @@ def sssp_prepare(ctx: Context, g):
     per weight array present), kept on g; sssp() then runs push/pull rounds
     over it (apspie_sssp_*_pull)."""
     import torch
+    _graph(g)
     g.extra["sssp_in"] = {}
     for kind, w in (("u32", g.w_u32), ("f32", g.w_f32)):
         if w is None:
@@ -337,9 +341,10 @@ def spmspv_set_params(ctx: Context, sort_factor: float = 4.0) -> None:
 
 
 def _csr(m, n, ptr, ind, val) -> Csr:
-    return Csr(int(m), int(n), int(ind.numel()) if ind is not None else 0,
-               _p(ptr), _p(ind),
-               _p(val))
+    nnz = int(ind.numel()) if ind is not None else 0
+    _row(ptr, int(m) + 1, "row offsets")
+    _row(val, nnz, "values")
+    return Csr(int(m), int(n), nnz, _p(ptr), _p(ind), _p(val))
 
 
 def spmv(ctx: Context, m: int, ptr, ind, val, x, semiring: int = 0, y=None):
@@ -350,6 +355,9 @@ def spmv(ctx: Context, m: int, ptr, ind, val, x, semiring: int = 0, y=None):
     if y is None:
         y = torch.empty(m, dtype=torch.float32, device=ptr.device)
     nnz = int(ind.numel()) if ind is not None else 0
+    _row(ptr, m + 1, "row offsets")
+    _row(val, nnz, "values")
+    _row(y, m, "y")
     check(lib.apspie_spmv(ctx.handle, int(semiring), int(m), nnz, _p(ptr), _p(ind), _p(val),
                           _p(x), _p(y)), ctx.handle, "apspie_spmv")
     return y
@@ -380,6 +388,7 @@ def spgemm_numeric(ctx: Context, A, B, ptr, ind, val):
     """Numeric phase of C = A * B into caller buffers ind / val (nnz(C)
     entries each), stream-ordered, no synchronisation."""
     a, b = _csr(*A), _csr(*B)
+    _row(ptr, a.m + 1, "C row offsets")
     check(lib.apspie_spgemm_numeric(ctx.handle, C.byref(a), C.byref(b), _p(ptr), _p(ind),
                                     _p(val)), ctx.handle, "apspie_spgemm_numeric")
 
@@ -444,6 +453,7 @@ def weights_device(ctx: Context, g, seed: int = 7, lo: int = 1, hi: int = 255):
     """graph.weights_u32 / weights_f32 computed on the device for a
     DeviceGraph: sets g.w_u32 (uint32 bits in an int32 tensor) and g.w_f32."""
     import torch
+    _graph(g)
     w = torch.empty(max(g.nnz, 1), dtype=torch.int32, device=g.ptr.device)
     wf = torch.empty(max(g.nnz, 1), dtype=torch.float32, device=g.ptr.device)
     check(lib.apspie_gen_weights_u32_device(ctx.handle, int(g.m), _p(g.ptr), _p(g.ind), seed, lo,
@@ -458,6 +468,7 @@ def tc_prepare(ctx: Context, g):
     """Degree-ordered strict lower triangle of a symmetric graph:
     returns (perm, Lptr, Lind) device tensors."""
     import torch
+    _graph(g)
     dev = g.ptr.device
     perm = torch.empty(g.m, dtype=torch.int32, device=dev)
     lp = torch.empty(g.m + 1, dtype=torch.int32, device=dev)
@@ -470,6 +481,7 @@ def tc_prepare(ctx: Context, g):
 
 def triangle_count(ctx: Context, m: int, lptr, lind) -> int:
     """Masked hash SpGEMM (L*L).*L summed in int64 (test/tc/main.cu:243-261)."""
+    _row(lptr, int(m) + 1, "L row offsets")
     out = C.c_int64()
     check(lib.apspie_tc(ctx.handle, int(m), int(lind.numel()), _p(lptr), _p(lind),
                         C.byref(out)), ctx.handle, "apspie_tc")
@@ -498,7 +510,9 @@ def _job_array(jobs: list[dict]):
     outs, keep = [], []
     arr = (Job * len(jobs))()
     for i, jd in enumerate(jobs):
-        g = jd["graph"]
+        g = _graph(jd["graph"])
+        if jd["type"] == "sssp":
+            _row(g.w_u32, g.nnz, "u32 weights")
         src = (C.c_int * len(jd["sources"]))(*[int(s) for s in jd["sources"]])
         keep.append(src)
         out = torch.empty((len(jd["sources"]), g.m), dtype=torch.int32, device=g.ptr.device)
@@ -586,6 +600,8 @@ def autotune_sssp(ctx: Context, g, sources) -> dict:
     import torch
     if g.w_u32 is None:
         raise ValueError("graph has no u32 weights")
+    _graph(g)
+    _row(g.w_u32, g.nnz, "u32 weights")
     dist = torch.empty(g.m, dtype=torch.int32, device=g.ptr.device)
     src = (C.c_int * len(sources))(*[int(s) for s in sources])
     tin = g.extra.get("sssp_in", {}).get("u32")
@@ -629,6 +645,7 @@ def autotune_bfs(ctx: Context, g, sources) -> dict:
     """Pick and cache the BFS direction thresholds and the persistent
     launch's blocks per SM for graph g."""
     import torch
+    _graph(g)
     depth = torch.empty(g.m, dtype=torch.int32, device=g.ptr.device)
     src = (C.c_int * len(sources))(*[int(s) for s in sources])
     sym = bool(getattr(g, "symmetric", False))
@@ -643,6 +660,8 @@ def autotune_bfs(ctx: Context, g, sources) -> dict:
 
 def autotune_spmspv(ctx: Context, g, val=None) -> float:
     import torch
+    _graph(g)
+    _row(val, g.nnz, "val")
     dev = g.ptr.device
     xi = torch.empty(g.m, dtype=torch.int32, device=dev)
     xv = torch.empty(g.m, dtype=torch.float32, device=dev)

@@ -84,3 +84,31 @@ def test_entry_points_refuse_short_outputs_and_host_tensors():
         ap.sssp(_Ctx(), g, 0, weights="f32")
     with pytest.raises(ValueError, match="CUDA tensor"):
         ap.mis(_Ctx(), g, torch.zeros(g.m, dtype=torch.int32))
+
+
+def test_matrix_entry_points_check_offsets_and_values():
+    z = lambda n, dt=torch.int32: torch.zeros(n, dtype=dt)
+    ctx = _Ctx()
+    # (m, n, ptr, ind, val): offsets must cover m + 1 rows, values every index
+    with pytest.raises(ValueError, match="row offsets"):
+        ap.spgemm(ctx, (4, 4, z(4), z(6), None), (4, 4, z(5), z(6), None))
+    with pytest.raises(ValueError, match="values"):
+        ap.spgemm(ctx, (4, 4, z(5), z(6), z(5, torch.float32)), (4, 4, z(5), z(6), None))
+    with pytest.raises(ValueError, match="row offsets"):
+        ap.csr_transpose(ctx, 4, 4, z(3), z(6))
+    with pytest.raises(ValueError, match="values"):
+        ap.spmv(ctx, 4, z(5), z(6), z(6, torch.float64), z(4, torch.float32))
+    with pytest.raises(ValueError, match="L row offsets"):
+        ap.triangle_count(ctx, 8, z(8), z(3))
+    # graph-taking builders and tuners check the graph first
+    bad = _Graph(ptr_len=3)
+    for call in (lambda: ap.bfs_prepare(ctx, bad), lambda: ap.tc_prepare(ctx, bad),
+                 lambda: ap.weights_device(ctx, bad), lambda: ap.autotune_bfs(ctx, bad, [0]),
+                 lambda: ap.autotune_sssp(ctx, bad, [0]),
+                 lambda: ap.batch_run(ctx, [{"type": "bfs", "graph": bad, "sources": [0]}])):
+        with pytest.raises(ValueError, match="graph row offsets"):
+            call()
+    g = _Graph()
+    g.w_u32 = z(g.nnz - 1)
+    with pytest.raises(ValueError, match="u32 weights"):
+        ap.batch_run(ctx, [{"type": "sssp", "graph": g, "sources": [0]}])
