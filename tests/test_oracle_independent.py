@@ -2,7 +2,8 @@
 reference code can run here (SpGEMM, whose reference arithmetic lives in
 absent moderngpu / cuSPARSE code; the SpMSpV semirings) and as a second pin
 for the rest (u32 / f64 SSSP against Dijkstra, BFS against an unweighted
-shortest path, triangle counts against trace(A^3) / 6).  SpGEMM and
+shortest path, triangle counts against trace(A^3) / 6, the MIS against
+Luby's rounds run in NumPy).  SpGEMM and
 plus-times SpMSpV sum in a different order here, so their values agree to
 1e-12 relative; everything else is exact."""
 import numpy as np
@@ -107,3 +108,41 @@ def test_tc_oracle_against_trace_of_a_cubed(scale):
     ref = int(round((A @ A).multiply(A).sum() / 6))
     _, lp, li = oracle.tc_build_lower(h.m, h.ptr, h.ind)
     assert oracle.tc_lower(h.m, lp, li) == ref
+
+
+def _luby_rounds(m, ptr, ind, prio):
+    """Luby's rounds, vectorised: every undecided vertex whose key (priority,
+    then id) beats all its undecided neighbours joins; their undecided
+    neighbours leave; repeat.  The reference's round loop
+    (src/spmspvMis.cuh:232-318) in plain NumPy, independent of the oracle's
+    one-pass greedy form."""
+    key = (prio.astype(np.uint64) << np.uint64(32)) | np.arange(m, dtype=np.uint64)
+    rows = np.repeat(np.arange(m), np.diff(ptr))
+    cols = ind.astype(np.int64)
+    off = rows != cols
+    state = np.full(m, -1)
+    for _ in range(m + 1):
+        und = state == -1
+        if not und.any():
+            break
+        live = off & und[rows] & und[cols]
+        nbmax = np.zeros(m, np.uint64)
+        np.maximum.at(nbmax, rows[live], key[cols[live]])
+        has_nb = np.zeros(m, bool)
+        has_nb[rows[live]] = True
+        join = und & (~has_nb | (key > nbmax))
+        state[join] = 1
+        drop = off & join[rows] & (state[cols] == -1)
+        state[cols[drop]] = 0
+    return state
+
+
+@pytest.mark.parametrize("which", ["rmat", "er", "grid"])
+def test_mis_oracle_against_luby_rounds(which):
+    g = {"rmat": lambda: ap.gen_rmat(11, 16, seed=6),
+         "er": lambda: ap.gen_er(1 << 11, 8, seed=6),
+         "grid": lambda: ap.gen_grid(40, 50)}[which]()
+    prio = ap.mt19937(5489, g.m)
+    ref = _luby_rounds(g.m, g.ptr, g.ind, prio)
+    assert np.all(ref >= 0)
+    np.testing.assert_array_equal(oracle.mis(g.m, g.ptr, g.ind, prio), ref)
